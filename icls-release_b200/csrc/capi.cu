@@ -1,0 +1,902 @@
+// capi.cu — the extern "C" entry points of include/icls_gpu.h and the host
+// orchestration of the ICLS time step on one B200.
+//
+// Each entry point replaces one subroutine of GeZhouyang/ICLS-release that
+// src/main.f90 calls (cited at the function), enqueuing its kernels on the
+// context's stream.  Host-side decisions that the reference takes on
+// globally reduced scalars (the mass-correction trigger, the divergence
+// abort, the NaN stop) read those scalars back; the reinitialisation early
+// exit is decided on the device.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "ctx.h"
+
+using namespace icls;
+
+struct icls_ctx {
+  Ctx c;
+};
+
+namespace {
+
+#define CK(x)                                  \
+  do {                                         \
+    cudaError_t e_ = (x);                      \
+    if (e_ != cudaSuccess) return ICLS_E_CUDA; \
+  } while (0)
+
+bool pow2(int n) { return n >= 4 && (n & (n - 1)) == 0; }
+
+int validate(const icls_config* c) {
+  if (!c) return ICLS_E_ARG;
+  if (!pow2(c->itot) || !pow2(c->jtot)) return ICLS_E_CONFIG;  // radix-2 FFT in x and y
+  if (c->itot > 4096 || c->jtot > 4096) return ICLS_E_CONFIG;
+  if (c->ktot < 6 || c->lmax < 1) return ICLS_E_CONFIG;
+  if (!(c->lx > 0 && c->ly > 0 && c->lz > 0 && c->timestep > 0)) return ICLS_E_CONFIG;
+  if (c->reinit_step < 1 || c->inflate_step < 1 || c->reinit_iter_max < 1) return ICLS_E_CONFIG;
+  if (c->ls_adv_space != ICLS_HOUC5 && c->ls_adv_space != ICLS_WENO5) return ICLS_E_CONFIG;
+  if (c->i_space != ICLS_HOUC5 && c->i_space != ICLS_WENO5) return ICLS_E_CONFIG;
+  if (c->precision != ICLS_FP64) return ICLS_E_UNSUPPORTED;
+  if (c->curvature_model != ICLS_CURV_STENCIL) return ICLS_E_UNSUPPORTED;
+  return ICLS_OK;
+}
+
+void fill_params(Ctx& c) {
+  const icls_config& f = c.cfg;
+  Params& P = c.P;
+  P.imax = f.itot; P.jmax = f.jtot; P.kmax = f.ktot;
+  P.i1 = P.imax + 1; P.j1 = P.jmax + 1; P.k1 = P.kmax + 1;
+  P.L = f.lmax;
+  P.nCx = P.imax + 2; P.nCy = P.jmax + 2; P.nCz = P.kmax + 2;
+  P.nLx = P.imax + 6; P.nLy = P.jmax + 6; P.nLz = P.kmax + 6;
+  P.nC = (long long)P.nCx * P.nCy * P.nCz;
+  P.nI = (long long)P.imax * P.jmax * P.kmax;
+  P.nL = (long long)P.nLx * P.nLy * P.nLz;
+  P.lx = f.lx; P.ly = f.ly; P.lz = f.lz;
+  // param.f90:37-41
+  P.dxi = f.itot / f.lx; P.dyi = f.jtot / f.ly; P.dzi = f.ktot / f.lz;
+  P.dx = 1. / P.dxi; P.dy = 1. / P.dyi; P.dz = 1. / P.dzi;
+  P.NB = 6. * P.dz;
+  P.pi = std::acos(-1.);
+  P.dt = f.timestep;
+  P.rho1 = f.rho1; P.rho2 = f.rho2; P.miu1 = f.miu1; P.miu2 = f.miu2;
+  P.rho0 = std::min(f.rho1, f.rho2);  // param.f90:63
+  P.visc = 1. / f.Re;                 // param.f90:73
+  P.iFr = f.iFr;
+  P.nondi = 1. / f.We;                // gfm.f90:40
+  P.g1 = f.g_unit[0]; P.g2 = f.g_unit[1]; P.g3 = f.g_unit[2];
+  P.v_lower = f.v_wall_lower; P.v_upper = f.v_wall_upper;
+  P.forceytot = f.constPoi ? -12. * P.visc / (f.lz * f.lz) : 0.;  // ab2.f90:104-110
+  P.TwoD = f.TwoD;
+  P.ls_adv_space = f.ls_adv_space; P.i_space = f.i_space;
+  P.ispeed_curv = (f.ispeed_dependence == ICLS_SPEED_CURV);
+}
+
+// init_matrix (init.f90:1587-1723): pseudo_inv_A = (A^T A)^-1 A^T of the
+// quadratic least-squares fit on the 27-point stencil; inverted by
+// Gauss-Jordan in long double.
+void init_matrix(Ctx& c) {
+  long double A[27][10];
+  int row = 0;
+  for (int dzs = -1; dzs <= 1; ++dzs)
+    for (int dys = -1; dys <= 1; ++dys)
+      for (int dxs = -1; dxs <= 1; ++dxs) {
+        long double a2 = (long double)(c.P.dx * dxs), a3 = (long double)(c.P.dy * dys),
+                    a4 = (long double)(c.P.dz * dzs);
+        long double* r = A[row++];
+        r[0] = 1; r[1] = a2; r[2] = a3; r[3] = a4;
+        r[4] = 0.5L * a2 * a2; r[5] = 0.5L * a3 * a3; r[6] = 0.5L * a4 * a4;
+        r[7] = a2 * a3; r[8] = a2 * a4; r[9] = a3 * a4;
+      }
+  long double M[10][20];
+  for (int r = 0; r < 10; ++r)
+    for (int q = 0; q < 10; ++q) {
+      long double s = 0;
+      for (int n = 0; n < 27; ++n) s += A[n][r] * A[n][q];
+      M[r][q] = s;
+      M[r][10 + q] = (r == q) ? 1 : 0;
+    }
+  for (int col = 0; col < 10; ++col) {
+    int piv = col;
+    for (int r = col + 1; r < 10; ++r)
+      if (fabsl(M[r][col]) > fabsl(M[piv][col])) piv = r;
+    if (piv != col)
+      for (int q = 0; q < 20; ++q) std::swap(M[col][q], M[piv][q]);
+    const long double d = M[col][col];
+    for (int q = 0; q < 20; ++q) M[col][q] /= d;
+    for (int r = 0; r < 10; ++r) {
+      if (r == col) continue;
+      const long double f = M[r][col];
+      if (f != 0)
+        for (int q = 0; q < 20; ++q) M[r][q] -= f * M[col][q];
+    }
+  }
+  for (int r = 0; r < 10; ++r)
+    for (int n = 0; n < 27; ++n) {
+      long double s = 0;
+      for (int q = 0; q < 10; ++q) s += M[r][10 + q] * A[n][q];
+      c.P10x27[r * 27 + n] = (double)s;
+    }
+}
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+  if (cudaMalloc((void**)p, n * sizeof(T) + 16) != cudaSuccess) return ICLS_E_NOMEM;
+  if (cudaMemset(*p, 0, n * sizeof(T) + 16) != cudaSuccess) return ICLS_E_CUDA;
+  return ICLS_OK;
+}
+
+#define AL(ptr, n)                  \
+  do {                              \
+    int rc_ = dalloc(&(ptr), (n));  \
+    if (rc_) return rc_;            \
+  } while (0)
+
+int allocate(Ctx& c) {
+  const Params& P = c.P;
+  for (double** f : {&c.u, &c.v, &c.w, &c.pnew, &c.pold, &c.p, &c.dudt, &c.dvdt, &c.dwdt, &c.px, &c.py, &c.pz,
+                     &c.pxold, &c.pyold, &c.pzold, &c.pjump, &c.miu, &c.rho, &c.jiemian, &c.curv, &c.recurv,
+                     &c.dheav, &c.kappa})
+    AL(*f, (size_t)P.nC);
+  for (int h = 0; h < 2; ++h) {
+    AL(c.duold[h], (size_t)P.nI); AL(c.dvold[h], (size_t)P.nI); AL(c.dwold[h], (size_t)P.nI);
+  }
+  for (double** f : {&c.rho_u, &c.rho_v, &c.rho_w, &c.ucc, &c.vcc, &c.wcc, &c.nrm_m, &c.ulc, &c.vlc, &c.wlc})
+    AL(*f, (size_t)P.nI);
+  c.lv.assign(P.L, nullptr);
+  for (int l = 0; l < P.L; ++l) AL(c.lv[l], (size_t)P.nL);
+  for (int s = 0; s < 4; ++s) AL(c.ls_scr[s], (size_t)P.nL);
+  AL(c.mask, (size_t)P.nI);
+  AL(c.d_nbcnt, (size_t)P.L);
+  AL(c.spec, (size_t)P.nI);
+  AL(c.twx, (size_t)P.imax);
+  AL(c.twy, (size_t)P.jmax);
+  AL(c.xyrt, (size_t)P.imax * P.jmax);
+  AL(c.zpiv, (size_t)P.nI);
+  AL(c.tri_a, (size_t)P.kmax + 1); AL(c.tri_b, (size_t)P.kmax + 1); AL(c.tri_c, (size_t)P.kmax + 1);
+  AL(c.partials, (size_t)kRedBlocks * std::max(P.L, 4) + (size_t)P.imax + 8);
+  AL(c.lpartials, (size_t)kRedBlocks);
+  AL(c.dsc, 1);
+  AL(c.dvol, (size_t)P.L); AL(c.dvol0, (size_t)P.L); AL(c.dmaxchk, (size_t)P.L);
+  CK(cudaMallocHost((void**)&c.h_vol, sizeof(double) * P.L));
+  CK(cudaMallocHost((void**)&c.h_sc, sizeof(DevScalars)));
+  CK(cudaEventCreateWithFlags(&c.ev_vol, cudaEventDisableTiming));
+  // normal%m = 1 outside the curvature band (interface.f90:44)
+  std::vector<double> ones((size_t)P.nI, 1.0);
+  CK(cudaMemcpy(c.nrm_m, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice));
+  c.inflated.assign(P.L, 0);
+  c.vol_dirty.assign(P.L, 0);
+  c.init_volume_h.assign(P.L, 0.);
+  return ICLS_OK;
+}
+
+void release(Ctx& c) {
+  for (double* f : {c.u, c.v, c.w, c.pnew, c.pold, c.p, c.dudt, c.dvdt, c.dwdt, c.px, c.py, c.pz, c.pxold,
+                    c.pyold, c.pzold, c.pjump, c.miu, c.rho, c.jiemian, c.curv, c.recurv, c.dheav, c.kappa,
+                    c.rho_u, c.rho_v, c.rho_w, c.ucc, c.vcc, c.wcc, c.nrm_m, c.ulc, c.vlc, c.wlc, c.spec,
+                    c.xyrt, c.zpiv, c.tri_a, c.tri_b, c.tri_c, c.partials, c.dvol, c.dvol0, c.dmaxchk})
+    if (f) cudaFree(f);
+  for (int h = 0; h < 2; ++h) {
+    if (c.duold[h]) cudaFree(c.duold[h]);
+    if (c.dvold[h]) cudaFree(c.dvold[h]);
+    if (c.dwold[h]) cudaFree(c.dwold[h]);
+  }
+  for (double* f : c.lv) if (f) cudaFree(f);
+  for (double* f : c.ls_scr) if (f) cudaFree(f);
+  if (c.mask) cudaFree(c.mask);
+  if (c.d_nbcnt) cudaFree(c.d_nbcnt);
+  if (c.twx) cudaFree(c.twx);
+  if (c.twy) cudaFree(c.twy);
+  if (c.lpartials) cudaFree(c.lpartials);
+  if (c.dsc) cudaFree(c.dsc);
+  if (c.h_vol) cudaFreeHost(c.h_vol);
+  if (c.h_sc) cudaFreeHost(c.h_sc);
+  if (c.ev_vol) cudaEventDestroy(c.ev_vol);
+  c.prof.release();
+  if (c.s) cudaStreamDestroy(c.s);
+}
+
+// field table: device pointer and element count
+double* field_ptr(Ctx& c, int id, int l, long long* n) {
+  const Params& P = c.P;
+  *n = P.nC;
+  switch (id) {
+    case ICLS_F_U: return c.u; case ICLS_F_V: return c.v; case ICLS_F_W: return c.w;
+    case ICLS_F_PNEW: return c.pnew; case ICLS_F_POLD: return c.pold; case ICLS_F_P: return c.p;
+    case ICLS_F_DUDT: return c.dudt; case ICLS_F_DVDT: return c.dvdt; case ICLS_F_DWDT: return c.dwdt;
+    case ICLS_F_PX: return c.px; case ICLS_F_PY: return c.py; case ICLS_F_PZ: return c.pz;
+    case ICLS_F_PXOLD: return c.pxold; case ICLS_F_PYOLD: return c.pyold; case ICLS_F_PZOLD: return c.pzold;
+    case ICLS_F_PJUMP: return c.pjump; case ICLS_F_MIU: return c.miu; case ICLS_F_RHO: return c.rho;
+    case ICLS_F_JIEMIAN: return c.jiemian; case ICLS_F_CURV: return c.curv;
+    default: break;
+  }
+  *n = P.nI;
+  switch (id) {
+    case ICLS_F_DUOLD: return c.duold[c.hist]; case ICLS_F_DVOLD: return c.dvold[c.hist];
+    case ICLS_F_DWOLD: return c.dwold[c.hist];
+    case ICLS_F_RHO_U: return c.rho_u; case ICLS_F_RHO_V: return c.rho_v; case ICLS_F_RHO_W: return c.rho_w;
+    case ICLS_F_UCC: return c.ucc; case ICLS_F_VCC: return c.vcc; case ICLS_F_WCC: return c.wcc;
+    case ICLS_F_NORMAL_M: return c.nrm_m;
+    default: break;
+  }
+  *n = P.nL;
+  if (id == ICLS_F_LVSET && l >= 1 && l <= P.L) return c.lv[l - 1];
+  return nullptr;
+}
+
+int check_launch() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? ICLS_OK : ICLS_E_CUDA;
+}
+
+// ----------------------------------------------------------- level set
+void update_materials(Ctx& c) {
+  for (int l = 0; l < c.P.L; ++l) launch_heaviside_drop(c, c.lv[l], l, l == 0);
+  launch_materials_final(c);
+  cudaMemcpyAsync(c.h_vol, c.dvol, sizeof(double) * c.P.L, cudaMemcpyDeviceToHost, c.s);
+  cudaEventRecord(c.ev_vol, c.s);
+  c.vol_pending = true;
+  std::fill(c.vol_dirty.begin(), c.vol_dirty.end(), 0);
+}
+
+void tube_construction(Ctx& c, int l) {
+  cudaMemsetAsync(c.d_nbcnt + l, 0, sizeof(long long), c.s);
+  launch_tube(c, c.lv[l], c.ls_scr[0], c.d_nbcnt + l);
+  std::swap(c.lv[l], c.ls_scr[0]);
+}
+
+// SSP-RK3 of ls_advection / inflation (levelset.f90:235-243, 558-565)
+void rk3(Ctx& c, int l, int scheme, const double* vu, const double* vv, const double* vw) {
+  const double dt = c.dt;
+  double* phi0 = c.lv[l];
+  double* s1 = c.ls_scr[1];
+  double* s2 = c.ls_scr[2];
+  launch_adv_stage(c, scheme, 1, phi0, phi0, 1., 0., 1. * dt, vu, vv, vw, s1);
+  launch_adv_stage(c, scheme, 0, phi0, s1, 3. / 4., 1. / 4., 1. / 4. * dt, vu, vv, vw, s2);
+  launch_adv_stage(c, scheme, 0, phi0, s2, 1. / 3., 2. / 3., 2. / 3. * dt, vu, vv, vw, s1);
+  std::swap(c.lv[l], c.ls_scr[1]);
+}
+
+void ls_advection(Ctx& c, int l) { rk3(c, l, c.cfg.ls_adv_space, c.ucc, c.vcc, c.wcc); }
+
+// inflation (levelset.f90:407-582)
+void inflation(Ctx& c, int l) {
+  launch_curvature(c, c.lv[l], c.kappa, c.nrm_m);
+  launch_inflate_sums(c, c.lv[l], l);
+  launch_inflate_vel(c);
+  rk3(c, l, c.cfg.i_space, c.ulc, c.vlc, c.wlc);
+  c.inflated[l] = 1;
+  c.vol_dirty[l] = 1;
+  ++c.last_inflated;
+}
+
+int volume_of(Ctx& c, int l, double* v) {
+  if (c.vol_dirty[l]) {
+    CK(cudaMemcpyAsync(v, c.dvol + l, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    return ICLS_OK;
+  }
+  if (c.vol_pending) {
+    CK(cudaEventSynchronize(c.ev_vol));
+    c.vol_pending = false;
+  }
+  *v = c.h_vol[l];
+  return ICLS_OK;
+}
+
+// ls_mass_correction (levelset.f90:377-400)
+int ls_mass_correction(Ctx& c, int istep, int l) {
+  c.inflated[l] = 0;
+  if (istep % c.cfg.inflate_step == 0) {
+    double vol;
+    int rc = volume_of(c, l, &vol);
+    if (rc) return rc;
+    const double v0 = c.init_volume_h[l];
+    const double massloss = (vol - v0) / v0;
+    if (std::fabs(massloss) > 1e-5) inflation(c, l);
+  }
+  return ICLS_OK;
+}
+
+// ls_reinit, WENO5/RK3 (levelset.f90:619-882); the early exit on
+// residual < dz**5 is decided on the device (k_reinit_check)
+void ls_reinit(Ctx& c, int l) {
+  const int maxiter = c.cfg.reinit_iter_max;
+  const double dz = c.P.dz;
+  const double dtau = 0.5 * dz;
+  const double thr = dz * dz * dz * dz * dz;
+  double* orig = c.lv[l];
+  double* X = orig;
+  double* A = c.ls_scr[0];
+  double* B = c.ls_scr[1];
+  double* Y = c.ls_scr[2];
+  double* Yalt = c.ls_scr[3];
+  launch_reinit_reset(c, maxiter);
+  for (int it = 1; it <= maxiter; ++it) {
+    launch_reinit_stage(c, 1, X, X, orig, dtau, A, 1);
+    launch_reinit_stage(c, 2, X, A, orig, dtau, B, 1);
+    launch_reinit_stage(c, 3, X, B, orig, dtau, Y, 1);
+    launch_reinit_check(c, it, maxiter, thr);
+    X = Y;
+    std::swap(Y, Yalt);
+    if (Y == orig) std::swap(Y, Yalt);
+  }
+  // X holds phi_new; make it the drop's buffer and recycle the original
+  for (int s = 0; s < 4; ++s)
+    if (c.ls_scr[s] == X) {
+      c.ls_scr[s] = orig;
+      break;
+    }
+  c.lv[l] = X;
+}
+
+int ls_main(Ctx& c, int istep) {
+  c.last_inflated = 0;
+  for (int l = 0; l < c.P.L; ++l) {
+    tube_construction(c, l);
+    ls_advection(c, l);
+    if (c.cfg.mass_correction) {
+      int rc = ls_mass_correction(c, istep, l);
+      if (rc) return rc;
+    }
+    if (c.cfg.re_initialization && istep % c.cfg.reinit_step == 0) ls_reinit(c, l);
+  }
+  update_materials(c);
+  return check_launch();
+}
+
+// gfm4p, GFM/'del' (gfm.f90:17-267); ipot is evaluated by icls_ipot
+void gfm4p(Ctx& c) {
+  std::swap(c.px, c.pxold);
+  std::swap(c.py, c.pyold);
+  std::swap(c.pz, c.pzold);
+  const size_t bytes = sizeof(double) * (size_t)c.P.nC;
+  cudaMemsetAsync(c.px, 0, bytes, c.s);
+  cudaMemsetAsync(c.py, 0, bytes, c.s);
+  cudaMemsetAsync(c.pz, 0, bytes, c.s);
+  cudaMemsetAsync(c.pjump, 0, bytes, c.s);
+  for (int l = 0; l < c.P.L; ++l) {
+    launch_curvature(c, c.lv[l], c.curv, c.nrm_m);
+    if (!c.cfg.TwoD) {
+      launch_recurvature(c, c.lv[l], c.curv, c.recurv);
+      std::swap(c.curv, c.recurv);
+    }
+    launch_jumps(c, c.lv[l], c.curv, l == 0);
+  }
+}
+
+int read_scalars(Ctx& c) {
+  CK(cudaMemcpyAsync(c.h_sc, c.dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  return ICLS_OK;
+}
+
+int chkdiv(Ctx& c, int istep, double* divtot, double* divmax, int* ijk) {
+  launch_chkdiv(c);
+  int rc = read_scalars(c);
+  if (rc) return rc;
+  if (divtot) *divtot = c.h_sc->divtot;
+  if (divmax) *divmax = c.h_sc->divmax;
+  if (ijk) {
+    long long q = c.h_sc->divloc;
+    if (q < 0) {
+      ijk[0] = ijk[1] = ijk[2] = 0;
+    } else {
+      ijk[0] = (int)(q % c.P.imax) + 1;
+      ijk[1] = (int)((q / c.P.imax) % c.P.jmax) + 1;
+      ijk[2] = (int)(q / ((long long)c.P.imax * c.P.jmax)) + 1;
+    }
+  }
+  if (c.h_sc->divmax > 1e-12 && istep != 0) return ICLS_E_DIVERGENCE;  // chkdiv.f90:60-87
+  return ICLS_OK;
+}
+
+}  // namespace
+
+// ======================================================================== C
+extern "C" {
+
+void icls_config_default(icls_config* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->itot = c->jtot = c->ktot = 32;
+  c->lmax = 1;
+  c->lx = c->ly = c->lz = 1.0;
+  c->timestep = 5e-4;
+  c->rho1 = 1.0; c->rho2 = 10.0; c->miu1 = 1.0; c->miu2 = 0.1;
+  c->Re = 10.0; c->We = 1.0; c->iFr = 0.0;
+  c->TwoD = 0; c->constPoi = 0; c->solveLS = 1;
+  c->ls_adv_space = ICLS_HOUC5;
+  c->re_initialization = 1; c->reinit_step = 20; c->reinit_iter_max = 1;
+  c->mass_correction = 1; c->inflate_step = 20;
+  c->ispeed_dependence = ICLS_SPEED_CURV; c->i_space = ICLS_HOUC5;
+  c->ioutchk = 20;
+  c->precision = ICLS_FP64; c->curvature_model = ICLS_CURV_STENCIL;
+  c->mlp_fallback_tol = 0.02;
+}
+
+int icls_status_string(int code, char* buf, int n) {
+  static const char* names[] = {"ok", "invalid or unsupported configuration", "CUDA error",
+                                "NaN in vnew(1,1,1)", "max divergence above 1e-12", "bad argument",
+                                "device allocation failed", "context not initialised",
+                                "option not built into this library"};
+  const char* s = (code >= 0 && code <= 8) ? names[code] : "unknown status";
+  if (buf && n > 0) {
+    std::strncpy(buf, s, (size_t)n - 1);
+    buf[n - 1] = 0;
+  }
+  return ICLS_OK;
+}
+
+int icls_create(const icls_config* cfg, icls_ctx** out) {
+  if (!out) return ICLS_E_ARG;
+  *out = nullptr;
+  int rc = validate(cfg);
+  if (rc) return rc;
+  icls_ctx* h = new (std::nothrow) icls_ctx();
+  if (!h) return ICLS_E_NOMEM;
+  Ctx& c = h->c;
+  c.cfg = *cfg;
+  fill_params(c);
+  if (cudaGetDevice(&c.device) != cudaSuccess || cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return ICLS_E_CUDA;
+  }
+  rc = allocate(c);
+  if (rc) {
+    release(c);
+    delete h;
+    return rc;
+  }
+  c.dt = cfg->timestep;
+  *out = h;
+  return ICLS_OK;
+}
+
+int icls_destroy(icls_ctx* h) {
+  if (!h) return ICLS_E_ARG;
+  cudaStreamSynchronize(h->c.s);
+  release(h->c);
+  delete h;
+  return ICLS_OK;
+}
+
+int icls_field_bounds(const icls_ctx* h, int id, int lo[3], int hi[3]) {
+  if (!h || !lo || !hi) return ICLS_E_ARG;
+  const Params& P = h->c.P;
+  int kind;
+  switch (id) {
+    case ICLS_F_DUOLD: case ICLS_F_DVOLD: case ICLS_F_DWOLD: case ICLS_F_RHO_U: case ICLS_F_RHO_V:
+    case ICLS_F_RHO_W: case ICLS_F_UCC: case ICLS_F_VCC: case ICLS_F_WCC: case ICLS_F_NORMAL_M:
+      kind = 1; break;
+    case ICLS_F_LVSET: kind = 2; break;
+    default:
+      if (id < 0 || id >= ICLS_F_COUNT) return ICLS_E_ARG;
+      kind = 0;
+  }
+  const int l0 = kind == 0 ? 0 : (kind == 1 ? 1 : -2);
+  const int pad = kind == 0 ? 1 : (kind == 1 ? 0 : 3);
+  lo[0] = lo[1] = lo[2] = l0;
+  hi[0] = P.imax + pad; hi[1] = P.jmax + pad; hi[2] = P.kmax + pad;
+  return ICLS_OK;
+}
+
+int icls_upload_field(icls_ctx* h, int id, int l, const double* host) {
+  if (!h || !host) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  long long n;
+  double* d = field_ptr(c, id, l, &n);
+  if (!d) return ICLS_E_ARG;
+  CK(cudaMemcpyAsync(d, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  return ICLS_OK;
+}
+
+int icls_download_field(icls_ctx* h, int id, int l, double* host) {
+  if (!h || !host) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  long long n;
+  double* d = field_ptr(c, id, l, &n);
+  if (!d) return ICLS_E_ARG;
+  CK(cudaMemcpyAsync(host, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  return ICLS_OK;
+}
+
+int icls_get_scalars(icls_ctx* h, icls_scalars* out) {
+  if (!h || !out) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  int rc = read_scalars(c);
+  if (rc) return rc;
+  out->time = c.time;
+  out->dt = c.dt;
+  out->rho_avr = c.h_sc->rho_avr;
+  out->v_bulk = c.h_sc->v_bulk;
+  out->norm_old = c.h_sc->norm;
+  out->reinit_residual = c.h_sc->residual;
+  out->reinit_iters = c.h_sc->reinit_iters;
+  out->last_inflated = c.last_inflated;
+  out->maxchk_glb = 0.;
+  if (c.cfg.mass_correction && c.inflated[c.P.L - 1]) {
+    CK(cudaMemcpy(&out->maxchk_glb, c.dmaxchk + c.P.L - 1, sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  return ICLS_OK;
+}
+
+int icls_get_volumes(icls_ctx* h, double* volume, double* init_volume) {
+  if (!h) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  if (volume) {
+    CK(cudaMemcpyAsync(volume, c.dvol, sizeof(double) * c.P.L, cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+  }
+  if (init_volume)
+    for (int l = 0; l < c.P.L; ++l) init_volume[l] = c.init_volume_h[l];
+  return ICLS_OK;
+}
+
+int icls_synchronize(icls_ctx* h) {
+  if (!h) return ICLS_E_ARG;
+  CK(cudaStreamSynchronize(h->c.s));
+  return check_launch();
+}
+
+// init_program, begin=0, GFM (init.f90:22-117)
+int icls_init_program(icls_ctx* h) {
+  if (!h) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  init_matrix(c);
+  set_pseudo_inverse(c.P10x27, c.s);
+  poisson_setup(c);
+  c.dt = c.cfg.timestep;
+  c.time = 0.;
+  CK(cudaMemsetAsync(c.dsc, 0, sizeof(DevScalars), c.s));
+  launch_bounduvw(c, c.u, c.v, c.w);
+  launch_bounduvw(c, c.dudt, c.dvdt, c.dwdt);
+  for (int l = 0; l < c.P.L; ++l) launch_boundmls(c, c.lv[l]);
+  launch_boundp(c, c.pnew);
+  launch_average_vel(c);
+  update_materials(c);
+  CK(cudaMemcpyAsync(c.dvol0, c.dvol, sizeof(double) * c.P.L, cudaMemcpyDeviceToDevice, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  c.vol_pending = false;
+  for (int l = 0; l < c.P.L; ++l) c.init_volume_h[l] = c.h_vol[l];
+  c.hist = 0;
+  launch_mom_main(c, c.duold[0], c.dvold[0], c.dwold[0]);
+  const size_t bytes = sizeof(double) * (size_t)c.P.nC;
+  CK(cudaMemcpyAsync(c.pold, c.pnew, bytes, cudaMemcpyDeviceToDevice, c.s));
+  CK(cudaMemcpyAsync(c.pxold, c.px, bytes, cudaMemcpyDeviceToDevice, c.s));
+  CK(cudaMemcpyAsync(c.pyold, c.py, bytes, cudaMemcpyDeviceToDevice, c.s));
+  CK(cudaMemcpyAsync(c.pzold, c.pz, bytes, cudaMemcpyDeviceToDevice, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  c.initialised = true;
+  return check_launch();
+}
+
+#define NEED(h)                                  \
+  do {                                           \
+    if (!(h)) return ICLS_E_ARG;                 \
+    if (!(h)->c.initialised) return ICLS_E_STATE; \
+  } while (0)
+#define LARG(h, l) \
+  if ((l) < 1 || (l) > (h)->c.P.L) return ICLS_E_ARG
+
+int icls_ls_main(icls_ctx* h, int istep) {
+  NEED(h);
+  return ls_main(h->c, istep);
+}
+
+int icls_average_stream_vel(icls_ctx* h, double* v_bulk) {
+  NEED(h);
+  launch_stream_vel(h->c);
+  if (v_bulk) {
+    int rc = read_scalars(h->c);
+    if (rc) return rc;
+    *v_bulk = h->c.h_sc->v_bulk;
+  }
+  return check_launch();
+}
+
+int icls_ab2(icls_ctx* h) {
+  NEED(h);
+  launch_ab2(h->c);
+  return check_launch();
+}
+
+int icls_fillps(icls_ctx* h) {
+  NEED(h);
+  launch_fillps(h->c, 0);
+  return check_launch();
+}
+
+int icls_gfm4p(icls_ctx* h) {
+  NEED(h);
+  gfm4p(h->c);
+  return check_launch();
+}
+
+int icls_add_pjump(icls_ctx* h) {
+  NEED(h);
+  launch_add_pjump(h->c);
+  return check_launch();
+}
+
+int icls_solver2d(icls_ctx* h) {
+  NEED(h);
+  launch_solver2d(h->c, 0);
+  return check_launch();
+}
+
+int icls_boundp(icls_ctx* h, int id) {
+  if (!h) return ICLS_E_ARG;
+  long long n;
+  double* d = field_ptr(h->c, id, 1, &n);
+  if (!d || n != h->c.P.nC) return ICLS_E_ARG;
+  launch_boundp(h->c, d);
+  return check_launch();
+}
+
+int icls_correc(icls_ctx* h) {
+  NEED(h);
+  launch_correc(h->c, 0);
+  return check_launch();
+}
+
+int icls_bounduvw(icls_ctx* h, int id) {
+  if (!h) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  if (id == ICLS_F_U) launch_bounduvw(c, c.u, c.v, c.w);
+  else if (id == ICLS_F_DUDT) launch_bounduvw(c, c.dudt, c.dvdt, c.dwdt);
+  else return ICLS_E_ARG;
+  return check_launch();
+}
+
+int icls_pressure_update(icls_ctx* h, int istep, int begin) {
+  NEED(h);
+  launch_pressure_update(h->c, istep == begin + 1);
+  return check_launch();
+}
+
+int icls_average_vel_at_center(icls_ctx* h) {
+  if (!h) return ICLS_E_ARG;
+  launch_average_vel(h->c);
+  return check_launch();
+}
+
+int icls_max_vel_at_center(icls_ctx* h, double* vel_max) {
+  if (!h || !vel_max) return ICLS_E_ARG;
+  launch_maxvel(h->c);
+  int rc = read_scalars(h->c);
+  if (rc) return rc;
+  *vel_max = h->c.h_sc->velmax;
+  return ICLS_OK;
+}
+
+int icls_chkdiv(icls_ctx* h, int istep, double* divtot, double* divmax, int ijk[3]) {
+  if (!h) return ICLS_E_ARG;
+  return chkdiv(h->c, istep, divtot, divmax, ijk);
+}
+
+// chkdt (chkdt.f90:11-105): maxima on the device, the rest on the host
+int icls_chkdt(icls_ctx* h, double* dtmax) {
+  if (!h || !dtmax) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  launch_chkdt(c);
+  int rc = read_scalars(c);
+  if (rc) return rc;
+  const Params& P = c.P;
+  const icls_config& f = c.cfg;
+  const double rho_avr = c.h_sc->rho_avr;
+  double speed_conv = (c.h_sc->umax / P.dx + c.h_sc->vmax / P.dy) + c.h_sc->wmax / P.dz;
+  const double* g = f.g_unit;
+  double gg[6] = {std::fabs(f.iFr * (1. - rho_avr / f.rho1) * g[0]), std::fabs(f.iFr * (1. - rho_avr / f.rho2) * g[0]),
+                  std::fabs(f.iFr * (1. - rho_avr / f.rho1) * g[1]), std::fabs(f.iFr * (1. - rho_avr / f.rho2) * g[1]),
+                  std::fabs(f.iFr * (1. - rho_avr / f.rho1) * g[2]), std::fabs(f.iFr * (1. - rho_avr / f.rho2) * g[2])};
+  double g_max = gg[0];
+  for (int q = 1; q < 6; ++q) g_max = std::max(g_max, gg[q]);
+  const double h_min = std::min(std::min(P.dx, P.dy), P.dz);
+  const double speed_grav = std::sqrt(g_max / h_min);
+  const double v1 = std::max(f.miu1 / f.rho1, f.miu2 / f.rho2) * P.visc;
+  const double v2 = (2. / (P.dx * P.dx) + 2. / (P.dy * P.dy)) + 2. / (P.dz * P.dz);
+  const double speed_visc = v1 * v2;
+  const double curv_max = f.TwoD ? 1. / h_min : 2. / h_min;
+  const double speed_surf = std::sqrt(curv_max / (f.We * P.rho0 * (h_min * h_min)));
+  const double s1 = speed_conv + speed_visc;
+  const double speed =
+      (s1 + std::sqrt((s1 * s1 + 4. * (speed_grav * speed_grav)) + 4. * (speed_surf * speed_surf))) / 2.;
+  *dtmax = 0.5 / speed;
+  return ICLS_OK;
+}
+
+int icls_ipot(icls_ctx* h, double* dmin) {
+  NEED(h);
+  Ctx& c = h->c;
+  const int L = c.P.L;
+  if (L < 2) {
+    if (dmin) dmin[0] = 0.;
+    return ICLS_OK;
+  }
+  double* dev = nullptr;
+  CK(cudaMallocAsync((void**)&dev, sizeof(double) * L * L, c.s));
+  CK(cudaMemsetAsync(dev, 0xFF, sizeof(double) * L * L, c.s));
+  launch_ipot(c, dev);
+  std::vector<unsigned long long> bits((size_t)L * L);
+  CK(cudaMemcpyAsync(bits.data(), dev, sizeof(double) * L * L, cudaMemcpyDeviceToHost, c.s));
+  CK(cudaFreeAsync(dev, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  std::vector<double> dt((size_t)L * L, 0.);
+  for (size_t q = 0; q < bits.size(); ++q) {
+    unsigned long long b = bits[q];
+    b = (b & 0x8000000000000000ull) ? (b & 0x7FFFFFFFFFFFFFFFull) : ~b;
+    double v;
+    std::memcpy(&v, &b, sizeof(v));
+    dt[q] = v;
+  }
+  if (dmin) {
+    for (size_t q = 0; q < (size_t)L * L; ++q) dmin[q] = 0.;
+    for (int m = 0; m < L - 1; ++m)
+      for (int n = m + 1; n < L; ++n) dmin[m + (size_t)L * n] = 0.5 * (dt[m + (size_t)L * n] + dt[n + (size_t)L * m]);
+  }
+  return ICLS_OK;
+}
+
+int icls_probe(icls_ctx* h, int id, int l, int i, int j, int k, double* value) {
+  if (!h || !value) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  int lo[3], hi[3];
+  int rc = icls_field_bounds(h, id, lo, hi);
+  if (rc) return rc;
+  if (i < lo[0] || i > hi[0] || j < lo[1] || j > hi[1] || k < lo[2] || k > hi[2]) return ICLS_E_ARG;
+  long long n;
+  double* d = field_ptr(c, id, l, &n);
+  if (!d) return ICLS_E_ARG;
+  const long long nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1;
+  const long long off = (i - lo[0]) + nx * ((j - lo[1]) + ny * (long long)(k - lo[2]));
+  CK(cudaMemcpyAsync(value, d + off, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  return ICLS_OK;
+}
+
+// one main-loop iteration (main.f90:107-258)
+int icls_step(icls_ctx* h, int istep, int begin) {
+  NEED(h);
+  Ctx& c = h->c;
+  c.time = c.time + c.dt;
+  int rc;
+  if (c.cfg.solveLS) {
+    rc = ls_main(c, istep);
+    if (rc) return rc;
+  }
+  launch_stream_vel(c);
+  launch_ab2(c);
+  if (c.cfg.solveLS) {
+    gfm4p(c);
+    launch_fillps(c, 1);  // fillps, then p = p + p_jump (main.f90:139-142)
+  } else {
+    launch_fillps(c, 0);
+  }
+  launch_solver2d(c, 1);   // solver2d + boundp(p)
+  launch_correc(c, 1);     // correc + bounduvw + average_vel_at_center + NaN probe
+  launch_pressure_update(c, istep == begin + 1);
+  rc = check_launch();
+  if (rc) return rc;
+  rc = read_scalars(c);
+  if (rc) return rc;
+  if (c.h_sc->nan_flag) return ICLS_E_NAN;
+  if (c.cfg.ioutchk > 0 && istep % c.cfg.ioutchk == 0) {
+    rc = chkdiv(c, istep, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    c.dt = c.cfg.timestep;  // main.f90:216
+  }
+  return ICLS_OK;
+}
+
+int icls_tube_construction(icls_ctx* h, int l) {
+  if (!h) return ICLS_E_ARG;
+  LARG(h, l);
+  tube_construction(h->c, l - 1);
+  return check_launch();
+}
+
+int icls_ls_advection(icls_ctx* h, int l) {
+  NEED(h);
+  LARG(h, l);
+  ls_advection(h->c, l - 1);
+  return check_launch();
+}
+
+int icls_ls_mass_correction(icls_ctx* h, int istep, int l) {
+  NEED(h);
+  LARG(h, l);
+  int rc = ls_mass_correction(h->c, istep, l - 1);
+  if (rc) return rc;
+  return check_launch();
+}
+
+int icls_ls_reinit_main(icls_ctx* h, int istep, int l) {
+  NEED(h);
+  LARG(h, l);
+  if (istep % h->c.cfg.reinit_step == 0) ls_reinit(h->c, l - 1);
+  return check_launch();
+}
+
+int icls_update_materials(icls_ctx* h) {
+  if (!h) return ICLS_E_ARG;
+  update_materials(h->c);
+  return check_launch();
+}
+
+int icls_get_curvature(icls_ctx* h, int l) {
+  NEED(h);
+  LARG(h, l);
+  launch_curvature(h->c, h->c.lv[l - 1], h->c.curv, h->c.nrm_m);
+  return check_launch();
+}
+
+int icls_band_count(icls_ctx* h, int l, long long* nb_cnt) {
+  if (!h || !nb_cnt) return ICLS_E_ARG;
+  LARG(h, l);
+  CK(cudaMemcpyAsync(nb_cnt, h->c.d_nbcnt + (l - 1), sizeof(long long), cudaMemcpyDeviceToHost, h->c.s));
+  CK(cudaStreamSynchronize(h->c.s));
+  return ICLS_OK;
+}
+
+
+int icls_profile_enable(icls_ctx* h, int on) {
+  if (!h) return ICLS_E_ARG;
+  CK(cudaStreamSynchronize(h->c.s));
+  h->c.prof.collect();
+  h->c.prof.on = on != 0;
+  return ICLS_OK;
+}
+
+int icls_profile_reset(icls_ctx* h) {
+  if (!h) return ICLS_E_ARG;
+  CK(cudaStreamSynchronize(h->c.s));
+  h->c.prof.collect();
+  for (auto& e : h->c.prof.table) { e.total_ms = 0.; e.launches = 0; e.timed = 0; }
+  h->c.prof.launches = 0;
+  return ICLS_OK;
+}
+
+int icls_profile_count(icls_ctx* h, int* n) {
+  if (!h || !n) return ICLS_E_ARG;
+  CK(cudaStreamSynchronize(h->c.s));
+  h->c.prof.collect();
+  *n = (int)h->c.prof.table.size();
+  return ICLS_OK;
+}
+
+int icls_profile_entry(icls_ctx* h, int idx, char* name, int name_len, double* total_ms, long long* launches,
+                       long long* timed) {
+  if (!h) return ICLS_E_ARG;
+  Prof& pr = h->c.prof;
+  if (idx < 0 || idx >= (int)pr.table.size()) return ICLS_E_ARG;
+  const ProfEntry& e = pr.table[idx];
+  if (name && name_len > 0) {
+    std::strncpy(name, e.name.c_str(), (size_t)name_len - 1);
+    name[name_len - 1] = 0;
+  }
+  if (total_ms) *total_ms = e.total_ms;
+  if (launches) *launches = e.launches;
+  if (timed) *timed = e.timed;
+  return ICLS_OK;
+}
+
+int icls_launch_count(icls_ctx* h, long long* n) {
+  if (!h || !n) return ICLS_E_ARG;
+  *n = h->c.prof.launches;
+  return ICLS_OK;
+}
+
+int icls_get_stream(icls_ctx* h, void** stream) {
+  if (!h || !stream) return ICLS_E_ARG;
+  *stream = (void*)h->c.s;
+  return ICLS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,158 @@
+// icls_common.cuh — device-side parameters, index maps and the numerical
+// building blocks shared by all kernels of the ICLS hot path.
+//
+// Arrays keep the reference's Fortran index space (src/common.f90:7-71):
+//   shape C (0:i1,0:j1,0:k1), shape I (1:imax,..), shape L (-2:i1+2,..),
+// column-major, i fastest.  The FP64 kernels are compiled with -fmad=false
+// and evaluate every expression in the reference's left-to-right order, so
+// the arithmetic matches the Fortran bit for bit wherever no
+// transcendental function or reordered reduction is involved.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace icls {
+
+struct Params {
+  int imax, jmax, kmax;      // one domain: imax=itot, ...
+  int i1, j1, k1;
+  int L;                     // number of level sets
+  // extents of the three array shapes
+  int nCx, nCy, nCz;         // C: imax+2, ...
+  int nLx, nLy, nLz;         // L: imax+6, ...
+  long long nC, nI, nL;      // element counts
+  double lx, ly, lz;
+  double dxi, dyi, dzi, dx, dy, dz;
+  double NB;                 // NarrowBand_2 = 6dz (param.f90:41)
+  double pi;
+  double dt;
+  double rho1, rho2, miu1, miu2, rho0, visc, iFr, nondi;
+  double g1, g2, g3;
+  double v_lower, v_upper;
+  double forceytot;
+  int TwoD;
+  int ls_adv_space, i_space, ispeed_curv;
+};
+
+// ---------------------------------------------------------------- indexing
+__host__ __device__ __forceinline__ long long idxC(const Params& p, int i, int j, int k) {
+  return (long long)i + (long long)p.nCx * ((long long)j + (long long)p.nCy * (long long)k);
+}
+__host__ __device__ __forceinline__ long long idxI(const Params& p, int i, int j, int k) {
+  return (long long)(i - 1) + (long long)p.imax * ((long long)(j - 1) + (long long)p.jmax * (long long)(k - 1));
+}
+__host__ __device__ __forceinline__ long long idxL(const Params& p, int i, int j, int k) {
+  return (long long)(i + 2) + (long long)p.nLx * ((long long)(j + 2) + (long long)p.nLy * (long long)(k + 2));
+}
+// periodic source index of a halo coordinate (x: 1..imax, y: 1..jmax)
+__host__ __device__ __forceinline__ int wrapx(const Params& p, int i) {
+  return i < 1 ? i + p.imax : (i > p.imax ? i - p.imax : i);
+}
+__host__ __device__ __forceinline__ int wrapy(const Params& p, int j) {
+  return j < 1 ? j + p.jmax : (j > p.jmax ? j - p.jmax : j);
+}
+
+template <typename T>
+__device__ __forceinline__ T sq(T x) { return x * x; }
+
+// ------------------------------------------------------------ WENO5, HOUC5
+// One WENO5 upwind-biased derivative from the five differences v1..v5
+// (hyperPDE.f90:545-576, repeated at 579-611, 622-687, 698-763, 2972-3180).
+template <typename T>
+__device__ __forceinline__ T weno5(T v1, T v2, T v3, T v4, T v5) {
+  const T eps_weno = (T)1.e-6;
+  const T sigma_1 = (T)0.1, sigma_2 = (T)0.6, sigma_3 = (T)0.3;
+  const T c1312 = (T)(13. / 12.), c14 = (T)(1. / 4.);
+  T S1 = c1312 * sq((v1 - (T)2. * v2) + v3) + c14 * sq((v1 - (T)4. * v2) + (T)3. * v3);
+  T S2 = c1312 * sq((v2 - (T)2. * v3) + v4) + c14 * sq(v2 - v4);
+  T S3 = c1312 * sq((v3 - (T)2. * v4) + v5) + c14 * sq(((T)3. * v3 - (T)4. * v4) + v5);
+  T a1 = sigma_1 / sq(eps_weno + S1);
+  T a2 = sigma_2 / sq(eps_weno + S2);
+  T a3 = sigma_3 / sq(eps_weno + S3);
+  T s = (a1 + a2) + a3;
+  T w1 = a1 / s, w2 = a2 / s, w3 = a3 / s;
+  const T c13 = (T)(1. / 3.), c76 = (T)(7. / 6.), c116 = (T)(11. / 6.), cm16 = (T)(-1. / 6.),
+          c56 = (T)(5. / 6.), c16 = (T)(1. / 6.);
+  return (w1 * ((c13 * v1 - c76 * v2) + c116 * v3) + w2 * ((cm16 * v2 + c56 * v3) + c13 * v4)) +
+         w3 * ((c13 * v3 + c56 * v4) - c16 * v5);
+}
+
+// HOUC5 6-point numerators (hyperPDE.f90:428-432)
+template <typename T>
+__device__ __forceinline__ T houc5_pos(T m3, T m2, T m1, T c0, T p1, T p2) {
+  return (T)(1. / 60.) * (((((-((T)2. * m3) + (T)15. * m2) - (T)60. * m1) + (T)20. * c0) + (T)30. * p1) - (T)3. * p2);
+}
+template <typename T>
+__device__ __forceinline__ T houc5_neg(T p3, T p2, T p1, T c0, T m1, T m2) {
+  return (T)(1. / 60.) * ((((((T)2. * p3 - (T)15. * p2) + (T)60. * p1) - (T)20. * c0) - (T)30. * m1) + (T)3. * m2);
+}
+
+// ------------------------------------------------------------- reductions
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+// Block-wide sum in a fixed tree order (result valid in thread 0).
+template <typename T, int NT>
+__device__ __forceinline__ T block_sum(T v) {
+  __shared__ T red[NT / 32];
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  if (ln == 0) red[w] = v;
+  __syncthreads();
+  T r = (T)0;
+  if (w == 0) {
+    r = (ln < NT / 32) ? red[ln] : (T)0;
+    r = warp_sum(r);
+  }
+  __syncthreads();
+  return r;
+}
+template <typename T, int NT>
+__device__ __forceinline__ T block_max(T v) {
+  __shared__ T red[NT / 32];
+  v = warp_max(v);
+  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  if (ln == 0) red[w] = v;
+  __syncthreads();
+  T r = (T)0;
+  if (w == 0) {
+    r = (ln < NT / 32) ? red[ln] : (T)(-1e300);
+    r = warp_max(r);
+  }
+  __syncthreads();
+  return r;
+}
+// atomic max of a non-negative double through its ordered bit pattern
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+// Device scalars kept in HBM between kernels (no host round trip).
+struct DevScalars {
+  double rho_avr;         // misc.f90:173
+  double v_bulk;          // misc.f90:642-655
+  double norm;            // main.f90:173-175
+  double norm_old;        // main.f90:183
+  double residual;        // levelset.f90:831
+  double area;            // levelset.f90:499-501
+  double heav_sum;        // levelset.f90:505
+  double inflate_temp;    // levelset.f90:514
+  double maxchk;          // levelset.f90:521
+  double divtot, divmax;  // chkdiv.f90
+  double umax, vmax, wmax;// chkdt.f90:42-44
+  double velmax;          // misc.f90:632
+  long long divloc;       // linear interior index of max|div|
+  int reinit_done;        // residual < dz**5 reached (levelset.f90:833)
+  int reinit_iters;
+  int nan_flag;           // main.f90:207
+  int pad;
+};
+
+}  // namespace icls

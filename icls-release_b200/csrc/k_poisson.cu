@@ -1,0 +1,357 @@
+// k_poisson.cu — the pressure Poisson solve of solver2d (solver.f90:68-196),
+// FP64, -fmad=false.
+//
+// Forward: real FFT along x of every (j,k) line, then along y of every
+// (i,k) column of those coefficients, with VFFTPACK's contract (fft.f:
+// 1123-1142): half-complex layout r0, Re1, Im1, ..., r_{N/2} and sqrt(1/N)
+// scaling.  Thomas elimination in z per (i,j) with diagonal b(k)+xyrt(i,j)
+// (solver.f90:119-160), the exactly-zero last pivot of mode (0,0) giving
+// p=0.  Inverse: y then x, the exact inverse of the forward transform
+// (fft.f:403-452).  The 2decomp transposes of the reference
+// (transpose_*.f90) are replaced by the access pattern of each kernel: the
+// x pass streams contiguous lines, the y pass loads 16-wide column tiles,
+// the z pass walks k with one thread per (i,j).
+//
+// Two real lines share one complex FFT (z = a + i b); the radix-2 passes
+// run in shared memory with one CTA per group of lines.
+#include <cmath>
+#include <vector>
+
+#include "ctx.h"
+
+namespace icls {
+
+namespace {
+
+constexpr int FT = 256;  // threads per FFT CTA
+
+__device__ __forceinline__ int bitrev(int x, int logn) { return (int)(__brev((unsigned)x) >> (32 - logn)); }
+
+// in-place radix-2 DIT over nl lines of length N stored at buf[l*ld + n],
+// input in bit-reversed order.  inv: e^{+i} twiddles.
+__device__ __forceinline__ void smem_fft(double2* buf, int nl, int N, int logN, int ld,
+                                         const double2* __restrict__ tw, int inv) {
+  const int halfN = N >> 1;
+  for (int s = 1; s <= logN; ++s) {
+    const int half = 1 << (s - 1);
+    const int tstride = N >> s;
+    for (int t = threadIdx.x; t < nl * halfN; t += blockDim.x) {
+      const int line = t / halfN, b = t - line * halfN;
+      const int grp = b / half, j = b - grp * half;
+      const int i0 = grp * 2 * half + j, i1 = i0 + half;
+      double2 w = __ldg(&tw[j * tstride]);
+      if (inv) w.y = -w.y;
+      double2* L = buf + line * ld;
+      const double2 x0 = L[i0], x1 = L[i1];
+      const double2 t1 = make_double2(x1.x * w.x - x1.y * w.y, x1.x * w.y + x1.y * w.x);
+      L[i0] = make_double2(x0.x + t1.x, x0.y + t1.y);
+      L[i1] = make_double2(x0.x - t1.x, x0.y - t1.y);
+    }
+    __syncthreads();
+  }
+}
+
+// split Z (FFT of a+ib) into the scaled half-complex spectra of a and b
+__device__ __forceinline__ void unpack_hc(const double2* Z, int N, int n, double s, double& ha, double& hb) {
+  // position n of the half-complex output
+  if (n == 0) { ha = s * Z[0].x; hb = s * Z[0].y; return; }
+  if (n == N - 1) { ha = s * Z[N / 2].x; hb = s * Z[N / 2].y; return; }
+  const int k = (n + 1) >> 1;
+  const double2 zk = Z[k], zn = Z[N - k];
+  // A_k = (Z_k + conj Z_{N-k})/2 ; B_k = (Z_k - conj Z_{N-k})/(2i)
+  if (n & 1) {  // real parts
+    ha = s * (0.5 * (zk.x + zn.x));
+    hb = s * (0.5 * (zk.y + zn.y));
+  } else {      // imaginary parts
+    ha = s * (0.5 * (zk.y - zn.y));
+    hb = s * (-0.5 * (zk.x - zn.x));
+  }
+}
+
+// Z_k of the Hermitian pair built from two half-complex lines a, b
+__device__ __forceinline__ double2 pack_hc(const double* a, const double* b, int N, int k, long long st) {
+  if (k == 0) return make_double2(a[0], b[0]);
+  if (k == N / 2) return make_double2(a[(N - 1) * st], b[(N - 1) * st]);
+  if (k < N / 2) {
+    const double ar = a[(2 * k - 1) * st], ai = a[(2 * k) * st];
+    const double br = b[(2 * k - 1) * st], bi = b[(2 * k) * st];
+    return make_double2(ar - bi, ai + br);
+  }
+  const int m = N - k;
+  const double ar = a[(2 * m - 1) * st], ai = a[(2 * m) * st];
+  const double br = b[(2 * m - 1) * st], bi = b[(2 * m) * st];
+  return make_double2(ar + bi, -ai + br);
+}
+
+// ---- x pass: lines (j,k) of length imax; CL complex lines per CTA --------
+// dir 0: p (shape C interior) -> spec ; dir 1: spec -> p (+ boundp halos)
+__global__ void __launch_bounds__(FT) k_fft_x(Params p, int dir, int CL, int logN, const double2* __restrict__ tw,
+                                              double* __restrict__ pp, double* __restrict__ spec, int halos) {
+  extern __shared__ double2 sm[];
+  const int N = p.imax;
+  const int ld = N + 1;
+  const long long nlines = (long long)p.jmax * p.kmax;
+  const long long l0 = (long long)blockIdx.x * (2 * CL);
+  const double s = sqrt(1.0 / N);
+  // load
+  for (int t = threadIdx.x; t < CL * N; t += blockDim.x) {
+    const int cl = t / N, n = t - cl * N;
+    const long long la = l0 + 2 * cl, lb = la + 1;
+    double2 z = make_double2(0., 0.);
+    if (lb < nlines) {
+      if (dir == 0) {
+        const int ja = (int)(la % p.jmax) + 1, ka = (int)(la / p.jmax) + 1;
+        const int jb = (int)(lb % p.jmax) + 1, kb = (int)(lb / p.jmax) + 1;
+        z = make_double2(pp[idxC(p, n + 1, ja, ka)], pp[idxC(p, n + 1, jb, kb)]);
+        sm[cl * ld + bitrev(n, logN)] = z;
+      } else {
+        const double* a = spec + la * N;
+        const double* b = spec + lb * N;
+        sm[cl * ld + bitrev(n, logN)] = pack_hc(a, b, N, n, 1);
+      }
+    }
+  }
+  __syncthreads();
+  smem_fft(sm, CL, N, logN, ld, tw, dir);
+  for (int t = threadIdx.x; t < CL * N; t += blockDim.x) {
+    const int cl = t / N, n = t - cl * N;
+    const long long la = l0 + 2 * cl, lb = la + 1;
+    if (lb >= nlines) continue;
+    if (dir == 0) {
+      double ha, hb;
+      unpack_hc(sm + cl * ld, N, n, s, ha, hb);
+      spec[la * N + n] = ha;
+      spec[lb * N + n] = hb;
+    } else {
+      const double2 z = sm[cl * ld + n];
+      const double va = s * z.x, vb = s * z.y;
+      for (int h = 0; h < 2; ++h) {
+        const long long ll = h ? lb : la;
+        const double v = h ? vb : va;
+        const int j = (int)(ll % p.jmax) + 1, k = (int)(ll / p.jmax) + 1;
+        const int i = n + 1;
+        if (!halos) {
+          pp[idxC(p, i, j, k)] = v;
+          continue;
+        }
+        // boundp (bound.f90:182-287): every image of (i,j,k)
+        const int nj = (j == 1) ? 2 : ((j == p.jmax) ? 2 : 1);
+        const int nk = (k == 1) ? 2 : ((k == p.kmax) ? 2 : 1);
+        const int ni = (i == 1) ? 2 : ((i == p.imax) ? 2 : 1);
+        for (int a = 0; a < ni; ++a) {
+          const int ii = a == 0 ? i : (i == 1 ? p.i1 : 0);
+          for (int b = 0; b < nj; ++b) {
+            const int jj = b == 0 ? j : (j == 1 ? p.j1 : 0);
+            for (int cidx = 0; cidx < nk; ++cidx) {
+              const int kk = cidx == 0 ? k : (k == 1 ? 0 : p.k1);
+              pp[idxC(p, ii, jj, kk)] = v;
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// ---- y pass: columns (i,k) of length jmax, TI real columns per CTA -------
+__global__ void __launch_bounds__(FT) k_fft_y(Params p, int dir, int TI, int logN, const double2* __restrict__ tw,
+                                              double* __restrict__ spec) {
+  extern __shared__ double2 sm[];
+  const int N = p.jmax;
+  const int CL = TI / 2;
+  const int ld = N + 1;
+  const int tiles_i = p.imax / TI;
+  const int k = blockIdx.x / tiles_i + 1;
+  const int i0 = (blockIdx.x % tiles_i) * TI + 1;
+  const long long sj = p.imax;
+  double* base = spec + (long long)(i0 - 1) + (long long)p.imax * (long long)p.jmax * (k - 1);
+  const double s = sqrt(1.0 / N);
+  // load: consecutive threads read consecutive i
+  for (int t = threadIdx.x; t < TI * N; t += blockDim.x) {
+    const int ti = t % TI, n = t / TI;
+    const double v = base[ti + n * sj];
+    double* slot = reinterpret_cast<double*>(&sm[(ti >> 1) * ld]);
+    if (dir == 0) {
+      slot[2 * bitrev(n, logN) + (ti & 1)] = v;
+    } else {
+      slot[2 * n + (ti & 1)] = v;  // raw half-complex, packed below
+    }
+  }
+  __syncthreads();
+  if (dir == 1) {
+    // build Z in a second buffer region then copy back in bit-reversed order
+    double2* tmp = sm + CL * ld;
+    for (int t = threadIdx.x; t < CL * N; t += blockDim.x) {
+      const int cl = t / N, kk = t - cl * N;
+      const double* raw = reinterpret_cast<const double*>(&sm[cl * ld]);
+      // raw[2n] = a_n, raw[2n+1] = b_n
+      tmp[cl * ld + bitrev(kk, logN)] = pack_hc(raw, raw + 1, N, kk, 2);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < CL * ld; t += blockDim.x) sm[t] = tmp[t];
+    __syncthreads();
+  }
+  smem_fft(sm, CL, N, logN, ld, tw, dir);
+  for (int t = threadIdx.x; t < TI * N; t += blockDim.x) {
+    const int ti = t % TI, n = t / TI;
+    const int cl = ti >> 1;
+    double v;
+    if (dir == 0) {
+      double ha, hb;
+      unpack_hc(sm + cl * ld, N, n, s, ha, hb);
+      v = (ti & 1) ? hb : ha;
+    } else {
+      const double2 z = sm[cl * ld + n];
+      v = (ti & 1) ? s * z.y : s * z.x;
+    }
+    base[ti + n * sj] = v;
+  }
+}
+
+// ---- Thomas elimination in z (solver.f90:119-160) -------------------------
+// zpiv(i,j,k) = 1/(b(k)+xyrt - a(k) d(k-1)) for k<kmax (z of the reference)
+// and the raw last divisor at k=kmax.
+__global__ void k_thomas_setup(Params p, const double* __restrict__ xyrt, const double* __restrict__ a,
+                               const double* __restrict__ b, const double* __restrict__ c,
+                               double* __restrict__ zpiv) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nxy = (long long)p.imax * p.jmax;
+  if (q >= nxy) return;
+  const double xy = xyrt[q];
+  double z = 1. / (b[1] + xy);
+  double d = c[1] * z;
+  zpiv[q] = z;
+  for (int k = 2; k <= p.kmax - 1; ++k) {
+    const double bb = b[k] + xy;
+    z = 1. / (bb - a[k] * d);
+    d = c[k] * z;
+    zpiv[q + (k - 1) * nxy] = z;
+  }
+  const double bb = b[p.kmax] + xy;
+  zpiv[q + (p.kmax - 1) * nxy] = bb - a[p.kmax] * d;
+}
+
+__global__ void k_thomas(Params p, const double* __restrict__ a, const double* __restrict__ c,
+                         const double* __restrict__ zpiv, double* __restrict__ spec) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nxy = (long long)p.imax * p.jmax;
+  if (q >= nxy) return;
+  const int K = p.kmax;
+  double* col = spec + q;
+  double z = zpiv[q];
+  double prev = col[0] * z;
+  col[0] = prev;
+  for (int k = 2; k <= K - 1; ++k) {
+    z = zpiv[q + (k - 1) * nxy];
+    const double v = (col[(k - 1) * nxy] - a[k] * prev) * z;
+    col[(k - 1) * nxy] = v;
+    prev = v;
+  }
+  const double zz = zpiv[q + (K - 1) * nxy];
+  double nxt;
+  if (zz != 0.) nxt = (col[(K - 1) * nxy] - a[K] * prev) / zz;
+  else nxt = 0.;
+  col[(K - 1) * nxy] = nxt;
+  for (int k = K - 1; k >= 1; --k) {
+    const double d = c[k] * zpiv[q + (k - 1) * nxy];
+    const double v = col[(k - 1) * nxy] - d * nxt;
+    col[(k - 1) * nxy] = v;
+    nxt = v;
+  }
+}
+
+int ilog2(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return l;
+}
+
+void make_twiddles(int N, std::vector<double2>& t) {
+  t.resize(N / 2 > 0 ? N / 2 : 1);
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int m = 0; m < N / 2; ++m) {
+    long double a = -2.0L * pi * (long double)m / (long double)N;
+    t[m] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+}
+
+}  // namespace
+
+// tables of initsolver (initsolver.f90:20-82) and the twiddles
+void poisson_setup(Ctx& c) {
+  const Params& P = c.P;
+  const int itot = P.imax, jtot = P.jmax, kmax = P.kmax;
+  std::vector<double> a(kmax + 1, 0.), b(kmax + 1, 0.), cc(kmax + 1, 0.);
+  for (int k = 1; k <= kmax; ++k) { a[k] = P.dzi * P.dzi; cc[k] = P.dzi * P.dzi; b[k] = -(a[k] + cc[k]); }
+  b[1] = b[1] + a[1];
+  b[kmax] = b[kmax] + cc[kmax];
+  a[1] = 0.; cc[kmax] = 0.;
+  std::vector<double> xrt(itot + 1, 0.), yrt(jtot + 1, 0.);
+  const double pi = P.pi;
+  for (int i = 3; i <= itot; i += 2) {
+    double s = std::sin((double)(i - 1) * pi / (2. * itot));
+    xrt[i - 1] = -4. * P.dxi * P.dxi * (s * s);
+    xrt[i] = xrt[i - 1];
+  }
+  xrt[1] = 0.; xrt[itot] = -4. * P.dxi * P.dxi;
+  for (int j = 3; j <= jtot; j += 2) {
+    double s = std::sin((double)(j - 1) * pi / (2. * jtot));
+    yrt[j - 1] = -4. * P.dyi * P.dyi * (s * s);
+    yrt[j] = yrt[j - 1];
+  }
+  yrt[1] = 0.; yrt[jtot] = -4. * P.dyi * P.dyi;
+  std::vector<double> xy((size_t)itot * jtot);
+  for (int j = 1; j <= jtot; ++j)
+    for (int i = 1; i <= itot; ++i) xy[(i - 1) + (size_t)itot * (j - 1)] = xrt[i] + yrt[j];
+  cudaMemcpyAsync(c.xyrt, xy.data(), xy.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
+  cudaMemcpyAsync(c.tri_a, a.data(), a.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
+  cudaMemcpyAsync(c.tri_b, b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
+  cudaMemcpyAsync(c.tri_c, cc.data(), cc.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
+  std::vector<double2> tx, ty;
+  make_twiddles(itot, tx);
+  make_twiddles(jtot, ty);
+  cudaMemcpyAsync(c.twx, tx.data(), tx.size() * sizeof(double2), cudaMemcpyHostToDevice, c.s);
+  cudaMemcpyAsync(c.twy, ty.data(), ty.size() * sizeof(double2), cudaMemcpyHostToDevice, c.s);
+  const long long nxy = (long long)itot * jtot;
+  k_thomas_setup<<<(unsigned)((nxy + 127) / 128), 128, 0, c.s>>>(P, c.xyrt, c.tri_a, c.tri_b, c.tri_c, c.zpiv);
+  cudaStreamSynchronize(c.s);  // host vectors above go out of scope
+}
+
+static int x_lines_per_cta(int N) {
+  int cl = 2048 / N;
+  if (cl < 1) cl = 1;
+  if (cl > 16) cl = 16;
+  return cl;
+}
+static int y_tile(int imax) {
+  int ti = 16;
+  while (ti > 2 && imax % ti) ti >>= 1;
+  return ti;
+}
+
+void launch_solver2d(Ctx& c, int write_halos) {
+  Scope sc_(c.prof, c.s, "solver2d", 5);
+  const Params& P = c.P;
+  const int lx = ilog2(P.imax), ly = ilog2(P.jmax);
+  const int CL = x_lines_per_cta(P.imax);
+  const long long nlines = (long long)P.jmax * P.kmax;
+  const unsigned gx = (unsigned)((nlines + 2 * CL - 1) / (2 * CL));
+  const size_t smx = (size_t)CL * (P.imax + 1) * sizeof(double2);
+  const int TI = y_tile(P.imax);
+  const unsigned gy = (unsigned)((P.imax / TI) * P.kmax);
+  const size_t smy = (size_t)2 * (TI / 2) * (P.jmax + 1) * sizeof(double2);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_fft_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set = true;
+  }
+  k_fft_x<<<gx, FT, smx, c.s>>>(P, 0, CL, lx, c.twx, c.p, c.spec, 0);
+  k_fft_y<<<gy, FT, smy, c.s>>>(P, 0, TI, ly, c.twy, c.spec);
+  const long long nxy = (long long)P.imax * P.jmax;
+  k_thomas<<<(unsigned)((nxy + 127) / 128), 128, 0, c.s>>>(P, c.tri_a, c.tri_c, c.zpiv, c.spec);
+  k_fft_y<<<gy, FT, smy, c.s>>>(P, 1, TI, ly, c.twy, c.spec);
+  k_fft_x<<<gx, FT, smx, c.s>>>(P, 1, CL, lx, c.twx, c.p, c.spec, write_halos);
+}
+
+}  // namespace icls

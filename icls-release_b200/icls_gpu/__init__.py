@@ -1,0 +1,18 @@
+"""B200-native ICLS hot path: Python mirror of the reference driver interface.
+
+The compute runs in ``libicls_gpu.so`` (CUDA, sm_100a) behind the C ABI of
+include/icls_gpu.h; this package only binds it.
+"""
+from .config import (CURV_MLP, CURV_STENCIL, FIELD_ID, FIELDS, FP32, FP64, HOUC5,
+                     SPEED_CURV, SPEED_UNFM, WENO5, IclsConfig, IclsScalars, Workload,
+                     field_shape, init_drops, initial_velocity, make_config, multi_drop,
+                     rising_bubble, seeded_drops, static_drop)
+from .binding import LIB_PATH, Backend, IclsError, Solver, gpu_backend
+
+__all__ = [
+    "CURV_MLP", "CURV_STENCIL", "FIELD_ID", "FIELDS", "FP32", "FP64", "HOUC5",
+    "SPEED_CURV", "SPEED_UNFM", "WENO5", "IclsConfig", "IclsScalars", "Workload",
+    "field_shape", "init_drops", "initial_velocity", "make_config", "multi_drop",
+    "rising_bubble", "seeded_drops", "static_drop", "LIB_PATH", "Backend", "IclsError",
+    "Solver", "gpu_backend",
+]

@@ -1,0 +1,298 @@
+"""CUDA path vs the CPU oracle on identical seeded inputs (needs a B200).
+
+Tolerances: stencil, band, boundary and reinitialisation arithmetic is
+bit-exact (same IEEE operations in the reference's order, no contraction);
+anything downstream of sin/cos (Heaviside, Dirac), of reordered sums
+(volumes) or of the FFT is compared at 1e-12 relative to the field's max;
+multi-step runs at the parity bar: relative L2 <= 1e-10 on phi, u, v, w, p.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+from icls_gpu import (HOUC5, WENO5, IclsError, Solver, field_shape, init_drops, initial_velocity,
+                      make_config, multi_drop, static_drop)
+from oracle.oracle import Oracle, set_threads
+
+set_threads(min(32, os.cpu_count() or 1))
+
+EXACT = ("lvset", "u", "v", "w", "pnew", "ucc", "vcc", "wcc")
+
+
+def smooth_velocity(cfg, amp=0.5, seed=0):
+    """A smooth, periodic-in-x,y velocity on shape C from a few Fourier modes."""
+    rng = np.random.default_rng(seed)
+    shp = field_shape(cfg, "u")
+    i = (np.arange(shp[0]) - 0.5) / cfg.itot
+    j = (np.arange(shp[1]) - 0.5) / cfg.jtot
+    k = (np.arange(shp[2]) - 0.5) / cfg.ktot
+    X, Y, Z = np.meshgrid(i, j, k, indexing="ij")
+    out = []
+    for _ in range(3):
+        f = np.zeros(shp)
+        for _m in range(3):
+            kx, ky = rng.integers(1, 3, size=2)
+            ph = rng.uniform(0, 2 * np.pi, 3)
+            f += rng.uniform(-1, 1) * np.sin(2 * np.pi * kx * X + ph[0]) * np.cos(2 * np.pi * ky * Y + ph[1]) * \
+                np.sin(np.pi * Z + ph[2])
+        out.append(np.asfortranarray(amp * f))
+    return out
+
+
+def paired(cfg, ls, u=None, v=None, w=None, p=None):
+    g = Solver(cfg)
+    o = Oracle(cfg)
+    for s in (g, o):
+        s.setup(ls, u, v, w, p)
+    return g, o
+
+
+def maxdiff(g, o, name, l=1):
+    a, b = g.download(name, l), o.download(name, l)
+    return float(np.max(np.abs(a - b))), float(np.max(np.abs(b)))
+
+
+def assert_exact(g, o, names, l=1):
+    for n in names:
+        d, m = maxdiff(g, o, n, l)
+        assert d == 0.0, "%s differs by %.3e (max %.3e)" % (n, d, m)
+
+
+def assert_close(g, o, names, tol=1e-12, l=1):
+    for n in names:
+        d, m = maxdiff(g, o, n, l)
+        assert d <= tol * max(m, 1e-300), "%s differs by %.3e (max %.3e)" % (n, d, m)
+
+
+def drop_case(n=24, scheme=WENO5, L=1, **kw):
+    cfg = make_config(itot=n, jtot=n, ktot=n, lmax=L, ls_adv_space=scheme, timestep=2e-4,
+                      rho1=1.0, rho2=10.0, miu1=1.0, miu2=10.0, Re=100.0, We=0.5, **kw)
+    if L == 1:
+        ls = init_drops(cfg, [(0.47, 0.52, 0.5)], [0.22])
+    else:
+        ls = init_drops(cfg, [(0.3, 0.3, 0.35), (0.7, 0.65, 0.6), (0.28, 0.75, 0.7)][:L], [0.15, 0.17, 0.13][:L],
+                        all_images=True)
+    return cfg, ls
+
+
+def test_init_program_parity():
+    cfg, ls = drop_case()
+    u, v, w = smooth_velocity(cfg)
+    rng = np.random.default_rng(1)
+    p = np.asfortranarray(rng.standard_normal(field_shape(cfg, "p")))
+    g, o = paired(cfg, ls, u, v, w, p)
+    assert_exact(g, o, EXACT)
+    assert_close(g, o, ["miu", "rho", "jiemian", "rho_u", "rho_v", "rho_w"], 1e-15)
+    assert_close(g, o, ["duold", "dvold", "dwold"], 1e-12)
+    vg, vo = g.volumes(), o.volumes()
+    assert np.allclose(vg[0], vo[0], rtol=1e-13, atol=0)
+
+
+@pytest.mark.parametrize("scheme", [HOUC5, WENO5])
+def test_tube_and_advection_bit_exact(scheme):
+    cfg, ls = drop_case(scheme=scheme)
+    u, v, w = smooth_velocity(cfg, amp=1.0, seed=2)
+    g, o = paired(cfg, ls, u, v, w)
+    for s in (g, o):
+        s.tube_construction(1)
+    assert_exact(g, o, ["lvset"])
+    assert g.band_count(1) == o.band_count(1) > 0
+    for s in (g, o):
+        s.ls_advection(1)
+    assert_exact(g, o, ["lvset"])
+
+
+def test_reinit_bit_exact():
+    cfg, ls = drop_case(reinit_step=1, reinit_iter_max=3)
+    # a distorted distance function so reinitialisation has work to do
+    ls = ls * (1.0 + 0.3 * np.sin(7.0 * ls))
+    g, o = paired(cfg, ls)
+    for s in (g, o):
+        s.tube_construction(1)
+        s.ls_reinit_main(1, 1)
+    assert_exact(g, o, ["lvset"])
+    sg, so = g.scalars(), o.scalars()
+    assert sg["reinit_iters"] == so["reinit_iters"]
+    assert sg["reinit_residual"] == so["reinit_residual"]
+
+
+def test_materials_parity_multidrop():
+    cfg, ls = drop_case(L=3)
+    g, o = paired(cfg, ls)
+    for s in (g, o):
+        s.update_materials()
+    assert_close(g, o, ["jiemian", "miu", "rho", "rho_u", "rho_v", "rho_w"], 1e-15)
+    assert np.allclose(g.volumes()[0], o.volumes()[0], rtol=1e-13, atol=0)
+
+
+def test_mass_correction_parity():
+    cfg, ls = drop_case(scheme=HOUC5, inflate_step=1)
+    g, o = paired(cfg, ls)
+    shrunk = init_drops(cfg, [(0.47, 0.52, 0.5)], [0.215])
+    u, v, w = smooth_velocity(cfg, amp=0.3, seed=4)
+    for s in (g, o):
+        s.upload("lvset", shrunk[..., 0], 1)
+        s.update_materials()
+        s.tube_construction(1)
+        s.ls_mass_correction(3, 1)
+    assert g.scalars()["last_inflated"] == o.scalars()["last_inflated"] == 1
+    assert_close(g, o, ["lvset"], 1e-12)
+    sg, so = g.scalars(), o.scalars()
+    assert abs(sg["maxchk_glb"] - so["maxchk_glb"]) <= 1e-10 * abs(so["maxchk_glb"])
+
+
+def test_gfm4p_parity():
+    cfg, ls = drop_case(L=2)
+    g, o = paired(cfg, ls)
+    for s in (g, o):
+        s.gfm4p()
+    assert_close(g, o, ["curv", "p_jump", "p_x", "p_y", "p_z", "normal_m"], 1e-12)
+    assert_exact(g, o, ["p_xold", "p_yold", "p_zold"])
+
+
+def test_predictor_projection_chain():
+    cfg, ls = drop_case()
+    u, v, w = smooth_velocity(cfg, amp=0.2, seed=5)
+    rng = np.random.default_rng(6)
+    p = np.asfortranarray(rng.standard_normal(field_shape(cfg, "p")))
+    g, o = paired(cfg, ls, u, v, w, p)
+    for s in (g, o):
+        s.ab2()
+    assert_close(g, o, ["dudt", "dvdt", "dwdt", "duold", "dvold", "dwold"], 1e-12)
+    for s in (g, o):
+        s.fillps()
+        s.gfm4p()
+        s.add_pjump()
+    assert_close(g, o, ["p", "p_jump"], 1e-12)
+    for s in (g, o):
+        s.solver2d()
+    # interior only: solver2d leaves halos untouched in both
+    pg, po = g.interior("p"), o.interior("p")
+    assert np.max(np.abs(pg - po)) <= 1e-11 * np.max(np.abs(po))
+    for s in (g, o):
+        s.boundp("p")
+        s.correc()
+        s.bounduvw("u")
+        s.pressure_update(1, 0)
+        s.average_vel_at_center()
+    assert_close(g, o, ["u", "v", "w", "pnew", "pold", "ucc", "vcc", "wcc"], 1e-10)
+    dg = g.chkdiv(1, raise_on_error=False)
+    do = o.chkdiv(1, raise_on_error=False)
+    assert dg[1] < 1e-12 and do[1] < 1e-12
+
+
+def test_fused_step_equals_call_sequence():
+    """icls_step (fused kernels) == the main.f90 sequence of separate calls."""
+    cfg, ls = drop_case(L=2, reinit_step=2, inflate_step=2)
+    u, v, w = smooth_velocity(cfg, amp=0.3, seed=8)
+    a = Solver(cfg)
+    b = Solver(cfg)
+    for s in (a, b):
+        s.setup(ls, u, v, w)
+    for istep in (1, 2, 3):
+        a.step(istep, 0)
+        b.ls_main(istep)
+        b.average_stream_vel()
+        b.ab2()
+        b.fillps()
+        b.gfm4p()
+        b.add_pjump()
+        b.solver2d()
+        b.boundp("p")
+        b.correc()
+        b.bounduvw("u")
+        b.pressure_update(istep, 0)
+        b.average_vel_at_center()
+    for name in ("lvset", "u", "v", "w", "pnew", "pold", "ucc", "duold", "p_x", "miu"):
+        x, y = a.download(name), b.download(name)
+        assert np.array_equal(x, y), name
+
+
+def run_pair(wl, nsteps, every=None):
+    cfg = wl.cfg
+    ls = init_drops(cfg, wl.centres, wl.radii, wl.all_images)
+    u, v, w = initial_velocity(cfg, wl.shear_v)
+    g, o = paired(cfg, ls, u, v, w)
+    worst = {}
+    for s in range(1, nsteps + 1):
+        g.step(s, 0)
+        o.step(s, 0)
+        if every and s % every == 0:
+            for name in ("u", "v", "w", "pnew"):
+                worst[name] = max(worst.get(name, 0.0), rel_l2(g.download(name), o.download(name)))
+    return g, o, worst
+
+
+def test_static_drop_32_multistep():
+    wl = static_drop(32, steps=20)
+    g, o, _ = run_pair(wl, 20)
+    for name in ("lvset", "u", "v", "w", "pnew"):
+        assert rel_l2(g.download(name), o.download(name)) <= 1e-10, name
+    assert abs(g.volumes()[0][0] - o.volumes()[0][0]) <= 1e-12
+
+
+def test_moving_multidrop_multistep():
+    wl = multi_drop(n=32, ndrop=3, seed=11, steps=12, rmin=0.12, rmax=0.16, dt=2e-4)
+    wl.cfg.reinit_step = 3
+    wl.cfg.inflate_step = 4
+    g, o, _ = run_pair(wl, 12)
+    for l in (1, 2, 3):
+        assert rel_l2(g.download("lvset", l), o.download("lvset", l)) <= 1e-10
+    for name in ("u", "v", "w", "pnew"):
+        assert rel_l2(g.download(name), o.download(name)) <= 1e-10, name
+
+
+def test_static_drop_64_200_steps():
+    """The CPU-runnable static-droplet configuration over its full 200 steps."""
+    wl = static_drop(64, steps=200)
+    g, o, _ = run_pair(wl, 200)
+    for name in ("lvset", "u", "v", "w", "pnew"):
+        e = rel_l2(g.download(name), o.download(name))
+        assert e <= 1e-10, (name, e)
+    # spurious currents (misc.f90:802-843 uses max|u| at cell centres)
+    mg, mo = g.max_vel_at_center(), o.max_vel_at_center()
+    assert abs(mg - mo) <= 1e-10 * mo
+
+
+def test_checks_parity():
+    cfg, ls = drop_case(L=3)
+    u, v, w = smooth_velocity(cfg, amp=0.4, seed=9)
+    g, o = paired(cfg, ls, u, v, w)
+    assert abs(g.chkdt() - o.chkdt()) <= 1e-14 * o.chkdt()
+    assert abs(g.max_vel_at_center() - o.max_vel_at_center()) <= 1e-14
+    assert abs(g.average_stream_vel() - o.average_stream_vel()) <= 1e-13
+    tg, mg, lg, _ = g.chkdiv(0, raise_on_error=False)
+    to, mo, lo, _ = o.chkdiv(0, raise_on_error=False)
+    assert mg == mo and lg == lo and abs(tg - to) <= 1e-9 * max(1.0, abs(to))
+    assert np.allclose(g.ipot(), o.ipot(), rtol=0, atol=1e-15)
+
+
+def test_error_paths_on_gpu():
+    cfg, ls = drop_case()
+    with pytest.raises(IclsError) as e:
+        Solver(make_config(itot=24, jtot=24, ktot=24))  # FFT lengths must be powers of two
+    assert e.value.code == 1
+    s = Solver(cfg)
+    with pytest.raises(IclsError) as e:
+        s.ab2()
+    assert e.value.code == 7
+    # NaN planted in the host data stops the run (main.f90:207-210)
+    u, v, w = smooth_velocity(cfg, amp=0.1)
+    v = v.copy(order="F")
+    v[1, 1, 1] = np.nan
+    s.setup(ls, u, v, w)
+    with pytest.raises(IclsError) as e:
+        s.step(1, 0)
+    assert e.value.code == 3
+    # a non-solenoidal field trips chkdiv (chkdiv.f90:60-87)
+    s2 = Solver(cfg)
+    rng = np.random.default_rng(0)
+    s2.setup(ls, *[np.asfortranarray(rng.standard_normal(field_shape(cfg, "u"))) for _ in range(3)])
+    with pytest.raises(IclsError) as e:
+        s2.chkdiv(5)
+    assert e.value.code == 4
