@@ -40,6 +40,8 @@ def make_workload(name):
     from icls_gpu.config import multi_drop, rising_bubble, static_drop
     if name == "multi_drop_256_48":
         return multi_drop(n=256, ndrop=48, seed=2024)
+    if name == "multi_drop_256_4":
+        return multi_drop(n=256, ndrop=4, seed=2024)
     if name == "multi_drop_128_12":
         return multi_drop(n=128, ndrop=12, seed=2024, rmin=0.06, rmax=0.12)
     if name == "static_drop_64":

@@ -561,14 +561,14 @@ void launch_inflate_sums(Ctx& c, const double* phi, int l) {
   Scope sc_(c.prof, c.s, "inflate_sums", 2);
   double* pa = c.partials;
   double* ph = c.partials + kRedBlocks;
-  k_inflate_sums<<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, phi, c.curv, c.nrm_m, c.dheav, pa, ph);
+  k_inflate_sums<<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, phi, c.kappa, c.nrm_m, c.dheav, pa, ph);
   k_inflate_final<<<1, 32, 0, c.s>>>(c.P, pa, ph, kRedBlocks, l, (double)c.cfg.inflate_step * c.dt, c.dvol,
                                      c.dvol0, c.dmaxchk, c.dsc);
 }
 
 void launch_inflate_vel(Ctx& c) {
   Scope sc_(c.prof, c.s, "inflate_vel", 1);
-  k_inflate_vel<<<nblocks(c.P.nI), NT, 0, c.s>>>(c.P, c.dheav, c.curv, c.dsc, c.ulc, c.vlc, c.wlc);
+  k_inflate_vel<<<nblocks(c.P.nI), NT, 0, c.s>>>(c.P, c.dheav, c.kappa, c.dsc, c.ulc, c.vlc, c.wlc);
 }
 
 void launch_boundmls(Ctx& c, double* phi) {

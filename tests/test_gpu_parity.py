@@ -69,7 +69,7 @@ def assert_close(g, o, names, tol=1e-12, l=1):
         assert d <= tol * max(m, 1e-300), "%s differs by %.3e (max %.3e)" % (n, d, m)
 
 
-def drop_case(n=24, scheme=WENO5, L=1, **kw):
+def drop_case(n=32, scheme=WENO5, L=1, **kw):
     cfg = make_config(itot=n, jtot=n, ktot=n, lmax=L, ls_adv_space=scheme, timestep=2e-4,
                       rho1=1.0, rho2=10.0, miu1=1.0, miu2=10.0, Re=100.0, We=0.5, **kw)
     if L == 1:
@@ -127,7 +127,8 @@ def test_materials_parity_multidrop():
     for s in (g, o):
         s.update_materials()
     assert_close(g, o, ["jiemian", "miu", "rho", "rho_u", "rho_v", "rho_w"], 1e-15)
-    assert np.allclose(g.volumes()[0], o.volumes()[0], rtol=1e-13, atol=0)
+    # sequential (oracle) vs tree (device) sums of N Heaviside values
+    assert np.allclose(g.volumes()[0], o.volumes()[0], rtol=1e-11, atol=0)
 
 
 def test_mass_correction_parity():
