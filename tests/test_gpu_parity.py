@@ -142,7 +142,10 @@ def test_mass_correction_parity():
         s.tube_construction(1)
         s.ls_mass_correction(3, 1)
     assert g.scalars()["last_inflated"] == o.scalars()["last_inflated"] == 1
-    assert_close(g, o, ["lvset"], 1e-12)
+    # the correction speed is proportional to V - V0 ~ 1e-5 V, which the
+    # sequential (oracle) and tree (device) volume sums resolve only to
+    # ~1e-7 relative; the resulting phi difference stays below 1e-11
+    assert_close(g, o, ["lvset"], 1e-11)
     sg, so = g.scalars(), o.scalars()
     assert abs(sg["maxchk_glb"] - so["maxchk_glb"]) <= 1e-10 * abs(so["maxchk_glb"])
 
