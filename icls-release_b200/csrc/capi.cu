@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -61,6 +62,11 @@ void fill_params(Ctx& c) {
   // param.f90:37-41
   P.dxi = f.itot / f.lx; P.dyi = f.jtot / f.ly; P.dzi = f.ktot / f.lz;
   P.dx = 1. / P.dxi; P.dy = 1. / P.dyi; P.dz = 1. / P.dzi;
+  P.rdx = 1. / P.dx; P.rdy = 1. / P.dy; P.rdz = 1. / P.dz;
+  {
+    int e;
+    P.pow2 = (std::frexp(P.dx, &e) == 0.5 && std::frexp(P.dy, &e) == 0.5 && std::frexp(P.dz, &e) == 0.5) ? 1 : 0;
+  }
   P.NB = 6. * P.dz;
   P.pi = std::acos(-1.);
   P.dt = f.timestep;
@@ -169,6 +175,16 @@ int allocate(Ctx& c) {
   // normal%m = 1 outside the curvature band (interface.f90:44)
   std::vector<double> ones((size_t)P.nI, 1.0);
   CK(cudaMemcpy(c.nrm_m, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice));
+  AL(c.d_bbox, (size_t)6 * P.L);
+  CK(cudaMallocHost((void**)&c.h_bbox, sizeof(int) * 6 * P.L));
+  CK(cudaEventCreateWithFlags(&c.ev_bbox, cudaEventDisableTiming));
+  c.win.assign(P.L, DropWin());
+  for (auto& w : c.win) w.box = w.valid = full_box(P);
+  c.outside.assign(P.L, 0.);
+  // ICLS_FULL_SWEEP=1 sweeps every drop's whole array (a check of the box
+  // bookkeeping: both give bit-identical fields)
+  const char* fs = std::getenv("ICLS_FULL_SWEEP");
+  c.use_boxes = (P.L <= kMaxDropsParam) && !(fs && fs[0] == '1');
   c.inflated.assign(P.L, 0);
   c.vol_dirty.assign(P.L, 0);
   c.init_volume_h.assign(P.L, 0.);
@@ -197,6 +213,9 @@ void release(Ctx& c) {
   if (c.h_vol) cudaFreeHost(c.h_vol);
   if (c.h_sc) cudaFreeHost(c.h_sc);
   if (c.ev_vol) cudaEventDestroy(c.ev_vol);
+  if (c.d_bbox) cudaFree(c.d_bbox);
+  if (c.h_bbox) cudaFreeHost(c.h_bbox);
+  if (c.ev_bbox) cudaEventDestroy(c.ev_bbox);
   c.prof.release();
   if (c.s) cudaStreamDestroy(c.s);
 }
@@ -235,40 +254,158 @@ int check_launch() {
 }
 
 // ----------------------------------------------------------- level set
+// Host replay of the far-field value: the same IEEE operations the kernels
+// apply to a cell whose whole stencil is uniform (compiled without
+// contraction, as the device code).
+double clip_h(double x, double NB) { return x > NB ? NB : (x < -NB ? -NB : x); }
+double reinit_sgn_h(const Params& p, double p0) {
+  if (p0 < -p.dz) return -1.;
+  if (p0 > p.dz) return 1.;
+  return p0 / std::sqrt(p0 * p0 + p.dz * p.dz);
+}
+// WENO5_reinit RHS of a uniform neighbourhood: every one-sided derivative
+// is exactly zero (hyperPDE.f90:2736)
+double reinit_rhs_h(const Params& p, double phis, double orig) {
+  if (!(std::fabs(phis) < p.NB + p.dz)) return 0.;
+  const double s = reinit_sgn_h(p, orig);
+  const double d = 0.5 * (0. + 0.);
+  return s * (1. - std::sqrt((d * d + d * d) + d * d));
+}
+
+bool is_full(const Params& P, const Box3& b) {
+  const int n[3] = {P.imax, P.jmax, P.kmax};
+  for (int a = 0; a < 3; ++a)
+    if (!(b.c0[a] <= -2 && b.c1[a] >= n[a] + 3)) return false;
+  return true;
+}
+
+// interior cells of drop l outside its compute region (their H is 1)
+double outside_count(const Ctx& c, const Box3& b) {
+  const int n[3] = {c.P.imax, c.P.jmax, c.P.kmax};
+  double inside = 1.;
+  for (int a = 0; a < 3; ++a) {
+    const int lo = std::max(1, b.c0[a]), hi = std::min(n[a], b.c1[a]);
+    inside *= (hi >= lo) ? (double)(hi - lo + 1) : 0.;
+  }
+  return (double)c.P.nI - inside;
+}
+
+// bounding boxes measured by the last tube_construction sweep
+int collect_bbox(Ctx& c) {
+  if (!c.bbox_pending) return ICLS_OK;
+  CK(cudaEventSynchronize(c.ev_bbox));
+  c.bbox_pending = false;
+  for (int l = 0; l < c.P.L; ++l) {
+    DropWin& w = c.win[l];
+    const int* b = c.h_bbox + 6 * l;
+    if (b[0] > b[3] || b[1] > b[4] || b[2] > b[5]) {
+      w.have_D = false;  // nothing but far field: sweep everything next time
+      continue;
+    }
+    for (int q = 0; q < 6; ++q) w.D[q] = b[q];
+    w.grow = w.pending_grow;
+    w.have_D = true;
+  }
+  return ICLS_OK;
+}
+
+// The region drop l sweeps in a step whose own spreading is g_now cells:
+// the last measured band box grown by what the field could have spread
+// since (tube skin 2, 9 per reinitialisation iteration).  An axis becomes
+// full when the box would reach the three cells next to a periodic seam
+// (whose images are halo cells) or the two next to a wall.
+Box3 sweep_box(const Ctx& c, int l, int g_now) {
+  const DropWin& w = c.win[l];
+  if (!c.use_boxes || !w.have_D || !w.bg_valid) return full_box(c.P);
+  // the band box is exact only if the clipped far field equals +6dz
+  if (clip_h(w.bg, c.P.NB) != c.P.NB || clip_h(w.bg_ghost, c.P.NB) != c.P.NB) return full_box(c.P);
+  const int n[3] = {c.P.imax, c.P.jmax, c.P.kmax};
+  const int lo_min[3] = {4, 4, 3};
+  const int hi_max[3] = {n[0] - 3, n[1] - 3, n[2] - 2};
+  const int g = w.grow + g_now;
+  Box3 b;
+  for (int a = 0; a < 3; ++a) {
+    const int lo = w.D[a] - g, hi = w.D[3 + a] + g;
+    if (lo < lo_min[a] || hi > hi_max[a]) {
+      b.c0[a] = b.w0[a] = -2;
+      b.c1[a] = b.w1[a] = n[a] + 3;
+    } else {
+      b.c0[a] = lo;
+      b.c1[a] = hi;
+      b.w0[a] = lo - 3;
+      b.w1[a] = hi + 3;
+    }
+  }
+  return b;
+}
+
+// Make drop l's stored array valid everywhere and sweep it whole from now
+// on (used before downloads and by the standalone routine calls).
+void make_full(Ctx& c, int l) {
+  DropWin& w = c.win[l];
+  if (!is_full(c.P, w.valid)) launch_materialize(c, w.valid, w.bg, w.bg_ghost, c.lv[l]);
+  w.box = w.valid = full_box(c.P);
+  w.have_D = false;
+}
+
 void update_materials(Ctx& c) {
-  for (int l = 0; l < c.P.L; ++l) launch_heaviside_drop(c, c.lv[l], l, l == 0);
-  launch_materials_final(c);
+  bool any_partial = false;
+  for (int l = 0; l < c.P.L; ++l) any_partial |= !is_full(c.P, c.win[l].box);
+  if (any_partial) launch_fill(c, c.jiemian, c.P.nC, 1.0);
+  for (int l = 0; l < c.P.L; ++l) {
+    launch_heaviside_drop(c, c.win[l].box, c.lv[l], l, (!any_partial && l == 0) ? 1 : 0);
+    c.outside[l] = outside_count(c, c.win[l].box);
+  }
+  launch_materials_final(c, c.outside.data());
   cudaMemcpyAsync(c.h_vol, c.dvol, sizeof(double) * c.P.L, cudaMemcpyDeviceToHost, c.s);
   cudaEventRecord(c.ev_vol, c.s);
   c.vol_pending = true;
   std::fill(c.vol_dirty.begin(), c.vol_dirty.end(), 0);
 }
 
-void tube_construction(Ctx& c, int l) {
+// tube_construction (levelset.f90:87-197) over the sweep box b
+void tube_construction(Ctx& c, int l, const Box3& b) {
+  DropWin& w = c.win[l];
   cudaMemsetAsync(c.d_nbcnt + l, 0, sizeof(long long), c.s);
-  launch_tube(c, c.lv[l], c.ls_scr[0], c.d_nbcnt + l);
+  cudaMemsetAsync(c.d_bbox + 6 * l, 0x7F, 3 * sizeof(int), c.s);
+  cudaMemsetAsync(c.d_bbox + 6 * l + 3, 0x80, 3 * sizeof(int), c.s);
+  launch_tube(c, b, w.valid, w.bg, w.bg_ghost, c.lv[l], c.ls_scr[0], c.d_nbcnt + l, c.d_bbox + 6 * l);
   std::swap(c.lv[l], c.ls_scr[0]);
+  w.box = w.valid = b;
+  // every cell outside the measured band box is +6dz after the clip
+  w.bg = c.P.NB;
+  w.bg_ghost = c.P.NB;
+  w.bg_valid = true;
 }
 
 // SSP-RK3 of ls_advection / inflation (levelset.f90:235-243, 558-565)
 void rk3(Ctx& c, int l, int scheme, const double* vu, const double* vv, const double* vw) {
+  DropWin& w = c.win[l];
+  const Box3 b = w.box;
   const double dt = c.dt;
   double* phi0 = c.lv[l];
   double* s1 = c.ls_scr[1];
   double* s2 = c.ls_scr[2];
-  launch_adv_stage(c, scheme, 1, phi0, phi0, 1., 0., 1. * dt, vu, vv, vw, s1);
-  launch_adv_stage(c, scheme, 0, phi0, s1, 3. / 4., 1. / 4., 1. / 4. * dt, vu, vv, vw, s2);
-  launch_adv_stage(c, scheme, 0, phi0, s2, 1. / 3., 2. / 3., 2. / 3. * dt, vu, vv, vw, s1);
+  const double g0 = w.bg, h0 = w.bg_ghost;
+  const double g1 = g0, h1 = h0;
+  const double g2 = 3. / 4. * g0 + 1. / 4. * g1, h2 = 3. / 4. * h0 + 1. / 4. * h1;
+  const double g3 = 1. / 3. * g0 + 2. / 3. * g2, h3 = 1. / 3. * h0 + 2. / 3. * h2;
+  launch_adv_stage(c, b, g1, h1, scheme, 1, phi0, phi0, 1., 0., 1. * dt, vu, vv, vw, s1);
+  launch_adv_stage(c, b, g2, h2, scheme, 0, phi0, s1, 3. / 4., 1. / 4., 1. / 4. * dt, vu, vv, vw, s2);
+  launch_adv_stage(c, b, g3, h3, scheme, 0, phi0, s2, 1. / 3., 2. / 3., 2. / 3. * dt, vu, vv, vw, s1);
   std::swap(c.lv[l], c.ls_scr[1]);
+  w.bg = g3;
+  w.bg_ghost = h3;
 }
 
 void ls_advection(Ctx& c, int l) { rk3(c, l, c.cfg.ls_adv_space, c.ucc, c.vcc, c.wcc); }
 
 // inflation (levelset.f90:407-582)
 void inflation(Ctx& c, int l) {
-  launch_curvature(c, c.lv[l], c.kappa, c.nrm_m);
-  launch_inflate_sums(c, c.lv[l], l);
-  launch_inflate_vel(c);
+  const Box3 b = c.win[l].box;
+  launch_curvature(c, b, c.lv[l], c.kappa, c.nrm_m);
+  launch_inflate_sums(c, b, c.lv[l], l, outside_count(c, b));
+  launch_inflate_vel(c, b);
   rk3(c, l, c.cfg.i_space, c.ulc, c.vlc, c.wlc);
   c.inflated[l] = 1;
   c.vol_dirty[l] = 1;
@@ -304,10 +441,16 @@ int ls_mass_correction(Ctx& c, int istep, int l) {
 }
 
 // ls_reinit, WENO5/RK3 (levelset.f90:619-882); the early exit on
-// residual < dz**5 is decided on the device (k_reinit_check)
+// residual < dz**5 is decided on the device (k_reinit_check).  Far-field
+// cells outside the sweep box change by |bg_new - bg_old| per iteration,
+// which enters the residual as the reference's maxval over all cells does.
 void ls_reinit(Ctx& c, int l) {
+  DropWin& w = c.win[l];
+  const Box3 b = w.box;
+  const bool partial = !is_full(c.P, b);
+  const Params& P = c.P;
   const int maxiter = c.cfg.reinit_iter_max;
-  const double dz = c.P.dz;
+  const double dz = P.dz;
   const double dtau = 0.5 * dz;
   const double thr = dz * dz * dz * dz * dz;
   double* orig = c.lv[l];
@@ -316,15 +459,26 @@ void ls_reinit(Ctx& c, int l) {
   double* B = c.ls_scr[1];
   double* Y = c.ls_scr[2];
   double* Yalt = c.ls_scr[3];
+  const double og = w.bg;  // sgn source of the far field
+  double xg = w.bg, xh = w.bg_ghost;
   launch_reinit_reset(c, maxiter);
   for (int it = 1; it <= maxiter; ++it) {
-    launch_reinit_stage(c, 1, X, X, orig, dtau, A, 1);
-    launch_reinit_stage(c, 2, X, A, orig, dtau, B, 1);
-    launch_reinit_stage(c, 3, X, B, orig, dtau, Y, 1);
-    launch_reinit_check(c, it, maxiter, thr);
+    const double ag = xg + dtau * reinit_rhs_h(P, xg, og);
+    const double ah = xh + dtau * 0.;
+    const double bgv = 3. / 4. * xg + 1. / 4. * (ag + dtau * reinit_rhs_h(P, ag, og));
+    const double bh = 3. / 4. * xh + 1. / 4. * (ah + dtau * 0.);
+    const double yg = 1. / 3. * xg + 2. / 3. * (bgv + dtau * reinit_rhs_h(P, bgv, og));
+    const double yh = 1. / 3. * xh + 2. / 3. * (bh + dtau * 0.);
+    launch_reinit_stage(c, b, ag, ah, 1, X, X, orig, dtau, A);
+    launch_reinit_stage(c, b, bgv, bh, 2, X, A, orig, dtau, B);
+    launch_reinit_stage(c, b, yg, yh, 3, X, B, orig, dtau, Y);
+    const double far = partial ? std::max(std::fabs(yg - xg), std::fabs(yh - xh)) : 0.;
+    launch_reinit_check(c, it, maxiter, thr, far);
     X = Y;
     std::swap(Y, Yalt);
     if (Y == orig) std::swap(Y, Yalt);
+    xg = yg;
+    xh = yh;
   }
   // X holds phi_new; make it the drop's buffer and recycle the original
   for (int s = 0; s < 4; ++s)
@@ -333,19 +487,33 @@ void ls_reinit(Ctx& c, int l) {
       break;
     }
   c.lv[l] = X;
+  // with a far field the residual never drops below dz**5 (the far field
+  // moves by ~dtau per iteration), so every iteration runs: the replayed
+  // values are exact
+  w.bg = xg;
+  w.bg_ghost = xh;
 }
 
 int ls_main(Ctx& c, int istep) {
   c.last_inflated = 0;
+  int rc = collect_bbox(c);
+  if (rc) return rc;
+  const bool reinit_now = c.cfg.re_initialization && istep % c.cfg.reinit_step == 0;
+  const int g_now = 2 + (reinit_now ? 9 * c.cfg.reinit_iter_max : 0);
   for (int l = 0; l < c.P.L; ++l) {
-    tube_construction(c, l);
+    const Box3 b = sweep_box(c, l, g_now);
+    tube_construction(c, l, b);
+    c.win[l].pending_grow = g_now;
     ls_advection(c, l);
     if (c.cfg.mass_correction) {
-      int rc = ls_mass_correction(c, istep, l);
+      rc = ls_mass_correction(c, istep, l);
       if (rc) return rc;
     }
-    if (c.cfg.re_initialization && istep % c.cfg.reinit_step == 0) ls_reinit(c, l);
+    if (reinit_now) ls_reinit(c, l);
   }
+  cudaMemcpyAsync(c.h_bbox, c.d_bbox, sizeof(int) * 6 * c.P.L, cudaMemcpyDeviceToHost, c.s);
+  cudaEventRecord(c.ev_bbox, c.s);
+  c.bbox_pending = true;
   update_materials(c);
   return check_launch();
 }
@@ -360,13 +528,24 @@ void gfm4p(Ctx& c) {
   cudaMemsetAsync(c.py, 0, bytes, c.s);
   cudaMemsetAsync(c.pz, 0, bytes, c.s);
   cudaMemsetAsync(c.pjump, 0, bytes, c.s);
+  bool any_partial = false;
+  for (int l = 0; l < c.P.L; ++l) any_partial |= !is_full(c.P, c.win[l].box);
+  // normal%m is 1 away from every band (interface.f90:44)
+  if (any_partial) launch_fill(c, c.nrm_m, c.P.nI, 1.0);
   for (int l = 0; l < c.P.L; ++l) {
-    launch_curvature(c, c.lv[l], c.curv, c.nrm_m);
+    const Box3 b = c.win[l].box;
+    const bool last = (l == c.P.L - 1);
+    if (last && !is_full(c.P, b)) {
+      // curv_cmn after the loop is the last drop's re_curvature, zero elsewhere
+      cudaMemsetAsync(c.curv, 0, bytes, c.s);
+      cudaMemsetAsync(c.recurv, 0, bytes, c.s);
+    }
+    launch_curvature(c, b, c.lv[l], c.curv, c.nrm_m);
     if (!c.cfg.TwoD) {
-      launch_recurvature(c, c.lv[l], c.curv, c.recurv);
+      launch_recurvature(c, b, c.lv[l], c.curv, c.recurv);
       std::swap(c.curv, c.recurv);
     }
-    launch_jumps(c, c.lv[l], c.curv, l == 0);
+    launch_jumps(c, b, c.lv[l], c.curv, l == 0);
   }
 }
 
@@ -493,6 +672,12 @@ int icls_upload_field(icls_ctx* h, int id, int l, const double* host) {
   if (!d) return ICLS_E_ARG;
   CK(cudaMemcpyAsync(d, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c.s));
   CK(cudaStreamSynchronize(c.s));
+  if (id == ICLS_F_LVSET) {  // a new level set: sweep it whole until its band is measured
+    DropWin& w = c.win[l - 1];
+    w.box = w.valid = full_box(c.P);
+    w.have_D = false;
+    w.bg_valid = false;
+  }
   return ICLS_OK;
 }
 
@@ -502,6 +687,10 @@ int icls_download_field(icls_ctx* h, int id, int l, double* host) {
   long long n;
   double* d = field_ptr(c, id, l, &n);
   if (!d) return ICLS_E_ARG;
+  if (id == ICLS_F_LVSET) {  // fill the far field outside the swept region
+    const DropWin& w = c.win[l - 1];
+    if (!is_full(c.P, w.valid)) launch_materialize(c, w.valid, w.bg, w.bg_ghost, d);
+  }
   CK(cudaMemcpyAsync(host, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c.s));
   CK(cudaStreamSynchronize(c.s));
   return ICLS_OK;
@@ -798,13 +987,15 @@ int icls_step(icls_ctx* h, int istep, int begin) {
 int icls_tube_construction(icls_ctx* h, int l) {
   if (!h) return ICLS_E_ARG;
   LARG(h, l);
-  tube_construction(h->c, l - 1);
+  make_full(h->c, l - 1);
+  tube_construction(h->c, l - 1, full_box(h->c.P));
   return check_launch();
 }
 
 int icls_ls_advection(icls_ctx* h, int l) {
   NEED(h);
   LARG(h, l);
+  make_full(h->c, l - 1);
   ls_advection(h->c, l - 1);
   return check_launch();
 }
@@ -812,6 +1003,7 @@ int icls_ls_advection(icls_ctx* h, int l) {
 int icls_ls_mass_correction(icls_ctx* h, int istep, int l) {
   NEED(h);
   LARG(h, l);
+  make_full(h->c, l - 1);
   int rc = ls_mass_correction(h->c, istep, l - 1);
   if (rc) return rc;
   return check_launch();
@@ -820,6 +1012,7 @@ int icls_ls_mass_correction(icls_ctx* h, int istep, int l) {
 int icls_ls_reinit_main(icls_ctx* h, int istep, int l) {
   NEED(h);
   LARG(h, l);
+  make_full(h->c, l - 1);
   if (istep % h->c.cfg.reinit_step == 0) ls_reinit(h->c, l - 1);
   return check_launch();
 }
@@ -833,7 +1026,8 @@ int icls_update_materials(icls_ctx* h) {
 int icls_get_curvature(icls_ctx* h, int l) {
   NEED(h);
   LARG(h, l);
-  launch_curvature(h->c, h->c.lv[l - 1], h->c.curv, h->c.nrm_m);
+  make_full(h->c, l - 1);
+  launch_curvature(h->c, full_box(h->c.P), h->c.lv[l - 1], h->c.curv, h->c.nrm_m);
   return check_launch();
 }
 

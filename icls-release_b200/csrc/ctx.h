@@ -17,6 +17,24 @@ namespace icls {
 
 constexpr int kRedBlocks = 1184;   // 8 x 148 SMs: fixed grid of the reduction kernels
 constexpr int kRedThreads = 256;
+constexpr int kMaxDropsParam = 256;  // drops whose far-field counts travel as a kernel parameter
+
+// Sweep state of one drop's level set.  Outside valid's write region every
+// cell holds the far-field value bg (the stored array there is stale);
+// box is the region the current step sweeps.  D is the bounding box of the
+// cells that differed from +6dz after the last tube_construction, grow the
+// number of cells the non-uniform region can have spread since.
+struct DropWin {
+  Box3 box;
+  Box3 valid;
+  double bg = 0.0;        // far field of rows 0..k1
+  double bg_ghost = 0.0;  // far field of the ghost rows k<0, k>k1
+  bool bg_valid = false;  // bg/bg_ghost hold the far-field values
+  bool have_D = false;
+  int pending_grow = 0;
+  int D[6] = {0, 0, 0, 0, 0, 0};
+  int grow = 0;
+};
 
 struct Ctx {
   icls_config cfg;
@@ -69,31 +87,45 @@ struct Ctx {
   int last_inflated = 0;
   double P10x27[270];
   Prof prof;
+  // per-drop sweep boxes
+  std::vector<DropWin> win;
+  bool use_boxes = true;
+  int* d_bbox = nullptr;                // 6 ints per drop, written by the tube kernel
+  int* h_bbox = nullptr;                // pinned copy
+  cudaEvent_t ev_bbox = nullptr;
+  bool bbox_pending = false;
+  std::vector<double> outside;          // interior cells outside each drop's box
 };
 
 // ---- kernel launchers (defined in the k_*.cu files) -----------------------
 void set_pseudo_inverse(const double* P270, cudaStream_t s);
 
 // level set (k_levelset.cu)
-void launch_tube(Ctx& c, const double* in, double* out, long long* cnt);
-void launch_adv_stage(Ctx& c, int scheme, int stage1, const double* phi0, const double* phis,
-                      double a, double b, double fdt, const double* vu, const double* vv,
-                      const double* vw, double* out);
-void launch_reinit_stage(Ctx& c, int stage, const double* phi0, const double* phis,
-                         const double* orig, double dtau, double* out, int check_done);
-void launch_reinit_check(Ctx& c, int it, int maxiter, double thr);
+dim3 grid_of(const int* r0, const int* r1);
+Box3 full_box(const Params& P);
+Box3 c_region(const Params& P, const Box3& b, int apron);
+void launch_tube(Ctx& c, const Box3& b, const Box3& vin, double bgin, double bgg, const double* in, double* out,
+                 long long* cnt, int* bbox);
+void launch_adv_stage(Ctx& c, const Box3& b, double bg_out, double bgg_out, int scheme, int stage1,
+                      const double* phi0, const double* phis, double a, double bb, double fdt, const double* vu,
+                      const double* vv, const double* vw, double* out);
+void launch_reinit_stage(Ctx& c, const Box3& b, double bg_out, double bgg_out, int stage, const double* phi0,
+                         const double* phis, const double* orig, double dtau, double* out);
+void launch_reinit_check(Ctx& c, int it, int maxiter, double thr, double far);
 void launch_reinit_reset(Ctx& c, int maxiter);
-void launch_heaviside_drop(Ctx& c, const double* phi, int l, int first);
-void launch_materials_final(Ctx& c);
-void launch_inflate_sums(Ctx& c, const double* phi, int l);
-void launch_inflate_vel(Ctx& c);
+void launch_heaviside_drop(Ctx& c, const Box3& b, const double* phi, int l, int first);
+void launch_fill(Ctx& c, double* a, long long n, double v);
+void launch_materials_final(Ctx& c, const double* outside);
+void launch_inflate_sums(Ctx& c, const Box3& b, const double* phi, int l, double outside);
+void launch_inflate_vel(Ctx& c, const Box3& b);
 void launch_copy(Ctx& c, double* dst, const double* src, long long n);
 void launch_boundmls(Ctx& c, double* phi);
+void launch_materialize(Ctx& c, const Box3& b, double bg, double bgg, double* phi);
 
 // interface / GFM (k_gfm.cu)
-void launch_curvature(Ctx& c, const double* phi, double* curv_out, double* nrm_m_out);
-void launch_recurvature(Ctx& c, const double* phi, const double* curv_in, double* out);
-void launch_jumps(Ctx& c, const double* phi, const double* cv, int first);
+void launch_curvature(Ctx& c, const Box3& b, const double* phi, double* curv_out, double* nrm_m_out);
+void launch_recurvature(Ctx& c, const Box3& b, const double* phi, const double* curv_in, double* out);
+void launch_jumps(Ctx& c, const Box3& b, const double* phi, const double* cv, int first);
 void launch_ipot(Ctx& c, double* dmin_dev);
 
 // Navier-Stokes (k_navier.cu)

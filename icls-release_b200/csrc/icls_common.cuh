@@ -23,6 +23,10 @@ struct Params {
   long long nC, nI, nL;      // element counts
   double lx, ly, lz;
   double dxi, dyi, dzi, dx, dy, dz;
+  // 1/dx, 1/dy, 1/dz; when all three spacings are powers of two these are
+  // exact and a/dx == a*rdx for every a, so divisions become products
+  double rdx, rdy, rdz;
+  int pow2;
   double NB;                 // NarrowBand_2 = 6dz (param.f90:41)
   double pi;
   double dt;
@@ -54,6 +58,38 @@ __host__ __device__ __forceinline__ int wrapy(const Params& p, int j) {
 
 template <typename T>
 __device__ __forceinline__ T sq(T x) { return x * x; }
+
+// a/dx, a/dy, a/dz exactly as the reference divides (a product when the
+// spacing is a power of two, which is then bit-identical)
+__device__ __forceinline__ double divx(const Params& p, double a) { return p.pow2 ? a * p.rdx : a / p.dx; }
+__device__ __forceinline__ double divy(const Params& p, double a) { return p.pow2 ? a * p.rdy : a / p.dy; }
+__device__ __forceinline__ double divz(const Params& p, double a) { return p.pow2 ? a * p.rdz : a / p.dz; }
+
+// ---------------------------------------------------------------- boxes
+// A per-drop sweep region in the Fortran coordinates of the level-set
+// array (-2:i1+2,..).  Cells in [c0,c1] are computed; cells of the write
+// region [w0,w1] outside it form the apron and receive the far-field value.
+// A full axis has c = w = the whole index range.
+struct Box3 {
+  int c0[3], c1[3];
+  int w0[3], w1[3];
+};
+__host__ __device__ __forceinline__ bool in_compute(const Box3& b, int i, int j, int k) {
+  return i >= b.c0[0] && i <= b.c1[0] && j >= b.c0[1] && j <= b.c1[1] && k >= b.c0[2] && k <= b.c1[2];
+}
+__host__ __device__ __forceinline__ bool in_write(const Box3& b, int i, int j, int k) {
+  return i >= b.w0[0] && i <= b.w1[0] && j >= b.w0[1] && j <= b.w1[1] && k >= b.w0[2] && k <= b.w1[2];
+}
+// 3-D launch over a region: 32 x 8 threads per block in (i,j), one k per
+// block layer.  The thread's cell is (r0 + ...), valid while <= r1.
+constexpr int BX = 32, BY = 8;
+__device__ __forceinline__ bool cell3(const int* r0, const int* r1, int& i, int& j, int& k) {
+  i = r0[0] + (int)(blockIdx.x * BX + threadIdx.x);
+  j = r0[1] + (int)(blockIdx.y * BY + threadIdx.y);
+  k = r0[2] + (int)blockIdx.z;
+  return i <= r1[0] && j <= r1[1] && k <= r1[2];
+}
+__device__ __forceinline__ int flat_tid() { return threadIdx.x + blockDim.x * threadIdx.y; }
 
 // ------------------------------------------------------------ WENO5, HOUC5
 // One WENO5 upwind-biased derivative from the five differences v1..v5
@@ -103,7 +139,8 @@ template <typename T, int NT>
 __device__ __forceinline__ T block_sum(T v) {
   __shared__ T red[NT / 32];
   v = warp_sum(v);
-  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  const int t = flat_tid();
+  const int w = t >> 5, ln = t & 31;
   if (ln == 0) red[w] = v;
   __syncthreads();
   T r = (T)0;
@@ -118,7 +155,8 @@ template <typename T, int NT>
 __device__ __forceinline__ T block_max(T v) {
   __shared__ T red[NT / 32];
   v = warp_max(v);
-  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  const int t = flat_tid();
+  const int w = t >> 5, ln = t & 31;
   if (ln == 0) red[w] = v;
   __syncthreads();
   T r = (T)0;

@@ -10,6 +10,8 @@
 // The 10x27 pseudo-inverse (init.f90:1587-1723) lives in constant memory:
 // every thread of a warp reads the same coefficient, which the constant
 // cache broadcasts.
+#include <algorithm>
+
 #include "ctx.h"
 
 namespace icls {
@@ -19,14 +21,7 @@ __constant__ double cP[270];
 namespace {
 
 constexpr int NT = 256;
-inline unsigned nblocks(long long n, int nt = NT) { return (unsigned)((n + nt - 1) / nt); }
 
-__device__ __forceinline__ void decodeC(const Params& p, long long n, int& i, int& j, int& k) {
-  i = (int)(n % p.nCx);
-  long long r = n / p.nCx;
-  j = (int)(r % p.nCy);
-  k = (int)(r / p.nCy);
-}
 
 // curvature at an interior cell (interface.f90:57-111); m = |grad phi| or 1
 __device__ __forceinline__ double curvature_at(const Params& p, const double* __restrict__ phi, int i, int j,
@@ -75,31 +70,30 @@ __device__ __forceinline__ double curvature_at(const Params& p, const double* __
   return cv;
 }
 
-// get_curvature + boundc over shape C: wall rows stay 0, halos are the
-// periodic copies (bound.f90:292-305).
-__global__ void __launch_bounds__(NT) k_curvature(Params p, const double* __restrict__ phi,
+// get_curvature + boundc over a drop's region of shape C: wall rows stay 0,
+// halos are the periodic copies (bound.f90:292-305), the apron (far field,
+// |phi| > 5dz) is 0.
+__global__ void __launch_bounds__(NT) k_curvature(Params p, Box3 r, const double* __restrict__ phi,
                                                   double* __restrict__ curv, double* __restrict__ nrm_m) {
-  const long long n = blockIdx.x * (long long)NT + threadIdx.x;
-  if (n >= p.nC) return;
   int i, j, k;
-  decodeC(p, n, i, j, k);
-  if (k == 0 || k == p.k1) { curv[n] = 0.; return; }
+  if (!cell3(r.w0, r.w1, i, j, k)) return;
+  const long long n = idxC(p, i, j, k);
+  if (k == 0 || k == p.k1 || !in_compute(r, i, j, k)) { curv[n] = 0.; return; }
   const int I = wrapx(p, i), J = wrapy(p, j);
   double m;
   curv[n] = curvature_at(p, phi, I, J, k, m);
   if (I == i && J == j && nrm_m) nrm_m[idxI(p, i, j, k)] = m;
 }
 
-// re_curvature + boundc (interface.f90:186-218)
-__global__ void __launch_bounds__(NT) k_recurvature(Params p, const double* __restrict__ phi,
+// re_curvature + boundc (interface.f90:186-218) over a drop's region
+__global__ void __launch_bounds__(NT) k_recurvature(Params p, Box3 r, const double* __restrict__ phi,
                                                     const double* __restrict__ cin, double* __restrict__ out) {
-  const long long n = blockIdx.x * (long long)NT + threadIdx.x;
-  if (n >= p.nC) return;
   int i, j, k;
-  decodeC(p, n, i, j, k);
-  if (k == 0 || k == p.k1) { out[n] = 0.; return; }
+  if (!cell3(r.w0, r.w1, i, j, k)) return;
+  const long long n = idxC(p, i, j, k);
+  if (k == 0 || k == p.k1 || !in_compute(r, i, j, k)) { out[n] = 0.; return; }
   const int I = wrapx(p, i), J = wrapy(p, j);
-  double r = 0.;
+  double acc = 0.;
   if (fabs(phi[idxL(p, I, J, k)]) < 2. * p.dz) {
     const long long c = idxC(p, I, J, k), sy = p.nCx, sz = (long long)p.nCx * p.nCy;
     int q = 0;
@@ -108,9 +102,9 @@ __global__ void __launch_bounds__(NT) k_recurvature(Params p, const double* __re
 #pragma unroll
       for (int dj = -1; dj <= 1; ++dj)
 #pragma unroll
-        for (int di = -1; di <= 1; ++di) r = r + cP[q++] * cin[c + di + dj * sy + dk * sz];
+        for (int di = -1; di <= 1; ++di) acc = acc + cP[q++] * cin[c + di + dj * sy + dk * sz];
   }
-  out[n] = r;
+  out[n] = acc;
 }
 
 // icurvature, 3-D and TwoD branches (interface.f90:126-179)
@@ -138,6 +132,11 @@ __device__ __forceinline__ double icurvature(const Params& p, int nb, double ph0
   (void)nb;
 }
 
+// a/(h*h) as the reference evaluates jump/dx**2 (gfm.f90:191)
+__device__ __forceinline__ double div2(const Params& p, double a, double h, double rh) {
+  return p.pow2 ? a * (rh * rh) : a / (h * h);
+}
+
 // jumps of one axis: jp(-1) + jp(0) + jp(1) and the + face jump
 __device__ __forceinline__ double axis_jump(const Params& p, const double* __restrict__ phi,
                                             const double* __restrict__ cv, long long cl, long long sl,
@@ -155,16 +154,13 @@ __device__ __forceinline__ double axis_jump(const Params& p, const double* __res
 }
 
 // gfm4p jump shell of drop l (gfm.f90:95-238); first=1 assigns (l=1)
-__global__ void __launch_bounds__(NT) k_jumps(Params p, const double* __restrict__ phi,
+__global__ void __launch_bounds__(NT) k_jumps(Params p, Box3 r, const double* __restrict__ phi,
                                               const double* __restrict__ cv, int first,
                                               double* __restrict__ pjump, double* __restrict__ px,
                                               double* __restrict__ py, double* __restrict__ pz) {
-  const long long q = blockIdx.x * (long long)NT + threadIdx.x;
-  if (q >= p.nI) return;
-  const int i = (int)(q % p.imax) + 1;
-  const long long r = q / p.imax;
-  const int j = (int)(r % p.jmax) + 1;
-  const int k = (int)(r / p.jmax) + 1;
+  int i, j, k;
+  if (!cell3(r.c0, r.c1, i, j, k)) return;
+  if (i < 1 || i > p.imax || j < 1 || j > p.jmax || k < 1 || k > p.kmax) return;
   const long long cl = idxL(p, i, j, k);
   const double lv = phi[cl];
   if (!(fabs(lv) <= 2. * p.dz)) return;
@@ -175,9 +171,9 @@ __global__ void __launch_bounds__(NT) k_jumps(Params p, const double* __restrict
   const double jump_z = axis_jump(p, phi, cv, cl, (long long)p.nLx * p.nLy, cc, (long long)p.nCx * p.nCy, fz);
   double pj;
   if (lv > 0.) {
-    pj = (jump_x / (p.dx * p.dx) + jump_y / (p.dy * p.dy)) + jump_z / (p.dz * p.dz);
+    pj = (div2(p, jump_x, p.dx, p.rdx) + div2(p, jump_y, p.dy, p.rdy)) + div2(p, jump_z, p.dz, p.rdz);
   } else if (lv < 0.) {
-    pj = -((jump_x / (p.dx * p.dx) + jump_y / (p.dy * p.dy)) + jump_z / (p.dz * p.dz));
+    pj = -((div2(p, jump_x, p.dx, p.rdx) + div2(p, jump_y, p.dy, p.rdy)) + div2(p, jump_z, p.dz, p.rdz));
     fx = -fx; fy = -fy; fz = -fz;
   } else {
     pj = 0.; fx = 0.; fy = 0.; fz = 0.;
@@ -194,12 +190,13 @@ __device__ __forceinline__ unsigned long long ord_bits(double x) {
   unsigned long long b = (unsigned long long)__double_as_longlong(x);
   return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
 }
-__global__ void __launch_bounds__(NT) k_ipot_pair(Params p, const double* __restrict__ pm,
+__global__ void __launch_bounds__(NT) k_ipot_pair(Params p, Box3 r, const double* __restrict__ pm,
                                                   const double* __restrict__ pn,
                                                   unsigned long long* __restrict__ out) {
-  const long long n = blockIdx.x * (long long)NT + threadIdx.x;
+  int i, j, k;
   double s = 1e3;
-  if (n < p.nL) {
+  if (cell3(r.w0, r.w1, i, j, k)) {
+    const long long n = idxL(p, i, j, k);
     const double a = pm[n], b = pn[n];
     if (a > -1. * p.dz && a < 1. * p.dz && b < p.NB) s = a + b;
   }
@@ -210,9 +207,9 @@ __global__ void __launch_bounds__(NT) k_ipot_pair(Params p, const double* __rest
     bits = t < bits ? t : bits;
   }
   __shared__ unsigned long long red[NT / 32];
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = bits;
+  if ((flat_tid() & 31) == 0) red[flat_tid() >> 5] = bits;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (flat_tid() == 0) {
     unsigned long long m = red[0];
     for (int w = 1; w < NT / 32; ++w) m = red[w] < m ? red[w] : m;
     atomicMin(out, m);
@@ -225,25 +222,42 @@ void set_pseudo_inverse(const double* P270, cudaStream_t s) {
   cudaMemcpyToSymbolAsync(cP, P270, 270 * sizeof(double), 0, cudaMemcpyHostToDevice, s);
 }
 
-void launch_curvature(Ctx& c, const double* phi, double* curv_out, double* nrm_m_out) {
+void launch_curvature(Ctx& c, const Box3& b, const double* phi, double* curv_out, double* nrm_m_out) {
   Scope sc_(c.prof, c.s, "curvature", 1);
-  k_curvature<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, phi, curv_out, nrm_m_out);
+  const Box3 r = c_region(c.P, b, 1);
+  k_curvature<<<grid_of(r.w0, r.w1), dim3(BX, BY, 1), 0, c.s>>>(c.P, r, phi, curv_out, nrm_m_out);
 }
-void launch_recurvature(Ctx& c, const double* phi, const double* curv_in, double* out) {
+void launch_recurvature(Ctx& c, const Box3& b, const double* phi, const double* curv_in, double* out) {
   Scope sc_(c.prof, c.s, "recurvature", 1);
-  k_recurvature<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, phi, curv_in, out);
+  const Box3 r = c_region(c.P, b, 1);
+  k_recurvature<<<grid_of(r.w0, r.w1), dim3(BX, BY, 1), 0, c.s>>>(c.P, r, phi, curv_in, out);
 }
-void launch_jumps(Ctx& c, const double* phi, const double* cv, int first) {
+void launch_jumps(Ctx& c, const Box3& b, const double* phi, const double* cv, int first) {
   Scope sc_(c.prof, c.s, "jumps", 1);
-  k_jumps<<<nblocks(c.P.nI), NT, 0, c.s>>>(c.P, phi, cv, first, c.pjump, c.px, c.py, c.pz);
+  const Box3 r = c_region(c.P, b, 0);
+  k_jumps<<<grid_of(r.c0, r.c1), dim3(BX, BY, 1), 0, c.s>>>(c.P, r, phi, cv, first, c.pjump, c.px, c.py, c.pz);
 }
 // dmin_dev: L*L unsigned long long ordered bits, filled here
+// only the overlap of the two drops' write regions can hold cells with
+// |phi_m| < dz and phi_n < 6dz: elsewhere one of them is in its far field
 void launch_ipot(Ctx& c, double* dmin_dev) {
   unsigned long long* o = reinterpret_cast<unsigned long long*>(dmin_dev);
   for (int m = 0; m < c.P.L; ++m)
     for (int n = 0; n < c.P.L; ++n) {
       if (m == n) continue;
-      k_ipot_pair<<<nblocks(c.P.nL), NT, 0, c.s>>>(c.P, c.lv[m], c.lv[n], o + m + (long long)c.P.L * n);
+      const Box3& a = c.win[m].valid;
+      const Box3& b = c.win[n].valid;
+      Box3 r;
+      bool empty = false;
+      for (int ax = 0; ax < 3; ++ax) {
+        r.w0[ax] = r.c0[ax] = std::max(a.w0[ax], b.w0[ax]);
+        r.w1[ax] = r.c1[ax] = std::min(a.w1[ax], b.w1[ax]);
+        if (r.w0[ax] > r.w1[ax]) empty = true;
+      }
+      if (empty) continue;
+      Scope sc_(c.prof, c.s, "ipot", 1);
+      k_ipot_pair<<<grid_of(r.w0, r.w1), dim3(BX, BY, 1), 0, c.s>>>(c.P, r, c.lv[m], c.lv[n],
+                                                                    o + m + (long long)c.P.L * n);
     }
 }
 

@@ -22,17 +22,26 @@ namespace {
 constexpr int NT = 256;
 inline unsigned nblocks(long long n, int nt = NT) { return (unsigned)((n + nt - 1) / nt); }
 
-__device__ __forceinline__ void decodeC(const Params& p, long long n, int& i, int& j, int& k) {
-  i = (int)(n % p.nCx);
-  long long r = n / p.nCx;
-  j = (int)(r % p.nCy);
-  k = (int)(r / p.nCy);
+__device__ __forceinline__ void decodeI(const Params& p, int q, int& i, int& j, int& k) {
+  i = q % p.imax + 1;
+  const int r = q / p.imax;
+  j = r % p.jmax + 1;
+  k = r / p.jmax + 1;
 }
-__device__ __forceinline__ void decodeI(const Params& p, long long q, int& i, int& j, int& k) {
-  i = (int)(q % p.imax) + 1;
-  long long r = q / p.imax;
-  j = (int)(r % p.jmax) + 1;
-  k = (int)(r / p.jmax) + 1;
+
+__constant__ int kC0[3] = {0, 0, 0};
+__constant__ int kI0[3] = {1, 1, 1};
+struct I3 {
+  int v[3];
+};
+__device__ __forceinline__ I3 cC1(const Params& p) { return I3{{p.i1, p.j1, p.k1}}; }
+__device__ __forceinline__ I3 cI1(const Params& p) { return I3{{p.imax, p.jmax, p.kmax}}; }
+const dim3 kBlock(BX, BY, 1);
+inline dim3 gridC(const Params& p) {
+  return dim3((unsigned)((p.nCx + BX - 1) / BX), (unsigned)((p.nCy + BY - 1) / BY), (unsigned)p.nCz);
+}
+inline dim3 gridI(const Params& p) {
+  return dim3((unsigned)((p.imax + BX - 1) / BX), (unsigned)((p.jmax + BY - 1) / BY), (unsigned)p.kmax);
 }
 
 struct MomArgs {
@@ -47,7 +56,6 @@ __device__ __forceinline__ double rhs_u(const Params& p, const MomArgs& a, int i
   const double *u = a.u, *v = a.v, *w = a.w, *miu = a.miu;
   const long long c = idxC(p, i, j, k);
   const long long sx = 1, sy = p.nCx, sz = (long long)p.nCx * p.nCy;
-  const double dx = p.dx, dy = p.dy, dz = p.dz;
   double RCu = 0.;
   if (!p.TwoD) {
     double uuip = 0.25 * (u[c + sx] + u[c]) * (u[c + sx] + u[c]);
@@ -56,29 +64,29 @@ __device__ __forceinline__ double rhs_u(const Params& p, const MomArgs& a, int i
     double uvjm = 0.25 * (u[c - sy] + u[c]) * (v[c + sx - sy] + v[c - sy]);
     double uwkp = 0.25 * (u[c + sz] + u[c]) * (w[c + sx] + w[c]);
     double uwkm = 0.25 * (u[c - sz] + u[c]) * (w[c + sx - sz] + w[c - sz]);
-    RCu = ((-uuip + uuim) / dx + (-uvjp + uvjm) / dy) + (-uwkp + uwkm) / dz;
+    RCu = (divx(p, (-uuip + uuim)) + divy(p, (-uvjp + uvjm))) + divz(p, (-uwkp + uwkm));
   }
   double RDu = 0.;
   if (!p.TwoD) {
-    double dudxp = (u[c + sx] - u[c]) / dx;
-    double dudxm = (u[c] - u[c - sx]) / dx;
-    double dudyp = (u[c + sy] - u[c]) / dy;
-    double dudym = (u[c] - u[c - sy]) / dy;
-    double dvdxp = (v[c + sx] - v[c]) / dx;
-    double dvdxm = (v[c + sx - sy] - v[c - sy]) / dx;
-    double dudzp = (u[c + sz] - u[c]) / dz;
-    double dudzm = (u[c] - u[c - sz]) / dz;
-    double dwdxp = (w[c + sx] - w[c]) / dx;
-    double dwdxm = (w[c + sx - sz] - w[c - sz]) / dx;
+    double dudxp = divx(p, (u[c + sx] - u[c]));
+    double dudxm = divx(p, (u[c] - u[c - sx]));
+    double dudyp = divy(p, (u[c + sy] - u[c]));
+    double dudym = divy(p, (u[c] - u[c - sy]));
+    double dvdxp = divx(p, (v[c + sx] - v[c]));
+    double dvdxm = divx(p, (v[c + sx - sy] - v[c - sy]));
+    double dudzp = divz(p, (u[c + sz] - u[c]));
+    double dudzm = divz(p, (u[c] - u[c - sz]));
+    double dwdxp = divx(p, (w[c + sx] - w[c]));
+    double dwdxm = divx(p, (w[c + sx - sz] - w[c - sz]));
     double ma1 = 0.25 * (((miu[c] + miu[c - sy]) + miu[c + sx - sy]) + miu[c + sx]);
     double ma2 = 0.25 * (((miu[c] + miu[c + sy]) + miu[c + sx + sy]) + miu[c + sx]);
     double ma3 = 0.25 * (((miu[c] + miu[c - sz]) + miu[c + sx - sz]) + miu[c + sx]);
     double ma4 = 0.25 * (((miu[c] + miu[c + sz]) + miu[c + sx + sz]) + miu[c + sx]);
-    double RD1 = 2. * (dudxp * miu[c + sx] - dudxm * miu[c]) / dx;
-    double RD2 = (dudyp * ma2 - dudym * ma1) / dy;
-    double RD3 = (dvdxp * ma2 - dvdxm * ma1) / dy;
-    double RD4 = (dudzp * ma4 - dudzm * ma3) / dz;
-    double RD5 = (dwdxp * ma4 - dwdxm * ma3) / dz;
+    double RD1 = divx(p, 2. * (dudxp * miu[c + sx] - dudxm * miu[c]));
+    double RD2 = divy(p, (dudyp * ma2 - dudym * ma1));
+    double RD3 = divy(p, (dvdxp * ma2 - dvdxm * ma1));
+    double RD4 = divz(p, (dudzp * ma4 - dudzm * ma3));
+    double RD5 = divz(p, (dwdxp * ma4 - dwdxm * ma3));
     RDu = ((((RD1 + RD2) + RD3) + RD4) + RD5) / a.rho_u[idxI(p, i, j, k)];
   }
   double RGu = p.TwoD ? 0. : p.iFr * (1. - rho_avr / a.rho_u[idxI(p, i, j, k)]) * p.g1;
@@ -89,33 +97,32 @@ __device__ __forceinline__ double rhs_v(const Params& p, const MomArgs& a, int i
   const double *u = a.u, *v = a.v, *w = a.w, *miu = a.miu;
   const long long c = idxC(p, i, j, k);
   const long long sx = 1, sy = p.nCx, sz = (long long)p.nCx * p.nCy;
-  const double dx = p.dx, dy = p.dy, dz = p.dz;
   double uvip = 0.25 * (u[c] + u[c + sy]) * (v[c] + v[c + sx]);
   double uvim = 0.25 * (u[c - sx] + u[c - sx + sy]) * (v[c] + v[c - sx]);
   double vvjp = 0.25 * (v[c] + v[c + sy]) * (v[c] + v[c + sy]);
   double vvjm = 0.25 * (v[c] + v[c - sy]) * (v[c] + v[c - sy]);
   double wvkp = 0.25 * (w[c] + w[c + sy]) * (v[c + sz] + v[c]);
   double wvkm = 0.25 * (w[c - sz] + w[c + sy - sz]) * (v[c - sz] + v[c]);
-  double RCv = ((-uvip + uvim) / dx + (-vvjp + vvjm) / dy) + (-wvkp + wvkm) / dz;
-  double dvdxp = (v[c + sx] - v[c]) / dx;
-  double dvdxm = (v[c] - v[c - sx]) / dx;
-  double dudyp = (u[c + sy] - u[c]) / dy;
-  double dudym = (u[c - sx + sy] - u[c - sx]) / dy;
-  double dvdyp = (v[c + sy] - v[c]) / dy;
-  double dvdym = (v[c] - v[c - sy]) / dy;
-  double dvdzp = (v[c + sz] - v[c]) / dz;
-  double dvdzm = (v[c] - v[c - sz]) / dz;
-  double dwdyp = (w[c + sy] - w[c]) / dy;
-  double dwdym = (w[c + sy - sz] - w[c - sz]) / dy;
+  double RCv = (divx(p, (-uvip + uvim)) + divy(p, (-vvjp + vvjm))) + divz(p, (-wvkp + wvkm));
+  double dvdxp = divx(p, (v[c + sx] - v[c]));
+  double dvdxm = divx(p, (v[c] - v[c - sx]));
+  double dudyp = divy(p, (u[c + sy] - u[c]));
+  double dudym = divy(p, (u[c - sx + sy] - u[c - sx]));
+  double dvdyp = divy(p, (v[c + sy] - v[c]));
+  double dvdym = divy(p, (v[c] - v[c - sy]));
+  double dvdzp = divz(p, (v[c + sz] - v[c]));
+  double dvdzm = divz(p, (v[c] - v[c - sz]));
+  double dwdyp = divy(p, (w[c + sy] - w[c]));
+  double dwdym = divy(p, (w[c + sy - sz] - w[c - sz]));
   double ma2 = 0.25 * (((miu[c] + miu[c + sy]) + miu[c + sx + sy]) + miu[c + sx]);
   double ma5 = 0.25 * (((miu[c] + miu[c + sy]) + miu[c - sx + sy]) + miu[c - sx]);
   double ma6 = 0.25 * (((miu[c] + miu[c - sz]) + miu[c + sy - sz]) + miu[c + sy]);
   double ma7 = 0.25 * (((miu[c] + miu[c + sz]) + miu[c + sy + sz]) + miu[c + sy]);
-  double RD1 = (dvdxp * ma2 - dvdxm * ma5) / dx;
-  double RD2 = (dudyp * ma2 - dudym * ma5) / dx;
-  double RD3 = 2. * (dvdyp * miu[c + sy] - dvdym * miu[c]) / dy;
-  double RD4 = (dvdzp * ma7 - dvdzm * ma6) / dz;
-  double RD5 = (dwdyp * ma7 - dwdym * ma6) / dz;
+  double RD1 = divx(p, (dvdxp * ma2 - dvdxm * ma5));
+  double RD2 = divx(p, (dudyp * ma2 - dudym * ma5));
+  double RD3 = divy(p, 2. * (dvdyp * miu[c + sy] - dvdym * miu[c]));
+  double RD4 = divz(p, (dvdzp * ma7 - dvdzm * ma6));
+  double RD5 = divz(p, (dwdyp * ma7 - dwdym * ma6));
   const double rv = a.rho_v[idxI(p, i, j, k)];
   double RDv = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rv;
   double RGv = p.iFr * (1. - rho_avr / rv) * p.g2;
@@ -126,33 +133,32 @@ __device__ __forceinline__ double rhs_w(const Params& p, const MomArgs& a, int i
   const double *u = a.u, *v = a.v, *w = a.w, *miu = a.miu;
   const long long c = idxC(p, i, j, k);
   const long long sx = 1, sy = p.nCx, sz = (long long)p.nCx * p.nCy;
-  const double dx = p.dx, dy = p.dy, dz = p.dz;
   double uwip = 0.25 * (w[c] + w[c + sx]) * (u[c] + u[c + sz]);
   double uwim = 0.25 * (w[c] + w[c - sx]) * (u[c - sx] + u[c - sx + sz]);
   double vwjp = 0.25 * (w[c] + w[c + sy]) * (v[c] + v[c + sz]);
   double vwjm = 0.25 * (w[c] + w[c - sy]) * (v[c - sy] + v[c - sy + sz]);
   double wwkp = 0.25 * (w[c] + w[c + sz]) * (w[c] + w[c + sz]);
   double wwkm = 0.25 * (w[c] + w[c - sz]) * (w[c] + w[c - sz]);
-  double RCw = ((-uwip + uwim) / dx + (-vwjp + vwjm) / dy) + (-wwkp + wwkm) / dz;
-  double dwdxp = (w[c + sx] - w[c]) / dx;
-  double dwdxm = (w[c] - w[c - sx]) / dx;
-  double dudzp = (u[c + sz] - u[c]) / dz;
-  double dudzm = (u[c - sx + sz] - u[c - sx]) / dz;
-  double dwdyp = (w[c + sy] - w[c]) / dy;
-  double dwdym = (w[c] - w[c - sy]) / dy;
-  double dvdzp = (v[c + sz] - v[c]) / dz;
-  double dvdzm = (v[c - sy + sz] - v[c - sy]) / dz;
-  double dwdzp = (w[c + sz] - w[c]) / dz;
-  double dwdzm = (w[c] - w[c - sz]) / dz;
+  double RCw = (divx(p, (-uwip + uwim)) + divy(p, (-vwjp + vwjm))) + divz(p, (-wwkp + wwkm));
+  double dwdxp = divx(p, (w[c + sx] - w[c]));
+  double dwdxm = divx(p, (w[c] - w[c - sx]));
+  double dudzp = divz(p, (u[c + sz] - u[c]));
+  double dudzm = divz(p, (u[c - sx + sz] - u[c - sx]));
+  double dwdyp = divy(p, (w[c + sy] - w[c]));
+  double dwdym = divy(p, (w[c] - w[c - sy]));
+  double dvdzp = divz(p, (v[c + sz] - v[c]));
+  double dvdzm = divz(p, (v[c - sy + sz] - v[c - sy]));
+  double dwdzp = divz(p, (w[c + sz] - w[c]));
+  double dwdzm = divz(p, (w[c] - w[c - sz]));
   double ma4 = 0.25 * (((miu[c] + miu[c + sz]) + miu[c + sx + sz]) + miu[c + sx]);
   double ma8 = 0.25 * (((miu[c] + miu[c + sz]) + miu[c - sx + sz]) + miu[c - sx]);
   double ma7 = 0.25 * (((miu[c] + miu[c + sz]) + miu[c + sy + sz]) + miu[c + sy]);
   double ma9 = 0.25 * (((miu[c] + miu[c + sz]) + miu[c - sy + sz]) + miu[c - sy]);
-  double RD1 = (dwdxp * ma4 - dwdxm * ma8) / dx;
-  double RD2 = (dudzp * ma4 - dudzm * ma8) / dx;
-  double RD3 = (dwdyp * ma7 - dwdym * ma9) / dy;
-  double RD4 = (dvdzp * ma7 - dvdzm * ma9) / dy;
-  double RD5 = 2. * (dwdzp * miu[c + sz] - dwdzm * miu[c]) / dz;
+  double RD1 = divx(p, (dwdxp * ma4 - dwdxm * ma8));
+  double RD2 = divx(p, (dudzp * ma4 - dudzm * ma8));
+  double RD3 = divy(p, (dwdyp * ma7 - dwdym * ma9));
+  double RD4 = divy(p, (dvdzp * ma7 - dvdzm * ma9));
+  double RD5 = divz(p, 2. * (dwdzp * miu[c + sz] - dwdzm * miu[c]));
   const double rw = a.rho_w[idxI(p, i, j, k)];
   double RDw = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rw;
   double RGw = p.iFr * (1. - rho_avr / rw) * p.g3;
@@ -202,10 +208,9 @@ __global__ void __launch_bounds__(NT) k_ab2(Params p, MomArgs a, double* __restr
                                             double* __restrict__ dvdt, double* __restrict__ dwdt,
                                             double* __restrict__ duold_out, double* __restrict__ dvold_out,
                                             double* __restrict__ dwold_out) {
-  const long long n = blockIdx.x * (long long)NT + threadIdx.x;
-  if (n >= p.nC) return;
   int i, j, k;
-  decodeC(p, n, i, j, k);
+  if (!cell3(kC0, cC1(p).v, i, j, k)) return;
+  const long long n = idxC(p, i, j, k);
   const int I = wrapx(p, i), J = wrapy(p, j);
   const double rho_avr = *a.rho_avr;
   double Ru, Rv, Rw, du, dv, dw;
@@ -237,10 +242,9 @@ __global__ void __launch_bounds__(NT) k_ab2(Params p, MomArgs a, double* __restr
 // mom_main alone (init.f90:90): RHS into shape-I arrays
 __global__ void __launch_bounds__(NT) k_mom_main(Params p, MomArgs a, double* __restrict__ ru,
                                                  double* __restrict__ rv, double* __restrict__ rw) {
-  const long long q = blockIdx.x * (long long)NT + threadIdx.x;
-  if (q >= p.nI) return;
   int i, j, k;
-  decodeI(p, q, i, j, k);
+  if (!cell3(kI0, cI1(p).v, i, j, k)) return;
+  const long long q = idxI(p, i, j, k);
   const double rho_avr = *a.rho_avr;
   ru[q] = rhs_u(p, a, i, j, k, rho_avr);
   rv[q] = rhs_v(p, a, i, j, k, rho_avr);
@@ -251,10 +255,9 @@ __global__ void __launch_bounds__(NT) k_mom_main(Params p, MomArgs a, double* __
 __global__ void __launch_bounds__(NT) k_fillps(Params p, const double* __restrict__ dudt,
                                                const double* __restrict__ dvdt, const double* __restrict__ dwdt,
                                                const double* __restrict__ pjump, int add, double* __restrict__ out) {
-  const long long q = blockIdx.x * (long long)NT + threadIdx.x;
-  if (q >= p.nI) return;
   int i, j, k;
-  decodeI(p, q, i, j, k);
+  if (!cell3(kI0, cI1(p).v, i, j, k)) return;
+  const long long q = idxI(p, i, j, k);
   const long long c = idxC(p, i, j, k);
   const double coef = p.rho0 / p.dt;
   const double vel_x = (dudt[c] - dudt[c - 1]) * p.dxi;
@@ -295,10 +298,9 @@ struct CorrArgs {
 
 // correc over the interior only (the separate reference call)
 __global__ void __launch_bounds__(NT) k_correc_interior(Params p, CorrArgs a) {
-  const long long q = blockIdx.x * (long long)NT + threadIdx.x;
-  if (q >= p.nI) return;
   int i, j, k;
-  decodeI(p, q, i, j, k);
+  if (!cell3(kI0, cI1(p).v, i, j, k)) return;
+  const long long q = idxI(p, i, j, k);
   const long long c = idxC(p, i, j, k);
   a.u[c] = corr_u(p, a.dudt, a.p, a.px, i, j, k);
   a.v[c] = corr_v(p, a.dvdt, a.p, a.py, i, j, k);
@@ -308,10 +310,9 @@ __global__ void __launch_bounds__(NT) k_correc_interior(Params p, CorrArgs a) {
 // correc + bounduvw(unew,vnew,wnew) + average_vel_at_center + NaN probe
 // (main.f90:159-160,190,207) over shape C
 __global__ void __launch_bounds__(NT) k_correc_fused(Params p, CorrArgs a) {
-  const long long n = blockIdx.x * (long long)NT + threadIdx.x;
-  if (n >= p.nC) return;
   int i, j, k;
-  decodeC(p, n, i, j, k);
+  if (!cell3(kC0, cC1(p).v, i, j, k)) return;
+  const long long n = idxC(p, i, j, k);
   const int I = wrapx(p, i), J = wrapy(p, j);
   double uu, vv, ww;
   if (k >= 1 && k <= p.kmax) {
@@ -345,10 +346,9 @@ __global__ void __launch_bounds__(NT) k_correc_fused(Params p, CorrArgs a) {
 // bounduvw (bound.f90:15-177, Dirichl z, periodic x,y) on an existing triple
 __global__ void __launch_bounds__(NT) k_bounduvw(Params p, double* __restrict__ u, double* __restrict__ v,
                                                  double* __restrict__ w) {
-  const long long n = blockIdx.x * (long long)NT + threadIdx.x;
-  if (n >= p.nC) return;
   int i, j, k;
-  decodeC(p, n, i, j, k);
+  if (!cell3(kC0, cC1(p).v, i, j, k)) return;
+  const long long n = idxC(p, i, j, k);
   const int I = wrapx(p, i), J = wrapy(p, j);
   const bool col = (I == i && J == j);
   if (k >= 1 && k <= p.kmax) {
@@ -371,10 +371,9 @@ __global__ void __launch_bounds__(NT) k_bounduvw(Params p, double* __restrict__ 
 
 // boundp (bound.f90:182-287, BC_in_y='Periodic')
 __global__ void __launch_bounds__(NT) k_boundp(Params p, double* __restrict__ a) {
-  const long long n = blockIdx.x * (long long)NT + threadIdx.x;
-  if (n >= p.nC) return;
   int i, j, k;
-  decodeC(p, n, i, j, k);
+  if (!cell3(kC0, cC1(p).v, i, j, k)) return;
+  const long long n = idxC(p, i, j, k);
   const int I = wrapx(p, i), J = wrapy(p, j);
   const int K = k == 0 ? 1 : (k == p.k1 ? p.kmax : k);
   if (I == i && J == j && K == k) return;
@@ -386,10 +385,9 @@ __global__ void __launch_bounds__(NT) k_average_vel(Params p, const double* __re
                                                     const double* __restrict__ v, const double* __restrict__ w,
                                                     double* __restrict__ ucc, double* __restrict__ vcc,
                                                     double* __restrict__ wcc) {
-  const long long q = blockIdx.x * (long long)NT + threadIdx.x;
-  if (q >= p.nI) return;
   int i, j, k;
-  decodeI(p, q, i, j, k);
+  if (!cell3(kI0, cI1(p).v, i, j, k)) return;
+  const long long q = idxI(p, i, j, k);
   const long long c = idxC(p, i, j, k);
   ucc[q] = (u[c - 1] + u[c]) / 2.;
   vcc[q] = (v[c - p.nCx] + v[c]) / 2.;
@@ -429,8 +427,7 @@ __global__ void __launch_bounds__(NT) k_pupdate(Params p, const double* __restri
 __global__ void __launch_bounds__(kRedThreads) k_sum_interior(Params p, const double* __restrict__ a,
                                                               double* __restrict__ partial) {
   double s = 0.;
-  for (long long q = blockIdx.x * (long long)kRedThreads + threadIdx.x; q < p.nI;
-       q += (long long)gridDim.x * kRedThreads) {
+  for (int q = blockIdx.x * kRedThreads + threadIdx.x; q < (int)p.nI; q += gridDim.x * kRedThreads) {
     int i, j, k;
     decodeI(p, q, i, j, k);
     s += a[idxC(p, i, j, k)];
@@ -453,8 +450,7 @@ __global__ void __launch_bounds__(kRedThreads) k_chkdiv(Params p, const double* 
                                                         long long* __restrict__ part_loc) {
   double s = 0., m = 0.;
   long long loc = -1;
-  for (long long q = blockIdx.x * (long long)kRedThreads + threadIdx.x; q < p.nI;
-       q += (long long)gridDim.x * kRedThreads) {
+  for (int q = blockIdx.x * kRedThreads + threadIdx.x; q < (int)p.nI; q += gridDim.x * kRedThreads) {
     int i, j, k;
     decodeI(p, q, i, j, k);
     const long long c = idxC(p, i, j, k);
@@ -462,7 +458,7 @@ __global__ void __launch_bounds__(kRedThreads) k_chkdiv(Params p, const double* 
                  (u[c] - u[c - 1]) * p.dxi;
     s += div;
     div = fabs(div);
-    if (div > m) { m = div; loc = q; }
+    if (div > m) { m = div; loc = (long long)q; }
   }
   __shared__ double sm[kRedThreads];
   __shared__ long long sl[kRedThreads];
@@ -498,14 +494,10 @@ __global__ void k_chkdiv_final(const double* __restrict__ part_sum, const double
 // chkdt maxima (chkdt.f90:31-52) and max_vel_at_center (misc.f90:619-633)
 __global__ void __launch_bounds__(NT) k_chkdt(Params p, const double* __restrict__ u, const double* __restrict__ v,
                                               const double* __restrict__ w, DevScalars* __restrict__ dsc) {
-  const long long q = blockIdx.x * (long long)NT + threadIdx.x;
-  const long long n1 = (long long)(p.imax + 1) * (p.jmax + 1) * (p.kmax + 1);
   double a = 0., b = 0., c = 0.;
-  if (q < n1) {
-    const int i = (int)(q % (p.imax + 1)) + 1;
-    const long long r = q / (p.imax + 1);
-    const int j = (int)(r % (p.jmax + 1)) + 1;
-    const int k = (int)(r / (p.jmax + 1)) + 1;
+  int i, j, k;
+  const I3 hi = cC1(p);
+  if (cell3(kI0, hi.v, i, j, k)) {
     const long long cc = idxC(p, i, j, k);
     a = fabs((u[cc] + u[cc - 1]) / 2.);
     b = fabs((v[cc] + v[cc - p.nCx]) / 2.);
@@ -514,7 +506,7 @@ __global__ void __launch_bounds__(NT) k_chkdt(Params p, const double* __restrict
   a = block_max<double, NT>(a);
   b = block_max<double, NT>(b);
   c = block_max<double, NT>(c);
-  if (threadIdx.x == 0) {
+  if (flat_tid() == 0) {
     atomic_max_nonneg(&dsc->umax, a);
     atomic_max_nonneg(&dsc->vmax, b);
     atomic_max_nonneg(&dsc->wmax, c);
@@ -554,35 +546,35 @@ void launch_ab2(Ctx& c) {
   Scope sc_(c.prof, c.s, "ab2", 1);
   MomArgs a = mom_args(c);
   const int o = c.hist ^ 1;
-  k_ab2<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, a, c.dudt, c.dvdt, c.dwdt, c.duold[o], c.dvold[o], c.dwold[o]);
+  k_ab2<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, a, c.dudt, c.dvdt, c.dwdt, c.duold[o], c.dvold[o], c.dwold[o]);
   c.hist = o;
 }
 void launch_mom_main(Ctx& c, double* du, double* dv, double* dw) {
   Scope sc_(c.prof, c.s, "mom_main", 1);
   MomArgs a = mom_args(c);
-  k_mom_main<<<nblocks(c.P.nI), NT, 0, c.s>>>(c.P, a, du, dv, dw);
+  k_mom_main<<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a, du, dv, dw);
 }
 void launch_fillps(Ctx& c, int add_pjump) {
   Scope sc_(c.prof, c.s, "fillps", 1);
-  k_fillps<<<nblocks(c.P.nI), NT, 0, c.s>>>(c.P, c.dudt, c.dvdt, c.dwdt, c.pjump, add_pjump, c.p);
+  k_fillps<<<gridI(c.P), kBlock, 0, c.s>>>(c.P, c.dudt, c.dvdt, c.dwdt, c.pjump, add_pjump, c.p);
 }
 void launch_add_pjump(Ctx& c) {
   Scope sc_(c.prof, c.s, "add_pjump", 1); k_add<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, c.pjump); }
 void launch_correc(Ctx& c, int fused_bc) {
   Scope sc_(c.prof, c.s, "correc", 1);
   CorrArgs a = corr_args(c);
-  if (fused_bc) k_correc_fused<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, a);
-  else k_correc_interior<<<nblocks(c.P.nI), NT, 0, c.s>>>(c.P, a);
+  if (fused_bc) k_correc_fused<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, a);
+  else k_correc_interior<<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);
 }
 void launch_bounduvw(Ctx& c, double* u, double* v, double* w) {
   Scope sc_(c.prof, c.s, "bounduvw", 1);
-  k_bounduvw<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, u, v, w);
+  k_bounduvw<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, u, v, w);
 }
 void launch_boundp(Ctx& c, double* pp) {
-  Scope sc_(c.prof, c.s, "boundp", 1); k_boundp<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, pp); }
+  Scope sc_(c.prof, c.s, "boundp", 1); k_boundp<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, pp); }
 void launch_average_vel(Ctx& c) {
   Scope sc_(c.prof, c.s, "average_vel", 1);
-  k_average_vel<<<nblocks(c.P.nI), NT, 0, c.s>>>(c.P, c.u, c.v, c.w, c.ucc, c.vcc, c.wcc);
+  k_average_vel<<<gridI(c.P), kBlock, 0, c.s>>>(c.P, c.u, c.v, c.w, c.ucc, c.vcc, c.wcc);
 }
 void launch_pressure_update(Ctx& c, int first) {
   Scope sc_(c.prof, c.s, "pressure_update", 2);
@@ -603,9 +595,8 @@ void launch_chkdiv(Ctx& c) {
 }
 void launch_chkdt(Ctx& c) {
   Scope sc_(c.prof, c.s, "chkdt", 1);
-  const long long n1 = (long long)(c.P.imax + 1) * (c.P.jmax + 1) * (c.P.kmax + 1);
   cudaMemsetAsync(&c.dsc->umax, 0, 3 * sizeof(double), c.s);
-  k_chkdt<<<nblocks(n1), NT, 0, c.s>>>(c.P, c.u, c.v, c.w, c.dsc);
+  k_chkdt<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, c.u, c.v, c.w, c.dsc);
 }
 void launch_maxvel(Ctx& c) {
   Scope sc_(c.prof, c.s, "maxvel", 1);
