@@ -602,8 +602,9 @@ int icls_status_string(int code, char* buf, int n) {
   static const char* names[] = {"ok", "invalid or unsupported configuration", "CUDA error",
                                 "NaN in vnew(1,1,1)", "max divergence above 1e-12", "bad argument",
                                 "device allocation failed", "context not initialised",
-                                "option not built into this library"};
-  const char* s = (code >= 0 && code <= 8) ? names[code] : "unknown status";
+                                "option not built into this library",
+                                "grid larger than the no-allocation divergence check handles"};
+  const char* s = (code >= 0 && code <= 9) ? names[code] : "unknown status";
   if (buf && n > 0) {
     std::strncpy(buf, s, (size_t)n - 1);
     buf[n - 1] = 0;

@@ -336,3 +336,17 @@ class Solver:
         lo = field_lo(name)
         s = 1 - lo
         return a[s:s + self.cfg.itot, s:s + self.cfg.jtot, s:s + self.cfg.ktot]
+
+
+def chkdiv_noalloc(u_ptr: int, v_ptr: int, w_ptr: int, imax: int, jmax: int, kmax: int,
+                   dxi: float, dyi: float, dzi: float, result_ptr: int, stream: int = 0) -> int:
+    """icls_chkdiv_noalloc on caller-owned device arrays (raw device
+    addresses).  The library allocates nothing for this call; it returns the
+    status code and leaves [divtot, divmax, i, j, k] in the 5-double device
+    buffer at result_ptr."""
+    lib = gpu_backend().lib
+    fn = lib.icls_chkdiv_noalloc
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                   C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
+    fn.restype = C.c_int
+    return fn(u_ptr, v_ptr, w_ptr, imax, jmax, kmax, dxi, dyi, dzi, result_ptr, stream or None)

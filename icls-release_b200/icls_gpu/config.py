@@ -20,10 +20,10 @@ FP64, FP32 = 0, 1
 CURV_STENCIL, CURV_MLP = 0, 1
 
 # status codes
-OK, E_CONFIG, E_CUDA, E_NAN, E_DIVERGENCE, E_ARG, E_NOMEM, E_STATE, E_UNSUPPORTED = range(9)
+OK, E_CONFIG, E_CUDA, E_NAN, E_DIVERGENCE, E_ARG, E_NOMEM, E_STATE, E_UNSUPPORTED, E_SIZE = range(10)
 STATUS_NAMES = {
     0: "OK", 1: "E_CONFIG", 2: "E_CUDA", 3: "E_NAN", 4: "E_DIVERGENCE",
-    5: "E_ARG", 6: "E_NOMEM", 7: "E_STATE", 8: "E_UNSUPPORTED",
+    5: "E_ARG", 6: "E_NOMEM", 7: "E_STATE", 8: "E_UNSUPPORTED", 9: "E_SIZE",
 }
 
 

@@ -36,7 +36,8 @@ enum {
   ICLS_E_ARG = 5,         /* bad argument (field id, drop index, pointer)  */
   ICLS_E_NOMEM = 6,       /* device allocation failed                      */
   ICLS_E_STATE = 7,       /* call made before icls_init_program            */
-  ICLS_E_UNSUPPORTED = 8  /* scheme/option not built into this library    */
+  ICLS_E_UNSUPPORTED = 8, /* scheme/option not built into this library    */
+  ICLS_E_SIZE = 9         /* grid larger than icls_chkdiv_noalloc handles */
 };
 
 /* ---- scheme selectors (param.f90 / mod_param_ls character parameters) */
@@ -181,6 +182,24 @@ int icls_get_curvature(icls_ctx* ctx, int l);               /* interface.f90:20-
 /* Number of band cells of drop l after the last tube_construction
  * (nb_cnt, levelset.f90:158).                                           */
 int icls_band_count(icls_ctx* ctx, int l, long long* nb_cnt);
+
+/* ---- divergence check without device allocation -----------------------
+ * No counterpart in the reference.  The chkdiv reduction for callers that
+ * cannot let the library allocate device memory (their device memory is
+ * claimed by their own pool, or a failed allocation inside a check is not
+ * acceptable).  u, v, w: device arrays of shape (0:imax+1,0:jmax+1,0:kmax+1),
+ * column-major; result: caller's device buffer of 5 doubles, set to
+ * [sum of div, max|div|, i, j, k of the first maximum].  The per-block
+ * partial sums live in a fixed file-scope device array (about 28 KB on every
+ * GPU that loads the library, until exit); the first call on a device looks
+ * up its address, so make it before any stream capture.  Calls share that
+ * array: calls that overlap on the GPU race.  Grids above
+ * ICLS_NOALLOC_MAX_CELLS interior cells return ICLS_E_SIZE.  Nothing is
+ * allocated; the call is asynchronous on `stream` (a cudaStream_t, 0 for
+ * the default stream).                                                   */
+#define ICLS_NOALLOC_MAX_CELLS 2147483647LL
+int icls_chkdiv_noalloc(const double* u, const double* v, const double* w, int imax, int jmax, int kmax,
+                        double dxi, double dyi, double dzi, double* result, void* stream);
 
 /* ---- instrumentation (not part of the reference interface) ------------
  * Per-launcher device time measured with CUDA events on the context's
