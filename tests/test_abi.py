@@ -1,0 +1,108 @@
+"""The C ABI without a GPU: the library loads, exports every entry point that
+include/icls_gpu.h declares, and rejects bad arguments and configurations on
+the host before any CUDA call (the validation the reference does at start-up
+in param.f90 / initsolver.f90 becomes status codes here)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+from icls_gpu.binding import LIB_PATH
+from icls_gpu.config import IclsConfig, STATUS_NAMES, make_config
+
+HEADER = os.path.join(ROOT, "include", "icls_gpu.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:int|void)\s+(icls_\w+)\s*\(", text, flags=re.M)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not os.path.exists(LIB_PATH):
+        pytest.fail("%s missing: run python __graft_entry__.py build" % LIB_PATH)
+    return C.CDLL(LIB_PATH)
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_functions()
+    assert len(names) >= 40, names
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings(lib):
+    f = lib.icls_status_string
+    f.argtypes = [C.c_int, C.c_char_p, C.c_int]
+    f.restype = C.c_int
+    buf = C.create_string_buffer(96)
+    seen = set()
+    for code in sorted(STATUS_NAMES):
+        assert f(code, buf, 96) == 0
+        assert buf.value, code
+        seen.add(buf.value)
+    assert len(seen) == len(STATUS_NAMES)
+    assert f(12345, buf, 96) == 0 and buf.value == b"unknown status"
+
+
+def test_config_default_matches_python_defaults(lib):
+    c = IclsConfig()
+    lib.icls_config_default.argtypes = [C.POINTER(IclsConfig)]
+    lib.icls_config_default.restype = None
+    lib.icls_config_default(C.byref(c))
+    ref = make_config()
+    for name, _ in IclsConfig._fields_:
+        a, b = getattr(c, name), getattr(ref, name)
+        if hasattr(a, "__len__"):
+            assert list(a) == list(b), name
+        else:
+            assert a == b, name
+
+
+@pytest.mark.parametrize("change,code", [
+    (dict(itot=24), "E_CONFIG"),            # radix-2 FFT in x
+    (dict(jtot=48), "E_CONFIG"),            # radix-2 FFT in y
+    (dict(itot=8192), "E_CONFIG"),
+    (dict(ktot=4), "E_CONFIG"),
+    (dict(lmax=0), "E_CONFIG"),
+    (dict(lx=0.0), "E_CONFIG"),
+    (dict(timestep=-1e-4), "E_CONFIG"),
+    (dict(reinit_step=0), "E_CONFIG"),
+    (dict(ls_adv_space=7), "E_CONFIG"),
+    (dict(precision=32), "E_UNSUPPORTED"),  # FP32 form not built
+    (dict(curvature_model=1), "E_UNSUPPORTED"),
+])
+def test_create_rejects_bad_configs_on_host(lib, change, code):
+    cfg = make_config(itot=32, jtot=32, ktot=32, lmax=1)
+    for k, v in change.items():
+        setattr(cfg, k, v)
+    lib.icls_create.argtypes = [C.POINTER(IclsConfig), C.POINTER(C.c_void_p)]
+    lib.icls_create.restype = C.c_int
+    h = C.c_void_p(1)
+    rc = lib.icls_create(C.byref(cfg), C.byref(h))
+    assert STATUS_NAMES.get(rc) == code, (change, rc)
+    assert not h.value
+    assert STATUS_NAMES.get(lib.icls_create(None, C.byref(h))) == "E_ARG"
+
+
+def test_null_context_is_an_argument_error(lib):
+    for name in ("icls_init_program", "icls_ab2", "icls_fillps", "icls_gfm4p", "icls_solver2d",
+                 "icls_correc", "icls_update_materials", "icls_synchronize"):
+        fn = getattr(lib, name)
+        fn.argtypes = [C.c_void_p]
+        fn.restype = C.c_int
+        assert STATUS_NAMES.get(fn(None)) == "E_ARG", name
+
+
+def test_noalloc_argument_checks_run_before_cuda(lib):
+    fn = lib.icls_chkdiv_noalloc
+    fn.argtypes = [C.c_void_p] * 3 + [C.c_int] * 3 + [C.c_double] * 3 + [C.c_void_p, C.c_void_p]
+    fn.restype = C.c_int
+    dummy = 0x1000  # never dereferenced: both checks return before any CUDA call
+    assert STATUS_NAMES.get(fn(None, dummy, dummy, 8, 8, 8, 1., 1., 1., dummy, None)) == "E_ARG"
+    assert STATUS_NAMES.get(fn(dummy, dummy, dummy, 0, 8, 8, 1., 1., 1., dummy, None)) == "E_ARG"
+    assert STATUS_NAMES.get(fn(dummy, dummy, dummy, 2048, 2048, 2048, 1., 1., 1., dummy, None)) == "E_SIZE"
