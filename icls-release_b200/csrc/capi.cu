@@ -37,6 +37,7 @@ int validate(const icls_config* c) {
   if (!c) return ICLS_E_ARG;
   if (!pow2(c->itot) || !pow2(c->jtot)) return ICLS_E_CONFIG;  // radix-2 FFT in x and y
   if (c->itot > 4096 || c->jtot > 4096) return ICLS_E_CONFIG;
+  if (c->itot < 8 || c->jtot < 8) return ICLS_E_CONFIG;  // periodic images of 3 halo layers
   if (c->ktot < 6 || c->lmax < 1) return ICLS_E_CONFIG;
   if (!(c->lx > 0 && c->ly > 0 && c->lz > 0 && c->timestep > 0)) return ICLS_E_CONFIG;
   if (c->reinit_step < 1 || c->inflate_step < 1 || c->reinit_iter_max < 1) return ICLS_E_CONFIG;
@@ -146,7 +147,7 @@ int dalloc(T** p, size_t n) {
 int allocate(Ctx& c) {
   const Params& P = c.P;
   for (double** f : {&c.u, &c.v, &c.w, &c.pnew, &c.pold, &c.p, &c.dudt, &c.dvdt, &c.dwdt, &c.px, &c.py, &c.pz,
-                     &c.pxold, &c.pyold, &c.pzold, &c.pjump, &c.miu, &c.rho, &c.jiemian, &c.curv, &c.recurv,
+                     &c.pxold, &c.pyold, &c.pzold, &c.pjump, &c.miu, &c.rho, &c.jiemian, &c.curv,
                      &c.dheav, &c.kappa})
     AL(*f, (size_t)P.nC);
   for (int h = 0; h < 2; ++h) {
@@ -156,8 +157,6 @@ int allocate(Ctx& c) {
     AL(*f, (size_t)P.nI);
   c.lv.assign(P.L, nullptr);
   for (int l = 0; l < P.L; ++l) AL(c.lv[l], (size_t)P.nL);
-  for (int s = 0; s < 4; ++s) AL(c.ls_scr[s], (size_t)P.nL);
-  AL(c.mask, (size_t)P.nI);
   AL(c.d_nbcnt, (size_t)P.L);
   AL(c.spec, (size_t)P.nI);
   AL(c.twx, (size_t)P.imax);
@@ -169,22 +168,42 @@ int allocate(Ctx& c) {
   AL(c.lpartials, (size_t)kRedBlocks);
   AL(c.dsc, 1);
   AL(c.dvol, (size_t)P.L); AL(c.dvol0, (size_t)P.L); AL(c.dmaxchk, (size_t)P.L);
+  AL(c.drs, (size_t)P.L);
+  c.red_cap = ((P.imax + TBX - 1) / TBX) * ((P.jmax + TBY - 1) / TBY);
+  AL(c.hpart, (size_t)std::max(P.L, 2) * c.red_cap);
   CK(cudaMallocHost((void**)&c.h_vol, sizeof(double) * P.L));
   CK(cudaMallocHost((void**)&c.h_sc, sizeof(DevScalars)));
   CK(cudaEventCreateWithFlags(&c.ev_vol, cudaEventDisableTiming));
   // normal%m = 1 outside the curvature band (interface.f90:44)
   std::vector<double> ones((size_t)P.nI, 1.0);
   CK(cudaMemcpy(c.nrm_m, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice));
-  AL(c.d_bbox, (size_t)6 * P.L);
-  CK(cudaMallocHost((void**)&c.h_bbox, sizeof(int) * 6 * P.L));
+  AL(c.d_bbox, (size_t)10 * P.L);
+  CK(cudaMallocHost((void**)&c.h_bbox, sizeof(int) * 10 * P.L));
   CK(cudaEventCreateWithFlags(&c.ev_bbox, cudaEventDisableTiming));
   c.win.assign(P.L, DropWin());
-  for (auto& w : c.win) w.box = w.valid = full_box(P);
+  for (auto& w : c.win) w.box = w.valid = full_region(P);
   c.outside.assign(P.L, 0.);
   // ICLS_FULL_SWEEP=1 sweeps every drop's whole array (a check of the box
   // bookkeeping: both give bit-identical fields)
   const char* fs = std::getenv("ICLS_FULL_SWEEP");
   c.use_boxes = (P.L <= kMaxDropsParam) && !(fs && fs[0] == '1');
+  // working buffers of a group of drops: as many drops as half the free
+  // HBM holds (ICLS_GROUP=n caps the group, e.g. to test the grouped path)
+  {
+    const size_t per = sizeof(double) * (3 * (size_t)P.nL + 2 * (size_t)P.nC) + (size_t)P.nI + 64;
+    size_t freeb = 0, totalb = 0;
+    CK(cudaMemGetInfo(&freeb, &totalb));
+    long long G = (long long)((freeb / 2) / per);
+    const char* gs = std::getenv("ICLS_GROUP");
+    if (gs && std::atoi(gs) > 0) G = std::min<long long>(G, std::atoi(gs));
+    G = std::max(1LL, std::min<long long>(G, P.L));
+    c.mem.assign((size_t)G, Ctx::Member());
+    for (Ctx::Member& m : c.mem) {
+      AL(m.s1, (size_t)P.nL); AL(m.s2, (size_t)P.nL); AL(m.s3, (size_t)P.nL);
+      AL(m.fit, (size_t)P.nC); AL(m.cv, (size_t)P.nC);
+      AL(m.mask, (size_t)P.nI);
+    }
+  }
   c.inflated.assign(P.L, 0);
   c.vol_dirty.assign(P.L, 0);
   c.init_volume_h.assign(P.L, 0.);
@@ -193,9 +212,9 @@ int allocate(Ctx& c) {
 
 void release(Ctx& c) {
   for (double* f : {c.u, c.v, c.w, c.pnew, c.pold, c.p, c.dudt, c.dvdt, c.dwdt, c.px, c.py, c.pz, c.pxold,
-                    c.pyold, c.pzold, c.pjump, c.miu, c.rho, c.jiemian, c.curv, c.recurv, c.dheav, c.kappa,
+                    c.pyold, c.pzold, c.pjump, c.miu, c.rho, c.jiemian, c.curv, c.dheav, c.kappa,
                     c.rho_u, c.rho_v, c.rho_w, c.ucc, c.vcc, c.wcc, c.nrm_m, c.ulc, c.vlc, c.wlc, c.spec,
-                    c.xyrt, c.zpiv, c.tri_a, c.tri_b, c.tri_c, c.partials, c.dvol, c.dvol0, c.dmaxchk})
+                    c.xyrt, c.zpiv, c.tri_a, c.tri_b, c.tri_c, c.partials, c.dvol, c.dvol0, c.dmaxchk, c.hpart})
     if (f) cudaFree(f);
   for (int h = 0; h < 2; ++h) {
     if (c.duold[h]) cudaFree(c.duold[h]);
@@ -203,12 +222,15 @@ void release(Ctx& c) {
     if (c.dwold[h]) cudaFree(c.dwold[h]);
   }
   for (double* f : c.lv) if (f) cudaFree(f);
-  for (double* f : c.ls_scr) if (f) cudaFree(f);
-  if (c.mask) cudaFree(c.mask);
+  for (Ctx::Member& m : c.mem) {
+    for (double* f : {m.s1, m.s2, m.s3, m.fit, m.cv}) if (f) cudaFree(f);
+    if (m.mask) cudaFree(m.mask);
+  }
   if (c.d_nbcnt) cudaFree(c.d_nbcnt);
   if (c.twx) cudaFree(c.twx);
   if (c.twy) cudaFree(c.twy);
   if (c.lpartials) cudaFree(c.lpartials);
+  if (c.drs) cudaFree(c.drs);
   if (c.dsc) cudaFree(c.dsc);
   if (c.h_vol) cudaFreeHost(c.h_vol);
   if (c.h_sc) cudaFreeHost(c.h_sc);
@@ -272,37 +294,52 @@ double reinit_rhs_h(const Params& p, double phis, double orig) {
   return s * (1. - std::sqrt((d * d + d * d) + d * d));
 }
 
-bool is_full(const Params& P, const Box3& b) {
-  const int n[3] = {P.imax, P.jmax, P.kmax};
-  for (int a = 0; a < 3; ++a)
-    if (!(b.c0[a] <= -2 && b.c1[a] >= n[a] + 3)) return false;
-  return true;
+bool is_full(const Params& P, const Region& r) { return region_full(P, r); }
+
+int wrap1(int v, int n) {
+  v = (v - 1) % n;
+  if (v < 0) v += n;
+  return v + 1;
 }
 
-// interior cells of drop l outside its compute region (their H is 1)
-double outside_count(const Ctx& c, const Box3& b) {
-  const int n[3] = {c.P.imax, c.P.jmax, c.P.kmax};
-  double inside = 1.;
-  for (int a = 0; a < 3; ++a) {
-    const int lo = std::max(1, b.c0[a]), hi = std::min(n[a], b.c1[a]);
-    inside *= (hi >= lo) ? (double)(hi - lo + 1) : 0.;
-  }
-  return (double)c.P.nI - inside;
+// interior cells of a drop outside the computed part of its region (their H is 1)
+double outside_count(const Ctx& c, const Region& r) {
+  const double nx = (double)(r.cx1 - r.cx0 + 1), ny = (double)(r.cy1 - r.cy0 + 1);
+  const int z0 = std::max(1, r.cz0), z1 = std::min(c.P.kmax, r.cz1);
+  const double nz = z1 >= z0 ? (double)(z1 - z0 + 1) : 0.;
+  return (double)c.P.nI - nx * ny * nz;
 }
 
-// bounding boxes measured by the last tube_construction sweep
+// band extents measured by the last tube_construction sweep.  A periodic
+// axis keeps the narrower of the spans seen from two frames half a period
+// apart, so a band across the seam gives its true width.
 int collect_bbox(Ctx& c) {
   if (!c.bbox_pending) return ICLS_OK;
   CK(cudaEventSynchronize(c.ev_bbox));
   c.bbox_pending = false;
-  for (int l = 0; l < c.P.L; ++l) {
+  const Params& P = c.P;
+  for (int l = 0; l < P.L; ++l) {
     DropWin& w = c.win[l];
-    const int* b = c.h_bbox + 6 * l;
-    if (b[0] > b[3] || b[1] > b[4] || b[2] > b[5]) {
+    const int* lo = c.h_bbox + 5 * l;
+    const int* hi = c.h_bbox + 5 * P.L + 5 * l;
+    if (lo[4] > hi[4]) {
       w.have_D = false;  // nothing but far field: sweep everything next time
       continue;
     }
-    for (int q = 0; q < 6; ++q) w.D[q] = b[q];
+    auto span = [](const int* lo2, const int* hi2, int n, int& a, int& len) {
+      const int nA = hi2[0] - lo2[0] + 1, nB = hi2[1] - lo2[1] + 1;
+      if (nA <= nB) {
+        a = lo2[0];
+        len = nA;
+      } else {
+        a = wrap1(lo2[1] - n / 2, n);
+        len = nB;
+      }
+    };
+    span(lo, hi, P.imax, w.Dxa, w.Dxn);
+    span(lo + 2, hi + 2, P.jmax, w.Dya, w.Dyn);
+    w.Dz0 = lo[4];
+    w.Dz1 = hi[4];
     w.grow = w.pending_grow;
     w.have_D = true;
   }
@@ -310,103 +347,190 @@ int collect_bbox(Ctx& c) {
 }
 
 // The region drop l sweeps in a step whose own spreading is g_now cells:
-// the last measured band box grown by what the field could have spread
-// since (tube skin 2, 9 per reinitialisation iteration).  An axis becomes
-// full when the box would reach the three cells next to a periodic seam
-// (whose images are halo cells) or the two next to a wall.
-Box3 sweep_box(const Ctx& c, int l, int g_now) {
+// the last measured band grown by what the field could have spread since
+// (tube skin 2, 9 per reinitialisation iteration), plus a 3-cell apron.  A
+// periodic axis becomes full when the span and its apron would cover the
+// period; z becomes full when the box would reach the two rows next to a
+// wall.
+Region sweep_region(const Ctx& c, int l, int g_now) {
   const DropWin& w = c.win[l];
-  if (!c.use_boxes || !w.have_D || !w.bg_valid) return full_box(c.P);
+  const Params& P = c.P;
+  if (!c.use_boxes || !w.have_D || !w.bg_valid) return full_region(P);
   // the band box is exact only if the clipped far field equals +6dz
-  if (clip_h(w.bg, c.P.NB) != c.P.NB || clip_h(w.bg_ghost, c.P.NB) != c.P.NB) return full_box(c.P);
-  const int n[3] = {c.P.imax, c.P.jmax, c.P.kmax};
-  const int lo_min[3] = {4, 4, 3};
-  const int hi_max[3] = {n[0] - 3, n[1] - 3, n[2] - 2};
+  if (clip_h(w.bg, P.NB) != P.NB || clip_h(w.bg_ghost, P.NB) != P.NB) return full_region(P);
   const int g = w.grow + g_now;
-  Box3 b;
-  for (int a = 0; a < 3; ++a) {
-    const int lo = w.D[a] - g, hi = w.D[3 + a] + g;
-    if (lo < lo_min[a] || hi > hi_max[a]) {
-      b.c0[a] = b.w0[a] = -2;
-      b.c1[a] = b.w1[a] = n[a] + 3;
-    } else {
-      b.c0[a] = lo;
-      b.c1[a] = hi;
-      b.w0[a] = lo - 3;
-      b.w1[a] = hi + 3;
-    }
+  Region r = full_region(P);
+  auto axis = [&](int Da, int Dn, int n, int& xa, int& xn, int& c0, int& c1) {
+    const int len = Dn + 2 * g;
+    if (len + 6 > n) return;  // stays full
+    xa = wrap1(Da - g - 3, n);
+    xn = len + 6;
+    c0 = 3;
+    c1 = 3 + len - 1;
+  };
+  axis(w.Dxa, w.Dxn, P.imax, r.xa, r.xn, r.cx0, r.cx1);
+  axis(w.Dya, w.Dyn, P.jmax, r.ya, r.yn, r.cy0, r.cy1);
+  const int lo = w.Dz0 - g, hi = w.Dz1 + g;
+  if (lo >= 3 && hi <= P.kmax - 2) {
+    r.cz0 = lo;
+    r.cz1 = hi;
+    r.z0 = lo - 3;
+    r.z1 = hi + 3;
   }
-  return b;
+  return r;
 }
+
+// batches of at most kTasks drops with region(l) as their regions
+template <class RegionOf>
+std::vector<LsBatch> make_batches(const std::vector<int>& drops, int kc, RegionOf region) {
+  std::vector<LsBatch> out;
+  for (size_t s = 0; s < drops.size(); s += kTasks) {
+    out.emplace_back();
+    LsBatch& b = out.back();
+    b.n = (int)std::min<size_t>(kTasks, drops.size() - s);
+    for (int q = 0; q < b.n; ++q) {
+      b.t[q] = LsTask();
+      b.t[q].l = drops[s + q];
+      b.t[q].r = region(drops[s + q]);
+    }
+    set_tiles(b, kc);
+  }
+  return out;
+}
+
+constexpr int kStageRows = 8;  // z rows per block of the level-set stage kernels
+
+Ctx::Member& member(Ctx& c, int l) { return c.mem[l % (int)c.mem.size()]; }
 
 // Make drop l's stored array valid everywhere and sweep it whole from now
 // on (used before downloads and by the standalone routine calls).
 void make_full(Ctx& c, int l) {
+  collect_bbox(c);  // a pending measurement must not revive the old box
   DropWin& w = c.win[l];
   if (!is_full(c.P, w.valid)) launch_materialize(c, w.valid, w.bg, w.bg_ghost, c.lv[l]);
-  w.box = w.valid = full_box(c.P);
+  w.box = w.valid = full_region(c.P);
   w.have_D = false;
 }
 
 void update_materials(Ctx& c) {
-  bool any_partial = false;
-  for (int l = 0; l < c.P.L; ++l) any_partial |= !is_full(c.P, c.win[l].box);
-  if (any_partial) launch_fill(c, c.jiemian, c.P.nC, 1.0);
-  for (int l = 0; l < c.P.L; ++l) {
-    launch_heaviside_drop(c, c.win[l].box, c.lv[l], l, (!any_partial && l == 0) ? 1 : 0);
-    c.outside[l] = outside_count(c, c.win[l].box);
+  const int L = c.P.L;
+  launch_fill(c, c.jiemian, c.P.nC, 1.0);
+  std::vector<int> all(L);
+  for (int l = 0; l < L; ++l) all[l] = l;
+  std::vector<int> ntiles(L, 0);
+  for (LsBatch& b : make_batches(all, 0, [&](int l) { return c_region(c.P, c.win[l].box, 0); })) {
+    for (int q = 0; q < b.n; ++q) {
+      b.t[q].phi0 = c.lv[b.t[q].l];
+      ntiles[b.t[q].l] = b.t[q].tx * b.t[q].ty;
+    }
+    launch_heaviside(c, b);
   }
-  launch_materials_final(c, c.outside.data());
-  cudaMemcpyAsync(c.h_vol, c.dvol, sizeof(double) * c.P.L, cudaMemcpyDeviceToHost, c.s);
+  for (int l = 0; l < L; ++l) c.outside[l] = outside_count(c, c.win[l].box);
+  launch_materials_final(c, c.outside.data(), ntiles.data());
+  cudaMemcpyAsync(c.h_vol, c.dvol, sizeof(double) * L, cudaMemcpyDeviceToHost, c.s);
   cudaEventRecord(c.ev_vol, c.s);
   c.vol_pending = true;
   std::fill(c.vol_dirty.begin(), c.vol_dirty.end(), 0);
 }
 
-// tube_construction (levelset.f90:87-197) over the sweep box b
-void tube_construction(Ctx& c, int l, const Box3& b) {
-  DropWin& w = c.win[l];
-  cudaMemsetAsync(c.d_nbcnt + l, 0, sizeof(long long), c.s);
-  cudaMemsetAsync(c.d_bbox + 6 * l, 0x7F, 3 * sizeof(int), c.s);
-  cudaMemsetAsync(c.d_bbox + 6 * l + 3, 0x80, 3 * sizeof(int), c.s);
-  launch_tube(c, b, w.valid, w.bg, w.bg_ghost, c.lv[l], c.ls_scr[0], c.d_nbcnt + l, c.d_bbox + 6 * l);
-  std::swap(c.lv[l], c.ls_scr[0]);
-  w.box = w.valid = b;
-  // every cell outside the measured band box is +6dz after the clip
-  w.bg = c.P.NB;
-  w.bg_ghost = c.P.NB;
-  w.bg_valid = true;
+// tube_construction (levelset.f90:87-197) of the batches' drops into
+// their members' s1 and band masks; every cell outside the measured band
+// box is +6dz afterwards
+void tube_batches(Ctx& c, std::vector<LsBatch>& bs) {
+  for (LsBatch& b : bs) {
+    for (int q = 0; q < b.n; ++q) {
+      LsTask& t = b.t[q];
+      const DropWin& w = c.win[t.l];
+      t.phi0 = c.lv[t.l];
+      t.vin = w.valid;
+      t.bgin = w.bg;
+      t.bggin = w.bg_ghost;
+      t.out = member(c, t.l).s1;
+      t.mask = member(c, t.l).mask;
+    }
+    launch_tube(c, b);
+    for (int q = 0; q < b.n; ++q) {
+      DropWin& w = c.win[b.t[q].l];
+      w.valid = w.box;
+      w.bg = c.P.NB;
+      w.bg_ghost = c.P.NB;
+      w.bg_valid = true;
+    }
+  }
 }
 
-// SSP-RK3 of ls_advection / inflation (levelset.f90:235-243, 558-565)
-void rk3(Ctx& c, int l, int scheme, const double* vu, const double* vv, const double* vw) {
-  DropWin& w = c.win[l];
-  const Box3 b = w.box;
+// SSP-RK3 of ls_advection / inflation (levelset.f90:235-243, 558-565) on
+// the batches' drops, with their members' buffers: from_tube, s1 -> s2 ->
+// s3 -> the drop's own array; else the drop's array -> s1 -> s2 -> itself
+void rk3_batches(Ctx& c, std::vector<LsBatch>& bs, int scheme, bool from_tube, const double* vu, const double* vv,
+                 const double* vw) {
   const double dt = c.dt;
-  double* phi0 = c.lv[l];
-  double* s1 = c.ls_scr[1];
-  double* s2 = c.ls_scr[2];
-  const double g0 = w.bg, h0 = w.bg_ghost;
-  const double g1 = g0, h1 = h0;
-  const double g2 = 3. / 4. * g0 + 1. / 4. * g1, h2 = 3. / 4. * h0 + 1. / 4. * h1;
-  const double g3 = 1. / 3. * g0 + 2. / 3. * g2, h3 = 1. / 3. * h0 + 2. / 3. * h2;
-  launch_adv_stage(c, b, g1, h1, scheme, 1, phi0, phi0, 1., 0., 1. * dt, vu, vv, vw, s1);
-  launch_adv_stage(c, b, g2, h2, scheme, 0, phi0, s1, 3. / 4., 1. / 4., 1. / 4. * dt, vu, vv, vw, s2);
-  launch_adv_stage(c, b, g3, h3, scheme, 0, phi0, s2, 1. / 3., 2. / 3., 2. / 3. * dt, vu, vv, vw, s1);
-  std::swap(c.lv[l], c.ls_scr[1]);
-  w.bg = g3;
-  w.bg_ghost = h3;
+  for (LsBatch& b : bs) {
+    double g[kTasks][4], h[kTasks][4];
+    for (int q = 0; q < b.n; ++q) {
+      const DropWin& w = c.win[b.t[q].l];
+      g[q][0] = w.bg;
+      h[q][0] = w.bg_ghost;
+      g[q][1] = g[q][0];
+      h[q][1] = h[q][0];
+      g[q][2] = 3. / 4. * g[q][0] + 1. / 4. * g[q][1];
+      h[q][2] = 3. / 4. * h[q][0] + 1. / 4. * h[q][1];
+      g[q][3] = 1. / 3. * g[q][0] + 2. / 3. * g[q][2];
+      h[q][3] = 1. / 3. * h[q][0] + 2. / 3. * h[q][2];
+    }
+    auto stage = [&](int st, double a, double bb, double fdt) {
+      for (int q = 0; q < b.n; ++q) {
+        LsTask& t = b.t[q];
+        Ctx::Member& m = member(c, t.l);
+        const double* src = from_tube ? m.s1 : c.lv[t.l];
+        double* A = from_tube ? m.s2 : m.s1;
+        double* B = from_tube ? m.s3 : m.s2;
+        t.mask = m.mask;
+        t.phi0 = src;
+        t.phis = st == 1 ? src : (st == 2 ? A : B);
+        t.out = st == 1 ? A : (st == 2 ? B : c.lv[t.l]);
+        t.bg = g[q][st];
+        t.bgg = h[q][st];
+      }
+      launch_adv_stage(c, b, scheme, st == 1 ? 1 : 0, a, bb, fdt, vu, vv, vw);
+    };
+    stage(1, 1., 0., 1. * dt);
+    stage(2, 3. / 4., 1. / 4., 1. / 4. * dt);
+    stage(3, 1. / 3., 2. / 3., 2. / 3. * dt);
+    for (int q = 0; q < b.n; ++q) {
+      DropWin& w = c.win[b.t[q].l];
+      w.bg = g[q][3];
+      w.bg_ghost = h[q][3];
+    }
+  }
 }
 
-void ls_advection(Ctx& c, int l) { rk3(c, l, c.cfg.ls_adv_space, c.ucc, c.vcc, c.wcc); }
+std::vector<LsBatch> single(const Ctx& c, int l, int kc, const Region& r) {
+  std::vector<int> one{l};
+  return make_batches(one, kc, [&](int) { return r; });
+}
+
+void ls_advection(Ctx& c, int l) {
+  std::vector<LsBatch> bs = single(c, l, kStageRows, c.win[l].box);
+  rk3_batches(c, bs, c.cfg.ls_adv_space, false, c.ucc, c.vcc, c.wcc);
+}
 
 // inflation (levelset.f90:407-582)
 void inflation(Ctx& c, int l) {
-  const Box3 b = c.win[l].box;
-  launch_curvature(c, b, c.lv[l], c.kappa, c.nrm_m);
-  launch_inflate_sums(c, b, c.lv[l], l, outside_count(c, b));
-  launch_inflate_vel(c, b);
-  rk3(c, l, c.cfg.i_space, c.ulc, c.vlc, c.wlc);
+  const Region b = c.win[l].box;
+  const Region r1 = c_region(c.P, b, 1);
+  std::vector<LsBatch> bc = single(c, l, kStageRows, r1);
+  bc[0].t[0].phi0 = c.lv[l];
+  bc[0].t[0].out = c.kappa;
+  launch_curvature(c, bc[0], c.nrm_m);
+  c.nrm_stale = true;
+  std::vector<LsBatch> bsum = single(c, l, 0, r1);
+  bsum[0].t[0].phi0 = c.lv[l];
+  launch_inflate_sums(c, bsum[0], outside_count(c, b));
+  std::vector<LsBatch> bvel = single(c, l, kStageRows, c_region(c.P, b, 0));
+  launch_inflate_vel(c, bvel[0]);
+  std::vector<LsBatch> bs = single(c, l, kStageRows, b);
+  rk3_batches(c, bs, c.cfg.i_space, false, c.ulc, c.vlc, c.wlc);
   c.inflated[l] = 1;
   c.vol_dirty[l] = 1;
   ++c.last_inflated;
@@ -440,85 +564,164 @@ int ls_mass_correction(Ctx& c, int istep, int l) {
   return ICLS_OK;
 }
 
-// ls_reinit, WENO5/RK3 (levelset.f90:619-882); the early exit on
-// residual < dz**5 is decided on the device (k_reinit_check).  Far-field
-// cells outside the sweep box change by |bg_new - bg_old| per iteration,
-// which enters the residual as the reference's maxval over all cells does.
-void ls_reinit(Ctx& c, int l) {
-  DropWin& w = c.win[l];
-  const Box3 b = w.box;
-  const bool partial = !is_full(c.P, b);
+// ls_reinit, WENO5/RK3 (levelset.f90:619-882) on the batches' drops; the
+// early exit on residual < dz**5 is decided per drop on the device
+// (k_reinit_check).  Far-field cells outside a drop's region change by
+// |bg_new - bg_old| per iteration, which enters its residual as the
+// reference's maxval over all cells does.  The original level set stays in
+// the drop's own array until the last stage, which overwrites it in place.
+void reinit_batches(Ctx& c, std::vector<LsBatch>& bs) {
   const Params& P = c.P;
   const int maxiter = c.cfg.reinit_iter_max;
   const double dz = P.dz;
   const double dtau = 0.5 * dz;
   const double thr = dz * dz * dz * dz * dz;
-  double* orig = c.lv[l];
-  double* X = orig;
-  double* A = c.ls_scr[0];
-  double* B = c.ls_scr[1];
-  double* Y = c.ls_scr[2];
-  double* Yalt = c.ls_scr[3];
-  const double og = w.bg;  // sgn source of the far field
-  double xg = w.bg, xh = w.bg_ghost;
-  launch_reinit_reset(c, maxiter);
-  for (int it = 1; it <= maxiter; ++it) {
-    const double ag = xg + dtau * reinit_rhs_h(P, xg, og);
-    const double ah = xh + dtau * 0.;
-    const double bgv = 3. / 4. * xg + 1. / 4. * (ag + dtau * reinit_rhs_h(P, ag, og));
-    const double bh = 3. / 4. * xh + 1. / 4. * (ah + dtau * 0.);
-    const double yg = 1. / 3. * xg + 2. / 3. * (bgv + dtau * reinit_rhs_h(P, bgv, og));
-    const double yh = 1. / 3. * xh + 2. / 3. * (bh + dtau * 0.);
-    launch_reinit_stage(c, b, ag, ah, 1, X, X, orig, dtau, A);
-    launch_reinit_stage(c, b, bgv, bh, 2, X, A, orig, dtau, B);
-    launch_reinit_stage(c, b, yg, yh, 3, X, B, orig, dtau, Y);
-    const double far = partial ? std::max(std::fabs(yg - xg), std::fabs(yh - xh)) : 0.;
-    launch_reinit_check(c, it, maxiter, thr, far);
-    X = Y;
-    std::swap(Y, Yalt);
-    if (Y == orig) std::swap(Y, Yalt);
-    xg = yg;
-    xh = yh;
-  }
-  // X holds phi_new; make it the drop's buffer and recycle the original
-  for (int s = 0; s < 4; ++s)
-    if (c.ls_scr[s] == X) {
-      c.ls_scr[s] = orig;
-      break;
+  for (LsBatch& b : bs) {
+    double xg[kTasks], xh[kTasks], og[kTasks];
+    bool partial[kTasks];
+    for (int q = 0; q < b.n; ++q) {
+      const DropWin& w = c.win[b.t[q].l];
+      xg[q] = w.bg;
+      xh[q] = w.bg_ghost;
+      og[q] = w.bg;  // sgn source of the far field
+      partial[q] = !is_full(P, w.box);
     }
-  c.lv[l] = X;
-  // with a far field the residual never drops below dz**5 (the far field
-  // moves by ~dtau per iteration), so every iteration runs: the replayed
-  // values are exact
-  w.bg = xg;
-  w.bg_ghost = xh;
+    launch_reinit_reset(c, b, maxiter);
+    for (int it = 1; it <= maxiter; ++it) {
+      double ag[kTasks], ah[kTasks], bgv[kTasks], bh[kTasks], yg[kTasks], yh[kTasks];
+      for (int q = 0; q < b.n; ++q) {
+        ag[q] = xg[q] + dtau * reinit_rhs_h(P, xg[q], og[q]);
+        ah[q] = xh[q] + dtau * 0.;
+        bgv[q] = 3. / 4. * xg[q] + 1. / 4. * (ag[q] + dtau * reinit_rhs_h(P, ag[q], og[q]));
+        bh[q] = 3. / 4. * xh[q] + 1. / 4. * (ah[q] + dtau * 0.);
+        yg[q] = 1. / 3. * xg[q] + 2. / 3. * (bgv[q] + dtau * reinit_rhs_h(P, bgv[q], og[q]));
+        yh[q] = 1. / 3. * xh[q] + 2. / 3. * (bh[q] + dtau * 0.);
+      }
+      auto stage = [&](int st) {
+        for (int q = 0; q < b.n; ++q) {
+          LsTask& t = b.t[q];
+          double* own = c.lv[t.l];
+          const Ctx::Member& m = member(c, t.l);
+          double* S1 = m.s1;
+          double* S2 = m.s2;
+          double* S3 = m.s3;
+          const double* X = it == 1 ? own : S3;
+          t.phi0 = X;
+          t.orig = own;
+          t.phis = st == 1 ? X : (st == 2 ? S1 : S2);
+          t.out = st == 1 ? S1 : (st == 2 ? S2 : (it == maxiter ? own : S3));
+          t.bg = st == 1 ? ag[q] : (st == 2 ? bgv[q] : yg[q]);
+          t.bgg = st == 1 ? ah[q] : (st == 2 ? bh[q] : yh[q]);
+          t.far = partial[q] ? std::max(std::fabs(yg[q] - xg[q]), std::fabs(yh[q] - xh[q])) : 0.;
+        }
+        launch_reinit_stage(c, b, st, dtau);
+      };
+      stage(1);
+      stage(2);
+      stage(3);
+      launch_reinit_check(c, b, it, maxiter, thr);
+      for (int q = 0; q < b.n; ++q) {
+        xg[q] = yg[q];
+        xh[q] = yh[q];
+      }
+    }
+    // with a far field the residual never drops below dz**5 (the far field
+    // moves by ~dtau per iteration), so every iteration runs: the replayed
+    // values are exact
+    for (int q = 0; q < b.n; ++q) {
+      DropWin& w = c.win[b.t[q].l];
+      w.bg = xg[q];
+      w.bg_ghost = xh[q];
+    }
+  }
 }
+
+void ls_reinit(Ctx& c, int l) {
+  std::vector<LsBatch> bs = single(c, l, kStageRows, c.win[l].box);
+  reinit_batches(c, bs);
+}
+
+// tube_construction of one drop over its whole array (standalone call)
+void tube_construction(Ctx& c, int l) {
+  std::vector<LsBatch> bs = single(c, l, kStageRows, c.win[l].box);
+  cudaMemsetAsync(c.d_nbcnt + l, 0, sizeof(long long), c.s);
+  tube_batches(c, bs);
+  std::swap(c.lv[l], member(c, l).s1);
+}
+
+// the drops of group g: [g*G, min(L, (g+1)*G))
+std::vector<int> group_drops(const Ctx& c, int g) {
+  const int G = (int)c.mem.size();
+  std::vector<int> d;
+  for (int l = g * G; l < std::min(c.P.L, (g + 1) * G); ++l) d.push_back(l);
+  return d;
+}
+int n_groups(const Ctx& c) { return (c.P.L + (int)c.mem.size() - 1) / (int)c.mem.size(); }
 
 int ls_main(Ctx& c, int istep) {
   c.last_inflated = 0;
   int rc = collect_bbox(c);
   if (rc) return rc;
+  const Params& P = c.P;
+  const int L = P.L;
   const bool reinit_now = c.cfg.re_initialization && istep % c.cfg.reinit_step == 0;
   const int g_now = 2 + (reinit_now ? 9 * c.cfg.reinit_iter_max : 0);
-  for (int l = 0; l < c.P.L; ++l) {
-    const Box3 b = sweep_box(c, l, g_now);
-    tube_construction(c, l, b);
+  for (int l = 0; l < L; ++l) {
+    c.win[l].box = sweep_region(c, l, g_now);
     c.win[l].pending_grow = g_now;
-    ls_advection(c, l);
-    if (c.cfg.mass_correction) {
-      rc = ls_mass_correction(c, istep, l);
-      if (rc) return rc;
-    }
-    if (reinit_now) ls_reinit(c, l);
   }
-  cudaMemcpyAsync(c.h_bbox, c.d_bbox, sizeof(int) * 6 * c.P.L, cudaMemcpyDeviceToHost, c.s);
+  cudaMemsetAsync(c.d_nbcnt, 0, sizeof(long long) * L, c.s);
+  cudaMemsetAsync(c.d_bbox, 0x7F, sizeof(int) * 5 * L, c.s);
+  cudaMemsetAsync(c.d_bbox + 5 * L, 0x80, sizeof(int) * 5 * L, c.s);
+  // per group: tube_construction, ls_advection, ls_mass_correction (which
+  // still reads the drop's band mask) and ls_reinit, as the reference runs
+  // them for each drop
+  for (int g = 0; g < n_groups(c); ++g) {
+    const std::vector<int> drops = group_drops(c, g);
+    std::vector<LsBatch> bs = make_batches(drops, kStageRows, [&](int l) { return c.win[l].box; });
+    tube_batches(c, bs);
+    rk3_batches(c, bs, c.cfg.ls_adv_space, true, c.ucc, c.vcc, c.wcc);
+    if (c.cfg.mass_correction)
+      for (int l : drops) {
+        rc = ls_mass_correction(c, istep, l);
+        if (rc) return rc;
+      }
+    if (reinit_now) reinit_batches(c, bs);
+  }
+  cudaMemcpyAsync(c.h_bbox, c.d_bbox, sizeof(int) * 10 * L, cudaMemcpyDeviceToHost, c.s);
   cudaEventRecord(c.ev_bbox, c.s);
   c.bbox_pending = true;
   update_materials(c);
   return check_launch();
 }
 
-// gfm4p, GFM/'del' (gfm.f90:17-267); ipot is evaluated by icls_ipot
+// curv and normal%m as the reference leaves them after its last
+// get_curvature/re_curvature call: the last drop's values, zero (one)
+// elsewhere
+void fix_curv(Ctx& c) {
+  if (!c.curv_stale && !c.nrm_stale) return;
+  const int l = c.P.L - 1;
+  const size_t bytes = sizeof(double) * (size_t)c.P.nC;
+  launch_fill(c, c.nrm_m, c.P.nI, 1.0);
+  cudaMemsetAsync(c.curv, 0, bytes, c.s);
+  std::vector<LsBatch> b = single(c, l, kStageRows, c_region(c.P, c.win[l].box, 1));
+  LsTask& t = b[0].t[0];
+  t.phi0 = c.lv[l];
+  if (c.cfg.TwoD) {
+    t.out = c.curv;
+    launch_curvature(c, b[0], c.nrm_m);
+  } else {
+    t.out = member(c, l).fit;
+    launch_curvature(c, b[0], c.nrm_m);
+    t.phis = member(c, l).fit;
+    t.out = c.curv;
+    launch_recurvature(c, b[0]);
+  }
+  c.curv_stale = c.nrm_stale = false;
+}
+
+// gfm4p, GFM/'del' (gfm.f90:17-267), one group of drops at a time, each
+// drop with its member's curvature buffers.  ipot is evaluated by icls_ipot.
 void gfm4p(Ctx& c) {
   std::swap(c.px, c.pxold);
   std::swap(c.py, c.pyold);
@@ -528,25 +731,38 @@ void gfm4p(Ctx& c) {
   cudaMemsetAsync(c.py, 0, bytes, c.s);
   cudaMemsetAsync(c.pz, 0, bytes, c.s);
   cudaMemsetAsync(c.pjump, 0, bytes, c.s);
-  bool any_partial = false;
-  for (int l = 0; l < c.P.L; ++l) any_partial |= !is_full(c.P, c.win[l].box);
-  // normal%m is 1 away from every band (interface.f90:44)
-  if (any_partial) launch_fill(c, c.nrm_m, c.P.nI, 1.0);
-  for (int l = 0; l < c.P.L; ++l) {
-    const Box3 b = c.win[l].box;
-    const bool last = (l == c.P.L - 1);
-    if (last && !is_full(c.P, b)) {
-      // curv_cmn after the loop is the last drop's re_curvature, zero elsewhere
-      cudaMemsetAsync(c.curv, 0, bytes, c.s);
-      cudaMemsetAsync(c.recurv, 0, bytes, c.s);
+  for (int g = 0; g < n_groups(c); ++g) {
+    const std::vector<int> drops = group_drops(c, g);
+    std::vector<LsBatch> b1 = make_batches(drops, kStageRows, [&](int l) { return c_region(c.P, c.win[l].box, 1); });
+    std::vector<LsBatch> b0 = make_batches(drops, kStageRows, [&](int l) { return c_region(c.P, c.win[l].box, 0); });
+    for (LsBatch& b : b1) {
+      for (int q = 0; q < b.n; ++q) {
+        LsTask& t = b.t[q];
+        t.phi0 = c.lv[t.l];
+        t.out = c.cfg.TwoD ? member(c, t.l).cv : member(c, t.l).fit;
+      }
+      launch_curvature(c, b, nullptr);
     }
-    launch_curvature(c, b, c.lv[l], c.curv, c.nrm_m);
-    if (!c.cfg.TwoD) {
-      launch_recurvature(c, b, c.lv[l], c.curv, c.recurv);
-      std::swap(c.curv, c.recurv);
+    if (!c.cfg.TwoD)
+      for (LsBatch& b : b1) {
+        for (int q = 0; q < b.n; ++q) {
+          LsTask& t = b.t[q];
+          t.phis = member(c, t.l).fit;
+          t.out = member(c, t.l).cv;
+        }
+        launch_recurvature(c, b);
+      }
+    for (LsBatch& b : b0) {
+      for (int q = 0; q < b.n; ++q) {
+        LsTask& t = b.t[q];
+        t.phi0 = c.lv[t.l];
+        t.phis = member(c, t.l).cv;
+      }
+      launch_jumps(c, b);
     }
-    launch_jumps(c, b, c.lv[l], c.curv, l == 0);
   }
+  c.curv_stale = true;
+  c.nrm_stale = true;
 }
 
 int read_scalars(Ctx& c) {
@@ -674,8 +890,9 @@ int icls_upload_field(icls_ctx* h, int id, int l, const double* host) {
   CK(cudaMemcpyAsync(d, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c.s));
   CK(cudaStreamSynchronize(c.s));
   if (id == ICLS_F_LVSET) {  // a new level set: sweep it whole until its band is measured
+    collect_bbox(c);
     DropWin& w = c.win[l - 1];
-    w.box = w.valid = full_box(c.P);
+    w.box = w.valid = full_region(c.P);
     w.have_D = false;
     w.bg_valid = false;
   }
@@ -692,6 +909,7 @@ int icls_download_field(icls_ctx* h, int id, int l, double* host) {
     const DropWin& w = c.win[l - 1];
     if (!is_full(c.P, w.valid)) launch_materialize(c, w.valid, w.bg, w.bg_ghost, d);
   }
+  if (id == ICLS_F_CURV || id == ICLS_F_NORMAL_M) fix_curv(c);
   CK(cudaMemcpyAsync(host, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c.s));
   CK(cudaStreamSynchronize(c.s));
   return ICLS_OK;
@@ -989,7 +1207,7 @@ int icls_tube_construction(icls_ctx* h, int l) {
   if (!h) return ICLS_E_ARG;
   LARG(h, l);
   make_full(h->c, l - 1);
-  tube_construction(h->c, l - 1, full_box(h->c.P));
+  tube_construction(h->c, l - 1);
   return check_launch();
 }
 
@@ -1027,8 +1245,13 @@ int icls_update_materials(icls_ctx* h) {
 int icls_get_curvature(icls_ctx* h, int l) {
   NEED(h);
   LARG(h, l);
-  make_full(h->c, l - 1);
-  launch_curvature(h->c, full_box(h->c.P), h->c.lv[l - 1], h->c.curv, h->c.nrm_m);
+  Ctx& c = h->c;
+  make_full(c, l - 1);
+  std::vector<LsBatch> b = single(c, l - 1, kStageRows, c_region(c.P, c.win[l - 1].box, 1));
+  b[0].t[0].phi0 = c.lv[l - 1];
+  b[0].t[0].out = c.curv;
+  launch_curvature(c, b[0], c.nrm_m);
+  c.curv_stale = c.nrm_stale = false;
   return check_launch();
 }
 

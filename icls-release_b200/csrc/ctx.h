@@ -19,20 +19,57 @@ constexpr int kRedBlocks = 1184;   // 8 x 148 SMs: fixed grid of the reduction k
 constexpr int kRedThreads = 256;
 constexpr int kMaxDropsParam = 256;  // drops whose far-field counts travel as a kernel parameter
 
-// Sweep state of one drop's level set.  Outside valid's write region every
+constexpr int kTasks = 64;          // drops per batched launch (tasks travel as a kernel parameter)
+constexpr int TBX = 32, TBY = 8;    // column tile of a batched launch
+
+// One drop's share of a batched launch.  A block of TBX x TBY threads
+// sweeps one column tile of the region over one chunk of z rows, each
+// thread walking its column upwards: chunk m covers rows z0 + m*kc ..
+// z0 + (m+1)*kc - 1, the last chunk runs to z1.  Every chunk holds at least
+// kc rows, so the rows a wall row extrapolates from lie in its chunk.
+struct LsTask {
+  Region r;
+  int tx, ty, nch, kc;
+  int l, pad;
+  double bg, bgg;        // far-field values of the apron: rows 0..k1 / ghost rows
+  const double* phi0;    // RK base (read at the thread's own cell only)
+  const double* phis;    // stage input (stencil reads)
+  const double* orig;    // reinitialisation: sgn source
+  double* out;
+  uint8_t* mask;         // the drop's band mask (tube writes, advection reads)
+  Region vin;            // tube: phi0 holds valid data on vin's written cells,
+  double bgin, bggin;    //       these far-field values elsewhere
+  double far;            // reinitialisation: change of the far field this iteration
+};
+struct LsBatch {
+  int n;
+  int start[kTasks + 1];  // first block of each task
+  LsTask t[kTasks];
+};
+
+// per-drop state of the reinitialisation early exit (levelset.f90:827-835)
+struct ReinitState {
+  double residual;  // max |phi_new - phi_0| of the running iteration
+  double last;      // residual of the last completed iteration
+  int done;         // residual < dz**5 reached
+  int iters;
+};
+
+// Sweep state of one drop's level set.  Outside valid's written cells every
 // cell holds the far-field value bg (the stored array there is stale);
-// box is the region the current step sweeps.  D is the bounding box of the
-// cells that differed from +6dz after the last tube_construction, grow the
-// number of cells the non-uniform region can have spread since.
+// box is the region the current step sweeps.  The band span (Dxa, Dxn),
+// (Dya, Dyn), [Dz0, Dz1] covers the cells that differed from +6dz after the
+// last tube_construction, grow the number of cells the non-uniform region
+// can have spread since.
 struct DropWin {
-  Box3 box;
-  Box3 valid;
+  Region box;
+  Region valid;
   double bg = 0.0;        // far field of rows 0..k1
   double bg_ghost = 0.0;  // far field of the ghost rows k<0, k>k1
   bool bg_valid = false;  // bg/bg_ghost hold the far-field values
   bool have_D = false;
   int pending_grow = 0;
-  int D[6] = {0, 0, 0, 0, 0, 0};
+  int Dxa = 1, Dxn = 0, Dya = 1, Dyn = 0, Dz0 = 0, Dz1 = -1;
   int grow = 0;
 };
 
@@ -46,7 +83,8 @@ struct Ctx {
   double *u = nullptr, *v = nullptr, *w = nullptr, *pnew = nullptr, *pold = nullptr, *p = nullptr;
   double *dudt = nullptr, *dvdt = nullptr, *dwdt = nullptr;
   double *px = nullptr, *py = nullptr, *pz = nullptr, *pxold = nullptr, *pyold = nullptr, *pzold = nullptr;
-  double *pjump = nullptr, *miu = nullptr, *rho = nullptr, *jiemian = nullptr, *curv = nullptr, *recurv = nullptr;
+  double *pjump = nullptr, *miu = nullptr, *rho = nullptr, *jiemian = nullptr;
+  double *curv = nullptr;      // curv_cmn: re_curvature of the last drop (get_curvature in TwoD)
   double *dheav = nullptr, *kappa = nullptr;
   // shape I
   double *duold[2] = {nullptr, nullptr}, *dvold[2] = {nullptr, nullptr}, *dwold[2] = {nullptr, nullptr};
@@ -54,10 +92,17 @@ struct Ctx {
   double *rho_u = nullptr, *rho_v = nullptr, *rho_w = nullptr;
   double *ucc = nullptr, *vcc = nullptr, *wcc = nullptr, *nrm_m = nullptr;
   double *ulc = nullptr, *vlc = nullptr, *wlc = nullptr;
-  // level sets (shape L): one buffer per drop plus four scratch buffers
+  // level sets (shape L): one buffer per drop
   std::vector<double*> lv;
-  double* ls_scr[4] = {nullptr, nullptr, nullptr, nullptr};
-  uint8_t* mask = nullptr;              // tube mask of the drop being advanced
+  // working buffers of the drops of one group (drop l uses member l % G):
+  // three level-set stage buffers, the band mask, get_curvature and
+  // re_curvature outputs.  G is sized to the free HBM at creation.
+  struct Member {
+    double *s1 = nullptr, *s2 = nullptr, *s3 = nullptr;  // shape L
+    double *fit = nullptr, *cv = nullptr;                // shape C
+    uint8_t* mask = nullptr;                             // shape I
+  };
+  std::vector<Member> mem;
   long long* d_nbcnt = nullptr;         // band counts per drop
   // Poisson
   double* spec = nullptr;               // compact (1:imax,1:jmax,1:kmax) spectral buffer
@@ -73,6 +118,9 @@ struct Ctx {
   double* dvol = nullptr;               // volume(1:L)
   double* dvol0 = nullptr;              // init_volume(1:L)
   double* dmaxchk = nullptr;            // per drop maxchk of the last inflation
+  ReinitState* drs = nullptr;           // per drop
+  double* hpart = nullptr;              // per-tile partial sums, red_cap per drop
+  int red_cap = 0;                      // column tiles of a whole x-y plane
   // pinned host mirrors
   double* h_vol = nullptr;
   DevScalars* h_sc = nullptr;
@@ -90,8 +138,12 @@ struct Ctx {
   // per-drop sweep boxes
   std::vector<DropWin> win;
   bool use_boxes = true;
-  int* d_bbox = nullptr;                // 6 ints per drop, written by the tube kernel
+  // 10 ints per drop, written by the tube kernel: minima then maxima of
+  // {x, x shifted by imax/2, y, y shifted by jmax/2, z} over the band
+  int* d_bbox = nullptr;
   int* h_bbox = nullptr;                // pinned copy
+  bool curv_stale = false;              // curv / normal%m hold more than the last drop
+  bool nrm_stale = false;
   cudaEvent_t ev_bbox = nullptr;
   bool bbox_pending = false;
   std::vector<double> outside;          // interior cells outside each drop's box
@@ -101,31 +153,30 @@ struct Ctx {
 void set_pseudo_inverse(const double* P270, cudaStream_t s);
 
 // level set (k_levelset.cu)
-dim3 grid_of(const int* r0, const int* r1);
-Box3 full_box(const Params& P);
-Box3 c_region(const Params& P, const Box3& b, int apron);
-void launch_tube(Ctx& c, const Box3& b, const Box3& vin, double bgin, double bgg, const double* in, double* out,
-                 long long* cnt, int* bbox);
-void launch_adv_stage(Ctx& c, const Box3& b, double bg_out, double bgg_out, int scheme, int stage1,
-                      const double* phi0, const double* phis, double a, double bb, double fdt, const double* vu,
-                      const double* vv, const double* vw, double* out);
-void launch_reinit_stage(Ctx& c, const Box3& b, double bg_out, double bgg_out, int stage, const double* phi0,
-                         const double* phis, const double* orig, double dtau, double* out);
-void launch_reinit_check(Ctx& c, int it, int maxiter, double thr, double far);
-void launch_reinit_reset(Ctx& c, int maxiter);
-void launch_heaviside_drop(Ctx& c, const Box3& b, const double* phi, int l, int first);
+Region full_region(const Params& P);
+bool region_full(const Params& P, const Region& r);
+Region c_region(const Params& P, const Region& r, int apron);
+void set_tiles(LsBatch& b, int kc);
+void launch_tube(Ctx& c, const LsBatch& b);
+void launch_adv_stage(Ctx& c, const LsBatch& b, int scheme, int stage1, double a, double bb, double fdt,
+                      const double* vu, const double* vv, const double* vw);
+void launch_reinit_stage(Ctx& c, const LsBatch& b, int stage, double dtau);
+void launch_reinit_reset(Ctx& c, const LsBatch& b, int maxiter);
+void launch_reinit_check(Ctx& c, const LsBatch& b, int it, int maxiter, double thr);
+void launch_heaviside(Ctx& c, const LsBatch& b);
 void launch_fill(Ctx& c, double* a, long long n, double v);
-void launch_materials_final(Ctx& c, const double* outside);
-void launch_inflate_sums(Ctx& c, const Box3& b, const double* phi, int l, double outside);
-void launch_inflate_vel(Ctx& c, const Box3& b);
+void launch_materials_final(Ctx& c, const double* outside, const int* ntiles);
+void launch_inflate_sums(Ctx& c, const LsBatch& b, double outside);
+void launch_inflate_vel(Ctx& c, const LsBatch& b);
 void launch_copy(Ctx& c, double* dst, const double* src, long long n);
 void launch_boundmls(Ctx& c, double* phi);
-void launch_materialize(Ctx& c, const Box3& b, double bg, double bgg, double* phi);
+void launch_materialize(Ctx& c, const Region& r, double bg, double bgg, double* phi);
 
-// interface / GFM (k_gfm.cu)
-void launch_curvature(Ctx& c, const Box3& b, const double* phi, double* curv_out, double* nrm_m_out);
-void launch_recurvature(Ctx& c, const Box3& b, const double* phi, const double* curv_in, double* out);
-void launch_jumps(Ctx& c, const Box3& b, const double* phi, const double* cv, int first);
+// interface / GFM (k_gfm.cu); the tasks carry shape-C regions
+// curvature: phi0 -> out (+ normal%m); recurvature: phis -> out; jumps: phi0, phis
+void launch_curvature(Ctx& c, const LsBatch& b, double* nrm_m_out);
+void launch_recurvature(Ctx& c, const LsBatch& b);
+void launch_jumps(Ctx& c, const LsBatch& b);
 void launch_ipot(Ctx& c, double* dmin_dev);
 
 // Navier-Stokes (k_navier.cu)

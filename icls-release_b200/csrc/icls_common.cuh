@@ -65,21 +65,27 @@ __device__ __forceinline__ double divx(const Params& p, double a) { return p.pow
 __device__ __forceinline__ double divy(const Params& p, double a) { return p.pow2 ? a * p.rdy : a / p.dy; }
 __device__ __forceinline__ double divz(const Params& p, double a) { return p.pow2 ? a * p.rdz : a / p.dz; }
 
-// ---------------------------------------------------------------- boxes
-// A per-drop sweep region in the Fortran coordinates of the level-set
-// array (-2:i1+2,..).  Cells in [c0,c1] are computed; cells of the write
-// region [w0,w1] outside it form the apron and receive the far-field value.
-// A full axis has c = w = the whole index range.
-struct Box3 {
-  int c0[3], c1[3];
-  int w0[3], w1[3];
+// -------------------------------------------------------------- regions
+// A per-drop sweep region.  x and y are periodic: the region holds the
+// interior columns xa, xa+1, ..., xa+xn-1 (mod imax) and likewise in y,
+// and a kernel that writes a column also writes its periodic halo images,
+// so the stored halos always equal their source columns.  z is walled: a
+// plain range of the storage index (ghost rows -2,-1 and k1+1,k1+2
+// included).  The computed part is given by offsets into the written
+// spans; written cells outside it form the apron and receive the far-field
+// value.  A full axis has xa = 1, xn = imax and no apron.
+struct Region {
+  int xa, xn, ya, yn;      // written columns
+  int cx0, cx1, cy0, cy1;  // computed part, offsets into the written spans
+  int z0, z1, cz0, cz1;    // written and computed storage rows
 };
-__host__ __device__ __forceinline__ bool in_compute(const Box3& b, int i, int j, int k) {
-  return i >= b.c0[0] && i <= b.c1[0] && j >= b.c0[1] && j <= b.c1[1] && k >= b.c0[2] && k <= b.c1[2];
+// column col (1..n) lies in the periodic span a..a+len-1
+__host__ __device__ __forceinline__ bool span_has(int a, int len, int n, int col) {
+  int d = col - a;
+  if (d < 0) d += n;
+  return d < len;
 }
-__host__ __device__ __forceinline__ bool in_write(const Box3& b, int i, int j, int k) {
-  return i >= b.w0[0] && i <= b.w1[0] && j >= b.w0[1] && j <= b.w1[1] && k >= b.w0[2] && k <= b.w1[2];
-}
+
 // 3-D launch over a region: 32 x 8 threads per block in (i,j), one k per
 // block layer.  The thread's cell is (r0 + ...), valid while <= r1.
 constexpr int BX = 32, BY = 8;

@@ -12,7 +12,7 @@
 // cache broadcasts.
 #include <algorithm>
 
-#include "ctx.h"
+#include "batch.cuh"
 
 namespace icls {
 
@@ -70,41 +70,50 @@ __device__ __forceinline__ double curvature_at(const Params& p, const double* __
   return cv;
 }
 
-// get_curvature + boundc over a drop's region of shape C: wall rows stay 0,
-// halos are the periodic copies (bound.f90:292-305), the apron (far field,
-// |phi| > 5dz) is 0.
-__global__ void __launch_bounds__(NT) k_curvature(Params p, Box3 r, const double* __restrict__ phi,
-                                                  double* __restrict__ curv, double* __restrict__ nrm_m) {
-  int i, j, k;
-  if (!cell3(r.w0, r.w1, i, j, k)) return;
-  const long long n = idxC(p, i, j, k);
-  if (k == 0 || k == p.k1 || !in_compute(r, i, j, k)) { curv[n] = 0.; return; }
-  const int I = wrapx(p, i), J = wrapy(p, j);
-  double m;
-  curv[n] = curvature_at(p, phi, I, J, k, m);
-  if (I == i && J == j && nrm_m) nrm_m[idxI(p, i, j, k)] = m;
+// get_curvature + boundc over the tasks' shape-C regions (phi0 = the
+// drop's level set, out = its curvature): wall rows stay 0, halos are the
+// periodic copies (bound.f90:292-305), the apron (far field, |phi| > 5dz)
+// is 0.
+__global__ void __launch_bounds__(NT) k_curvature(Params p, const __grid_constant__ LsBatch B,
+                                                  double* __restrict__ nrm_m) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  if (!c.ok) return;
+  for (int k = c.ka; k <= c.kb; ++k) {
+    double v = 0.;
+    if (k != 0 && k != p.k1 && computed(c, t.r, k)) {
+      double m;
+      v = curvature_at(p, t.phi0, c.i, c.j, k, m);
+      if (nrm_m) nrm_m[idxI(p, c.i, c.j, k)] = m;
+    }
+    putC(p, t.out, c.i, c.j, k, v);
+  }
 }
 
-// re_curvature + boundc (interface.f90:186-218) over a drop's region
-__global__ void __launch_bounds__(NT) k_recurvature(Params p, Box3 r, const double* __restrict__ phi,
-                                                    const double* __restrict__ cin, double* __restrict__ out) {
-  int i, j, k;
-  if (!cell3(r.w0, r.w1, i, j, k)) return;
-  const long long n = idxC(p, i, j, k);
-  if (k == 0 || k == p.k1 || !in_compute(r, i, j, k)) { out[n] = 0.; return; }
-  const int I = wrapx(p, i), J = wrapy(p, j);
-  double acc = 0.;
-  if (fabs(phi[idxL(p, I, J, k)]) < 2. * p.dz) {
-    const long long c = idxC(p, I, J, k), sy = p.nCx, sz = (long long)p.nCx * p.nCy;
-    int q = 0;
+// re_curvature + boundc (interface.f90:186-218) over the tasks' regions:
+// phis (get_curvature) -> out
+__global__ void __launch_bounds__(NT) k_recurvature(Params p, const __grid_constant__ LsBatch B) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const double* __restrict__ cin = t.phis;
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  if (!c.ok) return;
+  const long long sy = p.nCx, sz = (long long)p.nCx * p.nCy;
+  for (int k = c.ka; k <= c.kb; ++k) {
+    double acc = 0.;
+    if (k != 0 && k != p.k1 && computed(c, t.r, k) && fabs(t.phi0[idxL(p, c.i, c.j, k)]) < 2. * p.dz) {
+      const long long cc = idxC(p, c.i, c.j, k);
+      int q = 0;
 #pragma unroll
-    for (int dk = -1; dk <= 1; ++dk)
+      for (int dk = -1; dk <= 1; ++dk)
 #pragma unroll
-      for (int dj = -1; dj <= 1; ++dj)
+        for (int dj = -1; dj <= 1; ++dj)
 #pragma unroll
-        for (int di = -1; di <= 1; ++di) acc = acc + cP[q++] * cin[c + di + dj * sy + dk * sz];
+          for (int di = -1; di <= 1; ++di) acc = acc + cP[q++] * cin[cc + di + dj * sy + dk * sz];
+    }
+    putC(p, t.out, c.i, c.j, k, acc);
   }
-  out[n] = acc;
 }
 
 // icurvature, 3-D and TwoD branches (interface.f90:126-179)
@@ -153,35 +162,43 @@ __device__ __forceinline__ double axis_jump(const Params& p, const double* __res
   return (jm + 0.) + jp;
 }
 
-// gfm4p jump shell of drop l (gfm.f90:95-238); first=1 assigns (l=1)
-__global__ void __launch_bounds__(NT) k_jumps(Params p, Box3 r, const double* __restrict__ phi,
-                                              const double* __restrict__ cv, int first,
+// gfm4p jump shell of the tasks' drops (gfm.f90:95-238; phis = the drop's
+// re_curvature), added to the jump fields that gfm4p zeroed (gfm.f90:75-79).
+// The additions are atomic: where at most two drops reach a cell the sum is
+// the reference's exactly (0+a+b is exact in either order); a cell in the
+// shells of three or more drops may differ in the last bit.
+__global__ void __launch_bounds__(NT) k_jumps(Params p, const __grid_constant__ LsBatch B,
                                               double* __restrict__ pjump, double* __restrict__ px,
                                               double* __restrict__ py, double* __restrict__ pz) {
-  int i, j, k;
-  if (!cell3(r.c0, r.c1, i, j, k)) return;
-  if (i < 1 || i > p.imax || j < 1 || j > p.jmax || k < 1 || k > p.kmax) return;
-  const long long cl = idxL(p, i, j, k);
-  const double lv = phi[cl];
-  if (!(fabs(lv) <= 2. * p.dz)) return;
-  const long long cc = idxC(p, i, j, k);
-  double fx, fy, fz;
-  const double jump_x = axis_jump(p, phi, cv, cl, 1, cc, 1, fx);
-  const double jump_y = axis_jump(p, phi, cv, cl, p.nLx, cc, p.nCx, fy);
-  const double jump_z = axis_jump(p, phi, cv, cl, (long long)p.nLx * p.nLy, cc, (long long)p.nCx * p.nCy, fz);
-  double pj;
-  if (lv > 0.) {
-    pj = (div2(p, jump_x, p.dx, p.rdx) + div2(p, jump_y, p.dy, p.rdy)) + div2(p, jump_z, p.dz, p.rdz);
-  } else if (lv < 0.) {
-    pj = -((div2(p, jump_x, p.dx, p.rdx) + div2(p, jump_y, p.dy, p.rdy)) + div2(p, jump_z, p.dz, p.rdz));
-    fx = -fx; fy = -fy; fz = -fz;
-  } else {
-    pj = 0.; fx = 0.; fy = 0.; fz = 0.;
-  }
-  if (first) {
-    pjump[cc] = pj; px[cc] = fx; py[cc] = fy; pz[cc] = fz;
-  } else {
-    pjump[cc] = pjump[cc] + pj; px[cc] = px[cc] + fx; py[cc] = py[cc] + fy; pz[cc] = pz[cc] + fz;
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const double* __restrict__ cv = t.phis;
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  if (!c.ok || !c.cxy) return;
+  const double* __restrict__ phi = t.phi0;
+  const int i = c.i, j = c.j;
+  for (int k = max(c.ka, max(t.r.cz0, 1)); k <= min(c.kb, min(t.r.cz1, p.kmax)); ++k) {
+    const long long cl = idxL(p, i, j, k);
+    const double lv = phi[cl];
+    if (!(fabs(lv) <= 2. * p.dz)) continue;
+    const long long cc = idxC(p, i, j, k);
+    double fx, fy, fz;
+    const double jump_x = axis_jump(p, phi, cv, cl, 1, cc, 1, fx);
+    const double jump_y = axis_jump(p, phi, cv, cl, p.nLx, cc, p.nCx, fy);
+    const double jump_z = axis_jump(p, phi, cv, cl, (long long)p.nLx * p.nLy, cc, (long long)p.nCx * p.nCy, fz);
+    double pj;
+    if (lv > 0.) {
+      pj = (div2(p, jump_x, p.dx, p.rdx) + div2(p, jump_y, p.dy, p.rdy)) + div2(p, jump_z, p.dz, p.rdz);
+    } else if (lv < 0.) {
+      pj = -((div2(p, jump_x, p.dx, p.rdx) + div2(p, jump_y, p.dy, p.rdy)) + div2(p, jump_z, p.dz, p.rdz));
+      fx = -fx; fy = -fy; fz = -fz;
+    } else {
+      pj = 0.; fx = 0.; fy = 0.; fz = 0.;
+    }
+    atomicAdd(pjump + cc, pj);
+    atomicAdd(px + cc, fx);
+    atomicAdd(py + cc, fy);
+    atomicAdd(pz + cc, fz);
   }
 }
 
@@ -190,21 +207,27 @@ __device__ __forceinline__ unsigned long long ord_bits(double x) {
   unsigned long long b = (unsigned long long)__double_as_longlong(x);
   return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
 }
-__global__ void __launch_bounds__(NT) k_ipot_pair(Params p, Box3 r, const double* __restrict__ pm,
-                                                  const double* __restrict__ pn,
+// one pair (m, n): sweeps m's written cells (task 0, phi0 = phi_m); phi_n
+// is read where n's region wrote it and is its far field bgn elsewhere
+__global__ void __launch_bounds__(NT) k_ipot_pair(Params p, const __grid_constant__ LsBatch B, const double* __restrict__ pn,
+                                                  Region rn, double bgn, double bggn,
                                                   unsigned long long* __restrict__ out) {
-  int i, j, k;
+  const LsTask& t = B.t[0];
+  const Col c = col_of(p, t, (int)blockIdx.x);
   double s = 1e3;
-  if (cell3(r.w0, r.w1, i, j, k)) {
-    const long long n = idxL(p, i, j, k);
-    const double a = pm[n], b = pn[n];
-    if (a > -1. * p.dz && a < 1. * p.dz && b < p.NB) s = a + b;
+  if (c.ok) {
+    for (int k = c.ka; k <= c.kb; ++k) {
+      const long long n = idxL(p, c.i, c.j, k);
+      const double a = t.phi0[n];
+      const double b = in_written(p, rn, c.i, c.j, k) ? pn[n] : ((k < 0 || k > p.k1) ? bggn : bgn);
+      if (a > -1. * p.dz && a < 1. * p.dz && b < p.NB) s = fmin(s, a + b);
+    }
   }
   // block min through the ordered bit pattern
   unsigned long long bits = ord_bits(s);
   for (int o = 16; o > 0; o >>= 1) {
-    unsigned long long t = __shfl_down_sync(0xffffffffu, bits, o);
-    bits = t < bits ? t : bits;
+    unsigned long long q = __shfl_down_sync(0xffffffffu, bits, o);
+    bits = q < bits ? q : bits;
   }
   __shared__ unsigned long long red[NT / 32];
   if ((flat_tid() & 31) == 0) red[flat_tid() >> 5] = bits;
@@ -222,42 +245,44 @@ void set_pseudo_inverse(const double* P270, cudaStream_t s) {
   cudaMemcpyToSymbolAsync(cP, P270, 270 * sizeof(double), 0, cudaMemcpyHostToDevice, s);
 }
 
-void launch_curvature(Ctx& c, const Box3& b, const double* phi, double* curv_out, double* nrm_m_out) {
+const dim3 kTile(TBX, TBY, 1);
+
+void launch_curvature(Ctx& c, const LsBatch& b, double* nrm_m_out) {
+  if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "curvature", 1);
-  const Box3 r = c_region(c.P, b, 1);
-  k_curvature<<<grid_of(r.w0, r.w1), dim3(BX, BY, 1), 0, c.s>>>(c.P, r, phi, curv_out, nrm_m_out);
+  k_curvature<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, nrm_m_out);
 }
-void launch_recurvature(Ctx& c, const Box3& b, const double* phi, const double* curv_in, double* out) {
+void launch_recurvature(Ctx& c, const LsBatch& b) {
+  if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "recurvature", 1);
-  const Box3 r = c_region(c.P, b, 1);
-  k_recurvature<<<grid_of(r.w0, r.w1), dim3(BX, BY, 1), 0, c.s>>>(c.P, r, phi, curv_in, out);
+  k_recurvature<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b);
 }
-void launch_jumps(Ctx& c, const Box3& b, const double* phi, const double* cv, int first) {
+void launch_jumps(Ctx& c, const LsBatch& b) {
+  if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "jumps", 1);
-  const Box3 r = c_region(c.P, b, 0);
-  k_jumps<<<grid_of(r.c0, r.c1), dim3(BX, BY, 1), 0, c.s>>>(c.P, r, phi, cv, first, c.pjump, c.px, c.py, c.pz);
+  k_jumps<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.pjump, c.px, c.py, c.pz);
 }
-// dmin_dev: L*L unsigned long long ordered bits, filled here
-// only the overlap of the two drops' write regions can hold cells with
-// |phi_m| < dz and phi_n < 6dz: elsewhere one of them is in its far field
+// dmin_dev: L*L unsigned long long ordered bits, filled here; only cells
+// written by both drops' regions can hold |phi_m| < dz and phi_n < 6dz
+// unless a far field is below 6dz, so each pair sweeps m's written cells
 void launch_ipot(Ctx& c, double* dmin_dev) {
   unsigned long long* o = reinterpret_cast<unsigned long long*>(dmin_dev);
+  LsBatch b;
+  b.n = 1;
   for (int m = 0; m < c.P.L; ++m)
     for (int n = 0; n < c.P.L; ++n) {
       if (m == n) continue;
-      const Box3& a = c.win[m].valid;
-      const Box3& b = c.win[n].valid;
-      Box3 r;
-      bool empty = false;
-      for (int ax = 0; ax < 3; ++ax) {
-        r.w0[ax] = r.c0[ax] = std::max(a.w0[ax], b.w0[ax]);
-        r.w1[ax] = r.c1[ax] = std::min(a.w1[ax], b.w1[ax]);
-        if (r.w0[ax] > r.w1[ax]) empty = true;
-      }
-      if (empty) continue;
+      LsTask& t = b.t[0];
+      t = LsTask();
+      t.r = c.win[m].valid;
+      t.r.cx0 = 0; t.r.cx1 = t.r.xn - 1; t.r.cy0 = 0; t.r.cy1 = t.r.yn - 1;
+      t.r.cz0 = t.r.z0; t.r.cz1 = t.r.z1;
+      t.l = m;
+      t.phi0 = c.lv[m];
+      set_tiles(b, 8);
       Scope sc_(c.prof, c.s, "ipot", 1);
-      k_ipot_pair<<<grid_of(r.w0, r.w1), dim3(BX, BY, 1), 0, c.s>>>(c.P, r, c.lv[m], c.lv[n],
-                                                                    o + m + (long long)c.P.L * n);
+      k_ipot_pair<<<b.start[1], kTile, 0, c.s>>>(c.P, b, c.lv[n], c.win[n].valid, c.win[n].bg, c.win[n].bg_ghost,
+                                                 o + m + (long long)c.P.L * n);
     }
 }
 

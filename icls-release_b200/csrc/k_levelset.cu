@@ -8,30 +8,39 @@
 //   inflation          levelset.f90:407-582
 //   update_materials   misc.f90:79-290 with Heaviside 'trig' misc.f90:297-464
 //
-// Halo handling: instead of a separate boundsls pass, every output cell of
-// the (-2:i1+2,-2:j1+2,-2:k1+2) array is computed from its periodic source
-// column (I,J) = wrap(i,j); the wall rows k=0 and k=k1 evaluate the two
-// interior values they extrapolate from.  This reproduces boundsls
-// (z-extrapolation, then periodic x, then periodic y) exactly, because the
-// inputs already satisfy the periodic halo invariant.
+// Halo handling: instead of a separate boundsls pass, a thread computes an
+// interior column and writes it together with its periodic halo images;
+// the wall rows k=0 and k=k1 are the linear extrapolation of the two
+// interior values next to them, evaluated by the thread that computes
+// those.  This reproduces boundsls (z-extrapolation, then periodic x, then
+// periodic y) exactly, because the inputs satisfy the periodic halo
+// invariant.
 //
-// Sweep boxes: after tube_construction clips the level set to +-6dz, every
-// cell outside a drop's band holds the same far-field value, and every
-// kernel maps a uniform neighbourhood to a uniform value (the stencils of a
-// constant field are exactly zero).  Each per-drop kernel therefore sweeps
-// only a box around the band (Box3 compute region) and writes the
-// far-field value, replayed on the host with the same arithmetic, into a
-// 3-cell apron around it; reads never leave the box plus apron.  Full axes
-// (band near a periodic seam or a wall) fall back to the whole index range.
+// Sweep regions: after tube_construction clips the level set to +-6dz,
+// every cell outside a drop's band holds the same far-field value, and
+// every kernel maps a uniform neighbourhood to a uniform value (the
+// stencils of a constant field are exactly zero).  Each per-drop kernel
+// therefore sweeps only a region around the band (periodic column spans in
+// x and y, rows in z) and writes the far-field value, replayed on the host
+// with the same arithmetic, into a 3-cell apron around it; reads never
+// leave the region plus apron.  All drops of a step go through one launch
+// per stage (batch.cuh).
+//
+// In-place stages: the last RK stage may write the array it takes as its
+// pointwise base (phi0): a thread reads phi0 only in its own column, and
+// it writes a wall row only after it has computed the rows it extrapolates.
+#include <algorithm>
 #include <climits>
 
-#include "ctx.h"
+#include "batch.cuh"
 
 namespace icls {
 
 namespace {
 
-constexpr int NT = 256;
+constexpr int NT = TBX * TBY;
+const dim3 kTile(TBX, TBY, 1);
+const dim3 kBlock(BX, BY, 1);
 
 __device__ __forceinline__ double clipNB(double x, double NB) {
   return x > NB ? NB : (x < -NB ? -NB : x);
@@ -39,75 +48,80 @@ __device__ __forceinline__ double clipNB(double x, double NB) {
 __device__ __forceinline__ bool interior(const Params& p, int i, int j, int k) {
   return i >= 1 && i <= p.imax && j >= 1 && j <= p.jmax && k >= 1 && k <= p.kmax;
 }
-__device__ __forceinline__ void decode_box(const int* r0, const int* r1, int q, int& i, int& j, int& k) {
-  const int nx = r1[0] - r0[0] + 1, ny = r1[1] - r0[1] + 1;
-  i = r0[0] + q % nx;
-  const int r = q / nx;
-  j = r0[1] + r % ny;
-  k = r0[2] + r / ny;
-}
 
 // ---------------------------------------------------------------- tube
-// in is valid on vin's write region; elsewhere it holds bgin, except the
-// ghost rows k<0, k>k1 (never touched by the reinitialisation RHS), which
-// hold bgg.  Writes b's write region; the band mask for computed interior
-// cells; the band count; the bounding box of computed cells whose clipped
-// value is not +NB.
-__global__ void __launch_bounds__(NT) k_tube(Params p, Box3 b, Box3 vin, double bgin, double bgg,
-                                             const double* __restrict__ in, double* __restrict__ out,
-                                             uint8_t* __restrict__ mask, long long* __restrict__ cnt,
-                                             int* __restrict__ bbox) {
-  int i, j, k;
-  const bool ok = cell3(b.w0, b.w1, i, j, k);
+// Clip to +-NB (levelset.f90:120-128) and the band mask (130-160) over the
+// tasks' regions.  phi0 holds valid data on vin's written cells, bgin
+// (rows 0..k1) or bggin (ghost rows) elsewhere.  Counts the band per drop
+// and records the extent of the cells whose clipped value is not +NB:
+// bbox_lo[5 l + a], bbox_hi[5 l + a] for a = x, x shifted by imax/2, y, y
+// shifted by jmax/2, z.
+__global__ void __launch_bounds__(NT) k_tube(Params p, const __grid_constant__ LsBatch B,
+                                             long long* __restrict__ cnt, int* __restrict__ bbox_lo,
+                                             int* __restrict__ bbox_hi) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
   const double NB = p.NB;
-  int m = 0;
-  int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
-  auto rd = [&](int a, int bb, int cc) -> double {
-    return in_write(vin, a, bb, cc) ? in[idxL(p, a, bb, cc)] : ((cc < 0 || cc > p.k1) ? bgg : bgin);
+  const double* __restrict__ in = t.phi0;
+  int band = 0;
+  int lo[5] = {INT_MAX, INT_MAX, INT_MAX, INT_MAX, INT_MAX};
+  int hi[5] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN};
+  auto rd = [&](int a, int b, int k) -> double {
+    return in_written(p, t.vin, a, b, k) ? in[idxL(p, a, b, k)] : ((k < 0 || k > p.k1) ? t.bggin : t.bgin);
   };
-  if (ok) {
-    const long long n = idxL(p, i, j, k);
-    double val;
-    if (!in_compute(b, i, j, k)) {
-      val = clipNB((k < 0 || k > p.k1) ? bgg : bgin, NB);
-    } else {
-      const int I = wrapx(p, i), J = wrapy(p, j);
-      if (k == 0)
-        val = 2. * clipNB(rd(I, J, 1), NB) - clipNB(rd(I, J, 2), NB);
-      else if (k == p.k1)
-        val = 2. * clipNB(rd(I, J, p.kmax), NB) - clipNB(rd(I, J, p.kmax - 1), NB);
-      else
-        val = clipNB(rd(I, J, k), NB);
-      if (interior(p, i, j, k)) {
-        const double c0 = clipNB(rd(i, j, k), NB);
-        if (fabs(c0) < NB) {
-          m = 1;
-        } else {
-          double xs = 0., ys = 0., zs = 0.;
-          for (int d = -2; d <= 2; ++d) xs += fabs(clipNB(rd(i + d, j, k), NB)) - NB;
-          for (int d = -2; d <= 2; ++d) ys += fabs(clipNB(rd(i, j + d, k), NB)) - NB;
-          for (int d = -2; d <= 2; ++d) zs += fabs(clipNB(rd(i, j, k + d), NB)) - NB;
-          m = (xs == 0. && ys == 0. && zs == 0.) ? 0 : 1;
+  if (c.ok) {
+    const int i = c.i, j = c.j;
+    const int hx = p.imax / 2, hy = p.jmax / 2;
+    const int ib = i + hx > p.imax ? i + hx - p.imax : i + hx;
+    const int jb = j + hy > p.jmax ? j + hy - p.jmax : j + hy;
+    for (int k = c.ka; k <= c.kb; ++k) {
+      double val;
+      if (!computed(c, t.r, k)) {
+        val = clipNB((k < 0 || k > p.k1) ? t.bggin : t.bgin, NB);
+      } else {
+        if (k == 0)
+          val = 2. * clipNB(rd(i, j, 1), NB) - clipNB(rd(i, j, 2), NB);
+        else if (k == p.k1)
+          val = 2. * clipNB(rd(i, j, p.kmax), NB) - clipNB(rd(i, j, p.kmax - 1), NB);
+        else
+          val = clipNB(rd(i, j, k), NB);
+        if (k >= 1 && k <= p.kmax) {
+          int m;
+          if (fabs(val) < NB) {
+            m = 1;
+          } else {
+            double xs = 0., ys = 0., zs = 0.;
+            for (int d = -2; d <= 2; ++d) xs += fabs(clipNB(rd(i + d, j, k), NB)) - NB;
+            for (int d = -2; d <= 2; ++d) ys += fabs(clipNB(rd(i, j + d, k), NB)) - NB;
+            for (int d = -2; d <= 2; ++d) zs += fabs(clipNB(rd(i, j, k + d), NB)) - NB;
+            m = (xs == 0. && ys == 0. && zs == 0.) ? 0 : 1;
+          }
+          t.mask[idxI(p, i, j, k)] = (uint8_t)m;
+          band += m;
         }
-        mask[idxI(p, i, j, k)] = (uint8_t)m;
+        if (val != NB) {
+          lo[0] = min(lo[0], i); hi[0] = max(hi[0], i);
+          lo[1] = min(lo[1], ib); hi[1] = max(hi[1], ib);
+          lo[2] = min(lo[2], j); hi[2] = max(hi[2], j);
+          lo[3] = min(lo[3], jb); hi[3] = max(hi[3], jb);
+          lo[4] = min(lo[4], k); hi[4] = max(hi[4], k);
+        }
       }
-      if (val != NB) {
-        lo[0] = hi[0] = i; lo[1] = hi[1] = j; lo[2] = hi[2] = k;
-      }
+      putL(p, t.out, i, j, k, val);
     }
-    out[n] = val;
   }
-  int bs = block_sum<int, BX * BY>(m);
-  if (flat_tid() == 0 && bs) atomicAdd((unsigned long long*)cnt, (unsigned long long)bs);
-  for (int a = 0; a < 3; ++a) {
+  const int bs = block_sum<int, NT>(band);
+  if (flat_tid() == 0 && bs) atomicAdd((unsigned long long*)(cnt + t.l), (unsigned long long)bs);
+  for (int a = 0; a < 5; ++a) {
     int l = lo[a], h = hi[a];
     for (int o = 16; o > 0; o >>= 1) {
       l = min(l, __shfl_down_sync(0xffffffffu, l, o));
       h = max(h, __shfl_down_sync(0xffffffffu, h, o));
     }
     if ((flat_tid() & 31) == 0 && l != INT_MAX) {
-      atomicMin(&bbox[a], l);
-      atomicMax(&bbox[3 + a], h);
+      atomicMin(&bbox_lo[5 * t.l + a], l);
+      atomicMax(&bbox_hi[5 * t.l + a], h);
     }
   }
 }
@@ -204,30 +218,40 @@ __device__ __forceinline__ double adv_val(const Params& p, int stage1, const dou
   return v;
 }
 
+// One RK stage over the tasks' regions; out may equal phi0 (see above).
 template <int SCHEME>
-__global__ void __launch_bounds__(NT) k_adv_stage(Params p, Box3 b, double bg_out, double bgg_out, int stage1,
-                                                  const double* __restrict__ phi0, const double* __restrict__ phis,
-                                                  double a, double bb, double fdt, const double* __restrict__ vu,
-                                                  const double* __restrict__ vv, const double* __restrict__ vw,
-                                                  const uint8_t* __restrict__ mask, double* __restrict__ out) {
-  int i, j, k;
-  if (!cell3(b.w0, b.w1, i, j, k)) return;
-  const long long n = idxL(p, i, j, k);
-  if (!in_compute(b, i, j, k)) {
-    out[n] = (k < 0 || k > p.k1) ? bgg_out : bg_out;
-    return;
+__global__ void __launch_bounds__(NT) k_adv_stage(Params p, const __grid_constant__ LsBatch B, int stage1, double a,
+                                                  double bb, double fdt, const double* __restrict__ vu,
+                                                  const double* __restrict__ vv, const double* __restrict__ vw) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  if (!c.ok) return;
+  const int i = c.i, j = c.j;
+  double v1 = 0., v2 = 0., vkm = 0., vk = 0.;
+  bool wall0 = false;
+  for (int k = c.ka; k <= c.kb; ++k) {
+    if (!computed(c, t.r, k)) {
+      putL(p, t.out, i, j, k, (k < 0 || k > p.k1) ? t.bgg : t.bg);
+      continue;
+    }
+    if (k == 0) {  // written once rows 1 and 2 are known
+      wall0 = true;
+      continue;
+    }
+    double val;
+    if (k == p.k1) {
+      val = 2. * vk - vkm;
+    } else {
+      val = adv_val<SCHEME>(p, stage1, t.phi0, t.phis, a, bb, fdt, vu, vv, vw, t.mask, i, j, k);
+      if (k == 1) v1 = val;
+      if (k == 2) v2 = val;
+      if (k == p.kmax - 1) vkm = val;
+      if (k == p.kmax) vk = val;
+    }
+    putL(p, t.out, i, j, k, val);
+    if (k == 2 && wall0) putL(p, t.out, i, j, 0, 2. * v1 - v2);
   }
-  const int I = wrapx(p, i), J = wrapy(p, j);
-  double val;
-  if (k == 0)
-    val = 2. * adv_val<SCHEME>(p, stage1, phi0, phis, a, bb, fdt, vu, vv, vw, mask, I, J, 1) -
-          adv_val<SCHEME>(p, stage1, phi0, phis, a, bb, fdt, vu, vv, vw, mask, I, J, 2);
-  else if (k == p.k1)
-    val = 2. * adv_val<SCHEME>(p, stage1, phi0, phis, a, bb, fdt, vu, vv, vw, mask, I, J, p.kmax) -
-          adv_val<SCHEME>(p, stage1, phi0, phis, a, bb, fdt, vu, vv, vw, mask, I, J, p.kmax - 1);
-  else
-    val = adv_val<SCHEME>(p, stage1, phi0, phis, a, bb, fdt, vu, vv, vw, mask, I, J, k);
-  out[n] = val;
 }
 
 // ------------------------------------------------------------ reinit
@@ -295,60 +319,92 @@ __device__ __forceinline__ double reinit_val(const Params& p, int stage, const d
   return 1. / 3. * phi0[n] + 2. / 3. * (phis[n] + dtau * rhs);
 }
 
-__global__ void __launch_bounds__(NT) k_reinit_stage(Params p, Box3 b, double bg_out, double bgg_out, int stage,
-                                                     const double* __restrict__ phi0,
-                                                     const double* __restrict__ phis,
-                                                     const double* __restrict__ orig, double dtau,
-                                                     double* __restrict__ out, DevScalars* __restrict__ dsc) {
-  const int done = dsc->reinit_done;
-  int i, j, k;
-  const bool ok = cell3(b.w0, b.w1, i, j, k);
-  if (done) {
+// One SSP-RK3 stage of ls_reinit over the tasks' regions; stage 3 folds
+// max|phi_new - phi_0| into the drop's residual.  out may equal phi0.
+__global__ void __launch_bounds__(NT) k_reinit_stage(Params p, const __grid_constant__ LsBatch B, int stage,
+                                                     double dtau, ReinitState* __restrict__ rs) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  if (rs[t.l].done) {
     // an iteration after convergence is the identity (levelset.f90:833-835)
-    if (stage == 3 && ok) out[idxL(p, i, j, k)] = phi0[idxL(p, i, j, k)];
+    if (stage == 3 && c.ok && t.out != t.phi0)
+      for (int k = c.ka; k <= c.kb; ++k) putL(p, t.out, c.i, c.j, k, t.phi0[idxL(p, c.i, c.j, k)]);
     return;
   }
-  if (stage == 1 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && flat_tid() == 0) dsc->residual = 0.;
   double r = 0.;
-  if (ok) {
-    const long long n = idxL(p, i, j, k);
-    double val;
-    if (!in_compute(b, i, j, k)) {
-      val = (k < 0 || k > p.k1) ? bgg_out : bg_out;
-    } else {
-      const int I = wrapx(p, i), J = wrapy(p, j);
-      if (k == 0)
-        val = 2. * reinit_val(p, stage, phi0, phis, orig, dtau, I, J, 1) -
-              reinit_val(p, stage, phi0, phis, orig, dtau, I, J, 2);
-      else if (k == p.k1)
-        val = 2. * reinit_val(p, stage, phi0, phis, orig, dtau, I, J, p.kmax) -
-              reinit_val(p, stage, phi0, phis, orig, dtau, I, J, p.kmax - 1);
-      else
-        val = reinit_val(p, stage, phi0, phis, orig, dtau, I, J, k);
-      if (stage == 3) r = fabs(val - phi0[n]);
+  if (c.ok) {
+    const int i = c.i, j = c.j;
+    double v1 = 0., v2 = 0., vkm = 0., vk = 0.;
+    bool wall0 = false;
+    for (int k = c.ka; k <= c.kb; ++k) {
+      if (!computed(c, t.r, k)) {
+        putL(p, t.out, i, j, k, (k < 0 || k > p.k1) ? t.bgg : t.bg);
+        continue;
+      }
+      if (k == 0) {
+        wall0 = true;
+        continue;
+      }
+      double val;
+      if (k == p.k1) {
+        val = 2. * vk - vkm;
+      } else {
+        val = reinit_val(p, stage, t.phi0, t.phis, t.orig, dtau, i, j, k);
+        if (k == 1) v1 = val;
+        if (k == 2) v2 = val;
+        if (k == p.kmax - 1) vkm = val;
+        if (k == p.kmax) vk = val;
+      }
+      if (stage == 3) r = fmax(r, fabs(val - t.phi0[idxL(p, i, j, k)]));
+      putL(p, t.out, i, j, k, val);
+      if (k == 2 && wall0) {
+        const double v0 = 2. * v1 - v2;
+        if (stage == 3) r = fmax(r, fabs(v0 - t.phi0[idxL(p, i, j, 0)]));
+        putL(p, t.out, i, j, 0, v0);
+      }
     }
-    out[n] = val;
   }
   if (stage == 3) {
-    double bm = block_max<double, BX * BY>(r);
-    if (flat_tid() == 0) atomic_max_nonneg(&dsc->residual, bm);
+    const double bm = block_max<double, NT>(r);
+    if (flat_tid() == 0) atomic_max_nonneg(&rs[t.l].residual, bm);
   }
 }
 
-__global__ void k_reinit_reset(DevScalars* dsc, int maxiter) {
-  dsc->reinit_done = 0;
-  dsc->reinit_iters = maxiter;
-  dsc->residual = 0.;
+__global__ void k_reinit_reset(const __grid_constant__ LsBatch B, int maxiter, ReinitState* __restrict__ rs) {
+  for (int q = threadIdx.x; q < B.n; q += blockDim.x) {
+    ReinitState& s = rs[B.t[q].l];
+    s.residual = 0.;
+    s.last = 0.;
+    s.done = 0;
+    s.iters = maxiter;
+  }
 }
-// far: |change| of the far-field cells outside the box (0 when none)
-__global__ void k_reinit_check(DevScalars* dsc, int it, int maxiter, double thr, double far) {
-  if (dsc->reinit_done) return;
-  if (far > dsc->residual) dsc->residual = far;
-  if (dsc->residual < thr) {
-    dsc->reinit_done = 1;
-    dsc->reinit_iters = it;
-  } else {
-    dsc->reinit_iters = maxiter;
+// end of iteration `it`: far is the change of the far-field cells outside
+// the drop's region (0 when none); the last drop's state is also published
+// as the scalars of the last ls_reinit call
+__global__ void k_reinit_check(const __grid_constant__ LsBatch B, int it, int maxiter, double thr,
+                               ReinitState* __restrict__ rs, DevScalars* __restrict__ dsc, int last_drop) {
+  for (int q = threadIdx.x; q < B.n; q += blockDim.x) {
+    const int l = B.t[q].l;
+    ReinitState& s = rs[l];
+    if (!s.done) {
+      double r = s.residual;
+      if (B.t[q].far > r) r = B.t[q].far;
+      s.last = r;
+      s.residual = 0.;
+      if (r < thr) {
+        s.done = 1;
+        s.iters = it;
+      } else {
+        s.iters = maxiter;
+      }
+    }
+    if (l == last_drop) {
+      dsc->residual = s.last;
+      dsc->reinit_iters = s.iters;
+      dsc->reinit_done = s.done;
+    }
   }
 }
 
@@ -364,39 +420,62 @@ __device__ __forceinline__ double dirac_trig(const Params& p, double phi, double
   return 0.;
 }
 
-// jiemian = min(jiemian, H_l) over the region r (shape C coordinates),
-// partial sums of H_l over its interior cells (misc.f90:110-141).  Fixed
-// grid: deterministic partials.
-__global__ void __launch_bounds__(kRedThreads) k_heaviside_drop(Params p, Box3 r, const double* __restrict__ phi,
-                                                                int first, double* __restrict__ jiemian,
-                                                                double* __restrict__ partial) {
-  const double eps = 1.5 * p.dz;
-  const int n = (r.c1[0] - r.c0[0] + 1) * (r.c1[1] - r.c0[1] + 1) * (r.c1[2] - r.c0[2] + 1);
-  double s = 0.;
-  for (int q = blockIdx.x * kRedThreads + threadIdx.x; q < n; q += gridDim.x * kRedThreads) {
-    int i, j, k;
-    decode_box(r.c0, r.c1, q, i, j, k);
-    const double H = heav_trig(p, phi[idxL(p, i, j, k)], eps);
-    const long long c = idxC(p, i, j, k);
-    jiemian[c] = first ? H : fmin(jiemian[c], H);
-    if (interior(p, i, j, k)) s += H;
+// jiemian = min(jiemian, H_l) over the tasks' computed cells (shape-C
+// regions) and per-tile sums of H_l over their interior cells
+// (misc.f90:110-141).  jiemian starts at 1, the far-field value of H, so
+// only cells with H < 1 are touched; min is order-free, so drops may share
+// cells.  One chunk per tile: part[l*cap + tile] is deterministic.
+__device__ __forceinline__ void min_into(double* a, double v) {
+  unsigned long long* q = reinterpret_cast<unsigned long long*>(a);
+  unsigned long long old = *q;
+  while (v < __longlong_as_double((long long)old)) {
+    const unsigned long long prev = atomicCAS(q, old, (unsigned long long)__double_as_longlong(v));
+    if (prev == old) break;
+    old = prev;
   }
-  double bs = block_sum<double, kRedThreads>(s);
-  if (threadIdx.x == 0) partial[blockIdx.x] = bs;
+}
+__global__ void __launch_bounds__(NT) k_heaviside(Params p, const __grid_constant__ LsBatch B,
+                                                  double* __restrict__ jiemian, double* __restrict__ part, int cap) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  const double eps = 1.5 * p.dz;
+  double s = 0.;
+  if (c.ok && c.cxy) {
+    const int i = c.i, j = c.j;
+    const int ii = image_of<1>(i, p.imax), jj = image_of<1>(j, p.jmax);
+    const int ka = max(c.ka, t.r.cz0), kb = min(c.kb, t.r.cz1);
+    for (int k = ka; k <= kb; ++k) {
+      const double H = heav_trig(p, t.phi0[idxL(p, i, j, k)], eps);
+      if (H < 1.) {
+        min_into(jiemian + idxC(p, i, j, k), H);
+        if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, j, k), H);
+        if (jj != INT_MIN) {
+          min_into(jiemian + idxC(p, i, jj, k), H);
+          if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, jj, k), H);
+        }
+      }
+      if (k >= 1 && k <= p.kmax) s += H;
+    }
+  }
+  const double bs = block_sum<double, NT>(s);
+  if (flat_tid() == 0) part[(long long)t.l * cap + c.tile] = bs;
 }
 
-// volume(l) and rho_avr from the partial sums (misc.f90:139-173); outside[l]
-// interior cells of drop l lie in its far field, where H = 1
+// volume(l) and rho_avr from the per-tile sums (misc.f90:139-173);
+// outside[l] interior cells of drop l lie in its far field, where H = 1
 struct PerDrop {
   double v[kMaxDropsParam];
+  int n[kMaxDropsParam];
 };
-__global__ void k_volumes(Params p, const double* __restrict__ partials, int nblk, PerDrop outside,
+__global__ void k_volumes(Params p, const double* __restrict__ part, int cap, PerDrop pd, int uniform,
                           double* __restrict__ vol, DevScalars* __restrict__ dsc) {
   const double N = (1. * p.imax * p.jmax) * p.kmax;
   for (int l = threadIdx.x; l < p.L; l += blockDim.x) {
+    const int nb = uniform ? cap : pd.n[l];
     double s = 0.;
-    for (int b = 0; b < nblk; ++b) s += partials[(long long)l * nblk + b];
-    s += outside.v[l];
+    for (int b = 0; b < nb; ++b) s += part[(long long)l * cap + b];
+    if (!uniform) s += pd.v[l];
     vol[l] = 1. - s / N;
   }
   __syncthreads();
@@ -442,43 +521,42 @@ __global__ void __launch_bounds__(NT) k_materials_final(Params p, const double* 
 }
 
 // ------------------------------------------------------------ inflation
-// dheav with boundp semantics over the region r (shape C), the far-field
-// value 1 on its apron, and the area/volume partial sums over the interior
-// computed cells (levelset.f90:493-507, 525)
-__global__ void __launch_bounds__(kRedThreads) k_inflate_sums(Params p, Box3 r, const double* __restrict__ phi,
-                                                              const double* __restrict__ kappa,
-                                                              const double* __restrict__ nrm_m,
-                                                              double* __restrict__ dheav,
-                                                              double* __restrict__ part_area,
-                                                              double* __restrict__ part_heav) {
+// dheav with boundp semantics over the task's shape-C region (one task),
+// the far-field value 1 on its apron, and per-tile area/volume sums over
+// its interior computed cells (levelset.f90:493-507, 525)
+__global__ void __launch_bounds__(NT) k_inflate_sums(Params p, const __grid_constant__ LsBatch B,
+                                                     const double* __restrict__ kappa,
+                                                     const double* __restrict__ nrm_m, double* __restrict__ dheav,
+                                                     double* __restrict__ part_area, double* __restrict__ part_heav) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
   const double s1 = 1.5 * p.dz;
-  const int n = (r.w1[0] - r.w0[0] + 1) * (r.w1[1] - r.w0[1] + 1) * (r.w1[2] - r.w0[2] + 1);
   double sa = 0., sh = 0.;
-  for (int q = blockIdx.x * kRedThreads + threadIdx.x; q < n; q += gridDim.x * kRedThreads) {
-    int i, j, k;
-    decode_box(r.w0, r.w1, q, i, j, k);
-    const long long c = idxC(p, i, j, k);
-    if (!in_compute(r, i, j, k)) {
-      dheav[c] = 1.;
-      continue;
-    }
-    const int I = wrapx(p, i), J = wrapy(p, j);
-    const int K = k == 0 ? 1 : (k == p.k1 ? p.kmax : k);
-    dheav[c] = heav_trig(p, phi[idxL(p, I, J, K)], s1);
-    if (interior(p, i, j, k)) {
-      const double ph = phi[idxL(p, i, j, k)];
-      const double H = heav_trig(p, ph, s1);
-      const double del = dirac_trig(p, ph, s1);
-      const double m = nrm_m[idxI(p, i, j, k)];
-      sa += p.ispeed_curv ? (del * kappa[c]) * m : del * m;
-      sh += H;
+  if (c.ok) {
+    const int i = c.i, j = c.j;
+    for (int k = c.ka; k <= c.kb; ++k) {
+      if (!computed(c, t.r, k)) {
+        putC(p, dheav, i, j, k, 1.);
+        continue;
+      }
+      const int K = k == 0 ? 1 : (k == p.k1 ? p.kmax : k);
+      putC(p, dheav, i, j, k, heav_trig(p, t.phi0[idxL(p, i, j, K)], s1));
+      if (k >= 1 && k <= p.kmax) {
+        const double ph = t.phi0[idxL(p, i, j, k)];
+        const double H = heav_trig(p, ph, s1);
+        const double del = dirac_trig(p, ph, s1);
+        const double m = nrm_m[idxI(p, i, j, k)];
+        sa += p.ispeed_curv ? (del * kappa[idxC(p, i, j, k)]) * m : del * m;
+        sh += H;
+      }
     }
   }
-  double ba = block_sum<double, kRedThreads>(sa);
-  double bh = block_sum<double, kRedThreads>(sh);
-  if (threadIdx.x == 0) {
-    part_area[blockIdx.x] = ba;
-    part_heav[blockIdx.x] = bh;
+  const double ba = block_sum<double, NT>(sa);
+  const double bh = block_sum<double, NT>(sh);
+  if (flat_tid() == 0) {
+    part_area[c.tile] = ba;
+    part_heav[c.tile] = bh;
   }
 }
 
@@ -512,28 +590,33 @@ __device__ __forceinline__ double infl_face(const Params& p, const double* __res
   if (axis == 1) return -divy(p, temp * (dheav[n + p.nCx] - dheav[n]));
   return -divz(p, temp * (dheav[n + (long long)p.nCx * p.nCy] - dheav[n]));
 }
-__global__ void __launch_bounds__(NT) k_inflate_vel(Params p, Box3 r, const double* __restrict__ dheav,
+__global__ void __launch_bounds__(NT) k_inflate_vel(Params p, const __grid_constant__ LsBatch B,
+                                                    const double* __restrict__ dheav,
                                                     const double* __restrict__ kappa,
                                                     const DevScalars* __restrict__ dsc,
                                                     double* __restrict__ ulc, double* __restrict__ vlc,
                                                     double* __restrict__ wlc) {
-  int i, j, k;
-  if (!cell3(r.c0, r.c1, i, j, k)) return;
-  if (!interior(p, i, j, k)) return;
-  const long long q = idxI(p, i, j, k);
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  if (!c.ok || !c.cxy) return;
+  const int i = c.i, j = c.j;
   const double temp = dsc->inflate_temp;
-  const double ul_m = infl_face(p, dheav, temp, 0, wrapx(p, i - 1), j, k);
-  const double ul_0 = infl_face(p, dheav, temp, 0, i, j, k);
-  const double vl_m = infl_face(p, dheav, temp, 1, i, wrapy(p, j - 1), k);
-  const double vl_0 = infl_face(p, dheav, temp, 1, i, j, k);
-  const double wl_m = (k == 1) ? 0. : infl_face(p, dheav, temp, 2, i, j, k - 1);
-  const double wl_0 = (k == p.kmax) ? 0. : infl_face(p, dheav, temp, 2, i, j, k);
-  double a = (ul_m + ul_0) / 2., b = (vl_m + vl_0) / 2., c = (wl_m + wl_0) / 2.;
-  if (p.ispeed_curv) {
-    const double kp = kappa[idxC(p, i, j, k)];
-    a = a * kp; b = b * kp; c = c * kp;
+  for (int k = max(c.ka, max(t.r.cz0, 1)); k <= min(c.kb, min(t.r.cz1, p.kmax)); ++k) {
+    const long long q = idxI(p, i, j, k);
+    const double ul_m = infl_face(p, dheav, temp, 0, wrapx(p, i - 1), j, k);
+    const double ul_0 = infl_face(p, dheav, temp, 0, i, j, k);
+    const double vl_m = infl_face(p, dheav, temp, 1, i, wrapy(p, j - 1), k);
+    const double vl_0 = infl_face(p, dheav, temp, 1, i, j, k);
+    const double wl_m = (k == 1) ? 0. : infl_face(p, dheav, temp, 2, i, j, k - 1);
+    const double wl_0 = (k == p.kmax) ? 0. : infl_face(p, dheav, temp, 2, i, j, k);
+    double a = (ul_m + ul_0) / 2., b = (vl_m + vl_0) / 2., cc = (wl_m + wl_0) / 2.;
+    if (p.ispeed_curv) {
+      const double kp = kappa[idxC(p, i, j, k)];
+      a = a * kp; b = b * kp; cc = cc * kp;
+    }
+    ulc[q] = a; vlc[q] = b; wlc[q] = cc;
   }
-  ulc[q] = a; vlc[q] = b; wlc[q] = c;
 }
 
 // boundmls, extrap='line' (bound.f90:518-~657): three wall layers by
@@ -564,21 +647,19 @@ __global__ void __launch_bounds__(NT) k_boundmls(Params p, double* __restrict__ 
   }
 }
 
-// far-field value into every cell outside the write region of b (makes a
+// far-field value into every cell outside the written cells of r (makes a
 // drop's stored array valid everywhere, e.g. before a download)
-__global__ void __launch_bounds__(NT) k_materialize(Params p, Box3 b, double bg, double bgg, double* __restrict__ y) {
+__global__ void __launch_bounds__(NT) k_materialize(Params p, Region r, double bg, double bgg, double* __restrict__ y) {
   const int r0[3] = {-2, -2, -2}, r1[3] = {p.i1 + 2, p.j1 + 2, p.k1 + 2};
   int i, j, k;
   if (!cell3(r0, r1, i, j, k)) return;
-  if (!in_write(b, i, j, k)) y[idxL(p, i, j, k)] = (k < 0 || k > p.k1) ? bgg : bg;
+  if (!in_written(p, r, i, j, k)) y[idxL(p, i, j, k)] = (k < 0 || k > p.k1) ? bgg : bg;
 }
 
 __global__ void k_copy(double* __restrict__ dst, const double* __restrict__ src, long long n) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
     dst[q] = src[q];
 }
-
-const dim3 kBlock(BX, BY, 1);
 
 }  // namespace
 
@@ -587,74 +668,116 @@ dim3 grid_of(const int* r0, const int* r1) {
   return dim3((unsigned)((nx + BX - 1) / BX), (unsigned)((ny + BY - 1) / BY), (unsigned)nz);
 }
 
-Box3 full_box(const Params& P) {
-  Box3 b;
-  const int n[3] = {P.imax, P.jmax, P.kmax};
-  for (int a = 0; a < 3; ++a) {
-    b.c0[a] = b.w0[a] = -2;
-    b.c1[a] = b.w1[a] = n[a] + 3;
-  }
-  return b;
+namespace {
+int wrap1(int v, int n) {
+  v = (v - 1) % n;
+  if (v < 0) v += n;
+  return v + 1;
 }
+}  // namespace
 
-// the shape-C part of a level-set box, apron of width `ap` on partial axes
-Box3 c_region(const Params& P, const Box3& b, int ap) {
-  const int n[3] = {P.imax, P.jmax, P.kmax};
-  Box3 r;
-  for (int a = 0; a < 3; ++a) {
-    const bool full = (b.c0[a] <= -2 && b.c1[a] >= n[a] + 3);
-    if (full) {
-      r.c0[a] = r.w0[a] = 0;
-      r.c1[a] = r.w1[a] = n[a] + 1;
-    } else {
-      r.c0[a] = b.c0[a];
-      r.c1[a] = b.c1[a];
-      r.w0[a] = std::max(0, b.c0[a] - ap);
-      r.w1[a] = std::min(n[a] + 1, b.c1[a] + ap);
-    }
-  }
+Region full_region(const Params& P) {
+  Region r;
+  r.xa = 1; r.xn = P.imax; r.cx0 = 0; r.cx1 = P.imax - 1;
+  r.ya = 1; r.yn = P.jmax; r.cy0 = 0; r.cy1 = P.jmax - 1;
+  r.z0 = r.cz0 = -2;
+  r.z1 = r.cz1 = P.k1 + 2;
   return r;
 }
 
-// ================================================================ launchers
-void launch_tube(Ctx& c, const Box3& b, const Box3& vin, double bgin, double bgg, const double* in, double* out,
-                 long long* cnt, int* bbox) {
-  Scope sc_(c.prof, c.s, "tube", 1);
-  k_tube<<<grid_of(b.w0, b.w1), kBlock, 0, c.s>>>(c.P, b, vin, bgin, bgg, in, out, c.mask, cnt, bbox);
+bool region_full(const Params& P, const Region& r) {
+  return r.xn == P.imax && r.cx0 == 0 && r.cx1 == P.imax - 1 && r.yn == P.jmax && r.cy0 == 0 &&
+         r.cy1 == P.jmax - 1 && r.cz0 <= -2 && r.cz1 >= P.k1 + 2;
 }
 
-void launch_adv_stage(Ctx& c, const Box3& b, double bg_out, double bgg_out, int scheme, int stage1,
-                      const double* phi0, const double* phis, double a, double bb, double fdt, const double* vu,
-                      const double* vv, const double* vw, double* out) {
+// the shape-C region of a level-set region: the same computed columns with
+// an apron of `ap` columns; full z becomes rows 0..k1
+Region c_region(const Params& P, const Region& r, int ap) {
+  Region q;
+  auto axis = [&](int xa, int xn, int c0, int c1, int n, int& qa, int& qn, int& q0, int& q1) {
+    if (xn == n && c0 == 0 && c1 == n - 1) {
+      qa = 1; qn = n; q0 = 0; q1 = n - 1;
+      return;
+    }
+    const int a = wrap1(xa + c0, n), len = c1 - c0 + 1;
+    qa = wrap1(a - ap, n);
+    qn = len + 2 * ap;
+    q0 = ap;
+    q1 = ap + len - 1;
+  };
+  axis(r.xa, r.xn, r.cx0, r.cx1, P.imax, q.xa, q.xn, q.cx0, q.cx1);
+  axis(r.ya, r.yn, r.cy0, r.cy1, P.jmax, q.ya, q.yn, q.cy0, q.cy1);
+  if (r.cz0 <= -2 && r.cz1 >= P.k1 + 2) {
+    q.z0 = q.cz0 = 0;
+    q.z1 = q.cz1 = P.k1;
+  } else {
+    q.cz0 = r.cz0;
+    q.cz1 = r.cz1;
+    q.z0 = std::max(0, r.cz0 - ap);
+    q.z1 = std::min(P.k1, r.cz1 + ap);
+  }
+  return q;
+}
+
+// tiles, z chunks (kc rows each, the last one longer; kc <= 0: one chunk)
+// and block offsets of a batch
+void set_tiles(LsBatch& b, int kc) {
+  int s = 0;
+  for (int q = 0; q < b.n; ++q) {
+    LsTask& t = b.t[q];
+    t.tx = (t.r.xn + TBX - 1) / TBX;
+    t.ty = (t.r.yn + TBY - 1) / TBY;
+    const int nz = t.r.z1 - t.r.z0 + 1;
+    if (kc <= 0 || kc >= nz) {
+      t.nch = 1;
+      t.kc = nz;
+    } else {
+      t.nch = nz / kc;
+      t.kc = kc;
+    }
+    b.start[q] = s;
+    s += t.tx * t.ty * t.nch;
+  }
+  b.start[b.n] = s;
+}
+
+// ================================================================ launchers
+void launch_tube(Ctx& c, const LsBatch& b) {
+  if (b.n == 0) return;
+  Scope sc_(c.prof, c.s, "tube", 1);
+  k_tube<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.d_nbcnt, c.d_bbox, c.d_bbox + 5 * c.P.L);
+}
+
+void launch_adv_stage(Ctx& c, const LsBatch& b, int scheme, int stage1, double a, double bb, double fdt,
+                      const double* vu, const double* vv, const double* vw) {
+  if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "adv_stage", 1);
   if (scheme == ICLS_HOUC5)
-    k_adv_stage<ICLS_HOUC5><<<grid_of(b.w0, b.w1), kBlock, 0, c.s>>>(c.P, b, bg_out, bgg_out, stage1, phi0, phis,
-                                                                     a, bb, fdt, vu, vv, vw, c.mask, out);
+    k_adv_stage<ICLS_HOUC5><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, vu, vv, vw);
   else
-    k_adv_stage<ICLS_WENO5><<<grid_of(b.w0, b.w1), kBlock, 0, c.s>>>(c.P, b, bg_out, bgg_out, stage1, phi0, phis,
-                                                                     a, bb, fdt, vu, vv, vw, c.mask, out);
+    k_adv_stage<ICLS_WENO5><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, vu, vv, vw);
 }
 
-void launch_reinit_stage(Ctx& c, const Box3& b, double bg_out, double bgg_out, int stage, const double* phi0,
-                         const double* phis, const double* orig, double dtau, double* out) {
+void launch_reinit_stage(Ctx& c, const LsBatch& b, int stage, double dtau) {
+  if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "reinit_stage", 1);
-  k_reinit_stage<<<grid_of(b.w0, b.w1), kBlock, 0, c.s>>>(c.P, b, bg_out, bgg_out, stage, phi0, phis, orig, dtau,
-                                                          out, c.dsc);
+  k_reinit_stage<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs);
 }
-void launch_reinit_check(Ctx& c, int it, int maxiter, double thr, double far) {
-  Scope sc_(c.prof, c.s, "reinit_check", 1);
-  k_reinit_check<<<1, 1, 0, c.s>>>(c.dsc, it, maxiter, thr, far);
-}
-void launch_reinit_reset(Ctx& c, int maxiter) {
+void launch_reinit_reset(Ctx& c, const LsBatch& b, int maxiter) {
+  if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "reinit_reset", 1);
-  k_reinit_reset<<<1, 1, 0, c.s>>>(c.dsc, maxiter);
+  k_reinit_reset<<<1, 64, 0, c.s>>>(b, maxiter, c.drs);
+}
+void launch_reinit_check(Ctx& c, const LsBatch& b, int it, int maxiter, double thr) {
+  if (b.n == 0) return;
+  Scope sc_(c.prof, c.s, "reinit_check", 1);
+  k_reinit_check<<<1, 64, 0, c.s>>>(b, it, maxiter, thr, c.drs, c.dsc, c.P.L - 1);
 }
 
-void launch_heaviside_drop(Ctx& c, const Box3& b, const double* phi, int l, int first) {
-  Scope sc_(c.prof, c.s, "heaviside_drop", 1);
-  const Box3 r = c_region(c.P, b, 0);
-  k_heaviside_drop<<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, r, phi, first, c.jiemian,
-                                                        c.partials + (long long)l * kRedBlocks);
+void launch_heaviside(Ctx& c, const LsBatch& b) {
+  if (b.n == 0) return;
+  Scope sc_(c.prof, c.s, "heaviside", 1);
+  k_heaviside<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.jiemian, c.hpart, c.red_cap);
 }
 
 void launch_fill(Ctx& c, double* a, long long n, double v) {
@@ -662,29 +785,34 @@ void launch_fill(Ctx& c, double* a, long long n, double v) {
   k_fill<<<1184, NT, 0, c.s>>>(a, n, v);
 }
 
-void launch_materials_final(Ctx& c, const double* outside) {
+// outside/ntiles: per drop (null: every drop swept its whole grid)
+void launch_materials_final(Ctx& c, const double* outside, const int* ntiles) {
   Scope sc_(c.prof, c.s, "materials_final", 2);
   PerDrop o;
-  for (int l = 0; l < kMaxDropsParam; ++l) o.v[l] = (l < c.P.L) ? outside[l] : 0.;
-  k_volumes<<<1, 256, 0, c.s>>>(c.P, c.partials, kRedBlocks, o, c.dvol, c.dsc);
+  const int uniform = (outside == nullptr || c.P.L > kMaxDropsParam) ? 1 : 0;
+  for (int l = 0; l < kMaxDropsParam; ++l) {
+    o.v[l] = (!uniform && l < c.P.L) ? outside[l] : 0.;
+    o.n[l] = (!uniform && l < c.P.L) ? ntiles[l] : 0;
+  }
+  k_volumes<<<1, 256, 0, c.s>>>(c.P, c.hpart, c.red_cap, o, uniform, c.dvol, c.dsc);
   const int r0[3] = {0, 0, 0}, r1[3] = {c.P.i1, c.P.j1, c.P.k1};
   k_materials_final<<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, c.jiemian, c.miu, c.rho, c.rho_u, c.rho_v, c.rho_w);
 }
 
-void launch_inflate_sums(Ctx& c, const Box3& b, const double* phi, int l, double outside) {
+// b: one task (shape-C region of the drop, apron 1), phi0 = its level set
+void launch_inflate_sums(Ctx& c, const LsBatch& b, double outside) {
   Scope sc_(c.prof, c.s, "inflate_sums", 2);
-  double* pa = c.partials;
-  double* ph = c.partials + kRedBlocks;
-  const Box3 r = c_region(c.P, b, 1);
-  k_inflate_sums<<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, r, phi, c.kappa, c.nrm_m, c.dheav, pa, ph);
-  k_inflate_final<<<1, 32, 0, c.s>>>(c.P, pa, ph, kRedBlocks, l, (double)c.cfg.inflate_step * c.dt, outside,
+  double* pa = c.hpart;
+  double* ph = c.hpart + c.red_cap;
+  k_inflate_sums<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.kappa, c.nrm_m, c.dheav, pa, ph);
+  k_inflate_final<<<1, 32, 0, c.s>>>(c.P, pa, ph, b.start[b.n], b.t[0].l, (double)c.cfg.inflate_step * c.dt, outside,
                                      c.dvol, c.dvol0, c.dmaxchk, c.dsc);
 }
 
-void launch_inflate_vel(Ctx& c, const Box3& b) {
+// b: one task (shape-C region of the drop, apron 0)
+void launch_inflate_vel(Ctx& c, const LsBatch& b) {
   Scope sc_(c.prof, c.s, "inflate_vel", 1);
-  const Box3 r = c_region(c.P, b, 0);
-  k_inflate_vel<<<grid_of(r.c0, r.c1), kBlock, 0, c.s>>>(c.P, r, c.dheav, c.kappa, c.dsc, c.ulc, c.vlc, c.wlc);
+  k_inflate_vel<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.dheav, c.kappa, c.dsc, c.ulc, c.vlc, c.wlc);
 }
 
 void launch_boundmls(Ctx& c, double* phi) {
@@ -693,10 +821,10 @@ void launch_boundmls(Ctx& c, double* phi) {
   k_boundmls<<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, phi);
 }
 
-void launch_materialize(Ctx& c, const Box3& b, double bg, double bgg, double* phi) {
+void launch_materialize(Ctx& c, const Region& r, double bg, double bgg, double* phi) {
   Scope sc_(c.prof, c.s, "materialize", 1);
   const int r0[3] = {-2, -2, -2}, r1[3] = {c.P.i1 + 2, c.P.j1 + 2, c.P.k1 + 2};
-  k_materialize<<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, b, bg, bgg, phi);
+  k_materialize<<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, r, bg, bgg, phi);
 }
 
 void launch_copy(Ctx& c, double* dst, const double* src, long long n) {

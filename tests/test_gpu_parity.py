@@ -334,6 +334,29 @@ def test_sweep_boxes_bit_identical_to_full_sweep(monkeypatch):
     assert np.allclose(full.volumes()[0], boxed.volumes()[0], rtol=1e-11, atol=0)
 
 
+def test_drop_groups_bit_identical(monkeypatch):
+    """Drops processed one at a time (a group of one) give exactly the
+    fields of all drops in one group."""
+    wl = boxed_case(steps=8)
+    cfg = wl.cfg
+    ls = init_drops(cfg, wl.centres, wl.radii, wl.all_images)
+    u, v, w = initial_velocity(cfg, wl.shear_v)
+    monkeypatch.setenv("ICLS_GROUP", "1")
+    one = Solver(cfg)
+    monkeypatch.delenv("ICLS_GROUP")
+    all_ = Solver(cfg)
+    for s in (one, all_):
+        s.setup(ls, u, v, w)
+    for istep in range(1, 9):
+        one.step(istep, 0)
+        all_.step(istep, 0)
+    for l in range(1, cfg.lmax + 1):
+        assert np.array_equal(one.download("lvset", l), all_.download("lvset", l)), l
+    for name in ("u", "v", "w", "pnew", "miu", "p_jump", "curv", "normal_m"):
+        assert np.array_equal(one.download(name), all_.download(name)), name
+    assert np.array_equal(one.volumes()[0], all_.volumes()[0])
+
+
 def test_boxed_multidrop_128_parity():
     """Four drops on 128^3 (partial sweep boxes) against the oracle."""
     wl = boxed_case(steps=10)
