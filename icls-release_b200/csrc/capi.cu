@@ -73,6 +73,7 @@ void fill_params(Ctx& c) {
   P.dt = f.timestep;
   P.rho1 = f.rho1; P.rho2 = f.rho2; P.miu1 = f.miu1; P.miu2 = f.miu2;
   P.rho0 = std::min(f.rho1, f.rho2);  // param.f90:63
+  P.rrho0 = 1. / P.rho0;
   P.visc = 1. / f.Re;                 // param.f90:73
   P.iFr = f.iFr;
   P.nondi = 1. / f.We;                // gfm.f90:40

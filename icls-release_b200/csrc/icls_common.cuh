@@ -31,6 +31,7 @@ struct Params {
   double pi;
   double dt;
   double rho1, rho2, miu1, miu2, rho0, visc, iFr, nondi;
+  double rrho0;              // 1./rho0, the IEEE quotient the reference evaluates per cell
   double g1, g2, g3;
   double v_lower, v_upper;
   double forceytot;

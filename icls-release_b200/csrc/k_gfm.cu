@@ -29,23 +29,24 @@ __device__ __forceinline__ double curvature_at(const Params& p, const double* __
   const long long c = idxL(p, i, j, k);
   m = 1.;
   if (!(fabs(phi[c]) <= p.NB - 1. * p.dz)) return 0.;
-  double s27[27];
+  // x[r] = sum over the 27 stencil values in order q = 0..26 of P(r,q)*phi_q,
+  // accumulated while the stencil is read
+  double x[10];
+#pragma unroll
+  for (int r = 1; r < 10; ++r) x[r] = 0.;
   int n = 0;
   const long long sy = p.nLx, sz = (long long)p.nLx * p.nLy;
-#pragma unroll
+#pragma unroll 1
   for (int dk = -1; dk <= 1; ++dk)
 #pragma unroll
     for (int dj = -1; dj <= 1; ++dj)
 #pragma unroll
-      for (int di = -1; di <= 1; ++di) s27[n++] = phi[c + di + dj * sy + dk * sz];
-  double x[10];
+      for (int di = -1; di <= 1; ++di) {
+        const double v = phi[c + di + dj * sy + dk * sz];
 #pragma unroll
-  for (int r = 1; r < 10; ++r) {
-    double s = 0.;
-#pragma unroll
-    for (int q = 0; q < 27; ++q) s = s + cP[r * 27 + q] * s27[q];
-    x[r] = s;
-  }
+        for (int r = 1; r < 10; ++r) x[r] = x[r] + cP[r * 27 + n] * v;
+        ++n;
+      }
   const double dphidx = x[1], dphidy = x[2], dphidz = x[3];
   const double d2phidx = x[4], d2phidy = x[5], d2phidz = x[6];
   const double d2phidxdy = x[7], d2phidxdz = x[8], d2phidydz = x[9];

@@ -321,7 +321,7 @@ __device__ __forceinline__ double reinit_val(const Params& p, int stage, const d
 
 // One SSP-RK3 stage of ls_reinit over the tasks' regions; stage 3 folds
 // max|phi_new - phi_0| into the drop's residual.  out may equal phi0.
-__global__ void __launch_bounds__(NT) k_reinit_stage(Params p, const __grid_constant__ LsBatch B, int stage,
+__global__ void __launch_bounds__(NT, 2) k_reinit_stage(Params p, const __grid_constant__ LsBatch B, int stage,
                                                      double dtau, ReinitState* __restrict__ rs) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];

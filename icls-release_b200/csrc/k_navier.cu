@@ -13,7 +13,9 @@
 // Boundary rows and periodic halos are produced in the kernel that computes
 // the field: a halo or wall cell evaluates the interior value(s) it copies
 // or extrapolates from (bound.f90:36-75), so no separate boundary pass runs.
-#include "ctx.h"
+#include <algorithm>
+
+#include "batch.cuh"
 
 namespace icls {
 
@@ -51,192 +53,213 @@ struct MomArgs {
   const double* rho_avr;
 };
 
-// ---- RHS of mom_main for one component at interior (i,j,k) -------------
-__device__ __forceinline__ double rhs_u(const Params& p, const MomArgs& a, int i, int j, int k, double rho_avr) {
-  const double *u = a.u, *v = a.v, *w = a.w, *miu = a.miu;
-  const long long c = idxC(p, i, j, k);
-  const long long sx = 1, sy = p.nCx, sz = (long long)p.nCx * p.nCy;
+// ---- RHS of mom_main for one component ----------------------------------
+// U(di,dj,dk) returns u at (i+di, j+dj, k+dk), likewise V, W and M (miu):
+// the same expressions serve the shared-memory march of k_ab2 and the
+// global-memory k_mom_main.
+template <class FU, class FV, class FW, class FM>
+__device__ __forceinline__ double rhs_u(const Params& p, const FU& U, const FV& V, const FW& W, const FM& M,
+                                        double rho_u, double rho_avr) {
   double RCu = 0.;
   if (!p.TwoD) {
-    double uuip = 0.25 * (u[c + sx] + u[c]) * (u[c + sx] + u[c]);
-    double uuim = 0.25 * (u[c - sx] + u[c]) * (u[c - sx] + u[c]);
-    double uvjp = 0.25 * (u[c + sy] + u[c]) * (v[c + sx] + v[c]);
-    double uvjm = 0.25 * (u[c - sy] + u[c]) * (v[c + sx - sy] + v[c - sy]);
-    double uwkp = 0.25 * (u[c + sz] + u[c]) * (w[c + sx] + w[c]);
-    double uwkm = 0.25 * (u[c - sz] + u[c]) * (w[c + sx - sz] + w[c - sz]);
+    double uuip = 0.25 * (U(1, 0, 0) + U(0, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
+    double uuim = 0.25 * (U(-1, 0, 0) + U(0, 0, 0)) * (U(-1, 0, 0) + U(0, 0, 0));
+    double uvjp = 0.25 * (U(0, 1, 0) + U(0, 0, 0)) * (V(1, 0, 0) + V(0, 0, 0));
+    double uvjm = 0.25 * (U(0, -1, 0) + U(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
+    double uwkp = 0.25 * (U(0, 0, 1) + U(0, 0, 0)) * (W(1, 0, 0) + W(0, 0, 0));
+    double uwkm = 0.25 * (U(0, 0, -1) + U(0, 0, 0)) * (W(1, 0, -1) + W(0, 0, -1));
     RCu = (divx(p, (-uuip + uuim)) + divy(p, (-uvjp + uvjm))) + divz(p, (-uwkp + uwkm));
   }
   double RDu = 0.;
   if (!p.TwoD) {
-    double dudxp = divx(p, (u[c + sx] - u[c]));
-    double dudxm = divx(p, (u[c] - u[c - sx]));
-    double dudyp = divy(p, (u[c + sy] - u[c]));
-    double dudym = divy(p, (u[c] - u[c - sy]));
-    double dvdxp = divx(p, (v[c + sx] - v[c]));
-    double dvdxm = divx(p, (v[c + sx - sy] - v[c - sy]));
-    double dudzp = divz(p, (u[c + sz] - u[c]));
-    double dudzm = divz(p, (u[c] - u[c - sz]));
-    double dwdxp = divx(p, (w[c + sx] - w[c]));
-    double dwdxm = divx(p, (w[c + sx - sz] - w[c - sz]));
-    double ma1 = 0.25 * (((miu[c] + miu[c - sy]) + miu[c + sx - sy]) + miu[c + sx]);
-    double ma2 = 0.25 * (((miu[c] + miu[c + sy]) + miu[c + sx + sy]) + miu[c + sx]);
-    double ma3 = 0.25 * (((miu[c] + miu[c - sz]) + miu[c + sx - sz]) + miu[c + sx]);
-    double ma4 = 0.25 * (((miu[c] + miu[c + sz]) + miu[c + sx + sz]) + miu[c + sx]);
-    double RD1 = divx(p, 2. * (dudxp * miu[c + sx] - dudxm * miu[c]));
+    double dudxp = divx(p, (U(1, 0, 0) - U(0, 0, 0)));
+    double dudxm = divx(p, (U(0, 0, 0) - U(-1, 0, 0)));
+    double dudyp = divy(p, (U(0, 1, 0) - U(0, 0, 0)));
+    double dudym = divy(p, (U(0, 0, 0) - U(0, -1, 0)));
+    double dvdxp = divx(p, (V(1, 0, 0) - V(0, 0, 0)));
+    double dvdxm = divx(p, (V(1, -1, 0) - V(0, -1, 0)));
+    double dudzp = divz(p, (U(0, 0, 1) - U(0, 0, 0)));
+    double dudzm = divz(p, (U(0, 0, 0) - U(0, 0, -1)));
+    double dwdxp = divx(p, (W(1, 0, 0) - W(0, 0, 0)));
+    double dwdxm = divx(p, (W(1, 0, -1) - W(0, 0, -1)));
+    double ma1 = 0.25 * (((M(0, 0, 0) + M(0, -1, 0)) + M(1, -1, 0)) + M(1, 0, 0));
+    double ma2 = 0.25 * (((M(0, 0, 0) + M(0, 1, 0)) + M(1, 1, 0)) + M(1, 0, 0));
+    double ma3 = 0.25 * (((M(0, 0, 0) + M(0, 0, -1)) + M(1, 0, -1)) + M(1, 0, 0));
+    double ma4 = 0.25 * (((M(0, 0, 0) + M(0, 0, 1)) + M(1, 0, 1)) + M(1, 0, 0));
+    double RD1 = divx(p, 2. * (dudxp * M(1, 0, 0) - dudxm * M(0, 0, 0)));
     double RD2 = divy(p, (dudyp * ma2 - dudym * ma1));
     double RD3 = divy(p, (dvdxp * ma2 - dvdxm * ma1));
     double RD4 = divz(p, (dudzp * ma4 - dudzm * ma3));
     double RD5 = divz(p, (dwdxp * ma4 - dwdxm * ma3));
-    RDu = ((((RD1 + RD2) + RD3) + RD4) + RD5) / a.rho_u[idxI(p, i, j, k)];
+    RDu = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rho_u;
   }
-  double RGu = p.TwoD ? 0. : p.iFr * (1. - rho_avr / a.rho_u[idxI(p, i, j, k)]) * p.g1;
+  double RGu = p.TwoD ? 0. : p.iFr * (1. - rho_avr / rho_u) * p.g1;
   return (RCu + RDu * p.visc) + RGu;
 }
 
-__device__ __forceinline__ double rhs_v(const Params& p, const MomArgs& a, int i, int j, int k, double rho_avr) {
-  const double *u = a.u, *v = a.v, *w = a.w, *miu = a.miu;
-  const long long c = idxC(p, i, j, k);
-  const long long sx = 1, sy = p.nCx, sz = (long long)p.nCx * p.nCy;
-  double uvip = 0.25 * (u[c] + u[c + sy]) * (v[c] + v[c + sx]);
-  double uvim = 0.25 * (u[c - sx] + u[c - sx + sy]) * (v[c] + v[c - sx]);
-  double vvjp = 0.25 * (v[c] + v[c + sy]) * (v[c] + v[c + sy]);
-  double vvjm = 0.25 * (v[c] + v[c - sy]) * (v[c] + v[c - sy]);
-  double wvkp = 0.25 * (w[c] + w[c + sy]) * (v[c + sz] + v[c]);
-  double wvkm = 0.25 * (w[c - sz] + w[c + sy - sz]) * (v[c - sz] + v[c]);
+template <class FU, class FV, class FW, class FM>
+__device__ __forceinline__ double rhs_v(const Params& p, const FU& U, const FV& V, const FW& W, const FM& M,
+                                        double rv, double rho_avr) {
+  double uvip = 0.25 * (U(0, 0, 0) + U(0, 1, 0)) * (V(0, 0, 0) + V(1, 0, 0));
+  double uvim = 0.25 * (U(-1, 0, 0) + U(-1, 1, 0)) * (V(0, 0, 0) + V(-1, 0, 0));
+  double vvjp = 0.25 * (V(0, 0, 0) + V(0, 1, 0)) * (V(0, 0, 0) + V(0, 1, 0));
+  double vvjm = 0.25 * (V(0, 0, 0) + V(0, -1, 0)) * (V(0, 0, 0) + V(0, -1, 0));
+  double wvkp = 0.25 * (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 1) + V(0, 0, 0));
+  double wvkm = 0.25 * (W(0, 0, -1) + W(0, 1, -1)) * (V(0, 0, -1) + V(0, 0, 0));
   double RCv = (divx(p, (-uvip + uvim)) + divy(p, (-vvjp + vvjm))) + divz(p, (-wvkp + wvkm));
-  double dvdxp = divx(p, (v[c + sx] - v[c]));
-  double dvdxm = divx(p, (v[c] - v[c - sx]));
-  double dudyp = divy(p, (u[c + sy] - u[c]));
-  double dudym = divy(p, (u[c - sx + sy] - u[c - sx]));
-  double dvdyp = divy(p, (v[c + sy] - v[c]));
-  double dvdym = divy(p, (v[c] - v[c - sy]));
-  double dvdzp = divz(p, (v[c + sz] - v[c]));
-  double dvdzm = divz(p, (v[c] - v[c - sz]));
-  double dwdyp = divy(p, (w[c + sy] - w[c]));
-  double dwdym = divy(p, (w[c + sy - sz] - w[c - sz]));
-  double ma2 = 0.25 * (((miu[c] + miu[c + sy]) + miu[c + sx + sy]) + miu[c + sx]);
-  double ma5 = 0.25 * (((miu[c] + miu[c + sy]) + miu[c - sx + sy]) + miu[c - sx]);
-  double ma6 = 0.25 * (((miu[c] + miu[c - sz]) + miu[c + sy - sz]) + miu[c + sy]);
-  double ma7 = 0.25 * (((miu[c] + miu[c + sz]) + miu[c + sy + sz]) + miu[c + sy]);
+  double dvdxp = divx(p, (V(1, 0, 0) - V(0, 0, 0)));
+  double dvdxm = divx(p, (V(0, 0, 0) - V(-1, 0, 0)));
+  double dudyp = divy(p, (U(0, 1, 0) - U(0, 0, 0)));
+  double dudym = divy(p, (U(-1, 1, 0) - U(-1, 0, 0)));
+  double dvdyp = divy(p, (V(0, 1, 0) - V(0, 0, 0)));
+  double dvdym = divy(p, (V(0, 0, 0) - V(0, -1, 0)));
+  double dvdzp = divz(p, (V(0, 0, 1) - V(0, 0, 0)));
+  double dvdzm = divz(p, (V(0, 0, 0) - V(0, 0, -1)));
+  double dwdyp = divy(p, (W(0, 1, 0) - W(0, 0, 0)));
+  double dwdym = divy(p, (W(0, 1, -1) - W(0, 0, -1)));
+  double ma2 = 0.25 * (((M(0, 0, 0) + M(0, 1, 0)) + M(1, 1, 0)) + M(1, 0, 0));
+  double ma5 = 0.25 * (((M(0, 0, 0) + M(0, 1, 0)) + M(-1, 1, 0)) + M(-1, 0, 0));
+  double ma6 = 0.25 * (((M(0, 0, 0) + M(0, 0, -1)) + M(0, 1, -1)) + M(0, 1, 0));
+  double ma7 = 0.25 * (((M(0, 0, 0) + M(0, 0, 1)) + M(0, 1, 1)) + M(0, 1, 0));
   double RD1 = divx(p, (dvdxp * ma2 - dvdxm * ma5));
   double RD2 = divx(p, (dudyp * ma2 - dudym * ma5));
-  double RD3 = divy(p, 2. * (dvdyp * miu[c + sy] - dvdym * miu[c]));
+  double RD3 = divy(p, 2. * (dvdyp * M(0, 1, 0) - dvdym * M(0, 0, 0)));
   double RD4 = divz(p, (dvdzp * ma7 - dvdzm * ma6));
   double RD5 = divz(p, (dwdyp * ma7 - dwdym * ma6));
-  const double rv = a.rho_v[idxI(p, i, j, k)];
   double RDv = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rv;
   double RGv = p.iFr * (1. - rho_avr / rv) * p.g2;
   return (RCv + RDv * p.visc) + RGv;
 }
 
-__device__ __forceinline__ double rhs_w(const Params& p, const MomArgs& a, int i, int j, int k, double rho_avr) {
-  const double *u = a.u, *v = a.v, *w = a.w, *miu = a.miu;
-  const long long c = idxC(p, i, j, k);
-  const long long sx = 1, sy = p.nCx, sz = (long long)p.nCx * p.nCy;
-  double uwip = 0.25 * (w[c] + w[c + sx]) * (u[c] + u[c + sz]);
-  double uwim = 0.25 * (w[c] + w[c - sx]) * (u[c - sx] + u[c - sx + sz]);
-  double vwjp = 0.25 * (w[c] + w[c + sy]) * (v[c] + v[c + sz]);
-  double vwjm = 0.25 * (w[c] + w[c - sy]) * (v[c - sy] + v[c - sy + sz]);
-  double wwkp = 0.25 * (w[c] + w[c + sz]) * (w[c] + w[c + sz]);
-  double wwkm = 0.25 * (w[c] + w[c - sz]) * (w[c] + w[c - sz]);
+template <class FU, class FV, class FW, class FM>
+__device__ __forceinline__ double rhs_w(const Params& p, const FU& U, const FV& V, const FW& W, const FM& M,
+                                        double rw, double rho_avr) {
+  double uwip = 0.25 * (W(0, 0, 0) + W(1, 0, 0)) * (U(0, 0, 0) + U(0, 0, 1));
+  double uwim = 0.25 * (W(0, 0, 0) + W(-1, 0, 0)) * (U(-1, 0, 0) + U(-1, 0, 1));
+  double vwjp = 0.25 * (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 0) + V(0, 0, 1));
+  double vwjm = 0.25 * (W(0, 0, 0) + W(0, -1, 0)) * (V(0, -1, 0) + V(0, -1, 1));
+  double wwkp = 0.25 * (W(0, 0, 0) + W(0, 0, 1)) * (W(0, 0, 0) + W(0, 0, 1));
+  double wwkm = 0.25 * (W(0, 0, 0) + W(0, 0, -1)) * (W(0, 0, 0) + W(0, 0, -1));
   double RCw = (divx(p, (-uwip + uwim)) + divy(p, (-vwjp + vwjm))) + divz(p, (-wwkp + wwkm));
-  double dwdxp = divx(p, (w[c + sx] - w[c]));
-  double dwdxm = divx(p, (w[c] - w[c - sx]));
-  double dudzp = divz(p, (u[c + sz] - u[c]));
-  double dudzm = divz(p, (u[c - sx + sz] - u[c - sx]));
-  double dwdyp = divy(p, (w[c + sy] - w[c]));
-  double dwdym = divy(p, (w[c] - w[c - sy]));
-  double dvdzp = divz(p, (v[c + sz] - v[c]));
-  double dvdzm = divz(p, (v[c - sy + sz] - v[c - sy]));
-  double dwdzp = divz(p, (w[c + sz] - w[c]));
-  double dwdzm = divz(p, (w[c] - w[c - sz]));
-  double ma4 = 0.25 * (((miu[c] + miu[c + sz]) + miu[c + sx + sz]) + miu[c + sx]);
-  double ma8 = 0.25 * (((miu[c] + miu[c + sz]) + miu[c - sx + sz]) + miu[c - sx]);
-  double ma7 = 0.25 * (((miu[c] + miu[c + sz]) + miu[c + sy + sz]) + miu[c + sy]);
-  double ma9 = 0.25 * (((miu[c] + miu[c + sz]) + miu[c - sy + sz]) + miu[c - sy]);
+  double dwdxp = divx(p, (W(1, 0, 0) - W(0, 0, 0)));
+  double dwdxm = divx(p, (W(0, 0, 0) - W(-1, 0, 0)));
+  double dudzp = divz(p, (U(0, 0, 1) - U(0, 0, 0)));
+  double dudzm = divz(p, (U(-1, 0, 1) - U(-1, 0, 0)));
+  double dwdyp = divy(p, (W(0, 1, 0) - W(0, 0, 0)));
+  double dwdym = divy(p, (W(0, 0, 0) - W(0, -1, 0)));
+  double dvdzp = divz(p, (V(0, 0, 1) - V(0, 0, 0)));
+  double dvdzm = divz(p, (V(0, -1, 1) - V(0, -1, 0)));
+  double dwdzp = divz(p, (W(0, 0, 1) - W(0, 0, 0)));
+  double dwdzm = divz(p, (W(0, 0, 0) - W(0, 0, -1)));
+  double ma4 = 0.25 * (((M(0, 0, 0) + M(0, 0, 1)) + M(1, 0, 1)) + M(1, 0, 0));
+  double ma8 = 0.25 * (((M(0, 0, 0) + M(0, 0, 1)) + M(-1, 0, 1)) + M(-1, 0, 0));
+  double ma7 = 0.25 * (((M(0, 0, 0) + M(0, 0, 1)) + M(0, 1, 1)) + M(0, 1, 0));
+  double ma9 = 0.25 * (((M(0, 0, 0) + M(0, 0, 1)) + M(0, -1, 1)) + M(0, -1, 0));
   double RD1 = divx(p, (dwdxp * ma4 - dwdxm * ma8));
   double RD2 = divx(p, (dudzp * ma4 - dudzm * ma8));
   double RD3 = divy(p, (dwdyp * ma7 - dwdym * ma9));
   double RD4 = divy(p, (dvdzp * ma7 - dvdzm * ma9));
-  double RD5 = divz(p, 2. * (dwdzp * miu[c + sz] - dwdzm * miu[c]));
-  const double rw = a.rho_w[idxI(p, i, j, k)];
+  double RD5 = divz(p, 2. * (dwdzp * M(0, 0, 1) - dwdzm * M(0, 0, 0)));
   double RDw = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rw;
   double RGw = p.iFr * (1. - rho_avr / rw) * p.g3;
   return (RCw + RDw * p.visc) + RGw;
 }
 
-// ---- ab2 predictor of one component (ab2.f90:51-61, 79-129) -------------
-// R is the mom_main RHS stored as the next AB2 history.
-__device__ __forceinline__ double ab2_u(const Params& p, const MomArgs& a, int i, int j, int k, double rho_avr,
-                                        double& R) {
-  R = rhs_u(p, a, i, j, k, rho_avr);
-  const long long c = idxC(p, i, j, k), q = idxI(p, i, j, k);
-  double d = a.u[c] + p.dt * (1.5 * R - 0.5 * a.duold[q]);
-  const double ph_p = 2. * a.pnew[c + 1] - a.pold[c + 1];
+// ---- the ab2 update of one component (ab2.f90:51-61, 79-129) -------------
+// u0 = u at the cell, R = its mom_main RHS, rf = its face density; h the
+// offset of the + neighbour along the component's axis, dhi its 1/dx
+__device__ __forceinline__ double ab2_update(const Params& p, const MomArgs& a, long long c, long long h,
+                                             double u0, double R, double rold, double rf, const double* pj,
+                                             const double* pjold, double dhi) {
+  double d = u0 + p.dt * (1.5 * R - 0.5 * rold);
+  const double ph_p = 2. * a.pnew[c + h] - a.pold[c + h];
   const double ph_0 = 2. * a.pnew[c] - a.pold[c];
-  const double pj = 2. * a.px[c] - a.pxold[c];
-  const double dun = -((1. / a.rho_u[q] - 1. / p.rho0) * p.dxi * ((ph_p - pj) - ph_0));
-  return d + p.dt * dun;
-}
-__device__ __forceinline__ double ab2_v(const Params& p, const MomArgs& a, int i, int j, int k, double rho_avr,
-                                        double& R) {
-  R = rhs_v(p, a, i, j, k, rho_avr);
-  const long long c = idxC(p, i, j, k), q = idxI(p, i, j, k);
-  double d = a.v[c] + p.dt * (1.5 * R - 0.5 * a.dvold[q]);
-  const long long sy = p.nCx;
-  const double ph_p = 2. * a.pnew[c + sy] - a.pold[c + sy];
-  const double ph_0 = 2. * a.pnew[c] - a.pold[c];
-  const double pj = 2. * a.py[c] - a.pyold[c];
-  const double dvn = -((1. / a.rho_v[q] - 1. / p.rho0) * p.dyi * ((ph_p - pj) - ph_0));
-  return (d + p.dt * dvn) - p.forceytot * p.dt / a.rho_v[q];
-}
-__device__ __forceinline__ double ab2_w(const Params& p, const MomArgs& a, int i, int j, int k, double rho_avr,
-                                        double& R) {
-  R = rhs_w(p, a, i, j, k, rho_avr);
-  const long long c = idxC(p, i, j, k), q = idxI(p, i, j, k);
-  double d = a.w[c] + p.dt * (1.5 * R - 0.5 * a.dwold[q]);
-  const long long sz = (long long)p.nCx * p.nCy;
-  const double ph_p = 2. * a.pnew[c + sz] - a.pold[c + sz];
-  const double ph_0 = 2. * a.pnew[c] - a.pold[c];
-  const double pj = 2. * a.pz[c] - a.pzold[c];
-  const double dwn = -((1. / a.rho_w[q] - 1. / p.rho0) * p.dzi * ((ph_p - pj) - ph_0));
-  return d + p.dt * dwn;
+  const double pjh = 2. * pj[c] - pjold[c];
+  const double dn = -((1. / rf - p.rrho0) * dhi * ((ph_p - pjh) - ph_0));
+  return d + p.dt * dn;
 }
 
-// ab2 over shape C with bounduvw(dudt,dvdt,dwdt) (bound.f90:36-75) in-kernel
-__global__ void __launch_bounds__(NT) k_ab2(Params p, MomArgs a, double* __restrict__ dudt,
-                                            double* __restrict__ dvdt, double* __restrict__ dwdt,
-                                            double* __restrict__ duold_out, double* __restrict__ dvold_out,
-                                            double* __restrict__ dwold_out) {
-  int i, j, k;
-  if (!cell3(kC0, cC1(p).v, i, j, k)) return;
-  const long long n = idxC(p, i, j, k);
-  const int I = wrapx(p, i), J = wrapy(p, j);
+// ab2 over shape C with bounduvw(dudt,dvdt,dwdt) (bound.f90:36-75) in-kernel.
+// A block is a 32 x 8 column tile marching up a chunk of interior rows;
+// u, v, w and miu pass through a three-plane shared-memory ring (tile plus
+// one halo column each side), the rest is read once per cell.  A thread
+// writes its column's periodic halo images and, at k = 1 and k = kmax,
+// the wall rows k = 0 and k = k1.
+constexpr int MX = 32, MY = 8, MSX = MX + 2, MSY = MY + 2;
+__global__ void __launch_bounds__(MX * MY, 3) k_ab2(Params p, MomArgs a, double* __restrict__ dudt,
+                                                 double* __restrict__ dvdt, double* __restrict__ dwdt,
+                                                 double* __restrict__ duold_out, double* __restrict__ dvold_out,
+                                                 double* __restrict__ dwold_out, int kc, int nch) {
+  __shared__ double sm[4][3][MSY][MSX];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + MX * ty;
+  const int i0 = 1 + MX * (int)blockIdx.x, j0 = 1 + MY * (int)blockIdx.y;
+  const int ch = blockIdx.z;
+  const int ka = 1 + ch * kc, kb = (ch == nch - 1) ? p.kmax : ka + kc - 1;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool ok = i <= p.imax && j <= p.jmax;
+  const double* __restrict__ F0 = a.u;
+  const double* __restrict__ F1 = a.v;
+  const double* __restrict__ F2 = a.w;
+  const double* __restrict__ F3 = a.miu;
+  auto load_plane = [&](int kk) {
+    const int s = kk % 3;
+    for (int e = tid; e < MSX * MSY; e += MX * MY) {
+      const int sy = e / MSX, sx = e - sy * MSX;
+      const int gi = i0 - 1 + sx, gj = j0 - 1 + sy;
+      if (gi <= p.imax + 1 && gj <= p.jmax + 1) {
+        const long long g = idxC(p, gi, gj, kk);
+        sm[0][s][sy][sx] = F0[g];
+        sm[1][s][sy][sx] = F1[g];
+        sm[2][s][sy][sx] = F2[g];
+        sm[3][s][sy][sx] = F3[g];
+      }
+    }
+  };
+  load_plane(ka - 1);
+  load_plane(ka);
   const double rho_avr = *a.rho_avr;
-  double Ru, Rv, Rw, du, dv, dw;
-  if (k >= 1 && k <= p.kmax) {
-    du = ab2_u(p, a, I, J, k, rho_avr, Ru);
-    dv = ab2_v(p, a, I, J, k, rho_avr, Rv);
-    dw = ab2_w(p, a, I, J, k, rho_avr, Rw);
-    if (k == p.kmax) dw = 0.;
-    if (I == i && J == j) {
-      const long long q = idxI(p, i, j, k);
+  const long long sy = p.nCx, sz = (long long)p.nCx * p.nCy;
+  double dw_km1 = 0.;
+  for (int k = ka; k <= kb; ++k) {
+    load_plane(k + 1);
+    __syncthreads();
+    if (ok) {
+      const int s_m = (k + 2) % 3, s_0 = k % 3, s_p = (k + 1) % 3;
+      auto sl = [&](int dk) { return dk < 0 ? s_m : (dk > 0 ? s_p : s_0); };
+      auto U = [&](int di, int dj, int dk) { return sm[0][sl(dk)][ty + 1 + dj][tx + 1 + di]; };
+      auto V = [&](int di, int dj, int dk) { return sm[1][sl(dk)][ty + 1 + dj][tx + 1 + di]; };
+      auto W = [&](int di, int dj, int dk) { return sm[2][sl(dk)][ty + 1 + dj][tx + 1 + di]; };
+      auto M = [&](int di, int dj, int dk) { return sm[3][sl(dk)][ty + 1 + dj][tx + 1 + di]; };
+      const long long c = idxC(p, i, j, k), q = idxI(p, i, j, k);
+      const double ru = a.rho_u[q], rv = a.rho_v[q], rw = a.rho_w[q];
+      const double Ru = rhs_u(p, U, V, W, M, ru, rho_avr);
+      const double Rv = rhs_v(p, U, V, W, M, rv, rho_avr);
+      const double Rw = rhs_w(p, U, V, W, M, rw, rho_avr);
+      const double du = ab2_update(p, a, c, 1, U(0, 0, 0), Ru, a.duold[q], ru, a.px, a.pxold, p.dxi);
+      const double dv = ab2_update(p, a, c, sy, V(0, 0, 0), Rv, a.dvold[q], rv, a.py, a.pyold, p.dyi) -
+                        p.forceytot * p.dt / rv;
+      double dw = ab2_update(p, a, c, sz, W(0, 0, 0), Rw, a.dwold[q], rw, a.pz, a.pzold, p.dzi);
       duold_out[q] = Ru;
       dvold_out[q] = Rv;
       dwold_out[q] = Rw;
+      if (k == p.kmax - 1) dw_km1 = dw;
+      if (k == p.kmax) dw = 0.;
+      putC(p, dudt, i, j, k, du);
+      putC(p, dvdt, i, j, k, dv);
+      putC(p, dwdt, i, j, k, dw);
+      if (k == 1) {
+        putC(p, dudt, i, j, 0, -du);
+        putC(p, dvdt, i, j, 0, 2. * p.v_lower - dv);
+        putC(p, dwdt, i, j, 0, 0.);
+      }
+      if (k == p.kmax) {
+        putC(p, dudt, i, j, p.k1, -du);
+        putC(p, dvdt, i, j, p.k1, 2. * p.v_upper - dv);
+        putC(p, dwdt, i, j, p.k1, dw_km1);
+      }
     }
-  } else if (k == 0) {
-    du = -ab2_u(p, a, I, J, 1, rho_avr, Ru);
-    dv = 2. * p.v_lower - ab2_v(p, a, I, J, 1, rho_avr, Rv);
-    dw = 0.;
-  } else {
-    du = -ab2_u(p, a, I, J, p.kmax, rho_avr, Ru);
-    dv = 2. * p.v_upper - ab2_v(p, a, I, J, p.kmax, rho_avr, Rv);
-    dw = ab2_w(p, a, I, J, p.kmax - 1, rho_avr, Rw);
+    __syncthreads();
   }
-  dudt[n] = du;
-  dvdt[n] = dv;
-  dwdt[n] = dw;
 }
 
 // mom_main alone (init.f90:90): RHS into shape-I arrays
@@ -245,10 +268,16 @@ __global__ void __launch_bounds__(NT) k_mom_main(Params p, MomArgs a, double* __
   int i, j, k;
   if (!cell3(kI0, cI1(p).v, i, j, k)) return;
   const long long q = idxI(p, i, j, k);
+  const long long c = idxC(p, i, j, k);
+  const long long sy = p.nCx, sz = (long long)p.nCx * p.nCy;
   const double rho_avr = *a.rho_avr;
-  ru[q] = rhs_u(p, a, i, j, k, rho_avr);
-  rv[q] = rhs_v(p, a, i, j, k, rho_avr);
-  rw[q] = rhs_w(p, a, i, j, k, rho_avr);
+  auto U = [&](int di, int dj, int dk) { return a.u[c + di + dj * sy + dk * sz]; };
+  auto V = [&](int di, int dj, int dk) { return a.v[c + di + dj * sy + dk * sz]; };
+  auto W = [&](int di, int dj, int dk) { return a.w[c + di + dj * sy + dk * sz]; };
+  auto M = [&](int di, int dj, int dk) { return a.miu[c + di + dj * sy + dk * sz]; };
+  ru[q] = rhs_u(p, U, V, W, M, a.rho_u[q], rho_avr);
+  rv[q] = rhs_v(p, U, V, W, M, a.rho_v[q], rho_avr);
+  rw[q] = rhs_w(p, U, V, W, M, a.rho_w[q], rho_avr);
 }
 
 // fillps (fillps.f90:36-53), optionally followed by p = p + p_jump
@@ -546,7 +575,10 @@ void launch_ab2(Ctx& c) {
   Scope sc_(c.prof, c.s, "ab2", 1);
   MomArgs a = mom_args(c);
   const int o = c.hist ^ 1;
-  k_ab2<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, a, c.dudt, c.dvdt, c.dwdt, c.duold[o], c.dvold[o], c.dwold[o]);
+  const int kc = 16, nch = std::max(1, c.P.kmax / kc);
+  const dim3 grid((unsigned)((c.P.imax + MX - 1) / MX), (unsigned)((c.P.jmax + MY - 1) / MY), (unsigned)nch);
+  k_ab2<<<grid, dim3(MX, MY, 1), 0, c.s>>>(c.P, a, c.dudt, c.dvdt, c.dwdt, c.duold[o], c.dvold[o], c.dwold[o],
+                                          nch == 1 ? c.P.kmax : kc, nch);
   c.hist = o;
 }
 void launch_mom_main(Ctx& c, double* du, double* dv, double* dw) {
