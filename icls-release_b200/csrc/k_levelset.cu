@@ -220,7 +220,7 @@ __device__ __forceinline__ double adv_val(const Params& p, int stage1, const dou
 
 // One RK stage over the tasks' regions; out may equal phi0 (see above).
 template <int SCHEME>
-__global__ void __launch_bounds__(NT) k_adv_stage(Params p, const __grid_constant__ LsBatch B, int stage1, double a,
+__global__ void __launch_bounds__(NT, 4) k_adv_stage(Params p, const __grid_constant__ LsBatch B, int stage1, double a,
                                                   double bb, double fdt, const double* __restrict__ vu,
                                                   const double* __restrict__ vv, const double* __restrict__ vw) {
   const int ti = task_of(B);

@@ -27,25 +27,52 @@ constexpr int FT = 256;  // threads per FFT CTA
 
 __device__ __forceinline__ int bitrev(int x, int logn) { return (int)(__brev((unsigned)x) >> (32 - logn)); }
 
-// in-place radix-2 DIT over nl lines of length N stored at buf[l*ld + n],
-// input in bit-reversed order.  inv: e^{+i} twiddles.
+// in-place radix-2 DIT over nl lines of length N = 2^logN stored at
+// buf[l*ld + n], input in bit-reversed order.  inv: e^{+i} twiddles.
+// Two consecutive stages run fused on four values held in registers: the
+// same butterflies in the same order as stage-by-stage passes, with half
+// the shared-memory round trips and barriers.
+__device__ __forceinline__ void bfly(double2& x0, double2& x1, double2 w) {
+  const double2 t1 = make_double2(x1.x * w.x - x1.y * w.y, x1.x * w.y + x1.y * w.x);
+  x1 = make_double2(x0.x - t1.x, x0.y - t1.y);
+  x0 = make_double2(x0.x + t1.x, x0.y + t1.y);
+}
+__device__ __forceinline__ double2 twid(const double2* __restrict__ tw, int idx, int inv) {
+  double2 w = __ldg(&tw[idx]);
+  if (inv) w.y = -w.y;
+  return w;
+}
 __device__ __forceinline__ void smem_fft(double2* buf, int nl, int N, int logN, int ld,
                                          const double2* __restrict__ tw, int inv) {
-  const int halfN = N >> 1;
-  for (int s = 1; s <= logN; ++s) {
-    const int half = 1 << (s - 1);
-    const int tstride = N >> s;
+  int s = 1;
+  if (logN >= 2) {
+    const int q4 = N >> 2, lq4 = logN - 2;
+    for (; s + 1 <= logN; s += 2) {
+      const int lh = s - 1, h = 1 << lh;
+      for (int t = threadIdx.x; t < nl * q4; t += blockDim.x) {
+        const int line = t >> lq4, b = t & (q4 - 1);
+        const int grp = b >> lh, j = b & (h - 1);
+        double2* L = buf + line * ld + (grp << (lh + 2)) + j;
+        double2 x0 = L[0], x1 = L[h], x2 = L[2 * h], x3 = L[3 * h];
+        const double2 w1 = twid(tw, j << (logN - s), inv);
+        bfly(x0, x1, w1);
+        bfly(x2, x3, w1);
+        bfly(x0, x2, twid(tw, j << (logN - s - 1), inv));
+        bfly(x1, x3, twid(tw, (j + h) << (logN - s - 1), inv));
+        L[0] = x0; L[h] = x1; L[2 * h] = x2; L[3 * h] = x3;
+      }
+      __syncthreads();
+    }
+  }
+  if (s == logN) {  // an odd stage count leaves the last stage
+    const int lh = s - 1, h = 1 << lh, halfN = N >> 1, lhalf = logN - 1;
     for (int t = threadIdx.x; t < nl * halfN; t += blockDim.x) {
-      const int line = t / halfN, b = t - line * halfN;
-      const int grp = b / half, j = b - grp * half;
-      const int i0 = grp * 2 * half + j, i1 = i0 + half;
-      double2 w = __ldg(&tw[j * tstride]);
-      if (inv) w.y = -w.y;
-      double2* L = buf + line * ld;
-      const double2 x0 = L[i0], x1 = L[i1];
-      const double2 t1 = make_double2(x1.x * w.x - x1.y * w.y, x1.x * w.y + x1.y * w.x);
-      L[i0] = make_double2(x0.x + t1.x, x0.y + t1.y);
-      L[i1] = make_double2(x0.x - t1.x, x0.y - t1.y);
+      const int line = t >> lhalf, b = t & (halfN - 1);
+      const int grp = b >> lh, j = b & (h - 1);
+      double2* L = buf + line * ld + (grp << (lh + 1)) + j;
+      double2 x0 = L[0], x1 = L[h];
+      bfly(x0, x1, twid(tw, j << (logN - s), inv));
+      L[0] = x0; L[h] = x1;
     }
     __syncthreads();
   }
@@ -93,15 +120,16 @@ __global__ void __launch_bounds__(FT) k_fft_x(Params p, int dir, int CL, int log
   const long long nlines = (long long)p.jmax * p.kmax;
   const long long l0 = (long long)blockIdx.x * (2 * CL);
   const double s = sqrt(1.0 / N);
+  const int lj = __ffs(p.jmax) - 1, mj = p.jmax - 1;  // jmax is a power of two
   // load
   for (int t = threadIdx.x; t < CL * N; t += blockDim.x) {
-    const int cl = t / N, n = t - cl * N;
+    const int cl = t >> logN, n = t & (N - 1);
     const long long la = l0 + 2 * cl, lb = la + 1;
     double2 z = make_double2(0., 0.);
     if (lb < nlines) {
       if (dir == 0) {
-        const int ja = (int)(la % p.jmax) + 1, ka = (int)(la / p.jmax) + 1;
-        const int jb = (int)(lb % p.jmax) + 1, kb = (int)(lb / p.jmax) + 1;
+        const int ja = (int)(la & mj) + 1, ka = (int)(la >> lj) + 1;
+        const int jb = (int)(lb & mj) + 1, kb = (int)(lb >> lj) + 1;
         z = make_double2(pp[idxC(p, n + 1, ja, ka)], pp[idxC(p, n + 1, jb, kb)]);
         sm[cl * ld + bitrev(n, logN)] = z;
       } else {
@@ -114,7 +142,7 @@ __global__ void __launch_bounds__(FT) k_fft_x(Params p, int dir, int CL, int log
   __syncthreads();
   smem_fft(sm, CL, N, logN, ld, tw, dir);
   for (int t = threadIdx.x; t < CL * N; t += blockDim.x) {
-    const int cl = t / N, n = t - cl * N;
+    const int cl = t >> logN, n = t & (N - 1);
     const long long la = l0 + 2 * cl, lb = la + 1;
     if (lb >= nlines) continue;
     if (dir == 0) {
@@ -128,7 +156,7 @@ __global__ void __launch_bounds__(FT) k_fft_x(Params p, int dir, int CL, int log
       for (int h = 0; h < 2; ++h) {
         const long long ll = h ? lb : la;
         const double v = h ? vb : va;
-        const int j = (int)(ll % p.jmax) + 1, k = (int)(ll / p.jmax) + 1;
+        const int j = (int)(ll & mj) + 1, k = (int)(ll >> lj) + 1;
         const int i = n + 1;
         if (!halos) {
           pp[idxC(p, i, j, k)] = v;
@@ -163,12 +191,13 @@ __global__ void __launch_bounds__(FT) k_fft_y(Params p, int dir, int TI, int log
   const int tiles_i = p.imax / TI;
   const int k = blockIdx.x / tiles_i + 1;
   const int i0 = (blockIdx.x % tiles_i) * TI + 1;
+  const int lt = __ffs(TI) - 1;  // TI is a power of two
   const long long sj = p.imax;
   double* base = spec + (long long)(i0 - 1) + (long long)p.imax * (long long)p.jmax * (k - 1);
   const double s = sqrt(1.0 / N);
   // load: consecutive threads read consecutive i
   for (int t = threadIdx.x; t < TI * N; t += blockDim.x) {
-    const int ti = t % TI, n = t / TI;
+    const int ti = t & (TI - 1), n = t >> lt;
     const double v = base[ti + n * sj];
     double* slot = reinterpret_cast<double*>(&sm[(ti >> 1) * ld]);
     if (dir == 0) {
@@ -182,7 +211,7 @@ __global__ void __launch_bounds__(FT) k_fft_y(Params p, int dir, int TI, int log
     // build Z in a second buffer region then copy back in bit-reversed order
     double2* tmp = sm + CL * ld;
     for (int t = threadIdx.x; t < CL * N; t += blockDim.x) {
-      const int cl = t / N, kk = t - cl * N;
+      const int cl = t >> logN, kk = t & (N - 1);
       const double* raw = reinterpret_cast<const double*>(&sm[cl * ld]);
       // raw[2n] = a_n, raw[2n+1] = b_n
       tmp[cl * ld + bitrev(kk, logN)] = pack_hc(raw, raw + 1, N, kk, 2);
@@ -193,7 +222,7 @@ __global__ void __launch_bounds__(FT) k_fft_y(Params p, int dir, int TI, int log
   }
   smem_fft(sm, CL, N, logN, ld, tw, dir);
   for (int t = threadIdx.x; t < TI * N; t += blockDim.x) {
-    const int ti = t % TI, n = t / TI;
+    const int ti = t & (TI - 1), n = t >> lt;
     const int cl = ti >> 1;
     double v;
     if (dir == 0) {
@@ -231,32 +260,56 @@ __global__ void k_thomas_setup(Params p, const double* __restrict__ xyrt, const 
   zpiv[q + (p.kmax - 1) * nxy] = bb - a[p.kmax] * d;
 }
 
-__global__ void k_thomas(Params p, const double* __restrict__ a, const double* __restrict__ c,
-                         const double* __restrict__ zpiv, double* __restrict__ spec) {
+// The sweeps read 8 rows ahead of the dependency chain (same operations,
+// in the same order, as a row-by-row loop).
+constexpr int TU = 8;
+__global__ void __launch_bounds__(128) k_thomas(Params p, const double* __restrict__ a, const double* __restrict__ c,
+                                                const double* __restrict__ zpiv, double* __restrict__ spec) {
   const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long nxy = (long long)p.imax * p.jmax;
   if (q >= nxy) return;
   const int K = p.kmax;
-  double* col = spec + q;
-  double z = zpiv[q];
-  double prev = col[0] * z;
+  double* __restrict__ col = spec + q;
+  const double* __restrict__ zc = zpiv + q;
+  double prev = col[0] * zc[0];
   col[0] = prev;
-  for (int k = 2; k <= K - 1; ++k) {
-    z = zpiv[q + (k - 1) * nxy];
-    const double v = (col[(k - 1) * nxy] - a[k] * prev) * z;
-    col[(k - 1) * nxy] = v;
-    prev = v;
+  for (int k0 = 2; k0 <= K - 1; k0 += TU) {
+    double cv[TU], zv[TU];
+#pragma unroll
+    for (int u = 0; u < TU; ++u)
+      if (k0 + u <= K - 1) {
+        cv[u] = col[(k0 + u - 1) * nxy];
+        zv[u] = zc[(k0 + u - 1) * nxy];
+      }
+#pragma unroll
+    for (int u = 0; u < TU; ++u)
+      if (k0 + u <= K - 1) {
+        const double v = (cv[u] - a[k0 + u] * prev) * zv[u];
+        col[(k0 + u - 1) * nxy] = v;
+        prev = v;
+      }
   }
-  const double zz = zpiv[q + (K - 1) * nxy];
+  const double zz = zc[(K - 1) * nxy];
   double nxt;
   if (zz != 0.) nxt = (col[(K - 1) * nxy] - a[K] * prev) / zz;
   else nxt = 0.;
   col[(K - 1) * nxy] = nxt;
-  for (int k = K - 1; k >= 1; --k) {
-    const double d = c[k] * zpiv[q + (k - 1) * nxy];
-    const double v = col[(k - 1) * nxy] - d * nxt;
-    col[(k - 1) * nxy] = v;
-    nxt = v;
+  for (int k0 = K - 1; k0 >= 1; k0 -= TU) {
+    double cv[TU], zv[TU];
+#pragma unroll
+    for (int u = 0; u < TU; ++u)
+      if (k0 - u >= 1) {
+        cv[u] = col[(k0 - u - 1) * nxy];
+        zv[u] = zc[(k0 - u - 1) * nxy];
+      }
+#pragma unroll
+    for (int u = 0; u < TU; ++u)
+      if (k0 - u >= 1) {
+        const double d = c[k0 - u] * zv[u];
+        const double v = cv[u] - d * nxt;
+        col[(k0 - u - 1) * nxy] = v;
+        nxt = v;
+      }
   }
 }
 
