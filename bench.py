@@ -302,6 +302,13 @@ def ours_arm(args):
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
     kernels = {k: {"share": round(e["ms"] / tot, 4), "launches": e["timed"],
                    "ms_per_launch": e["ms"] / max(e["timed"], 1)} for k, e in table.items()}
+    torch.cuda.synchronize()
+
+    # ---- the precision form on the same workload ------------------------
+    prec = None
+    if not args.no_forms:
+        prec = precision_leg(args, wl, ls, u, v, w, torch, world, istep, s)
+        prec["speedup_vs_fp64"] = prec["value"] / value
     del s
     torch.cuda.synchronize()
 
@@ -324,13 +331,69 @@ def ours_arm(args):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded drops)",
             "config": config_block(wl, world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": launches, "clocks": clocks, "kernels": kernels,
+            "gpu_launches": launches, "clocks": clocks, "kernels": kernels, "precision_form": prec,
         }
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def precision_leg(args, wl, ls, u, v, w, torch, world, fp64_solver_steps, ref):
+    """The precision form (FP32 bulk, FP64 Poisson / volume / jumps) on the
+    same workload: the same warm-up and timed steps, timed like the plain
+    path; then its errors against the plain FP64 context `ref`, which has run
+    fp64_solver_steps steps from the same initial state."""
+    from icls_gpu import FP32, Solver
+    from icls_gpu.config import IclsConfig
+    cfg = IclsConfig.from_buffer_copy(wl.cfg)
+    cfg.precision = FP32
+    s = Solver(cfg)
+    s.setup(ls, u, v, w)
+    stream = torch.cuda.ExternalStream(s.stream_ptr())
+    istep = 0
+    for _ in range(args.warmup):
+        istep += 1
+        s.step(istep, 0)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        istep += 1
+        s.step(istep, 0)
+    e1.record(stream)
+    e1.synchronize()
+    barrier(world)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    cells = cfg.itot * cfg.jtot * cfg.ktot
+    out = {"value": cells * args.steps * world / (ms / 1000.0) / 1e6, "unit": UNIT,
+           "ms_per_step": ms / args.steps, "dtype": "f32 bulk, f64 Poisson/volume/jumps"}
+    # errors after the same number of steps as the FP64 reference context
+    while istep < fp64_solver_steps:
+        istep += 1
+        s.step(istep, 0)
+    if istep == fp64_solver_steps:
+        def rel(a, b):
+            return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+        dz = wl.cfg.lz / wl.cfg.ktot
+        band = 0.0
+        for l in range(1, min(wl.cfg.lmax, 4) + 1):
+            pa, pb = s.download("lvset", l), ref.download("lvset", l)
+            m = np.abs(pb) <= 4.0 * dz
+            band = max(band, rel(pa[m], pb[m]))
+        va, vb = s.volumes()[0], ref.volumes()[0]
+        out["errors_vs_fp64"] = {
+            "steps": istep, "phi_band_rel_l2": band,
+            "u_rel_l2": rel(s.download("u"), ref.download("u")),
+            "w_rel_l2": rel(s.download("w"), ref.download("w")),
+            "volume_max_rel": float(np.max(np.abs(va - vb) / vb)),
+            "curv_rel_l2": rel(s.download("curv"), ref.download("curv")),
+            "drops_compared_phi": min(wl.cfg.lmax, 4)}
+    del s
+    return out
 
 
 def run_e2e(args, wl, ls, u, v, w, torch, world):
@@ -410,6 +473,7 @@ def main():
     ap.add_argument("--workload", default="multi_drop_256_48")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the precision-form leg")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

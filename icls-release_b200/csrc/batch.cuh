@@ -67,7 +67,8 @@ __device__ __forceinline__ int image_of(int i, int n) {
   return i <= H ? i + n : (i > n - H ? i - n : INT_MIN);
 }
 // v into column (i,j) of row k and its periodic images, shape L
-__device__ __forceinline__ void putL(const Params& p, double* __restrict__ a, int i, int j, int k, double v) {
+template <typename T>
+__device__ __forceinline__ void putL(const Params& p, T* __restrict__ a, int i, int j, int k, T v) {
   const int ii = image_of<3>(i, p.imax), jj = image_of<3>(j, p.jmax);
   a[idxL(p, i, j, k)] = v;
   if (ii != INT_MIN) a[idxL(p, ii, j, k)] = v;
@@ -77,7 +78,8 @@ __device__ __forceinline__ void putL(const Params& p, double* __restrict__ a, in
   }
 }
 // the same for shape C (one halo layer)
-__device__ __forceinline__ void putC(const Params& p, double* __restrict__ a, int i, int j, int k, double v) {
+template <typename T>
+__device__ __forceinline__ void putC(const Params& p, T* __restrict__ a, int i, int j, int k, T v) {
   const int ii = image_of<1>(i, p.imax), jj = image_of<1>(j, p.jmax);
   a[idxC(p, i, j, k)] = v;
   if (ii != INT_MIN) a[idxC(p, ii, j, k)] = v;
@@ -91,5 +93,11 @@ __device__ __forceinline__ bool in_written(const Params& p, const Region& r, int
   return k >= r.z0 && k <= r.z1 && span_has(r.xa, r.xn, p.imax, wrapx(p, i)) &&
          span_has(r.ya, r.yn, p.jmax, wrapy(p, j));
 }
+
+// the field type T view of a task's type-erased level-set pointers
+template <typename T>
+__device__ __forceinline__ const T* cT(const double* q) { return reinterpret_cast<const T*>(q); }
+template <typename T>
+__device__ __forceinline__ T* mT(double* q) { return reinterpret_cast<T*>(q); }
 
 }  // namespace icls

@@ -43,7 +43,7 @@ int validate(const icls_config* c) {
   if (c->reinit_step < 1 || c->inflate_step < 1 || c->reinit_iter_max < 1) return ICLS_E_CONFIG;
   if (c->ls_adv_space != ICLS_HOUC5 && c->ls_adv_space != ICLS_WENO5) return ICLS_E_CONFIG;
   if (c->i_space != ICLS_HOUC5 && c->i_space != ICLS_WENO5) return ICLS_E_CONFIG;
-  if (c->precision != ICLS_FP64) return ICLS_E_UNSUPPORTED;
+  if (c->precision != ICLS_FP64 && c->precision != ICLS_FP32) return ICLS_E_CONFIG;
   if (c->curvature_model != ICLS_CURV_STENCIL) return ICLS_E_UNSUPPORTED;
   return ICLS_OK;
 }
@@ -74,6 +74,7 @@ void fill_params(Ctx& c) {
   P.rho1 = f.rho1; P.rho2 = f.rho2; P.miu1 = f.miu1; P.miu2 = f.miu2;
   P.rho0 = std::min(f.rho1, f.rho2);  // param.f90:63
   P.rrho0 = 1. / P.rho0;
+  P.f32 = f.precision == ICLS_FP32 ? 1 : 0;
   P.visc = 1. / f.Re;                 // param.f90:73
   P.iFr = f.iFr;
   P.nondi = 1. / f.We;                // gfm.f90:40
@@ -145,19 +146,27 @@ int dalloc(T** p, size_t n) {
     if (rc_) return rc_;            \
   } while (0)
 
+// doubles that hold n elements of the form's field type
+size_t tn(const Params& P, long long n) { return P.f32 ? (size_t)(n + 1) / 2 : (size_t)n; }
+
 int allocate(Ctx& c) {
   const Params& P = c.P;
-  for (double** f : {&c.u, &c.v, &c.w, &c.pnew, &c.pold, &c.p, &c.dudt, &c.dvdt, &c.dwdt, &c.px, &c.py, &c.pz,
-                     &c.pxold, &c.pyold, &c.pzold, &c.pjump, &c.miu, &c.rho, &c.jiemian, &c.curv,
-                     &c.dheav, &c.kappa})
+  // FP64 in both forms: pressures, jumps (the Poisson solve and the GFM
+  // assembly stay FP64)
+  for (double** f : {&c.pnew, &c.pold, &c.p, &c.px, &c.py, &c.pz, &c.pxold, &c.pyold, &c.pzold, &c.pjump})
     AL(*f, (size_t)P.nC);
+  // the form's field type
+  for (double** f : {&c.u, &c.v, &c.w, &c.dudt, &c.dvdt, &c.dwdt, &c.miu, &c.rho, &c.jiemian, &c.curv, &c.dheav,
+                     &c.kappa})
+    AL(*f, tn(P, P.nC));
   for (int h = 0; h < 2; ++h) {
-    AL(c.duold[h], (size_t)P.nI); AL(c.dvold[h], (size_t)P.nI); AL(c.dwold[h], (size_t)P.nI);
+    AL(c.duold[h], tn(P, P.nI)); AL(c.dvold[h], tn(P, P.nI)); AL(c.dwold[h], tn(P, P.nI));
   }
   for (double** f : {&c.rho_u, &c.rho_v, &c.rho_w, &c.ucc, &c.vcc, &c.wcc, &c.nrm_m, &c.ulc, &c.vlc, &c.wlc})
-    AL(*f, (size_t)P.nI);
+    AL(*f, tn(P, P.nI));
   c.lv.assign(P.L, nullptr);
-  for (int l = 0; l < P.L; ++l) AL(c.lv[l], (size_t)P.nL);
+  for (int l = 0; l < P.L; ++l) AL(c.lv[l], tn(P, P.nL));
+  if (P.f32) AL(c.stage, (size_t)P.nL);
   AL(c.d_nbcnt, (size_t)P.L);
   AL(c.spec, (size_t)P.nI);
   AL(c.twx, (size_t)P.imax);
@@ -176,8 +185,7 @@ int allocate(Ctx& c) {
   CK(cudaMallocHost((void**)&c.h_sc, sizeof(DevScalars)));
   CK(cudaEventCreateWithFlags(&c.ev_vol, cudaEventDisableTiming));
   // normal%m = 1 outside the curvature band (interface.f90:44)
-  std::vector<double> ones((size_t)P.nI, 1.0);
-  CK(cudaMemcpy(c.nrm_m, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice));
+  launch_fill(c, c.nrm_m, P.nI, 1.0, true);
   AL(c.d_bbox, (size_t)10 * P.L);
   CK(cudaMallocHost((void**)&c.h_bbox, sizeof(int) * 10 * P.L));
   CK(cudaEventCreateWithFlags(&c.ev_bbox, cudaEventDisableTiming));
@@ -191,7 +199,7 @@ int allocate(Ctx& c) {
   // working buffers of a group of drops: as many drops as half the free
   // HBM holds (ICLS_GROUP=n caps the group, e.g. to test the grouped path)
   {
-    const size_t per = sizeof(double) * (3 * (size_t)P.nL + 2 * (size_t)P.nC) + (size_t)P.nI + 64;
+    const size_t per = sizeof(double) * (3 * tn(P, P.nL) + 2 * tn(P, P.nC)) + (size_t)P.nI + 64;
     size_t freeb = 0, totalb = 0;
     CK(cudaMemGetInfo(&freeb, &totalb));
     long long G = (long long)((freeb / 2) / per);
@@ -200,8 +208,8 @@ int allocate(Ctx& c) {
     G = std::max(1LL, std::min<long long>(G, P.L));
     c.mem.assign((size_t)G, Ctx::Member());
     for (Ctx::Member& m : c.mem) {
-      AL(m.s1, (size_t)P.nL); AL(m.s2, (size_t)P.nL); AL(m.s3, (size_t)P.nL);
-      AL(m.fit, (size_t)P.nC); AL(m.cv, (size_t)P.nC);
+      AL(m.s1, tn(P, P.nL)); AL(m.s2, tn(P, P.nL)); AL(m.s3, tn(P, P.nL));
+      AL(m.fit, tn(P, P.nC)); AL(m.cv, tn(P, P.nC));
       AL(m.mask, (size_t)P.nI);
     }
   }
@@ -232,6 +240,7 @@ void release(Ctx& c) {
   if (c.twy) cudaFree(c.twy);
   if (c.lpartials) cudaFree(c.lpartials);
   if (c.drs) cudaFree(c.drs);
+  if (c.stage) cudaFree(c.stage);
   if (c.dsc) cudaFree(c.dsc);
   if (c.h_vol) cudaFreeHost(c.h_vol);
   if (c.h_sc) cudaFreeHost(c.h_sc);
@@ -269,6 +278,17 @@ double* field_ptr(Ctx& c, int id, int l, long long* n) {
   *n = P.nL;
   if (id == ICLS_F_LVSET && l >= 1 && l <= P.L) return c.lv[l - 1];
   return nullptr;
+}
+
+// the field is stored in the form's field type (else FP64 in both forms)
+bool tfield(int id) {
+  switch (id) {
+    case ICLS_F_PNEW: case ICLS_F_POLD: case ICLS_F_P: case ICLS_F_PX: case ICLS_F_PY: case ICLS_F_PZ:
+    case ICLS_F_PXOLD: case ICLS_F_PYOLD: case ICLS_F_PZOLD: case ICLS_F_PJUMP:
+      return false;
+    default:
+      return true;
+  }
 }
 
 int check_launch() {
@@ -415,7 +435,7 @@ void make_full(Ctx& c, int l) {
 
 void update_materials(Ctx& c) {
   const int L = c.P.L;
-  launch_fill(c, c.jiemian, c.P.nC, 1.0);
+  launch_fill(c, c.jiemian, c.P.nC, 1.0, true);
   std::vector<int> all(L);
   for (int l = 0; l < L; ++l) all[l] = l;
   std::vector<int> ntiles(L, 0);
@@ -702,8 +722,8 @@ int ls_main(Ctx& c, int istep) {
 void fix_curv(Ctx& c) {
   if (!c.curv_stale && !c.nrm_stale) return;
   const int l = c.P.L - 1;
-  const size_t bytes = sizeof(double) * (size_t)c.P.nC;
-  launch_fill(c, c.nrm_m, c.P.nI, 1.0);
+  const size_t bytes = (c.P.f32 ? sizeof(float) : sizeof(double)) * (size_t)c.P.nC;
+  launch_fill(c, c.nrm_m, c.P.nI, 1.0, true);
   cudaMemsetAsync(c.curv, 0, bytes, c.s);
   std::vector<LsBatch> b = single(c, l, kStageRows, c_region(c.P, c.win[l].box, 1));
   LsTask& t = b[0].t[0];
@@ -788,7 +808,10 @@ int chkdiv(Ctx& c, int istep, double* divtot, double* divmax, int* ijk) {
       ijk[2] = (int)(q / ((long long)c.P.imax * c.P.jmax)) + 1;
     }
   }
-  if (c.h_sc->divmax > 1e-12 && istep != 0) return ICLS_E_DIVERGENCE;  // chkdiv.f90:60-87
+  // chkdiv.f90:60-87 stops above 1e-12; the precision form scales that bound
+  // by the ratio of the FP32 and FP64 unit roundoffs, 2^-24 / 2^-53 = 2^29
+  const double bound = c.P.f32 ? 1e-12 * 536870912.0 : 1e-12;
+  if (c.h_sc->divmax > bound && istep != 0) return ICLS_E_DIVERGENCE;
   return ICLS_OK;
 }
 
@@ -888,7 +911,12 @@ int icls_upload_field(icls_ctx* h, int id, int l, const double* host) {
   long long n;
   double* d = field_ptr(c, id, l, &n);
   if (!d) return ICLS_E_ARG;
-  CK(cudaMemcpyAsync(d, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c.s));
+  if (c.P.f32 && tfield(id)) {  // through the FP64 staging buffer
+    CK(cudaMemcpyAsync(c.stage, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c.s));
+    launch_to_float(c, d, c.stage, n);
+  } else {
+    CK(cudaMemcpyAsync(d, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c.s));
+  }
   CK(cudaStreamSynchronize(c.s));
   if (id == ICLS_F_LVSET) {  // a new level set: sweep it whole until its band is measured
     collect_bbox(c);
@@ -911,7 +939,12 @@ int icls_download_field(icls_ctx* h, int id, int l, double* host) {
     if (!is_full(c.P, w.valid)) launch_materialize(c, w.valid, w.bg, w.bg_ghost, d);
   }
   if (id == ICLS_F_CURV || id == ICLS_F_NORMAL_M) fix_curv(c);
-  CK(cudaMemcpyAsync(host, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+  if (c.P.f32 && tfield(id)) {
+    launch_to_double(c, c.stage, d, n);
+    CK(cudaMemcpyAsync(host, c.stage, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+  } else {
+    CK(cudaMemcpyAsync(host, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+  }
   CK(cudaStreamSynchronize(c.s));
   return ICLS_OK;
 }
@@ -1044,7 +1077,7 @@ int icls_boundp(icls_ctx* h, int id) {
   if (!h) return ICLS_E_ARG;
   long long n;
   double* d = field_ptr(h->c, id, 1, &n);
-  if (!d || n != h->c.P.nC) return ICLS_E_ARG;
+  if (!d || n != h->c.P.nC || (h->c.P.f32 && tfield(id))) return ICLS_E_ARG;
   launch_boundp(h->c, d);
   return check_launch();
 }
@@ -1165,6 +1198,13 @@ int icls_probe(icls_ctx* h, int id, int l, int i, int j, int k, double* value) {
   if (!d) return ICLS_E_ARG;
   const long long nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1;
   const long long off = (i - lo[0]) + nx * ((j - lo[1]) + ny * (long long)(k - lo[2]));
+  if (c.P.f32 && tfield(id)) {
+    float f = 0.f;
+    CK(cudaMemcpyAsync(&f, reinterpret_cast<float*>(d) + off, sizeof(float), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    *value = f;
+    return ICLS_OK;
+  }
   CK(cudaMemcpyAsync(value, d + off, sizeof(double), cudaMemcpyDeviceToHost, c.s));
   CK(cudaStreamSynchronize(c.s));
   return ICLS_OK;

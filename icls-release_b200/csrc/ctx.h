@@ -119,6 +119,7 @@ struct Ctx {
   double* dvol0 = nullptr;              // init_volume(1:L)
   double* dmaxchk = nullptr;            // per drop maxchk of the last inflation
   ReinitState* drs = nullptr;           // per drop
+  double* stage = nullptr;              // precision form: FP64 staging of one field (upload/download)
   double* hpart = nullptr;              // per-tile partial sums, red_cap per drop
   int red_cap = 0;                      // column tiles of a whole x-y plane
   // pinned host mirrors
@@ -164,13 +165,15 @@ void launch_reinit_stage(Ctx& c, const LsBatch& b, int stage, double dtau);
 void launch_reinit_reset(Ctx& c, const LsBatch& b, int maxiter);
 void launch_reinit_check(Ctx& c, const LsBatch& b, int it, int maxiter, double thr);
 void launch_heaviside(Ctx& c, const LsBatch& b);
-void launch_fill(Ctx& c, double* a, long long n, double v);
+void launch_fill(Ctx& c, double* a, long long n, double v, bool tfield);
 void launch_materials_final(Ctx& c, const double* outside, const int* ntiles);
 void launch_inflate_sums(Ctx& c, const LsBatch& b, double outside);
 void launch_inflate_vel(Ctx& c, const LsBatch& b);
 void launch_copy(Ctx& c, double* dst, const double* src, long long n);
 void launch_boundmls(Ctx& c, double* phi);
 void launch_materialize(Ctx& c, const Region& r, double bg, double bgg, double* phi);
+void launch_to_float(Ctx& c, double* dst_f32, const double* src, long long n);
+void launch_to_double(Ctx& c, double* dst, const double* src_f32, long long n);
 
 // interface / GFM (k_gfm.cu); the tasks carry shape-C regions
 // curvature: phi0 -> out (+ normal%m); recurvature: phis -> out; jumps: phi0, phis

@@ -37,6 +37,7 @@ struct Params {
   double forceytot;
   int TwoD;
   int ls_adv_space, i_space, ispeed_curv;
+  int f32;                   // precision form: bulk fields stored and computed in FP32
 };
 
 // ---------------------------------------------------------------- indexing
@@ -62,9 +63,12 @@ __device__ __forceinline__ T sq(T x) { return x * x; }
 
 // a/dx, a/dy, a/dz exactly as the reference divides (a product when the
 // spacing is a power of two, which is then bit-identical)
-__device__ __forceinline__ double divx(const Params& p, double a) { return p.pow2 ? a * p.rdx : a / p.dx; }
-__device__ __forceinline__ double divy(const Params& p, double a) { return p.pow2 ? a * p.rdy : a / p.dy; }
-__device__ __forceinline__ double divz(const Params& p, double a) { return p.pow2 ? a * p.rdz : a / p.dz; }
+template <typename T>
+__device__ __forceinline__ T divx(const Params& p, T a) { return p.pow2 ? a * (T)p.rdx : a / (T)p.dx; }
+template <typename T>
+__device__ __forceinline__ T divy(const Params& p, T a) { return p.pow2 ? a * (T)p.rdy : a / (T)p.dy; }
+template <typename T>
+__device__ __forceinline__ T divz(const Params& p, T a) { return p.pow2 ? a * (T)p.rdz : a / (T)p.dz; }
 
 // -------------------------------------------------------------- regions
 // A per-drop sweep region.  x and y are periodic: the region holds the

@@ -9,7 +9,8 @@
 //
 // The 10x27 pseudo-inverse (init.f90:1587-1723) lives in constant memory:
 // every thread of a warp reads the same coefficient, which the constant
-// cache broadcasts.
+// cache broadcasts.  Curvature runs in the form's field type T (FP64 or the
+// precision form's FP32); the jump assembly reads T fields and runs in FP64.
 #include <algorithm>
 
 #include "batch.cuh"
@@ -17,23 +18,31 @@
 namespace icls {
 
 __constant__ double cP[270];
+__constant__ float cPf[270];  // the same coefficients rounded to FP32
 
 namespace {
 
 constexpr int NT = 256;
+#define TC(x) static_cast<T>(x)
 
+template <typename T>
+__device__ __forceinline__ T coef(int q);
+template <>
+__device__ __forceinline__ double coef<double>(int q) { return cP[q]; }
+template <>
+__device__ __forceinline__ float coef<float>(int q) { return cPf[q]; }
 
 // curvature at an interior cell (interface.f90:57-111); m = |grad phi| or 1
-__device__ __forceinline__ double curvature_at(const Params& p, const double* __restrict__ phi, int i, int j,
-                                               int k, double& m) {
+template <typename T>
+__device__ __forceinline__ T curvature_at(const Params& p, const T* __restrict__ phi, int i, int j, int k, T& m) {
   const long long c = idxL(p, i, j, k);
-  m = 1.;
-  if (!(fabs(phi[c]) <= p.NB - 1. * p.dz)) return 0.;
+  m = TC(1.);
+  if (!(fabs(phi[c]) <= TC(p.NB - 1. * p.dz))) return TC(0.);
   // x[r] = sum over the 27 stencil values in order q = 0..26 of P(r,q)*phi_q,
   // accumulated while the stencil is read
-  double x[10];
+  T x[10];
 #pragma unroll
-  for (int r = 1; r < 10; ++r) x[r] = 0.;
+  for (int r = 1; r < 10; ++r) x[r] = TC(0.);
   int n = 0;
   const long long sy = p.nLx, sz = (long long)p.nLx * p.nLy;
 #pragma unroll 1
@@ -42,32 +51,32 @@ __device__ __forceinline__ double curvature_at(const Params& p, const double* __
     for (int dj = -1; dj <= 1; ++dj)
 #pragma unroll
       for (int di = -1; di <= 1; ++di) {
-        const double v = phi[c + di + dj * sy + dk * sz];
+        const T v = phi[c + di + dj * sy + dk * sz];
 #pragma unroll
-        for (int r = 1; r < 10; ++r) x[r] = x[r] + cP[r * 27 + n] * v;
+        for (int r = 1; r < 10; ++r) x[r] = x[r] + coef<T>(r * 27 + n) * v;
         ++n;
       }
-  const double dphidx = x[1], dphidy = x[2], dphidz = x[3];
-  const double d2phidx = x[4], d2phidy = x[5], d2phidz = x[6];
-  const double d2phidxdy = x[7], d2phidxdz = x[8], d2phidydz = x[9];
-  const double norm_val = sqrt((dphidx * dphidx + dphidy * dphidy) + dphidz * dphidz);
+  const T dphidx = x[1], dphidy = x[2], dphidz = x[3];
+  const T d2phidx = x[4], d2phidy = x[5], d2phidz = x[6];
+  const T d2phidxdy = x[7], d2phidxdz = x[8], d2phidydz = x[9];
+  const T norm_val = sqrt((dphidx * dphidx + dphidy * dphidy) + dphidz * dphidz);
   m = norm_val;
-  double cv;
-  if (norm_val < 0.9) {
-    cv = 0.;
+  T cv;
+  if (norm_val < TC(0.9)) {
+    cv = TC(0.);
   } else {
-    const double n3 = norm_val * norm_val * norm_val;
-    const double term1 = ((d2phidx + d2phidy) + d2phidz) / norm_val;
-    double term2 = (dphidx * dphidx * d2phidx + dphidy * dphidy * d2phidy) + dphidz * dphidz * d2phidz;
+    const T n3 = norm_val * norm_val * norm_val;
+    const T term1 = ((d2phidx + d2phidy) + d2phidz) / norm_val;
+    T term2 = (dphidx * dphidx * d2phidx + dphidy * dphidy * d2phidy) + dphidz * dphidz * d2phidz;
     term2 = term2 / n3;
-    double term3 = (dphidx * dphidy * d2phidxdy + dphidx * dphidz * d2phidxdz) + dphidy * dphidz * d2phidydz;
-    term3 = 2. * term3 / n3;
+    T term3 = (dphidx * dphidy * d2phidxdy + dphidx * dphidz * d2phidxdz) + dphidy * dphidz * d2phidydz;
+    term3 = TC(2.) * term3 / n3;
     cv = -((term1 - term2) - term3);
   }
-  const double max_kappa = 1. / p.dz;
+  const T max_kappa = TC(1. / p.dz);
   if (cv < -max_kappa) cv = -max_kappa;
   else if (cv > max_kappa) cv = max_kappa;
-  else if (fabs(cv) < 1e-9) cv = 0.;
+  else if (fabs(cv) < TC(1e-9)) cv = TC(0.);
   return cv;
 }
 
@@ -75,35 +84,40 @@ __device__ __forceinline__ double curvature_at(const Params& p, const double* __
 // drop's level set, out = its curvature): wall rows stay 0, halos are the
 // periodic copies (bound.f90:292-305), the apron (far field, |phi| > 5dz)
 // is 0.
-__global__ void __launch_bounds__(NT) k_curvature(Params p, const __grid_constant__ LsBatch B,
-                                                  double* __restrict__ nrm_m) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_curvature(Params p, const __grid_constant__ LsBatch B, T* __restrict__ nrm_m) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
   if (!c.ok) return;
+  const T* phi = cT<T>(t.phi0);
+  T* out = mT<T>(t.out);
   for (int k = c.ka; k <= c.kb; ++k) {
-    double v = 0.;
+    T v = TC(0.);
     if (k != 0 && k != p.k1 && computed(c, t.r, k)) {
-      double m;
-      v = curvature_at(p, t.phi0, c.i, c.j, k, m);
+      T m;
+      v = curvature_at(p, phi, c.i, c.j, k, m);
       if (nrm_m) nrm_m[idxI(p, c.i, c.j, k)] = m;
     }
-    putC(p, t.out, c.i, c.j, k, v);
+    putC(p, out, c.i, c.j, k, v);
   }
 }
 
 // re_curvature + boundc (interface.f90:186-218) over the tasks' regions:
 // phis (get_curvature) -> out
+template <typename T>
 __global__ void __launch_bounds__(NT) k_recurvature(Params p, const __grid_constant__ LsBatch B) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
-  const double* __restrict__ cin = t.phis;
+  const T* __restrict__ cin = cT<T>(t.phis);
+  const T* __restrict__ phi = cT<T>(t.phi0);
+  T* out = mT<T>(t.out);
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
   if (!c.ok) return;
   const long long sy = p.nCx, sz = (long long)p.nCx * p.nCy;
   for (int k = c.ka; k <= c.kb; ++k) {
-    double acc = 0.;
-    if (k != 0 && k != p.k1 && computed(c, t.r, k) && fabs(t.phi0[idxL(p, c.i, c.j, k)]) < 2. * p.dz) {
+    T acc = TC(0.);
+    if (k != 0 && k != p.k1 && computed(c, t.r, k) && fabs(phi[idxL(p, c.i, c.j, k)]) < TC(2. * p.dz)) {
       const long long cc = idxC(p, c.i, c.j, k);
       int q = 0;
 #pragma unroll
@@ -111,9 +125,9 @@ __global__ void __launch_bounds__(NT) k_recurvature(Params p, const __grid_const
 #pragma unroll
         for (int dj = -1; dj <= 1; ++dj)
 #pragma unroll
-          for (int di = -1; di <= 1; ++di) acc = acc + cP[q++] * cin[cc + di + dj * sy + dk * sz];
+          for (int di = -1; di <= 1; ++di) acc = acc + coef<T>(q++) * cin[cc + di + dj * sy + dk * sz];
     }
-    putC(p, t.out, c.i, c.j, k, acc);
+    putC(p, out, c.i, c.j, k, acc);
   }
 }
 
@@ -148,9 +162,9 @@ __device__ __forceinline__ double div2(const Params& p, double a, double h, doub
 }
 
 // jumps of one axis: jp(-1) + jp(0) + jp(1) and the + face jump
-__device__ __forceinline__ double axis_jump(const Params& p, const double* __restrict__ phi,
-                                            const double* __restrict__ cv, long long cl, long long sl,
-                                            long long cc, long long sc, double& pface) {
+template <typename T>
+__device__ __forceinline__ double axis_jump(const Params& p, const T* __restrict__ phi, const T* __restrict__ cv,
+                                            long long cl, long long sl, long long cc, long long sc, double& pface) {
   const double ph0 = phi[cl], phm = phi[cl - sl], php = phi[cl + sl];
   const double c0 = cv[cc], cm = cv[cc - sc], cpp = cv[cc + sc];
   double jm = 0., jp = 0.;
@@ -168,15 +182,16 @@ __device__ __forceinline__ double axis_jump(const Params& p, const double* __res
 // The additions are atomic: where at most two drops reach a cell the sum is
 // the reference's exactly (0+a+b is exact in either order); a cell in the
 // shells of three or more drops may differ in the last bit.
+template <typename T>
 __global__ void __launch_bounds__(NT) k_jumps(Params p, const __grid_constant__ LsBatch B,
                                               double* __restrict__ pjump, double* __restrict__ px,
                                               double* __restrict__ py, double* __restrict__ pz) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
-  const double* __restrict__ cv = t.phis;
+  const T* __restrict__ cv = cT<T>(t.phis);
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
   if (!c.ok || !c.cxy) return;
-  const double* __restrict__ phi = t.phi0;
+  const T* __restrict__ phi = cT<T>(t.phi0);
   const int i = c.i, j = c.j;
   for (int k = max(c.ka, max(t.r.cz0, 1)); k <= min(c.kb, min(t.r.cz1, p.kmax)); ++k) {
     const long long cl = idxL(p, i, j, k);
@@ -210,17 +225,19 @@ __device__ __forceinline__ unsigned long long ord_bits(double x) {
 }
 // one pair (m, n): sweeps m's written cells (task 0, phi0 = phi_m); phi_n
 // is read where n's region wrote it and is its far field bgn elsewhere
-__global__ void __launch_bounds__(NT) k_ipot_pair(Params p, const __grid_constant__ LsBatch B, const double* __restrict__ pn,
+template <typename T>
+__global__ void __launch_bounds__(NT) k_ipot_pair(Params p, const __grid_constant__ LsBatch B, const T* __restrict__ pn,
                                                   Region rn, double bgn, double bggn,
                                                   unsigned long long* __restrict__ out) {
   const LsTask& t = B.t[0];
+  const T* pm = cT<T>(t.phi0);
   const Col c = col_of(p, t, (int)blockIdx.x);
   double s = 1e3;
   if (c.ok) {
     for (int k = c.ka; k <= c.kb; ++k) {
       const long long n = idxL(p, c.i, c.j, k);
-      const double a = t.phi0[n];
-      const double b = in_written(p, rn, c.i, c.j, k) ? pn[n] : ((k < 0 || k > p.k1) ? bggn : bgn);
+      const double a = pm[n];
+      const double b = in_written(p, rn, c.i, c.j, k) ? (double)pn[n] : ((k < 0 || k > p.k1) ? bggn : bgn);
       if (a > -1. * p.dz && a < 1. * p.dz && b < p.NB) s = fmin(s, a + b);
     }
   }
@@ -240,10 +257,15 @@ __global__ void __launch_bounds__(NT) k_ipot_pair(Params p, const __grid_constan
   }
 }
 
+#undef TC
 }  // namespace
 
 void set_pseudo_inverse(const double* P270, cudaStream_t s) {
+  static float f[270];
+  for (int q = 0; q < 270; ++q) f[q] = (float)P270[q];
   cudaMemcpyToSymbolAsync(cP, P270, 270 * sizeof(double), 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(cPf, f, 270 * sizeof(float), 0, cudaMemcpyHostToDevice, s);
+  cudaStreamSynchronize(s);
 }
 
 const dim3 kTile(TBX, TBY, 1);
@@ -251,17 +273,26 @@ const dim3 kTile(TBX, TBY, 1);
 void launch_curvature(Ctx& c, const LsBatch& b, double* nrm_m_out) {
   if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "curvature", 1);
-  k_curvature<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, nrm_m_out);
+  if (c.P.f32)
+    k_curvature<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, reinterpret_cast<float*>(nrm_m_out));
+  else
+    k_curvature<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, nrm_m_out);
 }
 void launch_recurvature(Ctx& c, const LsBatch& b) {
   if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "recurvature", 1);
-  k_recurvature<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b);
+  if (c.P.f32)
+    k_recurvature<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b);
+  else
+    k_recurvature<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b);
 }
 void launch_jumps(Ctx& c, const LsBatch& b) {
   if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "jumps", 1);
-  k_jumps<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.pjump, c.px, c.py, c.pz);
+  if (c.P.f32)
+    k_jumps<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.pjump, c.px, c.py, c.pz);
+  else
+    k_jumps<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.pjump, c.px, c.py, c.pz);
 }
 // dmin_dev: L*L unsigned long long ordered bits, filled here; only cells
 // written by both drops' regions can hold |phi_m| < dz and phi_n < 6dz
@@ -282,8 +313,13 @@ void launch_ipot(Ctx& c, double* dmin_dev) {
       t.phi0 = c.lv[m];
       set_tiles(b, 8);
       Scope sc_(c.prof, c.s, "ipot", 1);
-      k_ipot_pair<<<b.start[1], kTile, 0, c.s>>>(c.P, b, c.lv[n], c.win[n].valid, c.win[n].bg, c.win[n].bg_ghost,
-                                                 o + m + (long long)c.P.L * n);
+      if (c.P.f32)
+        k_ipot_pair<float><<<b.start[1], kTile, 0, c.s>>>(c.P, b, reinterpret_cast<const float*>(c.lv[n]),
+                                                          c.win[n].valid, c.win[n].bg, c.win[n].bg_ghost,
+                                                          o + m + (long long)c.P.L * n);
+      else
+        k_ipot_pair<double><<<b.start[1], kTile, 0, c.s>>>(c.P, b, c.lv[n], c.win[n].valid, c.win[n].bg,
+                                                           c.win[n].bg_ghost, o + m + (long long)c.P.L * n);
     }
 }
 

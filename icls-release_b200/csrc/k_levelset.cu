@@ -42,7 +42,13 @@ constexpr int NT = TBX * TBY;
 const dim3 kTile(TBX, TBY, 1);
 const dim3 kBlock(BX, BY, 1);
 
-__device__ __forceinline__ double clipNB(double x, double NB) {
+// T is the type the level-set fields are stored and computed in: double
+// for the reference form, float for the precision form.  TC(x) is the
+// constant x in T.
+#define TC(x) static_cast<T>(x)
+
+template <typename T>
+__device__ __forceinline__ T clipNB(T x, T NB) {
   return x > NB ? NB : (x < -NB ? -NB : x);
 }
 __device__ __forceinline__ bool interior(const Params& p, int i, int j, int k) {
@@ -55,20 +61,25 @@ __device__ __forceinline__ bool interior(const Params& p, int i, int j, int k) {
 // (rows 0..k1) or bggin (ghost rows) elsewhere.  Counts the band per drop
 // and records the extent of the cells whose clipped value is not +NB:
 // bbox_lo[5 l + a], bbox_hi[5 l + a] for a = x, x shifted by imax/2, y, y
-// shifted by jmax/2, z.
+// shifted by jmax/2, z.  A far-field cell is outside the band only if all
+// 15 axial neighbours clip to +-NB, so the test stops at the first that
+// does not (the reference's sums of |clip|-NB <= 0 are zero exactly then).
+template <typename T>
 __global__ void __launch_bounds__(NT) k_tube(Params p, const __grid_constant__ LsBatch B,
                                              long long* __restrict__ cnt, int* __restrict__ bbox_lo,
                                              int* __restrict__ bbox_hi) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
-  const double NB = p.NB;
-  const double* __restrict__ in = t.phi0;
+  const T NB = TC(p.NB);
+  const T* __restrict__ in = cT<T>(t.phi0);
+  T* __restrict__ out = mT<T>(t.out);
+  const T bgin = TC(t.bgin), bggin = TC(t.bggin);
   int band = 0;
   int lo[5] = {INT_MAX, INT_MAX, INT_MAX, INT_MAX, INT_MAX};
   int hi[5] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN};
-  auto rd = [&](int a, int b, int k) -> double {
-    return in_written(p, t.vin, a, b, k) ? in[idxL(p, a, b, k)] : ((k < 0 || k > p.k1) ? t.bggin : t.bgin);
+  auto rd = [&](int a, int b, int k) -> T {
+    return in_written(p, t.vin, a, b, k) ? in[idxL(p, a, b, k)] : ((k < 0 || k > p.k1) ? bggin : bgin);
   };
   if (c.ok) {
     const int i = c.i, j = c.j;
@@ -76,26 +87,24 @@ __global__ void __launch_bounds__(NT) k_tube(Params p, const __grid_constant__ L
     const int ib = i + hx > p.imax ? i + hx - p.imax : i + hx;
     const int jb = j + hy > p.jmax ? j + hy - p.jmax : j + hy;
     for (int k = c.ka; k <= c.kb; ++k) {
-      double val;
+      T val;
       if (!computed(c, t.r, k)) {
-        val = clipNB((k < 0 || k > p.k1) ? t.bggin : t.bgin, NB);
+        val = clipNB((k < 0 || k > p.k1) ? bggin : bgin, NB);
       } else {
         if (k == 0)
-          val = 2. * clipNB(rd(i, j, 1), NB) - clipNB(rd(i, j, 2), NB);
+          val = TC(2.) * clipNB(rd(i, j, 1), NB) - clipNB(rd(i, j, 2), NB);
         else if (k == p.k1)
-          val = 2. * clipNB(rd(i, j, p.kmax), NB) - clipNB(rd(i, j, p.kmax - 1), NB);
+          val = TC(2.) * clipNB(rd(i, j, p.kmax), NB) - clipNB(rd(i, j, p.kmax - 1), NB);
         else
           val = clipNB(rd(i, j, k), NB);
         if (k >= 1 && k <= p.kmax) {
-          int m;
+          int m = 0;
           if (fabs(val) < NB) {
             m = 1;
           } else {
-            double xs = 0., ys = 0., zs = 0.;
-            for (int d = -2; d <= 2; ++d) xs += fabs(clipNB(rd(i + d, j, k), NB)) - NB;
-            for (int d = -2; d <= 2; ++d) ys += fabs(clipNB(rd(i, j + d, k), NB)) - NB;
-            for (int d = -2; d <= 2; ++d) zs += fabs(clipNB(rd(i, j, k + d), NB)) - NB;
-            m = (xs == 0. && ys == 0. && zs == 0.) ? 0 : 1;
+            for (int d = -2; d <= 2 && !m; ++d) m = fabs(clipNB(rd(i + d, j, k), NB)) != NB;
+            for (int d = -2; d <= 2 && !m; ++d) m = fabs(clipNB(rd(i, j + d, k), NB)) != NB;
+            for (int d = -2; d <= 2 && !m; ++d) m = fabs(clipNB(rd(i, j, k + d), NB)) != NB;
           }
           t.mask[idxI(p, i, j, k)] = (uint8_t)m;
           band += m;
@@ -108,7 +117,7 @@ __global__ void __launch_bounds__(NT) k_tube(Params p, const __grid_constant__ L
           lo[4] = min(lo[4], k); hi[4] = max(hi[4], k);
         }
       }
-      putL(p, t.out, i, j, k, val);
+      putL(p, out, i, j, k, val);
     }
   }
   const int bs = block_sum<int, NT>(band);
@@ -128,33 +137,33 @@ __global__ void __launch_bounds__(NT) k_tube(Params p, const __grid_constant__ L
 
 // ------------------------------------------------------- advection RHS
 // dfdt of HOUC5_nb (hyperPDE.f90:397-495) or WENO5_nb (503-800) at (i,j,k)
-template <int SCHEME>
-__device__ __forceinline__ double adv_rhs(const Params& p, const double* __restrict__ phi,
-                                          double vu, double vv, double vw, int i, int j, int k) {
+template <int SCHEME, typename T>
+__device__ __forceinline__ T adv_rhs(const Params& p, const T* __restrict__ phi, T vu, T vv, T vw, int i, int j,
+                                     int k) {
   const long long c = idxL(p, i, j, k);
   const long long sx = 1, sy = p.nLx, sz = (long long)p.nLx * p.nLy;
 #define PH(o) phi[c + (o)]
-  double udfdx, vdfdy, wdfdz, dfx, dfy, dfz;
+  T udfdx, vdfdy, wdfdz, dfx, dfy, dfz;
   if (SCHEME == ICLS_HOUC5) {
     if (p.TwoD) {
-      udfdx = 0.;
+      udfdx = TC(0.);
     } else {
-      if (vu >= 0.)
+      if (vu >= TC(0.))
         dfx = houc5_pos(PH(-3 * sx), PH(-2 * sx), PH(-sx), PH(0), PH(sx), PH(2 * sx));
       else
         dfx = houc5_neg(PH(3 * sx), PH(2 * sx), PH(sx), PH(0), PH(-sx), PH(-2 * sx));
       udfdx = -divx(p, vu * dfx);
     }
-    if (vv >= 0.)
+    if (vv >= TC(0.))
       dfy = houc5_pos(PH(-3 * sy), PH(-2 * sy), PH(-sy), PH(0), PH(sy), PH(2 * sy));
     else
       dfy = houc5_neg(PH(3 * sy), PH(2 * sy), PH(sy), PH(0), PH(-sy), PH(-2 * sy));
     vdfdy = -divy(p, vv * dfy);
   } else {
     if (p.TwoD) {
-      udfdx = 0.;
+      udfdx = TC(0.);
     } else {
-      if (vu >= 0.)
+      if (vu >= TC(0.))
         dfx = weno5(divx(p, PH(-2 * sx) - PH(-3 * sx)), divx(p, PH(-sx) - PH(-2 * sx)), divx(p, PH(0) - PH(-sx)),
                     divx(p, PH(sx) - PH(0)), divx(p, PH(2 * sx) - PH(sx)));
       else
@@ -163,7 +172,7 @@ __device__ __forceinline__ double adv_rhs(const Params& p, const double* __restr
       udfdx = -(vu * dfx);
     }
     // y uses dx, as in the reference (hyperPDE.f90:622-626)
-    if (vv >= 0.)
+    if (vv >= TC(0.))
       dfy = weno5(divx(p, PH(-2 * sy) - PH(-3 * sy)), divx(p, PH(-sy) - PH(-2 * sy)), divx(p, PH(0) - PH(-sy)),
                   divx(p, PH(sy) - PH(0)), divx(p, PH(2 * sy) - PH(sy)));
     else
@@ -173,13 +182,13 @@ __device__ __forceinline__ double adv_rhs(const Params& p, const double* __restr
   }
   if (k > 2 && k < p.kmax - 1) {
     if (SCHEME == ICLS_HOUC5) {
-      if (vw >= 0.)
+      if (vw >= TC(0.))
         dfz = houc5_pos(PH(-3 * sz), PH(-2 * sz), PH(-sz), PH(0), PH(sz), PH(2 * sz));
       else
         dfz = houc5_neg(PH(3 * sz), PH(2 * sz), PH(sz), PH(0), PH(-sz), PH(-2 * sz));
       wdfdz = -divz(p, vw * dfz);
     } else {
-      if (vw >= 0.)
+      if (vw >= TC(0.))
         dfz = weno5(divz(p, PH(-2 * sz) - PH(-3 * sz)), divz(p, PH(-sz) - PH(-2 * sz)), divz(p, PH(0) - PH(-sz)),
                     divz(p, PH(sz) - PH(0)), divz(p, PH(2 * sz) - PH(sz)));
       else
@@ -188,13 +197,13 @@ __device__ __forceinline__ double adv_rhs(const Params& p, const double* __restr
       wdfdz = -(vw * dfz);
     }
   } else if (k == 2 || k == p.kmax - 1) {  // HOUC3 near the walls
-    if (vw >= 0.)
-      dfz = (((1. / 6.) * PH(-2 * sz) - PH(-sz)) + (1. / 2.) * PH(0)) + (1. / 3.) * PH(sz);
+    if (vw >= TC(0.))
+      dfz = ((TC(1. / 6.) * PH(-2 * sz) - PH(-sz)) + TC(1. / 2.) * PH(0)) + TC(1. / 3.) * PH(sz);
     else
-      dfz = ((-((1. / 6.) * PH(2 * sz)) + PH(sz)) - (1. / 2.) * PH(0)) - (1. / 3.) * PH(-sz);
+      dfz = ((-(TC(1. / 6.) * PH(2 * sz)) + PH(sz)) - TC(1. / 2.) * PH(0)) - TC(1. / 3.) * PH(-sz);
     wdfdz = -divz(p, vw * dfz);
   } else {  // first-order upwinding at k=1,kmax
-    if (vw >= 0.) dfz = PH(0) - PH(-sz);
+    if (vw >= TC(0.)) dfz = PH(0) - PH(-sz);
     else dfz = PH(sz) - PH(0);
     wdfdz = -divz(p, vw * dfz);
   }
@@ -203,14 +212,13 @@ __device__ __forceinline__ double adv_rhs(const Params& p, const double* __restr
 }
 
 // RK_nb value of one cell: phi_in (+ factor*dt*dfdt on the band)
-template <int SCHEME>
-__device__ __forceinline__ double adv_val(const Params& p, int stage1, const double* __restrict__ phi0,
-                                          const double* __restrict__ phis, double a, double b, double fdt,
-                                          const double* __restrict__ vu, const double* __restrict__ vv,
-                                          const double* __restrict__ vw, const uint8_t* __restrict__ mask,
-                                          int I, int J, int k) {
+template <int SCHEME, typename T>
+__device__ __forceinline__ T adv_val(const Params& p, int stage1, const T* __restrict__ phi0,
+                                     const T* __restrict__ phis, T a, T b, T fdt, const T* __restrict__ vu,
+                                     const T* __restrict__ vv, const T* __restrict__ vw,
+                                     const uint8_t* __restrict__ mask, int I, int J, int k) {
   const long long n = idxL(p, I, J, k);
-  double v = stage1 ? phi0[n] : a * phi0[n] + b * phis[n];
+  T v = stage1 ? phi0[n] : a * phi0[n] + b * phis[n];
   if (k >= 1 && k <= p.kmax) {
     const long long q = idxI(p, I, J, k);
     if (mask[q]) v = v + fdt * adv_rhs<SCHEME>(p, phis, vu[q], vv[q], vw[q], I, J, k);
@@ -219,57 +227,64 @@ __device__ __forceinline__ double adv_val(const Params& p, int stage1, const dou
 }
 
 // One RK stage over the tasks' regions; out may equal phi0 (see above).
-template <int SCHEME>
-__global__ void __launch_bounds__(NT, 4) k_adv_stage(Params p, const __grid_constant__ LsBatch B, int stage1, double a,
-                                                  double bb, double fdt, const double* __restrict__ vu,
-                                                  const double* __restrict__ vv, const double* __restrict__ vw) {
+template <int SCHEME, typename T>
+__global__ void __launch_bounds__(NT, 4) k_adv_stage(Params p, const __grid_constant__ LsBatch B, int stage1,
+                                                     double a_, double bb_, double fdt_, const T* __restrict__ vu,
+                                                     const T* __restrict__ vv, const T* __restrict__ vw) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
   if (!c.ok) return;
+  const T a = TC(a_), bb = TC(bb_), fdt = TC(fdt_);
+  const T* phi0 = cT<T>(t.phi0);
+  const T* phis = cT<T>(t.phis);
+  T* out = mT<T>(t.out);
   const int i = c.i, j = c.j;
-  double v1 = 0., v2 = 0., vkm = 0., vk = 0.;
+  T v1 = TC(0.), v2 = TC(0.), vkm = TC(0.), vk = TC(0.);
   bool wall0 = false;
   for (int k = c.ka; k <= c.kb; ++k) {
     if (!computed(c, t.r, k)) {
-      putL(p, t.out, i, j, k, (k < 0 || k > p.k1) ? t.bgg : t.bg);
+      putL(p, out, i, j, k, (k < 0 || k > p.k1) ? TC(t.bgg) : TC(t.bg));
       continue;
     }
     if (k == 0) {  // written once rows 1 and 2 are known
       wall0 = true;
       continue;
     }
-    double val;
+    T val;
     if (k == p.k1) {
-      val = 2. * vk - vkm;
+      val = TC(2.) * vk - vkm;
     } else {
-      val = adv_val<SCHEME>(p, stage1, t.phi0, t.phis, a, bb, fdt, vu, vv, vw, t.mask, i, j, k);
+      val = adv_val<SCHEME>(p, stage1, phi0, phis, a, bb, fdt, vu, vv, vw, t.mask, i, j, k);
       if (k == 1) v1 = val;
       if (k == 2) v2 = val;
       if (k == p.kmax - 1) vkm = val;
       if (k == p.kmax) vk = val;
     }
-    putL(p, t.out, i, j, k, val);
-    if (k == 2 && wall0) putL(p, t.out, i, j, 0, 2. * v1 - v2);
+    putL(p, out, i, j, k, val);
+    if (k == 2 && wall0) putL(p, out, i, j, 0, TC(2.) * v1 - v2);
   }
 }
 
 // ------------------------------------------------------------ reinit
 // sgn(phi_0) of ls_reinit (levelset.f90:668-678)
-__device__ __forceinline__ double reinit_sgn(const Params& p, double p0) {
-  if (p0 < -p.dz) return -1.;
-  if (p0 > p.dz) return 1.;
-  return p0 / sqrt(p0 * p0 + p.dz * p.dz);
+template <typename T>
+__device__ __forceinline__ T reinit_sgn(const Params& p, T p0) {
+  const T dz = TC(p.dz);
+  if (p0 < -dz) return TC(-1.);
+  if (p0 > dz) return TC(1.);
+  return p0 / sqrt(p0 * p0 + dz * dz);
 }
 
 // RHS of WENO5_reinit at an interior cell (hyperPDE.f90:2646-2746)
-__device__ __forceinline__ double reinit_rhs(const Params& p, const double* __restrict__ phi,
-                                             const double* __restrict__ orig, int i, int j, int k) {
+template <typename T>
+__device__ __forceinline__ T reinit_rhs(const Params& p, const T* __restrict__ phi, const T* __restrict__ orig,
+                                        int i, int j, int k) {
   const long long c = idxL(p, i, j, k);
-  if (!(fabs(phi[c]) < p.NB + p.dz)) return 0.;
+  if (!(fabs(phi[c]) < TC(p.NB + p.dz))) return TC(0.);
   const long long sx = 1, sy = p.nLx, sz = (long long)p.nLx * p.nLy;
 #define PH(o) phi[c + (o)]
-  double A = 0., B = 0., C, D, E, F;
+  T A = TC(0.), B = TC(0.), C, D, E, F;
   if (!p.TwoD) {
     A = weno5(divx(p, PH(-2 * sx) - PH(-3 * sx)), divx(p, PH(-sx) - PH(-2 * sx)), divx(p, PH(0) - PH(-sx)),
               divx(p, PH(sx) - PH(0)), divx(p, PH(2 * sx) - PH(sx)));
@@ -290,78 +305,85 @@ __device__ __forceinline__ double reinit_rhs(const Params& p, const double* __re
     F = divz(p, PH(sz) - PH(0));
   }
 #undef PH
-  const double s = reinit_sgn(p, orig[c]);
-  double dydx, dydy, dydz;
+  const T s = reinit_sgn(p, orig[c]);
+  T dydx, dydy, dydz;
   if (p.TwoD) {
-    dydx = 0.;
+    dydx = TC(0.);
   } else {
-    if ((B * s < 0.) && ((A + B) * s < 0.)) dydx = B;
-    else if ((A * s > 0.) && ((A + B) * s > 0.)) dydx = A;
-    else dydx = 0.5 * (A + B);
+    if ((B * s < TC(0.)) && ((A + B) * s < TC(0.))) dydx = B;
+    else if ((A * s > TC(0.)) && ((A + B) * s > TC(0.))) dydx = A;
+    else dydx = TC(0.5) * (A + B);
   }
-  if ((D * s < 0.) && ((C + D) * s < 0.)) dydy = D;
-  else if ((C * s > 0.) && ((C + D) * s > 0.)) dydy = C;
-  else dydy = 0.5 * (C + D);
-  if ((F * s < 0.) && ((E + F) * s < 0.)) dydz = F;
-  else if ((E * s > 0.) && ((E + F) * s > 0.)) dydz = E;
-  else dydz = 0.5 * (E + F);
-  return s * (1. - sqrt((dydx * dydx + dydy * dydy) + dydz * dydz));
+  if ((D * s < TC(0.)) && ((C + D) * s < TC(0.))) dydy = D;
+  else if ((C * s > TC(0.)) && ((C + D) * s > TC(0.))) dydy = C;
+  else dydy = TC(0.5) * (C + D);
+  if ((F * s < TC(0.)) && ((E + F) * s < TC(0.))) dydz = F;
+  else if ((E * s > TC(0.)) && ((E + F) * s > TC(0.))) dydz = E;
+  else dydz = TC(0.5) * (E + F);
+  return s * (TC(1.) - sqrt((dydx * dydx + dydy * dydy) + dydz * dydz));
 }
 
 // one SSP-RK3 stage value of ls_reinit (levelset.f90:800-810)
-__device__ __forceinline__ double reinit_val(const Params& p, int stage, const double* __restrict__ phi0,
-                                             const double* __restrict__ phis, const double* __restrict__ orig,
-                                             double dtau, int I, int J, int k) {
+template <typename T>
+__device__ __forceinline__ T reinit_val(const Params& p, int stage, const T* __restrict__ phi0,
+                                        const T* __restrict__ phis, const T* __restrict__ orig, T dtau, int I, int J,
+                                        int k) {
   const long long n = idxL(p, I, J, k);
-  const double rhs = (k >= 1 && k <= p.kmax) ? reinit_rhs(p, phis, orig, I, J, k) : 0.;
+  const T rhs = (k >= 1 && k <= p.kmax) ? reinit_rhs(p, phis, orig, I, J, k) : TC(0.);
   if (stage == 1) return phi0[n] + dtau * rhs;
-  if (stage == 2) return 3. / 4. * phi0[n] + 1. / 4. * (phis[n] + dtau * rhs);
-  return 1. / 3. * phi0[n] + 2. / 3. * (phis[n] + dtau * rhs);
+  if (stage == 2) return TC(3. / 4.) * phi0[n] + TC(1. / 4.) * (phis[n] + dtau * rhs);
+  return TC(1. / 3.) * phi0[n] + TC(2. / 3.) * (phis[n] + dtau * rhs);
 }
 
 // One SSP-RK3 stage of ls_reinit over the tasks' regions; stage 3 folds
 // max|phi_new - phi_0| into the drop's residual.  out may equal phi0.
+template <typename T>
 __global__ void __launch_bounds__(NT, 2) k_reinit_stage(Params p, const __grid_constant__ LsBatch B, int stage,
-                                                     double dtau, ReinitState* __restrict__ rs) {
+                                                        double dtau_, ReinitState* __restrict__ rs) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  const T* phi0 = cT<T>(t.phi0);
+  T* out = mT<T>(t.out);
   if (rs[t.l].done) {
     // an iteration after convergence is the identity (levelset.f90:833-835)
     if (stage == 3 && c.ok && t.out != t.phi0)
-      for (int k = c.ka; k <= c.kb; ++k) putL(p, t.out, c.i, c.j, k, t.phi0[idxL(p, c.i, c.j, k)]);
+      for (int k = c.ka; k <= c.kb; ++k) putL(p, out, c.i, c.j, k, phi0[idxL(p, c.i, c.j, k)]);
     return;
   }
+  const T dtau = TC(dtau_);
   double r = 0.;
   if (c.ok) {
+    const T* phis = cT<T>(t.phis);
+    const T* orig = cT<T>(t.orig);
     const int i = c.i, j = c.j;
-    double v1 = 0., v2 = 0., vkm = 0., vk = 0.;
+    T v1 = TC(0.), v2 = TC(0.), vkm = TC(0.), vk = TC(0.);
     bool wall0 = false;
     for (int k = c.ka; k <= c.kb; ++k) {
       if (!computed(c, t.r, k)) {
-        putL(p, t.out, i, j, k, (k < 0 || k > p.k1) ? t.bgg : t.bg);
+        putL(p, out, i, j, k, (k < 0 || k > p.k1) ? TC(t.bgg) : TC(t.bg));
         continue;
       }
       if (k == 0) {
         wall0 = true;
         continue;
       }
-      double val;
+      T val;
       if (k == p.k1) {
-        val = 2. * vk - vkm;
+        val = TC(2.) * vk - vkm;
       } else {
-        val = reinit_val(p, stage, t.phi0, t.phis, t.orig, dtau, i, j, k);
+        val = reinit_val(p, stage, phi0, phis, orig, dtau, i, j, k);
         if (k == 1) v1 = val;
         if (k == 2) v2 = val;
         if (k == p.kmax - 1) vkm = val;
         if (k == p.kmax) vk = val;
       }
-      if (stage == 3) r = fmax(r, fabs(val - t.phi0[idxL(p, i, j, k)]));
-      putL(p, t.out, i, j, k, val);
+      if (stage == 3) r = fmax(r, (double)fabs(val - phi0[idxL(p, i, j, k)]));
+      putL(p, out, i, j, k, val);
       if (k == 2 && wall0) {
-        const double v0 = 2. * v1 - v2;
-        if (stage == 3) r = fmax(r, fabs(v0 - t.phi0[idxL(p, i, j, 0)]));
-        putL(p, t.out, i, j, 0, v0);
+        const T v0 = TC(2.) * v1 - v2;
+        if (stage == 3) r = fmax(r, (double)fabs(v0 - phi0[idxL(p, i, j, 0)]));
+        putL(p, out, i, j, 0, v0);
       }
     }
   }
@@ -409,22 +431,25 @@ __global__ void k_reinit_check(const __grid_constant__ LsBatch B, int it, int ma
 }
 
 // --------------------------------------------------------- Heaviside
-__device__ __forceinline__ double heav_trig(const Params& p, double phi, double eps) {
-  if (phi < -eps) return 0.;
-  if (phi < eps) return (.5 + .5 * phi / eps) + .5 / p.pi * sin(p.pi * phi / eps);
-  return 1.;
+template <typename T>
+__device__ __forceinline__ T heav_trig(const Params& p, T phi, T eps) {
+  if (phi < -eps) return TC(0.);
+  if (phi < eps) return (TC(.5) + TC(.5) * phi / eps) + TC(.5) / TC(p.pi) * sin(TC(p.pi) * phi / eps);
+  return TC(1.);
 }
-__device__ __forceinline__ double dirac_trig(const Params& p, double phi, double eps) {
-  if (phi < -eps) return 0.;
-  if (phi < eps) return .5 / eps + .5 / eps * cos(p.pi * phi / eps);
-  return 0.;
+template <typename T>
+__device__ __forceinline__ T dirac_trig(const Params& p, T phi, T eps) {
+  if (phi < -eps) return TC(0.);
+  if (phi < eps) return TC(.5) / eps + TC(.5) / eps * cos(TC(p.pi) * phi / eps);
+  return TC(0.);
 }
 
 // jiemian = min(jiemian, H_l) over the tasks' computed cells (shape-C
 // regions) and per-tile sums of H_l over their interior cells
-// (misc.f90:110-141).  jiemian starts at 1, the far-field value of H, so
-// only cells with H < 1 are touched; min is order-free, so drops may share
-// cells.  One chunk per tile: part[l*cap + tile] is deterministic.
+// (misc.f90:110-141), the sums in FP64.  jiemian starts at 1, the
+// far-field value of H, so only cells with H < 1 are touched; min is
+// order-free, so drops may share cells.  One chunk per tile:
+// part[l*cap + tile] is deterministic.
 __device__ __forceinline__ void min_into(double* a, double v) {
   unsigned long long* q = reinterpret_cast<unsigned long long*>(a);
   unsigned long long old = *q;
@@ -434,20 +459,31 @@ __device__ __forceinline__ void min_into(double* a, double v) {
     old = prev;
   }
 }
+__device__ __forceinline__ void min_into(float* a, float v) {
+  unsigned int* q = reinterpret_cast<unsigned int*>(a);
+  unsigned int old = *q;
+  while (v < __uint_as_float(old)) {
+    const unsigned int prev = atomicCAS(q, old, __float_as_uint(v));
+    if (prev == old) break;
+    old = prev;
+  }
+}
+template <typename T>
 __global__ void __launch_bounds__(NT) k_heaviside(Params p, const __grid_constant__ LsBatch B,
-                                                  double* __restrict__ jiemian, double* __restrict__ part, int cap) {
+                                                  T* __restrict__ jiemian, double* __restrict__ part, int cap) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
-  const double eps = 1.5 * p.dz;
+  const T eps = TC(1.5 * p.dz);
+  const T* phi = cT<T>(t.phi0);
   double s = 0.;
   if (c.ok && c.cxy) {
     const int i = c.i, j = c.j;
     const int ii = image_of<1>(i, p.imax), jj = image_of<1>(j, p.jmax);
     const int ka = max(c.ka, t.r.cz0), kb = min(c.kb, t.r.cz1);
     for (int k = ka; k <= kb; ++k) {
-      const double H = heav_trig(p, t.phi0[idxL(p, i, j, k)], eps);
-      if (H < 1.) {
+      const T H = heav_trig(p, phi[idxL(p, i, j, k)], eps);
+      if (H < TC(1.)) {
         min_into(jiemian + idxC(p, i, j, k), H);
         if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, j, k), H);
         if (jj != INT_MIN) {
@@ -455,7 +491,7 @@ __global__ void __launch_bounds__(NT) k_heaviside(Params p, const __grid_constan
           if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, jj, k), H);
         }
       }
-      if (k >= 1 && k <= p.kmax) s += H;
+      if (k >= 1 && k <= p.kmax) s += (double)H;
     }
   }
   const double bs = block_sum<double, NT>(s);
@@ -486,69 +522,73 @@ __global__ void k_volumes(Params p, const double* __restrict__ part, int cap, Pe
   }
 }
 
-__global__ void __launch_bounds__(NT) k_fill(double* __restrict__ a, long long n, double v) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_fill(T* __restrict__ a, long long n, double v) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-    a[q] = v;
+    a[q] = TC(v);
 }
 
 // miu, rho (shape C) and the face densities (misc.f90:121-172)
-__global__ void __launch_bounds__(NT) k_materials_final(Params p, const double* __restrict__ jiemian,
-                                                        double* __restrict__ miu, double* __restrict__ rho,
-                                                        double* __restrict__ rho_u, double* __restrict__ rho_v,
-                                                        double* __restrict__ rho_w) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_materials_final(Params p, const T* __restrict__ jiemian, T* __restrict__ miu,
+                                                        T* __restrict__ rho, T* __restrict__ rho_u,
+                                                        T* __restrict__ rho_v, T* __restrict__ rho_w) {
   const int r0[3] = {0, 0, 0}, r1[3] = {p.i1, p.j1, p.k1};
   int i, j, k;
   if (!cell3(r0, r1, i, j, k)) return;
   const long long n = idxC(p, i, j, k);
-  const double J0 = jiemian[n];
-  miu[n] = p.miu1 * J0 + p.miu2 * (1. - J0);
-  const double r0v = p.rho1 * J0 + p.rho2 * (1. - J0);
+  const T rho1 = TC(p.rho1), rho2 = TC(p.rho2);
+  const T J0 = jiemian[n];
+  miu[n] = TC(p.miu1) * J0 + TC(p.miu2) * (TC(1.) - J0);
+  const T r0v = rho1 * J0 + rho2 * (TC(1.) - J0);
   rho[n] = r0v;
   if (interior(p, i, j, k)) {
     const long long q = idxI(p, i, j, k);
     if (p.rho1 == p.rho2) {
-      rho_u[q] = p.rho1; rho_v[q] = p.rho1; rho_w[q] = p.rho1;
+      rho_u[q] = rho1; rho_v[q] = rho1; rho_w[q] = rho1;
     } else {
-      const double Jx = jiemian[n + 1], Jy = jiemian[n + p.nCx], Jz = jiemian[n + (long long)p.nCx * p.nCy];
-      const double rx = p.rho1 * Jx + p.rho2 * (1. - Jx);
-      const double ry = p.rho1 * Jy + p.rho2 * (1. - Jy);
-      const double rz = p.rho1 * Jz + p.rho2 * (1. - Jz);
-      rho_u[q] = (r0v + rx) / 2.;
-      rho_v[q] = (r0v + ry) / 2.;
-      rho_w[q] = (r0v + rz) / 2.;
+      const T Jx = jiemian[n + 1], Jy = jiemian[n + p.nCx], Jz = jiemian[n + (long long)p.nCx * p.nCy];
+      const T rx = rho1 * Jx + rho2 * (TC(1.) - Jx);
+      const T ry = rho1 * Jy + rho2 * (TC(1.) - Jy);
+      const T rz = rho1 * Jz + rho2 * (TC(1.) - Jz);
+      rho_u[q] = (r0v + rx) / TC(2.);
+      rho_v[q] = (r0v + ry) / TC(2.);
+      rho_w[q] = (r0v + rz) / TC(2.);
     }
   }
 }
 
 // ------------------------------------------------------------ inflation
 // dheav with boundp semantics over the task's shape-C region (one task),
-// the far-field value 1 on its apron, and per-tile area/volume sums over
-// its interior computed cells (levelset.f90:493-507, 525)
+// the far-field value 1 on its apron, and per-tile area/volume sums (FP64)
+// over its interior computed cells (levelset.f90:493-507, 525)
+template <typename T>
 __global__ void __launch_bounds__(NT) k_inflate_sums(Params p, const __grid_constant__ LsBatch B,
-                                                     const double* __restrict__ kappa,
-                                                     const double* __restrict__ nrm_m, double* __restrict__ dheav,
-                                                     double* __restrict__ part_area, double* __restrict__ part_heav) {
+                                                     const T* __restrict__ kappa, const T* __restrict__ nrm_m,
+                                                     T* __restrict__ dheav, double* __restrict__ part_area,
+                                                     double* __restrict__ part_heav) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
-  const double s1 = 1.5 * p.dz;
+  const T s1 = TC(1.5 * p.dz);
+  const T* phi = cT<T>(t.phi0);
   double sa = 0., sh = 0.;
   if (c.ok) {
     const int i = c.i, j = c.j;
     for (int k = c.ka; k <= c.kb; ++k) {
       if (!computed(c, t.r, k)) {
-        putC(p, dheav, i, j, k, 1.);
+        putC(p, dheav, i, j, k, TC(1.));
         continue;
       }
       const int K = k == 0 ? 1 : (k == p.k1 ? p.kmax : k);
-      putC(p, dheav, i, j, k, heav_trig(p, t.phi0[idxL(p, i, j, K)], s1));
+      putC(p, dheav, i, j, k, heav_trig(p, phi[idxL(p, i, j, K)], s1));
       if (k >= 1 && k <= p.kmax) {
-        const double ph = t.phi0[idxL(p, i, j, k)];
-        const double H = heav_trig(p, ph, s1);
-        const double del = dirac_trig(p, ph, s1);
-        const double m = nrm_m[idxI(p, i, j, k)];
-        sa += p.ispeed_curv ? (del * kappa[idxC(p, i, j, k)]) * m : del * m;
-        sh += H;
+        const T ph = phi[idxL(p, i, j, k)];
+        const T H = heav_trig(p, ph, s1);
+        const T del = dirac_trig(p, ph, s1);
+        const T m = nrm_m[idxI(p, i, j, k)];
+        sa += (double)(p.ispeed_curv ? (del * kappa[idxC(p, i, j, k)]) * m : del * m);
+        sh += (double)H;
       }
     }
   }
@@ -583,36 +623,36 @@ __global__ void k_inflate_final(Params p, const double* __restrict__ part_area,
 
 // u_lc, v_lc, w_lc of levelset.f90:527-548, with u_l,v_l,w_l of 530-532
 // after bounduvw evaluated on the fly; computed interior cells of r
-__device__ __forceinline__ double infl_face(const Params& p, const double* __restrict__ dheav, double temp,
-                                            int axis, int i, int j, int k) {
+template <typename T>
+__device__ __forceinline__ T infl_face(const Params& p, const T* __restrict__ dheav, T temp, int axis, int i, int j,
+                                       int k) {
   const long long n = idxC(p, i, j, k);
   if (axis == 0) return -divx(p, temp * (dheav[n + 1] - dheav[n]));
   if (axis == 1) return -divy(p, temp * (dheav[n + p.nCx] - dheav[n]));
   return -divz(p, temp * (dheav[n + (long long)p.nCx * p.nCy] - dheav[n]));
 }
+template <typename T>
 __global__ void __launch_bounds__(NT) k_inflate_vel(Params p, const __grid_constant__ LsBatch B,
-                                                    const double* __restrict__ dheav,
-                                                    const double* __restrict__ kappa,
-                                                    const DevScalars* __restrict__ dsc,
-                                                    double* __restrict__ ulc, double* __restrict__ vlc,
-                                                    double* __restrict__ wlc) {
+                                                    const T* __restrict__ dheav, const T* __restrict__ kappa,
+                                                    const DevScalars* __restrict__ dsc, T* __restrict__ ulc,
+                                                    T* __restrict__ vlc, T* __restrict__ wlc) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
   if (!c.ok || !c.cxy) return;
   const int i = c.i, j = c.j;
-  const double temp = dsc->inflate_temp;
+  const T temp = TC(dsc->inflate_temp);
   for (int k = max(c.ka, max(t.r.cz0, 1)); k <= min(c.kb, min(t.r.cz1, p.kmax)); ++k) {
     const long long q = idxI(p, i, j, k);
-    const double ul_m = infl_face(p, dheav, temp, 0, wrapx(p, i - 1), j, k);
-    const double ul_0 = infl_face(p, dheav, temp, 0, i, j, k);
-    const double vl_m = infl_face(p, dheav, temp, 1, i, wrapy(p, j - 1), k);
-    const double vl_0 = infl_face(p, dheav, temp, 1, i, j, k);
-    const double wl_m = (k == 1) ? 0. : infl_face(p, dheav, temp, 2, i, j, k - 1);
-    const double wl_0 = (k == p.kmax) ? 0. : infl_face(p, dheav, temp, 2, i, j, k);
-    double a = (ul_m + ul_0) / 2., b = (vl_m + vl_0) / 2., cc = (wl_m + wl_0) / 2.;
+    const T ul_m = infl_face(p, dheav, temp, 0, wrapx(p, i - 1), j, k);
+    const T ul_0 = infl_face(p, dheav, temp, 0, i, j, k);
+    const T vl_m = infl_face(p, dheav, temp, 1, i, wrapy(p, j - 1), k);
+    const T vl_0 = infl_face(p, dheav, temp, 1, i, j, k);
+    const T wl_m = (k == 1) ? TC(0.) : infl_face(p, dheav, temp, 2, i, j, k - 1);
+    const T wl_0 = (k == p.kmax) ? TC(0.) : infl_face(p, dheav, temp, 2, i, j, k);
+    T a = (ul_m + ul_0) / TC(2.), b = (vl_m + vl_0) / TC(2.), cc = (wl_m + wl_0) / TC(2.);
     if (p.ispeed_curv) {
-      const double kp = kappa[idxC(p, i, j, k)];
+      const T kp = kappa[idxC(p, i, j, k)];
       a = a * kp; b = b * kp; cc = cc * kp;
     }
     ulc[q] = a; vlc[q] = b; wlc[q] = cc;
@@ -622,7 +662,8 @@ __global__ void __launch_bounds__(NT) k_inflate_vel(Params p, const __grid_const
 // boundmls, extrap='line' (bound.f90:518-~657): three wall layers by
 // repeated linear extrapolation from the interior column, then the periodic
 // copies.  Reads only interior cells, writes only the others.
-__global__ void __launch_bounds__(NT) k_boundmls(Params p, double* __restrict__ y) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_boundmls(Params p, T* __restrict__ y) {
   const int r0[3] = {-2, -2, -2}, r1[3] = {p.i1 + 2, p.j1 + 2, p.k1 + 2};
   int i, j, k;
   if (!cell3(r0, r1, i, j, k)) return;
@@ -633,33 +674,47 @@ __global__ void __launch_bounds__(NT) k_boundmls(Params p, double* __restrict__ 
     return;
   }
   if (k <= 0) {
-    const double y1 = y[idxL(p, I, J, 1)], y2 = y[idxL(p, I, J, 2)];
-    const double y0 = 2. * y1 - y2;
-    const double ym1 = 2. * y0 - y1;
-    const double ym2 = 2. * ym1 - y0;
+    const T y1 = y[idxL(p, I, J, 1)], y2 = y[idxL(p, I, J, 2)];
+    const T y0 = TC(2.) * y1 - y2;
+    const T ym1 = TC(2.) * y0 - y1;
+    const T ym2 = TC(2.) * ym1 - y0;
     y[n] = (k == 0) ? y0 : (k == -1 ? ym1 : ym2);
   } else {
-    const double yk = y[idxL(p, I, J, p.kmax)], ykm = y[idxL(p, I, J, p.kmax - 1)];
-    const double y0 = 2. * yk - ykm;
-    const double yp1 = 2. * y0 - yk;
-    const double yp2 = 2. * yp1 - y0;
+    const T yk = y[idxL(p, I, J, p.kmax)], ykm = y[idxL(p, I, J, p.kmax - 1)];
+    const T y0 = TC(2.) * yk - ykm;
+    const T yp1 = TC(2.) * y0 - yk;
+    const T yp2 = TC(2.) * yp1 - y0;
     y[n] = (k == p.k1) ? y0 : (k == p.k1 + 1 ? yp1 : yp2);
   }
 }
 
 // far-field value into every cell outside the written cells of r (makes a
 // drop's stored array valid everywhere, e.g. before a download)
-__global__ void __launch_bounds__(NT) k_materialize(Params p, Region r, double bg, double bgg, double* __restrict__ y) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_materialize(Params p, Region r, double bg, double bgg, T* __restrict__ y) {
   const int r0[3] = {-2, -2, -2}, r1[3] = {p.i1 + 2, p.j1 + 2, p.k1 + 2};
   int i, j, k;
   if (!cell3(r0, r1, i, j, k)) return;
-  if (!in_written(p, r, i, j, k)) y[idxL(p, i, j, k)] = (k < 0 || k > p.k1) ? bgg : bg;
+  if (!in_written(p, r, i, j, k)) y[idxL(p, i, j, k)] = (k < 0 || k > p.k1) ? TC(bgg) : TC(bg);
 }
 
-__global__ void k_copy(double* __restrict__ dst, const double* __restrict__ src, long long n) {
+template <typename T>
+__global__ void k_copy(T* __restrict__ dst, const T* __restrict__ src, long long n) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
     dst[q] = src[q];
 }
+
+// field conversions of the precision form (upload / download)
+__global__ void k_to_float(float* __restrict__ dst, const double* __restrict__ src, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    dst[q] = (float)src[q];
+}
+__global__ void k_to_double(double* __restrict__ dst, const float* __restrict__ src, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    dst[q] = (double)src[q];
+}
+
+#undef TC
 
 }  // namespace
 
@@ -742,26 +797,49 @@ void set_tiles(LsBatch& b, int kc) {
 }
 
 // ================================================================ launchers
+// Each launcher picks the field type of the context's form.
+#define BY_FORM(c, call_f32, call_f64) \
+  do {                                  \
+    if ((c).P.f32) {                    \
+      call_f32;                         \
+    } else {                            \
+      call_f64;                         \
+    }                                   \
+  } while (0)
+
 void launch_tube(Ctx& c, const LsBatch& b) {
   if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "tube", 1);
-  k_tube<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.d_nbcnt, c.d_bbox, c.d_bbox + 5 * c.P.L);
+  int* lo = c.d_bbox;
+  int* hi = c.d_bbox + 5 * c.P.L;
+  BY_FORM(c, (k_tube<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.d_nbcnt, lo, hi)),
+          (k_tube<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.d_nbcnt, lo, hi)));
 }
 
+template <typename T>
+void adv_launch(Ctx& c, const LsBatch& b, int scheme, int stage1, double a, double bb, double fdt, const double* vu,
+                const double* vv, const double* vw) {
+  const T* u = reinterpret_cast<const T*>(vu);
+  const T* v = reinterpret_cast<const T*>(vv);
+  const T* w = reinterpret_cast<const T*>(vw);
+  if (scheme == ICLS_HOUC5)
+    k_adv_stage<ICLS_HOUC5, T><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
+  else
+    k_adv_stage<ICLS_WENO5, T><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
+}
 void launch_adv_stage(Ctx& c, const LsBatch& b, int scheme, int stage1, double a, double bb, double fdt,
                       const double* vu, const double* vv, const double* vw) {
   if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "adv_stage", 1);
-  if (scheme == ICLS_HOUC5)
-    k_adv_stage<ICLS_HOUC5><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, vu, vv, vw);
-  else
-    k_adv_stage<ICLS_WENO5><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, vu, vv, vw);
+  BY_FORM(c, adv_launch<float>(c, b, scheme, stage1, a, bb, fdt, vu, vv, vw),
+          adv_launch<double>(c, b, scheme, stage1, a, bb, fdt, vu, vv, vw));
 }
 
 void launch_reinit_stage(Ctx& c, const LsBatch& b, int stage, double dtau) {
   if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "reinit_stage", 1);
-  k_reinit_stage<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs);
+  BY_FORM(c, (k_reinit_stage<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs)),
+          (k_reinit_stage<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs)));
 }
 void launch_reinit_reset(Ctx& c, const LsBatch& b, int maxiter) {
   if (b.n == 0) return;
@@ -777,12 +855,19 @@ void launch_reinit_check(Ctx& c, const LsBatch& b, int it, int maxiter, double t
 void launch_heaviside(Ctx& c, const LsBatch& b) {
   if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "heaviside", 1);
-  k_heaviside<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.jiemian, c.hpart, c.red_cap);
+  BY_FORM(c,
+          (k_heaviside<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, reinterpret_cast<float*>(c.jiemian), c.hpart,
+                                                                c.red_cap)),
+          (k_heaviside<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.jiemian, c.hpart, c.red_cap)));
 }
 
-void launch_fill(Ctx& c, double* a, long long n, double v) {
+// n elements of a; tfield: a holds the form's field type (else FP64)
+void launch_fill(Ctx& c, double* a, long long n, double v, bool tfield) {
   Scope sc_(c.prof, c.s, "fill", 1);
-  k_fill<<<1184, NT, 0, c.s>>>(a, n, v);
+  if (tfield && c.P.f32)
+    k_fill<float><<<1184, NT, 0, c.s>>>(reinterpret_cast<float*>(a), n, v);
+  else
+    k_fill<double><<<1184, NT, 0, c.s>>>(a, n, v);
 }
 
 // outside/ntiles: per drop (null: every drop swept its whole grid)
@@ -796,7 +881,14 @@ void launch_materials_final(Ctx& c, const double* outside, const int* ntiles) {
   }
   k_volumes<<<1, 256, 0, c.s>>>(c.P, c.hpart, c.red_cap, o, uniform, c.dvol, c.dsc);
   const int r0[3] = {0, 0, 0}, r1[3] = {c.P.i1, c.P.j1, c.P.k1};
-  k_materials_final<<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, c.jiemian, c.miu, c.rho, c.rho_u, c.rho_v, c.rho_w);
+  if (c.P.f32) {
+    auto f = [](double* q) { return reinterpret_cast<float*>(q); };
+    k_materials_final<float><<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, f(c.jiemian), f(c.miu), f(c.rho), f(c.rho_u),
+                                                                   f(c.rho_v), f(c.rho_w));
+  } else {
+    k_materials_final<double><<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, c.jiemian, c.miu, c.rho, c.rho_u, c.rho_v,
+                                                                    c.rho_w);
+  }
 }
 
 // b: one task (shape-C region of the drop, apron 1), phi0 = its level set
@@ -804,7 +896,12 @@ void launch_inflate_sums(Ctx& c, const LsBatch& b, double outside) {
   Scope sc_(c.prof, c.s, "inflate_sums", 2);
   double* pa = c.hpart;
   double* ph = c.hpart + c.red_cap;
-  k_inflate_sums<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.kappa, c.nrm_m, c.dheav, pa, ph);
+  if (c.P.f32) {
+    auto f = [](double* q) { return reinterpret_cast<float*>(q); };
+    k_inflate_sums<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, f(c.kappa), f(c.nrm_m), f(c.dheav), pa, ph);
+  } else {
+    k_inflate_sums<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.kappa, c.nrm_m, c.dheav, pa, ph);
+  }
   k_inflate_final<<<1, 32, 0, c.s>>>(c.P, pa, ph, b.start[b.n], b.t[0].l, (double)c.cfg.inflate_step * c.dt, outside,
                                      c.dvol, c.dvol0, c.dmaxchk, c.dsc);
 }
@@ -812,24 +909,40 @@ void launch_inflate_sums(Ctx& c, const LsBatch& b, double outside) {
 // b: one task (shape-C region of the drop, apron 0)
 void launch_inflate_vel(Ctx& c, const LsBatch& b) {
   Scope sc_(c.prof, c.s, "inflate_vel", 1);
-  k_inflate_vel<<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.dheav, c.kappa, c.dsc, c.ulc, c.vlc, c.wlc);
+  if (c.P.f32) {
+    auto f = [](double* q) { return reinterpret_cast<float*>(q); };
+    k_inflate_vel<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, f(c.dheav), f(c.kappa), c.dsc, f(c.ulc), f(c.vlc),
+                                                           f(c.wlc));
+  } else {
+    k_inflate_vel<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.dheav, c.kappa, c.dsc, c.ulc, c.vlc, c.wlc);
+  }
 }
 
 void launch_boundmls(Ctx& c, double* phi) {
   Scope sc_(c.prof, c.s, "boundmls", 1);
   const int r0[3] = {-2, -2, -2}, r1[3] = {c.P.i1 + 2, c.P.j1 + 2, c.P.k1 + 2};
-  k_boundmls<<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, phi);
+  BY_FORM(c, (k_boundmls<float><<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, reinterpret_cast<float*>(phi))),
+          (k_boundmls<double><<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, phi)));
 }
 
 void launch_materialize(Ctx& c, const Region& r, double bg, double bgg, double* phi) {
   Scope sc_(c.prof, c.s, "materialize", 1);
   const int r0[3] = {-2, -2, -2}, r1[3] = {c.P.i1 + 2, c.P.j1 + 2, c.P.k1 + 2};
-  k_materialize<<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, r, bg, bgg, phi);
+  BY_FORM(c,
+          (k_materialize<float><<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, r, bg, bgg, reinterpret_cast<float*>(phi))),
+          (k_materialize<double><<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, r, bg, bgg, phi)));
 }
 
 void launch_copy(Ctx& c, double* dst, const double* src, long long n) {
   Scope sc_(c.prof, c.s, "copy", 1);
-  k_copy<<<1184, 256, 0, c.s>>>(dst, src, n);
+  k_copy<double><<<1184, 256, 0, c.s>>>(dst, src, n);
+}
+
+void launch_to_float(Ctx& c, double* dst_f32, const double* src, long long n) {
+  k_to_float<<<1184, 256, 0, c.s>>>(reinterpret_cast<float*>(dst_f32), src, n);
+}
+void launch_to_double(Ctx& c, double* dst, const double* src_f32, long long n) {
+  k_to_double<<<1184, 256, 0, c.s>>>(dst, reinterpret_cast<const float*>(src_f32), n);
 }
 
 }  // namespace icls

@@ -22,6 +22,9 @@ namespace icls {
 namespace {
 
 constexpr int NT = 256;
+// T is the form's field type (double, or float in the precision form);
+// TC(x) is the constant x in T
+#define TC(x) static_cast<T>(x)
 inline unsigned nblocks(long long n, int nt = NT) { return (unsigned)((n + nt - 1) / nt); }
 
 __device__ __forceinline__ void decodeI(const Params& p, int q, int& i, int& j, int& k) {
@@ -56,127 +59,129 @@ struct MomArgs {
 // ---- RHS of mom_main for one component ----------------------------------
 // U(di,dj,dk) returns u at (i+di, j+dj, k+dk), likewise V, W and M (miu):
 // the same expressions serve the shared-memory march of k_ab2 and the
-// global-memory k_mom_main.
-template <class FU, class FV, class FW, class FM>
-__device__ __forceinline__ double rhs_u(const Params& p, const FU& U, const FV& V, const FW& W, const FM& M,
-                                        double rho_u, double rho_avr) {
-  double RCu = 0.;
+// global-memory k_mom_main.  T is the form's field type; TC(x) the
+// constant x in T.
+template <typename T, class FU, class FV, class FW, class FM>
+__device__ __forceinline__ T rhs_u(const Params& p, const FU& U, const FV& V, const FW& W, const FM& M,
+                                        T rho_u, T rho_avr) {
+  T RCu = TC(0.);
   if (!p.TwoD) {
-    double uuip = 0.25 * (U(1, 0, 0) + U(0, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
-    double uuim = 0.25 * (U(-1, 0, 0) + U(0, 0, 0)) * (U(-1, 0, 0) + U(0, 0, 0));
-    double uvjp = 0.25 * (U(0, 1, 0) + U(0, 0, 0)) * (V(1, 0, 0) + V(0, 0, 0));
-    double uvjm = 0.25 * (U(0, -1, 0) + U(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
-    double uwkp = 0.25 * (U(0, 0, 1) + U(0, 0, 0)) * (W(1, 0, 0) + W(0, 0, 0));
-    double uwkm = 0.25 * (U(0, 0, -1) + U(0, 0, 0)) * (W(1, 0, -1) + W(0, 0, -1));
+    T uuip = TC(0.25) * (U(1, 0, 0) + U(0, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
+    T uuim = TC(0.25) * (U(-1, 0, 0) + U(0, 0, 0)) * (U(-1, 0, 0) + U(0, 0, 0));
+    T uvjp = TC(0.25) * (U(0, 1, 0) + U(0, 0, 0)) * (V(1, 0, 0) + V(0, 0, 0));
+    T uvjm = TC(0.25) * (U(0, -1, 0) + U(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
+    T uwkp = TC(0.25) * (U(0, 0, 1) + U(0, 0, 0)) * (W(1, 0, 0) + W(0, 0, 0));
+    T uwkm = TC(0.25) * (U(0, 0, -1) + U(0, 0, 0)) * (W(1, 0, -1) + W(0, 0, -1));
     RCu = (divx(p, (-uuip + uuim)) + divy(p, (-uvjp + uvjm))) + divz(p, (-uwkp + uwkm));
   }
-  double RDu = 0.;
+  T RDu = TC(0.);
   if (!p.TwoD) {
-    double dudxp = divx(p, (U(1, 0, 0) - U(0, 0, 0)));
-    double dudxm = divx(p, (U(0, 0, 0) - U(-1, 0, 0)));
-    double dudyp = divy(p, (U(0, 1, 0) - U(0, 0, 0)));
-    double dudym = divy(p, (U(0, 0, 0) - U(0, -1, 0)));
-    double dvdxp = divx(p, (V(1, 0, 0) - V(0, 0, 0)));
-    double dvdxm = divx(p, (V(1, -1, 0) - V(0, -1, 0)));
-    double dudzp = divz(p, (U(0, 0, 1) - U(0, 0, 0)));
-    double dudzm = divz(p, (U(0, 0, 0) - U(0, 0, -1)));
-    double dwdxp = divx(p, (W(1, 0, 0) - W(0, 0, 0)));
-    double dwdxm = divx(p, (W(1, 0, -1) - W(0, 0, -1)));
-    double ma1 = 0.25 * (((M(0, 0, 0) + M(0, -1, 0)) + M(1, -1, 0)) + M(1, 0, 0));
-    double ma2 = 0.25 * (((M(0, 0, 0) + M(0, 1, 0)) + M(1, 1, 0)) + M(1, 0, 0));
-    double ma3 = 0.25 * (((M(0, 0, 0) + M(0, 0, -1)) + M(1, 0, -1)) + M(1, 0, 0));
-    double ma4 = 0.25 * (((M(0, 0, 0) + M(0, 0, 1)) + M(1, 0, 1)) + M(1, 0, 0));
-    double RD1 = divx(p, 2. * (dudxp * M(1, 0, 0) - dudxm * M(0, 0, 0)));
-    double RD2 = divy(p, (dudyp * ma2 - dudym * ma1));
-    double RD3 = divy(p, (dvdxp * ma2 - dvdxm * ma1));
-    double RD4 = divz(p, (dudzp * ma4 - dudzm * ma3));
-    double RD5 = divz(p, (dwdxp * ma4 - dwdxm * ma3));
+    T dudxp = divx(p, (U(1, 0, 0) - U(0, 0, 0)));
+    T dudxm = divx(p, (U(0, 0, 0) - U(-1, 0, 0)));
+    T dudyp = divy(p, (U(0, 1, 0) - U(0, 0, 0)));
+    T dudym = divy(p, (U(0, 0, 0) - U(0, -1, 0)));
+    T dvdxp = divx(p, (V(1, 0, 0) - V(0, 0, 0)));
+    T dvdxm = divx(p, (V(1, -1, 0) - V(0, -1, 0)));
+    T dudzp = divz(p, (U(0, 0, 1) - U(0, 0, 0)));
+    T dudzm = divz(p, (U(0, 0, 0) - U(0, 0, -1)));
+    T dwdxp = divx(p, (W(1, 0, 0) - W(0, 0, 0)));
+    T dwdxm = divx(p, (W(1, 0, -1) - W(0, 0, -1)));
+    T ma1 = TC(0.25) * (((M(0, 0, 0) + M(0, -1, 0)) + M(1, -1, 0)) + M(1, 0, 0));
+    T ma2 = TC(0.25) * (((M(0, 0, 0) + M(0, 1, 0)) + M(1, 1, 0)) + M(1, 0, 0));
+    T ma3 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, -1)) + M(1, 0, -1)) + M(1, 0, 0));
+    T ma4 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, 1)) + M(1, 0, 1)) + M(1, 0, 0));
+    T RD1 = divx(p, TC(2.) * (dudxp * M(1, 0, 0) - dudxm * M(0, 0, 0)));
+    T RD2 = divy(p, (dudyp * ma2 - dudym * ma1));
+    T RD3 = divy(p, (dvdxp * ma2 - dvdxm * ma1));
+    T RD4 = divz(p, (dudzp * ma4 - dudzm * ma3));
+    T RD5 = divz(p, (dwdxp * ma4 - dwdxm * ma3));
     RDu = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rho_u;
   }
-  double RGu = p.TwoD ? 0. : p.iFr * (1. - rho_avr / rho_u) * p.g1;
-  return (RCu + RDu * p.visc) + RGu;
+  T RGu = p.TwoD ? TC(0.) : TC(p.iFr) * (TC(1.) - rho_avr / rho_u) * TC(p.g1);
+  return (RCu + RDu * TC(p.visc)) + RGu;
 }
 
-template <class FU, class FV, class FW, class FM>
-__device__ __forceinline__ double rhs_v(const Params& p, const FU& U, const FV& V, const FW& W, const FM& M,
-                                        double rv, double rho_avr) {
-  double uvip = 0.25 * (U(0, 0, 0) + U(0, 1, 0)) * (V(0, 0, 0) + V(1, 0, 0));
-  double uvim = 0.25 * (U(-1, 0, 0) + U(-1, 1, 0)) * (V(0, 0, 0) + V(-1, 0, 0));
-  double vvjp = 0.25 * (V(0, 0, 0) + V(0, 1, 0)) * (V(0, 0, 0) + V(0, 1, 0));
-  double vvjm = 0.25 * (V(0, 0, 0) + V(0, -1, 0)) * (V(0, 0, 0) + V(0, -1, 0));
-  double wvkp = 0.25 * (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 1) + V(0, 0, 0));
-  double wvkm = 0.25 * (W(0, 0, -1) + W(0, 1, -1)) * (V(0, 0, -1) + V(0, 0, 0));
-  double RCv = (divx(p, (-uvip + uvim)) + divy(p, (-vvjp + vvjm))) + divz(p, (-wvkp + wvkm));
-  double dvdxp = divx(p, (V(1, 0, 0) - V(0, 0, 0)));
-  double dvdxm = divx(p, (V(0, 0, 0) - V(-1, 0, 0)));
-  double dudyp = divy(p, (U(0, 1, 0) - U(0, 0, 0)));
-  double dudym = divy(p, (U(-1, 1, 0) - U(-1, 0, 0)));
-  double dvdyp = divy(p, (V(0, 1, 0) - V(0, 0, 0)));
-  double dvdym = divy(p, (V(0, 0, 0) - V(0, -1, 0)));
-  double dvdzp = divz(p, (V(0, 0, 1) - V(0, 0, 0)));
-  double dvdzm = divz(p, (V(0, 0, 0) - V(0, 0, -1)));
-  double dwdyp = divy(p, (W(0, 1, 0) - W(0, 0, 0)));
-  double dwdym = divy(p, (W(0, 1, -1) - W(0, 0, -1)));
-  double ma2 = 0.25 * (((M(0, 0, 0) + M(0, 1, 0)) + M(1, 1, 0)) + M(1, 0, 0));
-  double ma5 = 0.25 * (((M(0, 0, 0) + M(0, 1, 0)) + M(-1, 1, 0)) + M(-1, 0, 0));
-  double ma6 = 0.25 * (((M(0, 0, 0) + M(0, 0, -1)) + M(0, 1, -1)) + M(0, 1, 0));
-  double ma7 = 0.25 * (((M(0, 0, 0) + M(0, 0, 1)) + M(0, 1, 1)) + M(0, 1, 0));
-  double RD1 = divx(p, (dvdxp * ma2 - dvdxm * ma5));
-  double RD2 = divx(p, (dudyp * ma2 - dudym * ma5));
-  double RD3 = divy(p, 2. * (dvdyp * M(0, 1, 0) - dvdym * M(0, 0, 0)));
-  double RD4 = divz(p, (dvdzp * ma7 - dvdzm * ma6));
-  double RD5 = divz(p, (dwdyp * ma7 - dwdym * ma6));
-  double RDv = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rv;
-  double RGv = p.iFr * (1. - rho_avr / rv) * p.g2;
-  return (RCv + RDv * p.visc) + RGv;
+template <typename T, class FU, class FV, class FW, class FM>
+__device__ __forceinline__ T rhs_v(const Params& p, const FU& U, const FV& V, const FW& W, const FM& M,
+                                        T rv, T rho_avr) {
+  T uvip = TC(0.25) * (U(0, 0, 0) + U(0, 1, 0)) * (V(0, 0, 0) + V(1, 0, 0));
+  T uvim = TC(0.25) * (U(-1, 0, 0) + U(-1, 1, 0)) * (V(0, 0, 0) + V(-1, 0, 0));
+  T vvjp = TC(0.25) * (V(0, 0, 0) + V(0, 1, 0)) * (V(0, 0, 0) + V(0, 1, 0));
+  T vvjm = TC(0.25) * (V(0, 0, 0) + V(0, -1, 0)) * (V(0, 0, 0) + V(0, -1, 0));
+  T wvkp = TC(0.25) * (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 1) + V(0, 0, 0));
+  T wvkm = TC(0.25) * (W(0, 0, -1) + W(0, 1, -1)) * (V(0, 0, -1) + V(0, 0, 0));
+  T RCv = (divx(p, (-uvip + uvim)) + divy(p, (-vvjp + vvjm))) + divz(p, (-wvkp + wvkm));
+  T dvdxp = divx(p, (V(1, 0, 0) - V(0, 0, 0)));
+  T dvdxm = divx(p, (V(0, 0, 0) - V(-1, 0, 0)));
+  T dudyp = divy(p, (U(0, 1, 0) - U(0, 0, 0)));
+  T dudym = divy(p, (U(-1, 1, 0) - U(-1, 0, 0)));
+  T dvdyp = divy(p, (V(0, 1, 0) - V(0, 0, 0)));
+  T dvdym = divy(p, (V(0, 0, 0) - V(0, -1, 0)));
+  T dvdzp = divz(p, (V(0, 0, 1) - V(0, 0, 0)));
+  T dvdzm = divz(p, (V(0, 0, 0) - V(0, 0, -1)));
+  T dwdyp = divy(p, (W(0, 1, 0) - W(0, 0, 0)));
+  T dwdym = divy(p, (W(0, 1, -1) - W(0, 0, -1)));
+  T ma2 = TC(0.25) * (((M(0, 0, 0) + M(0, 1, 0)) + M(1, 1, 0)) + M(1, 0, 0));
+  T ma5 = TC(0.25) * (((M(0, 0, 0) + M(0, 1, 0)) + M(-1, 1, 0)) + M(-1, 0, 0));
+  T ma6 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, -1)) + M(0, 1, -1)) + M(0, 1, 0));
+  T ma7 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, 1)) + M(0, 1, 1)) + M(0, 1, 0));
+  T RD1 = divx(p, (dvdxp * ma2 - dvdxm * ma5));
+  T RD2 = divx(p, (dudyp * ma2 - dudym * ma5));
+  T RD3 = divy(p, TC(2.) * (dvdyp * M(0, 1, 0) - dvdym * M(0, 0, 0)));
+  T RD4 = divz(p, (dvdzp * ma7 - dvdzm * ma6));
+  T RD5 = divz(p, (dwdyp * ma7 - dwdym * ma6));
+  T RDv = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rv;
+  T RGv = TC(p.iFr) * (TC(1.) - rho_avr / rv) * TC(p.g2);
+  return (RCv + RDv * TC(p.visc)) + RGv;
 }
 
-template <class FU, class FV, class FW, class FM>
-__device__ __forceinline__ double rhs_w(const Params& p, const FU& U, const FV& V, const FW& W, const FM& M,
-                                        double rw, double rho_avr) {
-  double uwip = 0.25 * (W(0, 0, 0) + W(1, 0, 0)) * (U(0, 0, 0) + U(0, 0, 1));
-  double uwim = 0.25 * (W(0, 0, 0) + W(-1, 0, 0)) * (U(-1, 0, 0) + U(-1, 0, 1));
-  double vwjp = 0.25 * (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 0) + V(0, 0, 1));
-  double vwjm = 0.25 * (W(0, 0, 0) + W(0, -1, 0)) * (V(0, -1, 0) + V(0, -1, 1));
-  double wwkp = 0.25 * (W(0, 0, 0) + W(0, 0, 1)) * (W(0, 0, 0) + W(0, 0, 1));
-  double wwkm = 0.25 * (W(0, 0, 0) + W(0, 0, -1)) * (W(0, 0, 0) + W(0, 0, -1));
-  double RCw = (divx(p, (-uwip + uwim)) + divy(p, (-vwjp + vwjm))) + divz(p, (-wwkp + wwkm));
-  double dwdxp = divx(p, (W(1, 0, 0) - W(0, 0, 0)));
-  double dwdxm = divx(p, (W(0, 0, 0) - W(-1, 0, 0)));
-  double dudzp = divz(p, (U(0, 0, 1) - U(0, 0, 0)));
-  double dudzm = divz(p, (U(-1, 0, 1) - U(-1, 0, 0)));
-  double dwdyp = divy(p, (W(0, 1, 0) - W(0, 0, 0)));
-  double dwdym = divy(p, (W(0, 0, 0) - W(0, -1, 0)));
-  double dvdzp = divz(p, (V(0, 0, 1) - V(0, 0, 0)));
-  double dvdzm = divz(p, (V(0, -1, 1) - V(0, -1, 0)));
-  double dwdzp = divz(p, (W(0, 0, 1) - W(0, 0, 0)));
-  double dwdzm = divz(p, (W(0, 0, 0) - W(0, 0, -1)));
-  double ma4 = 0.25 * (((M(0, 0, 0) + M(0, 0, 1)) + M(1, 0, 1)) + M(1, 0, 0));
-  double ma8 = 0.25 * (((M(0, 0, 0) + M(0, 0, 1)) + M(-1, 0, 1)) + M(-1, 0, 0));
-  double ma7 = 0.25 * (((M(0, 0, 0) + M(0, 0, 1)) + M(0, 1, 1)) + M(0, 1, 0));
-  double ma9 = 0.25 * (((M(0, 0, 0) + M(0, 0, 1)) + M(0, -1, 1)) + M(0, -1, 0));
-  double RD1 = divx(p, (dwdxp * ma4 - dwdxm * ma8));
-  double RD2 = divx(p, (dudzp * ma4 - dudzm * ma8));
-  double RD3 = divy(p, (dwdyp * ma7 - dwdym * ma9));
-  double RD4 = divy(p, (dvdzp * ma7 - dvdzm * ma9));
-  double RD5 = divz(p, 2. * (dwdzp * M(0, 0, 1) - dwdzm * M(0, 0, 0)));
-  double RDw = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rw;
-  double RGw = p.iFr * (1. - rho_avr / rw) * p.g3;
-  return (RCw + RDw * p.visc) + RGw;
+template <typename T, class FU, class FV, class FW, class FM>
+__device__ __forceinline__ T rhs_w(const Params& p, const FU& U, const FV& V, const FW& W, const FM& M,
+                                        T rw, T rho_avr) {
+  T uwip = TC(0.25) * (W(0, 0, 0) + W(1, 0, 0)) * (U(0, 0, 0) + U(0, 0, 1));
+  T uwim = TC(0.25) * (W(0, 0, 0) + W(-1, 0, 0)) * (U(-1, 0, 0) + U(-1, 0, 1));
+  T vwjp = TC(0.25) * (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 0) + V(0, 0, 1));
+  T vwjm = TC(0.25) * (W(0, 0, 0) + W(0, -1, 0)) * (V(0, -1, 0) + V(0, -1, 1));
+  T wwkp = TC(0.25) * (W(0, 0, 0) + W(0, 0, 1)) * (W(0, 0, 0) + W(0, 0, 1));
+  T wwkm = TC(0.25) * (W(0, 0, 0) + W(0, 0, -1)) * (W(0, 0, 0) + W(0, 0, -1));
+  T RCw = (divx(p, (-uwip + uwim)) + divy(p, (-vwjp + vwjm))) + divz(p, (-wwkp + wwkm));
+  T dwdxp = divx(p, (W(1, 0, 0) - W(0, 0, 0)));
+  T dwdxm = divx(p, (W(0, 0, 0) - W(-1, 0, 0)));
+  T dudzp = divz(p, (U(0, 0, 1) - U(0, 0, 0)));
+  T dudzm = divz(p, (U(-1, 0, 1) - U(-1, 0, 0)));
+  T dwdyp = divy(p, (W(0, 1, 0) - W(0, 0, 0)));
+  T dwdym = divy(p, (W(0, 0, 0) - W(0, -1, 0)));
+  T dvdzp = divz(p, (V(0, 0, 1) - V(0, 0, 0)));
+  T dvdzm = divz(p, (V(0, -1, 1) - V(0, -1, 0)));
+  T dwdzp = divz(p, (W(0, 0, 1) - W(0, 0, 0)));
+  T dwdzm = divz(p, (W(0, 0, 0) - W(0, 0, -1)));
+  T ma4 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, 1)) + M(1, 0, 1)) + M(1, 0, 0));
+  T ma8 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, 1)) + M(-1, 0, 1)) + M(-1, 0, 0));
+  T ma7 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, 1)) + M(0, 1, 1)) + M(0, 1, 0));
+  T ma9 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, 1)) + M(0, -1, 1)) + M(0, -1, 0));
+  T RD1 = divx(p, (dwdxp * ma4 - dwdxm * ma8));
+  T RD2 = divx(p, (dudzp * ma4 - dudzm * ma8));
+  T RD3 = divy(p, (dwdyp * ma7 - dwdym * ma9));
+  T RD4 = divy(p, (dvdzp * ma7 - dvdzm * ma9));
+  T RD5 = divz(p, TC(2.) * (dwdzp * M(0, 0, 1) - dwdzm * M(0, 0, 0)));
+  T RDw = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rw;
+  T RGw = TC(p.iFr) * (TC(1.) - rho_avr / rw) * TC(p.g3);
+  return (RCw + RDw * TC(p.visc)) + RGw;
 }
 
 // ---- the ab2 update of one component (ab2.f90:51-61, 79-129) -------------
 // u0 = u at the cell, R = its mom_main RHS, rf = its face density; h the
-// offset of the + neighbour along the component's axis, dhi its 1/dx
-__device__ __forceinline__ double ab2_update(const Params& p, const MomArgs& a, long long c, long long h,
-                                             double u0, double R, double rold, double rf, const double* pj,
-                                             const double* pjold, double dhi) {
-  double d = u0 + p.dt * (1.5 * R - 0.5 * rold);
+// offset of the + neighbour along the component's axis, dhi its 1/dx.  The
+// pressure-split term is formed in FP64 (the pressures are FP64 fields).
+template <typename T>
+__device__ __forceinline__ T ab2_update(const Params& p, const MomArgs& a, long long c, long long h, T u0, T R,
+                                        T rold, T rf, const double* pj, const double* pjold, double dhi) {
+  T d = u0 + TC(p.dt) * (TC(1.5) * R - TC(0.5) * rold);
   const double ph_p = 2. * a.pnew[c + h] - a.pold[c + h];
   const double ph_0 = 2. * a.pnew[c] - a.pold[c];
   const double pjh = 2. * pj[c] - pjold[c];
-  const double dn = -((1. / rf - p.rrho0) * dhi * ((ph_p - pjh) - ph_0));
-  return d + p.dt * dn;
+  const double dn = -((1. / (double)rf - p.rrho0) * dhi * ((ph_p - pjh) - ph_0));
+  return d + TC(p.dt * dn);
 }
 
 // ab2 over shape C with bounduvw(dudt,dvdt,dwdt) (bound.f90:36-75) in-kernel.
@@ -186,21 +191,28 @@ __device__ __forceinline__ double ab2_update(const Params& p, const MomArgs& a, 
 // writes its column's periodic halo images and, at k = 1 and k = kmax,
 // the wall rows k = 0 and k = k1.
 constexpr int MX = 32, MY = 8, MSX = MX + 2, MSY = MY + 2;
-__global__ void __launch_bounds__(MX * MY, 3) k_ab2(Params p, MomArgs a, double* __restrict__ dudt,
-                                                 double* __restrict__ dvdt, double* __restrict__ dwdt,
-                                                 double* __restrict__ duold_out, double* __restrict__ dvold_out,
-                                                 double* __restrict__ dwold_out, int kc, int nch) {
-  __shared__ double sm[4][3][MSY][MSX];
+template <typename T>
+__global__ void __launch_bounds__(MX * MY, 3) k_ab2(Params p, MomArgs a, T* __restrict__ dudt, T* __restrict__ dvdt,
+                                                    T* __restrict__ dwdt, T* __restrict__ duold_out,
+                                                    T* __restrict__ dvold_out, T* __restrict__ dwold_out, int kc,
+                                                    int nch) {
+  __shared__ T sm[4][3][MSY][MSX];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + MX * ty;
   const int i0 = 1 + MX * (int)blockIdx.x, j0 = 1 + MY * (int)blockIdx.y;
   const int ch = blockIdx.z;
   const int ka = 1 + ch * kc, kb = (ch == nch - 1) ? p.kmax : ka + kc - 1;
   const int i = i0 + tx, j = j0 + ty;
   const bool ok = i <= p.imax && j <= p.jmax;
-  const double* __restrict__ F0 = a.u;
-  const double* __restrict__ F1 = a.v;
-  const double* __restrict__ F2 = a.w;
-  const double* __restrict__ F3 = a.miu;
+  const T* __restrict__ F0 = cT<T>(a.u);
+  const T* __restrict__ F1 = cT<T>(a.v);
+  const T* __restrict__ F2 = cT<T>(a.w);
+  const T* __restrict__ F3 = cT<T>(a.miu);
+  const T* __restrict__ rhu = cT<T>(a.rho_u);
+  const T* __restrict__ rhv = cT<T>(a.rho_v);
+  const T* __restrict__ rhw = cT<T>(a.rho_w);
+  const T* __restrict__ hu = cT<T>(a.duold);
+  const T* __restrict__ hv = cT<T>(a.dvold);
+  const T* __restrict__ hw = cT<T>(a.dwold);
   auto load_plane = [&](int kk) {
     const int s = kk % 3;
     for (int e = tid; e < MSX * MSY; e += MX * MY) {
@@ -217,9 +229,9 @@ __global__ void __launch_bounds__(MX * MY, 3) k_ab2(Params p, MomArgs a, double*
   };
   load_plane(ka - 1);
   load_plane(ka);
-  const double rho_avr = *a.rho_avr;
+  const T rho_avr = TC(*a.rho_avr);
   const long long sy = p.nCx, sz = (long long)p.nCx * p.nCy;
-  double dw_km1 = 0.;
+  T dw_km1 = TC(0.);
   for (int k = ka; k <= kb; ++k) {
     load_plane(k + 1);
     __syncthreads();
@@ -231,30 +243,30 @@ __global__ void __launch_bounds__(MX * MY, 3) k_ab2(Params p, MomArgs a, double*
       auto W = [&](int di, int dj, int dk) { return sm[2][sl(dk)][ty + 1 + dj][tx + 1 + di]; };
       auto M = [&](int di, int dj, int dk) { return sm[3][sl(dk)][ty + 1 + dj][tx + 1 + di]; };
       const long long c = idxC(p, i, j, k), q = idxI(p, i, j, k);
-      const double ru = a.rho_u[q], rv = a.rho_v[q], rw = a.rho_w[q];
-      const double Ru = rhs_u(p, U, V, W, M, ru, rho_avr);
-      const double Rv = rhs_v(p, U, V, W, M, rv, rho_avr);
-      const double Rw = rhs_w(p, U, V, W, M, rw, rho_avr);
-      const double du = ab2_update(p, a, c, 1, U(0, 0, 0), Ru, a.duold[q], ru, a.px, a.pxold, p.dxi);
-      const double dv = ab2_update(p, a, c, sy, V(0, 0, 0), Rv, a.dvold[q], rv, a.py, a.pyold, p.dyi) -
-                        p.forceytot * p.dt / rv;
-      double dw = ab2_update(p, a, c, sz, W(0, 0, 0), Rw, a.dwold[q], rw, a.pz, a.pzold, p.dzi);
+      const T ru = rhu[q], rv = rhv[q], rw = rhw[q];
+      const T Ru = rhs_u<T>(p, U, V, W, M, ru, rho_avr);
+      const T Rv = rhs_v<T>(p, U, V, W, M, rv, rho_avr);
+      const T Rw = rhs_w<T>(p, U, V, W, M, rw, rho_avr);
+      const T du = ab2_update(p, a, c, 1, U(0, 0, 0), Ru, hu[q], ru, a.px, a.pxold, p.dxi);
+      const T dv = ab2_update(p, a, c, sy, V(0, 0, 0), Rv, hv[q], rv, a.py, a.pyold, p.dyi) -
+                   TC(p.forceytot * p.dt) / rv;
+      T dw = ab2_update(p, a, c, sz, W(0, 0, 0), Rw, hw[q], rw, a.pz, a.pzold, p.dzi);
       duold_out[q] = Ru;
       dvold_out[q] = Rv;
       dwold_out[q] = Rw;
       if (k == p.kmax - 1) dw_km1 = dw;
-      if (k == p.kmax) dw = 0.;
+      if (k == p.kmax) dw = TC(0.);
       putC(p, dudt, i, j, k, du);
       putC(p, dvdt, i, j, k, dv);
       putC(p, dwdt, i, j, k, dw);
       if (k == 1) {
         putC(p, dudt, i, j, 0, -du);
-        putC(p, dvdt, i, j, 0, 2. * p.v_lower - dv);
-        putC(p, dwdt, i, j, 0, 0.);
+        putC(p, dvdt, i, j, 0, TC(2. * p.v_lower) - dv);
+        putC(p, dwdt, i, j, 0, TC(0.));
       }
       if (k == p.kmax) {
         putC(p, dudt, i, j, p.k1, -du);
-        putC(p, dvdt, i, j, p.k1, 2. * p.v_upper - dv);
+        putC(p, dvdt, i, j, p.k1, TC(2. * p.v_upper) - dv);
         putC(p, dwdt, i, j, p.k1, dw_km1);
       }
     }
@@ -263,35 +275,38 @@ __global__ void __launch_bounds__(MX * MY, 3) k_ab2(Params p, MomArgs a, double*
 }
 
 // mom_main alone (init.f90:90): RHS into shape-I arrays
-__global__ void __launch_bounds__(NT) k_mom_main(Params p, MomArgs a, double* __restrict__ ru,
-                                                 double* __restrict__ rv, double* __restrict__ rw) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_mom_main(Params p, MomArgs a, T* __restrict__ ru, T* __restrict__ rv,
+                                                 T* __restrict__ rw) {
   int i, j, k;
   if (!cell3(kI0, cI1(p).v, i, j, k)) return;
   const long long q = idxI(p, i, j, k);
   const long long c = idxC(p, i, j, k);
   const long long sy = p.nCx, sz = (long long)p.nCx * p.nCy;
-  const double rho_avr = *a.rho_avr;
-  auto U = [&](int di, int dj, int dk) { return a.u[c + di + dj * sy + dk * sz]; };
-  auto V = [&](int di, int dj, int dk) { return a.v[c + di + dj * sy + dk * sz]; };
-  auto W = [&](int di, int dj, int dk) { return a.w[c + di + dj * sy + dk * sz]; };
-  auto M = [&](int di, int dj, int dk) { return a.miu[c + di + dj * sy + dk * sz]; };
-  ru[q] = rhs_u(p, U, V, W, M, a.rho_u[q], rho_avr);
-  rv[q] = rhs_v(p, U, V, W, M, a.rho_v[q], rho_avr);
-  rw[q] = rhs_w(p, U, V, W, M, a.rho_w[q], rho_avr);
+  const T rho_avr = TC(*a.rho_avr);
+  const T *u = cT<T>(a.u), *v = cT<T>(a.v), *w = cT<T>(a.w), *miu = cT<T>(a.miu);
+  auto U = [&](int di, int dj, int dk) { return u[c + di + dj * sy + dk * sz]; };
+  auto V = [&](int di, int dj, int dk) { return v[c + di + dj * sy + dk * sz]; };
+  auto W = [&](int di, int dj, int dk) { return w[c + di + dj * sy + dk * sz]; };
+  auto M = [&](int di, int dj, int dk) { return miu[c + di + dj * sy + dk * sz]; };
+  ru[q] = rhs_u<T>(p, U, V, W, M, cT<T>(a.rho_u)[q], rho_avr);
+  rv[q] = rhs_v<T>(p, U, V, W, M, cT<T>(a.rho_v)[q], rho_avr);
+  rw[q] = rhs_w<T>(p, U, V, W, M, cT<T>(a.rho_w)[q], rho_avr);
 }
 
 // fillps (fillps.f90:36-53), optionally followed by p = p + p_jump
-__global__ void __launch_bounds__(NT) k_fillps(Params p, const double* __restrict__ dudt,
-                                               const double* __restrict__ dvdt, const double* __restrict__ dwdt,
-                                               const double* __restrict__ pjump, int add, double* __restrict__ out) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_fillps(Params p, const T* __restrict__ dudt, const T* __restrict__ dvdt,
+                                               const T* __restrict__ dwdt, const double* __restrict__ pjump, int add,
+                                               double* __restrict__ out) {
   int i, j, k;
   if (!cell3(kI0, cI1(p).v, i, j, k)) return;
   const long long q = idxI(p, i, j, k);
   const long long c = idxC(p, i, j, k);
   const double coef = p.rho0 / p.dt;
-  const double vel_x = (dudt[c] - dudt[c - 1]) * p.dxi;
-  const double vel_y = (dvdt[c] - dvdt[c - p.nCx]) * p.dyi;
-  const double vel_z = (dwdt[c] - dwdt[c - (long long)p.nCx * p.nCy]) * p.dzi;
+  const double vel_x = ((double)dudt[c] - (double)dudt[c - 1]) * p.dxi;
+  const double vel_y = ((double)dvdt[c] - (double)dvdt[c - p.nCx]) * p.dyi;
+  const double vel_z = ((double)dwdt[c] - (double)dwdt[c - (long long)p.nCx * p.nCy]) * p.dzi;
   double v = coef * ((vel_x + vel_y) + vel_z);
   if (add) v = v + pjump[c];
   out[c] = v;
@@ -303,20 +318,28 @@ __global__ void __launch_bounds__(NT) k_add(Params p, double* __restrict__ a, co
 }
 
 // correc of one component (correc.f90:27-39)
-__device__ __forceinline__ double corr_u(const Params& p, const double* dudt, const double* pp, const double* px,
-                                         int i, int j, int k) {
+// (the pressure gradient in FP64, the result in the form's type T)
+template <typename T>
+__device__ __forceinline__ T corr_u(const Params& p, const T* dudt, const double* pp, const double* px, int i, int j,
+                                    int k) {
   const long long c = idxC(p, i, j, k);
-  return dudt[c] - p.dt * p.dxi * ((pp[c + 1] - pp[c]) - px[c]) / p.rho0;
+  if (sizeof(T) == sizeof(double)) return (T)(dudt[c] - p.dt * p.dxi * ((pp[c + 1] - pp[c]) - px[c]) / p.rho0);
+  return dudt[c] - (T)(p.dt * p.dxi * ((pp[c + 1] - pp[c]) - px[c]) / p.rho0);
 }
-__device__ __forceinline__ double corr_v(const Params& p, const double* dvdt, const double* pp, const double* py,
-                                         int i, int j, int k) {
+template <typename T>
+__device__ __forceinline__ T corr_v(const Params& p, const T* dvdt, const double* pp, const double* py, int i, int j,
+                                    int k) {
   const long long c = idxC(p, i, j, k);
-  return dvdt[c] - p.dt * p.dyi * ((pp[c + p.nCx] - pp[c]) - py[c]) / p.rho0;
+  if (sizeof(T) == sizeof(double)) return (T)(dvdt[c] - p.dt * p.dyi * ((pp[c + p.nCx] - pp[c]) - py[c]) / p.rho0);
+  return dvdt[c] - (T)(p.dt * p.dyi * ((pp[c + p.nCx] - pp[c]) - py[c]) / p.rho0);
 }
-__device__ __forceinline__ double corr_w(const Params& p, const double* dwdt, const double* pp, const double* pz,
-                                         int i, int j, int k) {
+template <typename T>
+__device__ __forceinline__ T corr_w(const Params& p, const T* dwdt, const double* pp, const double* pz, int i, int j,
+                                    int k) {
   const long long c = idxC(p, i, j, k);
-  return dwdt[c] - p.dt * p.dzi * ((pp[c + (long long)p.nCx * p.nCy] - pp[c]) - pz[c]) / p.rho0;
+  const long long sz = (long long)p.nCx * p.nCy;
+  if (sizeof(T) == sizeof(double)) return (T)(dwdt[c] - p.dt * p.dzi * ((pp[c + sz] - pp[c]) - pz[c]) / p.rho0);
+  return dwdt[c] - (T)(p.dt * p.dzi * ((pp[c + sz] - pp[c]) - pz[c]) / p.rho0);
 }
 
 struct CorrArgs {
@@ -326,55 +349,57 @@ struct CorrArgs {
 };
 
 // correc over the interior only (the separate reference call)
+template <typename T>
 __global__ void __launch_bounds__(NT) k_correc_interior(Params p, CorrArgs a) {
   int i, j, k;
   if (!cell3(kI0, cI1(p).v, i, j, k)) return;
-  const long long q = idxI(p, i, j, k);
   const long long c = idxC(p, i, j, k);
-  a.u[c] = corr_u(p, a.dudt, a.p, a.px, i, j, k);
-  a.v[c] = corr_v(p, a.dvdt, a.p, a.py, i, j, k);
-  a.w[c] = corr_w(p, a.dwdt, a.p, a.pz, i, j, k);
+  mT<T>(a.u)[c] = corr_u(p, cT<T>(a.dudt), a.p, a.px, i, j, k);
+  mT<T>(a.v)[c] = corr_v(p, cT<T>(a.dvdt), a.p, a.py, i, j, k);
+  mT<T>(a.w)[c] = corr_w(p, cT<T>(a.dwdt), a.p, a.pz, i, j, k);
 }
 
 // correc + bounduvw(unew,vnew,wnew) + average_vel_at_center + NaN probe
 // (main.f90:159-160,190,207) over shape C
+template <typename T>
 __global__ void __launch_bounds__(NT) k_correc_fused(Params p, CorrArgs a) {
   int i, j, k;
   if (!cell3(kC0, cC1(p).v, i, j, k)) return;
   const long long n = idxC(p, i, j, k);
   const int I = wrapx(p, i), J = wrapy(p, j);
-  double uu, vv, ww;
+  const T *du = cT<T>(a.dudt), *dv = cT<T>(a.dvdt), *dw = cT<T>(a.dwdt);
+  T uu, vv, ww;
   if (k >= 1 && k <= p.kmax) {
-    uu = corr_u(p, a.dudt, a.p, a.px, I, J, k);
-    vv = corr_v(p, a.dvdt, a.p, a.py, I, J, k);
-    ww = (k == p.kmax) ? 0. : corr_w(p, a.dwdt, a.p, a.pz, I, J, k);
+    uu = corr_u(p, du, a.p, a.px, I, J, k);
+    vv = corr_v(p, dv, a.p, a.py, I, J, k);
+    ww = (k == p.kmax) ? TC(0.) : corr_w(p, dw, a.p, a.pz, I, J, k);
   } else if (k == 0) {
-    uu = -corr_u(p, a.dudt, a.p, a.px, I, J, 1);
-    vv = 2. * p.v_lower - corr_v(p, a.dvdt, a.p, a.py, I, J, 1);
-    ww = 0.;
+    uu = -corr_u(p, du, a.p, a.px, I, J, 1);
+    vv = TC(2. * p.v_lower) - corr_v(p, dv, a.p, a.py, I, J, 1);
+    ww = TC(0.);
   } else {
-    uu = -corr_u(p, a.dudt, a.p, a.px, I, J, p.kmax);
-    vv = 2. * p.v_upper - corr_v(p, a.dvdt, a.p, a.py, I, J, p.kmax);
-    ww = corr_w(p, a.dwdt, a.p, a.pz, I, J, p.kmax - 1);
+    uu = -corr_u(p, du, a.p, a.px, I, J, p.kmax);
+    vv = TC(2. * p.v_upper) - corr_v(p, dv, a.p, a.py, I, J, p.kmax);
+    ww = corr_w(p, dw, a.p, a.pz, I, J, p.kmax - 1);
   }
-  a.u[n] = uu;
-  a.v[n] = vv;
-  a.w[n] = ww;
+  mT<T>(a.u)[n] = uu;
+  mT<T>(a.v)[n] = vv;
+  mT<T>(a.w)[n] = ww;
   if (i == I && j == J && k >= 1 && k <= p.kmax) {
     const long long q = idxI(p, i, j, k);
-    const double um = corr_u(p, a.dudt, a.p, a.px, wrapx(p, i - 1), j, k);
-    const double vm = corr_v(p, a.dvdt, a.p, a.py, i, wrapy(p, j - 1), k);
-    const double wm = (k == 1) ? 0. : corr_w(p, a.dwdt, a.p, a.pz, i, j, k - 1);
-    a.ucc[q] = (um + uu) / 2.;
-    a.vcc[q] = (vm + vv) / 2.;
-    a.wcc[q] = (wm + ww) / 2.;
+    const T um = corr_u(p, du, a.p, a.px, wrapx(p, i - 1), j, k);
+    const T vm = corr_v(p, dv, a.p, a.py, i, wrapy(p, j - 1), k);
+    const T wm = (k == 1) ? TC(0.) : corr_w(p, dw, a.p, a.pz, i, j, k - 1);
+    mT<T>(a.ucc)[q] = (um + uu) / TC(2.);
+    mT<T>(a.vcc)[q] = (vm + vv) / TC(2.);
+    mT<T>(a.wcc)[q] = (wm + ww) / TC(2.);
     if (i == 1 && j == 1 && k == 1 && isnan(vv)) a.dsc->nan_flag = 1;
   }
 }
 
 // bounduvw (bound.f90:15-177, Dirichl z, periodic x,y) on an existing triple
-__global__ void __launch_bounds__(NT) k_bounduvw(Params p, double* __restrict__ u, double* __restrict__ v,
-                                                 double* __restrict__ w) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_bounduvw(Params p, T* __restrict__ u, T* __restrict__ v, T* __restrict__ w) {
   int i, j, k;
   if (!cell3(kC0, cC1(p).v, i, j, k)) return;
   const long long n = idxC(p, i, j, k);
@@ -385,15 +410,15 @@ __global__ void __launch_bounds__(NT) k_bounduvw(Params p, double* __restrict__ 
       u[n] = u[idxC(p, I, J, k)];
       v[n] = v[idxC(p, I, J, k)];
     }
-    if (k == p.kmax) w[n] = 0.;
+    if (k == p.kmax) w[n] = TC(0.);
     else if (!col) w[n] = w[idxC(p, I, J, k)];
   } else if (k == 0) {
     u[n] = -u[idxC(p, I, J, 1)];
-    v[n] = 2. * p.v_lower - v[idxC(p, I, J, 1)];
-    w[n] = 0.;
+    v[n] = TC(2. * p.v_lower) - v[idxC(p, I, J, 1)];
+    w[n] = TC(0.);
   } else {
     u[n] = -u[idxC(p, I, J, p.kmax)];
-    v[n] = 2. * p.v_upper - v[idxC(p, I, J, p.kmax)];
+    v[n] = TC(2. * p.v_upper) - v[idxC(p, I, J, p.kmax)];
     w[n] = w[idxC(p, I, J, p.kmax - 1)];
   }
 }
@@ -410,17 +435,17 @@ __global__ void __launch_bounds__(NT) k_boundp(Params p, double* __restrict__ a)
 }
 
 // average_vel_at_center (misc.f90:587-604)
-__global__ void __launch_bounds__(NT) k_average_vel(Params p, const double* __restrict__ u,
-                                                    const double* __restrict__ v, const double* __restrict__ w,
-                                                    double* __restrict__ ucc, double* __restrict__ vcc,
-                                                    double* __restrict__ wcc) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_average_vel(Params p, const T* __restrict__ u, const T* __restrict__ v,
+                                                    const T* __restrict__ w, T* __restrict__ ucc, T* __restrict__ vcc,
+                                                    T* __restrict__ wcc) {
   int i, j, k;
   if (!cell3(kI0, cI1(p).v, i, j, k)) return;
   const long long q = idxI(p, i, j, k);
   const long long c = idxC(p, i, j, k);
-  ucc[q] = (u[c - 1] + u[c]) / 2.;
-  vcc[q] = (v[c - p.nCx] + v[c]) / 2.;
-  wcc[q] = (w[c - (long long)p.nCx * p.nCy] + w[c]) / 2.;
+  ucc[q] = (u[c - 1] + u[c]) / TC(2.);
+  vcc[q] = (v[c - p.nCx] + v[c]) / TC(2.);
+  wcc[q] = (w[c - (long long)p.nCx * p.nCy] + w[c]) / TC(2.);
 }
 
 // ---- pressure update (main.f90:164-185) ----------------------------------
@@ -453,13 +478,14 @@ __global__ void __launch_bounds__(NT) k_pupdate(Params p, const double* __restri
 }
 
 // ---- reductions ------------------------------------------------------------
-__global__ void __launch_bounds__(kRedThreads) k_sum_interior(Params p, const double* __restrict__ a,
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_sum_interior(Params p, const T* __restrict__ a,
                                                               double* __restrict__ partial) {
   double s = 0.;
   for (int q = blockIdx.x * kRedThreads + threadIdx.x; q < (int)p.nI; q += gridDim.x * kRedThreads) {
     int i, j, k;
     decodeI(p, q, i, j, k);
-    s += a[idxC(p, i, j, k)];
+    s += (double)a[idxC(p, i, j, k)];
   }
   double b = block_sum<double, kRedThreads>(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = b;
@@ -473,8 +499,9 @@ __global__ void k_stream_final(Params p, const double* __restrict__ partial, int
 }
 
 // chkdiv: sum of div and max|div| with its first column-major location
-__global__ void __launch_bounds__(kRedThreads) k_chkdiv(Params p, const double* __restrict__ u,
-                                                        const double* __restrict__ v, const double* __restrict__ w,
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_chkdiv(Params p, const T* __restrict__ u, const T* __restrict__ v,
+                                                        const T* __restrict__ w,
                                                         double* __restrict__ part_sum, double* __restrict__ part_max,
                                                         long long* __restrict__ part_loc) {
   double s = 0., m = 0.;
@@ -483,8 +510,9 @@ __global__ void __launch_bounds__(kRedThreads) k_chkdiv(Params p, const double* 
     int i, j, k;
     decodeI(p, q, i, j, k);
     const long long c = idxC(p, i, j, k);
-    double div = ((w[c] - w[c - (long long)p.nCx * p.nCy]) * p.dzi + (v[c] - v[c - p.nCx]) * p.dyi) +
-                 (u[c] - u[c - 1]) * p.dxi;
+    const double wc = w[c], wm = w[c - (long long)p.nCx * p.nCy], vc = v[c], vm = v[c - p.nCx];
+    const double uc = u[c], um = u[c - 1];
+    double div = ((wc - wm) * p.dzi + (vc - vm) * p.dyi) + (uc - um) * p.dxi;
     s += div;
     div = fabs(div);
     if (div > m) { m = div; loc = (long long)q; }
@@ -521,16 +549,17 @@ __global__ void k_chkdiv_final(const double* __restrict__ part_sum, const double
 }
 
 // chkdt maxima (chkdt.f90:31-52) and max_vel_at_center (misc.f90:619-633)
-__global__ void __launch_bounds__(NT) k_chkdt(Params p, const double* __restrict__ u, const double* __restrict__ v,
-                                              const double* __restrict__ w, DevScalars* __restrict__ dsc) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_chkdt(Params p, const T* __restrict__ u, const T* __restrict__ v,
+                                              const T* __restrict__ w, DevScalars* __restrict__ dsc) {
   double a = 0., b = 0., c = 0.;
   int i, j, k;
   const I3 hi = cC1(p);
   if (cell3(kI0, hi.v, i, j, k)) {
     const long long cc = idxC(p, i, j, k);
-    a = fabs((u[cc] + u[cc - 1]) / 2.);
-    b = fabs((v[cc] + v[cc - p.nCx]) / 2.);
-    c = fabs((w[cc] + w[cc - (long long)p.nCx * p.nCy]) / 2.);
+    a = fabs(((double)u[cc] + (double)u[cc - 1]) / 2.);
+    b = fabs(((double)v[cc] + (double)v[cc - p.nCx]) / 2.);
+    c = fabs(((double)w[cc] + (double)w[cc - (long long)p.nCx * p.nCy]) / 2.);
   }
   a = block_max<double, NT>(a);
   b = block_max<double, NT>(b);
@@ -541,12 +570,15 @@ __global__ void __launch_bounds__(NT) k_chkdt(Params p, const double* __restrict
     atomic_max_nonneg(&dsc->wmax, c);
   }
 }
-__global__ void __launch_bounds__(NT) k_maxvel(Params p, const double* __restrict__ ucc,
-                                               const double* __restrict__ vcc, const double* __restrict__ wcc,
-                                               DevScalars* __restrict__ dsc) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_maxvel(Params p, const T* __restrict__ ucc, const T* __restrict__ vcc,
+                                               const T* __restrict__ wcc, DevScalars* __restrict__ dsc) {
   const long long q = blockIdx.x * (long long)NT + threadIdx.x;
   double m = 0.;
-  if (q < p.nI) m = sqrt((ucc[q] * ucc[q] + vcc[q] * vcc[q]) + wcc[q] * wcc[q]);
+  if (q < p.nI) {
+    const double a = ucc[q], b = vcc[q], cc = wcc[q];
+    m = sqrt((a * a + b * b) + cc * cc);
+  }
   m = block_max<double, NT>(m);
   if (threadIdx.x == 0) atomic_max_nonneg(&dsc->velmax, m);
 }
@@ -568,45 +600,72 @@ CorrArgs corr_args(Ctx& c) {
   return a;
 }
 
+#undef TC
 }  // namespace
 
 // ================================================================ launchers
+template <typename T>
+T* fp(double* q) { return reinterpret_cast<T*>(q); }
+
+template <typename T>
+void ab2_launch(Ctx& c, const MomArgs& a, int o) {
+  const int kc = 16, nch = std::max(1, c.P.kmax / kc);
+  const dim3 grid((unsigned)((c.P.imax + MX - 1) / MX), (unsigned)((c.P.jmax + MY - 1) / MY), (unsigned)nch);
+  k_ab2<T><<<grid, dim3(MX, MY, 1), 0, c.s>>>(c.P, a, fp<T>(c.dudt), fp<T>(c.dvdt), fp<T>(c.dwdt),
+                                               fp<T>(c.duold[o]), fp<T>(c.dvold[o]), fp<T>(c.dwold[o]),
+                                               nch == 1 ? c.P.kmax : kc, nch);
+}
 void launch_ab2(Ctx& c) {
   Scope sc_(c.prof, c.s, "ab2", 1);
   MomArgs a = mom_args(c);
   const int o = c.hist ^ 1;
-  const int kc = 16, nch = std::max(1, c.P.kmax / kc);
-  const dim3 grid((unsigned)((c.P.imax + MX - 1) / MX), (unsigned)((c.P.jmax + MY - 1) / MY), (unsigned)nch);
-  k_ab2<<<grid, dim3(MX, MY, 1), 0, c.s>>>(c.P, a, c.dudt, c.dvdt, c.dwdt, c.duold[o], c.dvold[o], c.dwold[o],
-                                          nch == 1 ? c.P.kmax : kc, nch);
+  if (c.P.f32) ab2_launch<float>(c, a, o);
+  else ab2_launch<double>(c, a, o);
   c.hist = o;
 }
 void launch_mom_main(Ctx& c, double* du, double* dv, double* dw) {
   Scope sc_(c.prof, c.s, "mom_main", 1);
   MomArgs a = mom_args(c);
-  k_mom_main<<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a, du, dv, dw);
+  if (c.P.f32)
+    k_mom_main<float><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a, fp<float>(du), fp<float>(dv), fp<float>(dw));
+  else
+    k_mom_main<double><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a, du, dv, dw);
 }
 void launch_fillps(Ctx& c, int add_pjump) {
   Scope sc_(c.prof, c.s, "fillps", 1);
-  k_fillps<<<gridI(c.P), kBlock, 0, c.s>>>(c.P, c.dudt, c.dvdt, c.dwdt, c.pjump, add_pjump, c.p);
+  if (c.P.f32)
+    k_fillps<float><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, fp<float>(c.dudt), fp<float>(c.dvdt), fp<float>(c.dwdt),
+                                                     c.pjump, add_pjump, c.p);
+  else
+    k_fillps<double><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, c.dudt, c.dvdt, c.dwdt, c.pjump, add_pjump, c.p);
 }
 void launch_add_pjump(Ctx& c) {
   Scope sc_(c.prof, c.s, "add_pjump", 1); k_add<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, c.pjump); }
 void launch_correc(Ctx& c, int fused_bc) {
   Scope sc_(c.prof, c.s, "correc", 1);
   CorrArgs a = corr_args(c);
-  if (fused_bc) k_correc_fused<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, a);
-  else k_correc_interior<<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);
+  if (c.P.f32) {
+    if (fused_bc) k_correc_fused<float><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, a);
+    else k_correc_interior<float><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);
+  } else {
+    if (fused_bc) k_correc_fused<double><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, a);
+    else k_correc_interior<double><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);
+  }
 }
 void launch_bounduvw(Ctx& c, double* u, double* v, double* w) {
   Scope sc_(c.prof, c.s, "bounduvw", 1);
-  k_bounduvw<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, u, v, w);
+  if (c.P.f32) k_bounduvw<float><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, fp<float>(u), fp<float>(v), fp<float>(w));
+  else k_bounduvw<double><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, u, v, w);
 }
 void launch_boundp(Ctx& c, double* pp) {
   Scope sc_(c.prof, c.s, "boundp", 1); k_boundp<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, pp); }
 void launch_average_vel(Ctx& c) {
   Scope sc_(c.prof, c.s, "average_vel", 1);
-  k_average_vel<<<gridI(c.P), kBlock, 0, c.s>>>(c.P, c.u, c.v, c.w, c.ucc, c.vcc, c.wcc);
+  if (c.P.f32)
+    k_average_vel<float><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, fp<float>(c.u), fp<float>(c.v), fp<float>(c.w),
+                                                          fp<float>(c.ucc), fp<float>(c.vcc), fp<float>(c.wcc));
+  else
+    k_average_vel<double><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, c.u, c.v, c.w, c.ucc, c.vcc, c.wcc);
 }
 void launch_pressure_update(Ctx& c, int first) {
   Scope sc_(c.prof, c.s, "pressure_update", 2);
@@ -615,25 +674,34 @@ void launch_pressure_update(Ctx& c, int first) {
 }
 void launch_stream_vel(Ctx& c) {
   Scope sc_(c.prof, c.s, "stream_vel", 2);
-  k_sum_interior<<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, c.v, c.partials);
+  if (c.P.f32) k_sum_interior<float><<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, fp<float>(c.v), c.partials);
+  else k_sum_interior<double><<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, c.v, c.partials);
   k_stream_final<<<1, 32, 0, c.s>>>(c.P, c.partials, kRedBlocks, c.dsc);
 }
 void launch_chkdiv(Ctx& c) {
   Scope sc_(c.prof, c.s, "chkdiv", 2);
   double* ps = c.partials;
   double* pm = c.partials + kRedBlocks;
-  k_chkdiv<<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, c.u, c.v, c.w, ps, pm, c.lpartials);
+  if (c.P.f32)
+    k_chkdiv<float><<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, fp<float>(c.u), fp<float>(c.v), fp<float>(c.w), ps, pm,
+                                                          c.lpartials);
+  else
+    k_chkdiv<double><<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, c.u, c.v, c.w, ps, pm, c.lpartials);
   k_chkdiv_final<<<1, 32, 0, c.s>>>(ps, pm, c.lpartials, kRedBlocks, c.dsc);
 }
 void launch_chkdt(Ctx& c) {
   Scope sc_(c.prof, c.s, "chkdt", 1);
   cudaMemsetAsync(&c.dsc->umax, 0, 3 * sizeof(double), c.s);
-  k_chkdt<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, c.u, c.v, c.w, c.dsc);
+  if (c.P.f32) k_chkdt<float><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, fp<float>(c.u), fp<float>(c.v), fp<float>(c.w), c.dsc);
+  else k_chkdt<double><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, c.u, c.v, c.w, c.dsc);
 }
 void launch_maxvel(Ctx& c) {
   Scope sc_(c.prof, c.s, "maxvel", 1);
   cudaMemsetAsync(&c.dsc->velmax, 0, sizeof(double), c.s);
-  k_maxvel<<<nblocks(c.P.nI), NT, 0, c.s>>>(c.P, c.ucc, c.vcc, c.wcc, c.dsc);
+  if (c.P.f32)
+    k_maxvel<float><<<nblocks(c.P.nI), NT, 0, c.s>>>(c.P, fp<float>(c.ucc), fp<float>(c.vcc), fp<float>(c.wcc), c.dsc);
+  else
+    k_maxvel<double><<<nblocks(c.P.nI), NT, 0, c.s>>>(c.P, c.ucc, c.vcc, c.wcc, c.dsc);
 }
 
 }  // namespace icls

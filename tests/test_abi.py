@@ -73,7 +73,7 @@ def test_config_default_matches_python_defaults(lib):
     (dict(timestep=-1e-4), "E_CONFIG"),
     (dict(reinit_step=0), "E_CONFIG"),
     (dict(ls_adv_space=7), "E_CONFIG"),
-    (dict(precision=32), "E_UNSUPPORTED"),  # FP32 form not built
+    (dict(precision=5), "E_CONFIG"),        # neither ICLS_FP64 nor ICLS_FP32
     (dict(curvature_model=1), "E_UNSUPPORTED"),
 ])
 def test_create_rejects_bad_configs_on_host(lib, change, code):
