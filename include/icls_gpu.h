@@ -183,6 +183,13 @@ int icls_get_curvature(icls_ctx* ctx, int l);               /* interface.f90:20-
  * (nb_cnt, levelset.f90:158).                                           */
 int icls_band_count(icls_ctx* ctx, int l, long long* nb_cnt);
 
+/* ---- tensor-core tile check ----
+ * No counterpart in the reference.  d (128 x n FP32, row-major) = a (128 x k
+ * BF16, row-major) * b (n x k BF16, row-major)^T on one tcgen05 tile, the
+ * building block of the learned curvature's network; device pointers,
+ * n and k multiples of 16 in [16, 128]; synchronous on `stream`. */
+int icls_tc_gemm_bf16(const void* a, const void* b, float* d, int n, int k, void* stream);
+
 /* ---- divergence check without device allocation -----------------------
  * No counterpart in the reference.  The chkdiv reduction for callers that
  * cannot let the library allocate device memory (their device memory is
