@@ -19,6 +19,57 @@
 
 using namespace icls;
 
+namespace icls {
+// init_matrix (init.f90:1587-1723): pseudo_inv_A = (A^T A)^-1 A^T of the
+// quadratic least-squares fit on the 27-point stencil; inverted by
+// Gauss-Jordan in long double.
+// the 10x27 least-squares pseudo-inverse of init.f90:1587-1723 for spacings
+// (dx, dy, dz), into out[r*27 + n]
+void pseudo_inverse(double dx, double dy, double dz, double* out) {
+  long double A[27][10];
+  int row = 0;
+  for (int dzs = -1; dzs <= 1; ++dzs)
+    for (int dys = -1; dys <= 1; ++dys)
+      for (int dxs = -1; dxs <= 1; ++dxs) {
+        long double a2 = (long double)(dx * dxs), a3 = (long double)(dy * dys), a4 = (long double)(dz * dzs);
+        long double* r = A[row++];
+        r[0] = 1; r[1] = a2; r[2] = a3; r[3] = a4;
+        r[4] = 0.5L * a2 * a2; r[5] = 0.5L * a3 * a3; r[6] = 0.5L * a4 * a4;
+        r[7] = a2 * a3; r[8] = a2 * a4; r[9] = a3 * a4;
+      }
+  long double M[10][20];
+  for (int r = 0; r < 10; ++r)
+    for (int q = 0; q < 10; ++q) {
+      long double s = 0;
+      for (int n = 0; n < 27; ++n) s += A[n][r] * A[n][q];
+      M[r][q] = s;
+      M[r][10 + q] = (r == q) ? 1 : 0;
+    }
+  for (int col = 0; col < 10; ++col) {
+    int piv = col;
+    for (int r = col + 1; r < 10; ++r)
+      if (fabsl(M[r][col]) > fabsl(M[piv][col])) piv = r;
+    if (piv != col)
+      for (int q = 0; q < 20; ++q) std::swap(M[col][q], M[piv][q]);
+    const long double d = M[col][col];
+    for (int q = 0; q < 20; ++q) M[col][q] /= d;
+    for (int r = 0; r < 10; ++r) {
+      if (r == col) continue;
+      const long double f = M[r][col];
+      if (f != 0)
+        for (int q = 0; q < 20; ++q) M[r][q] -= f * M[col][q];
+    }
+  }
+  for (int r = 0; r < 10; ++r)
+    for (int n = 0; n < 27; ++n) {
+      long double s = 0;
+      for (int q = 0; q < 10; ++q) s += M[r][10 + q] * A[n][q];
+      out[r * 27 + n] = (double)s;
+    }
+}
+
+}  // namespace icls
+
 struct icls_ctx {
   Ctx c;
 };
@@ -86,52 +137,7 @@ void fill_params(Ctx& c) {
   P.ispeed_curv = (f.ispeed_dependence == ICLS_SPEED_CURV);
 }
 
-// init_matrix (init.f90:1587-1723): pseudo_inv_A = (A^T A)^-1 A^T of the
-// quadratic least-squares fit on the 27-point stencil; inverted by
-// Gauss-Jordan in long double.
-void init_matrix(Ctx& c) {
-  long double A[27][10];
-  int row = 0;
-  for (int dzs = -1; dzs <= 1; ++dzs)
-    for (int dys = -1; dys <= 1; ++dys)
-      for (int dxs = -1; dxs <= 1; ++dxs) {
-        long double a2 = (long double)(c.P.dx * dxs), a3 = (long double)(c.P.dy * dys),
-                    a4 = (long double)(c.P.dz * dzs);
-        long double* r = A[row++];
-        r[0] = 1; r[1] = a2; r[2] = a3; r[3] = a4;
-        r[4] = 0.5L * a2 * a2; r[5] = 0.5L * a3 * a3; r[6] = 0.5L * a4 * a4;
-        r[7] = a2 * a3; r[8] = a2 * a4; r[9] = a3 * a4;
-      }
-  long double M[10][20];
-  for (int r = 0; r < 10; ++r)
-    for (int q = 0; q < 10; ++q) {
-      long double s = 0;
-      for (int n = 0; n < 27; ++n) s += A[n][r] * A[n][q];
-      M[r][q] = s;
-      M[r][10 + q] = (r == q) ? 1 : 0;
-    }
-  for (int col = 0; col < 10; ++col) {
-    int piv = col;
-    for (int r = col + 1; r < 10; ++r)
-      if (fabsl(M[r][col]) > fabsl(M[piv][col])) piv = r;
-    if (piv != col)
-      for (int q = 0; q < 20; ++q) std::swap(M[col][q], M[piv][q]);
-    const long double d = M[col][col];
-    for (int q = 0; q < 20; ++q) M[col][q] /= d;
-    for (int r = 0; r < 10; ++r) {
-      if (r == col) continue;
-      const long double f = M[r][col];
-      if (f != 0)
-        for (int q = 0; q < 20; ++q) M[r][q] -= f * M[col][q];
-    }
-  }
-  for (int r = 0; r < 10; ++r)
-    for (int n = 0; n < 27; ++n) {
-      long double s = 0;
-      for (int q = 0; q < 10; ++q) s += M[r][10 + q] * A[n][q];
-      c.P10x27[r * 27 + n] = (double)s;
-    }
-}
+void init_matrix(Ctx& c) { pseudo_inverse(c.P.dx, c.P.dy, c.P.dz, c.P10x27); }
 
 template <typename T>
 int dalloc(T** p, size_t n) {

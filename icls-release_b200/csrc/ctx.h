@@ -150,6 +150,9 @@ struct Ctx {
   std::vector<double> outside;          // interior cells outside each drop's box
 };
 
+// the 10x27 least-squares pseudo-inverse for spacings (dx, dy, dz) (capi.cu)
+void pseudo_inverse(double dx, double dy, double dz, double* out);
+
 // ---- kernel launchers (defined in the k_*.cu files) -----------------------
 void set_pseudo_inverse(const double* P270, cudaStream_t s);
 

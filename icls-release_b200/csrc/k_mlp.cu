@@ -5,7 +5,13 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <vector>
+
 #include "../../include/icls_gpu.h"
+#include "ctx.h"
 #include "umma.cuh"
 
 namespace icls {
@@ -59,8 +65,786 @@ __global__ void __launch_bounds__(128) k_tc_gemm_check(const __nv_bfloat16* __re
   if (warp == 0) umma::tmem_free(tmem, 128);
 }
 
+
+// ============================================================== the network
+// 27 -> 128 -> 128 -> 64 -> 1, SiLU after the first three layers.  Inputs
+// are the 27 values (phi(x + o dx) - phi(x)) / dx of a 3x3x3 stencil (padded
+// to 32 with zeros), the output is kappa * dx.  FP32 master parameters in one
+// array (layout below), BF16 copies of W1..W3 as the tiles' B operands and
+// BF16 transposes of W2, W3 for back-propagation to the inputs.
+constexpr int kIn = 32, kH1 = 128, kH2 = 128, kH3 = 64;
+constexpr int oW1 = 0, oB1 = oW1 + kH1 * kIn, oW2 = oB1 + kH1, oB2 = oW2 + kH2 * kH1, oW3 = oB2 + kH2,
+              oB3 = oW3 + kH3 * kH2, oW4 = oB3 + kH3, oB4 = oW4 + kH3, kParams = oB4 + 1;
+
+struct Net {
+  const float* theta;              // FP32 parameters
+  const __nv_bfloat16* w1;         // [128][32]
+  const __nv_bfloat16* w2;         // [128][128]
+  const __nv_bfloat16* w3;         // [64][128]
+  const __nv_bfloat16* w2t;        // [128][128] = W2^T
+  const __nv_bfloat16* w3t;        // [128][64]  = W3^T
+};
+
+__device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+__device__ __forceinline__ float dsilu(float z) {
+  const float s = 1.f / (1.f + __expf(-z));
+  return s * (1.f + z * (1.f - s));
+}
+__device__ __forceinline__ void put_bf16(unsigned char* base, uint32_t off, float v) {
+  *reinterpret_cast<__nv_bfloat16*>(base + off) = __float2bfloat16(v);
+}
+
+// shared-memory plan of one tile (bytes)
+constexpr int SB_B = 0;                       // weight operand, up to 128 x 128
+constexpr int SB_ACT = SB_B + 32768;          // activations / deltas, A layout [128 x 128]
+constexpr int SB_XA = SB_ACT + 32768;         // inputs, A layout [128 x 32]
+constexpr int SB_XT = SB_XA + 8192;           // inputs transposed [32 x 128]
+constexpr int SB_H1T = SB_XT + 8192;          // H1^T [128 x 128]
+constexpr int SB_H2T = SB_H1T + 32768;        // H2^T [128 x 128]
+constexpr int SB_DZT = SB_H2T + 32768;        // delta^T [128 x 128]
+constexpr int SB_TRAIN = SB_DZT + 32768;      // 180224
+constexpr int SB_INFER = SB_XT;               // forward only: B, ACT, XA (73728)
+
+// a weight matrix [n][k] (row-major BF16, global) into the B operand layout
+__device__ __forceinline__ void stage_b(unsigned char* sb, const __nv_bfloat16* __restrict__ w, int n, int k) {
+  for (int e = threadIdx.x; e < n * k; e += blockDim.x) {
+    const int r = e / k, c = e - r * k;
+    *reinterpret_cast<__nv_bfloat16*>(sb + kmajor_off(r, c, n)) = w[e];
+  }
+}
+
+// The forward pass of one 128-sample tile; x (BF16, [rows][32]) holds the
+// tile's inputs, sample t of the tile is row t.  Returns y (kappa*dx) of this
+// thread's sample.  Training keeps the pre-activations z1..z3 (zg, per sample
+// 320 floats) and the transposed activations in shared memory.
+template <bool TRAIN>
+__device__ float forward_tile(const Net& net, const __nv_bfloat16* __restrict__ xrow, unsigned char* sm, uint32_t tmem,
+                              uint64_t* bar, uint32_t& phase, float* __restrict__ zrow, bool& ok) {
+  const int t = threadIdx.x, warp = t >> 5;
+  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  // inputs
+  for (int j = 0; j < kIn; ++j) {
+    const float v = xrow ? __bfloat162float(xrow[j]) : 0.f;
+    put_bf16(sm + SB_XA, kmajor_off(t, j, kRows), v);
+    if (TRAIN) put_bf16(sm + SB_XT, kmajor_off(j, t, kIn), v);
+  }
+  // layer 1
+  stage_b(sm + SB_B, net.w1, kH1, kIn);
+  ok &= umma::tile_gemm(sm + SB_XA, sm + SB_B, kH1, kIn, tmem, bar, phase);
+  for (int c = 0; c < kH1; c += 8) {
+    float v[8];
+    umma::tmem_ld8(lane_addr + c, v);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float z = v[q] + net.theta[oB1 + c + q];
+      const float h = silu(z);
+      put_bf16(sm + SB_ACT, kmajor_off(t, c + q, kRows), h);
+      if (TRAIN) {
+        put_bf16(sm + SB_H1T, kmajor_off(c + q, t, kH1), h);
+        zrow[c + q] = z;
+      }
+    }
+  }
+  // layer 2
+  stage_b(sm + SB_B, net.w2, kH2, kH1);
+  ok &= umma::tile_gemm(sm + SB_ACT, sm + SB_B, kH2, kH1, tmem, bar, phase);
+  for (int c = 0; c < kH2; c += 8) {
+    float v[8];
+    umma::tmem_ld8(lane_addr + c, v);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float z = v[q] + net.theta[oB2 + c + q];
+      const float h = silu(z);
+      put_bf16(sm + SB_ACT, kmajor_off(t, c + q, kRows), h);
+      if (TRAIN) {
+        put_bf16(sm + SB_H2T, kmajor_off(c + q, t, kH2), h);
+        zrow[kH1 + c + q] = z;
+      }
+    }
+  }
+  // layer 3 and the linear head
+  stage_b(sm + SB_B, net.w3, kH3, kH2);
+  ok &= umma::tile_gemm(sm + SB_ACT, sm + SB_B, kH3, kH2, tmem, bar, phase);
+  float y = net.theta[oB4];
+  for (int c = 0; c < kH3; c += 8) {
+    float v[8];
+    umma::tmem_ld8(lane_addr + c, v);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float z = v[q] + net.theta[oB3 + c + q];
+      y += net.theta[oW4 + c + q] * silu(z);
+      if (TRAIN) zrow[kH1 + kH2 + c + q] = z;
+    }
+  }
+  return y;
+}
+
+// warp-summed atomic add of this thread's v into *dst (one atomic per warp)
+__device__ __forceinline__ void warp_add(float* dst, float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(dst, v);
+}
+
+// One training tile: forward, MSE loss gradient (scale = 2/batch) and the
+// backward pass; parameter gradients are added into grad (FP32), the loss
+// sum into *loss.  Samples idx = (a * (base + t) + b) mod n (a per-epoch
+// affine shuffle of the n samples, n a power of two, a odd).
+__global__ void __launch_bounds__(128) k_mlp_train_tile(Net net, const __nv_bfloat16* __restrict__ X,
+                                                        const float* __restrict__ label, long long n, long long base,
+                                                        unsigned long long pa, unsigned long long pb, float scale,
+                                                        float* __restrict__ zbuf, float* __restrict__ grad,
+                                                        float* __restrict__ loss, int* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  const int t = threadIdx.x, warp = t >> 5;
+  if (t == 0) umma::mbar_init(&bar, 1);
+  if (warp == 0) umma::tmem_alloc(&tmem_slot, 128);
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  uint32_t phase = 0;
+  bool ok = true;
+  const long long gi = base + (long long)blockIdx.x * kRows + t;
+  const long long s = (long long)(((unsigned long long)gi * pa + pb) & (unsigned long long)(n - 1));
+  float* zrow = zbuf + ((long long)blockIdx.x * kRows + t) * (kH1 + kH2 + kH3);
+  const float y = forward_tile<true>(net, X + s * kIn, sm, tmem, &bar, phase, zrow, ok);
+  const float e = y - label[s];
+  warp_add(loss, e * e);
+  const float dy = scale * e;
+  // head: dW4 = sum dy h3, db4 = sum dy; delta3 = dy W4 silu'(z3)
+  warp_add(grad + oB4, dy);
+  for (int j = 0; j < kH3; ++j) {
+    const float z = zrow[kH1 + kH2 + j];
+    warp_add(grad + oW4 + j, dy * silu(z));
+    const float d3 = dy * net.theta[oW4 + j] * dsilu(z);
+    warp_add(grad + oB3 + j, d3);
+    put_bf16(sm + SB_ACT, kmajor_off(t, j, kRows), d3);
+    put_bf16(sm + SB_DZT, kmajor_off(j, t, kRows), d3);
+    put_bf16(sm + SB_DZT, kmajor_off(j + kH3, t, kRows), 0.f);  // rows 64..127 of delta3^T are padding
+  }
+  // dW3 = delta3^T H2 (rows 0..63 of a 128 x 128 tile)
+  ok &= umma::tile_gemm(sm + SB_DZT, sm + SB_H2T, kH2, kRows, tmem, &bar, phase);
+  if (t < kH3)
+    for (int c = 0; c < kH2; c += 8) {
+      float v[8];
+      umma::tmem_ld8(lane_addr + c, v);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) atomicAdd(grad + oW3 + t * kH2 + c + q, v[q]);
+    }
+  else
+    for (int c = 0; c < kH2; c += 8) {  // every lane of the warp takes part in tcgen05.ld
+      float v[8];
+      umma::tmem_ld8(lane_addr + c, v);
+    }
+  // dH2 = delta3 W3 -> delta2 = dH2 silu'(z2)
+  stage_b(sm + SB_B, net.w3t, kH2, kH3);
+  ok &= umma::tile_gemm(sm + SB_ACT, sm + SB_B, kH2, kH3, tmem, &bar, phase);
+  for (int c = 0; c < kH2; c += 8) {
+    float v[8];
+    umma::tmem_ld8(lane_addr + c, v);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float d2 = v[q] * dsilu(zrow[kH1 + c + q]);
+      warp_add(grad + oB2 + c + q, d2);
+      put_bf16(sm + SB_ACT, kmajor_off(t, c + q, kRows), d2);
+      put_bf16(sm + SB_DZT, kmajor_off(c + q, t, kRows), d2);
+    }
+  }
+  // dW2 = delta2^T H1
+  ok &= umma::tile_gemm(sm + SB_DZT, sm + SB_H1T, kH1, kRows, tmem, &bar, phase);
+  for (int c = 0; c < kH1; c += 8) {
+    float v[8];
+    umma::tmem_ld8(lane_addr + c, v);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) atomicAdd(grad + oW2 + t * kH1 + c + q, v[q]);
+  }
+  // dH1 = delta2 W2 -> delta1
+  stage_b(sm + SB_B, net.w2t, kH1, kH2);
+  ok &= umma::tile_gemm(sm + SB_ACT, sm + SB_B, kH1, kH2, tmem, &bar, phase);
+  for (int c = 0; c < kH1; c += 8) {
+    float v[8];
+    umma::tmem_ld8(lane_addr + c, v);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float d1 = v[q] * dsilu(zrow[c + q]);
+      warp_add(grad + oB1 + c + q, d1);
+      put_bf16(sm + SB_DZT, kmajor_off(c + q, t, kRows), d1);
+    }
+  }
+  // dW1 = delta1^T X
+  ok &= umma::tile_gemm(sm + SB_DZT, sm + SB_XT, kIn, kRows, tmem, &bar, phase);
+  for (int c = 0; c < kIn; c += 8) {
+    float v[8];
+    umma::tmem_ld8(lane_addr + c, v);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) atomicAdd(grad + oW1 + t * kIn + c + q, v[q]);
+  }
+  if (!ok && t == 0) atomicExch(err, 1);
+  umma::fence_before();
+  __syncthreads();
+  if (warp == 0) umma::tmem_free(tmem, 128);
+}
+
+// inference over n samples, one 128-sample tile per iteration
+__global__ void __launch_bounds__(128) k_mlp_infer(Net net, const __nv_bfloat16* __restrict__ X, long long n,
+                                                   float* __restrict__ y, int* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  const int t = threadIdx.x, warp = t >> 5;
+  if (t == 0) umma::mbar_init(&bar, 1);
+  if (warp == 0) umma::tmem_alloc(&tmem_slot, 128);
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tmem = tmem_slot;
+  uint32_t phase = 0;
+  bool ok = true;
+  const long long tiles = (n + kRows - 1) / kRows;
+  for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const long long s = tile * kRows + t;
+    const float v = forward_tile<false>(net, s < n ? X + s * kIn : nullptr, sm, tmem, &bar, phase, nullptr, ok);
+    if (s < n) y[s] = v;
+    if (!__syncthreads_and(ok)) break;  // block-uniform exit after a wait that gave up
+  }
+  if (!ok && t == 0) atomicExch(err, 1);
+  umma::fence_before();
+  __syncthreads();
+  if (warp == 0) umma::tmem_free(tmem, 128);
+}
+
+// Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the FP32 parameters, then the
+// BF16 copies and transposes; the gradient is cleared for the next batch
+__global__ void k_mlp_adam(float* __restrict__ theta, float* __restrict__ grad, float* __restrict__ m1,
+                           float* __restrict__ m2, float lr, float bc1, float bc2, __nv_bfloat16* __restrict__ w1,
+                           __nv_bfloat16* __restrict__ w2, __nv_bfloat16* __restrict__ w3,
+                           __nv_bfloat16* __restrict__ w2t, __nv_bfloat16* __restrict__ w3t) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= kParams) return;
+  const float g = grad[q];
+  grad[q] = 0.f;
+  const float a = 0.9f * m1[q] + 0.1f * g;
+  const float b = 0.999f * m2[q] + 0.001f * g * g;
+  m1[q] = a;
+  m2[q] = b;
+  const float w = theta[q] - lr * (a / bc1) / (sqrtf(b / bc2) + 1e-8f);
+  theta[q] = w;
+  const __nv_bfloat16 h = __float2bfloat16(w);
+  if (q >= oW1 && q < oB1) w1[q - oW1] = h;
+  if (q >= oW2 && q < oB2) {
+    const int r = (q - oW2) / kH1, c = (q - oW2) % kH1;
+    w2[q - oW2] = h;
+    w2t[c * kH2 + r] = h;
+  }
+  if (q >= oW3 && q < oB3) {
+    const int r = (q - oW3) / kH2, c = (q - oW3) % kH2;
+    w3[q - oW3] = h;
+    w3t[c * kH3 + r] = h;
+  }
+}
+
+// refresh the BF16 copies from theta (after initialisation or a set)
+__global__ void k_mlp_copies(const float* __restrict__ theta, __nv_bfloat16* __restrict__ w1,
+                             __nv_bfloat16* __restrict__ w2, __nv_bfloat16* __restrict__ w3,
+                             __nv_bfloat16* __restrict__ w2t, __nv_bfloat16* __restrict__ w3t) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= kParams) return;
+  const __nv_bfloat16 h = __float2bfloat16(theta[q]);
+  if (q >= oW1 && q < oB1) w1[q - oW1] = h;
+  if (q >= oW2 && q < oB2) {
+    const int r = (q - oW2) / kH1, c = (q - oW2) % kH1;
+    w2[q - oW2] = h;
+    w2t[c * kH2 + r] = h;
+  }
+  if (q >= oW3 && q < oB3) {
+    const int r = (q - oW3) / kH2, c = (q - oW3) % kH2;
+    w3[q - oW3] = h;
+    w3t[c * kH3 + r] = h;
+  }
+}
+
+// ===================================================== training samples
+// counter-based uniform in [0,1) (splitmix64 of seed, sample and draw)
+__device__ __forceinline__ double urand(unsigned long long seed, unsigned long long i, unsigned long long d) {
+  unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (i * 64ull + d + 1ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+__constant__ double cPu[270];  // the least-squares pseudo-inverse for unit spacing
+
+struct Shape {
+  double c[3];   // centre
+  double s[3];   // semi-axes (a sphere has three equal)
+  double R[9];   // body-to-world rotation, column-major
+  int sphere;
+};
+
+// signed distance to the shape (outside > 0); for an ellipsoid by bisection
+// on the Lagrange multiplier of the closest-point problem
+__device__ double sdist(const Shape& S, const double* x, double* foot) {
+  double d[3] = {x[0] - S.c[0], x[1] - S.c[1], x[2] - S.c[2]};
+  if (S.sphere) {
+    const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    return r - S.s[0];
+  }
+  double y[3];
+  for (int i = 0; i < 3; ++i) y[i] = S.R[0 + 3 * i] * d[0] + S.R[1 + 3 * i] * d[1] + S.R[2 + 3 * i] * d[2];
+  double g = 0.;
+  for (int i = 0; i < 3; ++i) g += y[i] * y[i] / (S.s[i] * S.s[i]);
+  const bool outside = g > 1.;
+  const double smin = fmin(S.s[0], fmin(S.s[1], S.s[2]));
+  auto F = [&](double t) {
+    double f = 0.;
+    for (int i = 0; i < 3; ++i) {
+      const double q = S.s[i] * y[i] / (S.s[i] * S.s[i] + t);
+      f += q * q;
+    }
+    return f - 1.;
+  };
+  double lo, hi;
+  if (outside) {
+    lo = 0.;
+    hi = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]) * fmax(S.s[0], fmax(S.s[1], S.s[2])) + 1.;
+  } else {
+    lo = -smin * smin;
+    hi = 0.;
+  }
+  for (int it = 0; it < 200; ++it) {  // F decreases in t on the bracket
+    const double mid = 0.5 * (lo + hi);
+    if (F(mid) > 0.) lo = mid;
+    else hi = mid;
+    if (hi - lo <= 1e-15 * fmax(1., fabs(mid))) break;
+  }
+  const double t = 0.5 * (lo + hi);
+  double q[3], dd = 0.;
+  for (int i = 0; i < 3; ++i) {
+    q[i] = S.s[i] * S.s[i] * y[i] / (S.s[i] * S.s[i] + t);
+    dd += (y[i] - q[i]) * (y[i] - q[i]);
+  }
+  if (foot)
+    for (int i = 0; i < 3; ++i) foot[i] = q[i];
+  return outside ? sqrt(dd) : -sqrt(dd);
+}
+
+// least-squares curvature of a 3x3x3 stencil f (order z-outer, x-inner) of
+// spacing h (interface.f90:57-111 without its clamps)
+__device__ double lsq_curv(const double* f, double h) {
+  double x[10];
+  for (int r = 1; r < 10; ++r) {
+    double acc = 0.;
+    for (int q = 0; q < 27; ++q) acc += cPu[r * 27 + q] * f[q];
+    x[r] = acc;
+  }
+  for (int r = 1; r <= 3; ++r) x[r] /= h;
+  for (int r = 4; r <= 9; ++r) x[r] /= h * h;
+  const double nv = sqrt(x[1] * x[1] + x[2] * x[2] + x[3] * x[3]);
+  const double n3 = nv * nv * nv;
+  const double t1 = (x[4] + x[5] + x[6]) / nv;
+  const double t2 = (x[1] * x[1] * x[4] + x[2] * x[2] * x[5] + x[3] * x[3] * x[6]) / n3;
+  const double t3 = 2. * (x[1] * x[2] * x[7] + x[1] * x[3] * x[8] + x[2] * x[3] * x[9]) / n3;
+  return -((t1 - t2) - t3);
+}
+
+// principal curvatures k1 >= k2 of an ellipsoid at the surface point q
+// (body frame), positive where convex
+__device__ void ellipsoid_principal(const Shape& S, const double* q, double& k1, double& k2) {
+  double g[3], gn = 0.;
+  for (int i = 0; i < 3; ++i) {
+    g[i] = 2. * q[i] / (S.s[i] * S.s[i]);
+    gn += g[i] * g[i];
+  }
+  gn = sqrt(gn);
+  double n[3] = {g[0] / gn, g[1] / gn, g[2] / gn};
+  // M = P H P / |g| with H = diag(2/s^2), P = I - n n^T: eigenvalues 0, k1, k2
+  double M[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double acc = 0.;
+      for (int k = 0; k < 3; ++k) {
+        const double Pik = (i == k ? 1. : 0.) - n[i] * n[k];
+        const double Pkj = (k == j ? 1. : 0.) - n[k] * n[j];
+        acc += Pik * (2. / (S.s[k] * S.s[k])) * Pkj;
+      }
+      M[i][j] = acc / gn;
+    }
+  const double T = M[0][0] + M[1][1] + M[2][2];
+  double T2 = 0.;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) T2 += M[i][j] * M[j][i];
+  const double Q = 0.5 * (T * T - T2);
+  const double disc = fmax(0.25 * T * T - Q, 0.);
+  k1 = 0.5 * T + sqrt(disc);
+  k2 = 0.5 * T - sqrt(disc);
+}
+
+// Sample i: a seeded sphere (R in [3,40] cells) or ellipsoid (semi-axes in
+// [4,40] cells, random rotation) on a unit grid, a grid node x with
+// |phi(x)| <= 3 near its surface, phi the exact signed distance.  Writes the
+// 27 inputs (phi(x+o) - phi(x), o in {-1,0,1}^3), the label (the
+// least-squares curvature of the stencil of spacing 1/4 at x, the method on a
+// grid refined 4x) and, in extra, the plain curvature at spacing 1, the
+// analytic curvature and the shape's smallest radius.
+__global__ void k_mlp_gen(unsigned long long seed, long long n, __nv_bfloat16* __restrict__ X,
+                          float* __restrict__ label, float* __restrict__ extra) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double pi2 = 6.283185307179586;
+  Shape S;
+  double x[3] = {0., 0., 0.}, kana = 0., lab = 0., ff[27];
+  int d = 0;
+  // Draw shapes and points until the node is near the surface (|phi| <= 3)
+  // and the level set through it is resolved: curvature radius of at least 3
+  // cells (|kappa dx| <= 2/3), the focal points more than two cells further
+  // in (1 + k_i (phi - 2) >= 1/2), and the refined-grid label within 0.02 of
+  // the exact curvature (its stencil does not straddle a kink of the signed
+  // distance).
+  for (int tries = 0; tries < 256; ++tries) {
+    S.sphere = urand(seed, i, d++) < 0.5;
+    for (int k = 0; k < 3; ++k) S.c[k] = urand(seed, i, d++);
+    if (S.sphere) {
+      const double R = 3. + 37. * urand(seed, i, d++);
+      S.s[0] = S.s[1] = S.s[2] = R;
+    } else {
+      for (int k = 0; k < 3; ++k) S.s[k] = 4. + 36. * urand(seed, i, d++);
+      const double u1 = urand(seed, i, d++), u2 = urand(seed, i, d++), u3 = urand(seed, i, d++);
+      const double qx = sqrt(1. - u1) * sin(pi2 * u2), qy = sqrt(1. - u1) * cos(pi2 * u2);
+      const double qz = sqrt(u1) * sin(pi2 * u3), qw = sqrt(u1) * cos(pi2 * u3);
+      S.R[0] = 1. - 2. * (qy * qy + qz * qz); S.R[1] = 2. * (qx * qy + qz * qw); S.R[2] = 2. * (qx * qz - qy * qw);
+      S.R[3] = 2. * (qx * qy - qz * qw); S.R[4] = 1. - 2. * (qx * qx + qz * qz); S.R[5] = 2. * (qy * qz + qx * qw);
+      S.R[6] = 2. * (qx * qz + qy * qw); S.R[7] = 2. * (qy * qz - qx * qw); S.R[8] = 1. - 2. * (qx * qx + qy * qy);
+    }
+    // a direction, a surface point along it, an offset along the normal
+    const double zz = 2. * urand(seed, i, d++) - 1., ph = pi2 * urand(seed, i, d++);
+    const double rr = sqrt(fmax(0., 1. - zz * zz));
+    const double u[3] = {rr * cos(ph), rr * sin(ph), zz};
+    const double off = 6. * urand(seed, i, d++) - 3.;
+    double p[3];
+    if (S.sphere) {
+      for (int k = 0; k < 3; ++k) p[k] = S.c[k] + (S.s[0] + off) * u[k];
+    } else {
+      double g = 0.;
+      for (int k = 0; k < 3; ++k) g += u[k] * u[k] / (S.s[k] * S.s[k]);
+      double q[3], nq[3], nn = 0.;
+      for (int k = 0; k < 3; ++k) {
+        q[k] = u[k] / sqrt(g);
+        nq[k] = q[k] / (S.s[k] * S.s[k]);
+        nn += nq[k] * nq[k];
+      }
+      nn = sqrt(nn);
+      double pb[3];
+      for (int k = 0; k < 3; ++k) pb[k] = q[k] + off * nq[k] / nn;
+      for (int k = 0; k < 3; ++k) p[k] = S.c[k] + S.R[k] * pb[0] + S.R[k + 3] * pb[1] + S.R[k + 6] * pb[2];
+    }
+    for (int k = 0; k < 3; ++k) x[k] = rint(p[k]);
+    double foot[3];
+    const double phi0 = sdist(S, x, foot);
+    if (fabs(phi0) > 3.) continue;
+    double k1, k2;
+    if (S.sphere) {
+      k1 = k2 = 1. / S.s[0];
+    } else {
+      ellipsoid_principal(S, foot, k1, k2);
+    }
+    // the level set through x: -(k1/(1+k1 phi) + k2/(1+k2 phi)), reference sign
+    const double f1 = 1. + k1 * phi0, f2 = 1. + k2 * phi0;
+    if (fmin(1. + k1 * (phi0 - 2.), 1. + k2 * (phi0 - 2.)) < 0.5) continue;
+    kana = -(k1 / f1 + k2 / f2);
+    if (fabs(kana) > 2. / 3.) continue;
+    int q = 0;
+    for (int dk = -1; dk <= 1; ++dk)
+      for (int dj = -1; dj <= 1; ++dj)
+        for (int di = -1; di <= 1; ++di) {
+          const double pf[3] = {x[0] + 0.25 * di, x[1] + 0.25 * dj, x[2] + 0.25 * dk};
+          ff[q++] = sdist(S, pf, nullptr);
+        }
+    lab = lsq_curv(ff, 0.25);
+    if (fabs(lab - kana) > 0.02) continue;
+    break;
+  }
+  double fc[27];
+  int q = 0;
+  for (int dk = -1; dk <= 1; ++dk)
+    for (int dj = -1; dj <= 1; ++dj)
+      for (int di = -1; di <= 1; ++di) {
+        const double pc[3] = {x[0] + di, x[1] + dj, x[2] + dk};
+        fc[q++] = sdist(S, pc, nullptr);
+      }
+  for (int k = 0; k < 27; ++k) X[i * kIn + k] = __float2bfloat16((float)(fc[k] - fc[13]));
+  for (int k = 27; k < kIn; ++k) X[i * kIn + k] = __float2bfloat16(0.f);
+  label[i] = (float)lab;
+  extra[3 * i + 0] = (float)lsq_curv(fc, 1.);
+  extra[3 * i + 1] = (float)kana;
+  extra[3 * i + 2] = (float)fmin(S.s[0], fmin(S.s[1], S.s[2]));
+}
+
 }  // namespace
 }  // namespace icls
+
+struct icls_mlp {
+  float *theta = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
+  __nv_bfloat16 *w1 = nullptr, *w2 = nullptr, *w3 = nullptr, *w2t = nullptr, *w3t = nullptr;
+  float* zbuf = nullptr;     // pre-activations of one batch
+  long long zcap = 0;        // samples zbuf holds
+  float* loss = nullptr;     // per-epoch loss sums
+  int nloss = 0;
+  int* err = nullptr;
+  __nv_bfloat16* X = nullptr;  // training inputs [n][32]
+  float *label = nullptr, *extra = nullptr;
+  long long n_train = 0;
+  __nv_bfloat16* Xh = nullptr;  // held-out set
+  float *labelh = nullptr, *extrah = nullptr, *yh = nullptr;
+  long long n_hold = 0;
+  long long step = 0;
+  cudaStream_t s = nullptr;
+};
+
+namespace {
+using namespace icls;
+
+Net net_of(const icls_mlp* m) { return Net{m->theta, m->w1, m->w2, m->w3, m->w2t, m->w3t}; }
+
+unsigned long long mix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+int sync_err(icls_mlp* m) {
+  int h = 0;
+  if (cudaMemcpyAsync(&h, m->err, sizeof(int), cudaMemcpyDeviceToHost, m->s) != cudaSuccess) return ICLS_E_CUDA;
+  if (cudaStreamSynchronize(m->s) != cudaSuccess) return ICLS_E_CUDA;
+  if (cudaGetLastError() != cudaSuccess) return ICLS_E_CUDA;
+  return h ? ICLS_E_CUDA : ICLS_OK;
+}
+
+int ensure_zbuf(icls_mlp* m, long long n) {
+  if (n <= m->zcap) return ICLS_OK;
+  if (m->zbuf) cudaFree(m->zbuf);
+  m->zbuf = nullptr;
+  if (cudaMalloc(&m->zbuf, sizeof(float) * (size_t)n * (kH1 + kH2 + kH3)) != cudaSuccess) return ICLS_E_NOMEM;
+  m->zcap = n;
+  return ICLS_OK;
+}
+
+void refresh_copies(icls_mlp* m) {
+  k_mlp_copies<<<(kParams + 255) / 256, 256, 0, m->s>>>(m->theta, m->w1, m->w2, m->w3, m->w2t, m->w3t);
+}
+
+}  // namespace
+
+extern "C" int icls_mlp_create(icls_mlp** out, unsigned long long seed) {
+  if (!out) return ICLS_E_ARG;
+  *out = nullptr;
+  icls_mlp* m = new (std::nothrow) icls_mlp();
+  if (!m) return ICLS_E_NOMEM;
+  bool ok = cudaStreamCreateWithFlags(&m->s, cudaStreamNonBlocking) == cudaSuccess;
+  for (float** f : {&m->theta, &m->grad, &m->m1, &m->m2}) ok = ok && cudaMalloc(f, sizeof(float) * kParams) == cudaSuccess;
+  ok = ok && cudaMalloc(&m->w1, 2 * kH1 * kIn) == cudaSuccess && cudaMalloc(&m->w2, 2 * kH2 * kH1) == cudaSuccess &&
+       cudaMalloc(&m->w3, 2 * kH3 * kH2) == cudaSuccess && cudaMalloc(&m->w2t, 2 * kH2 * kH1) == cudaSuccess &&
+       cudaMalloc(&m->w3t, 2 * kH3 * kH2) == cudaSuccess && cudaMalloc(&m->err, sizeof(int)) == cudaSuccess;
+  ok = ok && cudaFuncSetAttribute(icls::k_mlp_train_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, icls::SB_TRAIN) ==
+                 cudaSuccess &&
+       cudaFuncSetAttribute(icls::k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, icls::SB_INFER) ==
+           cudaSuccess;
+  if (!ok) {
+    icls_mlp_destroy(m);
+    return ICLS_E_NOMEM;
+  }
+  // uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) weights, zero biases; the
+  // padding inputs 27..31 of W1 stay zero
+  std::vector<float> th(kParams, 0.f);
+  unsigned long long st = seed;
+  auto unif = [&](float a) {
+    st = mix64(st);
+    return (float)((double)(st >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0) * a;
+  };
+  for (int r = 0; r < kH1; ++r)
+    for (int c = 0; c < 27; ++c) th[oW1 + r * kIn + c] = unif(1.f / sqrtf(27.f));
+  for (int q = 0; q < kH2 * kH1; ++q) th[oW2 + q] = unif(1.f / sqrtf((float)kH1));
+  for (int q = 0; q < kH3 * kH2; ++q) th[oW3 + q] = unif(1.f / sqrtf((float)kH2));
+  for (int q = 0; q < kH3; ++q) th[oW4 + q] = unif(1.f / sqrtf((float)kH3));
+  cudaMemcpyAsync(m->theta, th.data(), sizeof(float) * kParams, cudaMemcpyHostToDevice, m->s);
+  for (float* f : {m->grad, m->m1, m->m2}) cudaMemsetAsync(f, 0, sizeof(float) * kParams, m->s);
+  cudaMemsetAsync(m->err, 0, sizeof(int), m->s);
+  refresh_copies(m);
+  if (cudaStreamSynchronize(m->s) != cudaSuccess) {
+    icls_mlp_destroy(m);
+    return ICLS_E_CUDA;
+  }
+  *out = m;
+  return ICLS_OK;
+}
+
+extern "C" int icls_mlp_destroy(icls_mlp* m) {
+  if (!m) return ICLS_E_ARG;
+  if (m->s) cudaStreamSynchronize(m->s);
+  for (void* p : {(void*)m->theta, (void*)m->grad, (void*)m->m1, (void*)m->m2, (void*)m->w1, (void*)m->w2,
+                  (void*)m->w3, (void*)m->w2t, (void*)m->w3t, (void*)m->zbuf, (void*)m->loss, (void*)m->err,
+                  (void*)m->X, (void*)m->label, (void*)m->extra, (void*)m->Xh, (void*)m->labelh, (void*)m->extrah,
+                  (void*)m->yh})
+    if (p) cudaFree(p);
+  if (m->s) cudaStreamDestroy(m->s);
+  delete m;
+  return ICLS_OK;
+}
+
+// n_train a power of two (the epoch shuffle is an affine map mod n_train)
+extern "C" int icls_mlp_make_data(icls_mlp* m, unsigned long long seed, long long n_train, long long n_hold) {
+  if (!m || n_train < 128 || (n_train & (n_train - 1)) || n_hold < 1) return ICLS_E_ARG;
+  static bool pinv_set = false;
+  if (!pinv_set) {
+    double pu[270];
+    icls::pseudo_inverse(1., 1., 1., pu);
+    if (cudaMemcpyToSymbol(icls::cPu, pu, sizeof(pu)) != cudaSuccess) return ICLS_E_CUDA;
+    pinv_set = true;
+  }
+  for (void* p : {(void*)m->X, (void*)m->label, (void*)m->extra, (void*)m->Xh, (void*)m->labelh, (void*)m->extrah,
+                  (void*)m->yh})
+    if (p) cudaFree(p);
+  m->X = m->Xh = nullptr;
+  m->label = m->extra = m->labelh = m->extrah = m->yh = nullptr;
+  bool ok = cudaMalloc(&m->X, 2 * (size_t)n_train * kIn) == cudaSuccess &&
+            cudaMalloc(&m->label, 4 * (size_t)n_train) == cudaSuccess &&
+            cudaMalloc(&m->extra, 12 * (size_t)n_train) == cudaSuccess &&
+            cudaMalloc(&m->Xh, 2 * (size_t)n_hold * kIn) == cudaSuccess &&
+            cudaMalloc(&m->labelh, 4 * (size_t)n_hold) == cudaSuccess &&
+            cudaMalloc(&m->extrah, 12 * (size_t)n_hold) == cudaSuccess &&
+            cudaMalloc(&m->yh, 4 * (size_t)n_hold) == cudaSuccess;
+  if (!ok) return ICLS_E_NOMEM;
+  m->n_train = n_train;
+  m->n_hold = n_hold;
+  icls::k_mlp_gen<<<(unsigned)((n_train + 127) / 128), 128, 0, m->s>>>(seed, n_train, m->X, m->label, m->extra);
+  icls::k_mlp_gen<<<(unsigned)((n_hold + 127) / 128), 128, 0, m->s>>>(mix64(seed ^ 0x5bd1e995ull), n_hold, m->Xh,
+                                                                      m->labelh, m->extrah);
+  return sync_err(m);
+}
+
+// epochs over the training set in batches of `batch` (a multiple of 128
+// dividing n_train), Adam with step size lr; loss_out[e] = mean squared
+// error of epoch e (kappa*dx units), if given
+extern "C" int icls_mlp_train(icls_mlp* m, int epochs, int batch, double lr, unsigned long long seed,
+                              double* loss_out) {
+  if (!m || !m->X || epochs < 1 || batch < 128 || batch % 128 || m->n_train % batch) return ICLS_E_ARG;
+  int rc = ensure_zbuf(m, batch);
+  if (rc) return rc;
+  if (m->nloss < epochs) {
+    if (m->loss) cudaFree(m->loss);
+    if (cudaMalloc(&m->loss, sizeof(float) * epochs) != cudaSuccess) return ICLS_E_NOMEM;
+    m->nloss = epochs;
+  }
+  cudaMemsetAsync(m->loss, 0, sizeof(float) * epochs, m->s);
+  const Net net = net_of(m);
+  const long long steps = m->n_train / batch;
+  const float scale = 2.f / (float)batch;
+  for (int e = 0; e < epochs; ++e) {
+    const unsigned long long pa = mix64(seed + 2 * (unsigned long long)e) | 1ull;
+    const unsigned long long pb = mix64(seed + 2 * (unsigned long long)e + 1);
+    for (long long st = 0; st < steps; ++st) {
+      icls::k_mlp_train_tile<<<batch / 128, 128, icls::SB_TRAIN, m->s>>>(net, m->X, m->label, m->n_train,
+                                                                          st * batch, pa, pb, scale, m->zbuf,
+                                                                          m->grad, m->loss + e, m->err);
+      ++m->step;
+      const float bc1 = 1.f - powf(0.9f, (float)m->step), bc2 = 1.f - powf(0.999f, (float)m->step);
+      icls::k_mlp_adam<<<(kParams + 255) / 256, 256, 0, m->s>>>(m->theta, m->grad, m->m1, m->m2, (float)lr, bc1, bc2,
+                                                                 m->w1, m->w2, m->w3, m->w2t, m->w3t);
+    }
+  }
+  rc = sync_err(m);
+  if (rc) return rc;
+  if (loss_out) {
+    std::vector<float> l(epochs);
+    cudaMemcpy(l.data(), m->loss, sizeof(float) * epochs, cudaMemcpyDeviceToHost);
+    for (int e = 0; e < epochs; ++e) loss_out[e] = l[e] / (double)m->n_train;
+  }
+  return ICLS_OK;
+}
+
+// y[0..n) = network(X[0..n)) on device arrays (X BF16 [n][32])
+extern "C" int icls_mlp_infer(icls_mlp* m, const void* X, float* y, long long n, void* stream) {
+  if (!m || !X || !y || n < 1) return ICLS_E_ARG;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : m->s;
+  const long long tiles = (n + 127) / 128;
+  const int grid = (int)std::min<long long>(tiles, 2 * 148);
+  icls::k_mlp_infer<<<grid, 128, icls::SB_INFER, s>>>(net_of(m), static_cast<const __nv_bfloat16*>(X), n, y, m->err);
+  if (stream) return cudaGetLastError() == cudaSuccess ? ICLS_OK : ICLS_E_CUDA;
+  return sync_err(m);
+}
+
+// statistics of the held-out set, kappa*dx units: stats[0..3] = rms of
+// (mlp - label), (mlp - analytic), (plain - analytic), (label - analytic);
+// stats[4..5] = max |mlp - analytic|, max |plain - analytic|; stats[6] =
+// rms |analytic|; stats[7] = samples
+extern "C" int icls_mlp_eval(icls_mlp* m, double* stats) {
+  if (!m || !m->Xh || !stats) return ICLS_E_ARG;
+  int rc = icls_mlp_infer(m, m->Xh, m->yh, m->n_hold, nullptr);
+  if (rc) return rc;
+  const size_t n = (size_t)m->n_hold;
+  std::vector<float> y(n), lab(n), ex(3 * n);
+  cudaMemcpy(y.data(), m->yh, 4 * n, cudaMemcpyDeviceToHost);
+  cudaMemcpy(lab.data(), m->labelh, 4 * n, cudaMemcpyDeviceToHost);
+  cudaMemcpy(ex.data(), m->extrah, 12 * n, cudaMemcpyDeviceToHost);
+  double s[8] = {0, 0, 0, 0, 0, 0, 0, (double)n};
+  for (size_t i = 0; i < n; ++i) {
+    const double ka = ex[3 * i + 1], kp = ex[3 * i + 0];
+    s[0] += (y[i] - lab[i]) * (double)(y[i] - lab[i]);
+    s[1] += (y[i] - ka) * (y[i] - ka);
+    s[2] += (kp - ka) * (kp - ka);
+    s[3] += (lab[i] - ka) * (lab[i] - ka);
+    s[4] = std::max(s[4], std::fabs(y[i] - ka));
+    s[5] = std::max(s[5], std::fabs(kp - ka));
+    s[6] += ka * ka;
+  }
+  for (int q : {0, 1, 2, 3, 6}) s[q] = std::sqrt(s[q] / (double)n);
+  for (int q = 0; q < 8; ++q) stats[q] = s[q];
+  return ICLS_OK;
+}
+
+// the FP32 parameters (29057 floats in the layout of k_mlp.cu) to or from host
+extern "C" int icls_mlp_params(icls_mlp* m, float* host, int get) {
+  if (!m || !host) return ICLS_E_ARG;
+  if (get) {
+    if (cudaMemcpy(host, m->theta, sizeof(float) * kParams, cudaMemcpyDeviceToHost) != cudaSuccess) return ICLS_E_CUDA;
+    return ICLS_OK;
+  }
+  if (cudaMemcpy(m->theta, host, sizeof(float) * kParams, cudaMemcpyHostToDevice) != cudaSuccess) return ICLS_E_CUDA;
+  refresh_copies(m);
+  return sync_err(m);
+}
+
+// the gradient of the summed squared error x scale over samples 0..n-1 of X
+// (device BF16 [n][32], labels device FP32), n a power of two >= 128, into
+// host grad[29057]; loss = sum of squared errors
+extern "C" int icls_mlp_grad(icls_mlp* m, const void* X, const float* label, long long n, float scale, float* grad,
+                             double* loss) {
+  if (!m || !X || !label || !grad || n < 128 || (n & (n - 1))) return ICLS_E_ARG;
+  int rc = ensure_zbuf(m, n);
+  if (rc) return rc;
+  if (m->nloss < 1) {
+    if (cudaMalloc(&m->loss, sizeof(float)) != cudaSuccess) return ICLS_E_NOMEM;
+    m->nloss = 1;
+  }
+  cudaMemsetAsync(m->loss, 0, sizeof(float), m->s);
+  cudaMemsetAsync(m->grad, 0, sizeof(float) * kParams, m->s);
+  icls::k_mlp_train_tile<<<(unsigned)(n / 128), 128, icls::SB_TRAIN, m->s>>>(
+      net_of(m), static_cast<const __nv_bfloat16*>(X), label, n, 0, 1ull, 0ull, scale, m->zbuf, m->grad, m->loss,
+      m->err);
+  rc = sync_err(m);
+  if (rc) return rc;
+  cudaMemcpy(grad, m->grad, sizeof(float) * kParams, cudaMemcpyDeviceToHost);
+  float l = 0.f;
+  cudaMemcpy(&l, m->loss, sizeof(float), cudaMemcpyDeviceToHost);
+  if (loss) *loss = l;
+  cudaMemset(m->grad, 0, sizeof(float) * kParams);
+  return ICLS_OK;
+}
 
 extern "C" int icls_tc_gemm_bf16(const void* a, const void* b, float* d, int n, int k, void* stream) {
   if (!a || !b || !d) return ICLS_E_ARG;

@@ -117,7 +117,8 @@ __device__ __forceinline__ void tmem_ld8(uint32_t addr, float* v) {
 // the operands are in shared memory; returns false if the wait gave up.
 __device__ __forceinline__ bool tile_gemm(const void* a, const void* b, int n, int k, uint32_t d_tmem, uint64_t* bar,
                                           uint32_t& phase) {
-  fence_async_smem();
+  fence_async_smem();  // the operands' generic-proxy stores before the tensor core reads them
+  fence_before();      // earlier tensor-memory reads before the columns are overwritten
   __syncthreads();
   if (threadIdx.x == 0) {
     fence_after();

@@ -183,6 +183,34 @@ int icls_get_curvature(icls_ctx* ctx, int l);               /* interface.f90:20-
  * (nb_cnt, levelset.f90:158).                                           */
 int icls_band_count(icls_ctx* ctx, int l, long long* nb_cnt);
 
+/* ---- learned interface curvature ----
+ * No counterpart in the reference: the network that replaces the
+ * get_curvature stencil (interface.f90:20-119) near the interface in the
+ * learned form.  27 -> 128 -> 128 -> 64 -> 1 SiLU MLP, BF16 weights and
+ * activations on tcgen05 tiles, FP32 accumulation and FP32 Adam; input the
+ * stencil (phi(x + o dx) - phi(x)) / dx, o in {-1,0,1}^3 (z outer, x inner),
+ * output kappa * dx.  Training samples come from seeded spheres and
+ * ellipsoids (exact signed distance) with the least-squares curvature of a
+ * 4x refined stencil as label.  All arrays named "device" live in GPU memory. */
+typedef struct icls_mlp icls_mlp;
+#define ICLS_MLP_PARAMS 29057
+int icls_mlp_create(icls_mlp** out, unsigned long long seed);
+int icls_mlp_destroy(icls_mlp* m);
+/* training and held-out samples; n_train a power of two */
+int icls_mlp_make_data(icls_mlp* m, unsigned long long seed, long long n_train, long long n_hold);
+/* loss_out[epochs] (optional): mean squared error per epoch */
+int icls_mlp_train(icls_mlp* m, int epochs, int batch, double lr, unsigned long long seed, double* loss_out);
+/* held-out statistics (kappa*dx): rms(mlp-label), rms(mlp-analytic), rms(plain-analytic),
+ * rms(label-analytic), max|mlp-analytic|, max|plain-analytic|, rms|analytic|, samples */
+int icls_mlp_eval(icls_mlp* m, double stats[8]);
+/* y (device FP32 [n]) = network(X (device BF16 [n][32])); stream 0: synchronous */
+int icls_mlp_infer(icls_mlp* m, const void* X, float* y, long long n, void* stream);
+/* parameters to (get = 1) or from (get = 0) host float[ICLS_MLP_PARAMS] */
+int icls_mlp_params(icls_mlp* m, float* host, int get);
+/* gradient of scale * sum (y - label)^2 over n samples (power of two >= 128) into host grad */
+int icls_mlp_grad(icls_mlp* m, const void* X, const float* label, long long n, float scale, float* grad,
+                  double* loss);
+
 /* ---- tensor-core tile check ----
  * No counterpart in the reference.  d (128 x n FP32, row-major) = a (128 x k
  * BF16, row-major) * b (n x k BF16, row-major)^T on one tcgen05 tile, the

@@ -31,3 +31,95 @@ def test_tc_tile_matches_fp32_product(gpu_available, n, k):
     out = dd.cpu()
     err = float((out - ref).abs().max()) / float(ref.abs().max())
     assert err <= 1e-5, err
+
+
+# ---------------------------------------------------------------- network
+def _lib():
+    lib = gpu_backend().lib
+    P = C.c_void_p
+    sig = {
+        "icls_mlp_create": [C.POINTER(P), C.c_ulonglong],
+        "icls_mlp_destroy": [P],
+        "icls_mlp_make_data": [P, C.c_ulonglong, C.c_longlong, C.c_longlong],
+        "icls_mlp_train": [P, C.c_int, C.c_int, C.c_double, C.c_ulonglong, C.POINTER(C.c_double)],
+        "icls_mlp_eval": [P, C.POINTER(C.c_double)],
+        "icls_mlp_params": [P, C.POINTER(C.c_float), C.c_int],
+        "icls_mlp_grad": [P, P, P, C.c_longlong, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_double)],
+    }
+    for name, args in sig.items():
+        getattr(lib, name).argtypes = args
+        getattr(lib, name).restype = C.c_int
+    return lib
+
+
+def _sphere_stencils(n, seed):
+    """27-value stencils of signed distances to seeded spheres, as the network
+    takes them: (phi(x + o) - phi(x)), o in {-1,0,1}^3 (z outer), padded to 32"""
+    rng = np.random.default_rng(seed)
+    o = np.array([(i, j, k) for k in (-1, 0, 1) for j in (-1, 0, 1) for i in (-1, 0, 1)], dtype=float)
+    X = np.zeros((n, 32))
+    lab = np.zeros(n)
+    for s in range(n):
+        R = rng.uniform(3, 40)
+        u = rng.normal(size=3)
+        u /= np.linalg.norm(u)
+        x = np.rint(rng.uniform(size=3) + (R + rng.uniform(-2, 2)) * u)
+        c = rng.uniform(size=3)
+        phi = np.linalg.norm(x + o - c, axis=1) - R
+        X[s, :27] = phi - phi[13]
+        lab[s] = -2.0 / np.linalg.norm(x - c)
+    return X, lab
+
+
+def test_mlp_gradient_matches_cpu_oracle(gpu_available):
+    import torch
+    from oracle.mlp_oracle import NPARAMS, OFF, gradient
+    lib = _lib()
+    m = C.c_void_p()
+    assert lib.icls_mlp_create(C.byref(m), 7) == 0
+    try:
+        theta = np.zeros(NPARAMS, dtype=np.float32)
+        assert lib.icls_mlp_params(m, theta.ctypes.data_as(C.POINTER(C.c_float)), 1) == 0
+        n = 256
+        X, lab = _sphere_stencils(n, 11)
+        dX = torch.tensor(X, dtype=torch.float32).to(torch.bfloat16).cuda()
+        dl = torch.tensor(lab, dtype=torch.float32).cuda()
+        g = np.zeros(NPARAMS, dtype=np.float32)
+        loss = C.c_double()
+        scale = 2.0 / n
+        assert lib.icls_mlp_grad(m, dX.data_ptr(), dl.data_ptr(), n, scale, g.ctypes.data_as(C.POINTER(C.c_float)),
+                                 C.byref(loss)) == 0
+        ref, ref_loss = gradient(theta, dX.float().cpu().numpy(), dl.cpu().numpy(), scale)
+        print("\nloss gpu %.6e oracle %.6e" % (loss.value, ref_loss))
+        errs = {}
+        for name, (a, b) in OFF.items():
+            errs[name] = np.linalg.norm(g[a:b] - ref[a:b]) / max(np.linalg.norm(ref[a:b]), 1e-30)
+        print("gradient relative L2 per block", {k: "%.2e" % v for k, v in errs.items()})
+        assert abs(loss.value - ref_loss) <= 1e-4 * ref_loss
+        for name, err in errs.items():
+            assert err <= 2e-3, (name, err)
+    finally:
+        lib.icls_mlp_destroy(m)
+
+
+def test_mlp_training_beats_plain_stencil(gpu_available):
+    """4M seeded samples, 20 epochs of batch 8192 (the training configuration):
+    the network's held-out curvature error against the analytic curvature is
+    below the plain 10x27 stencil's."""
+    lib = _lib()
+    m = C.c_void_p()
+    assert lib.icls_mlp_create(C.byref(m), 2024) == 0
+    try:
+        assert lib.icls_mlp_make_data(m, 99, 1 << 22, 1 << 16) == 0
+        losses = (C.c_double * 20)()
+        assert lib.icls_mlp_train(m, 20, 8192, 1e-3, 5, losses) == 0
+        st = (C.c_double * 8)()
+        assert lib.icls_mlp_eval(m, st) == 0
+        print("\nloss per epoch", ["%.3e" % v for v in losses])
+        print("held-out (kappa*dx): rms mlp-label %.3e, mlp-analytic %.3e, plain-analytic %.3e, "
+              "label-analytic %.3e, max mlp-analytic %.3e, max plain-analytic %.3e, rms analytic %.3e, n %d"
+              % (tuple(st[:7]) + (int(st[7]),)))
+        assert losses[19] < 0.1 * losses[0]
+        assert st[1] < st[2]
+    finally:
+        lib.icls_mlp_destroy(m)
