@@ -95,7 +95,13 @@ int validate(const icls_config* c) {
   if (c->ls_adv_space != ICLS_HOUC5 && c->ls_adv_space != ICLS_WENO5) return ICLS_E_CONFIG;
   if (c->i_space != ICLS_HOUC5 && c->i_space != ICLS_WENO5) return ICLS_E_CONFIG;
   if (c->precision != ICLS_FP64 && c->precision != ICLS_FP32) return ICLS_E_CONFIG;
-  if (c->curvature_model != ICLS_CURV_STENCIL) return ICLS_E_UNSUPPORTED;
+  if (c->curvature_model != ICLS_CURV_STENCIL && c->curvature_model != ICLS_CURV_MLP) return ICLS_E_CONFIG;
+  if (c->curvature_model == ICLS_CURV_MLP) {
+    // the network reads the stencil in units of one isotropic spacing
+    const double dx = c->lx / c->itot, dy = c->ly / c->jtot, dz = c->lz / c->ktot;
+    if (dx != dy || dx != dz) return ICLS_E_UNSUPPORTED;
+    if (!(c->mlp_fallback_tol > 0.)) return ICLS_E_CONFIG;
+  }
   return ICLS_OK;
 }
 
@@ -219,6 +225,10 @@ int allocate(Ctx& c) {
       AL(m.mask, (size_t)P.nI);
     }
   }
+  if (c.cfg.curvature_model == ICLS_CURV_MLP) {
+    const int rc = mlp_buffers(c, (int)std::min<long long>(P.nI, 1LL << 21));
+    if (rc) return rc;
+  }
   c.inflated.assign(P.L, 0);
   c.vol_dirty.assign(P.L, 0);
   c.init_volume_h.assign(P.L, 0.);
@@ -247,6 +257,8 @@ void release(Ctx& c) {
   if (c.lpartials) cudaFree(c.lpartials);
   if (c.drs) cudaFree(c.drs);
   if (c.stage) cudaFree(c.stage);
+  for (void* f : {(void*)c.mlp_X, c.mlp_rec, (void*)c.mlp_y, (void*)c.mlp_count, (void*)c.mlp_stats})
+    if (f) cudaFree(f);
   if (c.dsc) cudaFree(c.dsc);
   if (c.h_vol) cudaFreeHost(c.h_vol);
   if (c.h_sc) cudaFreeHost(c.h_sc);
@@ -734,12 +746,15 @@ void fix_curv(Ctx& c) {
   std::vector<LsBatch> b = single(c, l, kStageRows, c_region(c.P, c.win[l].box, 1));
   LsTask& t = b[0].t[0];
   t.phi0 = c.lv[l];
+  const bool mlp = c.cfg.curvature_model == ICLS_CURV_MLP && c.net;
   if (c.cfg.TwoD) {
     t.out = c.curv;
     launch_curvature(c, b[0], c.nrm_m);
+    if (mlp) launch_mlp_curvature(c, b[0]);
   } else {
     t.out = member(c, l).fit;
     launch_curvature(c, b[0], c.nrm_m);
+    if (mlp) launch_mlp_curvature(c, b[0]);
     t.phis = member(c, l).fit;
     t.out = c.curv;
     launch_recurvature(c, b[0]);
@@ -748,8 +763,11 @@ void fix_curv(Ctx& c) {
 }
 
 // gfm4p, GFM/'del' (gfm.f90:17-267), one group of drops at a time, each
-// drop with its member's curvature buffers.  ipot is evaluated by icls_ipot.
-void gfm4p(Ctx& c) {
+// drop with its member's curvature buffers; with the learned curvature the
+// network replaces get_curvature's output near the interface.  ipot is
+// evaluated by icls_ipot.
+int gfm4p(Ctx& c) {
+  if (c.cfg.curvature_model == ICLS_CURV_MLP && !c.net) return ICLS_E_STATE;
   std::swap(c.px, c.pxold);
   std::swap(c.py, c.pyold);
   std::swap(c.pz, c.pzold);
@@ -769,6 +787,7 @@ void gfm4p(Ctx& c) {
         t.out = c.cfg.TwoD ? member(c, t.l).cv : member(c, t.l).fit;
       }
       launch_curvature(c, b, nullptr);
+      if (c.cfg.curvature_model == ICLS_CURV_MLP) launch_mlp_curvature(c, b);
     }
     if (!c.cfg.TwoD)
       for (LsBatch& b : b1) {
@@ -790,6 +809,7 @@ void gfm4p(Ctx& c) {
   }
   c.curv_stale = true;
   c.nrm_stale = true;
+  return ICLS_OK;
 }
 
 int read_scalars(Ctx& c) {
@@ -1063,7 +1083,8 @@ int icls_fillps(icls_ctx* h) {
 
 int icls_gfm4p(icls_ctx* h) {
   NEED(h);
-  gfm4p(h->c);
+  const int rc = gfm4p(h->c);
+  if (rc) return rc;
   return check_launch();
 }
 
@@ -1229,7 +1250,8 @@ int icls_step(icls_ctx* h, int istep, int begin) {
   launch_stream_vel(c);
   launch_ab2(c);
   if (c.cfg.solveLS) {
-    gfm4p(c);
+    rc = gfm4p(c);
+    if (rc) return rc;
     launch_fillps(c, 1);  // fillps, then p = p + p_jump (main.f90:139-142)
   } else {
     launch_fillps(c, 0);
@@ -1355,6 +1377,27 @@ int icls_profile_entry(icls_ctx* h, int idx, char* name, int name_len, double* t
 int icls_launch_count(icls_ctx* h, long long* n) {
   if (!h || !n) return ICLS_E_ARG;
   *n = h->c.prof.launches;
+  return ICLS_OK;
+}
+
+int icls_set_curvature_net(icls_ctx* h, icls_mlp* net) {
+  if (!h) return ICLS_E_ARG;
+  if (h->c.cfg.curvature_model != ICLS_CURV_MLP) return ICLS_E_CONFIG;
+  h->c.net = net;
+  return ICLS_OK;
+}
+
+int icls_curvature_stats(icls_ctx* h, long long* evaluated, long long* fallbacks, int reset) {
+  if (!h) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  unsigned long long st[2] = {0, 0};
+  if (c.mlp_stats) {
+    CK(cudaMemcpyAsync(st, c.mlp_stats, sizeof(st), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    if (reset) CK(cudaMemsetAsync(c.mlp_stats, 0, sizeof(st), c.s));
+  }
+  if (evaluated) *evaluated = (long long)st[0];
+  if (fallbacks) *fallbacks = (long long)st[1];
   return ICLS_OK;
 }
 

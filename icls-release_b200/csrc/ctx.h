@@ -4,6 +4,7 @@
 // src/main.f90 (duold..dwold, pold, p, p_jump) and the solver tables of
 // src/solver.f90:42-47.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -143,6 +144,15 @@ struct Ctx {
   // {x, x shifted by imax/2, y, y shifted by jmax/2, z} over the band
   int* d_bbox = nullptr;
   int* h_bbox = nullptr;                // pinned copy
+  // learned curvature (curvature_model = ICLS_CURV_MLP): the attached
+  // network and the buffers of the gathered interface cells
+  icls_mlp* net = nullptr;
+  float* mlp_X = nullptr;
+  void* mlp_rec = nullptr;
+  float* mlp_y = nullptr;
+  int* mlp_count = nullptr;
+  unsigned long long* mlp_stats = nullptr;  // cells evaluated, fallbacks to the stencil
+  int mlp_cap = 0;
   bool curv_stale = false;              // curv / normal%m hold more than the last drop
   bool nrm_stale = false;
   cudaEvent_t ev_bbox = nullptr;
@@ -184,6 +194,11 @@ void launch_curvature(Ctx& c, const LsBatch& b, double* nrm_m_out);
 void launch_recurvature(Ctx& c, const LsBatch& b);
 void launch_jumps(Ctx& c, const LsBatch& b);
 void launch_ipot(Ctx& c, double* dmin_dev);
+
+// learned curvature (k_mlp.cu)
+int launch_mlp_curvature(Ctx& c, const LsBatch& b);
+int mlp_buffers(Ctx& c, int cap);
+int mlp_constants();
 
 // Navier-Stokes (k_navier.cu)
 void launch_ab2(Ctx& c);

@@ -11,7 +11,7 @@
 #include <vector>
 
 #include "../../include/icls_gpu.h"
-#include "ctx.h"
+#include "batch.cuh"
 #include "umma.cuh"
 
 namespace icls {
@@ -68,17 +68,25 @@ __global__ void __launch_bounds__(128) k_tc_gemm_check(const __nv_bfloat16* __re
 
 // ============================================================== the network
 // 27 -> 128 -> 128 -> 64 -> 1, SiLU after the first three layers.  Inputs
-// are the 27 values (phi(x + o dx) - phi(x)) / dx of a 3x3x3 stencil (padded
-// to 32 with zeros), the output is kappa * dx.  FP32 master parameters in one
+// are the features of the 27 values (phi(x + o dx) - phi(x)) / dx of a
+// 3x3x3 stencil (mlp_features: its second-order part and unit gradient,
+// 30 values padded to 32), the output is the correction to the plain stencil's
+// kappa * dx: the learned curvature is kappa_stencil + output / dx, so a
+// well-resolved interface, where the stencil is already accurate, needs
+// only a small output.  FP32 master parameters in one
 // array (layout below), BF16 copies of W1..W3 as the tiles' B operands and
 // BF16 transposes of W2, W3 for back-propagation to the inputs.
 constexpr int kIn = 32, kH1 = 128, kH2 = 128, kH3 = 64;
+// layer 1 takes each FP32 input as a BF16 pair hi + lo (K = 2 x 32) against
+// W1 twice: the inputs' small second differences, which carry the
+// curvature, keep about 16 mantissa bits
+constexpr int kIn2 = 2 * kIn;
 constexpr int oW1 = 0, oB1 = oW1 + kH1 * kIn, oW2 = oB1 + kH1, oB2 = oW2 + kH2 * kH1, oW3 = oB2 + kH2,
               oB3 = oW3 + kH3 * kH2, oW4 = oB3 + kH3, oB4 = oW4 + kH3, kParams = oB4 + 1;
 
 struct Net {
   const float* theta;              // FP32 parameters
-  const __nv_bfloat16* w1;         // [128][32]
+  const __nv_bfloat16* w1;         // [128][64] = [W1 | W1]
   const __nv_bfloat16* w2;         // [128][128]
   const __nv_bfloat16* w3;         // [64][128]
   const __nv_bfloat16* w2t;        // [128][128] = W2^T
@@ -97,13 +105,13 @@ __device__ __forceinline__ void put_bf16(unsigned char* base, uint32_t off, floa
 // shared-memory plan of one tile (bytes)
 constexpr int SB_B = 0;                       // weight operand, up to 128 x 128
 constexpr int SB_ACT = SB_B + 32768;          // activations / deltas, A layout [128 x 128]
-constexpr int SB_XA = SB_ACT + 32768;         // inputs, A layout [128 x 32]
-constexpr int SB_XT = SB_XA + 8192;           // inputs transposed [32 x 128]
-constexpr int SB_H1T = SB_XT + 8192;          // H1^T [128 x 128]
+constexpr int SB_XA = SB_ACT + 32768;         // inputs hi|lo, A layout [128 x 64]
+constexpr int SB_XT = SB_XA + 16384;          // inputs transposed [64 x 128]
+constexpr int SB_H1T = SB_XT + 16384;         // H1^T [128 x 128]
 constexpr int SB_H2T = SB_H1T + 32768;        // H2^T [128 x 128]
 constexpr int SB_DZT = SB_H2T + 32768;        // delta^T [128 x 128]
-constexpr int SB_TRAIN = SB_DZT + 32768;      // 180224
-constexpr int SB_INFER = SB_XT;               // forward only: B, ACT, XA (73728)
+constexpr int SB_TRAIN = SB_DZT + 32768;      // 196608
+constexpr int SB_INFER = SB_XT;               // forward only: B, ACT, XA (81920)
 
 // a weight matrix [n][k] (row-major BF16, global) into the B operand layout
 __device__ __forceinline__ void stage_b(unsigned char* sb, const __nv_bfloat16* __restrict__ w, int n, int k) {
@@ -113,24 +121,30 @@ __device__ __forceinline__ void stage_b(unsigned char* sb, const __nv_bfloat16* 
   }
 }
 
-// The forward pass of one 128-sample tile; x (BF16, [rows][32]) holds the
+// The forward pass of one 128-sample tile; x (FP32, [rows][32]) holds the
 // tile's inputs, sample t of the tile is row t.  Returns y (kappa*dx) of this
 // thread's sample.  Training keeps the pre-activations z1..z3 (zg, per sample
 // 320 floats) and the transposed activations in shared memory.
 template <bool TRAIN>
-__device__ float forward_tile(const Net& net, const __nv_bfloat16* __restrict__ xrow, unsigned char* sm, uint32_t tmem,
+__device__ float forward_tile(const Net& net, const float* __restrict__ xrow, unsigned char* sm, uint32_t tmem,
                               uint64_t* bar, uint32_t& phase, float* __restrict__ zrow, bool& ok) {
   const int t = threadIdx.x, warp = t >> 5;
   const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
   // inputs
   for (int j = 0; j < kIn; ++j) {
-    const float v = xrow ? __bfloat162float(xrow[j]) : 0.f;
-    put_bf16(sm + SB_XA, kmajor_off(t, j, kRows), v);
-    if (TRAIN) put_bf16(sm + SB_XT, kmajor_off(j, t, kIn), v);
+    const float v = xrow ? xrow[j] : 0.f;
+    const float hi = __bfloat162float(__float2bfloat16(v));
+    const float lo = v - hi;
+    put_bf16(sm + SB_XA, kmajor_off(t, j, kRows), hi);
+    put_bf16(sm + SB_XA, kmajor_off(t, j + kIn, kRows), lo);
+    if (TRAIN) {
+      put_bf16(sm + SB_XT, kmajor_off(j, t, kIn2), hi);
+      put_bf16(sm + SB_XT, kmajor_off(j + kIn, t, kIn2), lo);
+    }
   }
   // layer 1
-  stage_b(sm + SB_B, net.w1, kH1, kIn);
-  ok &= umma::tile_gemm(sm + SB_XA, sm + SB_B, kH1, kIn, tmem, bar, phase);
+  stage_b(sm + SB_B, net.w1, kH1, kIn2);
+  ok &= umma::tile_gemm(sm + SB_XA, sm + SB_B, kH1, kIn2, tmem, bar, phase);
   for (int c = 0; c < kH1; c += 8) {
     float v[8];
     umma::tmem_ld8(lane_addr + c, v);
@@ -186,12 +200,13 @@ __device__ __forceinline__ void warp_add(float* dst, float v) {
   if ((threadIdx.x & 31) == 0) atomicAdd(dst, v);
 }
 
-// One training tile: forward, MSE loss gradient (scale = 2/batch) and the
-// backward pass; parameter gradients are added into grad (FP32), the loss
+// One training tile: forward, weighted squared-error gradient (dy = scale x
+// weight x error, scale = 2/batch; no weights: 1) and the backward pass; parameter gradients are added into grad (FP32), the loss
 // sum into *loss.  Samples idx = (a * (base + t) + b) mod n (a per-epoch
 // affine shuffle of the n samples, n a power of two, a odd).
-__global__ void __launch_bounds__(128) k_mlp_train_tile(Net net, const __nv_bfloat16* __restrict__ X,
-                                                        const float* __restrict__ label, long long n, long long base,
+__global__ void __launch_bounds__(128) k_mlp_train_tile(Net net, const float* __restrict__ X,
+                                                        const float* __restrict__ label,
+                                                        const float* __restrict__ weight, long long n, long long base,
                                                         unsigned long long pa, unsigned long long pb, float scale,
                                                         float* __restrict__ zbuf, float* __restrict__ grad,
                                                         float* __restrict__ loss, int* __restrict__ err) {
@@ -213,8 +228,9 @@ __global__ void __launch_bounds__(128) k_mlp_train_tile(Net net, const __nv_bflo
   float* zrow = zbuf + ((long long)blockIdx.x * kRows + t) * (kH1 + kH2 + kH3);
   const float y = forward_tile<true>(net, X + s * kIn, sm, tmem, &bar, phase, zrow, ok);
   const float e = y - label[s];
-  warp_add(loss, e * e);
-  const float dy = scale * e;
+  const float wt = weight ? weight[s] : 1.f;
+  warp_add(loss, wt * e * e);
+  const float dy = scale * wt * e;
   // head: dW4 = sum dy h3, db4 = sum dy; delta3 = dy W4 silu'(z3)
   warp_add(grad + oB4, dy);
   for (int j = 0; j < kH3; ++j) {
@@ -275,13 +291,14 @@ __global__ void __launch_bounds__(128) k_mlp_train_tile(Net net, const __nv_bflo
       put_bf16(sm + SB_DZT, kmajor_off(c + q, t, kRows), d1);
     }
   }
-  // dW1 = delta1^T X
-  ok &= umma::tile_gemm(sm + SB_DZT, sm + SB_XT, kIn, kRows, tmem, &bar, phase);
+  // dW1 = delta1^T X (the hi and lo halves both act through W1)
+  ok &= umma::tile_gemm(sm + SB_DZT, sm + SB_XT, kIn2, kRows, tmem, &bar, phase);
   for (int c = 0; c < kIn; c += 8) {
-    float v[8];
+    float v[8], w[8];
     umma::tmem_ld8(lane_addr + c, v);
+    umma::tmem_ld8(lane_addr + kIn + c, w);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) atomicAdd(grad + oW1 + t * kIn + c + q, v[q]);
+    for (int q = 0; q < 8; ++q) atomicAdd(grad + oW1 + t * kIn + c + q, v[q] + w[q]);
   }
   if (!ok && t == 0) atomicExch(err, 1);
   umma::fence_before();
@@ -290,7 +307,7 @@ __global__ void __launch_bounds__(128) k_mlp_train_tile(Net net, const __nv_bflo
 }
 
 // inference over n samples, one 128-sample tile per iteration
-__global__ void __launch_bounds__(128) k_mlp_infer(Net net, const __nv_bfloat16* __restrict__ X, long long n,
+__global__ void __launch_bounds__(128) k_mlp_infer(Net net, const float* __restrict__ X, long long n,
                                                    float* __restrict__ y, int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char sm[];
   __shared__ __align__(8) uint64_t bar;
@@ -317,6 +334,26 @@ __global__ void __launch_bounds__(128) k_mlp_infer(Net net, const __nv_bfloat16*
   if (warp == 0) umma::tmem_free(tmem, 128);
 }
 
+// parameter q's BF16 value into the tile copies
+__device__ __forceinline__ void put_copies(int q, __nv_bfloat16 h, __nv_bfloat16* w1, __nv_bfloat16* w2,
+                                           __nv_bfloat16* w3, __nv_bfloat16* w2t, __nv_bfloat16* w3t) {
+  if (q >= oW1 && q < oB1) {
+    const int r = (q - oW1) / kIn, c = (q - oW1) % kIn;
+    w1[r * kIn2 + c] = h;
+    w1[r * kIn2 + kIn + c] = h;
+  }
+  if (q >= oW2 && q < oB2) {
+    const int r = (q - oW2) / kH1, c = (q - oW2) % kH1;
+    w2[q - oW2] = h;
+    w2t[c * kH2 + r] = h;
+  }
+  if (q >= oW3 && q < oB3) {
+    const int r = (q - oW3) / kH2, c = (q - oW3) % kH2;
+    w3[q - oW3] = h;
+    w3t[c * kH3 + r] = h;
+  }
+}
+
 // Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the FP32 parameters, then the
 // BF16 copies and transposes; the gradient is cleared for the next batch
 __global__ void k_mlp_adam(float* __restrict__ theta, float* __restrict__ grad, float* __restrict__ m1,
@@ -334,17 +371,7 @@ __global__ void k_mlp_adam(float* __restrict__ theta, float* __restrict__ grad, 
   const float w = theta[q] - lr * (a / bc1) / (sqrtf(b / bc2) + 1e-8f);
   theta[q] = w;
   const __nv_bfloat16 h = __float2bfloat16(w);
-  if (q >= oW1 && q < oB1) w1[q - oW1] = h;
-  if (q >= oW2 && q < oB2) {
-    const int r = (q - oW2) / kH1, c = (q - oW2) % kH1;
-    w2[q - oW2] = h;
-    w2t[c * kH2 + r] = h;
-  }
-  if (q >= oW3 && q < oB3) {
-    const int r = (q - oW3) / kH2, c = (q - oW3) % kH2;
-    w3[q - oW3] = h;
-    w3t[c * kH3 + r] = h;
-  }
+  put_copies(q, h, w1, w2, w3, w2t, w3t);
 }
 
 // refresh the BF16 copies from theta (after initialisation or a set)
@@ -353,18 +380,7 @@ __global__ void k_mlp_copies(const float* __restrict__ theta, __nv_bfloat16* __r
                              __nv_bfloat16* __restrict__ w2t, __nv_bfloat16* __restrict__ w3t) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= kParams) return;
-  const __nv_bfloat16 h = __float2bfloat16(theta[q]);
-  if (q >= oW1 && q < oB1) w1[q - oW1] = h;
-  if (q >= oW2 && q < oB2) {
-    const int r = (q - oW2) / kH1, c = (q - oW2) % kH1;
-    w2[q - oW2] = h;
-    w2t[c * kH2 + r] = h;
-  }
-  if (q >= oW3 && q < oB3) {
-    const int r = (q - oW3) / kH2, c = (q - oW3) % kH2;
-    w3[q - oW3] = h;
-    w3t[c * kH3 + r] = h;
-  }
+  put_copies(q, __float2bfloat16(theta[q]), w1, w2, w3, w2t, w3t);
 }
 
 // ===================================================== training samples
@@ -378,6 +394,30 @@ __device__ __forceinline__ double urand(unsigned long long seed, unsigned long l
 }
 
 __constant__ double cPu[270];  // the least-squares pseudo-inverse for unit spacing
+
+// The network's inputs from a stencil f (phi(x + o) - phi(x), in cells,
+// o in {-1,0,1}^3 with z outer): the stencil minus its least-squares linear
+// part g.o (27 values, the second-order part that carries the curvature),
+// then the unit gradient g/|g| (3 values) and 2 zeros.  Removing the linear
+// part before the BF16 tiles keeps their rounding far below the curvature
+// signal.
+template <typename R>
+__device__ __forceinline__ void mlp_features(const R* f, float* out) {
+  R g[3] = {0, 0, 0};
+  for (int q = 0; q < 27; ++q)
+    for (int r = 1; r <= 3; ++r) g[r - 1] += (R)cPu[r * 27 + q] * f[q];
+  int q = 0;
+  for (int dk = -1; dk <= 1; ++dk)
+    for (int dj = -1; dj <= 1; ++dj)
+      for (int di = -1; di <= 1; ++di, ++q) out[q] = (float)(f[q] - (g[0] * di + g[1] * dj + g[2] * dk));
+  const R n = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+  const R rn = n > (R)0 ? (R)1 / n : (R)0;
+  out[27] = (float)(g[0] * rn);
+  out[28] = (float)(g[1] * rn);
+  out[29] = (float)(g[2] * rn);
+  out[30] = 0.f;
+  out[31] = 0.f;
+}
 
 struct Shape {
   double c[3];   // centre
@@ -489,10 +529,11 @@ __device__ void ellipsoid_principal(const Shape& S, const double* q, double& k1,
 // |phi(x)| <= 3 near its surface, phi the exact signed distance.  Writes the
 // 27 inputs (phi(x+o) - phi(x), o in {-1,0,1}^3), the label (the
 // least-squares curvature of the stencil of spacing 1/4 at x, the method on a
-// grid refined 4x) and, in extra, the plain curvature at spacing 1, the
-// analytic curvature and the shape's smallest radius.
-__global__ void k_mlp_gen(unsigned long long seed, long long n, __nv_bfloat16* __restrict__ X,
-                          float* __restrict__ label, float* __restrict__ extra) {
+// grid refined 4x, minus the plain curvature at spacing 1) and, in extra,
+// the plain curvature at spacing 1, the analytic curvature and the shape's
+// smallest radius.
+__global__ void k_mlp_gen(unsigned long long seed, long long n, float* __restrict__ X,
+                          float* __restrict__ label, float* __restrict__ weight, float* __restrict__ extra) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double pi2 = 6.283185307179586;
@@ -576,14 +617,140 @@ __global__ void k_mlp_gen(unsigned long long seed, long long n, __nv_bfloat16* _
         const double pc[3] = {x[0] + di, x[1] + dj, x[2] + dk};
         fc[q++] = sdist(S, pc, nullptr);
       }
-  for (int k = 0; k < 27; ++k) X[i * kIn + k] = __float2bfloat16((float)(fc[k] - fc[13]));
-  for (int k = 27; k < kIn; ++k) X[i * kIn + k] = __float2bfloat16(0.f);
-  label[i] = (float)lab;
-  extra[3 * i + 0] = (float)lsq_curv(fc, 1.);
+  double fd[27];
+  for (int k = 0; k < 27; ++k) fd[k] = fc[k] - fc[13];
+  mlp_features(fd, X + i * kIn);
+  const double plain = lsq_curv(fc, 1.);
+  label[i] = (float)(lab - plain);  // the correction the network learns
+  // the loss weight: errors relative to the curvature, so well-resolved
+  // interfaces (small kappa dx, where the stencil is already accurate)
+  // count as much as the under-resolved ones
+  const double wr = 0.1 / (fabs(lab) + 0.02);
+  weight[i] = (float)(wr * wr);
+  extra[3 * i + 0] = (float)plain;
   extra[3 * i + 1] = (float)kana;
   extra[3 * i + 2] = (float)fmin(S.s[0], fmin(S.s[1], S.s[2]));
 }
 
+
+// ================================================ the network in the loop
+// A gathered interface cell: task q of the batch, interior cell (i, j, k)
+struct MlpCell {
+  int q, i, j, k;
+};
+
+// Stencils of the tasks' interface cells (computed interior cells of the
+// shape-C regions with |phi| <= 4dz, the cells whose curvature
+// re_curvature and the jumps read) into X, slots by a warp-aggregated
+// counter; cells beyond cap keep the plain curvature.
+template <typename T>
+__global__ void __launch_bounds__(256) k_mlp_gather(Params p, const __grid_constant__ LsBatch B,
+                                                    float* __restrict__ X, MlpCell* __restrict__ rec,
+                                                    int* __restrict__ count, int cap) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  const T* __restrict__ phi = cT<T>(t.phi0);
+  const float rdz = (float)(1. / p.dz);
+  const T lim = (T)(4. * p.dz);
+  const long long sy = p.nLx, sz = (long long)p.nLx * p.nLy;
+  const unsigned lane = threadIdx.x & 31u;
+  const int k0 = max(c.ka, max(t.r.cz0, 1)), k1 = min(c.kb, min(t.r.cz1, p.kmax));
+  // every lane of the warp walks the same rows so the ballots line up
+  for (int k = c.ka; k <= c.kb; ++k) {
+    bool take = false;
+    long long cl = 0;
+    if (c.ok && c.cxy && k >= k0 && k <= k1) {
+      cl = idxL(p, c.i, c.j, k);
+      take = fabs(phi[cl]) <= lim;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (!m) continue;
+    int base = 0;
+    if (lane == (unsigned)(__ffs(m) - 1)) base = atomicAdd(count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+    if (!take) continue;
+    const int slot = base + __popc(m & ((1u << lane) - 1u));
+    if (slot >= cap) continue;
+    const float pc = (float)phi[cl];
+    float f[27];
+    int n = 0;
+    for (int dk = -1; dk <= 1; ++dk)
+      for (int dj = -1; dj <= 1; ++dj)
+        for (int di = -1; di <= 1; ++di) f[n++] = ((float)phi[cl + di + dj * sy + dk * sz] - pc) * rdz;
+    mlp_features(f, X + (long long)slot * kIn);
+    rec[slot] = MlpCell{ti, c.i, c.j, k};
+  }
+}
+
+// inference over the first min(*count, cap) rows of X
+__global__ void __launch_bounds__(128) k_mlp_infer_count(Net net, const float* __restrict__ X,
+                                                         const int* __restrict__ count, int cap, float* __restrict__ y,
+                                                         int* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  const int t = threadIdx.x, warp = t >> 5;
+  const long long n = min(*count, cap);
+  const long long tiles = (n + kRows - 1) / kRows;
+  if ((long long)blockIdx.x >= tiles) return;  // block-uniform: no tensor memory taken
+  if (t == 0) umma::mbar_init(&bar, 1);
+  if (warp == 0) umma::tmem_alloc(&tmem_slot, 128);
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tmem = tmem_slot;
+  uint32_t phase = 0;
+  bool ok = true;
+  for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const long long s = tile * kRows + t;
+    const float v = forward_tile<false>(net, s < n ? X + s * kIn : nullptr, sm, tmem, &bar, phase, nullptr, ok);
+    if (s < n) y[s] = v;
+    if (!__syncthreads_and(ok)) break;
+  }
+  if (!ok && t == 0) atomicExch(err, 1);
+  umma::fence_before();
+  __syncthreads();
+  if (warp == 0) umma::tmem_free(tmem, 128);
+}
+
+// the learned curvature kappa_plain + y/dx where it passes the checks, the
+// plain one otherwise (a correction |y| > tol, or a curvature radius below 3
+// cells, |kappa_plain| dx > 2/3); stats[0] += evaluated, stats[1] +=
+// fallbacks
+template <typename T>
+__global__ void __launch_bounds__(256) k_mlp_apply(Params p, const __grid_constant__ LsBatch B,
+                                                   const MlpCell* __restrict__ rec, const float* __restrict__ y,
+                                                   const int* __restrict__ count, int cap, double tol,
+                                                   unsigned long long* __restrict__ stats) {
+  const long long n = min(*count, cap);
+  const double dz = p.dz;
+  unsigned long long ev = 0, fb = 0;
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+    const MlpCell r = rec[s];
+    T* out = mT<T>(B.t[r.q].out);
+    const double kp = (double)out[idxC(p, r.i, r.j, r.k)];
+    double km = kp + (double)y[s] / dz;
+    ++ev;
+    if (fabs(kp) * dz > 2. / 3. || fabs(km - kp) * dz > tol) {
+      ++fb;
+      continue;
+    }
+    const double maxk = 1. / dz;  // the clamps of interface.f90:104-111
+    if (km < -maxk) km = -maxk;
+    else if (km > maxk) km = maxk;
+    else if (fabs(km) < 1e-9) km = 0.;
+    putC(p, out, r.i, r.j, r.k, (T)km);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ev += __shfl_down_sync(0xffffffffu, ev, o);
+    fb += __shfl_down_sync(0xffffffffu, fb, o);
+  }
+  if ((threadIdx.x & 31) == 0 && ev) {
+    atomicAdd(stats, ev);
+    atomicAdd(stats + 1, fb);
+  }
+}
 }  // namespace
 }  // namespace icls
 
@@ -595,11 +762,11 @@ struct icls_mlp {
   float* loss = nullptr;     // per-epoch loss sums
   int nloss = 0;
   int* err = nullptr;
-  __nv_bfloat16* X = nullptr;  // training inputs [n][32]
-  float *label = nullptr, *extra = nullptr;
+  float* X = nullptr;          // training inputs [n][32]
+  float *label = nullptr, *weight = nullptr, *extra = nullptr;
   long long n_train = 0;
-  __nv_bfloat16* Xh = nullptr;  // held-out set
-  float *labelh = nullptr, *extrah = nullptr, *yh = nullptr;
+  float* Xh = nullptr;         // held-out set
+  float *labelh = nullptr, *weighth = nullptr, *extrah = nullptr, *yh = nullptr;
   long long n_hold = 0;
   long long step = 0;
   cudaStream_t s = nullptr;
@@ -640,6 +807,62 @@ void refresh_copies(icls_mlp* m) {
 
 }  // namespace
 
+namespace icls {
+// get_curvature's output (the batch tasks' out buffers, computed by
+// launch_curvature) replaced by the network near the interface
+int launch_mlp_curvature(Ctx& c, const LsBatch& b) {
+  if (b.n == 0) return ICLS_OK;
+  if (!c.net) return ICLS_E_STATE;
+  Scope sc_(c.prof, c.s, "mlp_curvature", 3);
+  cudaMemsetAsync(c.mlp_count, 0, sizeof(int), c.s);
+  if (c.P.f32)
+    k_mlp_gather<float><<<b.start[b.n], dim3(TBX, TBY, 1), 0, c.s>>>(c.P, b, c.mlp_X, (MlpCell*)c.mlp_rec,
+                                                                      c.mlp_count, c.mlp_cap);
+  else
+    k_mlp_gather<double><<<b.start[b.n], dim3(TBX, TBY, 1), 0, c.s>>>(c.P, b, c.mlp_X, (MlpCell*)c.mlp_rec,
+                                                                       c.mlp_count, c.mlp_cap);
+  const int tiles = (c.mlp_cap + 127) / 128;
+  k_mlp_infer_count<<<std::min(tiles, 2 * 148), 128, SB_INFER, c.s>>>(net_of(c.net), c.mlp_X, c.mlp_count, c.mlp_cap,
+                                                                      c.mlp_y, c.net->err);
+  const double tol = c.cfg.mlp_fallback_tol;
+  if (c.P.f32)
+    k_mlp_apply<float><<<592, 256, 0, c.s>>>(c.P, b, (const MlpCell*)c.mlp_rec, c.mlp_y, c.mlp_count, c.mlp_cap, tol,
+                                             c.mlp_stats);
+  else
+    k_mlp_apply<double><<<592, 256, 0, c.s>>>(c.P, b, (const MlpCell*)c.mlp_rec, c.mlp_y, c.mlp_count, c.mlp_cap,
+                                              tol, c.mlp_stats);
+  return ICLS_OK;
+}
+
+// the unit-spacing pseudo-inverse the features and the labels use (once per
+// process and device-wide)
+int mlp_constants() {
+  static bool set = false;
+  if (set) return 0;
+  double pu[270];
+  pseudo_inverse(1., 1., 1., pu);
+  if (cudaMemcpyToSymbol(cPu, pu, sizeof(pu)) != cudaSuccess) return 1;
+  set = true;
+  return 0;
+}
+
+// device buffers of the context's gathered cells (16-byte cell records)
+int mlp_buffers(Ctx& c, int cap) {
+  if (mlp_constants()) return ICLS_E_CUDA;
+  if (cudaMalloc(&c.mlp_X, (size_t)cap * kIn * 4) != cudaSuccess) return ICLS_E_NOMEM;
+  if (cudaMalloc(&c.mlp_rec, (size_t)cap * sizeof(MlpCell)) != cudaSuccess) return ICLS_E_NOMEM;
+  if (cudaMalloc(&c.mlp_y, (size_t)cap * sizeof(float)) != cudaSuccess) return ICLS_E_NOMEM;
+  if (cudaMalloc(&c.mlp_count, sizeof(int)) != cudaSuccess) return ICLS_E_NOMEM;
+  if (cudaMalloc(&c.mlp_stats, 2 * sizeof(unsigned long long)) != cudaSuccess) return ICLS_E_NOMEM;
+  cudaMemset(c.mlp_stats, 0, 2 * sizeof(unsigned long long));
+  c.mlp_cap = cap;
+  return cudaFuncSetAttribute(k_mlp_infer_count, cudaFuncAttributeMaxDynamicSharedMemorySize, SB_INFER) ==
+                 cudaSuccess
+             ? ICLS_OK
+             : ICLS_E_CUDA;
+}
+}  // namespace icls
+
 extern "C" int icls_mlp_create(icls_mlp** out, unsigned long long seed) {
   if (!out) return ICLS_E_ARG;
   *out = nullptr;
@@ -647,7 +870,7 @@ extern "C" int icls_mlp_create(icls_mlp** out, unsigned long long seed) {
   if (!m) return ICLS_E_NOMEM;
   bool ok = cudaStreamCreateWithFlags(&m->s, cudaStreamNonBlocking) == cudaSuccess;
   for (float** f : {&m->theta, &m->grad, &m->m1, &m->m2}) ok = ok && cudaMalloc(f, sizeof(float) * kParams) == cudaSuccess;
-  ok = ok && cudaMalloc(&m->w1, 2 * kH1 * kIn) == cudaSuccess && cudaMalloc(&m->w2, 2 * kH2 * kH1) == cudaSuccess &&
+  ok = ok && cudaMalloc(&m->w1, 2 * kH1 * kIn2) == cudaSuccess && cudaMalloc(&m->w2, 2 * kH2 * kH1) == cudaSuccess &&
        cudaMalloc(&m->w3, 2 * kH3 * kH2) == cudaSuccess && cudaMalloc(&m->w2t, 2 * kH2 * kH1) == cudaSuccess &&
        cudaMalloc(&m->w3t, 2 * kH3 * kH2) == cudaSuccess && cudaMalloc(&m->err, sizeof(int)) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute(icls::k_mlp_train_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, icls::SB_TRAIN) ==
@@ -688,8 +911,8 @@ extern "C" int icls_mlp_destroy(icls_mlp* m) {
   if (m->s) cudaStreamSynchronize(m->s);
   for (void* p : {(void*)m->theta, (void*)m->grad, (void*)m->m1, (void*)m->m2, (void*)m->w1, (void*)m->w2,
                   (void*)m->w3, (void*)m->w2t, (void*)m->w3t, (void*)m->zbuf, (void*)m->loss, (void*)m->err,
-                  (void*)m->X, (void*)m->label, (void*)m->extra, (void*)m->Xh, (void*)m->labelh, (void*)m->extrah,
-                  (void*)m->yh})
+                  (void*)m->X, (void*)m->label, (void*)m->weight, (void*)m->extra, (void*)m->Xh, (void*)m->labelh,
+                  (void*)m->weighth, (void*)m->extrah, (void*)m->yh})
     if (p) cudaFree(p);
   if (m->s) cudaStreamDestroy(m->s);
   delete m;
@@ -699,39 +922,37 @@ extern "C" int icls_mlp_destroy(icls_mlp* m) {
 // n_train a power of two (the epoch shuffle is an affine map mod n_train)
 extern "C" int icls_mlp_make_data(icls_mlp* m, unsigned long long seed, long long n_train, long long n_hold) {
   if (!m || n_train < 128 || (n_train & (n_train - 1)) || n_hold < 1) return ICLS_E_ARG;
-  static bool pinv_set = false;
-  if (!pinv_set) {
-    double pu[270];
-    icls::pseudo_inverse(1., 1., 1., pu);
-    if (cudaMemcpyToSymbol(icls::cPu, pu, sizeof(pu)) != cudaSuccess) return ICLS_E_CUDA;
-    pinv_set = true;
-  }
-  for (void* p : {(void*)m->X, (void*)m->label, (void*)m->extra, (void*)m->Xh, (void*)m->labelh, (void*)m->extrah,
-                  (void*)m->yh})
+  if (icls::mlp_constants()) return ICLS_E_CUDA;
+  for (void* p : {(void*)m->X, (void*)m->label, (void*)m->weight, (void*)m->extra, (void*)m->Xh, (void*)m->labelh,
+                  (void*)m->weighth, (void*)m->extrah, (void*)m->yh})
     if (p) cudaFree(p);
   m->X = m->Xh = nullptr;
-  m->label = m->extra = m->labelh = m->extrah = m->yh = nullptr;
-  bool ok = cudaMalloc(&m->X, 2 * (size_t)n_train * kIn) == cudaSuccess &&
+  m->label = m->weight = m->extra = m->labelh = m->weighth = m->extrah = m->yh = nullptr;
+  bool ok = cudaMalloc(&m->X, 4 * (size_t)n_train * kIn) == cudaSuccess &&
             cudaMalloc(&m->label, 4 * (size_t)n_train) == cudaSuccess &&
+            cudaMalloc(&m->weight, 4 * (size_t)n_train) == cudaSuccess &&
+            cudaMalloc(&m->weighth, 4 * (size_t)n_hold) == cudaSuccess &&
             cudaMalloc(&m->extra, 12 * (size_t)n_train) == cudaSuccess &&
-            cudaMalloc(&m->Xh, 2 * (size_t)n_hold * kIn) == cudaSuccess &&
+            cudaMalloc(&m->Xh, 4 * (size_t)n_hold * kIn) == cudaSuccess &&
             cudaMalloc(&m->labelh, 4 * (size_t)n_hold) == cudaSuccess &&
             cudaMalloc(&m->extrah, 12 * (size_t)n_hold) == cudaSuccess &&
             cudaMalloc(&m->yh, 4 * (size_t)n_hold) == cudaSuccess;
   if (!ok) return ICLS_E_NOMEM;
   m->n_train = n_train;
   m->n_hold = n_hold;
-  icls::k_mlp_gen<<<(unsigned)((n_train + 127) / 128), 128, 0, m->s>>>(seed, n_train, m->X, m->label, m->extra);
+  icls::k_mlp_gen<<<(unsigned)((n_train + 127) / 128), 128, 0, m->s>>>(seed, n_train, m->X, m->label, m->weight,
+                                                                       m->extra);
   icls::k_mlp_gen<<<(unsigned)((n_hold + 127) / 128), 128, 0, m->s>>>(mix64(seed ^ 0x5bd1e995ull), n_hold, m->Xh,
-                                                                      m->labelh, m->extrah);
+                                                                      m->labelh, m->weighth, m->extrah);
   return sync_err(m);
 }
 
 // epochs over the training set in batches of `batch` (a multiple of 128
-// dividing n_train), Adam with step size lr; loss_out[e] = mean squared
-// error of epoch e (kappa*dx units), if given
-extern "C" int icls_mlp_train(icls_mlp* m, int epochs, int batch, double lr, unsigned long long seed,
-                              double* loss_out) {
+// dividing n_train), Adam with a step size decaying from lr to lr_final
+// along a half cosine; loss_out[e] = mean squared error of epoch e
+// (kappa*dx units), if given
+extern "C" int icls_mlp_train(icls_mlp* m, int epochs, int batch, double lr, double lr_final,
+                              unsigned long long seed, double* loss_out) {
   if (!m || !m->X || epochs < 1 || batch < 128 || batch % 128 || m->n_train % batch) return ICLS_E_ARG;
   int rc = ensure_zbuf(m, batch);
   if (rc) return rc;
@@ -743,18 +964,22 @@ extern "C" int icls_mlp_train(icls_mlp* m, int epochs, int batch, double lr, uns
   cudaMemsetAsync(m->loss, 0, sizeof(float) * epochs, m->s);
   const Net net = net_of(m);
   const long long steps = m->n_train / batch;
+  const long long total = steps * epochs;
+  long long done = 0;
   const float scale = 2.f / (float)batch;
   for (int e = 0; e < epochs; ++e) {
     const unsigned long long pa = mix64(seed + 2 * (unsigned long long)e) | 1ull;
     const unsigned long long pb = mix64(seed + 2 * (unsigned long long)e + 1);
     for (long long st = 0; st < steps; ++st) {
-      icls::k_mlp_train_tile<<<batch / 128, 128, icls::SB_TRAIN, m->s>>>(net, m->X, m->label, m->n_train,
+      icls::k_mlp_train_tile<<<batch / 128, 128, icls::SB_TRAIN, m->s>>>(net, m->X, m->label, m->weight, m->n_train,
                                                                           st * batch, pa, pb, scale, m->zbuf,
                                                                           m->grad, m->loss + e, m->err);
       ++m->step;
+      const double lr_t = lr_final + 0.5 * (lr - lr_final) * (1. + std::cos(3.141592653589793 * (double)done / (double)total));
+      ++done;
       const float bc1 = 1.f - powf(0.9f, (float)m->step), bc2 = 1.f - powf(0.999f, (float)m->step);
-      icls::k_mlp_adam<<<(kParams + 255) / 256, 256, 0, m->s>>>(m->theta, m->grad, m->m1, m->m2, (float)lr, bc1, bc2,
-                                                                 m->w1, m->w2, m->w3, m->w2t, m->w3t);
+      icls::k_mlp_adam<<<(kParams + 255) / 256, 256, 0, m->s>>>(m->theta, m->grad, m->m1, m->m2, (float)lr_t, bc1,
+                                                                 bc2, m->w1, m->w2, m->w3, m->w2t, m->w3t);
     }
   }
   rc = sync_err(m);
@@ -767,13 +992,13 @@ extern "C" int icls_mlp_train(icls_mlp* m, int epochs, int batch, double lr, uns
   return ICLS_OK;
 }
 
-// y[0..n) = network(X[0..n)) on device arrays (X BF16 [n][32])
+// y[0..n) = network(X[0..n)) on device arrays (X FP32 [n][32])
 extern "C" int icls_mlp_infer(icls_mlp* m, const void* X, float* y, long long n, void* stream) {
   if (!m || !X || !y || n < 1) return ICLS_E_ARG;
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : m->s;
   const long long tiles = (n + 127) / 128;
   const int grid = (int)std::min<long long>(tiles, 2 * 148);
-  icls::k_mlp_infer<<<grid, 128, icls::SB_INFER, s>>>(net_of(m), static_cast<const __nv_bfloat16*>(X), n, y, m->err);
+  icls::k_mlp_infer<<<grid, 128, icls::SB_INFER, s>>>(net_of(m), static_cast<const float*>(X), n, y, m->err);
   if (stream) return cudaGetLastError() == cudaSuccess ? ICLS_OK : ICLS_E_CUDA;
   return sync_err(m);
 }
@@ -794,11 +1019,12 @@ extern "C" int icls_mlp_eval(icls_mlp* m, double* stats) {
   double s[8] = {0, 0, 0, 0, 0, 0, 0, (double)n};
   for (size_t i = 0; i < n; ++i) {
     const double ka = ex[3 * i + 1], kp = ex[3 * i + 0];
-    s[0] += (y[i] - lab[i]) * (double)(y[i] - lab[i]);
-    s[1] += (y[i] - ka) * (y[i] - ka);
+    const double km = kp + y[i], kl = kp + lab[i];  // learned and refined-grid curvature
+    s[0] += (km - kl) * (km - kl);
+    s[1] += (km - ka) * (km - ka);
     s[2] += (kp - ka) * (kp - ka);
-    s[3] += (lab[i] - ka) * (lab[i] - ka);
-    s[4] = std::max(s[4], std::fabs(y[i] - ka));
+    s[3] += (kl - ka) * (kl - ka);
+    s[4] = std::max(s[4], std::fabs(km - ka));
     s[5] = std::max(s[5], std::fabs(kp - ka));
     s[6] += ka * ka;
   }
@@ -820,7 +1046,7 @@ extern "C" int icls_mlp_params(icls_mlp* m, float* host, int get) {
 }
 
 // the gradient of the summed squared error x scale over samples 0..n-1 of X
-// (device BF16 [n][32], labels device FP32), n a power of two >= 128, into
+// (device FP32 [n][32], labels device FP32), n a power of two >= 128, into
 // host grad[29057]; loss = sum of squared errors
 extern "C" int icls_mlp_grad(icls_mlp* m, const void* X, const float* label, long long n, float scale, float* grad,
                              double* loss) {
@@ -834,7 +1060,7 @@ extern "C" int icls_mlp_grad(icls_mlp* m, const void* X, const float* label, lon
   cudaMemsetAsync(m->loss, 0, sizeof(float), m->s);
   cudaMemsetAsync(m->grad, 0, sizeof(float) * kParams, m->s);
   icls::k_mlp_train_tile<<<(unsigned)(n / 128), 128, icls::SB_TRAIN, m->s>>>(
-      net_of(m), static_cast<const __nv_bfloat16*>(X), label, n, 0, 1ull, 0ull, scale, m->zbuf, m->grad, m->loss,
+      net_of(m), static_cast<const float*>(X), label, nullptr, n, 0, 1ull, 0ull, scale, m->zbuf, m->grad, m->loss,
       m->err);
   rc = sync_err(m);
   if (rc) return rc;

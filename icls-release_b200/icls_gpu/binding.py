@@ -350,3 +350,90 @@ def chkdiv_noalloc(u_ptr: int, v_ptr: int, w_ptr: int, imax: int, jmax: int, kma
                    C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     fn.restype = C.c_int
     return fn(u_ptr, v_ptr, w_ptr, imax, jmax, kmax, dxi, dyi, dzi, result_ptr, stream or None)
+
+
+class Mlp:
+    """The learned-curvature network (icls_mlp_* of the C ABI): 27-128-128-64-1
+    SiLU MLP trained and evaluated on the GPU's tensor cores."""
+
+    NPARAMS = 29057
+
+    def __init__(self, seed: int = 2024):
+        lib = gpu_backend().lib
+        P = C.c_void_p
+        sig = {
+            "icls_mlp_create": [C.POINTER(P), C.c_ulonglong],
+            "icls_mlp_destroy": [P],
+            "icls_mlp_make_data": [P, C.c_ulonglong, C.c_longlong, C.c_longlong],
+            "icls_mlp_train": [P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_ulonglong, C.POINTER(C.c_double)],
+            "icls_mlp_eval": [P, C.POINTER(C.c_double)],
+            "icls_mlp_params": [P, C.POINTER(C.c_float), C.c_int],
+            "icls_set_curvature_net": [P, P],
+            "icls_curvature_stats": [P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.c_int],
+        }
+        for name, args in sig.items():
+            getattr(lib, name).argtypes = args
+            getattr(lib, name).restype = C.c_int
+        self.lib = lib
+        h = P()
+        rc = lib.icls_mlp_create(C.byref(h), seed)
+        if rc:
+            raise IclsError(rc, "icls_mlp_create")
+        self.h = h
+
+    def _ok(self, rc, where):
+        if rc:
+            raise IclsError(rc, where)
+
+    def make_data(self, seed: int, n_train: int, n_hold: int):
+        self._ok(self.lib.icls_mlp_make_data(self.h, seed, n_train, n_hold), "icls_mlp_make_data")
+
+    def train(self, epochs: int = 20, batch: int = 8192, lr: float = 1e-3, lr_final: float = 1e-5, seed: int = 5):
+        losses = (C.c_double * epochs)()
+        self._ok(self.lib.icls_mlp_train(self.h, epochs, batch, lr, lr_final, seed, losses), "icls_mlp_train")
+        return list(losses)
+
+    def evaluate(self) -> dict:
+        st = (C.c_double * 8)()
+        self._ok(self.lib.icls_mlp_eval(self.h, st), "icls_mlp_eval")
+        keys = ("rms_mlp_label", "rms_mlp_analytic", "rms_plain_analytic", "rms_label_analytic",
+                "max_mlp_analytic", "max_plain_analytic", "rms_analytic", "samples")
+        return dict(zip(keys, list(st)))
+
+    def params(self) -> np.ndarray:
+        a = np.zeros(self.NPARAMS, dtype=np.float32)
+        self._ok(self.lib.icls_mlp_params(self.h, a.ctypes.data_as(C.POINTER(C.c_float)), 1), "icls_mlp_params")
+        return a
+
+    def set_params(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        self._ok(self.lib.icls_mlp_params(self.h, a.ctypes.data_as(C.POINTER(C.c_float)), 0), "icls_mlp_params")
+
+    def attach(self, solver: "Solver"):
+        """use this network for the solver's curvature (curvature_model MLP)"""
+        self._ok(self.lib.icls_set_curvature_net(solver.h, self.h), "icls_set_curvature_net")
+        solver._net = self
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.icls_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def curvature_stats(solver: "Solver", reset: bool = False):
+    """(cells the network evaluated, fallbacks to the stencil) of a solver"""
+    lib = gpu_backend().lib
+    fn = lib.icls_curvature_stats
+    fn.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.c_int]
+    fn.restype = C.c_int
+    e, f = C.c_longlong(), C.c_longlong()
+    rc = fn(solver.h, C.byref(e), C.byref(f), 1 if reset else 0)
+    if rc:
+        raise IclsError(rc, "icls_curvature_stats")
+    return e.value, f.value

@@ -187,9 +187,12 @@ int icls_band_count(icls_ctx* ctx, int l, long long* nb_cnt);
  * No counterpart in the reference: the network that replaces the
  * get_curvature stencil (interface.f90:20-119) near the interface in the
  * learned form.  27 -> 128 -> 128 -> 64 -> 1 SiLU MLP, BF16 weights and
- * activations on tcgen05 tiles, FP32 accumulation and FP32 Adam; input the
- * stencil (phi(x + o dx) - phi(x)) / dx, o in {-1,0,1}^3 (z outer, x inner),
- * output kappa * dx.  Training samples come from seeded spheres and
+ * activations on tcgen05 tiles (the FP32 inputs enter as BF16 hi + lo
+ * pairs), FP32 accumulation and FP32 Adam; input the features of the
+ * stencil (phi(x + o dx) - phi(x)) / dx, o in {-1,0,1}^3 (z outer, x inner):
+ * the stencil minus its least-squares linear part and the unit gradient,
+ * output the correction to the stencil's kappa * dx (learned kappa =
+ * kappa_stencil + output / dx).  Training samples come from seeded spheres and
  * ellipsoids (exact signed distance) with the least-squares curvature of a
  * 4x refined stencil as label.  All arrays named "device" live in GPU memory. */
 typedef struct icls_mlp icls_mlp;
@@ -198,18 +201,31 @@ int icls_mlp_create(icls_mlp** out, unsigned long long seed);
 int icls_mlp_destroy(icls_mlp* m);
 /* training and held-out samples; n_train a power of two */
 int icls_mlp_make_data(icls_mlp* m, unsigned long long seed, long long n_train, long long n_hold);
-/* loss_out[epochs] (optional): mean squared error per epoch */
-int icls_mlp_train(icls_mlp* m, int epochs, int batch, double lr, unsigned long long seed, double* loss_out);
+/* Adam on the squared error weighted by (0.1 / (|kappa dx| + 0.02))^2 (relative accuracy),
+ * step size from lr to lr_final along a half cosine; loss_out[epochs] (optional): mean
+ * weighted squared error per epoch */
+int icls_mlp_train(icls_mlp* m, int epochs, int batch, double lr, double lr_final, unsigned long long seed,
+                   double* loss_out);
 /* held-out statistics (kappa*dx): rms(mlp-label), rms(mlp-analytic), rms(plain-analytic),
  * rms(label-analytic), max|mlp-analytic|, max|plain-analytic|, rms|analytic|, samples */
 int icls_mlp_eval(icls_mlp* m, double stats[8]);
-/* y (device FP32 [n]) = network(X (device BF16 [n][32])); stream 0: synchronous */
+/* y (device FP32 [n]) = network(X (device FP32 [n][32])); stream 0: synchronous */
 int icls_mlp_infer(icls_mlp* m, const void* X, float* y, long long n, void* stream);
 /* parameters to (get = 1) or from (get = 0) host float[ICLS_MLP_PARAMS] */
 int icls_mlp_params(icls_mlp* m, float* host, int get);
 /* gradient of scale * sum (y - label)^2 over n samples (power of two >= 128) into host grad */
 int icls_mlp_grad(icls_mlp* m, const void* X, const float* label, long long n, float scale, float* grad,
                   double* loss);
+
+/* Attach a trained network to a context created with curvature_model =
+ * ICLS_CURV_MLP (grid spacing isotropic): gfm4p then uses the network's
+ * curvature at the cells with |phi| <= 4dz and falls back to the stencil
+ * per cell when the correction |kappa_mlp - kappa_stencil| dx > mlp_fallback_tol or
+ * |kappa_stencil| dx > 2/3 (curvature radius below 3 cells).  The network
+ * must outlive its use by the context. */
+int icls_set_curvature_net(icls_ctx* ctx, icls_mlp* net);
+/* cells the network evaluated and the fallbacks among them since the last reset */
+int icls_curvature_stats(icls_ctx* ctx, long long* evaluated, long long* fallbacks, int reset);
 
 /* ---- tensor-core tile check ----
  * No counterpart in the reference.  d (128 x n FP32, row-major) = a (128 x k

@@ -2,10 +2,12 @@
 
 A numpy restatement of the forward and backward pass that the tensor-core
 kernels (icls-release_b200/csrc/k_mlp.cu) compute, with the same rounding
-points: the inputs, the weights W1..W3, the hidden activations and the
-back-propagated deltas are rounded to BF16 (round to nearest even) where the
-kernels feed them to a BF16 tile; biases, W4, pre-activations, the head and
-every accumulation stay in higher precision (float64 here, FP32 on the GPU).
+points: each FP32 input enters as a BF16 pair hi = bf16(x), lo = bf16(x - hi);
+the weights W1..W3, the hidden activations and the back-propagated deltas
+are rounded to BF16 (round to nearest even) where the kernels feed them to a
+BF16 tile; biases, W4, pre-activations, the head and every accumulation stay
+in higher precision (float64 here, FP32 on the GPU).  The output is the
+correction to the plain stencil's kappa * dx.
 The network has no counterpart in the reference: it replaces the
 get_curvature stencil of interface.f90:20-119 in the learned form.
 
@@ -49,10 +51,13 @@ def dsilu(z):
 
 
 def forward(theta, X):
-    """y (kappa*dx) of BF16 inputs X [n][32] and the pre-activations"""
+    """y of FP32 inputs X [n][32] and the pre-activations"""
     W1, b1, W2, b2, W3, b3, W4, b4 = unpack(theta)
-    x = bf16(X)
-    z1 = x @ bf16(W1).T + b1
+    X32 = np.asarray(X, dtype=np.float32)
+    hi = bf16(X32)
+    lo = bf16(X32 - hi.astype(np.float32))
+    x = hi + lo  # both halves act through the same BF16 W1
+    z1 = hi @ bf16(W1).T + lo @ bf16(W1).T + b1
     h1 = bf16(silu(z1))
     z2 = h1 @ bf16(W2).T + b2
     h2 = bf16(silu(z2))
