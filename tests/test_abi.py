@@ -74,7 +74,9 @@ def test_config_default_matches_python_defaults(lib):
     (dict(reinit_step=0), "E_CONFIG"),
     (dict(ls_adv_space=7), "E_CONFIG"),
     (dict(precision=5), "E_CONFIG"),        # neither ICLS_FP64 nor ICLS_FP32
-    (dict(curvature_model=1), "E_UNSUPPORTED"),
+    (dict(curvature_model=2), "E_CONFIG"),      # neither stencil nor network
+    (dict(curvature_model=1, lx=2.0), "E_UNSUPPORTED"),  # the network needs isotropic spacing
+    (dict(curvature_model=1, mlp_fallback_tol=0.0), "E_CONFIG"),
 ])
 def test_create_rejects_bad_configs_on_host(lib, change, code):
     cfg = make_config(itot=32, jtot=32, ktot=32, lmax=1)
