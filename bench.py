@@ -8,12 +8,18 @@ pressure solve, projection, pressure update.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Default workload: the 256^3 box with 48 seeded drops (plain FP64).  Inputs
-(seven-plus GB of level sets and fields) are far larger than the 126 MB L2,
-so no flush is needed between steps.  Under torchrun each rank runs its own
-replica of the workload (the path is not sharded across GPUs here), the
-timed region is bracketed by a barrier and synchronisation on every rank,
-and the reported time is the max over ranks.
+Default workload: the 256^3 box with 48 seeded drops.  The headline value is
+the FP32 form with the learned curvature in the loop (FP64 kept for the
+Poisson solve, pressures, volume integral and GFM jumps), whose network is
+first trained on the GPU (4M seeded samples, 20 epochs); the same line
+carries the plain FP64 path on the same workload (value, per-kernel shares,
+roofline), the FP32 form with the plain stencil, and the form's errors
+against the FP64 run and against the analytic curvature of the seeded
+spheres.  Inputs (several GB of level sets and fields) are far larger than
+the 126 MB L2, so no flush is needed between steps.  Under torchrun each
+rank runs its own replica of the workload (the path is not sharded across
+GPUs), the timed region is bracketed by a barrier and synchronisation on
+every rank, and the reported time is the max over ranks.
 """
 import argparse
 import json
@@ -31,7 +37,7 @@ for p in (ROOT, os.path.join(ROOT, "icls-release_b200")):
 
 import numpy as np  # noqa: E402
 
-METRIC = "Mcell-steps/s at 256^3 (plain FP64 time step)"
+METRIC = "Mcell-steps/s at 256\u00b3: FP32+learned-\u03ba vs plain FP64 on B200, at stated vol/\u03ba error"
 UNIT = "Mcell-steps/s"
 
 
@@ -63,31 +69,47 @@ def initial_state(wl):
 
 
 # -------------------------------------------------- algorithmic byte model
-def alg_bytes_per_launch(name, cfg, stats):
-    """Compulsory HBM bytes of one launch of the named launcher group: the
-    per-cell value counts of an ideal fused implementation (8 B per FP64
-    value) times the cells that launch covers.  N = interior cells,
-    Nb = band cells of one drop, Ng = its |phi|<=2dz shell."""
-    N = cfg.itot * cfg.jtot * cfg.ktot
-    Nb = stats.get("band_mean", 0.0)
-    Ng = stats.get("shell_mean", 0.0)
-    v = {
-        "ab2": 24 * N,                  # u,v,w,miu,rho_uvw,duold x3,pnew,pold,p_xyz,p_xyz_old -> dudt x3,duold x3
-        "correc": 13 * N,               # dudt x3, p, p_xyz -> u,v,w, ucc,vcc,wcc
-        "fillps": 5 * N,                # dudt x3, p_jump -> p
-        "solver2d": 10 * N / 5,         # 5 passes read+write, per launch
-        "pressure_update": 4 * N / 2,   # p, pnew -> pnew, pold over two launches
-        "stream_vel": 1 * N / 2,
-        "materials_final": 6 * N / 2,   # jiemian -> miu, rho, rho_uvw
-        "tube": 2 * Nb,                 # phi -> clipped phi on the band
-        "adv_stage": (17.0 / 3.0) * Nb, # RK3 on the band, per stage
-        "heaviside_drop": 1 * Nb,       # phi read per band cell
-        "curvature": 2 * Ng,
-        "recurvature": 2 * Ng,
-        "jumps": 10 * Ng,
-        "reinit_stage": (11.0 / 3.0) * N,  # reinit region is the whole grid after clipping
-    }.get(name)
-    return None if v is None else 8.0 * v
+# Compulsory HBM values of one launcher scope (the unit the per-kernel device
+# timer brackets), as (bulk values, FP64 values, unit): bulk values are the
+# form's field type (8 B in plain FP64, 4 B in the FP32 form), FP64 values stay
+# 8 B in both (pressures, pressure gradients, Poisson RHS, jumps).  Units:
+# N interior cells, B band cells of all drops (one batched scope covers every
+# drop), S |phi| <= 2dz shell cells of all drops.
+ALG_VALUES = {
+    "ab2": (16, 8, "N"),             # u,v,w,miu,rho_uvw,duold x3 | pnew,pold,p_xyz,p_xyz_old -> dudt x3,duold x3
+    "correc": (9, 4, "N"),           # dudt x3 | p, p_xyz -> u,v,w, ucc,vcc,wcc
+    "fillps": (3, 2, "N"),           # dudt x3 | pjump -> p
+    "solver2d": (0, 2, "N"),         # p -> p (the transposes and sweeps between are not compulsory)
+    "pressure_update": (0, 4, "N"),  # p, pnew -> pnew, pold
+    "stream_vel": (1, 0, "N"),
+    "materials_final": (6, 0, "N"),  # jiemian -> miu, rho, rho_uvw
+    "tube": (2, 0, "B"),             # phi -> clipped phi on the band
+    "adv_stage": (17.0 / 3.0, 0, "B"),  # one RK3 stage on the band
+    "heaviside": (1, 0, "B"),
+    "curvature": (2, 0, "S"),
+    "recurvature": (2, 0, "S"),
+    "jumps": (4, 6, "S"),
+}
+
+
+# tensor-core FLOPs of one network evaluation: the three BF16 tile products
+# (layer 1 takes its 32 inputs as hi + lo pairs, K = 64)
+MLP_FLOPS_PER_CELL = 2 * (128 * 64 + 128 * 128 + 64 * 128)
+
+# DRAM bytes (read + write) of one scope of the dominant kernel, from an ncu
+# capture of the default workload: (kernel, FP32 form) -> bytes.
+TRAFFIC = {}
+
+
+def alg_bytes_per_launch(name, cfg, stats, f32=False):
+    """Compulsory HBM bytes of one scope of the named launcher."""
+    e = ALG_VALUES.get(name)
+    if e is None:
+        return None
+    bulk, f64, unit = e
+    n = {"N": cfg.itot * cfg.jtot * cfg.ktot, "B": stats.get("band_total", 0.0),
+         "S": stats.get("shell_total", 0.0)}[unit]
+    return (bulk * (4.0 if f32 else 8.0) + f64 * 8.0) * n
 
 
 # ------------------------------------------------------------------ clocks
@@ -210,7 +232,7 @@ def reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": steps, "warmup": 1, "ms_per_step": 1000.0 * dt / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_block(wl, world),
+        "config": config_block(wl, world, "fp64 (the reference's only form)"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": n, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "C++ restatement of the reference (oracle/, OpenMP); the Fortran/MPI reference cannot be "
@@ -220,60 +242,59 @@ def reference_arm(args):
     return 0
 
 
-def config_block(wl, world):
+def config_block(wl, world, form):
     c = wl.cfg
     return {"workload": wl.name, "grid": [c.itot, c.jtot, c.ktot], "drops": c.lmax,
             "dt": c.timestep, "scheme": "HOUC5" if c.ls_adv_space == 0 else "WENO5",
             "reinit_step": c.reinit_step, "reinit_iter_max": c.reinit_iter_max,
-            "inflate_step": c.inflate_step, "precision": "fp64",
+            "inflate_step": c.inflate_step, "form": form,
             "l2": "inputs larger than L2 (no flush)", "parallelism": "replicas x%d" % world}
 
 
-def ours_arm(args):
-    import torch
-    rank, world, local = dist_env()
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    else:
-        torch.cuda.set_device(local)
-    from icls_gpu import Solver
-    wl = make_workload(args.workload)
-    cfg = wl.cfg
-    ls, u, v, w = initial_state(wl)
-    cells = cfg.itot * cfg.jtot * cfg.ktot
-    shell = shell_and_band(wl, ls)
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
 
-    s = Solver(cfg)
-    s.setup(ls, u, v, w)
+
+def timed_steps(s, args, world, torch, istep, label, sampler=None):
+    """W warm-up steps, then K steps between barriers and synchronisations,
+    timed with CUDA events on the context's stream; max over ranks.  The K
+    steps sit in the NVTX push/pop range `label` (an ncu launch list of one
+    form selects them with --nvtx --nvtx-include "<label>/")."""
     stream = torch.cuda.ExternalStream(s.stream_ptr())
-    istep = 0
     for _ in range(args.warmup):
         istep += 1
         s.step(istep, 0)
-    sampler = ClockSampler(local)
     launches0 = s.launch_count()
-    sampler.start()
+    if sampler:
+        sampler.start()
     barrier(world)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push(label)
     e0.record(stream)
     for _ in range(args.steps):
         istep += 1
         s.step(istep, 0)
     e1.record(stream)
+    torch.cuda.nvtx.range_pop()
     e1.synchronize()
     torch.cuda.synchronize()
     barrier(world)
-    clocks = sampler.stop()
+    clocks = sampler.stop() if sampler else None
     ms = max_over_ranks(e0.elapsed_time(e1), world)
-    launches = s.launch_count() - launches0
-    value = cells * args.steps * world / (ms / 1000.0) / 1e6
+    return ms, istep, s.launch_count() - launches0, clocks
 
-    # ---- per-kernel device times over the same number of steps ----------
+
+def kernel_table(s, args, cfg, stats, istep, f32, mlp_cells=None):
+    """K more steps with every launcher scope bracketed by CUDA events: the
+    per-kernel shares and the roofline of the dominant one.  The network's
+    scope (gather + tiles) is rated against the tensor peak by its products'
+    FLOPs, mlp_cells evaluated cells per step."""
     s.profile(True)
     s.profile_reset()
     for _ in range(args.steps):
@@ -281,41 +302,168 @@ def ours_arm(args):
         s.step(istep, 0)
     table = s.profile_table()
     s.profile(False)
-    bands = [s.band_count(l + 1) for l in range(cfg.lmax)]
-    stats = {"band_mean": float(np.mean(bands)), "shell_mean": shell}
     tot = sum(e["ms"] for e in table.values()) or 1.0
-    top = max(table.items(), key=lambda kv: kv[1]["ms"])
-    name, ent = top
+    name, ent = max(table.items(), key=lambda kv: kv[1]["ms"])
     per_launch_ms = ent["ms"] / max(ent["timed"], 1)
-    alg = alg_bytes_per_launch(name, cfg, stats)
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except Exception:
-        pass
+    alg = alg_bytes_per_launch(name, cfg, stats, f32)
+    peaks = load_peaks()
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = (alg / (per_launch_ms / 1000.0) / 1e9) if alg else None
-    roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": None,
-                "share": ent["ms"] / tot, "launch_ms": per_launch_ms,
-                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
-    kernels = {k: {"share": round(e["ms"] / tot, 4), "launches": e["timed"],
-                   "ms_per_launch": e["ms"] / max(e["timed"], 1)} for k, e in table.items()}
+    tpeak = peaks.get("bf16_tflops", 1590.0)
+    if name == "mlp_curvature" and mlp_cells:
+        tf = MLP_FLOPS_PER_CELL * mlp_cells / (per_launch_ms / 1000.0) / 1e12
+        roofline = {"bound": "tensor", "kernel": name, "achieved": tf, "peak": tpeak, "unit": "TFLOP/s",
+                    "frac": tf / tpeak, "traffic": TRAFFIC.get((name, f32)), "flops": MLP_FLOPS_PER_CELL * mlp_cells,
+                    "share": ent["ms"] / tot, "launch_ms": per_launch_ms,
+                    "peak_source": "measured (cuBLAS bf16 burst)" if "bf16_tflops" in peaks else "fallback"}
+    else:
+        roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": (achieved / peak) if achieved else None, "traffic": TRAFFIC.get((name, f32)),
+                    "alg_bytes": alg, "share": ent["ms"] / tot, "launch_ms": per_launch_ms,
+                    "peak_source": "measured (burst copy)" if "hbm_gbs" in peaks else "fallback"}
+    kernels = {}
+    for k, e in sorted(table.items(), key=lambda kv: -kv[1]["ms"]):
+        if e["timed"] == 0:
+            continue
+        ms1 = e["ms"] / e["timed"]
+        ab = alg_bytes_per_launch(k, cfg, stats, f32)
+        kernels[k] = {"share": round(e["ms"] / tot, 4), "scopes": e["timed"], "ms_per_scope": round(ms1, 5),
+                      "hbm_frac": round(ab / (ms1 / 1000.0) / 1e9 / peak, 3) if ab else None}
+        if k == "mlp_curvature" and mlp_cells:
+            tf = MLP_FLOPS_PER_CELL * mlp_cells / (ms1 / 1000.0) / 1e12
+            kernels[k].update({"tflops": round(tf, 2), "tensor_frac": round(tf / tpeak, 4), "cells": mlp_cells})
+    return roofline, kernels, istep
+
+
+def drop_shells(wl):
+    """Per drop, the shape-C cells with ||x - c| - R| <= 1.5 dx (minimum image
+    in x and y) from the seeded geometry: flat Fortran-order indices and
+    distances |x - c|.  The drops move by far less than a cell in the steps
+    the bench runs, so the initial spheres locate the shells."""
+    cfg = wl.cfg
+    n1, n2, n3 = cfg.itot + 2, cfg.jtot + 2, cfg.ktot + 2
+    h = cfg.lz / cfg.ktot
+    out = []
+    for c, R in zip(wl.centres, wl.radii):
+        ax = []
+        for d, (nn, L) in enumerate(((n1, cfg.lx), (n2, cfg.ly), (n3, cfg.lz))):
+            lo = int(np.floor((c[d] - R - 2 * h) / h)) + 1
+            hi = int(np.ceil((c[d] + R + 2 * h) / h)) + 1
+            idx = np.arange(lo, hi + 1)
+            x = (idx - 0.5) * h
+            if d < 2:
+                idx = (idx - 1) % (nn - 2) + 1  # interior image of a periodic index
+                dd = x - c[d]
+            else:
+                keep = (idx >= 0) & (idx < nn)
+                idx, dd = idx[keep], (x - c[d])[keep]
+            ax.append((idx, dd))
+        I, J, K = np.meshgrid(ax[0][0], ax[1][0], ax[2][0], indexing="ij")
+        X, Y, Z = np.meshgrid(ax[0][1], ax[1][1], ax[2][1], indexing="ij")
+        r = np.sqrt(X * X + Y * Y + Z * Z)
+        m = np.abs(r - R) <= 1.5 * h
+        flat = (I[m] + n1 * (J[m] + n2 * K[m])).astype(np.int64)
+        out.append((flat, r[m]))
+    return out
+
+
+def train_network(torch):
+    """The learned curvature's network, trained on the GPU by the project's
+    own kernels: 4M seeded sphere/ellipsoid samples, 20 epochs of batch 8192,
+    Adam lr 1e-3 with a cosine decay to 1e-5."""
+    from icls_gpu.binding import Mlp
+    net = Mlp(2024)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    net.make_data(99, 1 << 22, 1 << 16)
+    t1 = time.perf_counter()
+    losses = net.train(epochs=20, batch=8192, lr=1e-3, lr_final=1e-5, seed=5)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    ev = net.evaluate()
+    info = {"samples": 1 << 22, "held_out": int(ev["samples"]), "epochs": 20, "batch": 8192,
+            "generate_s": round(t1 - t0, 3), "train_s": round(t2 - t1, 3),
+            "loss_first_epoch": losses[0], "loss_last_epoch": losses[-1],
+            "held_out_kdx_rms_vs_analytic": {"network": ev["rms_mlp_analytic"], "stencil": ev["rms_plain_analytic"],
+                                             "refined_label": ev["rms_label_analytic"]}}
+    return net, info
+
+
+def ours_arm(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from icls_gpu import CURV_MLP, FP32, Solver
+    from icls_gpu.binding import curvature_stats
+    from icls_gpu.config import IclsConfig
+    wl = make_workload(args.workload)
+    cfg = wl.cfg
+    ls, u, v, w = initial_state(wl)
+    cells = cfg.itot * cfg.jtot * cfg.ktot
+    h = cfg.lz / cfg.ktot
+    shells = drop_shells(wl)
+    shell = shell_and_band(wl, ls)
+
+    # ---- the network: trained before any timing --------------------------
+    net, net_info = (None, None)
+    if not args.no_forms:
+        net, net_info = train_network(torch)
+
+    # ---- plain FP64 -------------------------------------------------------
+    ref = Solver(cfg)
+    ref.setup(ls, u, v, w)
+    ms64, istep, launches64, clocks64 = timed_steps(ref, args, world, torch, 0, "fp64", ClockSampler(local))
+    stats = {"band_total": float(sum(ref.band_count(l + 1) for l in range(cfg.lmax))),
+             "shell_total": shell * cfg.lmax}
+    roof64, kern64, istep = kernel_table(ref, args, cfg, stats, istep, False)
+    v64 = cells * args.steps * world / (ms64 / 1000.0) / 1e6
+    plain = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / args.steps, "dtype": "f64",
+             "gpu_launches": launches64, "clocks": clocks64, "roofline": roof64, "kernels": kern64}
     torch.cuda.synchronize()
 
-    # ---- the precision form on the same workload ------------------------
-    prec = None
+    form = None
     if not args.no_forms:
-        prec = precision_leg(args, wl, ls, u, v, w, torch, world, istep, s)
-        prec["speedup_vs_fp64"] = prec["value"] / value
-    del s
+        # ---- FP32 + learned curvature (the headline form) -------------------
+        cf = IclsConfig.from_buffer_copy(cfg)
+        cf.precision = FP32
+        cf.curvature_model = CURV_MLP
+        s = Solver(cf)
+        net.attach(s)
+        s.setup(ls, u, v, w)
+        ms, istep_f, launches, clocks = timed_steps(s, args, world, torch, 0, "fp32_learned_kappa",
+                                                     ClockSampler(local))
+        ev, fb = curvature_stats(s, reset=True)
+        roof, kern, istep_f = kernel_table(s, args, cfg, stats, istep_f, True,
+                                           ev / max(args.warmup + args.steps, 1))
+        assert istep_f == istep
+        errors = form_errors(s, ref, wl, shells, h, istep)
+        errors["fallback_fraction"] = fb / max(ev, 1)
+        errors["network_cells_per_step"] = ev / max(args.warmup + args.steps, 1)
+        form = {"value": cells * args.steps * world / (ms / 1000.0) / 1e6, "ms_per_step": ms / args.steps,
+                "gpu_launches": launches, "clocks": clocks, "roofline": roof, "kernels": kern, "errors": errors}
+        del s
+        torch.cuda.synchronize()
+        # ---- FP32 with the plain stencil (splits the gain) -------------------
+        cs = IclsConfig.from_buffer_copy(cfg)
+        cs.precision = FP32
+        s = Solver(cs)
+        s.setup(ls, u, v, w)
+        ms32, _, _, _ = timed_steps(s, args, world, torch, 0, "fp32_stencil")
+        form["fp32_stencil"] = {"value": cells * args.steps * world / (ms32 / 1000.0) / 1e6,
+                                "ms_per_step": ms32 / args.steps}
+        del s
+        torch.cuda.synchronize()
+    del ref
     torch.cuda.synchronize()
 
     # ---- end to end through the per-subroutine C ABI, host buffers -------
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, wl, ls, u, v, w, torch, world)
+        e2e = run_e2e(args, wl, ls, u, v, w, torch, world, net)
 
     # ---- CPU baseline: the oracle on a bounded sample ---------------------
     cpu = None
@@ -323,16 +471,32 @@ def ours_arm(args):
         threads = os.cpu_count() or 1
         cv, n, dt = cpu_sample(wl, ls, u, v, w, 1, threads)
         cpu = {"value": cv, "unit": UNIT, "cores": n, "kind": "port",
-               "sample": "one time step of %s on %d host threads after one untimed step (%.1f s)" % (wl.name, n, dt)}
+               "sample": "one plain FP64 time step of %s on %d host threads after one untimed step (%.1f s)"
+                         % (wl.name, n, dt)}
+    if net is not None:
+        net.close()
 
     if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded drops)",
-            "config": config_block(wl, world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": launches, "clocks": clocks, "kernels": kernels, "precision_form": prec,
-        }
+        if form is not None:
+            line = {
+                "metric": METRIC, "value": form["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": form["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 (f64 Poisson/pressure, volume integral, GFM jumps; bf16 network, f32 accumulate)",
+                "data": "synthetic (seeded drops; network trained on seeded spheres/ellipsoids)",
+                "config": config_block(wl, world, "fp32+learned-curvature"),
+                "roofline": form["roofline"], "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": form["gpu_launches"], "clocks": form["clocks"],
+                "speedup_vs_fp64": form["value"] / v64, "errors": form["errors"],
+                "plain_fp64": plain, "fp32_stencil": form["fp32_stencil"], "network": net_info,
+                "kernels": form["kernels"]}
+        else:
+            line = {
+                "metric": METRIC, "value": v64, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms64 / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded drops)",
+                "config": config_block(wl, world, "fp64"), "roofline": roof64, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches64, "clocks": clocks64, "kernels": kern64}
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
@@ -340,68 +504,61 @@ def ours_arm(args):
     return 0
 
 
-def precision_leg(args, wl, ls, u, v, w, torch, world, fp64_solver_steps, ref):
-    """The precision form (FP32 bulk, FP64 Poisson / volume / jumps) on the
-    same workload: the same warm-up and timed steps, timed like the plain
-    path; then its errors against the plain FP64 context `ref`, which has run
-    fp64_solver_steps steps from the same initial state."""
-    from icls_gpu import FP32, Solver
-    from icls_gpu.config import IclsConfig
-    cfg = IclsConfig.from_buffer_copy(wl.cfg)
-    cfg.precision = FP32
-    s = Solver(cfg)
-    s.setup(ls, u, v, w)
-    stream = torch.cuda.ExternalStream(s.stream_ptr())
-    istep = 0
-    for _ in range(args.warmup):
-        istep += 1
-        s.step(istep, 0)
-    barrier(world)
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        istep += 1
-        s.step(istep, 0)
-    e1.record(stream)
-    e1.synchronize()
-    barrier(world)
-    ms = max_over_ranks(e0.elapsed_time(e1), world)
-    cells = cfg.itot * cfg.jtot * cfg.ktot
-    out = {"value": cells * args.steps * world / (ms / 1000.0) / 1e6, "unit": UNIT,
-           "ms_per_step": ms / args.steps, "dtype": "f32 bulk, f64 Poisson/volume/jumps"}
-    # errors after the same number of steps as the FP64 reference context
-    while istep < fp64_solver_steps:
-        istep += 1
-        s.step(istep, 0)
-    if istep == fp64_solver_steps:
-        def rel(a, b):
-            return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
-        dz = wl.cfg.lz / wl.cfg.ktot
-        band = 0.0
-        for l in range(1, min(wl.cfg.lmax, 4) + 1):
-            pa, pb = s.download("lvset", l), ref.download("lvset", l)
-            m = np.abs(pb) <= 4.0 * dz
-            band = max(band, rel(pa[m], pb[m]))
-        va, vb = s.volumes()[0], ref.volumes()[0]
-        out["errors_vs_fp64"] = {
-            "steps": istep, "phi_band_rel_l2": band,
-            "u_rel_l2": rel(s.download("u"), ref.download("u")),
-            "w_rel_l2": rel(s.download("w"), ref.download("w")),
-            "volume_max_rel": float(np.max(np.abs(va - vb) / vb)),
-            "curv_rel_l2": rel(s.download("curv"), ref.download("curv")),
-            "drops_compared_phi": min(wl.cfg.lmax, 4)}
-    del s
+def form_errors(s, ref, wl, shells, h, istep):
+    """The form against the plain FP64 context after the same steps from the
+    same initial state: phi on the |phi| <= 4dz band (first four drops),
+    velocities, per-drop volume; each context's volume drift since the
+    initial state; and, drop by drop, the curvature get_curvature gives on
+    the drop's shell (the network's, with its fallback, in the form) against
+    the FP64 stencil's and against the analytic -2/r of the seeded sphere."""
+    def rel(a, b):
+        return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+    band = 0.0
+    for l in range(1, min(wl.cfg.lmax, 4) + 1):
+        pa, pb = s.download("lvset", l), ref.download("lvset", l)
+        m = np.abs(pb) <= 4.0 * h
+        band = max(band, rel(pa[m], pb[m]))
+    va, va0 = s.volumes()
+    vb, vb0 = ref.volumes()
+    out = {
+        "steps": istep, "drops_compared_phi": min(wl.cfg.lmax, 4), "phi_band_rel_l2": band,
+        "u_rel_l2": rel(s.download("u"), ref.download("u")), "v_rel_l2": rel(s.download("v"), ref.download("v")),
+        "w_rel_l2": rel(s.download("w"), ref.download("w")),
+        "volume_max_rel_vs_fp64": float(np.max(np.abs(va - vb) / vb)),
+        "volume_drift_max_rel": {"form": float(np.max(np.abs(va - va0) / va0)),
+                                 "fp64": float(np.max(np.abs(vb - vb0) / vb0))},
+    }
+    acc = {"form": [0.0, 0.0], "fp64_stencil": [0.0, 0.0]}
+    d2, p2, cells = 0.0, 0.0, 0
+    for l, (flat, r) in enumerate(shells, start=1):
+        kap = {}
+        for name, ctx in (("form", s), ("fp64_stencil", ref)):
+            ctx.get_curvature(l)
+            kap[name] = ctx.download("curv").ravel(order="F")[flat]
+            acc[name][0] += float(np.sum((kap[name] + 2.0 / r) ** 2))
+        acc["form"][1] += float(np.sum((2.0 / r) ** 2))
+        d2 += float(np.sum((kap["form"] - kap["fp64_stencil"]) ** 2))
+        p2 += float(np.sum(kap["fp64_stencil"] ** 2))
+        cells += flat.size
+    out["curv_shell_rel_l2_vs_fp64"] = float(np.sqrt(d2 / max(p2, 1e-300)))
+    out["curv_vs_analytic"] = {
+        name: {"kdx_rms": float(np.sqrt(e2 / max(cells, 1))) * h, "rel": float(np.sqrt(e2 / acc["form"][1]))}
+        for name, (e2, _) in acc.items()}
+    out["curv_vs_analytic"]["shell_cells"] = cells
     return out
 
 
-def run_e2e(args, wl, ls, u, v, w, torch, world):
+def run_e2e(args, wl, ls, u, v, w, torch, world, net=None):
     """Upload the initial state from pinned host memory, init_program, K steps
     through the subroutines main.f90 calls (with its per-step NaN probe),
-    download the final fields; all inside the timed region."""
-    from icls_gpu import Solver
-    cfg = wl.cfg
+    download the final fields; all inside the timed region.  With a network
+    the context is the FP32 + learned-curvature form."""
+    from icls_gpu import CURV_MLP, FP32, Solver
+    from icls_gpu.config import IclsConfig
+    cfg = IclsConfig.from_buffer_copy(wl.cfg)
+    if net is not None:
+        cfg.precision = FP32
+        cfg.curvature_model = CURV_MLP
 
     def pinned(a):
         t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
@@ -416,6 +573,8 @@ def run_e2e(args, wl, ls, u, v, w, torch, world):
     h2d = 8 * (4 * u.size + cfg.lmax * hls[0].numel())
     d2h = 8 * (4 * u.size + cfg.lmax * hls[0].numel())
     s = Solver(cfg)
+    if net is not None:
+        net.attach(s)
     stream = torch.cuda.ExternalStream(s.stream_ptr())
     barrier(world)
     torch.cuda.synchronize()
@@ -460,7 +619,8 @@ def run_e2e(args, wl, ls, u, v, w, torch, world):
     del s
     return {"value": cells * args.steps * world / (ms / 1000.0) / 1e6, "unit": UNIT,
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": (d2h + 8 * probes) / args.steps,
-            "path": "per-subroutine C ABI (upload, init_program, ls_main..average_vel_at_center, download)",
+            "path": "per-subroutine C ABI (FP64 host arrays; upload, init_program, ls_main..average_vel_at_center, "
+                    "download)", "form": "fp32+learned-curvature" if net is not None else "fp64",
             "ms_total": ms}
 
 
@@ -473,7 +633,8 @@ def main():
     ap.add_argument("--workload", default="multi_drop_256_48")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-forms", action="store_true", help="skip the precision-form leg")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="plain FP64 only (no network training, no FP32 forms)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -257,7 +257,7 @@ void release(Ctx& c) {
   if (c.lpartials) cudaFree(c.lpartials);
   if (c.drs) cudaFree(c.drs);
   if (c.stage) cudaFree(c.stage);
-  for (void* f : {(void*)c.mlp_X, c.mlp_rec, (void*)c.mlp_y, (void*)c.mlp_count, (void*)c.mlp_stats})
+  for (void* f : {(void*)c.mlp_X, c.mlp_rec, (void*)c.mlp_count, (void*)c.mlp_stats})
     if (f) cudaFree(f);
   if (c.dsc) cudaFree(c.dsc);
   if (c.h_vol) cudaFreeHost(c.h_vol);
@@ -1320,6 +1320,11 @@ int icls_get_curvature(icls_ctx* h, int l) {
   b[0].t[0].phi0 = c.lv[l - 1];
   b[0].t[0].out = c.curv;
   launch_curvature(c, b[0], c.nrm_m);
+  // the learned form: the network's curvature near the interface, as gfm4p uses it
+  if (c.cfg.curvature_model == ICLS_CURV_MLP && c.net) {
+    const int rc = launch_mlp_curvature(c, b[0]);
+    if (rc) return rc;
+  }
   c.curv_stale = c.nrm_stale = false;
   return check_launch();
 }

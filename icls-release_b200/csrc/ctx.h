@@ -149,7 +149,6 @@ struct Ctx {
   icls_mlp* net = nullptr;
   float* mlp_X = nullptr;
   void* mlp_rec = nullptr;
-  float* mlp_y = nullptr;
   int* mlp_count = nullptr;
   unsigned long long* mlp_stats = nullptr;  // cells evaluated, fallbacks to the stencil
   int mlp_cap = 0;

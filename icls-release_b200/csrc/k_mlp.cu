@@ -111,7 +111,6 @@ constexpr int SB_H1T = SB_XT + 16384;         // H1^T [128 x 128]
 constexpr int SB_H2T = SB_H1T + 32768;        // H2^T [128 x 128]
 constexpr int SB_DZT = SB_H2T + 32768;        // delta^T [128 x 128]
 constexpr int SB_TRAIN = SB_DZT + 32768;      // 196608
-constexpr int SB_INFER = SB_XT;               // forward only: B, ACT, XA (81920)
 
 // a weight matrix [n][k] (row-major BF16, global) into the B operand layout
 __device__ __forceinline__ void stage_b(unsigned char* sb, const __nv_bfloat16* __restrict__ w, int n, int k) {
@@ -306,32 +305,154 @@ __global__ void __launch_bounds__(128) k_mlp_train_tile(Net net, const float* __
   if (warp == 0) umma::tmem_free(tmem, 128);
 }
 
-// inference over n samples, one 128-sample tile per iteration
-__global__ void __launch_bounds__(128) k_mlp_infer(Net net, const float* __restrict__ X, long long n,
-                                                   float* __restrict__ y, int* __restrict__ err) {
+// ---- inference with the weights resident in shared memory --------------
+// A persistent CTA stages W1..W3 (B operands) and the biases once and then
+// runs its 128-sample tiles back to back.  The first 16 KB of the
+// activation buffer also hold a tile's inputs (hi | lo, A layout [128 x 64]):
+// layer 1 has finished reading them before its epilogue writes the first
+// activations.  99,856 bytes: two CTAs per SM.
+constexpr int SI_W1 = 0;                          // [128 x 64]
+constexpr int SI_W2 = SI_W1 + kH1 * kIn2 * 2;     // [128 x 128]
+constexpr int SI_W3 = SI_W2 + kH2 * kH1 * 2;      // [64 x 128]
+constexpr int SI_ACT = SI_W3 + kH3 * kH2 * 2;     // [128 x 128], inputs in its first 16 KB
+constexpr int SI_PAR = SI_ACT + kRows * kH1 * 2;  // b1, b2, b3, w4, b4 (FP32)
+constexpr int PB1 = 0, PB2 = PB1 + kH1, PB3 = PB2 + kH2, PW4 = PB3 + kH3, PB4 = PW4 + kH3;
+constexpr int SB_INFER = SI_PAR + 4 * (PB4 + 4);
+
+// SiLU for the forward-only path (the BF16 rounding that follows dwarfs the
+// approximate divide); the exponent is capped so the divisor stays finite
+__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.f + __expf(fminf(-z, 80.f))); }
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);  // a at the lower address
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// a weight matrix [n][k] (row-major BF16, 16-byte aligned rows) into the
+// B-operand layout, one 16-byte chunk per store
+__device__ __forceinline__ void stage_rows(unsigned char* dst, const __nv_bfloat16* __restrict__ w, int n, int k) {
+  for (int e = threadIdx.x; e < n * (k / 8); e += blockDim.x) {
+    const int c = e / n, r = e - c * n;
+    *reinterpret_cast<uint4*>(dst + kmajor_off(r, 8 * c, n)) =
+        *reinterpret_cast<const uint4*>(w + (size_t)r * k + 8 * c);
+  }
+}
+
+// row t of the tile: the sample's 32 FP32 inputs as BF16 hi (k 0..31) and
+// lo (k 32..63); zeros past the end
+__device__ __forceinline__ void stage_inputs(unsigned char* act, const float* __restrict__ x, int t) {
+#pragma unroll
+  for (int c = 0; c < kIn / 8; ++c) {
+    float v[8];
+    if (x) {
+      const float4 a = *reinterpret_cast<const float4*>(x + 8 * c);
+      const float4 b = *reinterpret_cast<const float4*>(x + 8 * c + 4);
+      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = 0.f;
+    }
+    float hi[8], lo[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      hi[q] = __bfloat162float(__float2bfloat16(v[q]));
+      lo[q] = v[q] - hi[q];
+    }
+    *reinterpret_cast<uint4*>(act + kmajor_off(t, 8 * c, kRows)) =
+        make_uint4(pack_bf16(hi[0], hi[1]), pack_bf16(hi[2], hi[3]), pack_bf16(hi[4], hi[5]), pack_bf16(hi[6], hi[7]));
+    *reinterpret_cast<uint4*>(act + kmajor_off(t, kIn + 8 * c, kRows)) =
+        make_uint4(pack_bf16(lo[0], lo[1]), pack_bf16(lo[2], lo[3]), pack_bf16(lo[4], lo[5]), pack_bf16(lo[6], lo[7]));
+  }
+}
+
+// a hidden layer's epilogue: row t of SiLU(D + bias) as the next A operand
+__device__ __forceinline__ void hidden_epilogue(uint32_t lane_addr, const float* bias, int n, unsigned char* act,
+                                                int t) {
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    float v[32];
+    umma::tmem_ld32(lane_addr + (uint32_t)c0, v);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      float h[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) h[q] = silu_fast(v[8 * m + q] + bias[c0 + 8 * m + q]);
+      *reinterpret_cast<uint4*>(act + kmajor_off(t, c0 + 8 * m, kRows)) =
+          make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]), pack_bf16(h[6], h[7]));
+    }
+  }
+}
+
+// The forward pass over samples 0..n-1 of X (FP32 [n][32], 16-byte
+// aligned), tiles blockIdx.x, blockIdx.x + gridDim.x, ...; out(s, y) takes
+// each sample's output.  All 128 threads call it.
+template <class Out>
+__device__ __forceinline__ void infer_tiles(const Net& net, const float* __restrict__ X, long long n, Out& out,
+                                            int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char sm[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_slot;
   const int t = threadIdx.x, warp = t >> 5;
-  if (t == 0) umma::mbar_init(&bar, 1);
+  const long long tiles = (n + kRows - 1) / kRows;
+  if ((long long)blockIdx.x >= tiles) return;  // block-uniform: no tensor memory taken
+  stage_rows(sm + SI_W1, net.w1, kH1, kIn2);
+  stage_rows(sm + SI_W2, net.w2, kH2, kH1);
+  stage_rows(sm + SI_W3, net.w3, kH3, kH2);
+  float* par = reinterpret_cast<float*>(sm + SI_PAR);
+  for (int e = t; e < kH1; e += blockDim.x) par[PB1 + e] = net.theta[oB1 + e];
+  for (int e = t; e < kH2; e += blockDim.x) par[PB2 + e] = net.theta[oB2 + e];
+  for (int e = t; e < kH3; e += blockDim.x) {
+    par[PB3 + e] = net.theta[oB3 + e];
+    par[PW4 + e] = net.theta[oW4 + e];
+  }
+  if (t == 0) {
+    par[PB4] = net.theta[oB4];
+    umma::mbar_init(&bar, 1);
+  }
   if (warp == 0) umma::tmem_alloc(&tmem_slot, 128);
   umma::fence_before();
   __syncthreads();
   umma::fence_after();
   const uint32_t tmem = tmem_slot;
+  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
   uint32_t phase = 0;
   bool ok = true;
-  const long long tiles = (n + kRows - 1) / kRows;
   for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const long long s = tile * kRows + t;
-    const float v = forward_tile<false>(net, s < n ? X + s * kIn : nullptr, sm, tmem, &bar, phase, nullptr, ok);
-    if (s < n) y[s] = v;
+    stage_inputs(sm + SI_ACT, s < n ? X + s * kIn : nullptr, t);
+    ok &= umma::tile_gemm(sm + SI_ACT, sm + SI_W1, kH1, kIn2, tmem, &bar, phase);
+    hidden_epilogue(lane_addr, par + PB1, kH1, sm + SI_ACT, t);
+    ok &= umma::tile_gemm(sm + SI_ACT, sm + SI_W2, kH2, kH1, tmem, &bar, phase);
+    hidden_epilogue(lane_addr, par + PB2, kH2, sm + SI_ACT, t);
+    ok &= umma::tile_gemm(sm + SI_ACT, sm + SI_W3, kH3, kH2, tmem, &bar, phase);
+    float y = par[PB4];
+    for (int c0 = 0; c0 < kH3; c0 += 32) {
+      float v[32];
+      umma::tmem_ld32(lane_addr + (uint32_t)c0, v);
+#pragma unroll
+      for (int q = 0; q < 32; ++q) y += par[PW4 + c0 + q] * silu_fast(v[q] + par[PB3 + c0 + q]);
+    }
+    if (s < n) out(s, y);
     if (!__syncthreads_and(ok)) break;  // block-uniform exit after a wait that gave up
   }
-  if (!ok && t == 0) atomicExch(err, 1);
+  if (!ok) {
+    if (t == 0) atomicExch(err, 1);
+    umma::mbar_wait(&bar, phase ^ 1u);  // let a late completion land before the columns are freed
+  }
   umma::fence_before();
   __syncthreads();
   if (warp == 0) umma::tmem_free(tmem, 128);
+}
+
+struct StoreOut {
+  float* y;
+  __device__ void operator()(long long s, float v) const { y[s] = v; }
+};
+
+// inference over n samples into y
+__global__ void __launch_bounds__(128, 2) k_mlp_infer(Net net, const float* __restrict__ X, long long n,
+                                                      float* __restrict__ y, int* __restrict__ err) {
+  StoreOut o{y};
+  infer_tiles(net, X, n, o, err);
 }
 
 // parameter q's BF16 value into the tile copies
@@ -644,7 +765,7 @@ struct MlpCell {
 // re_curvature and the jumps read) into X, slots by a warp-aggregated
 // counter; cells beyond cap keep the plain curvature.
 template <typename T>
-__global__ void __launch_bounds__(256) k_mlp_gather(Params p, const __grid_constant__ LsBatch B,
+__global__ void __launch_bounds__(256, 2) k_mlp_gather(Params p, const __grid_constant__ LsBatch B,
                                                     float* __restrict__ X, MlpCell* __restrict__ rec,
                                                     int* __restrict__ count, int cap) {
   const int ti = task_of(B);
@@ -678,63 +799,36 @@ __global__ void __launch_bounds__(256) k_mlp_gather(Params p, const __grid_const
     for (int dk = -1; dk <= 1; ++dk)
       for (int dj = -1; dj <= 1; ++dj)
         for (int di = -1; di <= 1; ++di) f[n++] = ((float)phi[cl + di + dj * sy + dk * sz] - pc) * rdz;
-    mlp_features(f, X + (long long)slot * kIn);
+    float o[kIn];
+    mlp_features(f, o);
+    float4* dst = reinterpret_cast<float4*>(X + (long long)slot * kIn);
+#pragma unroll
+    for (int q = 0; q < kIn / 4; ++q) dst[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
     rec[slot] = MlpCell{ti, c.i, c.j, k};
   }
 }
 
-// inference over the first min(*count, cap) rows of X
-__global__ void __launch_bounds__(128) k_mlp_infer_count(Net net, const float* __restrict__ X,
-                                                         const int* __restrict__ count, int cap, float* __restrict__ y,
-                                                         int* __restrict__ err) {
-  extern __shared__ __align__(16) unsigned char sm[];
-  __shared__ __align__(8) uint64_t bar;
-  __shared__ uint32_t tmem_slot;
-  const int t = threadIdx.x, warp = t >> 5;
-  const long long n = min(*count, cap);
-  const long long tiles = (n + kRows - 1) / kRows;
-  if ((long long)blockIdx.x >= tiles) return;  // block-uniform: no tensor memory taken
-  if (t == 0) umma::mbar_init(&bar, 1);
-  if (warp == 0) umma::tmem_alloc(&tmem_slot, 128);
-  umma::fence_before();
-  __syncthreads();
-  umma::fence_after();
-  const uint32_t tmem = tmem_slot;
-  uint32_t phase = 0;
-  bool ok = true;
-  for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const long long s = tile * kRows + t;
-    const float v = forward_tile<false>(net, s < n ? X + s * kIn : nullptr, sm, tmem, &bar, phase, nullptr, ok);
-    if (s < n) y[s] = v;
-    if (!__syncthreads_and(ok)) break;
-  }
-  if (!ok && t == 0) atomicExch(err, 1);
-  umma::fence_before();
-  __syncthreads();
-  if (warp == 0) umma::tmem_free(tmem, 128);
-}
-
 // the learned curvature kappa_plain + y/dx where it passes the checks, the
 // plain one otherwise (a correction |y| > tol, or a curvature radius below 3
-// cells, |kappa_plain| dx > 2/3); stats[0] += evaluated, stats[1] +=
-// fallbacks
+// cells, |kappa_plain| dx > 2/3), written straight from the last layer's
+// epilogue of the gathered cells' tiles
 template <typename T>
-__global__ void __launch_bounds__(256) k_mlp_apply(Params p, const __grid_constant__ LsBatch B,
-                                                   const MlpCell* __restrict__ rec, const float* __restrict__ y,
-                                                   const int* __restrict__ count, int cap, double tol,
-                                                   unsigned long long* __restrict__ stats) {
-  const long long n = min(*count, cap);
-  const double dz = p.dz;
-  unsigned long long ev = 0, fb = 0;
-  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+struct ApplyOut {
+  const Params& p;
+  const LsBatch& B;
+  const MlpCell* __restrict__ rec;
+  double tol;
+  unsigned long long ev, fb;
+  __device__ void operator()(long long s, float y) {
     const MlpCell r = rec[s];
     T* out = mT<T>(B.t[r.q].out);
+    const double dz = p.dz;
     const double kp = (double)out[idxC(p, r.i, r.j, r.k)];
-    double km = kp + (double)y[s] / dz;
+    double km = kp + (double)y / dz;
     ++ev;
     if (fabs(kp) * dz > 2. / 3. || fabs(km - kp) * dz > tol) {
       ++fb;
-      continue;
+      return;
     }
     const double maxk = 1. / dz;  // the clamps of interface.f90:104-111
     if (km < -maxk) km = -maxk;
@@ -742,9 +836,23 @@ __global__ void __launch_bounds__(256) k_mlp_apply(Params p, const __grid_consta
     else if (fabs(km) < 1e-9) km = 0.;
     putC(p, out, r.i, r.j, r.k, (T)km);
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    ev += __shfl_down_sync(0xffffffffu, ev, o);
-    fb += __shfl_down_sync(0xffffffffu, fb, o);
+};
+
+// the network over the first min(*count, cap) gathered cells and the
+// per-cell choice; stats[0] += evaluated, stats[1] += fallbacks
+template <typename T>
+__global__ void __launch_bounds__(128, 2) k_mlp_curv(Net net, const float* __restrict__ X,
+                                                     const int* __restrict__ count, int cap, Params p,
+                                                     const __grid_constant__ LsBatch B,
+                                                     const MlpCell* __restrict__ rec, double tol,
+                                                     unsigned long long* __restrict__ stats, int* __restrict__ err) {
+  const long long n = min(*count, cap);
+  ApplyOut<T> o{p, B, rec, tol, 0ull, 0ull};
+  infer_tiles(net, X, n, o, err);
+  unsigned long long ev = o.ev, fb = o.fb;
+  for (int d = 16; d > 0; d >>= 1) {
+    ev += __shfl_down_sync(0xffffffffu, ev, d);
+    fb += __shfl_down_sync(0xffffffffu, fb, d);
   }
   if ((threadIdx.x & 31) == 0 && ev) {
     atomicAdd(stats, ev);
@@ -813,7 +921,7 @@ namespace icls {
 int launch_mlp_curvature(Ctx& c, const LsBatch& b) {
   if (b.n == 0) return ICLS_OK;
   if (!c.net) return ICLS_E_STATE;
-  Scope sc_(c.prof, c.s, "mlp_curvature", 3);
+  Scope sc_(c.prof, c.s, "mlp_curvature", 2);
   cudaMemsetAsync(c.mlp_count, 0, sizeof(int), c.s);
   if (c.P.f32)
     k_mlp_gather<float><<<b.start[b.n], dim3(TBX, TBY, 1), 0, c.s>>>(c.P, b, c.mlp_X, (MlpCell*)c.mlp_rec,
@@ -821,16 +929,14 @@ int launch_mlp_curvature(Ctx& c, const LsBatch& b) {
   else
     k_mlp_gather<double><<<b.start[b.n], dim3(TBX, TBY, 1), 0, c.s>>>(c.P, b, c.mlp_X, (MlpCell*)c.mlp_rec,
                                                                        c.mlp_count, c.mlp_cap);
-  const int tiles = (c.mlp_cap + 127) / 128;
-  k_mlp_infer_count<<<std::min(tiles, 2 * 148), 128, SB_INFER, c.s>>>(net_of(c.net), c.mlp_X, c.mlp_count, c.mlp_cap,
-                                                                      c.mlp_y, c.net->err);
+  const int grid = std::min((c.mlp_cap + kRows - 1) / kRows, 2 * 148);
   const double tol = c.cfg.mlp_fallback_tol;
   if (c.P.f32)
-    k_mlp_apply<float><<<592, 256, 0, c.s>>>(c.P, b, (const MlpCell*)c.mlp_rec, c.mlp_y, c.mlp_count, c.mlp_cap, tol,
-                                             c.mlp_stats);
+    k_mlp_curv<float><<<grid, 128, SB_INFER, c.s>>>(net_of(c.net), c.mlp_X, c.mlp_count, c.mlp_cap, c.P, b,
+                                                    (const MlpCell*)c.mlp_rec, tol, c.mlp_stats, c.net->err);
   else
-    k_mlp_apply<double><<<592, 256, 0, c.s>>>(c.P, b, (const MlpCell*)c.mlp_rec, c.mlp_y, c.mlp_count, c.mlp_cap,
-                                              tol, c.mlp_stats);
+    k_mlp_curv<double><<<grid, 128, SB_INFER, c.s>>>(net_of(c.net), c.mlp_X, c.mlp_count, c.mlp_cap, c.P, b,
+                                                     (const MlpCell*)c.mlp_rec, tol, c.mlp_stats, c.net->err);
   return ICLS_OK;
 }
 
@@ -851,13 +957,14 @@ int mlp_buffers(Ctx& c, int cap) {
   if (mlp_constants()) return ICLS_E_CUDA;
   if (cudaMalloc(&c.mlp_X, (size_t)cap * kIn * 4) != cudaSuccess) return ICLS_E_NOMEM;
   if (cudaMalloc(&c.mlp_rec, (size_t)cap * sizeof(MlpCell)) != cudaSuccess) return ICLS_E_NOMEM;
-  if (cudaMalloc(&c.mlp_y, (size_t)cap * sizeof(float)) != cudaSuccess) return ICLS_E_NOMEM;
   if (cudaMalloc(&c.mlp_count, sizeof(int)) != cudaSuccess) return ICLS_E_NOMEM;
   if (cudaMalloc(&c.mlp_stats, 2 * sizeof(unsigned long long)) != cudaSuccess) return ICLS_E_NOMEM;
   cudaMemset(c.mlp_stats, 0, 2 * sizeof(unsigned long long));
   c.mlp_cap = cap;
-  return cudaFuncSetAttribute(k_mlp_infer_count, cudaFuncAttributeMaxDynamicSharedMemorySize, SB_INFER) ==
-                 cudaSuccess
+  return cudaFuncSetAttribute(k_mlp_curv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, SB_INFER) ==
+                     cudaSuccess &&
+                 cudaFuncSetAttribute(k_mlp_curv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, SB_INFER) ==
+                     cudaSuccess
              ? ICLS_OK
              : ICLS_E_CUDA;
 }
@@ -994,7 +1101,7 @@ extern "C" int icls_mlp_train(icls_mlp* m, int epochs, int batch, double lr, dou
 
 // y[0..n) = network(X[0..n)) on device arrays (X FP32 [n][32])
 extern "C" int icls_mlp_infer(icls_mlp* m, const void* X, float* y, long long n, void* stream) {
-  if (!m || !X || !y || n < 1) return ICLS_E_ARG;
+  if (!m || !X || !y || n < 1 || (reinterpret_cast<uintptr_t>(X) & 15)) return ICLS_E_ARG;
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : m->s;
   const long long tiles = (n + 127) / 128;
   const int grid = (int)std::min<long long>(tiles, 2 * 148);

@@ -368,6 +368,7 @@ class Mlp:
             "icls_mlp_train": [P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_ulonglong, C.POINTER(C.c_double)],
             "icls_mlp_eval": [P, C.POINTER(C.c_double)],
             "icls_mlp_params": [P, C.POINTER(C.c_float), C.c_int],
+            "icls_mlp_grad": [P, P, P, C.c_longlong, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_double)],
             "icls_set_curvature_net": [P, P],
             "icls_curvature_stats": [P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.c_int],
         }
@@ -408,6 +409,17 @@ class Mlp:
     def set_params(self, a):
         a = np.ascontiguousarray(a, dtype=np.float32)
         self._ok(self.lib.icls_mlp_params(self.h, a.ctypes.data_as(C.POINTER(C.c_float)), 0), "icls_mlp_params")
+
+    def grad(self, x_ptr: int, label_ptr: int, n: int, scale: float):
+        """gradient of the parameters for n FP32 samples [n][32] and labels
+        (device addresses; n a power of two, at least 128, one 128-sample
+        tile per block): dy = scale * (y - label) per sample; returns
+        (gradient [NPARAMS], sum of squared errors)"""
+        g = np.zeros(self.NPARAMS, dtype=np.float32)
+        loss = C.c_double()
+        self._ok(self.lib.icls_mlp_grad(self.h, x_ptr, label_ptr, n, scale, g.ctypes.data_as(C.POINTER(C.c_float)),
+                                        C.byref(loss)), "icls_mlp_grad")
+        return g, loss.value
 
     def attach(self, solver: "Solver"):
         """use this network for the solver's curvature (curvature_model MLP)"""

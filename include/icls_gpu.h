@@ -179,6 +179,8 @@ int icls_ls_mass_correction(icls_ctx* ctx, int istep, int l); /* levelset.f90:37
 int icls_ls_reinit_main(icls_ctx* ctx, int istep, int l);   /* levelset.f90:592-612 */
 int icls_update_materials(icls_ctx* ctx);                   /* misc.f90:79-290      */
 int icls_get_curvature(icls_ctx* ctx, int l);               /* interface.f90:20-119 -> CURV, NORMAL_M */
+/* (with curvature_model ICLS_CURV_MLP and a network attached, CURV near drop
+ * l's interface is the network's, with the per-cell fallback gfm4p uses) */
 /* Number of band cells of drop l after the last tube_construction
  * (nb_cnt, levelset.f90:158).                                           */
 int icls_band_count(icls_ctx* ctx, int l, long long* nb_cnt);
@@ -209,7 +211,8 @@ int icls_mlp_train(icls_mlp* m, int epochs, int batch, double lr, double lr_fina
 /* held-out statistics (kappa*dx): rms(mlp-label), rms(mlp-analytic), rms(plain-analytic),
  * rms(label-analytic), max|mlp-analytic|, max|plain-analytic|, rms|analytic|, samples */
 int icls_mlp_eval(icls_mlp* m, double stats[8]);
-/* y (device FP32 [n]) = network(X (device FP32 [n][32])); stream 0: synchronous */
+/* y (device FP32 [n]) = network(X (device FP32 [n][32], 16-byte aligned)); stream 0:
+ * synchronous */
 int icls_mlp_infer(icls_mlp* m, const void* X, float* y, long long n, void* stream);
 /* parameters to (get = 1) or from (get = 0) host float[ICLS_MLP_PARAMS] */
 int icls_mlp_params(icls_mlp* m, float* host, int get);

@@ -137,7 +137,18 @@ def _shell_error(solver, h, radius_cells):
     return float(np.sqrt(np.mean((solver.download("curv")[shell] + 2.0 / r[shell]) ** 2)) * h)
 
 
-def test_learned_curvature_in_the_loop(gpu_available):
+@pytest.fixture(scope="module")
+def trained_net(gpu_available):
+    """the network trained as in the training test, on 4M samples"""
+    from icls_gpu.binding import Mlp
+    net = Mlp(2024)
+    net.make_data(99, 1 << 22, 1 << 14)
+    net.train(epochs=20)
+    yield net
+    net.close()
+
+
+def test_learned_curvature_in_the_loop(trained_net):
     """Static drops of radius 5 and 16 cells: the curvature gfm4p uses at the
     interface, from the network (with per-cell fallback) and from the plain
     stencil, against the analytic -2/r (after re_curvature's smoothing, which
@@ -147,11 +158,9 @@ def test_learned_curvature_in_the_loop(gpu_available):
     (test above) does not carry over to a single sphere; then 20 steps run
     with the network in the loop."""
     from icls_gpu import CURV_MLP, Solver, init_drops, initial_velocity, static_drop
-    from icls_gpu.binding import Mlp, curvature_stats
+    from icls_gpu.binding import curvature_stats
     from icls_gpu.config import IclsConfig
-    net = Mlp(2024)
-    net.make_data(99, 1 << 22, 1 << 14)
-    net.train(epochs=20)
+    net = trained_net
     res = {}
     for rc in (5, 16):
         wl = static_drop(64, steps=20)
@@ -179,3 +188,36 @@ def test_learned_curvature_in_the_loop(gpu_available):
             assert np.isfinite(sm.max_vel_at_center())
     assert res[5][1] < 1.5 * res[5][0]
     assert res[16][1] < 0.01 * (2.0 / 16)
+
+
+def test_fp32_form_with_learned_curvature(trained_net):
+    """The combined form (FP32 bulk, FP64 Poisson/volume/jumps, network
+    curvature with per-cell fallback) on the 64^3 static drop of radius 16
+    cells for 20 steps, against the plain FP64 stencil run: drop volume
+    within 1e-6, interface curvature within 1% of kappa, velocities finite."""
+    from icls_gpu import CURV_MLP, FP32, Solver, init_drops, initial_velocity, static_drop
+    from icls_gpu.binding import curvature_stats
+    from icls_gpu.config import IclsConfig
+    wl = static_drop(64, steps=20)
+    cf = IclsConfig.from_buffer_copy(wl.cfg)
+    cf.precision = FP32
+    cf.curvature_model = CURV_MLP
+    ls = init_drops(wl.cfg, wl.centres, wl.radii, wl.all_images)
+    u, v, w = initial_velocity(wl.cfg, wl.shear_v)
+    sp, sf = Solver(wl.cfg), Solver(cf)
+    trained_net.attach(sf)
+    for s in (sp, sf):
+        s.setup(ls, u, v, w)
+        for istep in range(1, 21):
+            s.step(istep, 0)
+    h = 1.0 / 64
+    ep, ef = _shell_error(sp, h, 16), _shell_error(sf, h, 16)
+    vp, vf = sp.volumes()[0][0], sf.volumes()[0][0]
+    ev, fb = curvature_stats(sf)
+    print("\nFP32 + network, 20 steps: kappa*dx rms vs -2/r stencil(FP64) %.3e, form %.3e; volume rel diff %.2e; "
+          "spurious max|u| FP64 %.3e, form %.3e; fallback fraction %.3f"
+          % (ep, ef, abs(vf - vp) / vp, sp.max_vel_at_center(), sf.max_vel_at_center(), fb / max(ev, 1)))
+    assert ev > 0
+    assert np.isfinite(sf.max_vel_at_center())
+    assert abs(vf - vp) / vp <= 1e-6
+    assert ef < 0.01 * (2.0 / 16)
