@@ -52,6 +52,8 @@ def make_workload(name):
         return multi_drop(n=128, ndrop=12, seed=2024, rmin=0.06, rmax=0.12)
     if name == "static_drop_64":
         return static_drop(64)
+    if name == "static_drop_256":  # one drop: full-size field kernels with a few GB on the device
+        return static_drop(256)
     if name == "rising_bubble_128":
         return rising_bubble(128)
     raise SystemExit("unknown workload %s" % name)

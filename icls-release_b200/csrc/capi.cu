@@ -184,7 +184,7 @@ int allocate(Ctx& c) {
   AL(c.twx, (size_t)P.imax);
   AL(c.twy, (size_t)P.jmax);
   AL(c.xyrt, (size_t)P.imax * P.jmax);
-  AL(c.zpiv, (size_t)P.nI);
+  AL(c.zpiv, (size_t)(P.imax / 2 + 1) * (P.jmax / 2 + 1) * P.kmax);  // pivots per distinct (xrt, yrt)
   AL(c.tri_a, (size_t)P.kmax + 1); AL(c.tri_b, (size_t)P.kmax + 1); AL(c.tri_c, (size_t)P.kmax + 1);
   AL(c.partials, (size_t)kRedBlocks * std::max(P.L, 4) + (size_t)P.imax + 8);
   AL(c.lpartials, (size_t)kRedBlocks);

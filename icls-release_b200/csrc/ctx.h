@@ -109,8 +109,8 @@ struct Ctx {
   double* spec = nullptr;               // compact (1:imax,1:jmax,1:kmax) spectral buffer
   double2* twx = nullptr;               // e^{-2 pi i m/N}, m < N/2, x and y
   double2* twy = nullptr;
-  double* xyrt = nullptr;               // eigenvalues (initsolver.f90:76-82)
-  double* zpiv = nullptr;               // 1/pivot of the Thomas sweep per (i,j,k)
+  double* xyrt = nullptr;               // distinct eigenvalue sums (initsolver.f90:76-82)
+  double* zpiv = nullptr;               // 1/pivot of the Thomas sweep per distinct (xrt, yrt) and k
   double* tri_a = nullptr, *tri_b = nullptr, *tri_c = nullptr;  // (kmax)
   // reductions and device scalars
   double* partials = nullptr;           // kRedBlocks * max(L,4)

@@ -170,87 +170,124 @@ __device__ __forceinline__ T rhs_w(const Params& p, const FU& U, const FV& V, co
 }
 
 // ---- the ab2 update of one component (ab2.f90:51-61, 79-129) -------------
-// u0 = u at the cell, R = its mom_main RHS, rf = its face density; h the
-// offset of the + neighbour along the component's axis, dhi its 1/dx.  The
-// pressure-split term is formed in FP64 (the pressures are FP64 fields).
+// u0 = u at the cell, R = its mom_main RHS, rold the previous RHS, rf its
+// face density, dhi the 1/dx of the component's axis; the pressure-split
+// term is formed in FP64 (the pressures are FP64 fields) from: ph_p / ph_0 the
+// extrapolated pressures 2 pnew - pold at the + neighbour and the cell,
+// pjh the extrapolated pressure gradient 2 p_x - p_x,old
 template <typename T>
-__device__ __forceinline__ T ab2_update(const Params& p, const MomArgs& a, long long c, long long h, T u0, T R,
-                                        T rold, T rf, const double* pj, const double* pjold, double dhi) {
+__device__ __forceinline__ T ab2_update_v(const Params& p, T u0, T R, T rold, T rf, double ph_p, double ph_0,
+                                          double pjh, double dhi) {
   T d = u0 + TC(p.dt) * (TC(1.5) * R - TC(0.5) * rold);
-  const double ph_p = 2. * a.pnew[c + h] - a.pold[c + h];
-  const double ph_0 = 2. * a.pnew[c] - a.pold[c];
-  const double pjh = 2. * pj[c] - pjold[c];
   const double dn = -((1. / (double)rf - p.rrho0) * dhi * ((ph_p - pjh) - ph_0));
   return d + TC(p.dt * dn);
 }
 
-// ab2 over shape C with bounduvw(dudt,dvdt,dwdt) (bound.f90:36-75) in-kernel.
-// A block is a 32 x 8 column tile marching up a chunk of interior rows;
-// u, v, w and miu pass through a three-plane shared-memory ring (tile plus
-// one halo column each side), the rest is read once per cell.  A thread
-// writes its column's periodic halo images and, at k = 1 and k = kmax,
-// the wall rows k = 0 and k = k1.
-constexpr int MX = 32, MY = 8, MSX = MX + 2, MSY = MY + 2;
+// element copies global -> shared that complete asynchronously (waited for
+// with cp_async_wait_all before the block's barrier)
 template <typename T>
-__global__ void __launch_bounds__(MX * MY, 3) k_ab2(Params p, MomArgs a, T* __restrict__ dudt, T* __restrict__ dvdt,
-                                                    T* __restrict__ dwdt, T* __restrict__ duold_out,
-                                                    T* __restrict__ dvold_out, T* __restrict__ dwold_out, int kc,
-                                                    int nch) {
-  __shared__ T sm[4][3][MSY][MSX];
+__device__ __forceinline__ void cp_async_el(T* dst, const T* src) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  if (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// ab2 over shape C with bounduvw(dudt,dvdt,dwdt) (bound.f90:36-75) in-kernel.
+// A block is a 32 x 8 column tile marching up a chunk of interior rows.
+// u, v, w, miu (tile plus one halo column each side) and pnew, pold (tile
+// plus the + neighbours in x and y) pass through a four-plane shared-memory
+// ring filled by asynchronous copies: at row k the block issues row k+1's
+// planes and this cell's own operands together, then waits once, so one
+// memory latency is exposed per row and the ring needs one barrier per row
+// (the slot a row's copies fill is not one any thread can still be reading).
+// A thread writes its column's periodic halo images and, at k = 1 and
+// k = kmax, the wall rows k = 0 and k = k1.
+constexpr int MX = 32, MY = 8, MSX = MX + 2, MSY = MY + 2, MPX = MX + 1, MPY = MY + 1, MRING = 4;
+template <typename T>
+constexpr int ab2_smem() {
+  return (int)(4 * MRING * MSY * MSX * sizeof(T) + 2 * MRING * MPY * MPX * sizeof(double));
+}
+template <typename T>
+__global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 3))
+    k_ab2(Params p, MomArgs a, T* __restrict__ dudt, T* __restrict__ dvdt, T* __restrict__ dwdt,
+          T* __restrict__ duold_out, T* __restrict__ dvold_out, T* __restrict__ dwold_out, int kc, int nch) {
+  extern __shared__ __align__(16) unsigned char ab2_dyn[];
+  typedef T Plane[MSY][MSX];
+  typedef double PPlane[MPY][MPX];
+  Plane* ring = reinterpret_cast<Plane*>(ab2_dyn);  // [field * MRING + slot]
+  PPlane* pring = reinterpret_cast<PPlane*>(ab2_dyn + 4 * MRING * sizeof(Plane));
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + MX * ty;
   const int i0 = 1 + MX * (int)blockIdx.x, j0 = 1 + MY * (int)blockIdx.y;
   const int ch = blockIdx.z;
   const int ka = 1 + ch * kc, kb = (ch == nch - 1) ? p.kmax : ka + kc - 1;
   const int i = i0 + tx, j = j0 + ty;
   const bool ok = i <= p.imax && j <= p.jmax;
-  const T* __restrict__ F0 = cT<T>(a.u);
-  const T* __restrict__ F1 = cT<T>(a.v);
-  const T* __restrict__ F2 = cT<T>(a.w);
-  const T* __restrict__ F3 = cT<T>(a.miu);
+  const T* __restrict__ F[4] = {cT<T>(a.u), cT<T>(a.v), cT<T>(a.w), cT<T>(a.miu)};
   const T* __restrict__ rhu = cT<T>(a.rho_u);
   const T* __restrict__ rhv = cT<T>(a.rho_v);
   const T* __restrict__ rhw = cT<T>(a.rho_w);
   const T* __restrict__ hu = cT<T>(a.duold);
   const T* __restrict__ hv = cT<T>(a.dvold);
   const T* __restrict__ hw = cT<T>(a.dwold);
-  auto load_plane = [&](int kk) {
-    const int s = kk % 3;
+  auto issue_plane = [&](int kk) {
+    const int s = kk & (MRING - 1);
     for (int e = tid; e < MSX * MSY; e += MX * MY) {
       const int sy = e / MSX, sx = e - sy * MSX;
       const int gi = i0 - 1 + sx, gj = j0 - 1 + sy;
       if (gi <= p.imax + 1 && gj <= p.jmax + 1) {
         const long long g = idxC(p, gi, gj, kk);
-        sm[0][s][sy][sx] = F0[g];
-        sm[1][s][sy][sx] = F1[g];
-        sm[2][s][sy][sx] = F2[g];
-        sm[3][s][sy][sx] = F3[g];
+#pragma unroll
+        for (int f = 0; f < 4; ++f) cp_async_el(&ring[f * MRING + s][sy][sx], F[f] + g);
+      }
+    }
+    for (int e = tid; e < MPX * MPY; e += MX * MY) {
+      const int sy = e / MPX, sx = e - sy * MPX;
+      const int gi = i0 + sx, gj = j0 + sy;
+      if (gi <= p.imax + 1 && gj <= p.jmax + 1) {
+        const long long g = idxC(p, gi, gj, kk);
+        cp_async_el(&pring[s][sy][sx], a.pnew + g);
+        cp_async_el(&pring[MRING + s][sy][sx], a.pold + g);
       }
     }
   };
-  load_plane(ka - 1);
-  load_plane(ka);
+  issue_plane(ka - 1);
+  issue_plane(ka);
   const T rho_avr = TC(*a.rho_avr);
-  const long long sy = p.nCx, sz = (long long)p.nCx * p.nCy;
   T dw_km1 = TC(0.);
   for (int k = ka; k <= kb; ++k) {
-    load_plane(k + 1);
+    // this cell's own operands, in flight together with row k+1's planes
+    T ru = TC(1.), rv = TC(1.), rw = TC(1.), ou = TC(0.), ov = TC(0.), ow = TC(0.);
+    double qx = 0., qxo = 0., qy = 0., qyo = 0., qz = 0., qzo = 0.;
+    const long long c = idxC(p, i, j, k), q = idxI(p, i, j, k);
+    if (ok) {
+      ru = rhu[q]; rv = rhv[q]; rw = rhw[q];
+      ou = hu[q]; ov = hv[q]; ow = hw[q];
+      qx = a.px[c]; qxo = a.pxold[c]; qy = a.py[c]; qyo = a.pyold[c]; qz = a.pz[c]; qzo = a.pzold[c];
+    }
+    issue_plane(k + 1);
+    cp_async_wait_all();
     __syncthreads();
     if (ok) {
-      const int s_m = (k + 2) % 3, s_0 = k % 3, s_p = (k + 1) % 3;
+      const int s_m = (k - 1) & (MRING - 1), s_0 = k & (MRING - 1), s_p = (k + 1) & (MRING - 1);
       auto sl = [&](int dk) { return dk < 0 ? s_m : (dk > 0 ? s_p : s_0); };
-      auto U = [&](int di, int dj, int dk) { return sm[0][sl(dk)][ty + 1 + dj][tx + 1 + di]; };
-      auto V = [&](int di, int dj, int dk) { return sm[1][sl(dk)][ty + 1 + dj][tx + 1 + di]; };
-      auto W = [&](int di, int dj, int dk) { return sm[2][sl(dk)][ty + 1 + dj][tx + 1 + di]; };
-      auto M = [&](int di, int dj, int dk) { return sm[3][sl(dk)][ty + 1 + dj][tx + 1 + di]; };
-      const long long c = idxC(p, i, j, k), q = idxI(p, i, j, k);
-      const T ru = rhu[q], rv = rhv[q], rw = rhw[q];
+      auto U = [&](int di, int dj, int dk) { return ring[0 * MRING + sl(dk)][ty + 1 + dj][tx + 1 + di]; };
+      auto V = [&](int di, int dj, int dk) { return ring[1 * MRING + sl(dk)][ty + 1 + dj][tx + 1 + di]; };
+      auto W = [&](int di, int dj, int dk) { return ring[2 * MRING + sl(dk)][ty + 1 + dj][tx + 1 + di]; };
+      auto M = [&](int di, int dj, int dk) { return ring[3 * MRING + sl(dk)][ty + 1 + dj][tx + 1 + di]; };
+      auto PH = [&](int di, int dj, int dk) {
+        return 2. * pring[sl(dk)][ty + dj][tx + di] - pring[MRING + sl(dk)][ty + dj][tx + di];
+      };
+      const double ph0 = PH(0, 0, 0);
       const T Ru = rhs_u<T>(p, U, V, W, M, ru, rho_avr);
       const T Rv = rhs_v<T>(p, U, V, W, M, rv, rho_avr);
       const T Rw = rhs_w<T>(p, U, V, W, M, rw, rho_avr);
-      const T du = ab2_update(p, a, c, 1, U(0, 0, 0), Ru, hu[q], ru, a.px, a.pxold, p.dxi);
-      const T dv = ab2_update(p, a, c, sy, V(0, 0, 0), Rv, hv[q], rv, a.py, a.pyold, p.dyi) -
+      const T du = ab2_update_v(p, U(0, 0, 0), Ru, ou, ru, PH(1, 0, 0), ph0, 2. * qx - qxo, p.dxi);
+      const T dv = ab2_update_v(p, V(0, 0, 0), Rv, ov, rv, PH(0, 1, 0), ph0, 2. * qy - qyo, p.dyi) -
                    TC(p.forceytot * p.dt) / rv;
-      T dw = ab2_update(p, a, c, sz, W(0, 0, 0), Rw, hw[q], rw, a.pz, a.pzold, p.dzi);
+      T dw = ab2_update_v(p, W(0, 0, 0), Rw, ow, rw, PH(0, 0, 1), ph0, 2. * qz - qzo, p.dzi);
       duold_out[q] = Ru;
       dvold_out[q] = Rv;
       dwold_out[q] = Rw;
@@ -270,7 +307,6 @@ __global__ void __launch_bounds__(MX * MY, 3) k_ab2(Params p, MomArgs a, T* __re
         putC(p, dwdt, i, j, p.k1, dw_km1);
       }
     }
-    __syncthreads();
   }
 }
 
@@ -451,17 +487,17 @@ __global__ void __launch_bounds__(NT) k_average_vel(Params p, const T* __restric
 // ---- pressure update (main.f90:164-185) ----------------------------------
 // norm = sum(sum(pnew(:,:,1),2),1) in the Fortran order: for each i the
 // sum over j, then the sum of those over i.
-__global__ void k_plane_norm(Params p, const double* __restrict__ pp, double* __restrict__ colsum,
-                             DevScalars* __restrict__ dsc) {
-  for (int i = threadIdx.x; i <= p.i1; i += blockDim.x) {
-    double s = 0.;
-    for (int j = 0; j <= p.j1; ++j) s += pp[idxC(p, i, j, 1)];
-    colsum[i] = s;
-  }
-  __syncthreads();
+// the mean of p over the k = 1 plane, halo included (main.f90:173-175), by
+// one block: the plane's (i, j) cells in a fixed strided order per thread,
+// then a fixed tree
+constexpr int kNormThreads = 1024;
+__global__ void __launch_bounds__(kNormThreads) k_plane_norm(Params p, const double* __restrict__ pp,
+                                                             DevScalars* __restrict__ dsc) {
+  const long long n = (long long)p.nCx * p.nCy, base = idxC(p, 0, 0, 1);
+  double s = 0.;
+  for (long long e = threadIdx.x; e < n; e += kNormThreads) s += pp[base + e];
+  s = block_sum<double, kNormThreads>(s);
   if (threadIdx.x == 0) {
-    double s = 0.;
-    for (int i = 0; i <= p.i1; ++i) s += colsum[i];
     dsc->norm_old = dsc->norm;
     dsc->norm = s / (1. * (p.imax) * p.jmax);
   }
@@ -478,24 +514,33 @@ __global__ void __launch_bounds__(NT) k_pupdate(Params p, const double* __restri
 }
 
 // ---- reductions ------------------------------------------------------------
+// sum over the interior: block b takes rows (j, k) b, b + gridDim.x, ...,
+// its threads the i of each row (coalesced)
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_sum_interior(Params p, const T* __restrict__ a,
                                                               double* __restrict__ partial) {
-  double s = 0.;
-  for (int q = blockIdx.x * kRedThreads + threadIdx.x; q < (int)p.nI; q += gridDim.x * kRedThreads) {
-    int i, j, k;
-    decodeI(p, q, i, j, k);
-    s += (double)a[idxC(p, i, j, k)];
+  // four rows per pass with separate partial sums, so four loads are in flight
+  double s[4] = {0., 0., 0., 0.};
+  const int rows = p.jmax * p.kmax, G = gridDim.x;
+  for (int r = blockIdx.x; r < rows; r += 4 * G) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int ru = r + u * G;
+      if (ru < rows) {
+        const long long c = idxC(p, 1, 1 + ru % p.jmax, 1 + ru / p.jmax);
+        for (int i = threadIdx.x; i < p.imax; i += kRedThreads) s[u] += (double)a[c + i];
+      }
+    }
   }
-  double b = block_sum<double, kRedThreads>(s);
+  double b = block_sum<double, kRedThreads>((s[0] + s[1]) + (s[2] + s[3]));
   if (threadIdx.x == 0) partial[blockIdx.x] = b;
 }
-__global__ void k_stream_final(Params p, const double* __restrict__ partial, int nblk,
-                               DevScalars* __restrict__ dsc) {
-  if (threadIdx.x) return;
+__global__ void __launch_bounds__(kRedThreads) k_stream_final(Params p, const double* __restrict__ partial, int nblk,
+                                                              DevScalars* __restrict__ dsc) {
   double s = 0.;
-  for (int b = 0; b < nblk; ++b) s += partial[b];
-  dsc->v_bulk = s / (double)((long long)p.imax * p.jmax * p.kmax);
+  for (int b = threadIdx.x; b < nblk; b += kRedThreads) s += partial[b];
+  s = block_sum<double, kRedThreads>(s);
+  if (threadIdx.x == 0) dsc->v_bulk = s / (double)((long long)p.imax * p.jmax * p.kmax);
 }
 
 // chkdiv: sum of div and max|div| with its first column-major location
@@ -611,7 +656,14 @@ template <typename T>
 void ab2_launch(Ctx& c, const MomArgs& a, int o) {
   const int kc = 16, nch = std::max(1, c.P.kmax / kc);
   const dim3 grid((unsigned)((c.P.imax + MX - 1) / MX), (unsigned)((c.P.jmax + MY - 1) / MY), (unsigned)nch);
-  k_ab2<T><<<grid, dim3(MX, MY, 1), 0, c.s>>>(c.P, a, fp<T>(c.dudt), fp<T>(c.dvdt), fp<T>(c.dwdt),
+  static unsigned attr = 0;  // devices this instance's shared-memory limit is raised on
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(attr & (1u << (dev & 31)))) {
+    cudaFuncSetAttribute(k_ab2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ab2_smem<T>());
+    attr |= 1u << (dev & 31);
+  }
+  k_ab2<T><<<grid, dim3(MX, MY, 1), ab2_smem<T>(), c.s>>>(c.P, a, fp<T>(c.dudt), fp<T>(c.dvdt), fp<T>(c.dwdt),
                                                fp<T>(c.duold[o]), fp<T>(c.dvold[o]), fp<T>(c.dwold[o]),
                                                nch == 1 ? c.P.kmax : kc, nch);
 }
@@ -669,14 +721,14 @@ void launch_average_vel(Ctx& c) {
 }
 void launch_pressure_update(Ctx& c, int first) {
   Scope sc_(c.prof, c.s, "pressure_update", 2);
-  k_plane_norm<<<1, 512, 0, c.s>>>(c.P, c.p, c.partials, c.dsc);
+  k_plane_norm<<<1, kNormThreads, 0, c.s>>>(c.P, c.p, c.dsc);
   k_pupdate<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, c.pnew, c.pold, first, c.dsc);
 }
 void launch_stream_vel(Ctx& c) {
   Scope sc_(c.prof, c.s, "stream_vel", 2);
   if (c.P.f32) k_sum_interior<float><<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, fp<float>(c.v), c.partials);
   else k_sum_interior<double><<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, c.v, c.partials);
-  k_stream_final<<<1, 32, 0, c.s>>>(c.P, c.partials, kRedBlocks, c.dsc);
+  k_stream_final<<<1, kRedThreads, 0, c.s>>>(c.P, c.partials, kRedBlocks, c.dsc);
 }
 void launch_chkdiv(Ctx& c) {
   Scope sc_(c.prof, c.s, "chkdiv", 2);

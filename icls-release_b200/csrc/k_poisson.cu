@@ -12,8 +12,12 @@
 // x pass streams contiguous lines, the y pass loads 16-wide column tiles,
 // the z pass walks k with one thread per (i,j).
 //
-// Two real lines share one complex FFT (z = a + i b); the radix-2 passes
-// run in shared memory with one CTA per group of lines.
+// Two real lines share one complex FFT (z = a + i b).  Lines of 64, 128 or
+// 256 points take the two-level transform (k_fft2): N = R1 x R2 with
+// R1 = 16, a radix-16 DFT of every R2-strided subsequence in registers
+// (each thread has its 32 loads in flight), the N-point twiddles, one
+// padded shared-memory exchange, and a radix-R2 DFT in registers; other
+// lengths take radix-2 passes in shared memory (k_fft_x, k_fft_y).
 #include <cmath>
 #include <vector>
 
@@ -237,14 +241,213 @@ __global__ void __launch_bounds__(FT) k_fft_y(Params p, int dir, int TI, int log
   }
 }
 
+// ---- two-level transform for N = R1 x R2 -----------------------------------
+// The DFT of z[n], n = R2 n1 + n2, at k = k1 + R1 k2:
+//   Z[k] = sum_n2 W_N^(n2 k1) [sum_n1 z[R2 n1 + n2] W_R1^(n1 k1)] W_R2^(n2 k2),
+// W = e^{-2 pi i / N} (e^{+} for the inverse).  Register DFTs are radix-2
+// decimation in time with the bit reversal done by register renaming.
+constexpr int bitrev_c(int x, int bits) {
+  int r = 0;
+  for (int b = 0; b < bits; ++b) r |= ((x >> b) & 1) << (bits - 1 - b);
+  return r;
+}
+constexpr int ilog2_c(int n) { return n <= 1 ? 0 : 1 + ilog2_c(n >> 1); }
+
+// W_N^m from the half table tw[m] = W_N^m, m < N/2 (W_N^(m+N/2) = -W_N^m)
+__device__ __forceinline__ double2 twid_full(const double2* __restrict__ tw, int m, int N, int inv) {
+  double2 w = __ldg(&tw[m & (N / 2 - 1)]);
+  if (m & (N / 2)) w = make_double2(-w.x, -w.y);
+  if (inv) w.y = -w.y;
+  return w;
+}
+
+// in-register DFT of R points, natural order in and out; tw is the N-point
+// half table, W_R^m = W_N^(m N/R)
+template <int R>
+__device__ __forceinline__ void reg_dft(double2 (&x)[R], const double2* __restrict__ tw, int N, int inv) {
+  constexpr int LR = ilog2_c(R);
+  double2 y[R];
+#pragma unroll
+  for (int n = 0; n < R; ++n) y[bitrev_c(n, LR)] = x[n];
+#pragma unroll
+  for (int h = 1; h < R; h <<= 1) {
+#pragma unroll
+    for (int g = 0; g < R; g += 2 * h) {
+#pragma unroll
+      for (int j = 0; j < h; ++j) {
+        if (j == 0) {  // W^0 = 1: the product is exact, skip it
+          const double2 a = y[g], b = y[g + h];
+          y[g] = make_double2(a.x + b.x, a.y + b.y);
+          y[g + h] = make_double2(a.x - b.x, a.y - b.y);
+        } else {
+          bfly(y[g + j], y[g + j + h], twid(tw, j * (R / (2 * h)) * (N / R), inv));
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < R; ++n) x[n] = y[n];
+}
+
+// One CTA transforms LPC complex lines (2 LPC real lines).  YPASS false:
+// x lines (j,k), contiguous; the R lanes of a line are adjacent threads.
+// YPASS true: columns (i,k), columns adjacent in memory; the lines of a CTA
+// are adjacent threads.  dir 0: p (x) or spec (y) -> half-complex spec;
+// dir 1: the inverse, into spec (y) or p (x, with the boundp images when
+// halos is set).
+template <int R1, int R2, bool YPASS>
+__global__ void __launch_bounds__(256, 2) k_fft2(Params p, int dir, const double2* __restrict__ tw,
+                                                 double* __restrict__ pp, double* __restrict__ spec, int halos) {
+  constexpr int N = R1 * R2;
+  constexpr int TPL = R1 > R2 ? R1 : R2;  // threads per complex line
+  constexpr int LPC = 256 / TPL;          // complex lines per CTA
+  constexpr int SLD = R1 + 1;             // exchange row (padded)
+  constexpr int LS = R2 * SLD + 1;        // exchange line stride (padded)
+  constexpr int ZLD = N + 1;              // natural-order line stride
+  extern __shared__ double2 sm[];
+  const int lt = YPASS ? (int)threadIdx.x % LPC : (int)threadIdx.x / TPL;
+  const int lane = YPASS ? (int)threadIdx.x / LPC : (int)threadIdx.x % TPL;
+  const double s = sqrt(1.0 / N);
+  // the two real lines: element n of line a at A[n * st], of line b at B[n * st]
+  const double* A;
+  const double* B;
+  long long st;
+  bool live;
+  int ja = 0, ka = 0, jb = 0, kb = 0;  // x pass: the (j,k) of lines a and b
+  double* colbase = nullptr;            // y pass: the first column of the pair
+  if (!YPASS) {
+    const long long nlines = (long long)p.jmax * p.kmax;
+    const long long la = 2 * ((long long)blockIdx.x * LPC + lt), lb = la + 1;
+    live = lb < nlines;
+    ja = (int)(la % p.jmax) + 1; ka = (int)(la / p.jmax) + 1;
+    jb = (int)(lb % p.jmax) + 1; kb = (int)(lb / p.jmax) + 1;
+    st = 1;
+    if (dir == 0) {
+      A = pp + idxC(p, 1, ja, ka);
+      B = pp + idxC(p, 1, jb, kb);
+    } else {
+      A = spec + la * N;
+      B = spec + lb * N;
+    }
+  } else {
+    const int tiles_i = p.imax / (2 * LPC);
+    const int k = (int)blockIdx.x / tiles_i + 1;
+    const int i0 = ((int)blockIdx.x % tiles_i) * (2 * LPC) + 2 * lt;  // 0-based column
+    live = true;
+    colbase = spec + (long long)i0 + (long long)p.imax * p.jmax * (k - 1);
+    st = p.imax;
+    A = colbase;
+    B = colbase + 1;
+  }
+  double2* S = sm + lt * LS;
+  // step 1: lane n2 < R2 transforms z[R2 n1 + n2] over n1
+  if (lane < R2 && live) {
+    double2 x[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) {
+      const int n = R2 * n1 + lane;
+      x[n1] = dir == 0 ? make_double2(A[n * st], B[n * st]) : pack_hc(A, B, N, n, st);
+    }
+    reg_dft<R1>(x, tw, N, dir);
+#pragma unroll
+    for (int k1 = 1; k1 < R1; ++k1) {
+      if (lane == 0) continue;
+      const double2 w = twid_full(tw, lane * k1, N, dir);
+      const double2 v = x[k1];
+      x[k1] = make_double2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) S[lane * SLD + k1] = x[k1];
+  }
+  __syncthreads();
+  // step 2: lane k1 < R1 transforms over n2 -> Z[k1 + R1 k2]
+  double2 X[R2];
+  if (lane < R1 && live) {
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) X[n2] = S[n2 * SLD + lane];
+    reg_dft<R2>(X, tw, N, dir);
+  }
+  if (dir == 1) {
+    if (lane < R1 && live) {
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) {
+        const int n = lane + R1 * k2;
+        const double va = s * X[k2].x, vb = s * X[k2].y;
+        if (YPASS) {
+          colbase[(long long)n * st] = va;
+          colbase[(long long)n * st + 1] = vb;
+        } else {
+        for (int h = 0; h < 2; ++h) {
+          const int j = h ? jb : ja, k = h ? kb : ka;
+          const double v = h ? vb : va;
+          const int i = n + 1;
+          if (!halos) {
+            pp[idxC(p, i, j, k)] = v;
+            continue;
+          }
+          // boundp (bound.f90:182-287): every image of (i,j,k)
+          const int nj = (j == 1 || j == p.jmax) ? 2 : 1;
+          const int nk = (k == 1 || k == p.kmax) ? 2 : 1;
+          const int ni = (i == 1 || i == p.imax) ? 2 : 1;
+          for (int a = 0; a < ni; ++a) {
+            const int ii = a == 0 ? i : (i == 1 ? p.i1 : 0);
+            for (int b = 0; b < nj; ++b) {
+              const int jj = b == 0 ? j : (j == 1 ? p.j1 : 0);
+              for (int cidx = 0; cidx < nk; ++cidx) {
+                const int kk = cidx == 0 ? k : (k == 1 ? 0 : p.k1);
+                pp[idxC(p, ii, jj, kk)] = v;
+              }
+            }
+          }
+        }
+        }
+      }
+    }
+    return;
+  }
+  // forward: natural order through shared memory for the half-complex split
+  __syncthreads();  // every read of S is done
+  double2* Z = sm + lt * ZLD;
+  if (lane < R1 && live) {
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) Z[lane + R1 * k2] = X[k2];
+  }
+  __syncthreads();
+  if (!live) return;
+  for (int n = lane; n < N; n += TPL) {
+    double ha, hb;
+    unpack_hc(Z, N, n, s, ha, hb);
+    if (YPASS) {
+      colbase[(long long)n * st] = ha;
+      colbase[(long long)n * st + 1] = hb;
+    } else {
+      const long long la = 2 * ((long long)blockIdx.x * LPC + lt);
+      spec[la * N + n] = ha;
+      spec[(la + 1) * N + n] = hb;
+    }
+  }
+}
+template <int R1, int R2>
+constexpr size_t fft2_smem() {
+  constexpr int TPL = R1 > R2 ? R1 : R2, LPC = 256 / TPL;
+  constexpr int ex = LPC * (R2 * (R1 + 1) + 1), nat = LPC * (R1 * R2 + 1);
+  return (size_t)(ex > nat ? ex : nat) * sizeof(double2);
+}
+
 // ---- Thomas elimination in z (solver.f90:119-160) -------------------------
-// zpiv(i,j,k) = 1/(b(k)+xyrt - a(k) d(k-1)) for k<kmax (z of the reference)
-// and the raw last divisor at k=kmax.
+// zpiv(d,k) = 1/(b(k)+xy - a(k) d(k-1)) for k<kmax (z of the reference)
+// and the raw last divisor at k=kmax.  The pivots depend on (i,j) only
+// through xy = xrt(i) + yrt(j), and xrt(2m) = xrt(2m+1), yrt likewise, so
+// one column per distinct pair d = (i/2) + (imax/2+1) (j/2) serves every
+// (i,j) that shares it: (imax/2+1)(jmax/2+1) columns, L2-resident at 256^2.
+__host__ __device__ __forceinline__ long long pivot_columns(const Params& p) {
+  return (long long)(p.imax / 2 + 1) * (p.jmax / 2 + 1);
+}
 __global__ void k_thomas_setup(Params p, const double* __restrict__ xyrt, const double* __restrict__ a,
                                const double* __restrict__ b, const double* __restrict__ c,
                                double* __restrict__ zpiv) {
   const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long nxy = (long long)p.imax * p.jmax;
+  const long long nxy = pivot_columns(p);
   if (q >= nxy) return;
   const double xy = xyrt[q];
   double z = 1. / (b[1] + xy);
@@ -266,11 +469,12 @@ constexpr int TU = 8;
 __global__ void __launch_bounds__(128) k_thomas(Params p, const double* __restrict__ a, const double* __restrict__ c,
                                                 const double* __restrict__ zpiv, double* __restrict__ spec) {
   const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long nxy = (long long)p.imax * p.jmax;
+  const long long nxy = (long long)p.imax * p.jmax, nd = pivot_columns(p);
   if (q >= nxy) return;
   const int K = p.kmax;
+  const int i = (int)(q % p.imax) + 1, j = (int)(q / p.imax) + 1;
   double* __restrict__ col = spec + q;
-  const double* __restrict__ zc = zpiv + q;
+  const double* __restrict__ zc = zpiv + (i >> 1) + (long long)(p.imax / 2 + 1) * (j >> 1);
   double prev = col[0] * zc[0];
   col[0] = prev;
   for (int k0 = 2; k0 <= K - 1; k0 += TU) {
@@ -279,7 +483,7 @@ __global__ void __launch_bounds__(128) k_thomas(Params p, const double* __restri
     for (int u = 0; u < TU; ++u)
       if (k0 + u <= K - 1) {
         cv[u] = col[(k0 + u - 1) * nxy];
-        zv[u] = zc[(k0 + u - 1) * nxy];
+        zv[u] = zc[(k0 + u - 1) * nd];
       }
 #pragma unroll
     for (int u = 0; u < TU; ++u)
@@ -289,7 +493,7 @@ __global__ void __launch_bounds__(128) k_thomas(Params p, const double* __restri
         prev = v;
       }
   }
-  const double zz = zc[(K - 1) * nxy];
+  const double zz = zc[(K - 1) * nd];
   double nxt;
   if (zz != 0.) nxt = (col[(K - 1) * nxy] - a[K] * prev) / zz;
   else nxt = 0.;
@@ -300,7 +504,7 @@ __global__ void __launch_bounds__(128) k_thomas(Params p, const double* __restri
     for (int u = 0; u < TU; ++u)
       if (k0 - u >= 1) {
         cv[u] = col[(k0 - u - 1) * nxy];
-        zv[u] = zc[(k0 - u - 1) * nxy];
+        zv[u] = zc[(k0 - u - 1) * nd];
       }
 #pragma unroll
     for (int u = 0; u < TU; ++u)
@@ -353,9 +557,15 @@ void poisson_setup(Ctx& c) {
     yrt[j] = yrt[j - 1];
   }
   yrt[1] = 0.; yrt[jtot] = -4. * P.dyi * P.dyi;
-  std::vector<double> xy((size_t)itot * jtot);
-  for (int j = 1; j <= jtot; ++j)
-    for (int i = 1; i <= itot; ++i) xy[(i - 1) + (size_t)itot * (j - 1)] = xrt[i] + yrt[j];
+  // one entry per distinct (xrt, yrt) pair: column d = ix + (itot/2+1) iy
+  // stands for i = 1 (ix = 0) or i = 2 ix, j likewise
+  const int nxd = itot / 2 + 1, nyd = jtot / 2 + 1;
+  std::vector<double> xy((size_t)nxd * nyd);
+  for (int iy = 0; iy < nyd; ++iy)
+    for (int ix = 0; ix < nxd; ++ix) {
+      const int i = ix == 0 ? 1 : 2 * ix, j = iy == 0 ? 1 : 2 * iy;
+      xy[ix + (size_t)nxd * iy] = xrt[i] + yrt[j];
+    }
   cudaMemcpyAsync(c.xyrt, xy.data(), xy.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
   cudaMemcpyAsync(c.tri_a, a.data(), a.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
   cudaMemcpyAsync(c.tri_b, b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
@@ -365,8 +575,8 @@ void poisson_setup(Ctx& c) {
   make_twiddles(jtot, ty);
   cudaMemcpyAsync(c.twx, tx.data(), tx.size() * sizeof(double2), cudaMemcpyHostToDevice, c.s);
   cudaMemcpyAsync(c.twy, ty.data(), ty.size() * sizeof(double2), cudaMemcpyHostToDevice, c.s);
-  const long long nxy = (long long)itot * jtot;
-  k_thomas_setup<<<(unsigned)((nxy + 127) / 128), 128, 0, c.s>>>(P, c.xyrt, c.tri_a, c.tri_b, c.tri_c, c.zpiv);
+  const long long nd = pivot_columns(P);
+  k_thomas_setup<<<(unsigned)((nd + 127) / 128), 128, 0, c.s>>>(P, c.xyrt, c.tri_a, c.tri_b, c.tri_c, c.zpiv);
   cudaStreamSynchronize(c.s);  // host vectors above go out of scope
 }
 
@@ -382,6 +592,38 @@ static int y_tile(int imax) {
   return ti;
 }
 
+template <int R1, int R2, bool Y>
+void fft2_launch(Ctx& c, int dir, const double2* tw, int halos) {
+  const Params& P = c.P;
+  constexpr int TPL = R1 > R2 ? R1 : R2, LPC = 256 / TPL;
+  static unsigned attr = 0;  // devices this instance's shared-memory limit is raised on
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(attr & (1u << (dev & 31)))) {
+    cudaFuncSetAttribute(k_fft2<R1, R2, Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft2_smem<R1, R2>());
+    attr |= 1u << (dev & 31);
+  }
+  const long long units = Y ? (long long)(P.imax / (2 * LPC)) * P.kmax
+                            : ((long long)P.jmax * P.kmax + 2 * LPC - 1) / (2 * LPC);
+  k_fft2<R1, R2, Y><<<(unsigned)units, 256, fft2_smem<R1, R2>(), c.s>>>(P, dir, tw, c.p, c.spec, halos);
+}
+
+// the two-level transform of one pass if its length has one (and, for the
+// y pass, the columns tile the CTAs); false: the radix-2 kernels
+template <bool Y>
+bool fft2_pass(Ctx& c, int dir, int halos) {
+  const Params& P = c.P;
+  const int N = Y ? P.jmax : P.imax;
+  const double2* tw = Y ? c.twy : c.twx;
+  auto fits = [&](int lpc) { return !Y || P.imax % (2 * lpc) == 0; };
+  switch (N) {
+    case 64: if (!fits(16)) return false; fft2_launch<16, 4, Y>(c, dir, tw, halos); return true;
+    case 128: if (!fits(16)) return false; fft2_launch<16, 8, Y>(c, dir, tw, halos); return true;
+    case 256: if (!fits(16)) return false; fft2_launch<16, 16, Y>(c, dir, tw, halos); return true;
+    default: return false;
+  }
+}
+
 void launch_solver2d(Ctx& c, int write_halos) {
   Scope sc_(c.prof, c.s, "solver2d", 5);
   const Params& P = c.P;
@@ -393,18 +635,20 @@ void launch_solver2d(Ctx& c, int write_halos) {
   const int TI = y_tile(P.imax);
   const unsigned gy = (unsigned)((P.imax / TI) * P.kmax);
   const size_t smy = (size_t)2 * (TI / 2) * (P.jmax + 1) * sizeof(double2);
-  static bool attr_set = false;
-  if (!attr_set) {
+  static unsigned attr = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(attr & (1u << (dev & 31)))) {
     cudaFuncSetAttribute(k_fft_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
+    attr |= 1u << (dev & 31);
   }
-  k_fft_x<<<gx, FT, smx, c.s>>>(P, 0, CL, lx, c.twx, c.p, c.spec, 0);
-  k_fft_y<<<gy, FT, smy, c.s>>>(P, 0, TI, ly, c.twy, c.spec);
+  if (!fft2_pass<false>(c, 0, 0)) k_fft_x<<<gx, FT, smx, c.s>>>(P, 0, CL, lx, c.twx, c.p, c.spec, 0);
+  if (!fft2_pass<true>(c, 0, 0)) k_fft_y<<<gy, FT, smy, c.s>>>(P, 0, TI, ly, c.twy, c.spec);
   const long long nxy = (long long)P.imax * P.jmax;
   k_thomas<<<(unsigned)((nxy + 127) / 128), 128, 0, c.s>>>(P, c.tri_a, c.tri_c, c.zpiv, c.spec);
-  k_fft_y<<<gy, FT, smy, c.s>>>(P, 1, TI, ly, c.twy, c.spec);
-  k_fft_x<<<gx, FT, smx, c.s>>>(P, 1, CL, lx, c.twx, c.p, c.spec, write_halos);
+  if (!fft2_pass<true>(c, 1, 0)) k_fft_y<<<gy, FT, smy, c.s>>>(P, 1, TI, ly, c.twy, c.spec);
+  if (!fft2_pass<false>(c, 1, write_halos)) k_fft_x<<<gx, FT, smx, c.s>>>(P, 1, CL, lx, c.twx, c.p, c.spec, write_halos);
 }
 
 }  // namespace icls

@@ -190,6 +190,24 @@ def test_predictor_projection_chain():
     assert dg[1] < 1e-12 and do[1] < 1e-12
 
 
+@pytest.mark.parametrize("ni,nj,nk", [(16, 16, 8), (32, 64, 8), (64, 64, 12), (128, 64, 8), (64, 256, 6),
+                                      (256, 256, 8)])
+def test_solver2d_lengths(ni, nj, nk):
+    """solver2d on a random right-hand side at line lengths that take the
+    two-level transform (64, 128, 256) and the radix-2 passes (16, 32), x
+    and y: the interior against the oracle's FFT/Thomas solve."""
+    cfg = make_config(itot=ni, jtot=nj, ktot=nk, lmax=1, lx=ni / 64.0, ly=nj / 64.0, lz=nk / 64.0)
+    ls = init_drops(cfg, [(0.5 * cfg.lx, 0.5 * cfg.ly, 0.5 * cfg.lz)], [0.02])
+    rng = np.random.default_rng(ni + 7 * nj + 31 * nk)
+    p = np.asfortranarray(rng.standard_normal(field_shape(cfg, "p")))
+    g, o = paired(cfg, ls, p=p)
+    for s in (g, o):
+        s.upload("p", p)
+        s.solver2d()
+    pg, po = g.interior("p"), o.interior("p")
+    assert np.max(np.abs(pg - po)) <= 1e-11 * np.max(np.abs(po))
+
+
 def test_fused_step_equals_call_sequence():
     """icls_step (fused kernels) == the main.f90 sequence of separate calls."""
     cfg, ls = drop_case(L=2, reinit_step=2, inflate_step=2)
