@@ -98,9 +98,12 @@ ALG_VALUES = {
 # (layer 1 takes its 32 inputs as hi + lo pairs, K = 64)
 MLP_FLOPS_PER_CELL = 2 * (128 * 64 + 128 * 128 + 64 * 128)
 
-# DRAM bytes (read + write) of one scope of the dominant kernel, from an ncu
-# capture of the default workload: (kernel, FP32 form) -> bytes.
-TRAFFIC = {}
+# DRAM bytes (read + write) of one launch of the dominant kernel at 256^3,
+# (kernel, FP32 form) -> bytes: ncu's dram__bytes_read.sum + write.sum of
+# the launch on the 128^3 workload (profiles/k_ab2_*_multi_drop_128_12.md),
+# times the 8x cells (the traffic equals the algorithmic bytes there, so it
+# scales with the cells)
+TRAFFIC = {("ab2", False): 8 * (318.122240e6 + 86.022144e6), ("ab2", True): 8 * (229.303552e6 + 37.673984e6)}
 
 
 def alg_bytes_per_launch(name, cfg, stats, f32=False):

@@ -514,25 +514,35 @@ __global__ void __launch_bounds__(NT) k_pupdate(Params p, const double* __restri
 }
 
 // ---- reductions ------------------------------------------------------------
-// sum over the interior: block b takes rows (j, k) b, b + gridDim.x, ...,
-// its threads the i of each row (coalesced)
+// sum over the interior in 32-cell row chunks: warp w of the grid takes
+// chunks w, w + W, ... (W warps), eight at a time with every load issued
+// before the adds (fixed grid, fixed order)
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_sum_interior(Params p, const T* __restrict__ a,
                                                               double* __restrict__ partial) {
-  // four rows per pass with separate partial sums, so four loads are in flight
-  double s[4] = {0., 0., 0., 0.};
-  const int rows = p.jmax * p.kmax, G = gridDim.x;
-  for (int r = blockIdx.x; r < rows; r += 4 * G) {
+  const int cpr = (p.imax + 31) / 32;
+  const long long rows = (long long)p.jmax * p.kmax, nchunks = rows * cpr;
+  const long long nw = ((long long)gridDim.x * kRedThreads) >> 5;
+  const long long wid = ((long long)blockIdx.x * kRedThreads + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  double acc[8] = {0., 0., 0., 0., 0., 0., 0., 0.};
+  for (long long base = wid; base < nchunks; base += 8 * nw) {
+    double v[8];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int ru = r + u * G;
-      if (ru < rows) {
-        const long long c = idxC(p, 1, 1 + ru % p.jmax, 1 + ru / p.jmax);
-        for (int i = threadIdx.x; i < p.imax; i += kRedThreads) s[u] += (double)a[c + i];
+    for (int u = 0; u < 8; ++u) {
+      v[u] = 0.;
+      const long long ch = base + u * nw;
+      if (ch < nchunks) {
+        const long long row = ch / cpr;
+        const int off = (int)(ch - row * cpr) * 32 + lane;
+        if (off < p.imax) v[u] = (double)a[idxC(p, 1 + off, 1 + (int)(row % p.jmax), 1 + (int)(row / p.jmax))];
       }
     }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc[u] += v[u];
   }
-  double b = block_sum<double, kRedThreads>((s[0] + s[1]) + (s[2] + s[3]));
+  const double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+  double b = block_sum<double, kRedThreads>(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = b;
 }
 __global__ void __launch_bounds__(kRedThreads) k_stream_final(Params p, const double* __restrict__ partial, int nblk,
