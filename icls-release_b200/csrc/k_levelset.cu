@@ -284,6 +284,20 @@ __device__ __forceinline__ T reinit_rhs(const Params& p, const T* __restrict__ p
   if (!(fabs(phi[c]) < TC(p.NB + p.dz))) return TC(0.);
   const long long sx = 1, sy = p.nLx, sz = (long long)p.nLx * p.nLy;
 #define PH(o) phi[c + (o)]
+  // A uniform neighbourhood (most of a drop's region is clipped far field):
+  // every difference below is exactly +0, so every WENO5 derivative, the
+  // Godunov choices and the gradient norm are exactly 0 and the right-hand
+  // side is sgn * (1 - sqrt(0)) = sgn, bit for bit.  The test reads the
+  // three axial neighbours each way (a superset of what the wall rows use).
+  {
+    const T c0 = PH(0);
+    bool uni = true;
+#pragma unroll
+    for (int d = 1; d <= 3; ++d)
+      uni = uni & (PH(d * sx) == c0) & (PH(-d * sx) == c0) & (PH(d * sy) == c0) & (PH(-d * sy) == c0) &
+            (PH(d * sz) == c0) & (PH(-d * sz) == c0);
+    if (uni) return reinit_sgn(p, orig[c]);
+  }
   T A = TC(0.), B = TC(0.), C, D, E, F;
   if (!p.TwoD) {
     A = weno5(divx(p, PH(-2 * sx) - PH(-3 * sx)), divx(p, PH(-sx) - PH(-2 * sx)), divx(p, PH(0) - PH(-sx)),

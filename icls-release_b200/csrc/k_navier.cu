@@ -514,32 +514,25 @@ __global__ void __launch_bounds__(NT) k_pupdate(Params p, const double* __restri
 }
 
 // ---- reductions ------------------------------------------------------------
-// sum over the interior in 32-cell row chunks: warp w of the grid takes
-// chunks w, w + W, ... (W warps), eight at a time with every load issued
+// sum over the interior: warp w of the grid takes rows (j,k) w, w + W, ...
+// (W warps), its lanes the i of a row, eight loads in flight per lane
 // before the adds (fixed grid, fixed order)
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_sum_interior(Params p, const T* __restrict__ a,
                                                               double* __restrict__ partial) {
-  const int cpr = (p.imax + 31) / 32;
-  const long long rows = (long long)p.jmax * p.kmax, nchunks = rows * cpr;
-  const long long nw = ((long long)gridDim.x * kRedThreads) >> 5;
-  const long long wid = ((long long)blockIdx.x * kRedThreads + threadIdx.x) >> 5;
+  const int rows = p.jmax * p.kmax;
+  const int W = (int)((gridDim.x * kRedThreads) >> 5);
   const int lane = threadIdx.x & 31;
   double acc[8] = {0., 0., 0., 0., 0., 0., 0., 0.};
-  for (long long base = wid; base < nchunks; base += 8 * nw) {
-    double v[8];
+  for (int r = (int)((blockIdx.x * kRedThreads + threadIdx.x) >> 5); r < rows; r += W) {
+    const T* __restrict__ row = a + idxC(p, 1, 1 + r % p.jmax, 1 + r / p.jmax);
+    for (int i0 = lane; i0 < p.imax; i0 += 256) {
+      double v[8];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      v[u] = 0.;
-      const long long ch = base + u * nw;
-      if (ch < nchunks) {
-        const long long row = ch / cpr;
-        const int off = (int)(ch - row * cpr) * 32 + lane;
-        if (off < p.imax) v[u] = (double)a[idxC(p, 1 + off, 1 + (int)(row % p.jmax), 1 + (int)(row / p.jmax))];
-      }
+      for (int u = 0; u < 8; ++u) v[u] = (i0 + 32 * u < p.imax) ? (double)row[i0 + 32 * u] : 0.;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc[u] += v[u];
     }
-#pragma unroll
-    for (int u = 0; u < 8; ++u) acc[u] += v[u];
   }
   const double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
   double b = block_sum<double, kRedThreads>(s);
