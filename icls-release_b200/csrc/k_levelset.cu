@@ -78,33 +78,49 @@ __global__ void __launch_bounds__(NT) k_tube(Params p, const __grid_constant__ L
   int band = 0;
   int lo[5] = {INT_MAX, INT_MAX, INT_MAX, INT_MAX, INT_MAX};
   int hi[5] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN};
-  auto rd = [&](int a, int b, int k) -> T {
-    return in_written(p, t.vin, a, b, k) ? in[idxL(p, a, b, k)] : ((k < 0 || k > p.k1) ? bggin : bgin);
-  };
   if (c.ok) {
     const int i = c.i, j = c.j;
     const int hx = p.imax / 2, hy = p.jmax / 2;
     const int ib = i + hx > p.imax ? i + hx - p.imax : i + hx;
     const int jb = j + hy > p.jmax ? j + hy - p.jmax : j + hy;
+    // whether the input region holds columns i+d (x) and j+d (y), d = -2..2:
+    // the in-region test of every read, hoisted out of the row loop
+    bool inx[5], iny[5];
+#pragma unroll
+    for (int d = -2; d <= 2; ++d) {
+      inx[d + 2] = span_has(t.vin.xa, t.vin.xn, p.imax, wrapx(p, i + d));
+      iny[d + 2] = span_has(t.vin.ya, t.vin.yn, p.jmax, wrapy(p, j + d));
+    }
+    const bool colin = inx[2] && iny[2];
+    const long long sy = p.nLx, sz = (long long)p.nLx * p.nLy;
+    // phi at storage index `at` (row k, a column the input region holds if
+    // `held`), the input's far-field value where the region does not hold it
+    auto rdo = [&](long long at, bool held, int k) -> T {
+      return (held && k >= t.vin.z0 && k <= t.vin.z1) ? in[at] : ((k < 0 || k > p.k1) ? bggin : bgin);
+    };
     for (int k = c.ka; k <= c.kb; ++k) {
       T val;
+      const long long c0 = idxL(p, i, j, k);
       if (!computed(c, t.r, k)) {
         val = clipNB((k < 0 || k > p.k1) ? bggin : bgin, NB);
       } else {
         if (k == 0)
-          val = TC(2.) * clipNB(rd(i, j, 1), NB) - clipNB(rd(i, j, 2), NB);
+          val = TC(2.) * clipNB(rdo(c0 + sz, colin, 1), NB) - clipNB(rdo(c0 + 2 * sz, colin, 2), NB);
         else if (k == p.k1)
-          val = TC(2.) * clipNB(rd(i, j, p.kmax), NB) - clipNB(rd(i, j, p.kmax - 1), NB);
+          val = TC(2.) * clipNB(rdo(c0 - sz, colin, p.kmax), NB) - clipNB(rdo(c0 - 2 * sz, colin, p.kmax - 1), NB);
         else
-          val = clipNB(rd(i, j, k), NB);
+          val = clipNB(rdo(c0, colin, k), NB);
         if (k >= 1 && k <= p.kmax) {
           int m = 0;
           if (fabs(val) < NB) {
             m = 1;
           } else {
-            for (int d = -2; d <= 2 && !m; ++d) m = fabs(clipNB(rd(i + d, j, k), NB)) != NB;
-            for (int d = -2; d <= 2 && !m; ++d) m = fabs(clipNB(rd(i, j + d, k), NB)) != NB;
-            for (int d = -2; d <= 2 && !m; ++d) m = fabs(clipNB(rd(i, j, k + d), NB)) != NB;
+            for (int d = -2; d <= 2 && !m; ++d)
+              m = fabs(clipNB(rdo(c0 + d, inx[d + 2] && iny[2], k), NB)) != NB;
+            for (int d = -2; d <= 2 && !m; ++d)
+              m = fabs(clipNB(rdo(c0 + d * sy, inx[2] && iny[d + 2], k), NB)) != NB;
+            for (int d = -2; d <= 2 && !m; ++d)
+              m = fabs(clipNB(rdo(c0 + d * sz, colin, k + d), NB)) != NB;
           }
           t.mask[idxI(p, i, j, k)] = (uint8_t)m;
           band += m;
@@ -464,7 +480,16 @@ __device__ __forceinline__ T dirac_trig(const Params& p, T phi, T eps) {
 // far-field value of H, so only cells with H < 1 are touched; min is
 // order-free, so drops may share cells.  One chunk per tile:
 // part[l*cap + tile] is deterministic.
+// For v >= +0 the signed-integer order of the bit patterns is the numeric
+// order against every non-negative value, and every negative value (sign
+// bit set) compares below it, as it does numerically: one atomicMin that
+// returns nothing (the thread does not wait for it).  A negative v (H is
+// negative only by rounding, ~1e-17) takes the compare-and-swap loop.
 __device__ __forceinline__ void min_into(double* a, double v) {
+  if (!(v < 0.)) {
+    atomicMin(reinterpret_cast<long long*>(a), __double_as_longlong(v));
+    return;
+  }
   unsigned long long* q = reinterpret_cast<unsigned long long*>(a);
   unsigned long long old = *q;
   while (v < __longlong_as_double((long long)old)) {
@@ -474,6 +499,10 @@ __device__ __forceinline__ void min_into(double* a, double v) {
   }
 }
 __device__ __forceinline__ void min_into(float* a, float v) {
+  if (!(v < 0.f)) {
+    atomicMin(reinterpret_cast<int*>(a), __float_as_int(v));
+    return;
+  }
   unsigned int* q = reinterpret_cast<unsigned int*>(a);
   unsigned int old = *q;
   while (v < __uint_as_float(old)) {
