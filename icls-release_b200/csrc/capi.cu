@@ -749,11 +749,11 @@ void fix_curv(Ctx& c) {
   const bool mlp = c.cfg.curvature_model == ICLS_CURV_MLP && c.net;
   if (c.cfg.TwoD) {
     t.out = c.curv;
-    launch_curvature(c, b[0], c.nrm_m);
+    launch_curvature(c, b[0], c.nrm_m, mlp);
     if (mlp) launch_mlp_curvature(c, b[0]);
   } else {
     t.out = member(c, l).fit;
-    launch_curvature(c, b[0], c.nrm_m);
+    launch_curvature(c, b[0], c.nrm_m, mlp);
     if (mlp) launch_mlp_curvature(c, b[0]);
     t.phis = member(c, l).fit;
     t.out = c.curv;
@@ -786,8 +786,9 @@ int gfm4p(Ctx& c) {
         t.phi0 = c.lv[t.l];
         t.out = c.cfg.TwoD ? member(c, t.l).cv : member(c, t.l).fit;
       }
-      launch_curvature(c, b, nullptr);
-      if (c.cfg.curvature_model == ICLS_CURV_MLP) launch_mlp_curvature(c, b);
+      const bool mlp = c.cfg.curvature_model == ICLS_CURV_MLP;
+      launch_curvature(c, b, nullptr, mlp);
+      if (mlp) launch_mlp_curvature(c, b);
     }
     if (!c.cfg.TwoD)
       for (LsBatch& b : b1) {
@@ -1319,9 +1320,10 @@ int icls_get_curvature(icls_ctx* h, int l) {
   std::vector<LsBatch> b = single(c, l - 1, kStageRows, c_region(c.P, c.win[l - 1].box, 1));
   b[0].t[0].phi0 = c.lv[l - 1];
   b[0].t[0].out = c.curv;
-  launch_curvature(c, b[0], c.nrm_m);
   // the learned form: the network's curvature near the interface, as gfm4p uses it
-  if (c.cfg.curvature_model == ICLS_CURV_MLP && c.net) {
+  const bool mlp = c.cfg.curvature_model == ICLS_CURV_MLP && c.net;
+  launch_curvature(c, b[0], c.nrm_m, mlp);
+  if (mlp) {
     const int rc = launch_mlp_curvature(c, b[0]);
     if (rc) return rc;
   }

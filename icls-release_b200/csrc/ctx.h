@@ -189,7 +189,14 @@ void launch_to_double(Ctx& c, double* dst, const double* src_f32, long long n);
 
 // interface / GFM (k_gfm.cu); the tasks carry shape-C regions
 // curvature: phi0 -> out (+ normal%m); recurvature: phis -> out; jumps: phi0, phis
-void launch_curvature(Ctx& c, const LsBatch& b, double* nrm_m_out);
+// A near-interface cell recorded for the learned curvature: task q of the
+// batch, interior cell (i, j, k)
+struct MlpCell {
+  int q, i, j, k;
+};
+// get_curvature over the batch; with collect, also records the computed
+// cells with |phi| <= 4dz for the network (count reset here)
+void launch_curvature(Ctx& c, const LsBatch& b, double* nrm_m_out, bool collect = false);
 void launch_recurvature(Ctx& c, const LsBatch& b);
 void launch_jumps(Ctx& c, const LsBatch& b);
 void launch_ipot(Ctx& c, double* dmin_dev);

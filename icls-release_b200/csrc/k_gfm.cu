@@ -85,21 +85,38 @@ __device__ __forceinline__ T curvature_at(const Params& p, const T* __restrict__
 // periodic copies (bound.f90:292-305), the apron (far field, |phi| > 5dz)
 // is 0.
 template <typename T>
-__global__ void __launch_bounds__(NT) k_curvature(Params p, const __grid_constant__ LsBatch B, T* __restrict__ nrm_m) {
+__global__ void __launch_bounds__(NT) k_curvature(Params p, const __grid_constant__ LsBatch B, T* __restrict__ nrm_m,
+                                                  MlpCell* __restrict__ rec, int* __restrict__ count, int cap) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
-  if (!c.ok) return;
   const T* phi = cT<T>(t.phi0);
   T* out = mT<T>(t.out);
+  const T lim = TC(4. * p.dz);
+  const unsigned lane = threadIdx.x & 31u;
+  // every lane of the warp walks the same rows, so the ballots line up
   for (int k = c.ka; k <= c.kb; ++k) {
-    T v = TC(0.);
-    if (k != 0 && k != p.k1 && computed(c, t.r, k)) {
-      T m;
-      v = curvature_at(p, phi, c.i, c.j, k, m);
-      if (nrm_m) nrm_m[idxI(p, c.i, c.j, k)] = m;
+    if (c.ok) {
+      T v = TC(0.);
+      if (k != 0 && k != p.k1 && computed(c, t.r, k)) {
+        T m;
+        v = curvature_at(p, phi, c.i, c.j, k, m);
+        if (nrm_m) nrm_m[idxI(p, c.i, c.j, k)] = m;
+      }
+      putC(p, out, c.i, c.j, k, v);
     }
-    putC(p, out, c.i, c.j, k, v);
+    if (rec) {  // the network's cells: slots by a warp-aggregated counter
+      const bool take = c.ok && k >= 1 && k <= p.kmax && computed(c, t.r, k) &&
+                        fabs(phi[idxL(p, c.i, c.j, k)]) <= lim;
+      const unsigned msk = __ballot_sync(0xffffffffu, take);
+      if (msk) {
+        int base = 0;
+        if (lane == (unsigned)(__ffs(msk) - 1)) base = atomicAdd(count, __popc(msk));
+        base = __shfl_sync(0xffffffffu, base, __ffs(msk) - 1);
+        const int slot = base + __popc(msk & ((1u << lane) - 1u));
+        if (take && slot < cap) rec[slot] = MlpCell{ti, c.i, c.j, k};
+      }
+    }
   }
 }
 
@@ -270,13 +287,16 @@ void set_pseudo_inverse(const double* P270, cudaStream_t s) {
 
 const dim3 kTile(TBX, TBY, 1);
 
-void launch_curvature(Ctx& c, const LsBatch& b, double* nrm_m_out) {
+void launch_curvature(Ctx& c, const LsBatch& b, double* nrm_m_out, bool collect) {
   if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "curvature", 1);
+  MlpCell* rec = collect ? reinterpret_cast<MlpCell*>(c.mlp_rec) : nullptr;
+  if (collect) cudaMemsetAsync(c.mlp_count, 0, sizeof(int), c.s);
   if (c.P.f32)
-    k_curvature<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, reinterpret_cast<float*>(nrm_m_out));
+    k_curvature<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, reinterpret_cast<float*>(nrm_m_out), rec, c.mlp_count,
+                                                        c.mlp_cap);
   else
-    k_curvature<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, nrm_m_out);
+    k_curvature<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, nrm_m_out, rec, c.mlp_count, c.mlp_cap);
 }
 void launch_recurvature(Ctx& c, const LsBatch& b) {
   if (b.n == 0) return;

@@ -152,99 +152,124 @@ __global__ void __launch_bounds__(NT) k_tube(Params p, const __grid_constant__ L
 }
 
 // ------------------------------------------------------- advection RHS
-// dfdt of HOUC5_nb (hyperPDE.f90:397-495) or WENO5_nb (503-800) at (i,j,k)
+// The 19 values of the axial stencil at storage index c (the centre and
+// offsets -3..3 along each axis), read before anything is decided so that
+// they are in flight together with the row's other operands.
+template <typename T>
+struct Axial19 {
+  T c, x[7], y[7], z[7];  // x[d + 3] = phi at offset d along x (x[3] == c), likewise y, z
+};
+template <typename T>
+__device__ __forceinline__ Axial19<T> read_axial(const T* __restrict__ phi, long long c, long long sy, long long sz) {
+  Axial19<T> a;
+  a.c = phi[c];
+#pragma unroll
+  for (int d = -3; d <= 3; ++d) {
+    if (d == 0) continue;
+    a.x[d + 3] = phi[c + d];
+    a.y[d + 3] = phi[c + d * sy];
+    a.z[d + 3] = phi[c + d * sz];
+  }
+  a.x[3] = a.y[3] = a.z[3] = a.c;
+  return a;
+}
+
+// dfdt of HOUC5_nb (hyperPDE.f90:397-495) or WENO5_nb (503-800) at row k
+// from its axial stencil S
 template <int SCHEME, typename T>
-__device__ __forceinline__ T adv_rhs(const Params& p, const T* __restrict__ phi, T vu, T vv, T vw, int i, int j,
-                                     int k) {
-  const long long c = idxL(p, i, j, k);
-  const long long sx = 1, sy = p.nLx, sz = (long long)p.nLx * p.nLy;
-#define PH(o) phi[c + (o)]
+__device__ __forceinline__ T adv_rhs(const Params& p, const Axial19<T>& S, T vu, T vv, T vw, int k) {
+#define PX(d) S.x[(d) + 3]
+#define PY(d) S.y[(d) + 3]
+#define PZ(d) S.z[(d) + 3]
   T udfdx, vdfdy, wdfdz, dfx, dfy, dfz;
   if (SCHEME == ICLS_HOUC5) {
     if (p.TwoD) {
       udfdx = TC(0.);
     } else {
       if (vu >= TC(0.))
-        dfx = houc5_pos(PH(-3 * sx), PH(-2 * sx), PH(-sx), PH(0), PH(sx), PH(2 * sx));
+        dfx = houc5_pos(PX(-3), PX(-2), PX(-1), PX(0), PX(1), PX(2));
       else
-        dfx = houc5_neg(PH(3 * sx), PH(2 * sx), PH(sx), PH(0), PH(-sx), PH(-2 * sx));
+        dfx = houc5_neg(PX(3), PX(2), PX(1), PX(0), PX(-1), PX(-2));
       udfdx = -divx(p, vu * dfx);
     }
     if (vv >= TC(0.))
-      dfy = houc5_pos(PH(-3 * sy), PH(-2 * sy), PH(-sy), PH(0), PH(sy), PH(2 * sy));
+      dfy = houc5_pos(PY(-3), PY(-2), PY(-1), PY(0), PY(1), PY(2));
     else
-      dfy = houc5_neg(PH(3 * sy), PH(2 * sy), PH(sy), PH(0), PH(-sy), PH(-2 * sy));
+      dfy = houc5_neg(PY(3), PY(2), PY(1), PY(0), PY(-1), PY(-2));
     vdfdy = -divy(p, vv * dfy);
   } else {
     if (p.TwoD) {
       udfdx = TC(0.);
     } else {
       if (vu >= TC(0.))
-        dfx = weno5(divx(p, PH(-2 * sx) - PH(-3 * sx)), divx(p, PH(-sx) - PH(-2 * sx)), divx(p, PH(0) - PH(-sx)),
-                    divx(p, PH(sx) - PH(0)), divx(p, PH(2 * sx) - PH(sx)));
+        dfx = weno5(divx(p, PX(-2) - PX(-3)), divx(p, PX(-1) - PX(-2)), divx(p, PX(0) - PX(-1)),
+                    divx(p, PX(1) - PX(0)), divx(p, PX(2) - PX(1)));
       else
-        dfx = weno5(divx(p, PH(3 * sx) - PH(2 * sx)), divx(p, PH(2 * sx) - PH(sx)), divx(p, PH(sx) - PH(0)),
-                    divx(p, PH(0) - PH(-sx)), divx(p, PH(-sx) - PH(-2 * sx)));
+        dfx = weno5(divx(p, PX(3) - PX(2)), divx(p, PX(2) - PX(1)), divx(p, PX(1) - PX(0)),
+                    divx(p, PX(0) - PX(-1)), divx(p, PX(-1) - PX(-2)));
       udfdx = -(vu * dfx);
     }
     // y uses dx, as in the reference (hyperPDE.f90:622-626)
     if (vv >= TC(0.))
-      dfy = weno5(divx(p, PH(-2 * sy) - PH(-3 * sy)), divx(p, PH(-sy) - PH(-2 * sy)), divx(p, PH(0) - PH(-sy)),
-                  divx(p, PH(sy) - PH(0)), divx(p, PH(2 * sy) - PH(sy)));
+      dfy = weno5(divx(p, PY(-2) - PY(-3)), divx(p, PY(-1) - PY(-2)), divx(p, PY(0) - PY(-1)),
+                  divx(p, PY(1) - PY(0)), divx(p, PY(2) - PY(1)));
     else
-      dfy = weno5(divx(p, PH(3 * sy) - PH(2 * sy)), divx(p, PH(2 * sy) - PH(sy)), divx(p, PH(sy) - PH(0)),
-                  divx(p, PH(0) - PH(-sy)), divx(p, PH(-sy) - PH(-2 * sy)));
+      dfy = weno5(divx(p, PY(3) - PY(2)), divx(p, PY(2) - PY(1)), divx(p, PY(1) - PY(0)),
+                  divx(p, PY(0) - PY(-1)), divx(p, PY(-1) - PY(-2)));
     vdfdy = -(vv * dfy);
   }
   if (k > 2 && k < p.kmax - 1) {
     if (SCHEME == ICLS_HOUC5) {
       if (vw >= TC(0.))
-        dfz = houc5_pos(PH(-3 * sz), PH(-2 * sz), PH(-sz), PH(0), PH(sz), PH(2 * sz));
+        dfz = houc5_pos(PZ(-3), PZ(-2), PZ(-1), PZ(0), PZ(1), PZ(2));
       else
-        dfz = houc5_neg(PH(3 * sz), PH(2 * sz), PH(sz), PH(0), PH(-sz), PH(-2 * sz));
+        dfz = houc5_neg(PZ(3), PZ(2), PZ(1), PZ(0), PZ(-1), PZ(-2));
       wdfdz = -divz(p, vw * dfz);
     } else {
       if (vw >= TC(0.))
-        dfz = weno5(divz(p, PH(-2 * sz) - PH(-3 * sz)), divz(p, PH(-sz) - PH(-2 * sz)), divz(p, PH(0) - PH(-sz)),
-                    divz(p, PH(sz) - PH(0)), divz(p, PH(2 * sz) - PH(sz)));
+        dfz = weno5(divz(p, PZ(-2) - PZ(-3)), divz(p, PZ(-1) - PZ(-2)), divz(p, PZ(0) - PZ(-1)),
+                    divz(p, PZ(1) - PZ(0)), divz(p, PZ(2) - PZ(1)));
       else
-        dfz = weno5(divz(p, PH(3 * sz) - PH(2 * sz)), divz(p, PH(2 * sz) - PH(sz)), divz(p, PH(sz) - PH(0)),
-                    divz(p, PH(0) - PH(-sz)), divz(p, PH(-sz) - PH(-2 * sz)));
+        dfz = weno5(divz(p, PZ(3) - PZ(2)), divz(p, PZ(2) - PZ(1)), divz(p, PZ(1) - PZ(0)),
+                    divz(p, PZ(0) - PZ(-1)), divz(p, PZ(-1) - PZ(-2)));
       wdfdz = -(vw * dfz);
     }
   } else if (k == 2 || k == p.kmax - 1) {  // HOUC3 near the walls
     if (vw >= TC(0.))
-      dfz = ((TC(1. / 6.) * PH(-2 * sz) - PH(-sz)) + TC(1. / 2.) * PH(0)) + TC(1. / 3.) * PH(sz);
+      dfz = ((TC(1. / 6.) * PZ(-2) - PZ(-1)) + TC(1. / 2.) * PZ(0)) + TC(1. / 3.) * PZ(1);
     else
-      dfz = ((-(TC(1. / 6.) * PH(2 * sz)) + PH(sz)) - TC(1. / 2.) * PH(0)) - TC(1. / 3.) * PH(-sz);
+      dfz = ((-(TC(1. / 6.) * PZ(2)) + PZ(1)) - TC(1. / 2.) * PZ(0)) - TC(1. / 3.) * PZ(-1);
     wdfdz = -divz(p, vw * dfz);
   } else {  // first-order upwinding at k=1,kmax
-    if (vw >= TC(0.)) dfz = PH(0) - PH(-sz);
-    else dfz = PH(sz) - PH(0);
+    if (vw >= TC(0.)) dfz = PZ(0) - PZ(-1);
+    else dfz = PZ(1) - PZ(0);
     wdfdz = -divz(p, vw * dfz);
   }
-#undef PH
+#undef PX
+#undef PY
+#undef PZ
   return (udfdx + vdfdy) + wdfdz;
 }
-
-// RK_nb value of one cell: phi_in (+ factor*dt*dfdt on the band)
+// One stage value at row k of column (I,J): every operand (phi0, phis' axial
+// stencil, the band flag and the velocities) is read first, so one memory
+// latency is exposed per row; the stencil result is used on band cells only.
 template <int SCHEME, typename T>
-__device__ __forceinline__ T adv_val(const Params& p, int stage1, const T* __restrict__ phi0,
-                                     const T* __restrict__ phis, T a, T b, T fdt, const T* __restrict__ vu,
-                                     const T* __restrict__ vv, const T* __restrict__ vw,
+__device__ __forceinline__ T adv_val(const Params& p, int stage1, const T* phi0, const T* phis, T a, T b, T fdt,
+                                     const T* __restrict__ vu, const T* __restrict__ vv, const T* __restrict__ vw,
                                      const uint8_t* __restrict__ mask, int I, int J, int k) {
   const long long n = idxL(p, I, J, k);
-  T v = stage1 ? phi0[n] : a * phi0[n] + b * phis[n];
-  if (k >= 1 && k <= p.kmax) {
-    const long long q = idxI(p, I, J, k);
-    if (mask[q]) v = v + fdt * adv_rhs<SCHEME>(p, phis, vu[q], vv[q], vw[q], I, J, k);
-  }
-  return v;
+  const T f0 = phi0[n];
+  if (!(k >= 1 && k <= p.kmax)) return stage1 ? f0 : a * f0 + b * phis[n];
+  const long long q = idxI(p, I, J, k);
+  const uint8_t m = mask[q];
+  const T u = vu[q], v = vv[q], w = vw[q];
+  const Axial19<T> S = read_axial(phis, n, (long long)p.nLx, (long long)p.nLx * p.nLy);
+  T val = stage1 ? f0 : a * f0 + b * S.c;
+  if (m) val = val + fdt * adv_rhs<SCHEME>(p, S, u, v, w, k);
+  return val;
 }
-
-// One RK stage over the tasks' regions; out may equal phi0 (see above).
 template <int SCHEME, typename T>
-__global__ void __launch_bounds__(NT, 4) k_adv_stage(Params p, const __grid_constant__ LsBatch B, int stage1,
+__global__ void __launch_bounds__(NT, 3) k_adv_stage(Params p, const __grid_constant__ LsBatch B, int stage1,
                                                      double a_, double bb_, double fdt_, const T* __restrict__ vu,
                                                      const T* __restrict__ vv, const T* __restrict__ vw) {
   const int ti = task_of(B);
@@ -518,23 +543,34 @@ __global__ void __launch_bounds__(NT) k_heaviside(Params p, const __grid_constan
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
   const T eps = TC(1.5 * p.dz);
-  const T* phi = cT<T>(t.phi0);
+  const T* __restrict__ phi = cT<T>(t.phi0);
   double s = 0.;
   if (c.ok && c.cxy) {
     const int i = c.i, j = c.j;
     const int ii = image_of<1>(i, p.imax), jj = image_of<1>(j, p.jmax);
     const int ka = max(c.ka, t.r.cz0), kb = min(c.kb, t.r.cz1);
-    for (int k = ka; k <= kb; ++k) {
-      const T H = heav_trig(p, phi[idxL(p, i, j, k)], eps);
-      if (H < TC(1.)) {
-        min_into(jiemian + idxC(p, i, j, k), H);
-        if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, j, k), H);
-        if (jj != INT_MIN) {
-          min_into(jiemian + idxC(p, i, jj, k), H);
-          if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, jj, k), H);
+    const long long sz = (long long)p.nLx * p.nLy;
+    // eight rows' phi in flight before their minima and sums (same order)
+    for (int k0 = ka; k0 <= kb; k0 += 8) {
+      T f[8];
+      const long long c0 = idxL(p, i, j, k0);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) f[u] = (k0 + u <= kb) ? phi[c0 + u * sz] : TC(1.);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int k = k0 + u;
+        if (k > kb) break;
+        const T H = heav_trig(p, f[u], eps);
+        if (H < TC(1.)) {
+          min_into(jiemian + idxC(p, i, j, k), H);
+          if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, j, k), H);
+          if (jj != INT_MIN) {
+            min_into(jiemian + idxC(p, i, jj, k), H);
+            if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, jj, k), H);
+          }
         }
+        if (k >= 1 && k <= p.kmax) s += (double)H;
       }
-      if (k >= 1 && k <= p.kmax) s += (double)H;
     }
   }
   const double bs = block_sum<double, NT>(s);

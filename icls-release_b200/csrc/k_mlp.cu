@@ -756,55 +756,35 @@ __global__ void k_mlp_gen(unsigned long long seed, long long n, float* __restric
 
 // ================================================ the network in the loop
 // A gathered interface cell: task q of the batch, interior cell (i, j, k)
-struct MlpCell {
-  int q, i, j, k;
-};
 
-// Stencils of the tasks' interface cells (computed interior cells of the
-// shape-C regions with |phi| <= 4dz, the cells whose curvature
-// re_curvature and the jumps read) into X, slots by a warp-aggregated
-// counter; cells beyond cap keep the plain curvature.
+// The features of the recorded near-interface cells (k_curvature records
+// the computed cells with |phi| <= 4dz, the cells re_curvature and the
+// jumps read) into X, one thread per cell; cells beyond cap keep the plain
+// curvature.
 template <typename T>
-__global__ void __launch_bounds__(256, 2) k_mlp_gather(Params p, const __grid_constant__ LsBatch B,
-                                                    float* __restrict__ X, MlpCell* __restrict__ rec,
-                                                    int* __restrict__ count, int cap) {
-  const int ti = task_of(B);
-  const LsTask& t = B.t[ti];
-  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
-  const T* __restrict__ phi = cT<T>(t.phi0);
+__global__ void __launch_bounds__(256) k_mlp_features(Params p, const __grid_constant__ LsBatch B,
+                                                      const MlpCell* __restrict__ rec, const int* __restrict__ count,
+                                                      int cap, float* __restrict__ X) {
+  const int n = min(*count, cap);
   const float rdz = (float)(1. / p.dz);
-  const T lim = (T)(4. * p.dz);
   const long long sy = p.nLx, sz = (long long)p.nLx * p.nLy;
-  const unsigned lane = threadIdx.x & 31u;
-  const int k0 = max(c.ka, max(t.r.cz0, 1)), k1 = min(c.kb, min(t.r.cz1, p.kmax));
-  // every lane of the warp walks the same rows so the ballots line up
-  for (int k = c.ka; k <= c.kb; ++k) {
-    bool take = false;
-    long long cl = 0;
-    if (c.ok && c.cxy && k >= k0 && k <= k1) {
-      cl = idxL(p, c.i, c.j, k);
-      take = fabs(phi[cl]) <= lim;
-    }
-    const unsigned m = __ballot_sync(0xffffffffu, take);
-    if (!m) continue;
-    int base = 0;
-    if (lane == (unsigned)(__ffs(m) - 1)) base = atomicAdd(count, __popc(m));
-    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-    if (!take) continue;
-    const int slot = base + __popc(m & ((1u << lane) - 1u));
-    if (slot >= cap) continue;
-    const float pc = (float)phi[cl];
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const MlpCell r = rec[s];
+    const T* __restrict__ phi = cT<T>(B.t[r.q].phi0);
+    const long long cl = idxL(p, r.i, r.j, r.k);
     float f[27];
-    int n = 0;
+    int m = 0;
     for (int dk = -1; dk <= 1; ++dk)
       for (int dj = -1; dj <= 1; ++dj)
-        for (int di = -1; di <= 1; ++di) f[n++] = ((float)phi[cl + di + dj * sy + dk * sz] - pc) * rdz;
+        for (int di = -1; di <= 1; ++di) f[m++] = (float)phi[cl + di + dj * sy + dk * sz];
+    const float pc = f[13];
+#pragma unroll
+    for (int q = 0; q < 27; ++q) f[q] = (f[q] - pc) * rdz;
     float o[kIn];
     mlp_features(f, o);
-    float4* dst = reinterpret_cast<float4*>(X + (long long)slot * kIn);
+    float4* dst = reinterpret_cast<float4*>(X + (long long)s * kIn);
 #pragma unroll
     for (int q = 0; q < kIn / 4; ++q) dst[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
-    rec[slot] = MlpCell{ti, c.i, c.j, k};
   }
 }
 
@@ -917,18 +897,18 @@ void refresh_copies(icls_mlp* m) {
 
 namespace icls {
 // get_curvature's output (the batch tasks' out buffers, computed by
-// launch_curvature) replaced by the network near the interface
+// launch_curvature with collect set, which also recorded the cells)
+// replaced by the network near the interface
 int launch_mlp_curvature(Ctx& c, const LsBatch& b) {
   if (b.n == 0) return ICLS_OK;
   if (!c.net) return ICLS_E_STATE;
   Scope sc_(c.prof, c.s, "mlp_curvature", 2);
-  cudaMemsetAsync(c.mlp_count, 0, sizeof(int), c.s);
   if (c.P.f32)
-    k_mlp_gather<float><<<b.start[b.n], dim3(TBX, TBY, 1), 0, c.s>>>(c.P, b, c.mlp_X, (MlpCell*)c.mlp_rec,
-                                                                      c.mlp_count, c.mlp_cap);
+    k_mlp_features<float><<<4 * 148, 256, 0, c.s>>>(c.P, b, (const MlpCell*)c.mlp_rec, c.mlp_count, c.mlp_cap,
+                                                    c.mlp_X);
   else
-    k_mlp_gather<double><<<b.start[b.n], dim3(TBX, TBY, 1), 0, c.s>>>(c.P, b, c.mlp_X, (MlpCell*)c.mlp_rec,
-                                                                       c.mlp_count, c.mlp_cap);
+    k_mlp_features<double><<<4 * 148, 256, 0, c.s>>>(c.P, b, (const MlpCell*)c.mlp_rec, c.mlp_count, c.mlp_cap,
+                                                     c.mlp_X);
   const int grid = std::min((c.mlp_cap + kRows - 1) / kRows, 2 * 148);
   const double tol = c.cfg.mlp_fallback_tol;
   if (c.P.f32)
