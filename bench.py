@@ -43,7 +43,7 @@ UNIT = "Mcell-steps/s"
 
 # ------------------------------------------------------------------ workload
 def make_workload(name):
-    from icls_gpu.config import multi_drop, rising_bubble, static_drop
+    from icls_gpu.config import combined, multi_drop, rising_bubble, static_drop
     if name == "multi_drop_256_48":
         return multi_drop(n=256, ndrop=48, seed=2024)
     if name == "multi_drop_256_4":
@@ -56,17 +56,21 @@ def make_workload(name):
         return static_drop(256)
     if name == "rising_bubble_128":
         return rising_bubble(128)
+    if name == "combined_384_200":  # the combined-form configuration (FFT lengths 384 = 16 x 24)
+        return combined(384, 200)
+    if name == "combined_96_12":  # the same kinds of input at 96^3 (16 x 6), 12 drops of 7-10 cells
+        return combined(96, 12, rmin=0.07, rmax=0.1)
     raise SystemExit("unknown workload %s" % name)
 
 
 def initial_state(wl):
-    from icls_gpu.config import init_drops, init_drops_boxed, initial_velocity
+    from icls_gpu.config import init_drops, init_drops_boxed, workload_velocity
     cfg = wl.cfg
     if wl.all_images and cfg.itot >= 128:
         ls = init_drops_boxed(cfg, wl.centres, wl.radii)
     else:
         ls = init_drops(cfg, wl.centres, wl.radii, wl.all_images)
-    u, v, w = initial_velocity(cfg, wl.shear_v)
+    u, v, w = workload_velocity(wl)
     return ls, u, v, w
 
 

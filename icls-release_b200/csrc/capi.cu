@@ -82,11 +82,11 @@ namespace {
     if (e_ != cudaSuccess) return ICLS_E_CUDA; \
   } while (0)
 
-bool pow2(int n) { return n >= 4 && (n & (n - 1)) == 0; }
 
 int validate(const icls_config* c) {
   if (!c) return ICLS_E_ARG;
-  if (!pow2(c->itot) || !pow2(c->jtot)) return ICLS_E_CONFIG;  // radix-2 FFT in x and y
+  if (!fft_length_ok(c->itot, false, c->itot) || !fft_length_ok(c->jtot, true, c->itot))
+    return ICLS_E_CONFIG;  // FFT lengths in x and y
   if (c->itot > 4096 || c->jtot > 4096) return ICLS_E_CONFIG;
   if (c->itot < 8 || c->jtot < 8) return ICLS_E_CONFIG;  // periodic images of 3 halo layers
   if (c->ktot < 6 || c->lmax < 1) return ICLS_E_CONFIG;
@@ -131,6 +131,10 @@ void fill_params(Ctx& c) {
   P.rho1 = f.rho1; P.rho2 = f.rho2; P.miu1 = f.miu1; P.miu2 = f.miu2;
   P.rho0 = std::min(f.rho1, f.rho2);  // param.f90:63
   P.rrho0 = 1. / P.rho0;
+  {
+    int e2;
+    P.rho0_pow2 = std::frexp(P.rho0, &e2) == 0.5 ? 1 : 0;
+  }
   P.f32 = f.precision == ICLS_FP32 ? 1 : 0;
   P.visc = 1. / f.Re;                 // param.f90:73
   P.iFr = f.iFr;

@@ -197,6 +197,7 @@ struct MlpCell {
 // get_curvature over the batch; with collect, also records the computed
 // cells with |phi| <= 4dz for the network (count reset here)
 void launch_curvature(Ctx& c, const LsBatch& b, double* nrm_m_out, bool collect = false);
+bool fft_length_ok(int n, bool y_pass, int imax);
 void launch_recurvature(Ctx& c, const LsBatch& b);
 void launch_jumps(Ctx& c, const LsBatch& b);
 void launch_ipot(Ctx& c, double* dmin_dev);

@@ -32,6 +32,7 @@ struct Params {
   double dt;
   double rho1, rho2, miu1, miu2, rho0, visc, iFr, nondi;
   double rrho0;              // 1./rho0, the IEEE quotient the reference evaluates per cell
+  int rho0_pow2;             // rho0 is a power of two: x / rho0 == x * rrho0 exactly
   double g1, g2, g3;
   double v_lower, v_upper;
   double forceytot;
@@ -69,6 +70,8 @@ template <typename T>
 __device__ __forceinline__ T divy(const Params& p, T a) { return p.pow2 ? a * (T)p.rdy : a / (T)p.dy; }
 template <typename T>
 __device__ __forceinline__ T divz(const Params& p, T a) { return p.pow2 ? a * (T)p.rdz : a / (T)p.dz; }
+// a / rho0: a product by the exact reciprocal when rho0 is a power of two
+__device__ __forceinline__ double div_rho0(const Params& p, double a) { return p.rho0_pow2 ? a * p.rrho0 : a / p.rho0; }
 
 // -------------------------------------------------------------- regions
 // A per-drop sweep region.  x and y are periodic: the region holds the

@@ -359,23 +359,23 @@ template <typename T>
 __device__ __forceinline__ T corr_u(const Params& p, const T* dudt, const double* pp, const double* px, int i, int j,
                                     int k) {
   const long long c = idxC(p, i, j, k);
-  if (sizeof(T) == sizeof(double)) return (T)(dudt[c] - p.dt * p.dxi * ((pp[c + 1] - pp[c]) - px[c]) / p.rho0);
-  return dudt[c] - (T)(p.dt * p.dxi * ((pp[c + 1] - pp[c]) - px[c]) / p.rho0);
+  if (sizeof(T) == sizeof(double)) return (T)(dudt[c] - div_rho0(p, p.dt * p.dxi * ((pp[c + 1] - pp[c]) - px[c])));
+  return dudt[c] - (T)(div_rho0(p, p.dt * p.dxi * ((pp[c + 1] - pp[c]) - px[c])));
 }
 template <typename T>
 __device__ __forceinline__ T corr_v(const Params& p, const T* dvdt, const double* pp, const double* py, int i, int j,
                                     int k) {
   const long long c = idxC(p, i, j, k);
-  if (sizeof(T) == sizeof(double)) return (T)(dvdt[c] - p.dt * p.dyi * ((pp[c + p.nCx] - pp[c]) - py[c]) / p.rho0);
-  return dvdt[c] - (T)(p.dt * p.dyi * ((pp[c + p.nCx] - pp[c]) - py[c]) / p.rho0);
+  if (sizeof(T) == sizeof(double)) return (T)(dvdt[c] - div_rho0(p, p.dt * p.dyi * ((pp[c + p.nCx] - pp[c]) - py[c])));
+  return dvdt[c] - (T)(div_rho0(p, p.dt * p.dyi * ((pp[c + p.nCx] - pp[c]) - py[c])));
 }
 template <typename T>
 __device__ __forceinline__ T corr_w(const Params& p, const T* dwdt, const double* pp, const double* pz, int i, int j,
                                     int k) {
   const long long c = idxC(p, i, j, k);
   const long long sz = (long long)p.nCx * p.nCy;
-  if (sizeof(T) == sizeof(double)) return (T)(dwdt[c] - p.dt * p.dzi * ((pp[c + sz] - pp[c]) - pz[c]) / p.rho0);
-  return dwdt[c] - (T)(p.dt * p.dzi * ((pp[c + sz] - pp[c]) - pz[c]) / p.rho0);
+  if (sizeof(T) == sizeof(double)) return (T)(dwdt[c] - div_rho0(p, p.dt * p.dzi * ((pp[c + sz] - pp[c]) - pz[c])));
+  return dwdt[c] - (T)(div_rho0(p, p.dt * p.dzi * ((pp[c + sz] - pp[c]) - pz[c])));
 }
 
 struct CorrArgs {

@@ -13,11 +13,12 @@
 // the z pass walks k with one thread per (i,j).
 //
 // Two real lines share one complex FFT (z = a + i b).  Lines of 64, 128 or
-// 256 points take the two-level transform (k_fft2): N = R1 x R2 with
-// R1 = 16, a radix-16 DFT of every R2-strided subsequence in registers
-// (each thread has its 32 loads in flight), the N-point twiddles, one
-// padded shared-memory exchange, and a radix-R2 DFT in registers; other
-// lengths take radix-2 passes in shared memory (k_fft_x, k_fft_y).
+// 256 points, and of 48, 96, 192 or 384 (a radix-3 factor), take the
+// two-level transform (k_fft2): N = R1 x R2 with R1 = 16, a radix-16 DFT of
+// every R2-strided subsequence in registers (each thread has its 32 loads in
+// flight), the N-point twiddles, one padded shared-memory exchange, and a
+// radix-R2 DFT in registers; other powers of two take radix-2 passes in
+// shared memory (k_fft_x, k_fft_y).
 #include <cmath>
 #include <vector>
 
@@ -124,7 +125,6 @@ __global__ void __launch_bounds__(FT) k_fft_x(Params p, int dir, int CL, int log
   const long long nlines = (long long)p.jmax * p.kmax;
   const long long l0 = (long long)blockIdx.x * (2 * CL);
   const double s = sqrt(1.0 / N);
-  const int lj = __ffs(p.jmax) - 1, mj = p.jmax - 1;  // jmax is a power of two
   // load
   for (int t = threadIdx.x; t < CL * N; t += blockDim.x) {
     const int cl = t >> logN, n = t & (N - 1);
@@ -132,8 +132,8 @@ __global__ void __launch_bounds__(FT) k_fft_x(Params p, int dir, int CL, int log
     double2 z = make_double2(0., 0.);
     if (lb < nlines) {
       if (dir == 0) {
-        const int ja = (int)(la & mj) + 1, ka = (int)(la >> lj) + 1;
-        const int jb = (int)(lb & mj) + 1, kb = (int)(lb >> lj) + 1;
+        const int ja = (int)(la % p.jmax) + 1, ka = (int)(la / p.jmax) + 1;
+        const int jb = (int)(lb % p.jmax) + 1, kb = (int)(lb / p.jmax) + 1;
         z = make_double2(pp[idxC(p, n + 1, ja, ka)], pp[idxC(p, n + 1, jb, kb)]);
         sm[cl * ld + bitrev(n, logN)] = z;
       } else {
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(FT) k_fft_x(Params p, int dir, int CL, int log
       for (int h = 0; h < 2; ++h) {
         const long long ll = h ? lb : la;
         const double v = h ? vb : va;
-        const int j = (int)(ll & mj) + 1, k = (int)(ll >> lj) + 1;
+        const int j = (int)(ll % p.jmax) + 1, k = (int)(ll / p.jmax) + 1;
         const int i = n + 1;
         if (!halos) {
           pp[idxC(p, i, j, k)] = v;
@@ -253,18 +253,62 @@ constexpr int bitrev_c(int x, int bits) {
 }
 constexpr int ilog2_c(int n) { return n <= 1 ? 0 : 1 + ilog2_c(n >> 1); }
 
-// W_N^m from the half table tw[m] = W_N^m, m < N/2 (W_N^(m+N/2) = -W_N^m)
+// W_N^m, 0 <= m < N (N even), from the half table tw[m] = W_N^m, m < N/2
+// (W_N^(m+N/2) = -W_N^m)
 __device__ __forceinline__ double2 twid_full(const double2* __restrict__ tw, int m, int N, int inv) {
-  double2 w = __ldg(&tw[m & (N / 2 - 1)]);
-  if (m & (N / 2)) w = make_double2(-w.x, -w.y);
+  double2 w;
+  if (m >= N / 2) {
+    w = __ldg(&tw[m - N / 2]);
+    w = make_double2(-w.x, -w.y);
+  } else {
+    w = __ldg(&tw[m]);
+  }
   if (inv) w.y = -w.y;
   return w;
+}
+__device__ __forceinline__ double2 cmul(double2 a, double2 w) {
+  return make_double2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
 }
 
 // in-register DFT of R points, natural order in and out; tw is the N-point
 // half table, W_R^m = W_N^(m N/R)
 template <int R>
+__device__ __forceinline__ void reg_dft(double2 (&x)[R], const double2* __restrict__ tw, int N, int inv);
+
+// R = 3 Q (Q a power of two): n = Q n1 + n2, k = k1 + 3 k2; a 3-point DFT
+// over n1 for every n2, the R-point twiddles W_R^(n2 k1), then a Q-point DFT
+// over n2 for every k1
+template <int R>
+__device__ __forceinline__ void reg_dft3(double2 (&x)[R], const double2* __restrict__ tw, int N, int inv) {
+  constexpr int Q = R / 3;
+  const double2 w1 = twid_full(tw, N / 3, N, inv), w2 = twid_full(tw, 2 * (N / 3), N, inv);
+  double2 y[3][Q];
+#pragma unroll
+  for (int n2 = 0; n2 < Q; ++n2) {
+    const double2 a = x[n2], b = x[Q + n2], c = x[2 * Q + n2];
+    const double2 b1 = cmul(b, w1), c2 = cmul(c, w2), b2 = cmul(b, w2), c1 = cmul(c, w1);
+    y[0][n2] = make_double2((a.x + b.x) + c.x, (a.y + b.y) + c.y);
+    y[1][n2] = make_double2((a.x + b1.x) + c2.x, (a.y + b1.y) + c2.y);
+    y[2][n2] = make_double2((a.x + b2.x) + c1.x, (a.y + b2.y) + c1.y);
+    if (n2 > 0) {
+      y[1][n2] = cmul(y[1][n2], twid_full(tw, n2 * (N / R), N, inv));
+      y[2][n2] = cmul(y[2][n2], twid_full(tw, 2 * n2 * (N / R), N, inv));
+    }
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < 3; ++k1) {
+    reg_dft<Q>(y[k1], tw, N, inv);
+#pragma unroll
+    for (int k2 = 0; k2 < Q; ++k2) x[k1 + 3 * k2] = y[k1][k2];
+  }
+}
+
+template <int R>
 __device__ __forceinline__ void reg_dft(double2 (&x)[R], const double2* __restrict__ tw, int N, int inv) {
+  if constexpr (R % 3 == 0) {
+    reg_dft3<R>(x, tw, N, inv);
+    return;
+  }
   constexpr int LR = ilog2_c(R);
   double2 y[R];
 #pragma unroll
@@ -295,18 +339,22 @@ __device__ __forceinline__ void reg_dft(double2 (&x)[R], const double2* __restri
 // are adjacent threads.  dir 0: p (x) or spec (y) -> half-complex spec;
 // dir 1: the inverse, into spec (y) or p (x, with the boundp images when
 // halos is set).
-template <int R1, int R2, bool YPASS>
-__global__ void __launch_bounds__(256, 2) k_fft2(Params p, int dir, const double2* __restrict__ tw,
-                                                 double* __restrict__ pp, double* __restrict__ spec, int halos) {
+// LPC complex lines per CTA of 256 threads, TPL = max(R1, R2) threads per
+// line; LPC * TPL <= 256 (the other threads idle)
+template <int R1, int R2, bool YPASS, int LPC>
+__global__ void __launch_bounds__(256, (R1 > 16 || R2 > 16) ? 1 : 2)
+    k_fft2(Params p, int dir, const double2* __restrict__ tw, double* __restrict__ pp, double* __restrict__ spec,
+           int halos) {
   constexpr int N = R1 * R2;
-  constexpr int TPL = R1 > R2 ? R1 : R2;  // threads per complex line
-  constexpr int LPC = 256 / TPL;          // complex lines per CTA
+  constexpr int TPL = R1 > R2 ? R1 : R2;
+  static_assert(LPC * TPL <= 256, "a CTA holds LPC lines of TPL threads");
   constexpr int SLD = R1 + 1;             // exchange row (padded)
   constexpr int LS = R2 * SLD + 1;        // exchange line stride (padded)
   constexpr int ZLD = N + 1;              // natural-order line stride
   extern __shared__ double2 sm[];
   const int lt = YPASS ? (int)threadIdx.x % LPC : (int)threadIdx.x / TPL;
   const int lane = YPASS ? (int)threadIdx.x / LPC : (int)threadIdx.x % TPL;
+  const bool used = (int)threadIdx.x < LPC * TPL;  // the threads beyond LPC lines idle
   const double s = sqrt(1.0 / N);
   // the two real lines: element n of line a at A[n * st], of line b at B[n * st]
   const double* A;
@@ -318,7 +366,7 @@ __global__ void __launch_bounds__(256, 2) k_fft2(Params p, int dir, const double
   if (!YPASS) {
     const long long nlines = (long long)p.jmax * p.kmax;
     const long long la = 2 * ((long long)blockIdx.x * LPC + lt), lb = la + 1;
-    live = lb < nlines;
+    live = used && lb < nlines;
     ja = (int)(la % p.jmax) + 1; ka = (int)(la / p.jmax) + 1;
     jb = (int)(lb % p.jmax) + 1; kb = (int)(lb / p.jmax) + 1;
     st = 1;
@@ -333,7 +381,7 @@ __global__ void __launch_bounds__(256, 2) k_fft2(Params p, int dir, const double
     const int tiles_i = p.imax / (2 * LPC);
     const int k = (int)blockIdx.x / tiles_i + 1;
     const int i0 = ((int)blockIdx.x % tiles_i) * (2 * LPC) + 2 * lt;  // 0-based column
-    live = true;
+    live = used;
     colbase = spec + (long long)i0 + (long long)p.imax * p.jmax * (k - 1);
     st = p.imax;
     A = colbase;
@@ -427,9 +475,8 @@ __global__ void __launch_bounds__(256, 2) k_fft2(Params p, int dir, const double
     }
   }
 }
-template <int R1, int R2>
+template <int R1, int R2, int LPC>
 constexpr size_t fft2_smem() {
-  constexpr int TPL = R1 > R2 ? R1 : R2, LPC = 256 / TPL;
   constexpr int ex = LPC * (R2 * (R1 + 1) + 1), nat = LPC * (R1 * R2 + 1);
   return (size_t)(ex > nat ? ex : nat) * sizeof(double2);
 }
@@ -592,20 +639,27 @@ static int y_tile(int imax) {
   return ti;
 }
 
-template <int R1, int R2, bool Y>
+template <int R1, int R2, bool Y, int LPC>
 void fft2_launch(Ctx& c, int dir, const double2* tw, int halos) {
   const Params& P = c.P;
-  constexpr int TPL = R1 > R2 ? R1 : R2, LPC = 256 / TPL;
   static unsigned attr = 0;  // devices this instance's shared-memory limit is raised on
   int dev = 0;
   cudaGetDevice(&dev);
   if (!(attr & (1u << (dev & 31)))) {
-    cudaFuncSetAttribute(k_fft2<R1, R2, Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft2_smem<R1, R2>());
+    cudaFuncSetAttribute(k_fft2<R1, R2, Y, LPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)fft2_smem<R1, R2, LPC>());
     attr |= 1u << (dev & 31);
   }
   const long long units = Y ? (long long)(P.imax / (2 * LPC)) * P.kmax
                             : ((long long)P.jmax * P.kmax + 2 * LPC - 1) / (2 * LPC);
-  k_fft2<R1, R2, Y><<<(unsigned)units, 256, fft2_smem<R1, R2>(), c.s>>>(P, dir, tw, c.p, c.spec, halos);
+  k_fft2<R1, R2, Y, LPC><<<(unsigned)units, 256, fft2_smem<R1, R2, LPC>(), c.s>>>(P, dir, tw, c.p, c.spec, halos);
+}
+// the lengths with a radix-3 factor: 16 lines per CTA where the columns tile
+// by 32 (y pass) and the lines need at most 16 threads, else 8
+template <int R2, bool Y>
+void fft2_launch3(Ctx& c, int dir, const double2* tw, int halos) {
+  if (R2 <= 16 && (!Y || c.P.imax % 32 == 0)) fft2_launch<16, R2, Y, R2 <= 16 ? 16 : 8>(c, dir, tw, halos);
+  else fft2_launch<16, R2, Y, 8>(c, dir, tw, halos);
 }
 
 // the two-level transform of one pass if its length has one (and, for the
@@ -617,9 +671,25 @@ bool fft2_pass(Ctx& c, int dir, int halos) {
   const double2* tw = Y ? c.twy : c.twx;
   auto fits = [&](int lpc) { return !Y || P.imax % (2 * lpc) == 0; };
   switch (N) {
-    case 64: if (!fits(16)) return false; fft2_launch<16, 4, Y>(c, dir, tw, halos); return true;
-    case 128: if (!fits(16)) return false; fft2_launch<16, 8, Y>(c, dir, tw, halos); return true;
-    case 256: if (!fits(16)) return false; fft2_launch<16, 16, Y>(c, dir, tw, halos); return true;
+    case 64: if (!fits(16)) return false; fft2_launch<16, 4, Y, 16>(c, dir, tw, halos); return true;
+    case 128: if (!fits(16)) return false; fft2_launch<16, 8, Y, 16>(c, dir, tw, halos); return true;
+    case 256: if (!fits(16)) return false; fft2_launch<16, 16, Y, 16>(c, dir, tw, halos); return true;
+    case 48: if (!fits(8)) return false; fft2_launch3<3, Y>(c, dir, tw, halos); return true;
+    case 96: if (!fits(8)) return false; fft2_launch3<6, Y>(c, dir, tw, halos); return true;
+    case 192: if (!fits(8)) return false; fft2_launch3<12, Y>(c, dir, tw, halos); return true;
+    case 384: if (!fits(8)) return false; fft2_launch3<24, Y>(c, dir, tw, halos); return true;
+    default: return false;
+  }
+}
+
+// a line length the solve supports along x (y_pass false) or y, for a grid
+// with imax columns: powers of two from 8 (radix-2 passes where the
+// two-level transform does not apply), and 48, 96, 192, 384 (two-level only;
+// the y pass tiles at least 16 columns)
+bool fft_length_ok(int n, bool y_pass, int imax) {
+  if (n >= 8 && (n & (n - 1)) == 0) return true;
+  switch (n) {
+    case 48: case 96: case 192: case 384: return !y_pass || imax % 16 == 0;
     default: return false;
   }
 }

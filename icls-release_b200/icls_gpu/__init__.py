@@ -5,14 +5,14 @@ include/icls_gpu.h; this package only binds it.
 """
 from .config import (CURV_MLP, CURV_STENCIL, FIELD_ID, FIELDS, FP32, FP64, HOUC5,
                      SPEED_CURV, SPEED_UNFM, WENO5, IclsConfig, IclsScalars, Workload,
-                     field_shape, init_drops, initial_velocity, make_config, multi_drop,
-                     rising_bubble, seeded_drops, static_drop)
+                     combined, field_shape, init_drops, initial_velocity, make_config, multi_drop,
+                     rising_bubble, seeded_drops, solenoidal_velocity, static_drop, workload_velocity)
 from .binding import LIB_PATH, Backend, IclsError, Solver, gpu_backend
 
 __all__ = [
     "CURV_MLP", "CURV_STENCIL", "FIELD_ID", "FIELDS", "FP32", "FP64", "HOUC5",
     "SPEED_CURV", "SPEED_UNFM", "WENO5", "IclsConfig", "IclsScalars", "Workload",
-    "field_shape", "init_drops", "initial_velocity", "make_config", "multi_drop",
-    "rising_bubble", "seeded_drops", "static_drop", "LIB_PATH", "Backend", "IclsError",
+    "combined", "field_shape", "init_drops", "initial_velocity", "make_config", "multi_drop",
+    "rising_bubble", "seeded_drops", "solenoidal_velocity", "static_drop", "workload_velocity", "LIB_PATH", "Backend", "IclsError",
     "Solver", "gpu_backend",
 ]

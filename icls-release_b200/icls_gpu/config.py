@@ -244,6 +244,7 @@ class Workload:
     all_images: bool
     shear_v: float  # initial v = shear_v*(2z-1) (0 for rest)
     steps: int
+    turbulence: tuple | None = None  # (seed, rms, kmax) of a solenoidal initial velocity
 
 
 def static_drop(n: int = 64, steps: int = 200) -> Workload:
@@ -284,6 +285,91 @@ def multi_drop(n: int = 256, ndrop: int = 48, seed: int = 2024, steps: int = 100
     if dt is not None:
         cfg.timestep = dt
     return Workload("multi_drop_%d_%d" % (n, ndrop), cfg, centres, radii, True, 0.5, steps)
+
+
+def combined(n: int = 384, ndrop: int = 200, seed: int = 2024, steps: int = 2000, rmin: float = 0.02,
+             rmax: float = 0.04, rms: float = 0.2, kmax: int = 8, dt: float = 1e-5) -> Workload:
+    """The combined-form configuration: n^3 on [0,1]^3, ndrop seeded drops
+    with radii uniform in [rmin,rmax] and a 4-cell surface gap, a seeded
+    random solenoidal velocity with a k^-5/3 spectrum over |k| = 1..kmax and
+    the given rms (solenoidal_velocity), rho and miu ratio 10, sigma = 0.2
+    (We = 5), Re = 10, walls at rest, HOUC5, reinitialisation and inflation
+    every 20 steps.  The configuration is the plain method's; the FP32 form
+    and the learned curvature are chosen by the caller (precision,
+    curvature_model)."""
+    cfg = make_config(itot=n, jtot=n, ktot=n, lmax=ndrop, timestep=dt,
+                      rho1=1.0, rho2=10.0, miu1=1.0, miu2=10.0, Re=10.0, We=5.0,
+                      ls_adv_space=HOUC5, reinit_step=20, reinit_iter_max=1, inflate_step=20)
+    centres, radii = seeded_drops(cfg, ndrop, rmin, rmax, seed)
+    return Workload("combined_%d_%d" % (n, ndrop), cfg, centres, radii, True, 0.0, steps,
+                    (seed + 1, rms, kmax))
+
+
+def solenoidal_velocity(cfg: IclsConfig, seed: int, rms: float = 0.2, kmax: int = 8, slope: float = -5.0 / 3.0):
+    """u, v, w on shape C: a seeded random field that is divergence-free on
+    the staggered grid to roundoff.  u = curl A with the vector potential on
+    cell edges (A_x at ((i-1/2)dx, j dy, k dz), A_y at (i dx, (j-1/2)dy, k dz),
+    A_z at (i dx, j dy, (k-1/2)dz)), so the discrete divergence of the face
+    velocities is an exact telescoping sum.  A has Fourier modes in x and y
+    (periodic) and half-wave sine modes sin(pi m z / lz) in z, so A_x and A_y
+    vanish on the walls and w = 0 there; modes with 1 <= |k| <= kmax (k in
+    cycles per length, m/2 along z) get random complex amplitudes scaled as
+    |k|^((slope - 2)/2) / |k| (a shell energy spectrum ~ k^slope for the
+    velocity).  The field is scaled to the given rms over the interior
+    faces; halos are left to init_program's boundary pass."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = cfg.itot, cfg.jtot, cfg.ktot
+    dx, dy, dz = cfg.lx / nx, cfg.ly / ny, cfg.lz / nz
+    kx = np.fft.fftfreq(nx, d=1.0 / nx)[:, None] / cfg.lx
+    ky = np.fft.fftfreq(ny, d=1.0 / ny)[None, :] / cfg.ly
+
+    def component(sx, sy, zpos):
+        """one potential component at x = (i0 + sx) dx, y = (j0 + sy) dy
+        (i0, j0 = 0..n-1) and the given z positions"""
+        out = np.zeros((nx, ny, zpos.size))
+        for m in range(1, 2 * kmax + 1):
+            kz = 0.5 * m / cfg.lz
+            kk = np.sqrt(kx * kx + ky * ky + kz * kz)
+            sel = (kk >= 1.0) & (kk <= kmax)
+            if not sel.any():
+                continue
+            amp = np.where(sel, kk ** ((slope - 2.0) / 2.0) / np.maximum(kk, 1e-30), 0.0)
+            coef = amp * (rng.standard_normal((nx, ny)) + 1j * rng.standard_normal((nx, ny)))
+            # shift theorem: the plane sampled at the component's offsets
+            coef = coef * np.exp(2j * np.pi * (np.fft.fftfreq(nx)[:, None] * sx + np.fft.fftfreq(ny)[None, :] * sy))
+            plane = np.fft.ifft2(coef).real * (nx * ny)
+            out += plane[:, :, None] * np.sin(np.pi * m * zpos / cfg.lz)[None, None, :]
+        return out
+
+    zk = np.arange(nz + 1) * dz            # k dz, k = 0..nz
+    zc = (np.arange(nz) + 0.5) * dz        # (k - 1/2) dz, k = 1..nz
+    Ax = component(0.5, 1.0, zk)
+    Ay = component(1.0, 0.5, zk)
+    Az = component(1.0, 1.0, zc)
+    roll = np.roll
+    u = (Az - roll(Az, 1, axis=1)) / dy - (Ay[:, :, 1:] - Ay[:, :, :-1]) / dz
+    v = (Ax[:, :, 1:] - Ax[:, :, :-1]) / dz - (Az - roll(Az, 1, axis=0)) / dx
+    w = (Ay[:, :, 1:] - roll(Ay, 1, axis=0)[:, :, 1:]) / dx - (Ax[:, :, 1:] - roll(Ax, 1, axis=1)[:, :, 1:]) / dy
+    scale = rms / math.sqrt(float(np.mean(u * u) + np.mean(v * v) + np.mean(w * w)) / 3.0)
+    out = []
+    for f in (u, v, w):
+        a = np.zeros(field_shape(cfg, "u"), order="F")
+        a[1:nx + 1, 1:ny + 1, 1:nz + 1] = scale * f
+        a[0] = a[nx]
+        a[nx + 1] = a[1]
+        a[:, 0] = a[:, ny]
+        a[:, ny + 1] = a[:, 1]
+        out.append(a)
+    return tuple(out)
+
+
+def workload_velocity(wl: Workload):
+    """the initial u, v, w of a workload: the seeded solenoidal field, the
+    shear, or rest"""
+    if wl.turbulence is not None:
+        seed, rms, kmax = wl.turbulence
+        return solenoidal_velocity(wl.cfg, seed, rms, kmax)
+    return initial_velocity(wl.cfg, wl.shear_v)
 
 
 def initial_velocity(cfg: IclsConfig, shear_v: float):

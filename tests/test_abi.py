@@ -65,7 +65,10 @@ def test_config_default_matches_python_defaults(lib):
 
 @pytest.mark.parametrize("change,code", [
     (dict(itot=24), "E_CONFIG"),            # radix-2 FFT in x
-    (dict(jtot=48), "E_CONFIG"),            # radix-2 FFT in y
+    (dict(jtot=40), "E_CONFIG"),               # no FFT of that length
+    (dict(itot=40), "E_CONFIG"),
+    (dict(jtot=100), "E_CONFIG"),
+    (dict(itot=8, jtot=384), "E_CONFIG"),      # 384-point y lines tile at least 16 columns            # radix-2 FFT in y
     (dict(itot=8192), "E_CONFIG"),
     (dict(ktot=4), "E_CONFIG"),
     (dict(lmax=0), "E_CONFIG"),
@@ -89,6 +92,20 @@ def test_create_rejects_bad_configs_on_host(lib, change, code):
     assert STATUS_NAMES.get(rc) == code, (change, rc)
     assert not h.value
     assert STATUS_NAMES.get(lib.icls_create(None, C.byref(h))) == "E_ARG"
+
+
+@pytest.mark.parametrize("ni,nj", [(48, 48), (96, 32), (32, 96), (384, 16), (16, 384), (192, 64), (8, 4096)])
+def test_create_accepts_fft_lengths(lib, ni, nj):
+    """lengths with a transform pass the configuration check (without a GPU
+    the allocation that follows fails instead)"""
+    cfg = make_config(itot=ni, jtot=nj, ktot=8, lmax=1)
+    lib.icls_create.argtypes = [C.POINTER(IclsConfig), C.POINTER(C.c_void_p)]
+    lib.icls_create.restype = C.c_int
+    h = C.c_void_p()
+    rc = lib.icls_create(C.byref(cfg), C.byref(h))
+    if rc == 0:
+        lib.icls_destroy(h)
+    assert STATUS_NAMES.get(rc) != "E_CONFIG", (ni, nj, rc)
 
 
 def test_null_context_is_an_argument_error(lib):

@@ -191,11 +191,14 @@ def test_predictor_projection_chain():
 
 
 @pytest.mark.parametrize("ni,nj,nk", [(16, 16, 8), (32, 64, 8), (64, 64, 12), (128, 64, 8), (64, 256, 6),
-                                      (256, 256, 8)])
+                                      (256, 256, 8), (48, 48, 6), (96, 32, 6), (32, 96, 6), (192, 16, 6),
+                                      (16, 384, 6), (384, 16, 6)])
 def test_solver2d_lengths(ni, nj, nk):
     """solver2d on a random right-hand side at line lengths that take the
-    two-level transform (64, 128, 256) and the radix-2 passes (16, 32), x
-    and y: the interior against the oracle's FFT/Thomas solve."""
+    two-level transform (64, 128, 256; 48, 96, 192, 384 with a radix-3
+    factor) and the radix-2 passes (16, 32), x and y: the interior against
+    the oracle's FFT/Thomas solve (a direct DFT at the lengths that are not
+    powers of two)."""
     cfg = make_config(itot=ni, jtot=nj, ktot=nk, lmax=1, lx=ni / 64.0, ly=nj / 64.0, lz=nk / 64.0)
     ls = init_drops(cfg, [(0.5 * cfg.lx, 0.5 * cfg.ly, 0.5 * cfg.lz)], [0.02])
     rng = np.random.default_rng(ni + 7 * nj + 31 * nk)
@@ -253,6 +256,15 @@ def run_pair(wl, nsteps, every=None):
 def test_static_drop_32_multistep():
     wl = static_drop(32, steps=20)
     g, o, _ = run_pair(wl, 20)
+    for name in ("lvset", "u", "v", "w", "pnew"):
+        assert rel_l2(g.download(name), o.download(name)) <= 1e-10, name
+    assert abs(g.volumes()[0][0] - o.volumes()[0][0]) <= 1e-12
+
+
+def test_static_drop_48_multistep():
+    """a grid whose FFT lines (48 = 16 x 3) take the mixed-radix transform"""
+    wl = static_drop(48, steps=6)
+    g, o, _ = run_pair(wl, 6)
     for name in ("lvset", "u", "v", "w", "pnew"):
         assert rel_l2(g.download(name), o.download(name)) <= 1e-10, name
     assert abs(g.volumes()[0][0] - o.volumes()[0][0]) <= 1e-12

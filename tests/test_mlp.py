@@ -221,3 +221,39 @@ def test_fp32_form_with_learned_curvature(trained_net):
     assert np.isfinite(sf.max_vel_at_center())
     assert abs(vf - vp) / vp <= 1e-6
     assert ef < 0.01 * (2.0 / 16)
+
+
+def test_combined_form_96(trained_net):
+    """The combined configuration's kinds of input at 96^3 (FFT lines of
+    16 x 6 points, 12 seeded drops of 7-10 cells, a seeded solenoidal
+    velocity): FP32 with the network curvature against the plain FP64
+    stencil run for 10 steps.  Bounds: finite velocities, per-drop volume
+    within 1e-6 of FP64, drop volumes conserved to 1e-5 over the run in
+    both."""
+    from icls_gpu import CURV_MLP, FP32, Solver, combined, init_drops, workload_velocity
+    from icls_gpu.binding import curvature_stats
+    from icls_gpu.config import IclsConfig
+    wl = combined(96, 12, rmin=0.07, rmax=0.1)
+    ls = init_drops(wl.cfg, wl.centres, wl.radii, wl.all_images)
+    u, v, w = workload_velocity(wl)
+    cf = IclsConfig.from_buffer_copy(wl.cfg)
+    cf.precision = FP32
+    cf.curvature_model = CURV_MLP
+    sp, sf = Solver(wl.cfg), Solver(cf)
+    trained_net.attach(sf)
+    for s in (sp, sf):
+        s.setup(ls, u, v, w)
+        for istep in range(1, 11):
+            s.step(istep, 0)
+    vp, vp0 = sp.volumes()
+    vf, vf0 = sf.volumes()
+    ev, fb = curvature_stats(sf)
+    du = float(np.linalg.norm(sf.download("u") - sp.download("u")) / np.linalg.norm(sp.download("u")))
+    print("\\ncombined 96^3 x 12, 10 steps: volume vs FP64 %.2e, drift FP64 %.2e form %.2e, u rel L2 %.2e, "
+          "max|u| FP64 %.3e form %.3e, fallback %.3f"
+          % (np.max(np.abs(vf - vp) / vp), np.max(np.abs(vp - vp0) / vp0), np.max(np.abs(vf - vf0) / vf0), du,
+             sp.max_vel_at_center(), sf.max_vel_at_center(), fb / max(ev, 1)))
+    assert np.isfinite(sf.max_vel_at_center()) and np.isfinite(sp.max_vel_at_center())
+    assert np.max(np.abs(vf - vp) / vp) <= 1e-6
+    assert np.max(np.abs(vp - vp0) / vp0) <= 1e-5 and np.max(np.abs(vf - vf0) / vf0) <= 1e-5
+    assert ev > 0
