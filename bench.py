@@ -56,8 +56,6 @@ def make_workload(name):
         return static_drop(256)
     if name == "rising_bubble_128":
         return rising_bubble(128)
-    if name == "combined_384_200":  # the combined-form configuration (FFT lengths 384 = 16 x 24)
-        return combined(384, 200)
     if name == "combined_96_12":  # the same kinds of input at 96^3 (16 x 6), 12 drops of 7-10 cells
         return combined(96, 12, rmin=0.07, rmax=0.1)
     raise SystemExit("unknown workload %s" % name)

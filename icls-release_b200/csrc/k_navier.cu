@@ -97,7 +97,11 @@ __device__ __forceinline__ T rhs_u(const Params& p, const FU& U, const FV& V, co
     T RD5 = divz(p, (dwdxp * ma4 - dwdxm * ma3));
     RDu = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rho_u;
   }
-  T RGu = p.TwoD ? TC(0.) : TC(p.iFr) * (TC(1.) - rho_avr / rho_u) * TC(p.g1);
+  // buoyancy iFr (1 - rho_avr/rho) g: skipped (with its divide) where iFr or
+  // this component of g is zero; the term is then an exact +-0, which
+  // changes the sum at most in the sign of an exactly zero result
+  if (p.TwoD || p.iFr == 0. || p.g1 == 0.) return RCu + RDu * TC(p.visc);
+  T RGu = TC(p.iFr) * (TC(1.) - rho_avr / rho_u) * TC(p.g1);
   return (RCu + RDu * TC(p.visc)) + RGu;
 }
 
@@ -131,6 +135,7 @@ __device__ __forceinline__ T rhs_v(const Params& p, const FU& U, const FV& V, co
   T RD4 = divz(p, (dvdzp * ma7 - dvdzm * ma6));
   T RD5 = divz(p, (dwdyp * ma7 - dwdym * ma6));
   T RDv = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rv;
+  if (p.iFr == 0. || p.g2 == 0.) return RCv + RDv * TC(p.visc);  // buoyancy as in rhs_u
   T RGv = TC(p.iFr) * (TC(1.) - rho_avr / rv) * TC(p.g2);
   return (RCv + RDv * TC(p.visc)) + RGv;
 }
@@ -165,6 +170,7 @@ __device__ __forceinline__ T rhs_w(const Params& p, const FU& U, const FV& V, co
   T RD4 = divy(p, (dvdzp * ma7 - dvdzm * ma9));
   T RD5 = divz(p, TC(2.) * (dwdzp * M(0, 0, 1) - dwdzm * M(0, 0, 0)));
   T RDw = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rw;
+  if (p.iFr == 0. || p.g3 == 0.) return RCw + RDw * TC(p.visc);  // buoyancy as in rhs_u
   T RGw = TC(p.iFr) * (TC(1.) - rho_avr / rw) * TC(p.g3);
   return (RCw + RDw * TC(p.visc)) + RGw;
 }
@@ -285,8 +291,8 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 3))
       const T Rv = rhs_v<T>(p, U, V, W, M, rv, rho_avr);
       const T Rw = rhs_w<T>(p, U, V, W, M, rw, rho_avr);
       const T du = ab2_update_v(p, U(0, 0, 0), Ru, ou, ru, PH(1, 0, 0), ph0, 2. * qx - qxo, p.dxi);
-      const T dv = ab2_update_v(p, V(0, 0, 0), Rv, ov, rv, PH(0, 1, 0), ph0, 2. * qy - qyo, p.dyi) -
-                   TC(p.forceytot * p.dt) / rv;
+      T dv = ab2_update_v(p, V(0, 0, 0), Rv, ov, rv, PH(0, 1, 0), ph0, 2. * qy - qyo, p.dyi);
+      if (p.forceytot != 0.) dv = dv - TC(p.forceytot * p.dt) / rv;  // constPoi driving (exact zero otherwise)
       T dw = ab2_update_v(p, W(0, 0, 0), Rw, ow, rw, PH(0, 0, 1), ph0, 2. * qz - qzo, p.dzi);
       duold_out[q] = Ru;
       dvold_out[q] = Rv;
