@@ -65,7 +65,7 @@ __device__ __forceinline__ bool interior(const Params& p, int i, int j, int k) {
 // 15 axial neighbours clip to +-NB, so the test stops at the first that
 // does not (the reference's sums of |clip|-NB <= 0 are zero exactly then).
 template <typename T>
-__global__ void __launch_bounds__(NT) k_tube(Params p, const __grid_constant__ LsBatch B,
+__global__ void __launch_bounds__(NT, 3) k_tube(Params p, const __grid_constant__ LsBatch B,
                                              long long* __restrict__ cnt, int* __restrict__ bbox_lo,
                                              int* __restrict__ bbox_hi) {
   const int ti = task_of(B);
@@ -78,27 +78,66 @@ __global__ void __launch_bounds__(NT) k_tube(Params p, const __grid_constant__ L
   int band = 0;
   int lo[5] = {INT_MAX, INT_MAX, INT_MAX, INT_MAX, INT_MAX};
   int hi[5] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN};
-  if (c.ok) {
-    const int i = c.i, j = c.j;
-    const int hx = p.imax / 2, hy = p.jmax / 2;
-    const int ib = i + hx > p.imax ? i + hx - p.imax : i + hx;
-    const int jb = j + hy > p.jmax ? j + hy - p.jmax : j + hy;
-    // whether the input region holds columns i+d (x) and j+d (y), d = -2..2:
-    // the in-region test of every read, hoisted out of the row loop
-    bool inx[5], iny[5];
-#pragma unroll
-    for (int d = -2; d <= 2; ++d) {
-      inx[d + 2] = span_has(t.vin.xa, t.vin.xn, p.imax, wrapx(p, i + d));
-      iny[d + 2] = span_has(t.vin.ya, t.vin.yn, p.jmax, wrapy(p, j + d));
+  // The band test reads, per row, in-band flags |clip(phi)| != NB of the
+  // tile's columns and a 2-column halo from a shared-memory plane (double
+  // buffered, one barrier per row) and of its own column's rows k-2..k+2
+  // from a register window.  Every flag comes from the input as the
+  // original reads did: the input region's value where it holds the
+  // column (tested on the wrapped column index) and row, else its far-field
+  // value.
+  __shared__ uint8_t F[2][TBY + 4][TBX + 4];
+  const int tx = (int)threadIdx.x, ty = (int)threadIdx.y, tid = tx + TBX * ty;
+  const int X0 = c.X - tx, Y0 = c.Y - ty;  // the tile's first column in region coordinates
+  auto wrapn = [](int v, int n) { v %= n; return v < 0 ? v + n : v; };
+  auto column = [&](int X, int Y, int& iw, int& jw, bool& held) {
+    iw = wrapn(t.r.xa - 1 + X, p.imax) + 1;
+    jw = wrapn(t.r.ya - 1 + Y, p.jmax) + 1;
+    held = span_has(t.vin.xa, t.vin.xn, p.imax, iw) && span_has(t.vin.ya, t.vin.yn, p.jmax, jw);
+  };
+  auto rdo = [&](long long at, bool held, int k) -> T {
+    return (held && k >= t.vin.z0 && k <= t.vin.z1) ? in[at] : ((k < 0 || k > p.k1) ? bggin : bgin);
+  };
+  auto flag = [&](T v) -> uint8_t { return fabs(clipNB(v, NB)) != NB ? 1 : 0; };
+  const long long sz = (long long)p.nLx * p.nLy;
+  // this thread's column (in or out of the region) and its halo cell, if any
+  int iw, jw, hi_w = 0, hj_w = 0, hxs = 0, hys = 0;
+  bool held, hheld = false;
+  column(c.X, c.Y, iw, jw, held);
+  const bool has_halo = tid < 4 * TBY + 4 * TBX;  // 4 halo columns x TBY rows, 4 halo rows x TBX columns
+  if (has_halo) {
+    int xo, yo;
+    if (tid < 4 * TBY) {
+      const int side = tid / TBY;  // columns -2, -1, TBX, TBX+1
+      xo = side < 2 ? side - 2 : TBX + side - 2;
+      yo = tid % TBY;
+    } else {
+      const int u = tid - 4 * TBY, side = u / TBX;  // rows -2, -1, TBY, TBY+1
+      xo = u % TBX;
+      yo = side < 2 ? side - 2 : TBY + side - 2;
     }
-    const bool colin = inx[2] && iny[2];
-    const long long sy = p.nLx, sz = (long long)p.nLx * p.nLy;
-    // phi at storage index `at` (row k, a column the input region holds if
-    // `held`), the input's far-field value where the region does not hold it
-    auto rdo = [&](long long at, bool held, int k) -> T {
-      return (held && k >= t.vin.z0 && k <= t.vin.z1) ? in[at] : ((k < 0 || k > p.k1) ? bggin : bgin);
-    };
-    for (int k = c.ka; k <= c.kb; ++k) {
+    column(X0 + xo, Y0 + yo, hi_w, hj_w, hheld);
+    hxs = xo + 2;
+    hys = yo + 2;
+  }
+  const long long cw = idxL(p, iw, jw, 0), hw = idxL(p, hi_w, hj_w, 0);
+  // z window: flags of this column at rows k-2 .. k+2
+  uint8_t fz[5];
+#pragma unroll
+  for (int d = -2; d <= 1; ++d) fz[d + 3] = flag(rdo(cw + (c.ka + d) * sz, held, c.ka + d));
+  const int i = c.i, j = c.j;
+  const int hx = p.imax / 2, hy = p.jmax / 2;
+  const int ib = i + hx > p.imax ? i + hx - p.imax : i + hx;
+  const int jb = j + hy > p.jmax ? j + hy - p.jmax : j + hy;
+  const bool colin = held;
+  for (int k = c.ka; k <= c.kb; ++k) {
+#pragma unroll
+    for (int d = 0; d < 4; ++d) fz[d] = fz[d + 1];
+    fz[4] = flag(rdo(cw + (k + 2) * sz, held, k + 2));
+    const int buf = k & 1;
+    F[buf][ty + 2][tx + 2] = fz[2];
+    if (has_halo) F[buf][hys][hxs] = flag(rdo(hw + k * sz, hheld, k));
+    __syncthreads();
+    if (c.ok) {
       T val;
       const long long c0 = idxL(p, i, j, k);
       if (!computed(c, t.r, k)) {
@@ -111,17 +150,10 @@ __global__ void __launch_bounds__(NT) k_tube(Params p, const __grid_constant__ L
         else
           val = clipNB(rdo(c0, colin, k), NB);
         if (k >= 1 && k <= p.kmax) {
-          int m = 0;
-          if (fabs(val) < NB) {
-            m = 1;
-          } else {
-            for (int d = -2; d <= 2 && !m; ++d)
-              m = fabs(clipNB(rdo(c0 + d, inx[d + 2] && iny[2], k), NB)) != NB;
-            for (int d = -2; d <= 2 && !m; ++d)
-              m = fabs(clipNB(rdo(c0 + d * sy, inx[2] && iny[d + 2], k), NB)) != NB;
-            for (int d = -2; d <= 2 && !m; ++d)
-              m = fabs(clipNB(rdo(c0 + d * sz, colin, k + d), NB)) != NB;
-          }
+          const uint8_t(&Fp)[TBY + 4][TBX + 4] = F[buf];
+          const int m = (fz[2] | Fp[ty + 2][tx] | Fp[ty + 2][tx + 1] | Fp[ty + 2][tx + 3] | Fp[ty + 2][tx + 4] |
+                         Fp[ty][tx + 2] | Fp[ty + 1][tx + 2] | Fp[ty + 3][tx + 2] | Fp[ty + 4][tx + 2] | fz[0] |
+                         fz[1] | fz[3] | fz[4]) != 0;
           t.mask[idxI(p, i, j, k)] = (uint8_t)m;
           band += m;
         }

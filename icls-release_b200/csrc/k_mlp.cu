@@ -338,20 +338,13 @@ __device__ __forceinline__ void stage_rows(unsigned char* dst, const __nv_bfloat
   }
 }
 
-// row t of the tile: the sample's 32 FP32 inputs as BF16 hi (k 0..31) and
-// lo (k 32..63); zeros past the end
-__device__ __forceinline__ void stage_inputs(unsigned char* act, const float* __restrict__ x, int t) {
+// row t of the tile: the sample's 32 FP32 inputs (from registers; zeros
+// past the end) as BF16 hi (k 0..31) and lo (k 32..63)
+__device__ __forceinline__ void stage_inputs_regs(unsigned char* act, const float4 (&xv)[kIn / 4], int t) {
 #pragma unroll
   for (int c = 0; c < kIn / 8; ++c) {
-    float v[8];
-    if (x) {
-      const float4 a = *reinterpret_cast<const float4*>(x + 8 * c);
-      const float4 b = *reinterpret_cast<const float4*>(x + 8 * c + 4);
-      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-    } else {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) v[q] = 0.f;
-    }
+    const float4 a = xv[2 * c], b = xv[2 * c + 1];
+    const float v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
     float hi[8], lo[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -383,8 +376,10 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t lane_addr, const float*
 }
 
 // The forward pass over samples 0..n-1 of X (FP32 [n][32], 16-byte
-// aligned), tiles blockIdx.x, blockIdx.x + gridDim.x, ...; out(s, y) takes
-// each sample's output.  All 128 threads call it.
+// aligned), tiles blockIdx.x, blockIdx.x + gridDim.x, ...; out.begin(s,
+// live) is called when a tile starts (what the output step will need can be
+// read then) and out(s, y) takes each sample's output.  The next tile's
+// inputs are read while the current tile runs.  All 128 threads call it.
 template <class Out>
 __device__ __forceinline__ void infer_tiles(const Net& net, const float* __restrict__ X, long long n, Out& out,
                                             int* __restrict__ err) {
@@ -416,9 +411,18 @@ __device__ __forceinline__ void infer_tiles(const Net& net, const float* __restr
   const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
   uint32_t phase = 0;
   bool ok = true;
+  float4 xv[kIn / 4];
+  auto load_x = [&](long long s) {
+#pragma unroll
+    for (int q = 0; q < kIn / 4; ++q)
+      xv[q] = s < n ? reinterpret_cast<const float4*>(X + s * kIn)[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+  };
+  load_x((long long)blockIdx.x * kRows + t);
   for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const long long s = tile * kRows + t;
-    stage_inputs(sm + SI_ACT, s < n ? X + s * kIn : nullptr, t);
+    out.begin(s, s < n);
+    stage_inputs_regs(sm + SI_ACT, xv, t);
+    load_x(s + (long long)gridDim.x * kRows);  // in flight during this tile
     ok &= umma::tile_gemm(sm + SI_ACT, sm + SI_W1, kH1, kIn2, tmem, &bar, phase);
     hidden_epilogue(lane_addr, par + PB1, kH1, sm + SI_ACT, t);
     ok &= umma::tile_gemm(sm + SI_ACT, sm + SI_W2, kH2, kH1, tmem, &bar, phase);
@@ -445,6 +449,7 @@ __device__ __forceinline__ void infer_tiles(const Net& net, const float* __restr
 
 struct StoreOut {
   float* y;
+  __device__ void begin(long long, bool) {}
   __device__ void operator()(long long s, float v) const { y[s] = v; }
 };
 
@@ -799,11 +804,16 @@ struct ApplyOut {
   const MlpCell* __restrict__ rec;
   double tol;
   unsigned long long ev, fb;
-  __device__ void operator()(long long s, float y) {
-    const MlpCell r = rec[s];
+  MlpCell r;  // this thread's cell of the current tile and its stencil curvature
+  double kp;
+  __device__ void begin(long long s, bool live) {
+    if (!live) return;
+    r = rec[s];
+    kp = (double)mT<T>(B.t[r.q].out)[idxC(p, r.i, r.j, r.k)];
+  }
+  __device__ void operator()(long long, float y) {
     T* out = mT<T>(B.t[r.q].out);
     const double dz = p.dz;
-    const double kp = (double)out[idxC(p, r.i, r.j, r.k)];
     double km = kp + (double)y / dz;
     ++ev;
     if (fabs(kp) * dz > 2. / 3. || fabs(km - kp) * dz > tol) {
@@ -827,7 +837,7 @@ __global__ void __launch_bounds__(128, 2) k_mlp_curv(Net net, const float* __res
                                                      const MlpCell* __restrict__ rec, double tol,
                                                      unsigned long long* __restrict__ stats, int* __restrict__ err) {
   const long long n = min(*count, cap);
-  ApplyOut<T> o{p, B, rec, tol, 0ull, 0ull};
+  ApplyOut<T> o{p, B, rec, tol, 0ull, 0ull, MlpCell{0, 0, 0, 0}, 0.};
   infer_tiles(net, X, n, o, err);
   unsigned long long ev = o.ev, fb = o.fb;
   for (int d = 16; d > 0; d >>= 1) {
