@@ -120,10 +120,16 @@ __global__ void __launch_bounds__(NT, 3) k_tube(Params p, const __grid_constant_
     hys = yo + 2;
   }
   const long long cw = idxL(p, iw, jw, 0), hw = idxL(p, hi_w, hj_w, 0);
-  // z window: flags of this column at rows k-2 .. k+2
+  // z window: flags of this column at rows k-2 .. k+2 (slots 1..4 hold rows
+  // ka-2..ka+1; each row shifts down one slot and reads row k+2 into slot 4)
   uint8_t fz[5];
+  fz[0] = 0;
 #pragma unroll
   for (int d = -2; d <= 1; ++d) fz[d + 3] = flag(rdo(cw + (c.ka + d) * sz, held, c.ka + d));
+  // the values a row turns into flags (row k+2 of this column, row k of the
+  // halo cell) were read one row earlier, so a barrier waits on no fresh load
+  T nz = rdo(cw + (c.ka + 2) * sz, held, c.ka + 2);
+  T nh = has_halo ? rdo(hw + c.ka * sz, hheld, c.ka) : bgin;
   const int i = c.i, j = c.j;
   const int hx = p.imax / 2, hy = p.jmax / 2;
   const int ib = i + hx > p.imax ? i + hx - p.imax : i + hx;
@@ -132,10 +138,14 @@ __global__ void __launch_bounds__(NT, 3) k_tube(Params p, const __grid_constant_
   for (int k = c.ka; k <= c.kb; ++k) {
 #pragma unroll
     for (int d = 0; d < 4; ++d) fz[d] = fz[d + 1];
-    fz[4] = flag(rdo(cw + (k + 2) * sz, held, k + 2));
+    fz[4] = flag(nz);
+    nz = rdo(cw + (k + 3) * sz, held, k + 3);
     const int buf = k & 1;
     F[buf][ty + 2][tx + 2] = fz[2];
-    if (has_halo) F[buf][hys][hxs] = flag(rdo(hw + k * sz, hheld, k));
+    if (has_halo) {
+      F[buf][hys][hxs] = flag(nh);
+      nh = rdo(hw + (k + 1) * sz, hheld, k + 1);
+    }
     __syncthreads();
     if (c.ok) {
       T val;
