@@ -217,7 +217,7 @@ constexpr int ab2_smem() {
   return (int)(4 * MRING * MSY * MSX * sizeof(T) + 2 * MRING * MPY * MPX * sizeof(double));
 }
 template <typename T>
-__global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 3))
+__global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
     k_ab2(Params p, MomArgs a, T* __restrict__ dudt, T* __restrict__ dvdt, T* __restrict__ dwdt,
           T* __restrict__ duold_out, T* __restrict__ dvold_out, T* __restrict__ dwold_out, int kc, int nch) {
   extern __shared__ __align__(16) unsigned char ab2_dyn[];
@@ -663,7 +663,9 @@ T* fp(double* q) { return reinterpret_cast<T*>(q); }
 
 template <typename T>
 void ab2_launch(Ctx& c, const MomArgs& a, int o) {
-  const int kc = 16, nch = std::max(1, c.P.kmax / kc);
+  // rows per block: 32 for the FP32 form (four blocks per SM, shorter
+  // ring prologues), 16 for FP64 (two blocks per SM, more blocks per wave)
+  const int kc = sizeof(T) == 8 ? 16 : 32, nch = std::max(1, c.P.kmax / kc);
   const dim3 grid((unsigned)((c.P.imax + MX - 1) / MX), (unsigned)((c.P.jmax + MY - 1) / MY), (unsigned)nch);
   static unsigned attr = 0;  // devices this instance's shared-memory limit is raised on
   int dev = 0;
