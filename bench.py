@@ -105,7 +105,7 @@ MLP_FLOPS_PER_CELL = 2 * (128 * 64 + 128 * 128 + 64 * 128)
 # the launch on the 128^3 workload (profiles/k_ab2_*_multi_drop_128_12.md),
 # times the 8x cells (the traffic equals the algorithmic bytes there, so it
 # scales with the cells)
-TRAFFIC = {("ab2", False): 8 * (318.122240e6 + 86.022144e6), ("ab2", True): 8 * (229.303552e6 + 37.673984e6)}
+TRAFFIC = {("ab2", False): 8 * (318.163968e6 + 83.975936e6), ("ab2", True): 8 * (226.014976e6 + 37.924352e6)}
 
 
 def alg_bytes_per_launch(name, cfg, stats, f32=False):
