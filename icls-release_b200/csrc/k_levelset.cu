@@ -194,27 +194,12 @@ __global__ void __launch_bounds__(NT, 3) k_tube(Params p, const __grid_constant_
 }
 
 // ------------------------------------------------------- advection RHS
-// The 19 values of the axial stencil at storage index c (the centre and
-// offsets -3..3 along each axis), read before anything is decided so that
-// they are in flight together with the row's other operands.
+// The 19 values of the axial stencil of a cell (the centre and offsets
+// -3..3 along each axis).
 template <typename T>
 struct Axial19 {
   T c, x[7], y[7], z[7];  // x[d + 3] = phi at offset d along x (x[3] == c), likewise y, z
 };
-template <typename T>
-__device__ __forceinline__ Axial19<T> read_axial(const T* __restrict__ phi, long long c, long long sy, long long sz) {
-  Axial19<T> a;
-  a.c = phi[c];
-#pragma unroll
-  for (int d = -3; d <= 3; ++d) {
-    if (d == 0) continue;
-    a.x[d + 3] = phi[c + d];
-    a.y[d + 3] = phi[c + d * sy];
-    a.z[d + 3] = phi[c + d * sz];
-  }
-  a.x[3] = a.y[3] = a.z[3] = a.c;
-  return a;
-}
 
 // dfdt of HOUC5_nb (hyperPDE.f90:397-495) or WENO5_nb (503-800) at row k
 // from its axial stencil S
@@ -292,24 +277,6 @@ __device__ __forceinline__ T adv_rhs(const Params& p, const Axial19<T>& S, T vu,
 #undef PZ
   return (udfdx + vdfdy) + wdfdz;
 }
-// One stage value at row k of column (I,J): every operand (phi0, phis' axial
-// stencil, the band flag and the velocities) is read first, so one memory
-// latency is exposed per row; the stencil result is used on band cells only.
-template <int SCHEME, typename T>
-__device__ __forceinline__ T adv_val(const Params& p, int stage1, const T* phi0, const T* phis, T a, T b, T fdt,
-                                     const T* __restrict__ vu, const T* __restrict__ vv, const T* __restrict__ vw,
-                                     const uint8_t* __restrict__ mask, int I, int J, int k) {
-  const long long n = idxL(p, I, J, k);
-  const T f0 = phi0[n];
-  if (!(k >= 1 && k <= p.kmax)) return stage1 ? f0 : a * f0 + b * phis[n];
-  const long long q = idxI(p, I, J, k);
-  const uint8_t m = mask[q];
-  const T u = vu[q], v = vv[q], w = vw[q];
-  const Axial19<T> S = read_axial(phis, n, (long long)p.nLx, (long long)p.nLx * p.nLy);
-  T val = stage1 ? f0 : a * f0 + b * S.c;
-  if (m) val = val + fdt * adv_rhs<SCHEME>(p, S, u, v, w, k);
-  return val;
-}
 template <int SCHEME, typename T>
 __global__ void __launch_bounds__(NT, 3) k_adv_stage(Params p, const __grid_constant__ LsBatch B, int stage1,
                                                      double a_, double bb_, double fdt_, const T* __restrict__ vu,
@@ -319,15 +286,32 @@ __global__ void __launch_bounds__(NT, 3) k_adv_stage(Params p, const __grid_cons
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
   if (!c.ok) return;
   const T a = TC(a_), bb = TC(bb_), fdt = TC(fdt_);
-  const T* phi0 = cT<T>(t.phi0);
-  const T* phis = cT<T>(t.phis);
-  T* out = mT<T>(t.out);
   const int i = c.i, j = c.j;
+  // This column's storage, and that of its periodic images in out, from
+  // row 0; row k is `k * sz` further (32-bit offsets within one array).
+  const int sy = p.nLx, sz = p.nLx * p.nLy, szI = p.imax * p.jmax;
+  const long long col = idxL(p, i, j, 0);
+  const T* f0c = cT<T>(t.phi0) + col;
+  const T* fsc = cT<T>(t.phis) + col;
+  T* out = mT<T>(t.out);
+  T* const o0 = out + col;
+  const int ii = image_of<3>(i, p.imax), jj = image_of<3>(j, p.jmax);
+  T* const o1 = ii != INT_MIN ? out + idxL(p, ii, j, 0) : nullptr;
+  T* const o2 = jj != INT_MIN ? out + idxL(p, i, jj, 0) : nullptr;
+  T* const o3 = (ii != INT_MIN && jj != INT_MIN) ? out + idxL(p, ii, jj, 0) : nullptr;
+  const long long qc = idxI(p, i, j, 1);  // row k at qc + (k - 1) * szI
+  auto put = [&](int k, T v) {
+    const int o = k * sz;
+    o0[o] = v;
+    if (o1) o1[o] = v;
+    if (o2) o2[o] = v;
+    if (o3) o3[o] = v;
+  };
   T v1 = TC(0.), v2 = TC(0.), vkm = TC(0.), vk = TC(0.);
   bool wall0 = false;
   for (int k = c.ka; k <= c.kb; ++k) {
     if (!computed(c, t.r, k)) {
-      putL(p, out, i, j, k, (k < 0 || k > p.k1) ? TC(t.bgg) : TC(t.bg));
+      put(k, (k < 0 || k > p.k1) ? TC(t.bgg) : TC(t.bg));
       continue;
     }
     if (k == 0) {  // written once rows 1 and 2 are known
@@ -338,14 +322,38 @@ __global__ void __launch_bounds__(NT, 3) k_adv_stage(Params p, const __grid_cons
     if (k == p.k1) {
       val = TC(2.) * vk - vkm;
     } else {
-      val = adv_val<SCHEME>(p, stage1, phi0, phis, a, bb, fdt, vu, vv, vw, t.mask, i, j, k);
+      // every operand (phi0, phis' axial stencil, the band flag and the
+      // velocities) is read first, so one memory latency is exposed per row;
+      // the stencil result is used on band cells only
+      const int o = k * sz;
+      const T f0 = f0c[o];
+      if (!(k >= 1 && k <= p.kmax)) {
+        val = stage1 ? f0 : a * f0 + bb * fsc[o];
+      } else {
+        const long long q = qc + (long long)(k - 1) * szI;
+        const uint8_t m = t.mask[q];
+        const T u = vu[q], v = vv[q], w = vw[q];
+        const T* f = fsc + o;
+        Axial19<T> S;
+        S.c = f[0];
+#pragma unroll
+        for (int d = -3; d <= 3; ++d) {
+          if (d == 0) continue;
+          S.x[d + 3] = f[d];
+          S.y[d + 3] = f[d * sy];
+          S.z[d + 3] = f[d * sz];
+        }
+        S.x[3] = S.y[3] = S.z[3] = S.c;
+        val = stage1 ? f0 : a * f0 + bb * S.c;
+        if (m) val = val + fdt * adv_rhs<SCHEME>(p, S, u, v, w, k);
+      }
       if (k == 1) v1 = val;
       if (k == 2) v2 = val;
       if (k == p.kmax - 1) vkm = val;
       if (k == p.kmax) vk = val;
     }
-    putL(p, out, i, j, k, val);
-    if (k == 2 && wall0) putL(p, out, i, j, 0, TC(2.) * v1 - v2);
+    put(k, val);
+    if (k == 2 && wall0) put(0, TC(2.) * v1 - v2);
   }
 }
 
