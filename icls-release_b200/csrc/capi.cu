@@ -191,6 +191,7 @@ int allocate(Ctx& c) {
   AL(c.zpiv, (size_t)(P.imax / 2 + 1) * (P.jmax / 2 + 1) * P.kmax);  // pivots per distinct (xrt, yrt)
   AL(c.tri_a, (size_t)P.kmax + 1); AL(c.tri_b, (size_t)P.kmax + 1); AL(c.tri_c, (size_t)P.kmax + 1);
   AL(c.partials, (size_t)kRedBlocks * std::max(P.L, 4) + (size_t)P.imax + 8);
+  AL(c.diag, (size_t)7 * kRedBlocks + 8);
   AL(c.lpartials, (size_t)kRedBlocks);
   AL(c.dsc, 1);
   AL(c.dvol, (size_t)P.L); AL(c.dvol0, (size_t)P.L); AL(c.dmaxchk, (size_t)P.L);
@@ -243,7 +244,8 @@ void release(Ctx& c) {
   for (double* f : {c.u, c.v, c.w, c.pnew, c.pold, c.p, c.dudt, c.dvdt, c.dwdt, c.px, c.py, c.pz, c.pxold,
                     c.pyold, c.pzold, c.pjump, c.miu, c.rho, c.jiemian, c.curv, c.dheav, c.kappa,
                     c.rho_u, c.rho_v, c.rho_w, c.ucc, c.vcc, c.wcc, c.nrm_m, c.ulc, c.vlc, c.wlc, c.spec,
-                    c.xyrt, c.zpiv, c.tri_a, c.tri_b, c.tri_c, c.partials, c.dvol, c.dvol0, c.dmaxchk, c.hpart})
+                    c.xyrt, c.zpiv, c.tri_a, c.tri_b, c.tri_c, c.partials, c.diag, c.dvol, c.dvol0, c.dmaxchk,
+                    c.hpart})
     if (f) cudaFree(f);
   for (int h = 0; h < 2; ++h) {
     if (c.duold[h]) cudaFree(c.duold[h]);
@@ -1148,6 +1150,22 @@ int icls_max_vel_at_center(icls_ctx* h, double* vel_max) {
   if (rc) return rc;
   *vel_max = h->c.h_sc->velmax;
   return ICLS_OK;
+}
+
+// disp_cg and disp_speed (write_vtk.f90:438-566) of drop l: sums on the
+// device, the two quotients here
+int icls_disp(icls_ctx* h, int l, double* cg, double* vel) {
+  if (!h || !cg || !vel) return ICLS_E_ARG;
+  LARG(h, l);
+  Ctx& c = h->c;
+  launch_disp(c, l - 1);
+  double sm[7];
+  CK(cudaMemcpyAsync(sm, c.diag + 7 * kRedBlocks, sizeof(sm), cudaMemcpyDeviceToHost, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  for (int q = 0; q < 3; ++q) cg[q] = sm[1 + q] / sm[0];
+  const double vol = ((c.cfg.lx * c.cfg.ly) * c.cfg.lz) * c.init_volume_h[l - 1];
+  for (int q = 0; q < 3; ++q) vel[q] = sm[4 + q] / vol;
+  return check_launch();
 }
 
 int icls_chkdiv(icls_ctx* h, int istep, double* divtot, double* divmax, int ijk[3]) {

@@ -114,6 +114,7 @@ struct Ctx {
   double* tri_a = nullptr, *tri_b = nullptr, *tri_c = nullptr;  // (kmax)
   // reductions and device scalars
   double* partials = nullptr;           // kRedBlocks * max(L,4)
+  double* diag = nullptr;               // disp partials: 7 * kRedBlocks, then the 7 sums
   long long* lpartials = nullptr;
   DevScalars* dsc = nullptr;
   double* dvol = nullptr;               // volume(1:L)
@@ -226,5 +227,6 @@ void launch_nan_probe(Ctx& c);
 // Poisson (k_poisson.cu)
 void poisson_setup(Ctx& c);
 void launch_solver2d(Ctx& c, int write_halos);
+void launch_disp(Ctx& c, int l);
 
 }  // namespace icls

@@ -549,6 +549,55 @@ __device__ __forceinline__ T dirac_trig(const Params& p, T phi, T eps) {
   return TC(0.);
 }
 
+// disp_cg and disp_speed (write_vtk.f90:438-566) of one drop: over the
+// interior cells with phi <= 1.5 dz, the count, the sums of the cell-centre
+// coordinates (i - 1/2)/dxi, ... and of ucc dx dy dz (1 - H), ... (H the
+// 'trig' Heaviside of the drop).  Warp w of the grid takes the rows (j,k)
+// w, w + W, ...; per-block partials part[7 * block + q] in a fixed order.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_disp(Params p, const T* __restrict__ phi,
+                                                      const T* __restrict__ ucc, const T* __restrict__ vcc,
+                                                      const T* __restrict__ wcc, double* __restrict__ part) {
+  double s[7] = {0., 0., 0., 0., 0., 0., 0.};
+  const int rows = p.jmax * p.kmax;
+  const int W = (int)((gridDim.x * kRedThreads) >> 5);
+  const int lane = threadIdx.x & 31;
+  const T lim = TC(1.5 * p.dz), eps = TC(1.5 * p.dz);
+  for (int r = (int)((blockIdx.x * kRedThreads + threadIdx.x) >> 5); r < rows; r += W) {
+    const int j = 1 + r % p.jmax, k = 1 + r / p.jmax;
+    const double cy = (j - 0.5) / p.dyi, cz = (k - 0.5) / p.dzi;
+    for (int i = 1 + lane; i <= p.imax; i += 32) {
+      const T f = phi[idxL(p, i, j, k)];
+      if (f <= lim) {
+        const long long q = idxI(p, i, j, k);
+        const double g = 1. - (double)heav_trig(p, f, eps);
+        s[0] += 1.;
+        s[1] += (i - 0.5) / p.dxi;
+        s[2] += cy;
+        s[3] += cz;
+        s[4] += ((((double)ucc[q] * p.dx) * p.dy) * p.dz) * g;
+        s[5] += ((((double)vcc[q] * p.dx) * p.dy) * p.dz) * g;
+        s[6] += ((((double)wcc[q] * p.dx) * p.dy) * p.dz) * g;
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 7; ++q) {
+    const double b = block_sum<double, kRedThreads>(s[q]);
+    if (threadIdx.x == 0) part[7 * blockIdx.x + q] = b;
+  }
+}
+__global__ void __launch_bounds__(kRedThreads) k_disp_final(const double* __restrict__ part, int nblk,
+                                                            double* __restrict__ out) {
+#pragma unroll 1
+  for (int q = 0; q < 7; ++q) {
+    double s = 0.;
+    for (int b = threadIdx.x; b < nblk; b += kRedThreads) s += part[7 * b + q];
+    s = block_sum<double, kRedThreads>(s);
+    if (threadIdx.x == 0) out[q] = s;
+  }
+}
+
 // jiemian = min(jiemian, H_l) over the tasks' computed cells (shape-C
 // regions) and per-tile sums of H_l over their interior cells
 // (misc.f90:110-141), the sums in FP64.  jiemian starts at 1, the
@@ -1000,6 +1049,16 @@ void launch_fill(Ctx& c, double* a, long long n, double v, bool tfield) {
 }
 
 // outside/ntiles: per drop (null: every drop swept its whole grid)
+void launch_disp(Ctx& c, int l) {
+  Scope sc_(c.prof, c.s, "disp", 2);
+  BY_FORM(c, (k_disp<float><<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, reinterpret_cast<const float*>(c.lv[l]),
+                                                                  reinterpret_cast<const float*>(c.ucc),
+                                                                  reinterpret_cast<const float*>(c.vcc),
+                                                                  reinterpret_cast<const float*>(c.wcc), c.diag)),
+          (k_disp<double><<<kRedBlocks, kRedThreads, 0, c.s>>>(c.P, c.lv[l], c.ucc, c.vcc, c.wcc, c.diag)));
+  k_disp_final<<<1, kRedThreads, 0, c.s>>>(c.diag, kRedBlocks, c.diag + 7 * kRedBlocks);
+}
+
 void launch_materials_final(Ctx& c, const double* outside, const int* ntiles) {
   Scope sc_(c.prof, c.s, "materials_final", 2);
   PerDrop o;

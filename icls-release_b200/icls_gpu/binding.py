@@ -47,6 +47,7 @@ _SIGS = {
     "pressure_update": [_I, _I],
     "average_vel_at_center": [],
     "max_vel_at_center": [_DP],
+    "disp": [_I, _DP, _DP],
     "chkdiv": [_I, _DP, _DP, _IP],
     "chkdt": [_DP],
     "ipot": [_DP],
@@ -243,6 +244,12 @@ class Solver:
         x = C.c_double()
         self._call("max_vel_at_center", C.byref(x))
         return x.value
+
+    def disp(self, l: int = 1):
+        """disp_cg and disp_speed of drop l: (centroid[3], velocity[3])"""
+        cg, vel = np.zeros(3), np.zeros(3)
+        self._call("disp", l, cg.ctypes.data_as(_DP), vel.ctypes.data_as(_DP))
+        return cg, vel
 
     def chkdiv(self, istep: int, raise_on_error: bool = True):
         tot, mx = C.c_double(), C.c_double()

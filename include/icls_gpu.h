@@ -157,6 +157,9 @@ int icls_bounduvw(icls_ctx* ctx, int field_id_u);           /* bound.f90:15-177;
 int icls_pressure_update(icls_ctx* ctx, int istep, int begin); /* main.f90:164-185  */
 int icls_average_vel_at_center(icls_ctx* ctx);              /* misc.f90:587-604     */
 int icls_max_vel_at_center(icls_ctx* ctx, double* vel_max); /* misc.f90:610-636     */
+/* disp_cg, disp_speed (write_vtk.f90:438-566): drop l's centroid of its cells with
+ * phi <= 1.5dz, cg[3], and velocity sum ucc dV (1 - H_l) / (lx ly lz init_volume(l)), vel[3] */
+int icls_disp(icls_ctx* ctx, int l, double cg[3], double vel[3]);
 /* Returns ICLS_E_DIVERGENCE when max|div| > 1e-12 and istep != 0.        */
 int icls_chkdiv(icls_ctx* ctx, int istep, double* divtot, double* divmax,
                 int ijk[3]);                                /* chkdiv.f90:10-90     */

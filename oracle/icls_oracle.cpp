@@ -473,6 +473,39 @@ struct ora_ctx {
           wccnew(i, j, k) = (wnew(i, j, k - 1) + wnew(i, j, k)) / 2.;
         }
   }
+  // disp_cg and disp_speed (write_vtk.f90:438-566) of drop l (0-based), one
+  // rank: the centroid of the cells with lvset <= 1.5dz and their velocity
+  // integral ucc dx dy dz (1 - hnew_mls) over lx ly lz init_volume(l)
+  void disp(int l, double* cg, double* vel) {
+    double counter = 0., xd = 0., yd = 0., zd = 0., ud = 0., vd = 0., wd = 0.;
+    for (int k = 1; k <= kmax; ++k) {
+      const double coorz = (k - 0.5) / dzi;
+      for (int j = 1; j <= jmax; ++j) {
+        const double coory = 0. + (j - 0.5) / dyi;
+        for (int i = 1; i <= imax; ++i) {
+          const double coorx = 0. + (i - 0.5) / dxi;
+          if (lvset[l](i, j, k) <= 1.5 * dz) {
+            counter = counter + 1.;
+            xd = xd + coorx;
+            yd = yd + coory;
+            zd = zd + coorz;
+            const double g = 1. - hnew_mls[l](i, j, k);
+            ud = ud + uccnew(i, j, k) * dx * dy * dz * g;
+            vd = vd + vccnew(i, j, k) * dx * dy * dz * g;
+            wd = wd + wccnew(i, j, k) * dx * dy * dz * g;
+          }
+        }
+      }
+    }
+    cg[0] = xd / counter;
+    cg[1] = yd / counter;
+    cg[2] = zd / counter;
+    const double v0 = lx * ly * lz * init_volume[l];
+    vel[0] = ud / v0;
+    vel[1] = vd / v0;
+    vel[2] = wd / v0;
+  }
+
   // max_vel_at_center (misc.f90:610-636)
   double max_vel_at_center() {
     double m = 0; bool first = true;
@@ -1450,6 +1483,11 @@ int ora_bounduvw(ora_ctx* o, int id) {
 int ora_pressure_update(ora_ctx* o, int istep, int begin) { NEED_INIT; o->pressure_update(istep, begin); return ICLS_OK; }
 int ora_average_vel_at_center(ora_ctx* o) { o->average_vel_at_center(); return ICLS_OK; }
 int ora_max_vel_at_center(ora_ctx* o, double* vm) { *vm = o->max_vel_at_center(); return ICLS_OK; }
+int ora_disp(ora_ctx* o, int l, double* cg, double* vel) {
+  if (!o || !cg || !vel || l < 1 || l > o->L) return ICLS_E_ARG;
+  o->disp(l - 1, cg, vel);
+  return ICLS_OK;
+}
 int ora_chkdiv(ora_ctx* o, int istep, double* dt_, double* dm, int ijk[3]) { return o->chkdiv(istep, dt_, dm, ijk); }
 int ora_chkdt(ora_ctx* o, double* dtmax) { *dtmax = o->chkdt(); return ICLS_OK; }
 int ora_ipot(ora_ctx* o, double* dmin) {

@@ -44,6 +44,7 @@ int ora_bounduvw(ora_ctx* ctx, int field_id_u);
 int ora_pressure_update(ora_ctx* ctx, int istep, int begin);
 int ora_average_vel_at_center(ora_ctx* ctx);
 int ora_max_vel_at_center(ora_ctx* ctx, double* vel_max);
+int ora_disp(ora_ctx* ctx, int l, double cg[3], double vel[3]);
 int ora_chkdiv(ora_ctx* ctx, int istep, double* divtot, double* divmax, int ijk[3]);
 int ora_chkdt(ora_ctx* ctx, double* dtmax);
 int ora_ipot(ora_ctx* ctx, double* dmin);

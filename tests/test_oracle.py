@@ -21,7 +21,7 @@ from conftest import rel_l2
 
 from oracle.oracle import Oracle, set_threads, vrfftb, vrfftf
 from icls_gpu import (HOUC5, WENO5, field_shape, init_drops, initial_velocity, make_config,
-                      static_drop)
+                      rising_bubble, static_drop)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 set_threads(min(8, os.cpu_count() or 1))
@@ -140,6 +140,27 @@ def test_static_drop_divergence_free_and_conserving():
     tot, mx, ijk, rc = o.chkdiv(5, raise_on_error=False)
     assert rc == 0 and mx < 1e-12
     assert abs(o.volumes()[0][0] - v0) / v0 < 1e-4
+
+
+def test_disp_diagnostics_known_answers():
+    """disp_cg / disp_speed (write_vtk.f90:438-566): a drop centred in the box
+    has its centroid at the centre and no velocity at rest; a rising bubble
+    (gravity along -z, lighter than its surroundings) moves up."""
+    wl = static_drop(32, steps=1)
+    ls = init_drops(wl.cfg, wl.centres, wl.radii, wl.all_images)
+    o = Oracle(wl.cfg)
+    o.setup(ls, *initial_velocity(wl.cfg, 0.0))
+    cg, vel = o.disp(1)
+    assert np.max(np.abs(cg - 0.5)) <= 1e-12
+    assert np.max(np.abs(vel)) == 0.0
+    wb = rising_bubble(32, steps=3)
+    lb = init_drops(wb.cfg, wb.centres, wb.radii, wb.all_images)
+    b = Oracle(wb.cfg)
+    b.setup(lb, *initial_velocity(wb.cfg, 0.0))
+    for s in range(1, 4):
+        b.step(s, 0)
+    cg, vel = b.disp(1)
+    assert abs(cg[2] - 0.5) <= 1e-3 and vel[2] > 0.0 and abs(vel[0]) < 1e-3 * vel[2]
 
 
 def test_oracle_regression_record():
