@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "ctx.h"
@@ -876,8 +877,9 @@ int icls_status_string(int code, char* buf, int n) {
                                 "NaN in vnew(1,1,1)", "max divergence above 1e-12", "bad argument",
                                 "device allocation failed", "context not initialised",
                                 "option not built into this library",
-                                "grid larger than the no-allocation divergence check handles"};
-  const char* s = (code >= 0 && code <= 9) ? names[code] : "unknown status";
+                                "grid larger than the no-allocation divergence check handles",
+                                "checkpoint file could not be written or read"};
+  const char* s = (code >= 0 && code <= 10) ? names[code] : "unknown status";
   if (buf && n > 0) {
     std::strncpy(buf, s, (size_t)n - 1);
     buf[n - 1] = 0;
@@ -1150,6 +1152,150 @@ int icls_max_vel_at_center(icls_ctx* h, double* vel_max) {
   if (rc) return rc;
   *vel_max = h->c.h_sc->velmax;
   return ICLS_OK;
+}
+
+// ------------------------------------------------------------ checkpoints
+namespace {
+// the fields of loadflds (loadd.f90:66-103) in file order: (field id, drop)
+std::vector<std::pair<int, int>> checkpoint_fields(const Ctx& c) {
+  std::vector<std::pair<int, int>> f = {{ICLS_F_U, 1}, {ICLS_F_V, 1}, {ICLS_F_W, 1}, {ICLS_F_PNEW, 1}};
+  for (int l = 1; l <= c.P.L; ++l) f.push_back({ICLS_F_LVSET, l});
+  f.push_back({ICLS_F_JIEMIAN, 1});
+  return f;
+}
+// the fields of path.hist, whole arrays (halos included): the AB2 and
+// pressure history, then the level sets again, whose outer wall-normal
+// ghost layers (k = -2, -1, k1+1, k1+2) are carried from step to step
+// (boundsls refills only k = 0 and k1) and so are not implied by the interior
+std::vector<std::pair<int, int>> hist_fields(const Ctx& c) {
+  std::vector<std::pair<int, int>> f;
+  for (int id : {ICLS_F_DUOLD, ICLS_F_DVOLD, ICLS_F_DWOLD, ICLS_F_POLD, ICLS_F_PX, ICLS_F_PY, ICLS_F_PZ,
+                 ICLS_F_PXOLD, ICLS_F_PYOLD, ICLS_F_PZOLD})
+    f.push_back({id, 1});
+  for (int l = 1; l <= c.P.L; ++l) f.push_back({ICLS_F_LVSET, l});
+  return f;
+}
+const char kHistMagic[8] = {'I', 'C', 'L', 'S', 'H', 'S', 'T', '1'};
+
+struct Shape3 {
+  int lo[3], hi[3];
+  long long n() const { return (long long)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1); }
+  long long at(int i, int j, int k) const {
+    return (i - lo[0]) + (long long)(hi[0] - lo[0] + 1) * ((j - lo[1]) + (long long)(hi[1] - lo[1] + 1) * (k - lo[2]));
+  }
+};
+Shape3 shape_of(const icls_ctx* h, int id) {
+  Shape3 s;
+  icls_field_bounds(h, id, s.lo, s.hi);
+  return s;
+}
+}  // namespace
+
+int icls_write_checkpoint(icls_ctx* h, const char* path, int nr, int history) {
+  NEED(h);
+  if (!path) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  const int I = c.P.imax, J = c.P.jmax, K = c.P.kmax;
+  std::vector<double> full, in((size_t)I * J * K);
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return ICLS_E_IO;
+  int rc = ICLS_OK;
+  for (const auto& fl : checkpoint_fields(c)) {
+    const Shape3 sh = shape_of(h, fl.first);
+    full.assign((size_t)sh.n(), 0.);
+    rc = icls_download_field(h, fl.first, fl.second, full.data());
+    if (rc) break;
+    size_t q = 0;
+    for (int k = 1; k <= K; ++k)
+      for (int j = 1; j <= J; ++j)
+        for (int i = 1; i <= I; ++i) in[q++] = full[(size_t)sh.at(i, j, k)];
+    if (std::fwrite(in.data(), sizeof(double), in.size(), f) != in.size()) { rc = ICLS_E_IO; break; }
+  }
+  const double info[3] = {c.time, 1. * nr, c.dt};
+  if (!rc && std::fwrite(info, sizeof(double), 3, f) != 3) rc = ICLS_E_IO;
+  if (std::fclose(f) != 0 && !rc) rc = ICLS_E_IO;
+  if (rc || !history) return rc;
+  const std::string hp = std::string(path) + ".hist";
+  f = std::fopen(hp.c_str(), "wb");
+  if (!f) return ICLS_E_IO;
+  const int dims[4] = {I, J, K, c.P.L};
+  bool ok = std::fwrite(kHistMagic, 1, 8, f) == 8 && std::fwrite(dims, sizeof(int), 4, f) == 4;
+  for (const auto& fl : hist_fields(c)) {
+    if (!ok) break;
+    const Shape3 sh = shape_of(h, fl.first);
+    full.assign((size_t)sh.n(), 0.);
+    rc = icls_download_field(h, fl.first, fl.second, full.data());
+    if (rc) break;
+    ok = std::fwrite(full.data(), sizeof(double), full.size(), f) == full.size();
+  }
+  double norm = 0.;
+  if (!rc && ok) {
+    rc = read_scalars(c);
+    norm = c.h_sc->norm;
+  }
+  if (!rc && ok) ok = std::fwrite(&norm, sizeof(double), 1, f) == 1 &&
+                      std::fwrite(c.init_volume_h.data(), sizeof(double), (size_t)c.P.L, f) == (size_t)c.P.L;
+  if (std::fclose(f) != 0) ok = false;
+  if (rc) return rc;
+  return ok ? ICLS_OK : ICLS_E_IO;
+}
+
+int icls_read_checkpoint(icls_ctx* h, const char* path, int* nr) {
+  if (!h || !path) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  const int I = c.P.imax, J = c.P.jmax, K = c.P.kmax;
+  std::vector<double> full, in((size_t)I * J * K);
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return ICLS_E_IO;
+  int rc = ICLS_OK;
+  for (const auto& fl : checkpoint_fields(c)) {
+    if (std::fread(in.data(), sizeof(double), in.size(), f) != in.size()) { rc = ICLS_E_IO; break; }
+    const Shape3 sh = shape_of(h, fl.first);
+    full.assign((size_t)sh.n(), 0.);  // halos follow from init_program's boundary passes
+    size_t q = 0;
+    for (int k = 1; k <= K; ++k)
+      for (int j = 1; j <= J; ++j)
+        for (int i = 1; i <= I; ++i) full[(size_t)sh.at(i, j, k)] = in[q++];
+    rc = icls_upload_field(h, fl.first, fl.second, full.data());
+    if (rc) break;
+  }
+  double info[3] = {0., 0., 0.};
+  if (!rc && std::fread(info, sizeof(double), 3, f) != 3) rc = ICLS_E_IO;
+  std::fclose(f);
+  if (rc) return rc;
+  rc = icls_init_program(h);
+  if (rc) return rc;
+  c.time = info[0];
+  c.dt = info[2];
+  if (nr) *nr = (int)info[1];
+  const std::string hp = std::string(path) + ".hist";
+  f = std::fopen(hp.c_str(), "rb");
+  if (!f) return ICLS_OK;  // the reference's restart: init_program's Euler start
+  char magic[8];
+  int dims[4];
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kHistMagic, 8) == 0 &&
+            std::fread(dims, sizeof(int), 4, f) == 4 && dims[0] == I && dims[1] == J && dims[2] == K &&
+            dims[3] == c.P.L;
+  for (const auto& fl : hist_fields(c)) {
+    if (!ok) break;
+    const Shape3 sh = shape_of(h, fl.first);
+    full.assign((size_t)sh.n(), 0.);
+    ok = std::fread(full.data(), sizeof(double), full.size(), f) == full.size();
+    if (ok) rc = icls_upload_field(h, fl.first, fl.second, full.data());
+    if (rc) break;
+  }
+  double norm = 0.;
+  std::vector<double> v0((size_t)c.P.L);
+  if (ok && !rc) ok = std::fread(&norm, sizeof(double), 1, f) == 1 &&
+                      std::fread(v0.data(), sizeof(double), v0.size(), f) == v0.size();
+  std::fclose(f);
+  if (rc) return rc;
+  if (!ok) return ICLS_E_IO;
+  CK(cudaMemcpyAsync(&c.dsc->norm, &norm, sizeof(double), cudaMemcpyHostToDevice, c.s));
+  CK(cudaMemcpyAsync(c.dvol0, v0.data(), sizeof(double) * v0.size(), cudaMemcpyHostToDevice, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  c.init_volume_h = v0;
+  return check_launch();
 }
 
 // disp_cg and disp_speed (write_vtk.f90:438-566) of drop l: sums on the

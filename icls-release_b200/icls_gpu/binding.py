@@ -48,6 +48,8 @@ _SIGS = {
     "average_vel_at_center": [],
     "max_vel_at_center": [_DP],
     "disp": [_I, _DP, _DP],
+    "write_checkpoint": [C.c_char_p, _I, _I],
+    "read_checkpoint": [C.c_char_p, _IP],
     "chkdiv": [_I, _DP, _DP, _IP],
     "chkdt": [_DP],
     "ipot": [_DP],
@@ -272,6 +274,22 @@ class Solver:
 
     def step(self, istep: int, begin: int = 0):
         self._call("step", istep, begin)
+
+    def write_checkpoint(self, path: str, nr: int, history: bool = True):
+        """loadflds('w', nr) (loadd.f90:28-103): u, v, w, pnew, lvset(1..L)
+        and jiemian over the interior, then (time, nr, dt).  With
+        ``history`` also ``path.hist``: the AB2 and pressure history, the
+        pressure-normalisation mean and the initial drop volumes, which an
+        exact continuation needs."""
+        self._call("write_checkpoint", os.fsencode(path), nr, 1 if history else 0)
+
+    def read_checkpoint(self, path: str) -> int:
+        """loadflds('r') followed by init_program; restores ``path.hist``
+        when it exists.  Returns nr.  Continue with ``step(istep, begin=0)``
+        for istep > nr to reproduce the uninterrupted run."""
+        nr = C.c_int()
+        self._call("read_checkpoint", os.fsencode(path), C.byref(nr))
+        return nr.value
 
     # --- the routines those subroutines are built from ----------------
     def tube_construction(self, l: int):

@@ -20,10 +20,11 @@ FP64, FP32 = 0, 1
 CURV_STENCIL, CURV_MLP = 0, 1
 
 # status codes
-OK, E_CONFIG, E_CUDA, E_NAN, E_DIVERGENCE, E_ARG, E_NOMEM, E_STATE, E_UNSUPPORTED, E_SIZE = range(10)
+OK, E_CONFIG, E_CUDA, E_NAN, E_DIVERGENCE, E_ARG, E_NOMEM, E_STATE, E_UNSUPPORTED, E_SIZE, E_IO = range(11)
 STATUS_NAMES = {
     0: "OK", 1: "E_CONFIG", 2: "E_CUDA", 3: "E_NAN", 4: "E_DIVERGENCE",
     5: "E_ARG", 6: "E_NOMEM", 7: "E_STATE", 8: "E_UNSUPPORTED", 9: "E_SIZE",
+    10: "E_IO",
 }
 
 

@@ -37,7 +37,8 @@ enum {
   ICLS_E_NOMEM = 6,       /* device allocation failed                      */
   ICLS_E_STATE = 7,       /* call made before icls_init_program            */
   ICLS_E_UNSUPPORTED = 8, /* scheme/option not built into this library    */
-  ICLS_E_SIZE = 9         /* grid larger than icls_chkdiv_noalloc handles */
+  ICLS_E_SIZE = 9,        /* grid larger than icls_chkdiv_noalloc handles */
+  ICLS_E_IO = 10          /* checkpoint file could not be written or read  */
 };
 
 /* ---- scheme selectors (param.f90 / mod_param_ls character parameters) */
@@ -160,6 +161,24 @@ int icls_max_vel_at_center(icls_ctx* ctx, double* vel_max); /* misc.f90:610-636 
 /* disp_cg, disp_speed (write_vtk.f90:438-566): drop l's centroid of its cells with
  * phi <= 1.5dz, cg[3], and velocity sum ucc dV (1 - H_l) / (lx ly lz init_volume(l)), vel[3] */
 int icls_disp(icls_ctx* ctx, int l, double cg[3], double vel[3]);
+
+/* ---- checkpoint / restart -----------------------------------------------
+ * loadflds(1, nr) (loadd.f90:66-103): the file `path` (the reference names it
+ * datadir//'fld'//nr, 7 digits) holds u, v, w, pnew, lvset(1..lmax), jiemian,
+ * each over the interior (itot x jtot x ktot FP64, i fastest, then j, then
+ * k), then (time, nr, dt).  With history != 0 the file `path`.hist also
+ * holds what the reference does not keep (it restarts with an Euler step,
+ * init.f90:90): the AB2 history duold, dvold, dwold, pold, p_x, p_y, p_z
+ * and their previous values, the whole level-set arrays (boundsls refills
+ * only the first wall ghost layer, so the outer two carry over from step
+ * to step), the pressure-normalisation mean and the initial drop volumes,
+ * so that a restart continues the run exactly (call icls_step with
+ * begin = 0).  Whole arrays are stored in the field's own layout.        */
+int icls_write_checkpoint(icls_ctx* ctx, const char* path, int nr, int history);
+/* loadflds(0, nr) (loadd.f90:28-64) into a created context, then
+ * init_program; the history of `path`.hist is restored when that file
+ * exists.  *nr = the step the file was written at.                       */
+int icls_read_checkpoint(icls_ctx* ctx, const char* path, int* nr);
 /* Returns ICLS_E_DIVERGENCE when max|div| > 1e-12 and istep != 0.        */
 int icls_chkdiv(icls_ctx* ctx, int istep, double* divtot, double* divmax,
                 int ijk[3]);                                /* chkdiv.f90:10-90     */

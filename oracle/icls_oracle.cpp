@@ -1548,3 +1548,127 @@ int ora_init_drops(const icls_config* cfg, int ndrop, const double* xc, const do
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------- checkpoint / restart
+// loadflds (loadd.f90:28-103): u, v, w, pnew, lvset(1..L), jiemian over the
+// interior, FP64, i fastest, then (time, nr, dt); path.hist: the AB2 and
+// pressure history, the normalisation mean and the initial volumes (the
+// same layout as the CUDA library writes)
+namespace {
+// whole arrays: the AB2 and pressure history, then the level sets with the
+// ghost layers boundsls leaves untouched (k = -2, -1, k1+1, k1+2)
+std::vector<std::pair<int, int>> ora_hist_fields(int L) {
+  std::vector<std::pair<int, int>> f;
+  for (int id : {ICLS_F_DUOLD, ICLS_F_DVOLD, ICLS_F_DWOLD, ICLS_F_POLD, ICLS_F_PX, ICLS_F_PY, ICLS_F_PZ,
+                 ICLS_F_PXOLD, ICLS_F_PYOLD, ICLS_F_PZOLD})
+    f.push_back({id, 1});
+  for (int l = 1; l <= L; ++l) f.push_back({ICLS_F_LVSET, l});
+  return f;
+}
+struct OraShape {
+  int lo[3], hi[3];
+  size_t n() const { return (size_t)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1); }
+  size_t at(int i, int j, int k) const {
+    return (size_t)(i - lo[0]) + (size_t)(hi[0] - lo[0] + 1) * ((size_t)(j - lo[1]) + (size_t)(hi[1] - lo[1] + 1) * (k - lo[2]));
+  }
+};
+std::vector<std::pair<int, int>> ora_ck_fields(int L) {
+  std::vector<std::pair<int, int>> f = {{ICLS_F_U, 1}, {ICLS_F_V, 1}, {ICLS_F_W, 1}, {ICLS_F_PNEW, 1}};
+  for (int l = 1; l <= L; ++l) f.push_back({ICLS_F_LVSET, l});
+  f.push_back({ICLS_F_JIEMIAN, 1});
+  return f;
+}
+}  // namespace
+
+int ora_write_checkpoint(ora_ctx* o, const char* path, int nr, int history) {
+  if (!o || !path) return ICLS_E_ARG;
+  const int I = o->imax, J = o->jmax, K = o->kmax;
+  std::vector<double> full, in((size_t)I * J * K);
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return ICLS_E_IO;
+  bool ok = true;
+  for (const auto& fl : ora_ck_fields(o->L)) {
+    OraShape sh;
+    ora_field_bounds(o, fl.first, sh.lo, sh.hi);
+    full.assign(sh.n(), 0.);
+    ora_download_field(o, fl.first, fl.second, full.data());
+    size_t q = 0;
+    for (int k = 1; k <= K; ++k)
+      for (int j = 1; j <= J; ++j)
+        for (int i = 1; i <= I; ++i) in[q++] = full[sh.at(i, j, k)];
+    ok = ok && std::fwrite(in.data(), sizeof(double), in.size(), f) == in.size();
+  }
+  const double info[3] = {o->time, 1. * nr, o->dt};
+  ok = ok && std::fwrite(info, sizeof(double), 3, f) == 3;
+  if (std::fclose(f) != 0) ok = false;
+  if (!ok) return ICLS_E_IO;
+  if (!history) return ICLS_OK;
+  f = std::fopen((std::string(path) + ".hist").c_str(), "wb");
+  if (!f) return ICLS_E_IO;
+  const char magic[8] = {'I', 'C', 'L', 'S', 'H', 'S', 'T', '1'};
+  const int dims[4] = {I, J, K, o->L};
+  ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(dims, sizeof(int), 4, f) == 4;
+  for (const auto& fl : ora_hist_fields(o->L)) {
+    OraShape sh;
+    ora_field_bounds(o, fl.first, sh.lo, sh.hi);
+    full.assign(sh.n(), 0.);
+    ora_download_field(o, fl.first, fl.second, full.data());
+    ok = ok && std::fwrite(full.data(), sizeof(double), full.size(), f) == full.size();
+  }
+  ok = ok && std::fwrite(&o->norm_old, sizeof(double), 1, f) == 1 &&
+       std::fwrite(o->init_volume.data(), sizeof(double), (size_t)o->L, f) == (size_t)o->L;
+  if (std::fclose(f) != 0) ok = false;
+  return ok ? ICLS_OK : ICLS_E_IO;
+}
+
+int ora_read_checkpoint(ora_ctx* o, const char* path, int* nr) {
+  if (!o || !path) return ICLS_E_ARG;
+  const int I = o->imax, J = o->jmax, K = o->kmax;
+  std::vector<double> full, in((size_t)I * J * K);
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return ICLS_E_IO;
+  bool ok = true;
+  for (const auto& fl : ora_ck_fields(o->L)) {
+    ok = ok && std::fread(in.data(), sizeof(double), in.size(), f) == in.size();
+    if (!ok) break;
+    OraShape sh;
+    ora_field_bounds(o, fl.first, sh.lo, sh.hi);
+    full.assign(sh.n(), 0.);
+    size_t q = 0;
+    for (int k = 1; k <= K; ++k)
+      for (int j = 1; j <= J; ++j)
+        for (int i = 1; i <= I; ++i) full[sh.at(i, j, k)] = in[q++];
+    ora_upload_field(o, fl.first, fl.second, full.data());
+  }
+  double info[3] = {0., 0., 0.};
+  ok = ok && std::fread(info, sizeof(double), 3, f) == 3;
+  std::fclose(f);
+  if (!ok) return ICLS_E_IO;
+  int rc = ora_init_program(o);
+  if (rc) return rc;
+  o->time = info[0];
+  o->dt = info[2];
+  if (nr) *nr = (int)info[1];
+  f = std::fopen((std::string(path) + ".hist").c_str(), "rb");
+  if (!f) return ICLS_OK;
+  char magic[8];
+  int dims[4];
+  ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "ICLSHST1", 8) == 0 &&
+       std::fread(dims, sizeof(int), 4, f) == 4 && dims[0] == I && dims[1] == J && dims[2] == K && dims[3] == o->L;
+  for (const auto& fl : ora_hist_fields(o->L)) {
+    if (!ok) break;
+    OraShape sh;
+    ora_field_bounds(o, fl.first, sh.lo, sh.hi);
+    full.assign(sh.n(), 0.);
+    ok = std::fread(full.data(), sizeof(double), full.size(), f) == full.size();
+    if (ok) ora_upload_field(o, fl.first, fl.second, full.data());
+  }
+  std::vector<double> v0((size_t)o->L);
+  double norm = 0.;
+  ok = ok && std::fread(&norm, sizeof(double), 1, f) == 1 && std::fread(v0.data(), sizeof(double), v0.size(), f) == v0.size();
+  std::fclose(f);
+  if (!ok) return ICLS_E_IO;
+  o->norm_old = norm;
+  o->init_volume = v0;
+  return ICLS_OK;
+}

@@ -45,6 +45,8 @@ int ora_pressure_update(ora_ctx* ctx, int istep, int begin);
 int ora_average_vel_at_center(ora_ctx* ctx);
 int ora_max_vel_at_center(ora_ctx* ctx, double* vel_max);
 int ora_disp(ora_ctx* ctx, int l, double cg[3], double vel[3]);
+int ora_write_checkpoint(ora_ctx* ctx, const char* path, int nr, int history);
+int ora_read_checkpoint(ora_ctx* ctx, const char* path, int* nr);
 int ora_chkdiv(ora_ctx* ctx, int istep, double* divtot, double* divmax, int ijk[3]);
 int ora_chkdt(ora_ctx* ctx, double* dtmax);
 int ora_ipot(ora_ctx* ctx, double* dmin);
