@@ -86,8 +86,12 @@ namespace {
 
 int validate(const icls_config* c) {
   if (!c) return ICLS_E_ARG;
-  if (!fft_length_ok(c->itot, false, c->itot) || !fft_length_ok(c->jtot, true, c->itot))
-    return ICLS_E_CONFIG;  // FFT lengths in x and y
+  if (c->bc_y < ICLS_BCY_PERIODIC || c->bc_y > ICLS_BCY_OUTOUT) return ICLS_E_CONFIG;
+  if (c->ns_conv == ICLS_NS_WENO5) return ICLS_E_UNSUPPORTED;  // boundfu stops (bound.f90:310-322)
+  if (c->ns_conv != ICLS_NS_CNTR2) return ICLS_E_CONFIG;
+  if (!fft_length_ok(c->itot, false, c->itot)) return ICLS_E_CONFIG;  // FFT length in x
+  if (c->bc_y == ICLS_BCY_PERIODIC && !fft_length_ok(c->jtot, true, c->itot)) return ICLS_E_CONFIG;
+  if (c->bc_y != ICLS_BCY_PERIODIC && c->ktot > kCosqMaxN) return ICLS_E_CONFIG;  // z cosine lines
   if (c->itot > 4096 || c->jtot > 4096) return ICLS_E_CONFIG;
   if (c->itot < 8 || c->jtot < 8) return ICLS_E_CONFIG;  // periodic images of 3 halo layers
   if (c->ktot < 6 || c->lmax < 1) return ICLS_E_CONFIG;
@@ -142,7 +146,9 @@ void fill_params(Ctx& c) {
   P.nondi = 1. / f.We;                // gfm.f90:40
   P.g1 = f.g_unit[0]; P.g2 = f.g_unit[1]; P.g3 = f.g_unit[2];
   P.v_lower = f.v_wall_lower; P.v_upper = f.v_wall_upper;
-  P.forceytot = f.constPoi ? -12. * P.visc / (f.lz * f.lz) : 0.;  // ab2.f90:104-110
+  P.bcy = f.bc_y;
+  // ab2.f90:103-118: the driving gradient only with periodic y
+  P.forceytot = (f.bc_y == ICLS_BCY_PERIODIC && f.constPoi) ? -12. * P.visc / (f.lz * f.lz) : 0.;
   P.TwoD = f.TwoD;
   P.ls_adv_space = f.ls_adv_space; P.i_space = f.i_space;
   P.ispeed_curv = (f.ispeed_dependence == ICLS_SPEED_CURV);
@@ -188,9 +194,17 @@ int allocate(Ctx& c) {
   AL(c.spec, (size_t)P.nI);
   AL(c.twx, (size_t)P.imax);
   AL(c.twy, (size_t)P.jmax);
-  AL(c.xyrt, (size_t)P.imax * P.jmax);
-  AL(c.zpiv, (size_t)(P.imax / 2 + 1) * (P.jmax / 2 + 1) * P.kmax);  // pivots per distinct (xrt, yrt)
-  AL(c.tri_a, (size_t)P.kmax + 1); AL(c.tri_b, (size_t)P.kmax + 1); AL(c.tri_c, (size_t)P.kmax + 1);
+  if (P.bcy == ICLS_BCY_PERIODIC) {
+    AL(c.xyrt, (size_t)P.imax * P.jmax);
+    AL(c.zpiv, (size_t)(P.imax / 2 + 1) * (P.jmax / 2 + 1) * P.kmax);  // pivots per distinct (xrt, yrt)
+    AL(c.tri_a, (size_t)P.kmax + 1); AL(c.tri_b, (size_t)P.kmax + 1); AL(c.tri_c, (size_t)P.kmax + 1);
+  } else {
+    AL(c.xyrt, (size_t)(P.imax / 2 + 1) * P.kmax);                      // distinct xzrt
+    AL(c.zpiv, (size_t)(P.imax / 2 + 1) * P.kmax * P.jmax);             // pivots per distinct (xrt, zrt)
+    AL(c.tri_a, (size_t)P.jmax + 1); AL(c.tri_b, (size_t)P.jmax + 1); AL(c.tri_c, (size_t)P.jmax + 1);
+    AL(c.cosb, (size_t)P.kmax * P.kmax); AL(c.cosf, (size_t)P.kmax * P.kmax);
+  }
+  AL(c.vin, (size_t)(P.i1 + 1) * (P.k1 + 1));
   AL(c.partials, (size_t)kRedBlocks * std::max(P.L, 4) + (size_t)P.imax + 8);
   AL(c.diag, (size_t)7 * kRedBlocks + 8);
   AL(c.lpartials, (size_t)kRedBlocks);
@@ -246,7 +260,7 @@ void release(Ctx& c) {
                     c.pyold, c.pzold, c.pjump, c.miu, c.rho, c.jiemian, c.curv, c.dheav, c.kappa,
                     c.rho_u, c.rho_v, c.rho_w, c.ucc, c.vcc, c.wcc, c.nrm_m, c.ulc, c.vlc, c.wlc, c.spec,
                     c.xyrt, c.zpiv, c.tri_a, c.tri_b, c.tri_c, c.partials, c.diag, c.dvol, c.dvol0, c.dmaxchk,
-                    c.hpart})
+                    c.hpart, c.cosb, c.cosf, c.vin})
     if (f) cudaFree(f);
   for (int h = 0; h < 2; ++h) {
     if (c.duold[h]) cudaFree(c.duold[h]);
@@ -1067,6 +1081,15 @@ int icls_ls_main(icls_ctx* h, int istep) {
   return ls_main(h->c, istep);
 }
 
+int icls_set_inflow(icls_ctx* h, const double* v_inflow) {
+  if (!h || !v_inflow) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  CK(cudaMemcpyAsync(c.vin, v_inflow, sizeof(double) * (size_t)(c.P.i1 + 1) * (c.P.k1 + 1),
+                     cudaMemcpyHostToDevice, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  return ICLS_OK;
+}
+
 int icls_average_stream_vel(icls_ctx* h, double* v_bulk) {
   NEED(h);
   launch_stream_vel(h->c);
@@ -1426,7 +1449,14 @@ int icls_step(icls_ctx* h, int istep, int begin) {
     launch_fillps(c, 0);
   }
   launch_solver2d(c, 1);   // solver2d + boundp(p)
-  launch_correc(c, 1);     // correc + bounduvw + average_vel_at_center + NaN probe
+  if (c.P.bcy == ICLS_BCY_PERIODIC) {
+    launch_correc(c, 1);   // correc + bounduvw + average_vel_at_center + NaN probe
+  } else {                 // the y walls change vnew before the cell-centre averages
+    launch_correc(c, 0);
+    launch_bounduvw(c, c.u, c.v, c.w);
+    launch_average_vel(c);
+    launch_nan_probe(c);
+  }
   launch_pressure_update(c, istep == begin + 1);
   rc = check_launch();
   if (rc) return rc;

@@ -17,6 +17,7 @@
 namespace icls {
 
 constexpr int kRedBlocks = 1184;   // 8 x 148 SMs: fixed grid of the reduction kernels
+constexpr int kCosqMaxN = 768;     // longest z line of solver2d_cos (one shared-memory tile)
 constexpr int kRedThreads = 256;
 constexpr int kMaxDropsParam = 256;  // drops whose far-field counts travel as a kernel parameter
 
@@ -111,7 +112,11 @@ struct Ctx {
   double2* twy = nullptr;
   double* xyrt = nullptr;               // distinct eigenvalue sums (initsolver.f90:76-82)
   double* zpiv = nullptr;               // 1/pivot of the Thomas sweep per distinct (xrt, yrt) and k
-  double* tri_a = nullptr, *tri_b = nullptr, *tri_c = nullptr;  // (kmax)
+  double* tri_a = nullptr, *tri_b = nullptr, *tri_c = nullptr;  // (kmax), or (jtot) for solver2d_cos
+  // solver2d_cos: the VCOSQB and VCOSQF matrices (kmax x kmax, row m = output
+  // m), and v_inflow(0:i1,0:k1) of the inflow boundary
+  double* cosb = nullptr, *cosf = nullptr;
+  double* vin = nullptr;
   // reductions and device scalars
   double* partials = nullptr;           // kRedBlocks * max(L,4)
   double* diag = nullptr;               // disp partials: 7 * kRedBlocks, then the 7 sums
@@ -216,6 +221,11 @@ void launch_add_pjump(Ctx& c);
 void launch_correc(Ctx& c, int fused_bc);
 void launch_bounduvw(Ctx& c, double* u, double* v, double* w);
 void launch_boundp(Ctx& c, double* p);
+// the y-wall rows of bounduvw / boundp (bound.f90:81-282) for bc_y != periodic,
+// applied after the periodic halos (i = 1..imax, k = 1..kmax)
+void launch_ywalls_uvw(Ctx& c, double* u, double* v, double* w);
+void launch_ywalls_p(Ctx& c, double* p);
+void launch_nan_probe(Ctx& c);
 void launch_average_vel(Ctx& c);
 void launch_pressure_update(Ctx& c, int first);
 void launch_stream_vel(Ctx& c);

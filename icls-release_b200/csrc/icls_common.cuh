@@ -36,6 +36,7 @@ struct Params {
   double g1, g2, g3;
   double v_lower, v_upper;
   double forceytot;
+  int bcy;                   // BC_in_y: ICLS_BCY_* (param.f90:115)
   int TwoD;
   int ls_adv_space, i_space, ispeed_curv;
   int f32;                   // precision form: bulk fields stored and computed in FP32

@@ -809,11 +809,32 @@ __device__ __forceinline__ T infl_face(const Params& p, const T* __restrict__ dh
   if (axis == 1) return -divy(p, temp * (dheav[n + p.nCx] - dheav[n]));
   return -divz(p, temp * (dheav[n + (long long)p.nCx * p.nCy] - dheav[n]));
 }
+// v_l(i,0,k) and v_l(i,jmax,k) with the y walls of boundp(dheav) and
+// bounduvw(u_l,v_l,w_l) (levelset.f90:466-478, bound.f90:81-282) for
+// BC_in_y = Walls, InOut, OutOut: v_l = 0 on a wall, v_inflow at the inlet,
+// the OutOut extrapolation at y = 0, and dheav(i,j1,k) = -dheav(i,jmax,k) at
+// an outflow end
+template <typename T>
+__device__ __forceinline__ T infl_v_front(const Params& p, const T* __restrict__ dheav, T temp, int i, int k,
+                                          const double* __restrict__ vin) {
+  if (p.bcy == ICLS_BCY_WALLS) return TC(0.);
+  if (p.bcy == ICLS_BCY_INOUT) return TC(vin[i + (long long)(p.i1 + 1) * k]);
+  const T wl_1 = (k == p.kmax) ? TC(0.) : infl_face(p, dheav, temp, 2, i, 1, k);
+  const T wl_0 = (k == 1) ? TC(0.) : infl_face(p, dheav, temp, 2, i, 1, k - 1);
+  return infl_face(p, dheav, temp, 1, i, 1, k) + TC(p.dy / p.dz) * (wl_1 - wl_0);
+}
+template <typename T>
+__device__ __forceinline__ T infl_v_back(const Params& p, const T* __restrict__ dheav, T temp, int i, int k) {
+  if (p.bcy == ICLS_BCY_WALLS) return TC(0.);
+  const T h = dheav[idxC(p, i, p.jmax, k)];
+  return -divy(p, temp * (-h - h));
+}
 template <typename T>
 __global__ void __launch_bounds__(NT) k_inflate_vel(Params p, const __grid_constant__ LsBatch B,
                                                     const T* __restrict__ dheav, const T* __restrict__ kappa,
                                                     const DevScalars* __restrict__ dsc, T* __restrict__ ulc,
-                                                    T* __restrict__ vlc, T* __restrict__ wlc) {
+                                                    T* __restrict__ vlc, T* __restrict__ wlc,
+                                                    const double* __restrict__ vin) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
@@ -824,8 +845,14 @@ __global__ void __launch_bounds__(NT) k_inflate_vel(Params p, const __grid_const
     const long long q = idxI(p, i, j, k);
     const T ul_m = infl_face(p, dheav, temp, 0, wrapx(p, i - 1), j, k);
     const T ul_0 = infl_face(p, dheav, temp, 0, i, j, k);
-    const T vl_m = infl_face(p, dheav, temp, 1, i, wrapy(p, j - 1), k);
-    const T vl_0 = infl_face(p, dheav, temp, 1, i, j, k);
+    T vl_m, vl_0;
+    if (p.bcy == ICLS_BCY_PERIODIC || (j != 1 && j != p.jmax)) {
+      vl_m = infl_face(p, dheav, temp, 1, i, wrapy(p, j - 1), k);
+      vl_0 = infl_face(p, dheav, temp, 1, i, j, k);
+    } else {
+      vl_m = j == 1 ? infl_v_front(p, dheav, temp, i, k, vin) : infl_face(p, dheav, temp, 1, i, j - 1, k);
+      vl_0 = j == p.jmax ? infl_v_back(p, dheav, temp, i, k) : infl_face(p, dheav, temp, 1, i, j, k);
+    }
     const T wl_m = (k == 1) ? TC(0.) : infl_face(p, dheav, temp, 2, i, j, k - 1);
     const T wl_0 = (k == p.kmax) ? TC(0.) : infl_face(p, dheav, temp, 2, i, j, k);
     T a = (ul_m + ul_0) / TC(2.), b = (vl_m + vl_0) / TC(2.), cc = (wl_m + wl_0) / TC(2.);
@@ -1100,9 +1127,9 @@ void launch_inflate_vel(Ctx& c, const LsBatch& b) {
   if (c.P.f32) {
     auto f = [](double* q) { return reinterpret_cast<float*>(q); };
     k_inflate_vel<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, f(c.dheav), f(c.kappa), c.dsc, f(c.ulc), f(c.vlc),
-                                                           f(c.wlc));
+                                                           f(c.wlc), c.vin);
   } else {
-    k_inflate_vel<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.dheav, c.kappa, c.dsc, c.ulc, c.vlc, c.wlc);
+    k_inflate_vel<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.dheav, c.kappa, c.dsc, c.ulc, c.vlc, c.wlc, c.vin);
   }
 }
 

@@ -476,6 +476,51 @@ __global__ void __launch_bounds__(NT) k_boundp(Params p, double* __restrict__ a)
   a[n] = a[idxC(p, I, J, K)];
 }
 
+// the y boundaries of bounduvw for BC_in_y = Walls, InOut, OutOut
+// (bound.f90:81-172), over i = 1..imax, k = 1..kmax once the periodic halos
+// are in place: a thread does its (i,k) front row, then its back row
+template <typename T>
+__global__ void __launch_bounds__(NT) k_ywalls_uvw(Params p, T* __restrict__ u, T* __restrict__ v,
+                                                   T* __restrict__ w, const double* __restrict__ vin) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y + 1;
+  if (i > p.imax) return;
+  const long long f0 = idxC(p, i, 0, k), f1 = idxC(p, i, 1, k);
+  if (p.bcy == ICLS_BCY_WALLS || p.bcy == ICLS_BCY_INOUT) {
+    u[f0] = -u[f1];
+    w[f0] = -w[f1];
+    v[f0] = p.bcy == ICLS_BCY_WALLS ? TC(0.) : TC(vin[i + (long long)(p.i1 + 1) * k]);
+  } else {
+    u[f0] = u[f1];
+    w[f0] = w[f1];
+    v[f0] = v[f1] + TC(p.dy / p.dz) * (w[f1] - w[idxC(p, i, 1, k - 1)]);
+  }
+  const long long bj = idxC(p, i, p.jmax, k), b1 = idxC(p, i, p.j1, k);
+  if (p.bcy == ICLS_BCY_WALLS) {
+    u[b1] = -u[bj];
+    v[bj] = TC(0.);
+    v[b1] = v[bj];
+    w[b1] = -w[bj];
+  } else {
+    u[b1] = u[bj];
+    v[b1] = TC(2.) * v[bj] - v[idxC(p, i, p.jmax - 1, k)];
+    w[b1] = w[bj];
+  }
+}
+// the y boundaries of boundp (bound.f90:207-282): zero Neumann, or zero
+// Dirichlet at an outflow end
+__global__ void __launch_bounds__(NT) k_ywalls_p(Params p, double* __restrict__ a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y + 1;
+  if (i > p.imax) return;
+  const double f = a[idxC(p, i, 1, k)], b = a[idxC(p, i, p.jmax, k)];
+  a[idxC(p, i, 0, k)] = p.bcy == ICLS_BCY_OUTOUT ? -f : f;
+  a[idxC(p, i, p.j1, k)] = p.bcy == ICLS_BCY_WALLS ? b : -b;
+}
+// isnan(vnew(1,1,1)) (main.f90:207)
+template <typename T>
+__global__ void k_nan_probe(Params p, const T* __restrict__ v, DevScalars* __restrict__ dsc) {
+  if (isnan(v[idxC(p, 1, 1, 1)])) dsc->nan_flag = 1;
+}
+
 // average_vel_at_center (misc.f90:587-604)
 template <typename T>
 __global__ void __launch_bounds__(NT) k_average_vel(Params p, const T* __restrict__ u, const T* __restrict__ v,
@@ -510,9 +555,14 @@ __global__ void __launch_bounds__(kNormThreads) k_plane_norm(Params p, const dou
 }
 __global__ void __launch_bounds__(NT) k_pupdate(Params p, const double* __restrict__ pp,
                                                 double* __restrict__ pnew, double* __restrict__ pold, int first,
-                                                const DevScalars* __restrict__ dsc) {
+                                                int normalise, const DevScalars* __restrict__ dsc) {
   const long long n = blockIdx.x * (long long)NT + threadIdx.x;
   if (n >= p.nC) return;
+  if (!normalise) {
+    pold[n] = pnew[n];
+    pnew[n] = pp[n];
+    return;
+  }
   const double norm = dsc->norm;
   const double po = pnew[n];
   pold[n] = first ? po - norm : (po + dsc->norm_old) - norm;
@@ -684,6 +734,7 @@ void launch_ab2(Ctx& c) {
   const int o = c.hist ^ 1;
   if (c.P.f32) ab2_launch<float>(c, a, o);
   else ab2_launch<double>(c, a, o);
+  launch_ywalls_uvw(c, c.dudt, c.dvdt, c.dwdt);  // the y walls of bounduvw(dudt,dvdt,dwdt)
   c.hist = o;
 }
 void launch_mom_main(Ctx& c, double* du, double* dv, double* dw) {
@@ -719,9 +770,29 @@ void launch_bounduvw(Ctx& c, double* u, double* v, double* w) {
   Scope sc_(c.prof, c.s, "bounduvw", 1);
   if (c.P.f32) k_bounduvw<float><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, fp<float>(u), fp<float>(v), fp<float>(w));
   else k_bounduvw<double><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, u, v, w);
+  launch_ywalls_uvw(c, u, v, w);
 }
 void launch_boundp(Ctx& c, double* pp) {
-  Scope sc_(c.prof, c.s, "boundp", 1); k_boundp<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, pp); }
+  Scope sc_(c.prof, c.s, "boundp", 1);
+  k_boundp<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, pp);
+  launch_ywalls_p(c, pp);
+}
+inline dim3 grid_ik(const Params& p) { return dim3((unsigned)((p.imax + NT - 1) / NT), (unsigned)p.kmax, 1); }
+void launch_ywalls_uvw(Ctx& c, double* u, double* v, double* w) {
+  if (c.P.bcy == ICLS_BCY_PERIODIC) return;
+  if (c.P.f32)
+    k_ywalls_uvw<float><<<grid_ik(c.P), NT, 0, c.s>>>(c.P, fp<float>(u), fp<float>(v), fp<float>(w), c.vin);
+  else
+    k_ywalls_uvw<double><<<grid_ik(c.P), NT, 0, c.s>>>(c.P, u, v, w, c.vin);
+}
+void launch_ywalls_p(Ctx& c, double* pp) {
+  if (c.P.bcy == ICLS_BCY_PERIODIC) return;
+  k_ywalls_p<<<grid_ik(c.P), NT, 0, c.s>>>(c.P, pp);
+}
+void launch_nan_probe(Ctx& c) {
+  if (c.P.f32) k_nan_probe<float><<<1, 1, 0, c.s>>>(c.P, fp<float>(c.v), c.dsc);
+  else k_nan_probe<double><<<1, 1, 0, c.s>>>(c.P, c.v, c.dsc);
+}
 void launch_average_vel(Ctx& c) {
   Scope sc_(c.prof, c.s, "average_vel", 1);
   if (c.P.f32)
@@ -732,8 +803,11 @@ void launch_average_vel(Ctx& c) {
 }
 void launch_pressure_update(Ctx& c, int first) {
   Scope sc_(c.prof, c.s, "pressure_update", 2);
-  k_plane_norm<<<1, kNormThreads, 0, c.s>>>(c.P, c.p, c.dsc);
-  k_pupdate<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, c.pnew, c.pold, first, c.dsc);
+  // the plane-1 normalisation runs for BC_in_y Periodic and Walls only
+  // (main.f90:169-185); otherwise pold = pnew, pnew = p
+  const int norm = c.P.bcy == ICLS_BCY_PERIODIC || c.P.bcy == ICLS_BCY_WALLS;
+  if (norm) k_plane_norm<<<1, kNormThreads, 0, c.s>>>(c.P, c.p, c.dsc);
+  k_pupdate<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, c.pnew, c.pold, first, norm, c.dsc);
 }
 void launch_stream_vel(Ctx& c) {
   Scope sc_(c.prof, c.s, "stream_vel", 2);

@@ -490,38 +490,37 @@ constexpr size_t fft2_smem() {
 __host__ __device__ __forceinline__ long long pivot_columns(const Params& p) {
   return (long long)(p.imax / 2 + 1) * (p.jmax / 2 + 1);
 }
-__global__ void k_thomas_setup(Params p, const double* __restrict__ xyrt, const double* __restrict__ a,
+// 1/pivots of the Thomas elimination (solver.f90:119-160, 245-283) of each
+// distinct eigenvalue column q < nd: zpiv[q + (r-1) nd], r = 1..K-1, and the
+// last pivot itself at r = K
+__global__ void k_thomas_setup(const double* __restrict__ eig, long long nd, int K, const double* __restrict__ a,
                                const double* __restrict__ b, const double* __restrict__ c,
                                double* __restrict__ zpiv) {
   const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long nxy = pivot_columns(p);
-  if (q >= nxy) return;
-  const double xy = xyrt[q];
+  if (q >= nd) return;
+  const double xy = eig[q];
   double z = 1. / (b[1] + xy);
   double d = c[1] * z;
   zpiv[q] = z;
-  for (int k = 2; k <= p.kmax - 1; ++k) {
+  for (int k = 2; k <= K - 1; ++k) {
     const double bb = b[k] + xy;
     z = 1. / (bb - a[k] * d);
     d = c[k] * z;
-    zpiv[q + (k - 1) * nxy] = z;
+    zpiv[q + (k - 1) * nd] = z;
   }
-  const double bb = b[p.kmax] + xy;
-  zpiv[q + (p.kmax - 1) * nxy] = bb - a[p.kmax] * d;
+  const double bb = b[K] + xy;
+  zpiv[q + (K - 1) * nd] = bb - a[K] * d;
 }
 
 // The sweeps read 8 rows ahead of the dependency chain (same operations,
 // in the same order, as a row-by-row loop).
 constexpr int TU = 8;
-__global__ void __launch_bounds__(128) k_thomas(Params p, const double* __restrict__ a, const double* __restrict__ c,
-                                                const double* __restrict__ zpiv, double* __restrict__ spec) {
-  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long nxy = (long long)p.imax * p.jmax, nd = pivot_columns(p);
-  if (q >= nxy) return;
-  const int K = p.kmax;
-  const int i = (int)(q % p.imax) + 1, j = (int)(q / p.imax) + 1;
-  double* __restrict__ col = spec + q;
-  const double* __restrict__ zc = zpiv + (i >> 1) + (long long)(p.imax / 2 + 1) * (j >> 1);
+// one line of K values at col[0], col[st], ...: forward elimination with the
+// stored 1/pivots zc[0], zc[nd], ..., the zero-pivot rule of the last row
+// (p = 0, the singular mode), back substitution with d = c z
+__device__ __forceinline__ void thomas_line(double* __restrict__ col, long long st, int K,
+                                            const double* __restrict__ zc, long long nd,
+                                            const double* __restrict__ a, const double* __restrict__ c) {
   double prev = col[0] * zc[0];
   col[0] = prev;
   for (int k0 = 2; k0 <= K - 1; k0 += TU) {
@@ -529,28 +528,28 @@ __global__ void __launch_bounds__(128) k_thomas(Params p, const double* __restri
 #pragma unroll
     for (int u = 0; u < TU; ++u)
       if (k0 + u <= K - 1) {
-        cv[u] = col[(k0 + u - 1) * nxy];
+        cv[u] = col[(k0 + u - 1) * st];
         zv[u] = zc[(k0 + u - 1) * nd];
       }
 #pragma unroll
     for (int u = 0; u < TU; ++u)
       if (k0 + u <= K - 1) {
         const double v = (cv[u] - a[k0 + u] * prev) * zv[u];
-        col[(k0 + u - 1) * nxy] = v;
+        col[(k0 + u - 1) * st] = v;
         prev = v;
       }
   }
   const double zz = zc[(K - 1) * nd];
   double nxt;
-  if (zz != 0.) nxt = (col[(K - 1) * nxy] - a[K] * prev) / zz;
+  if (zz != 0.) nxt = (col[(K - 1) * st] - a[K] * prev) / zz;
   else nxt = 0.;
-  col[(K - 1) * nxy] = nxt;
+  col[(K - 1) * st] = nxt;
   for (int k0 = K - 1; k0 >= 1; k0 -= TU) {
     double cv[TU], zv[TU];
 #pragma unroll
     for (int u = 0; u < TU; ++u)
       if (k0 - u >= 1) {
-        cv[u] = col[(k0 - u - 1) * nxy];
+        cv[u] = col[(k0 - u - 1) * st];
         zv[u] = zc[(k0 - u - 1) * nd];
       }
 #pragma unroll
@@ -558,9 +557,69 @@ __global__ void __launch_bounds__(128) k_thomas(Params p, const double* __restri
       if (k0 - u >= 1) {
         const double d = c[k0 - u] * zv[u];
         const double v = cv[u] - d * nxt;
-        col[(k0 - u - 1) * nxy] = v;
+        col[(k0 - u - 1) * st] = v;
         nxt = v;
       }
+  }
+}
+// solver2d: lines along z, one thread per (i,j)
+__global__ void __launch_bounds__(128) k_thomas(Params p, const double* __restrict__ a, const double* __restrict__ c,
+                                                const double* __restrict__ zpiv, double* __restrict__ spec) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nxy = (long long)p.imax * p.jmax, nd = pivot_columns(p);
+  if (q >= nxy) return;
+  const int i = (int)(q % p.imax) + 1, j = (int)(q / p.imax) + 1;
+  thomas_line(spec + q, nxy, p.kmax, zpiv + (i >> 1) + (long long)(p.imax / 2 + 1) * (j >> 1), nd, a, c);
+}
+// solver2d_cos (solver.f90:245-283): lines along y, one thread per (i,k),
+// diagonal b(j) + xzrt(i,k); the distinct columns are (i>>1, k)
+__global__ void __launch_bounds__(128) k_thomas_y(Params p, const double* __restrict__ a, const double* __restrict__ c,
+                                                  const double* __restrict__ zpiv, double* __restrict__ spec) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nxz = (long long)p.imax * p.kmax, nd = (long long)(p.imax / 2 + 1) * p.kmax;
+  if (q >= nxz) return;
+  const int i = (int)(q % p.imax) + 1, k = (int)(q / p.imax) + 1;
+  thomas_line(spec + (i - 1) + (long long)p.imax * p.jmax * (k - 1), p.imax, p.jmax,
+              zpiv + (i >> 1) + (long long)(p.imax / 2 + 1) * (k - 1), nd, a, c);
+}
+
+// VCOSQB (dir 0) / VCOSQF (dir 1) along z of every (i,j) line of spec, as
+// the matrix product out[m] = sum_k T[m][k] x[k] with the kmax x kmax table
+// T of the transform's definition (fft.f:120-124, 270-274).  A CTA holds 32
+// consecutive i of one j (all k) in shared memory; warp w forms rows
+// m = 4w.., 4 at a time, each lane one i, summing in k order with fused
+// multiply-adds.
+constexpr int CZ_TI = 32, CZ_ROWS = 4;
+__global__ void __launch_bounds__(256) k_cosq_z(Params p, const double* __restrict__ T, double* __restrict__ spec) {
+  extern __shared__ double czx[];  // [kmax][CZ_TI]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int i0 = 1 + CZ_TI * (int)blockIdx.x, j = 1 + (int)blockIdx.y;
+  const int K = p.kmax;
+  const long long plane = (long long)p.imax * p.jmax;
+  double* __restrict__ base = spec + (i0 - 1) + (long long)p.imax * (j - 1);
+  const int ni = min(CZ_TI, p.imax - i0 + 1);
+  for (int t = threadIdx.x; t < K * CZ_TI; t += blockDim.x) {
+    const int k = t / CZ_TI, l = t - k * CZ_TI;
+    czx[t] = l < ni ? base[l + plane * k] : 0.;
+  }
+  __syncthreads();
+  if (lane >= ni) return;
+  for (int m0 = CZ_ROWS * warp; m0 < K; m0 += CZ_ROWS * 8) {
+    double acc[CZ_ROWS];
+    const double* __restrict__ tr[CZ_ROWS];
+#pragma unroll
+    for (int r = 0; r < CZ_ROWS; ++r) {
+      acc[r] = 0.;
+      tr[r] = T + (long long)min(m0 + r, K - 1) * K;
+    }
+    for (int k = 0; k < K; ++k) {
+      const double xv = czx[k * CZ_TI + lane];
+#pragma unroll
+      for (int r = 0; r < CZ_ROWS; ++r) acc[r] = __fma_rn(__ldg(tr[r] + k), xv, acc[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < CZ_ROWS; ++r)
+      if (m0 + r < K) base[lane + plane * (m0 + r)] = acc[r];
   }
 }
 
@@ -582,7 +641,12 @@ void make_twiddles(int N, std::vector<double2>& t) {
 }  // namespace
 
 // tables of initsolver (initsolver.f90:20-82) and the twiddles
+void poisson_setup_cos(Ctx& c);
 void poisson_setup(Ctx& c) {
+  if (c.P.bcy != ICLS_BCY_PERIODIC) {
+    poisson_setup_cos(c);
+    return;
+  }
   const Params& P = c.P;
   const int itot = P.imax, jtot = P.jmax, kmax = P.kmax;
   std::vector<double> a(kmax + 1, 0.), b(kmax + 1, 0.), cc(kmax + 1, 0.);
@@ -623,7 +687,72 @@ void poisson_setup(Ctx& c) {
   cudaMemcpyAsync(c.twx, tx.data(), tx.size() * sizeof(double2), cudaMemcpyHostToDevice, c.s);
   cudaMemcpyAsync(c.twy, ty.data(), ty.size() * sizeof(double2), cudaMemcpyHostToDevice, c.s);
   const long long nd = pivot_columns(P);
-  k_thomas_setup<<<(unsigned)((nd + 127) / 128), 128, 0, c.s>>>(P, c.xyrt, c.tri_a, c.tri_b, c.tri_c, c.zpiv);
+  k_thomas_setup<<<(unsigned)((nd + 127) / 128), 128, 0, c.s>>>(c.xyrt, nd, P.kmax, c.tri_a, c.tri_b, c.tri_c,
+                                                                 c.zpiv);
+  cudaStreamSynchronize(c.s);  // host vectors above go out of scope
+}
+
+namespace {
+// cos(m pi / (2n)) with m reduced mod 4n, in long double
+double cos_quarter(long long m, int n) {
+  const long long q = 4LL * n;
+  m %= q;
+  const long double pi = 3.141592653589793238462643383279502884L;
+  return (double)cosl((long double)m * pi / (2.0L * n));
+}
+}  // namespace
+
+// initsolver for BC_in_y = Walls, InOut, OutOut (initsolver.f90:85-156):
+// a(j), b(j), c(j) with the end rows of the y boundary, xzrt = xrt(i) +
+// zrt(k) per distinct column (i>>1, k), their Thomas pivots, the x twiddles
+// and the VCOSQB / VCOSQF matrices (fft.f:120-124, 270-274)
+void poisson_setup_cos(Ctx& c) {
+  const Params& P = c.P;
+  const int itot = P.imax, jtot = P.jmax, kmax = P.kmax;
+  std::vector<double> a(jtot + 1, 0.), b(jtot + 1, 0.), cc(jtot + 1, 0.);
+  for (int j = 1; j <= jtot; ++j) { a[j] = P.dyi * P.dyi; cc[j] = P.dyi * P.dyi; b[j] = -(a[j] + cc[j]); }
+  if (P.bcy == ICLS_BCY_WALLS) {
+    b[1] = b[1] + a[1];
+    b[jtot] = b[jtot] + cc[jtot];
+  } else if (P.bcy == ICLS_BCY_INOUT) {
+    b[1] = b[1] + a[1];
+    b[jtot] = b[jtot] - cc[jtot];
+  } else {
+    b[1] = b[1] - a[1];
+    b[jtot] = b[jtot] - cc[jtot];
+  }
+  a[1] = 0.; cc[jtot] = 0.;
+  std::vector<double> xrt(itot + 1, 0.), zrt(kmax + 1, 0.);
+  const double pi = P.pi;
+  for (int i = 3; i <= itot; i += 2) {
+    double s = std::sin((double)(i - 1) * pi / (2. * itot));
+    xrt[i - 1] = -4. * P.dxi * P.dxi * (s * s);
+    xrt[i] = xrt[i - 1];
+  }
+  xrt[1] = 0.; xrt[itot] = -4. * P.dxi * P.dxi;
+  for (int k = 1; k <= kmax; ++k) zrt[k] = (P.dzi * P.dzi) * (-2. + 2. * std::cos((double)(k - 1) * pi / kmax));
+  const int nxd = itot / 2 + 1;
+  std::vector<double> xz((size_t)nxd * kmax);
+  for (int k = 1; k <= kmax; ++k)
+    for (int ix = 0; ix < nxd; ++ix) xz[ix + (size_t)nxd * (k - 1)] = xrt[ix == 0 ? 1 : 2 * ix] + zrt[k];
+  std::vector<double> tb((size_t)kmax * kmax), tf((size_t)kmax * kmax);
+  const double sb = 4. / std::sqrt(4. * kmax), sf = 1. / std::sqrt(4. * kmax);
+  for (int m = 0; m < kmax; ++m)
+    for (int k = 0; k < kmax; ++k) {
+      tb[(size_t)m * kmax + k] = sb * cos_quarter((long long)(2 * k + 1) * m, kmax);
+      tf[(size_t)m * kmax + k] = sf * (k == 0 ? 1. : 2. * cos_quarter((long long)(2 * m + 1) * k, kmax));
+    }
+  cudaMemcpyAsync(c.xyrt, xz.data(), xz.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
+  cudaMemcpyAsync(c.tri_a, a.data(), a.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
+  cudaMemcpyAsync(c.tri_b, b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
+  cudaMemcpyAsync(c.tri_c, cc.data(), cc.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
+  cudaMemcpyAsync(c.cosb, tb.data(), tb.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
+  cudaMemcpyAsync(c.cosf, tf.data(), tf.size() * sizeof(double), cudaMemcpyHostToDevice, c.s);
+  std::vector<double2> tx;
+  make_twiddles(itot, tx);
+  cudaMemcpyAsync(c.twx, tx.data(), tx.size() * sizeof(double2), cudaMemcpyHostToDevice, c.s);
+  const long long nd = (long long)nxd * kmax;
+  k_thomas_setup<<<(unsigned)((nd + 127) / 128), 128, 0, c.s>>>(c.xyrt, nd, jtot, c.tri_a, c.tri_b, c.tri_c, c.zpiv);
   cudaStreamSynchronize(c.s);  // host vectors above go out of scope
 }
 
@@ -694,7 +823,12 @@ bool fft_length_ok(int n, bool y_pass, int imax) {
   }
 }
 
+void launch_solver2d_cos(Ctx& c, int write_halos);
 void launch_solver2d(Ctx& c, int write_halos) {
+  if (c.P.bcy != ICLS_BCY_PERIODIC) {
+    launch_solver2d_cos(c, write_halos);
+    return;
+  }
   Scope sc_(c.prof, c.s, "solver2d", 5);
   const Params& P = c.P;
   const int lx = ilog2(P.imax), ly = ilog2(P.jmax);
@@ -719,6 +853,35 @@ void launch_solver2d(Ctx& c, int write_halos) {
   k_thomas<<<(unsigned)((nxy + 127) / 128), 128, 0, c.s>>>(P, c.tri_a, c.tri_c, c.zpiv, c.spec);
   if (!fft2_pass<true>(c, 1, 0)) k_fft_y<<<gy, FT, smy, c.s>>>(P, 1, TI, ly, c.twy, c.spec);
   if (!fft2_pass<false>(c, 1, write_halos)) k_fft_x<<<gx, FT, smx, c.s>>>(P, 1, CL, lx, c.twx, c.p, c.spec, write_halos);
+}
+
+// solver2d_cos (solver.f90:202-317): x FFT, VCOSQB in z, Thomas in y,
+// VCOSQF in z, inverse x FFT (+ boundp halos and the y-wall rows)
+void launch_solver2d_cos(Ctx& c, int write_halos) {
+  Scope sc_(c.prof, c.s, "solver2d", 5);
+  const Params& P = c.P;
+  const int lx = ilog2(P.imax);
+  const int CL = x_lines_per_cta(P.imax);
+  const long long nlines = (long long)P.jmax * P.kmax;
+  const unsigned gx = (unsigned)((nlines + 2 * CL - 1) / (2 * CL));
+  const size_t smx = (size_t)CL * (P.imax + 1) * sizeof(double2);
+  const size_t smz = (size_t)P.kmax * CZ_TI * sizeof(double);
+  static unsigned attr = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(attr & (1u << (dev & 31)))) {
+    cudaFuncSetAttribute(k_fft_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_cosq_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kCosqMaxN * CZ_TI * sizeof(double)));
+    attr |= 1u << (dev & 31);
+  }
+  const dim3 gz((unsigned)((P.imax + CZ_TI - 1) / CZ_TI), (unsigned)P.jmax, 1);
+  if (!fft2_pass<false>(c, 0, 0)) k_fft_x<<<gx, FT, smx, c.s>>>(P, 0, CL, lx, c.twx, c.p, c.spec, 0);
+  k_cosq_z<<<gz, 256, smz, c.s>>>(P, c.cosb, c.spec);
+  const long long nxz = (long long)P.imax * P.kmax;
+  k_thomas_y<<<(unsigned)((nxz + 127) / 128), 128, 0, c.s>>>(P, c.tri_a, c.tri_c, c.zpiv, c.spec);
+  k_cosq_z<<<gz, 256, smz, c.s>>>(P, c.cosf, c.spec);
+  if (!fft2_pass<false>(c, 1, write_halos)) k_fft_x<<<gx, FT, smx, c.s>>>(P, 1, CL, lx, c.twx, c.p, c.spec, write_halos);
+  if (write_halos) launch_ywalls_p(c, c.p);
 }
 
 }  // namespace icls

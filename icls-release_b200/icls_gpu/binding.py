@@ -47,6 +47,7 @@ _SIGS = {
     "pressure_update": [_I, _I],
     "average_vel_at_center": [],
     "max_vel_at_center": [_DP],
+    "set_inflow": [_DP],
     "disp": [_I, _DP, _DP],
     "write_checkpoint": [C.c_char_p, _I, _I],
     "read_checkpoint": [C.c_char_p, _IP],
@@ -246,6 +247,12 @@ class Solver:
         x = C.c_double()
         self._call("max_vel_at_center", C.byref(x))
         return x.value
+
+    def set_inflow(self, v_inflow: np.ndarray):
+        """v_inflow(0:i1,0:k1) of bc_y = INOUT (bound.f90:118-130)."""
+        a = np.asfortranarray(v_inflow, dtype=np.float64)
+        assert a.shape == (self.cfg.itot + 2, self.cfg.ktot + 2)
+        self._call("set_inflow", a.ctypes.data_as(_DP))
 
     def disp(self, l: int = 1):
         """disp_cg and disp_speed of drop l: (centroid[3], velocity[3])"""

@@ -18,6 +18,8 @@ HOUC5, WENO5 = 0, 1
 SPEED_UNFM, SPEED_CURV = 0, 1
 FP64, FP32 = 0, 1
 CURV_STENCIL, CURV_MLP = 0, 1
+BCY_PERIODIC, BCY_WALLS, BCY_INOUT, BCY_OUTOUT = 0, 1, 2, 3
+NS_CNTR2, NS_WENO5 = 0, 1
 
 # status codes
 OK, E_CONFIG, E_CUDA, E_NAN, E_DIVERGENCE, E_ARG, E_NOMEM, E_STATE, E_UNSUPPORTED, E_SIZE, E_IO = range(11)
@@ -44,6 +46,7 @@ class IclsConfig(C.Structure):
         ("ispeed_dependence", C.c_int), ("i_space", C.c_int),
         ("ioutchk", C.c_int), ("precision", C.c_int), ("curvature_model", C.c_int),
         ("mlp_fallback_tol", C.c_double),
+        ("bc_y", C.c_int), ("ns_conv", C.c_int),
     ]
 
     def as_dict(self):
@@ -60,6 +63,27 @@ class IclsScalars(C.Structure):
         ("v_bulk", C.c_double), ("norm_old", C.c_double), ("maxchk_glb", C.c_double),
         ("reinit_residual", C.c_double), ("reinit_iters", C.c_int), ("last_inflated", C.c_int),
     ]
+
+
+def inflow_profile(cfg: IclsConfig, v_bulk_desired: float = 1.0) -> np.ndarray:
+    """v_inflow(0:i1,0:k1) of inflow_profile (init.f90:418-455), one process:
+    a parabola over k = 1..9 and itot/3 < i <= 2 itot/3 whose mean over the
+    inlet plane is v_bulk_desired (param.f90:49)."""
+    itot, ktot = cfg.itot, cfg.ktot
+    dz = cfg.lz / ktot
+    v = np.zeros((itot + 2, ktot + 2), order="F")
+    i_start, i_end = itot // 3, itot // 3 * 2
+    k_start, k_end = 0, 9
+    ratio_i = 1.0 * (i_end - i_start) / itot
+    ratio_k = 1.0 * (k_end - k_start) / ktot
+    v_mean = v_bulk_desired / (ratio_i * ratio_k)
+    for k in range(1, ktot + 1):
+        if k_start < k <= k_end:
+            coorz = (k - 0.5) * dz / (cfg.lz * ratio_k)
+            for i in range(1, itot + 1):
+                if i_start < i <= i_end:
+                    v[i, k] = 6. * v_mean * coorz * (1. - coorz)
+    return v
 
 
 def make_config(**kw) -> IclsConfig:

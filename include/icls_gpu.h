@@ -46,13 +46,21 @@ enum { ICLS_HOUC5 = 0, ICLS_WENO5 = 1 };              /* ls_adv_space, i_space *
 enum { ICLS_SPEED_UNFM = 0, ICLS_SPEED_CURV = 1 };    /* ispeed_dependence     */
 enum { ICLS_FP64 = 0, ICLS_FP32 = 1 };                /* precision form        */
 enum { ICLS_CURV_STENCIL = 0, ICLS_CURV_MLP = 1 };    /* curvature model       */
+/* BC_in_y (param.f90:115): the y boundary of velocity and pressure, and
+ * with it the pressure solver (main.f90:147-153): periodic -> solver2d;
+ * walls, inflow/outflow, outflow/outflow -> solver2d_cos               */
+enum { ICLS_BCY_PERIODIC = 0, ICLS_BCY_WALLS = 1, ICLS_BCY_INOUT = 2, ICLS_BCY_OUTOUT = 3 };
+/* NS_conv (param.f90:135).  'WENO5' stops the reference in boundfu
+ * (bound.f90:310-322: "WENO5 is not fully implemented yet"); icls_create
+ * returns ICLS_E_UNSUPPORTED for it.                                    */
+enum { ICLS_NS_CNTR2 = 0, ICLS_NS_WENO5 = 1 };
 
 /*
  * Runtime configuration.  Restates the compile-time parameters of
  * src/param.f90 (grid 27-38, dt 47, materials 58-63, Re/We/iFr 69-77,
  * flags 93-172) and src/param.f90 module mod_param_ls (199-275).
- * Fixed choices of the reference defaults that this path implements:
- * BC_in_y='Periodic' (solver2d), BC_in_z='Dirichl', NS_conv='CNTR2',
+ * BC_in_y and NS_conv are selectable (bc_y, ns_conv).  Fixed choices of
+ * the reference defaults that this path implements: BC_in_z='Dirichl',
  * NS_diff_discretization='del', surface_tension_method='GFM',
  * ls_adv_time='RK3', ls_reinit_time='RK3', ls_reinit_space='WENO5',
  * attractive=.false., Riblet=.false., Contact_line=.false.
@@ -83,6 +91,8 @@ typedef struct icls_config {
   int curvature_model;           /* ICLS_CURV_STENCIL / ICLS_CURV_MLP        */
   double mlp_fallback_tol;       /* |k_mlp-k_plain|*dx above which the plain
                                     stencil value is kept (MLP form only)   */
+  int bc_y;                      /* ICLS_BCY_* (param.f90:115)               */
+  int ns_conv;                   /* ICLS_NS_* (param.f90:135)                */
 } icls_config;
 
 /* Fill *cfg with the reference defaults of src/param.f90 for a 3-D run. */
@@ -147,6 +157,10 @@ int icls_init_program(icls_ctx* ctx);
 /* ---- the subroutines main.f90 calls (main.f90:103-291) ---------------- */
 int icls_ls_main(icls_ctx* ctx, int istep);                 /* levelset.f90:28-76   */
 int icls_average_stream_vel(icls_ctx* ctx, double* v_bulk); /* misc.f90:642-655     */
+/* v_inflow(0:i1,0:k1) (common.f90:36), i fastest, the inflow profile of
+ * bc_y = ICLS_BCY_INOUT at the y = 0 boundary (bound.f90:118-130); the
+ * reference fills it in inflow_profile (init.f90:418-455).  Zero until set. */
+int icls_set_inflow(icls_ctx* ctx, const double* v_inflow);
 int icls_ab2(icls_ctx* ctx);                                /* ab2.f90:21-138       */
 int icls_fillps(icls_ctx* ctx);                             /* fillps.f90:13-57     */
 int icls_gfm4p(icls_ctx* ctx);                              /* gfm.f90:17-267       */

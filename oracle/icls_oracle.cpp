@@ -166,6 +166,40 @@ void rfftb_line(int n, double* r) {
   for (int j = 0; j < n; ++j) r[j] = s * a[j].real();
 }
 
+// VCOSQB / VCOSQF (fft.f:218-372 / 68-216) on one line, from their
+// documented definitions (fft.f:120-124, 270-274), summed directly in long
+// double: backward (the forward transform of solver2d_cos)
+//   x(i) = sum_{k=1..n} 4 x(k) cos((2k-1)(i-1) pi/(2n)) / sqrt(4n),
+// forward (its normalised inverse)
+//   x(i) = (x(1) + sum_{k=2..n} 2 x(k) cos((2i-1)(k-1) pi/(2n))) / sqrt(4n).
+// Angles are reduced exactly: cos(m pi/(2n)) with m taken mod 4n.
+long double cos_q(long long m, int n) {
+  const long long q = 4LL * n;
+  m %= q;
+  if (m < 0) m += q;
+  return std::cos((long double)m * 3.14159265358979323846264338327950288L / (2.0L * n));
+}
+void cosqb_line(int n, double* x) {
+  std::vector<long double> o(n, 0.0L);
+  const long double s = 4.0L / std::sqrt(4.0L * n);
+  for (int i = 0; i < n; ++i) {
+    long double acc = 0.0L;
+    for (int k = 0; k < n; ++k) acc += (long double)x[k] * cos_q((long long)(2 * k + 1) * i, n);
+    o[i] = s * acc;
+  }
+  for (int i = 0; i < n; ++i) x[i] = (double)o[i];
+}
+void cosqf_line(int n, double* x) {
+  std::vector<long double> o(n, 0.0L);
+  const long double s = 1.0L / std::sqrt(4.0L * n);
+  for (int i = 0; i < n; ++i) {
+    long double acc = x[0];
+    for (int k = 1; k < n; ++k) acc += 2.0L * (long double)x[k] * cos_q((long long)(2 * i + 1) * k, n);
+    o[i] = s * acc;
+  }
+  for (int i = 0; i < n; ++i) x[i] = (double)o[i];
+}
+
 }  // namespace
 
 // ======================================================================
@@ -195,6 +229,11 @@ struct ora_ctx {
   bool initialised = false;
   // solver (solver.f90:42-47)
   std::vector<double> xyrt, ta, tb, tc;
+  // solver2d_cos (solver.f90:202-317): tridiagonal in y, eigenvalues
+  // xzrt(i,k) = xrt(i) + zrt(k) (initsolver.f90:85-156)
+  std::vector<double> xzrt;
+  std::vector<double> v_inflow;            // v_inflow(0:i1,0:k1) (common.f90:36)
+  int bcy = ICLS_BCY_PERIODIC;
 
   // ------------------------------------------------------------ shapes
   void shapeC(F3& a) { a.init(0, i1, 0, j1, 0, k1); }
@@ -206,6 +245,10 @@ struct ora_ctx {
     itot = c.itot; jtot = c.jtot; ktot = c.ktot; L = c.lmax;
     if (itot < 4 || jtot < 4 || ktot < 6 || L < 1) return ICLS_E_CONFIG;
     if (itot % 2 || jtot % 2) return ICLS_E_CONFIG;
+    if (c.bc_y < ICLS_BCY_PERIODIC || c.bc_y > ICLS_BCY_OUTOUT) return ICLS_E_CONFIG;
+    if (c.ns_conv == ICLS_NS_WENO5) return ICLS_E_UNSUPPORTED;  // boundfu stops (bound.f90:310-322)
+    if (c.ns_conv != ICLS_NS_CNTR2) return ICLS_E_CONFIG;
+    bcy = c.bc_y;
     imax = itot; jmax = jtot; kmax = ktot;
     i1 = imax + 1; j1 = jmax + 1; k1 = kmax + 1;
     lx = c.lx; ly = c.ly; lz = c.lz;
@@ -228,6 +271,7 @@ struct ora_ctx {
     mask.assign((size_t)imax * jmax * kmax, 0);
     nb_cnt.assign(L, 0);
     volume.assign(L, 0.); init_volume.assign(L, 0.); dmin.assign((size_t)L * L, 0.);
+    v_inflow.assign((size_t)(i1 + 1) * (k1 + 1), 0.);
     nrm_m.fill(1.);
     return ICLS_OK;
   }
@@ -282,12 +326,53 @@ struct ora_ctx {
         w(i, j, k1) = w(i, j, kmax - 1);
       }
     updthalos(u); updthalos(v); updthalos(w);
+    if (bcy != ICLS_BCY_PERIODIC) ywalls_uvw(u, v, w);
+  }
+  // the y boundaries of bounduvw for BC_in_y = Walls, InOut, OutOut
+  // (bound.f90:81-172), over i = 1..imax, k = 1..kmax, after the halos
+  void ywalls_uvw(F3& u, F3& v, F3& w) {
+    for (int k = 1; k <= kmax; ++k)
+      for (int i = 1; i <= imax; ++i) {
+        if (bcy == ICLS_BCY_WALLS) {
+          u(i, 0, k) = -u(i, 1, k);
+          w(i, 0, k) = -w(i, 1, k);
+          v(i, 0, k) = 0.;
+        } else if (bcy == ICLS_BCY_INOUT) {
+          u(i, 0, k) = -u(i, 1, k);
+          w(i, 0, k) = -w(i, 1, k);
+          v(i, 0, k) = v_inflow[(size_t)i + (size_t)(i1 + 1) * k];
+        } else {
+          u(i, 0, k) = u(i, 1, k);
+          w(i, 0, k) = w(i, 1, k);
+          v(i, 0, k) = v(i, 1, k) + dy / dz * (w(i, 1, k) - w(i, 1, k - 1));
+        }
+      }
+    for (int k = 1; k <= kmax; ++k)
+      for (int i = 1; i <= imax; ++i) {
+        if (bcy == ICLS_BCY_WALLS) {
+          u(i, j1, k) = -u(i, jmax, k);
+          v(i, jmax, k) = 0.;
+          v(i, j1, k) = v(i, jmax, k);
+          w(i, j1, k) = -w(i, jmax, k);
+        } else {
+          u(i, j1, k) = u(i, jmax, k);
+          v(i, j1, k) = 2. * v(i, jmax, k) - v(i, jmax - 1, k);
+          w(i, j1, k) = w(i, jmax, k);
+        }
+      }
   }
   // boundp, BC_in_y='Periodic' (bound.f90:182-287)
   void boundp(F3& a) {
     for (int j = 0; j <= j1; ++j)
       for (int i = 0; i <= i1; ++i) { a(i, j, 0) = a(i, j, 1); a(i, j, k1) = a(i, j, kmax); }
     updthalos(a);
+    if (bcy == ICLS_BCY_PERIODIC) return;
+    // y boundaries (bound.f90:207-282): zero Neumann, or zero Dirichlet at
+    // an outflow end
+    for (int k = 1; k <= kmax; ++k)
+      for (int i = 1; i <= imax; ++i) a(i, 0, k) = bcy == ICLS_BCY_OUTOUT ? -a(i, 1, k) : a(i, 1, k);
+    for (int k = 1; k <= kmax; ++k)
+      for (int i = 1; i <= imax; ++i) a(i, j1, k) = bcy == ICLS_BCY_WALLS ? a(i, jmax, k) : -a(i, jmax, k);
   }
   // boundc (bound.f90:292-305)
   void boundc(F3& a) { updthalos(a); }
@@ -359,8 +444,36 @@ struct ora_ctx {
       }
   }
 
+  // initsolver, BC_in_y='Walls','InOut','OutOut' (initsolver.f90:85-156):
+  // tridiagonal in y, cosine eigenvalues in z
+  void initsolver_cos() {
+    ta.assign(jtot + 1, 0); tb.assign(jtot + 1, 0); tc.assign(jtot + 1, 0);
+    for (int j = 1; j <= jtot; ++j) { ta[j] = dyi * dyi; tc[j] = dyi * dyi; tb[j] = -(ta[j] + tc[j]); }
+    if (bcy == ICLS_BCY_WALLS) {
+      tb[1] = tb[1] + ta[1];
+      tb[jtot] = tb[jtot] + tc[jtot];
+    } else if (bcy == ICLS_BCY_INOUT) {
+      tb[1] = tb[1] + ta[1];
+      tb[jtot] = tb[jtot] - tc[jtot];
+    } else {
+      tb[1] = tb[1] - ta[1];
+      tb[jtot] = tb[jtot] - tc[jtot];
+    }
+    ta[1] = 0.; tc[jtot] = 0.;
+    std::vector<double> xrt(itot + 1), zrt(kmax + 1);
+    for (int i = 3; i <= itot; i += 2) {
+      xrt[i - 1] = -4. * dxi * dxi * sq(std::sin((double)(i - 1) * pi / (2. * itot)));
+      xrt[i] = xrt[i - 1];
+    }
+    xrt[1] = 0.; xrt[itot] = -4. * dxi * dxi;
+    for (int k = 1; k <= kmax; ++k) zrt[k] = (dzi * dzi) * (-2. + 2. * std::cos((double)(k - 1) * pi / kmax));
+    xzrt.assign((size_t)imax * kmax, 0);
+    for (int k = 1; k <= kmax; ++k)
+      for (int i = 1; i <= imax; ++i) xzrt[(i - 1) + (size_t)imax * (k - 1)] = xrt[i] + zrt[k];
+  }
   // initsolver, BC_in_y='Periodic' (initsolver.f90:20-82)
   void initsolver() {
+    if (bcy != ICLS_BCY_PERIODIC) { initsolver_cos(); return; }
     ta.assign(kmax + 1, 0); tb.assign(kmax + 1, 0); tc.assign(kmax + 1, 0);
     for (int k = 1; k <= kmax; ++k) { ta[k] = dzi * dzi; tc[k] = dzi * dzi; tb[k] = -(ta[k] + tc[k]); }
     tb[1] = tb[1] + ta[1];
@@ -1101,7 +1214,7 @@ struct ora_ctx {
           dvnew(i, j, k) = -((1. / rho_v(i, j, k) - 1. / rho0) * dyi * ((phat(i, j + 1, k) - pjy(i, j, k)) - phat(i, j, k)));
           dwnew(i, j, k) = -((1. / rho_w(i, j, k) - 1. / rho0) * dzi * ((phat(i, j, k + 1) - pjz(i, j, k)) - phat(i, j, k)));
         }
-    forceytot = c.constPoi ? -12. * visc / (lz * lz) : 0.;
+    forceytot = (bcy == ICLS_BCY_PERIODIC && c.constPoi) ? -12. * visc / (lz * lz) : 0.;  // ab2.f90:103-118
 #pragma omp parallel for
     for (int k = 1; k <= kmax; ++k)
       for (int j = 1; j <= jmax; ++j)
@@ -1268,6 +1381,75 @@ struct ora_ctx {
     }
   }
 
+  // solver2d_cos (solver.f90:202-317) on p(1:imax,1:jmax,1:kmax): real FFT
+  // in x, VCOSQB in z, Gauss elimination in y with diagonal b(j)+xzrt(i,k),
+  // VCOSQF in z, inverse FFT in x
+  void solver2d_cos() {
+#pragma omp parallel for
+    for (int k = 1; k <= kmax; ++k) {
+      std::vector<double> line(imax);
+      for (int j = 1; j <= jmax; ++j) {
+        for (int i = 1; i <= imax; ++i) line[i - 1] = p(i, j, k);
+        rfftf_line(imax, line.data());
+        for (int i = 1; i <= imax; ++i) p(i, j, k) = line[i - 1];
+      }
+    }
+#pragma omp parallel for
+    for (int j = 1; j <= jmax; ++j) {
+      std::vector<double> line(kmax);
+      for (int i = 1; i <= imax; ++i) {
+        for (int k = 1; k <= kmax; ++k) line[k - 1] = p(i, j, k);
+        cosqb_line(kmax, line.data());
+        for (int k = 1; k <= kmax; ++k) p(i, j, k) = line[k - 1];
+      }
+    }
+    // Gauss elimination in y (solver.f90:245-283)
+#pragma omp parallel for
+    for (int k = 1; k <= kmax; ++k) {
+      std::vector<double> d(jtot + 1);
+      for (int i = 1; i <= imax; ++i) {
+        const double xz = xzrt[(i - 1) + (size_t)imax * (k - 1)];
+        double z = 1. / (tb[1] + xz);
+        d[1] = tc[1] * z;
+        p(i, 1, k) = p(i, 1, k) * z;
+        for (int j = 2; j <= jtot - 1; ++j) {
+          double bb = tb[j] + xz;
+          z = 1. / (bb - ta[j] * d[j - 1]);
+          d[j] = tc[j] * z;
+          p(i, j, k) = (p(i, j, k) - ta[j] * p(i, j - 1, k)) * z;
+        }
+        double bb = tb[jtot] + xz;
+        z = bb - ta[jtot] * d[jtot - 1];
+        if (z != 0.) p(i, jtot, k) = (p(i, jtot, k) - ta[jtot] * p(i, jtot - 1, k)) / z;
+        else p(i, jtot, k) = 0.;
+        for (int j = jtot - 1; j >= 1; --j) p(i, j, k) = p(i, j, k) - d[j] * p(i, j + 1, k);
+      }
+    }
+#pragma omp parallel for
+    for (int j = 1; j <= jmax; ++j) {
+      std::vector<double> line(kmax);
+      for (int i = 1; i <= imax; ++i) {
+        for (int k = 1; k <= kmax; ++k) line[k - 1] = p(i, j, k);
+        cosqf_line(kmax, line.data());
+        for (int k = 1; k <= kmax; ++k) p(i, j, k) = line[k - 1];
+      }
+    }
+#pragma omp parallel for
+    for (int k = 1; k <= kmax; ++k) {
+      std::vector<double> line(imax);
+      for (int j = 1; j <= jmax; ++j) {
+        for (int i = 1; i <= imax; ++i) line[i - 1] = p(i, j, k);
+        rfftb_line(imax, line.data());
+        for (int i = 1; i <= imax; ++i) p(i, j, k) = line[i - 1];
+      }
+    }
+  }
+  // the pressure solve main.f90 selects by BC_in_y (main.f90:147-153)
+  void pressure_solve() {
+    if (bcy == ICLS_BCY_PERIODIC) solver2d();
+    else solver2d_cos();
+  }
+
   // correc (correc.f90:15-44)
   void correc() {
 #pragma omp parallel for
@@ -1285,6 +1467,7 @@ struct ora_ctx {
     pold.v = pnew.v;
     pnew.v = p.v;
     boundp(pnew);
+    if (bcy != ICLS_BCY_PERIODIC && bcy != ICLS_BCY_WALLS) return;  // main.f90:169-185
     const int k = 1;
     double norm = 0.;
     for (int i = 0; i <= i1; ++i) {
@@ -1381,7 +1564,7 @@ struct ora_ctx {
     ab2();
     fillps();
     if (c.solveLS) { gfm4p(); add_pjump(); }
-    solver2d();
+    pressure_solve();
     boundp(p);
     correc();
     bounduvw(unew, vnew, wnew);
@@ -1466,7 +1649,12 @@ int ora_ab2(ora_ctx* o) { NEED_INIT; o->ab2(); return ICLS_OK; }
 int ora_fillps(ora_ctx* o) { NEED_INIT; o->fillps(); return ICLS_OK; }
 int ora_gfm4p(ora_ctx* o) { NEED_INIT; o->gfm4p(); return ICLS_OK; }
 int ora_add_pjump(ora_ctx* o) { NEED_INIT; o->add_pjump(); return ICLS_OK; }
-int ora_solver2d(ora_ctx* o) { NEED_INIT; o->solver2d(); return ICLS_OK; }
+int ora_solver2d(ora_ctx* o) { NEED_INIT; o->pressure_solve(); return ICLS_OK; }
+int ora_set_inflow(ora_ctx* o, const double* v) {
+  if (!o || !v) return ICLS_E_ARG;
+  std::memcpy(o->v_inflow.data(), v, o->v_inflow.size() * sizeof(double));
+  return ICLS_OK;
+}
 int ora_boundp(ora_ctx* o, int id) {
   F3* f = o->field(id, 1);
   if (!f || f->l0 != 0) return ICLS_E_ARG;
@@ -1515,6 +1703,14 @@ int ora_vrfftf(int m, int n, double* r) {
 }
 int ora_vrfftb(int m, int n, double* r) {
   for (int s = 0; s < m; ++s) rfftb_line(n, r + (size_t)s * n);
+  return ICLS_OK;
+}
+int ora_vcosqf(int m, int n, double* r) {
+  for (int l = 0; l < m; ++l) cosqf_line(n, r + (size_t)l * n);
+  return ICLS_OK;
+}
+int ora_vcosqb(int m, int n, double* r) {
+  for (int l = 0; l < m; ++l) cosqb_line(n, r + (size_t)l * n);
   return ICLS_OK;
 }
 

@@ -45,6 +45,7 @@ int ora_pressure_update(ora_ctx* ctx, int istep, int begin);
 int ora_average_vel_at_center(ora_ctx* ctx);
 int ora_max_vel_at_center(ora_ctx* ctx, double* vel_max);
 int ora_disp(ora_ctx* ctx, int l, double cg[3], double vel[3]);
+int ora_set_inflow(ora_ctx* ctx, const double* v_inflow);
 int ora_write_checkpoint(ora_ctx* ctx, const char* path, int nr, int history);
 int ora_read_checkpoint(ora_ctx* ctx, const char* path, int* nr);
 int ora_chkdiv(ora_ctx* ctx, int istep, double* divtot, double* divmax, int ijk[3]);
@@ -64,6 +65,8 @@ int ora_band_count(ora_ctx* ctx, int l, long long* nb_cnt);
  * m sequences of length n, sequence s stored contiguously at r + s*n.    */
 int ora_vrfftf(int m, int n, double* r);
 int ora_vrfftb(int m, int n, double* r);
+int ora_vcosqf(int m, int n, double* r);  /* fft.f:68-216, per row */
+int ora_vcosqb(int m, int n, double* r);  /* fft.f:218-372, per row */
 
 /* Initial level sets of init.f90 'drp' (717-753) and 'mdp' (901-984)
  * generalised to arbitrary centres/radii: writes lvset(:,:,:,l) for

@@ -44,6 +44,8 @@ def backend() -> Backend:
         lib.ora_set_dt.argtypes = [C.c_void_p, C.c_double]
         lib.ora_vrfftf.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
         lib.ora_vrfftb.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+        lib.ora_vcosqf.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+        lib.ora_vcosqb.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
         lib.ora_get_pseudo_inv.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     return _BACKEND
 
@@ -70,6 +72,22 @@ def vrfftf(x: np.ndarray) -> np.ndarray:
     a = np.ascontiguousarray(x, dtype=np.float64).copy()
     m, n = a.shape
     backend().lib.ora_vrfftf(m, n, a.ctypes.data_as(C.POINTER(C.c_double)))
+    return a
+
+
+def vcosqf(x: np.ndarray) -> np.ndarray:
+    """VFFTPACK VCOSQF contract (fft.f:68-216) on each row."""
+    a = np.ascontiguousarray(x, dtype=np.float64).copy()
+    m, n = a.shape
+    backend().lib.ora_vcosqf(m, n, a.ctypes.data_as(C.POINTER(C.c_double)))
+    return a
+
+
+def vcosqb(x: np.ndarray) -> np.ndarray:
+    """VFFTPACK VCOSQB contract (fft.f:218-372) on each row."""
+    a = np.ascontiguousarray(x, dtype=np.float64).copy()
+    m, n = a.shape
+    backend().lib.ora_vcosqb(m, n, a.ctypes.data_as(C.POINTER(C.c_double)))
     return a
 
 
