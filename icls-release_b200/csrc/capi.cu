@@ -193,7 +193,7 @@ int allocate(Ctx& c) {
   AL(c.d_nbcnt, (size_t)P.L);
   AL(c.spec, (size_t)P.nI);
   AL(c.twx, (size_t)P.imax);
-  AL(c.twy, (size_t)P.jmax);
+  AL(c.twy, (size_t)std::max(P.jmax, P.kmax));  // y twiddles, or z twiddles of solver2d_cos
   if (P.bcy == ICLS_BCY_PERIODIC) {
     AL(c.xyrt, (size_t)P.imax * P.jmax);
     AL(c.zpiv, (size_t)(P.imax / 2 + 1) * (P.jmax / 2 + 1) * P.kmax);  // pivots per distinct (xrt, yrt)
@@ -203,6 +203,7 @@ int allocate(Ctx& c) {
     AL(c.zpiv, (size_t)(P.imax / 2 + 1) * P.kmax * P.jmax);             // pivots per distinct (xrt, zrt)
     AL(c.tri_a, (size_t)P.jmax + 1); AL(c.tri_b, (size_t)P.jmax + 1); AL(c.tri_c, (size_t)P.jmax + 1);
     AL(c.cosb, (size_t)P.kmax * P.kmax); AL(c.cosf, (size_t)P.kmax * P.kmax);
+    AL(c.czw, (size_t)P.kmax);
   }
   AL(c.vin, (size_t)(P.i1 + 1) * (P.k1 + 1));
   AL(c.partials, (size_t)kRedBlocks * std::max(P.L, 4) + (size_t)P.imax + 8);
@@ -275,6 +276,7 @@ void release(Ctx& c) {
   if (c.d_nbcnt) cudaFree(c.d_nbcnt);
   if (c.twx) cudaFree(c.twx);
   if (c.twy) cudaFree(c.twy);
+  if (c.czw) cudaFree(c.czw);
   if (c.lpartials) cudaFree(c.lpartials);
   if (c.drs) cudaFree(c.drs);
   if (c.stage) cudaFree(c.stage);

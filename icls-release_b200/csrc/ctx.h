@@ -116,6 +116,7 @@ struct Ctx {
   // solver2d_cos: the VCOSQB and VCOSQF matrices (kmax x kmax, row m = output
   // m), and v_inflow(0:i1,0:k1) of the inflow boundary
   double* cosb = nullptr, *cosf = nullptr;
+  double2* czw = nullptr;               // (cos, sin)(pi k/(2 kmax)), k < kmax
   double* vin = nullptr;
   // reductions and device scalars
   double* partials = nullptr;           // kRedBlocks * max(L,4)

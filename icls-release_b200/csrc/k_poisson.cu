@@ -590,6 +590,7 @@ __global__ void __launch_bounds__(128) k_thomas_y(Params p, const double* __rest
 // m = 4w.., 4 at a time, each lane one i, summing in k order with fused
 // multiply-adds.
 constexpr int CZ_TI = 32, CZ_ROWS = 4;
+constexpr int kCosqFftMaxN = 512;  // CZ_LINES x (N+1) complex values in shared memory
 __global__ void __launch_bounds__(256) k_cosq_z(Params p, const double* __restrict__ T, double* __restrict__ spec) {
   extern __shared__ double czx[];  // [kmax][CZ_TI]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -620,6 +621,66 @@ __global__ void __launch_bounds__(256) k_cosq_z(Params p, const double* __restri
 #pragma unroll
     for (int r = 0; r < CZ_ROWS; ++r)
       if (m0 + r < K) base[lane + plane * (m0 + r)] = acc[r];
+  }
+}
+
+// The same transforms for a power-of-two kmax up to kCosqFftMaxN through one
+// N-point complex FFT per two lines (Makhoul's reordering; J. Makhoul, "A
+// fast cosine transform in one and two dimensions", IEEE Trans. ASSP 28,
+// 1980): with W_k = e^{i pi k/(2N)},
+//   VCOSQB: v = (x0, x2, ..., x3, x1), V = FFT(v), out_k = (2/sqrt N) Re(conj(W_k) V_k);
+//   VCOSQF: V_k = W_k (y_k - i y_{N-k})/2 (y_N = 0), z = sum_k V_k e^{+2 pi i kn/N},
+//           out_{2n} = z_n/sqrt N, out_{2n+1} = z_{N-1-n}/sqrt N.
+// Columns 2c and 2c+1 of the CTA's 32 i travel as the real and imaginary
+// parts of complex line c; the transform is smem_fft (bit-reversed input).
+constexpr int CZ_LINES = CZ_TI / 2;
+__device__ __forceinline__ int makhoul_pos(int k, int N) { return (k & 1) ? N - 1 - (k >> 1) : (k >> 1); }
+__global__ void __launch_bounds__(256) k_cosq_fft_z(Params p, int dir, int logN, const double2* __restrict__ tw,
+                                                    const double2* __restrict__ cw, double* __restrict__ spec) {
+  extern __shared__ double2 czb[];  // [CZ_LINES][N+1]
+  const int N = p.kmax, ld = N + 1;
+  const int i0 = 1 + CZ_TI * (int)blockIdx.x, j = 1 + (int)blockIdx.y;
+  const long long plane = (long long)p.imax * p.jmax;
+  double* __restrict__ base = spec + (i0 - 1) + (long long)p.imax * (j - 1);
+  const int ni = min(CZ_TI, p.imax - i0 + 1);
+  const double rs = 1. / sqrt((double)N);
+  if (dir == 0) {
+    for (int t = threadIdx.x; t < N * CZ_TI; t += blockDim.x) {
+      const int k = t / CZ_TI, l = t - k * CZ_TI;
+      double* slot = reinterpret_cast<double*>(&czb[(l >> 1) * ld + bitrev(makhoul_pos(k, N), logN)]) + (l & 1);
+      *slot = l < ni ? base[l + plane * k] : 0.;
+    }
+  } else {
+    for (int t = threadIdx.x; t < N * CZ_LINES; t += blockDim.x) {
+      const int k = t / CZ_LINES, c = t - k * CZ_LINES, la = 2 * c, lb = la + 1;
+      const double ya = la < ni ? base[la + plane * k] : 0., yb = lb < ni ? base[lb + plane * k] : 0.;
+      const double yan = (k && la < ni) ? base[la + plane * (N - k)] : 0.;
+      const double ybn = (k && lb < ni) ? base[lb + plane * (N - k)] : 0.;
+      const double2 w = cw[k];
+      const double2 va = make_double2(0.5 * (w.x * ya + w.y * yan), 0.5 * (w.y * ya - w.x * yan));
+      const double2 vb = make_double2(0.5 * (w.x * yb + w.y * ybn), 0.5 * (w.y * yb - w.x * ybn));
+      czb[c * ld + bitrev(k, logN)] = make_double2(va.x - vb.y, va.y + vb.x);
+    }
+  }
+  __syncthreads();
+  smem_fft(czb, CZ_LINES, N, logN, ld, tw, dir);
+  for (int t = threadIdx.x; t < N * CZ_TI; t += blockDim.x) {
+    const int k = t / CZ_TI, l = t - k * CZ_TI;
+    if (l >= ni) continue;
+    const double2* L = czb + (l >> 1) * ld;
+    double out;
+    if (dir == 0) {
+      const double2 zk = L[k], zn = L[(N - k) & (N - 1)];
+      double vr, vi;
+      if (l & 1) { vr = 0.5 * (zk.y + zn.y); vi = -0.5 * (zk.x - zn.x); }
+      else { vr = 0.5 * (zk.x + zn.x); vi = 0.5 * (zk.y - zn.y); }
+      const double2 w = cw[k];
+      out = (2. * rs) * (w.x * vr + w.y * vi);
+    } else {
+      const double2 z = L[makhoul_pos(k, N)];
+      out = ((l & 1) ? z.y : z.x) * rs;
+    }
+    base[l + plane * k] = out;
   }
 }
 
@@ -751,6 +812,17 @@ void poisson_setup_cos(Ctx& c) {
   std::vector<double2> tx;
   make_twiddles(itot, tx);
   cudaMemcpyAsync(c.twx, tx.data(), tx.size() * sizeof(double2), cudaMemcpyHostToDevice, c.s);
+  std::vector<double2> tz, wz(kmax);
+  make_twiddles(kmax, tz);
+  {
+    const long double pi_l = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < kmax; ++k) {
+      const long double a = pi_l * (long double)k / (2.0L * kmax);
+      wz[k] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+  }
+  cudaMemcpyAsync(c.twy, tz.data(), tz.size() * sizeof(double2), cudaMemcpyHostToDevice, c.s);
+  cudaMemcpyAsync(c.czw, wz.data(), wz.size() * sizeof(double2), cudaMemcpyHostToDevice, c.s);
   const long long nd = (long long)nxd * kmax;
   k_thomas_setup<<<(unsigned)((nd + 127) / 128), 128, 0, c.s>>>(c.xyrt, nd, jtot, c.tri_a, c.tri_b, c.tri_c, c.zpiv);
   cudaStreamSynchronize(c.s);  // host vectors above go out of scope
@@ -872,14 +944,23 @@ void launch_solver2d_cos(Ctx& c, int write_halos) {
   if (!(attr & (1u << (dev & 31)))) {
     cudaFuncSetAttribute(k_fft_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_cosq_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kCosqMaxN * CZ_TI * sizeof(double)));
+    cudaFuncSetAttribute(k_cosq_fft_z, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(CZ_LINES * (kCosqFftMaxN + 1) * sizeof(double2)));
     attr |= 1u << (dev & 31);
   }
   const dim3 gz((unsigned)((P.imax + CZ_TI - 1) / CZ_TI), (unsigned)P.jmax, 1);
+  const bool fz = (P.kmax & (P.kmax - 1)) == 0 && P.kmax >= 8 && P.kmax <= kCosqFftMaxN;
+  const int lz = ilog2(P.kmax);
+  const size_t smf = (size_t)CZ_LINES * (P.kmax + 1) * sizeof(double2);
+  auto cosq = [&](int dir) {
+    if (fz) k_cosq_fft_z<<<gz, 256, smf, c.s>>>(P, dir, lz, c.twy, c.czw, c.spec);
+    else k_cosq_z<<<gz, 256, smz, c.s>>>(P, dir ? c.cosf : c.cosb, c.spec);
+  };
   if (!fft2_pass<false>(c, 0, 0)) k_fft_x<<<gx, FT, smx, c.s>>>(P, 0, CL, lx, c.twx, c.p, c.spec, 0);
-  k_cosq_z<<<gz, 256, smz, c.s>>>(P, c.cosb, c.spec);
+  cosq(0);
   const long long nxz = (long long)P.imax * P.kmax;
   k_thomas_y<<<(unsigned)((nxz + 127) / 128), 128, 0, c.s>>>(P, c.tri_a, c.tri_c, c.zpiv, c.spec);
-  k_cosq_z<<<gz, 256, smz, c.s>>>(P, c.cosf, c.spec);
+  cosq(1);
   if (!fft2_pass<false>(c, 1, write_halos)) k_fft_x<<<gx, FT, smx, c.s>>>(P, 1, CL, lx, c.twx, c.p, c.spec, write_halos);
   if (write_halos) launch_ywalls_p(c, c.p);
 }
