@@ -1000,6 +1000,56 @@ int icls_download_field(icls_ctx* h, int id, int l, double* host) {
   return ICLS_OK;
 }
 
+int icls_download_plane_x(icls_ctx* h, int id, int l, int i, double* host) {
+  if (!h || !host) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  int lo[3], hi[3];
+  int rc = icls_field_bounds(h, id, lo, hi);
+  if (rc) return rc;
+  if (i < lo[0] || i > hi[0]) return ICLS_E_ARG;
+  long long n;
+  double* d = field_ptr(c, id, l, &n);
+  if (!d) return ICLS_E_ARG;
+  if (id == ICLS_F_LVSET) {  // fill the far field outside the swept region
+    const DropWin& w = c.win[l - 1];
+    if (!is_full(c.P, w.valid)) launch_materialize(c, w.valid, w.bg, w.bg_ghost, d);
+  }
+  if (id == ICLS_F_CURV || id == ICLS_F_NORMAL_M) fix_curv(c);
+  const long long nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1;
+  const int n1 = (int)ny, n2 = hi[2] - lo[2] + 1;
+  double* dev = nullptr;
+  CK(cudaMallocAsync((void**)&dev, sizeof(double) * (size_t)n1 * n2, c.s));
+  launch_gather_plane_x(c, d, c.P.f32 && tfield(id), nx, ny, i - lo[0], n1, n2, dev);
+  CK(cudaMemcpyAsync(host, dev, sizeof(double) * (size_t)n1 * n2, cudaMemcpyDeviceToHost, c.s));
+  CK(cudaFreeAsync(dev, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  return check_launch();
+}
+
+int icls_timestep_record(icls_ctx* h, int istep, double rec[6]) {
+  if (!h || !rec) return ICLS_E_ARG;
+  Ctx& c = h->c;
+  const int L = c.P.L;
+  icls_scalars sc;
+  int rc = icls_get_scalars(h, &sc);
+  if (rc) return rc;
+  std::vector<double> vol(L), vol0(L);
+  rc = icls_get_volumes(h, vol.data(), vol0.data());
+  if (rc) return rc;
+  double massloss = 0.;
+  for (int l = 0; l < L; ++l) massloss = massloss + (1. - vol[l] / vol0[l]);
+  double quck = 0.;
+  if (L >= 2) {
+    std::vector<double> dm((size_t)L * L);
+    rc = icls_ipot(h, dm.data());
+    if (rc) return rc;
+    quck = dm[0 + (size_t)L * 1] / c.P.dz;  // dmin(1,2)/dz
+  }
+  rec[0] = 1. * istep; rec[1] = c.time; rec[2] = c.dt;
+  rec[3] = massloss; rec[4] = quck; rec[5] = sc.maxchk_glb;
+  return ICLS_OK;
+}
+
 int icls_get_scalars(icls_ctx* h, icls_scalars* out) {
   if (!h || !out) return ICLS_E_ARG;
   Ctx& c = h->c;
@@ -1385,7 +1435,14 @@ int icls_ipot(icls_ctx* h, double* dmin) {
   }
   double* dev = nullptr;
   CK(cudaMallocAsync((void**)&dev, sizeof(double) * L * L, c.s));
-  CK(cudaMemsetAsync(dev, 0xFF, sizeof(double) * L * L, c.s));
+  // every pair starts at the ordered bits of 1e3, the reference's initial
+  // super_phi (interface.f90:250): the value of a pair with no cell to sweep
+  unsigned long long init = 0;
+  const double big = 1e3;
+  std::memcpy(&init, &big, sizeof(init));
+  init |= 0x8000000000000000ull;
+  const std::vector<unsigned long long> preset((size_t)L * L, init);
+  CK(cudaMemcpyAsync(dev, preset.data(), sizeof(double) * L * L, cudaMemcpyHostToDevice, c.s));
   launch_ipot(c, dev);
   std::vector<unsigned long long> bits((size_t)L * L);
   CK(cudaMemcpyAsync(bits.data(), dev, sizeof(double) * L * L, cudaMemcpyDeviceToHost, c.s));

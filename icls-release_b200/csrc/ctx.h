@@ -227,6 +227,9 @@ void launch_boundp(Ctx& c, double* p);
 void launch_ywalls_uvw(Ctx& c, double* u, double* v, double* w);
 void launch_ywalls_p(Ctx& c, double* p);
 void launch_nan_probe(Ctx& c);
+// dst(j,k) = d(ioff + nx j + nx ny k) in FP64 (d holds float when f32)
+void launch_gather_plane_x(Ctx& c, const double* d, bool f32, long long nx, long long ny, long long ioff, int n1,
+                           int n2, double* dst);
 void launch_average_vel(Ctx& c);
 void launch_pressure_update(Ctx& c, int first);
 void launch_stream_vel(Ctx& c);
@@ -234,6 +237,9 @@ void launch_chkdiv(Ctx& c);
 void launch_chkdt(Ctx& c);
 void launch_maxvel(Ctx& c);
 void launch_nan_probe(Ctx& c);
+// dst(j,k) = d(ioff + nx j + nx ny k) in FP64 (d holds float when f32)
+void launch_gather_plane_x(Ctx& c, const double* d, bool f32, long long nx, long long ny, long long ioff, int n1,
+                           int n2, double* dst);
 
 // Poisson (k_poisson.cu)
 void poisson_setup(Ctx& c);

@@ -314,9 +314,21 @@ void launch_jumps(Ctx& c, const LsBatch& b) {
   else
     k_jumps<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.pjump, c.px, c.py, c.pz);
 }
+// the periodic column spans a..a+la-1 and b..b+lb-1 of n columns share a
+// column (two arcs meet iff one starts inside the other)
+bool spans_meet(int a, int la, int b, int lb, int n) {
+  if (la >= n || lb >= n) return la > 0 && lb > 0;
+  if (la <= 0 || lb <= 0) return false;
+  const int d1 = ((b - a) % n + n) % n, d2 = ((a - b) % n + n) % n;
+  return d1 < la || d2 < lb;
+}
 // dmin_dev: L*L unsigned long long ordered bits, filled here; only cells
 // written by both drops' regions can hold |phi_m| < dz and phi_n < 6dz
-// unless a far field is below 6dz, so each pair sweeps m's written cells
+// unless a far field is below 6dz, so each pair sweeps m's written cells.
+// A pair whose written regions are disjoint, with n's far fields at or
+// above 6dz, has no such cell: the reference's minimum stays at its initial
+// 1e3 (interface.f90:250-260), which the buffer's preset bits already hold
+// for every pair not launched (ordered bits of 1e3), so it is not swept.
 void launch_ipot(Ctx& c, double* dmin_dev) {
   unsigned long long* o = reinterpret_cast<unsigned long long*>(dmin_dev);
   LsBatch b;
@@ -324,6 +336,11 @@ void launch_ipot(Ctx& c, double* dmin_dev) {
   for (int m = 0; m < c.P.L; ++m)
     for (int n = 0; n < c.P.L; ++n) {
       if (m == n) continue;
+      const Region& rm = c.win[m].valid;
+      const Region& rn = c.win[n].valid;
+      const bool meet = spans_meet(rm.xa, rm.xn, rn.xa, rn.xn, c.P.imax) &&
+                        spans_meet(rm.ya, rm.yn, rn.ya, rn.yn, c.P.jmax) && rm.z0 <= rn.z1 && rn.z0 <= rm.z1;
+      if (!meet && c.win[n].bg >= c.P.NB && c.win[n].bg_ghost >= c.P.NB) continue;
       LsTask& t = b.t[0];
       t = LsTask();
       t.r = c.win[m].valid;

@@ -521,6 +521,17 @@ __global__ void k_nan_probe(Params p, const T* __restrict__ v, DevScalars* __res
   if (isnan(v[idxC(p, 1, 1, 1)])) dsc->nan_flag = 1;
 }
 
+// the plane i = const of an array with extents nx x ny x nz: dst(j,k) =
+// src(ioff + nx j + nx ny k), j < n1, k < n2, converted to FP64
+template <typename T>
+__global__ void __launch_bounds__(NT) k_gather_plane_x(const T* __restrict__ src, long long nx, long long nxy, long long ioff,
+                                                       int n1, int n2, double* __restrict__ dst) {
+  const long long q = blockIdx.x * (long long)NT + threadIdx.x;
+  if (q >= (long long)n1 * n2) return;
+  const long long j = q % n1, k = q / n1;
+  dst[q] = (double)src[ioff + nx * j + nxy * k];
+}
+
 // average_vel_at_center (misc.f90:587-604)
 template <typename T>
 __global__ void __launch_bounds__(NT) k_average_vel(Params p, const T* __restrict__ u, const T* __restrict__ v,
@@ -788,6 +799,12 @@ void launch_ywalls_uvw(Ctx& c, double* u, double* v, double* w) {
 void launch_ywalls_p(Ctx& c, double* pp) {
   if (c.P.bcy == ICLS_BCY_PERIODIC) return;
   k_ywalls_p<<<grid_ik(c.P), NT, 0, c.s>>>(c.P, pp);
+}
+void launch_gather_plane_x(Ctx& c, const double* d, bool f32, long long nx, long long ny, long long ioff, int n1,
+                           int n2, double* dst) {
+  const unsigned g = nblocks((long long)n1 * n2);
+  if (f32) k_gather_plane_x<float><<<g, NT, 0, c.s>>>(reinterpret_cast<const float*>(d), nx, nx * ny, ioff, n1, n2, dst);
+  else k_gather_plane_x<double><<<g, NT, 0, c.s>>>(d, nx, nx * ny, ioff, n1, n2, dst);
 }
 void launch_nan_probe(Ctx& c) {
   if (c.P.f32) k_nan_probe<float><<<1, 1, 0, c.s>>>(c.P, fp<float>(c.v), c.dsc);

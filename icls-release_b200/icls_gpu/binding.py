@@ -48,6 +48,8 @@ _SIGS = {
     "average_vel_at_center": [],
     "max_vel_at_center": [_DP],
     "set_inflow": [_DP],
+    "download_plane_x": [_I, _I, _I, _DP],
+    "timestep_record": [_I, _DP],
     "disp": [_I, _DP, _DP],
     "write_checkpoint": [C.c_char_p, _I, _I],
     "read_checkpoint": [C.c_char_p, _IP],
@@ -247,6 +249,21 @@ class Solver:
         x = C.c_double()
         self._call("max_vel_at_center", C.byref(x))
         return x.value
+
+    def download_plane_x(self, name: str, i: int, l: int = 1) -> np.ndarray:
+        """The plane i = const of a field over its own (j, k) bounds, indexed
+        [j - lo1, k - lo2]."""
+        lo, hi = self.bounds(name)
+        a = np.zeros((hi[1] - lo[1] + 1, hi[2] - lo[2] + 1), order="F")
+        self._call("download_plane_x", FIELD_ID[name], l, i, a.ctypes.data_as(_DP))
+        return a
+
+    def timestep_record(self, istep: int) -> np.ndarray:
+        """(istep, time, dt, massloss, dmin(1,2)/dz, maxchk_glb), the
+        timestep.txt record of main.f90:243-256."""
+        r = np.zeros(6)
+        self._call("timestep_record", istep, r.ctypes.data_as(_DP))
+        return r
 
     def set_inflow(self, v_inflow: np.ndarray):
         """v_inflow(0:i1,0:k1) of bc_y = INOUT (bound.f90:118-130)."""

@@ -161,6 +161,13 @@ int icls_average_stream_vel(icls_ctx* ctx, double* v_bulk); /* misc.f90:642-655 
  * bc_y = ICLS_BCY_INOUT at the y = 0 boundary (bound.f90:118-130); the
  * reference fills it in inflow_profile (init.f90:418-455).  Zero until set. */
 int icls_set_inflow(icls_ctx* ctx, const double* v_inflow);
+/* The plane i = const of a field, for 2-D output (post2d, output.f90:179-432):
+ * out(j,k) over the field's own j and k bounds, j fastest, FP64.          */
+int icls_download_plane_x(icls_ctx* ctx, int id, int l, int i, double* out);
+/* The timestep.txt record of main.f90:243-256: rec = (istep, time, dt,
+ * massloss = sum_l (1 - volume(l)/init_volume(l)), dmin(1,2)/dz from ipot
+ * (0 with one drop), maxchk_glb).  Runs ipot when lmax >= 2.            */
+int icls_timestep_record(icls_ctx* ctx, int istep, double rec[6]);
 int icls_ab2(icls_ctx* ctx);                                /* ab2.f90:21-138       */
 int icls_fillps(icls_ctx* ctx);                             /* fillps.f90:13-57     */
 int icls_gfm4p(icls_ctx* ctx);                              /* gfm.f90:17-267       */

@@ -1684,6 +1684,29 @@ int ora_ipot(ora_ctx* o, double* dmin) {
   return ICLS_OK;
 }
 int ora_step(ora_ctx* o, int istep, int begin) { NEED_INIT; return o->step(istep, begin); }
+// the plane i = const of a field: out(j,k), j fastest
+int ora_download_plane_x(ora_ctx* o, int id, int l, int i, double* out) {
+  F3* f = o->field(id, l);
+  if (!f || !out) return ICLS_E_ARG;
+  if (i < f->l0 || i > f->l0 + f->n0 - 1) return ICLS_E_ARG;
+  size_t q = 0;
+  for (int k = f->l2; k < f->l2 + f->n2; ++k)
+    for (int j = f->l1; j < f->l1 + f->n1; ++j) out[q++] = (*f)(i, j, k);
+  return ICLS_OK;
+}
+// timestep.txt record (main.f90:243-256)
+int ora_timestep_record(ora_ctx* o, int istep, double rec[6]) {
+  double massloss = 0.;
+  for (int l = 0; l < o->L; ++l) massloss = massloss + (1. - o->volume[l] / o->init_volume[l]);
+  double quck = 0.;
+  if (o->L >= 2) {
+    o->ipot();
+    quck = o->dmin[0 + (size_t)o->L * 1] / o->dz;
+  }
+  rec[0] = 1. * istep; rec[1] = o->time; rec[2] = o->dt;
+  rec[3] = massloss; rec[4] = quck; rec[5] = o->maxchk_glb;
+  return ICLS_OK;
+}
 int ora_tube_construction(ora_ctx* o, int l) { LCHK; o->tube_construction(l - 1); return ICLS_OK; }
 int ora_ls_advection(ora_ctx* o, int l) { NEED_INIT; LCHK; o->ls_advection(l - 1); return ICLS_OK; }
 int ora_ls_mass_correction(ora_ctx* o, int istep, int l) { NEED_INIT; LCHK; o->ls_mass_correction(istep, l - 1); return ICLS_OK; }

@@ -46,6 +46,8 @@ int ora_average_vel_at_center(ora_ctx* ctx);
 int ora_max_vel_at_center(ora_ctx* ctx, double* vel_max);
 int ora_disp(ora_ctx* ctx, int l, double cg[3], double vel[3]);
 int ora_set_inflow(ora_ctx* ctx, const double* v_inflow);
+int ora_download_plane_x(ora_ctx* ctx, int id, int l, int i, double* out);
+int ora_timestep_record(ora_ctx* ctx, int istep, double rec[6]);
 int ora_write_checkpoint(ora_ctx* ctx, const char* path, int nr, int history);
 int ora_read_checkpoint(ora_ctx* ctx, const char* path, int* nr);
 int ora_chkdiv(ora_ctx* ctx, int istep, double* divtot, double* divmax, int ijk[3]);
