@@ -375,33 +375,40 @@ double outside_count(const Ctx& c, const Region& r) {
 // band extents measured by the last tube_construction sweep.  A periodic
 // axis keeps the narrower of the spans seen from two frames half a period
 // apart, so a band across the seam gives its true width.
+// drop l's band box from the host copy of the device extents; false when
+// the drop's array held nothing but far field
+bool read_band(Ctx& c, int l) {
+  const Params& P = c.P;
+  DropWin& w = c.win[l];
+  const int* lo = c.h_bbox + 5 * l;
+  const int* hi = c.h_bbox + 5 * P.L + 5 * l;
+  if (lo[4] > hi[4]) return false;
+  auto span = [](const int* lo2, const int* hi2, int n, int& a, int& len) {
+    const int nA = hi2[0] - lo2[0] + 1, nB = hi2[1] - lo2[1] + 1;
+    if (nA <= nB) {
+      a = lo2[0];
+      len = nA;
+    } else {
+      a = wrap1(lo2[1] - n / 2, n);
+      len = nB;
+    }
+  };
+  span(lo, hi, P.imax, w.Dxa, w.Dxn);
+  span(lo + 2, hi + 2, P.jmax, w.Dya, w.Dyn);
+  w.Dz0 = lo[4];
+  w.Dz1 = hi[4];
+  return true;
+}
 int collect_bbox(Ctx& c) {
   if (!c.bbox_pending) return ICLS_OK;
   CK(cudaEventSynchronize(c.ev_bbox));
   c.bbox_pending = false;
-  const Params& P = c.P;
-  for (int l = 0; l < P.L; ++l) {
+  for (int l = 0; l < c.P.L; ++l) {
     DropWin& w = c.win[l];
-    const int* lo = c.h_bbox + 5 * l;
-    const int* hi = c.h_bbox + 5 * P.L + 5 * l;
-    if (lo[4] > hi[4]) {
+    if (!read_band(c, l)) {
       w.have_D = false;  // nothing but far field: sweep everything next time
       continue;
     }
-    auto span = [](const int* lo2, const int* hi2, int n, int& a, int& len) {
-      const int nA = hi2[0] - lo2[0] + 1, nB = hi2[1] - lo2[1] + 1;
-      if (nA <= nB) {
-        a = lo2[0];
-        len = nA;
-      } else {
-        a = wrap1(lo2[1] - n / 2, n);
-        len = nB;
-      }
-    };
-    span(lo, hi, P.imax, w.Dxa, w.Dxn);
-    span(lo + 2, hi + 2, P.jmax, w.Dya, w.Dyn);
-    w.Dz0 = lo[4];
-    w.Dz1 = hi[4];
     w.grow = w.pending_grow;
     w.have_D = true;
   }
@@ -720,6 +727,58 @@ std::vector<int> group_drops(const Ctx& c, int g) {
 }
 int n_groups(const Ctx& c) { return (c.P.L + (int)c.mem.size() - 1) / (int)c.mem.size(); }
 
+// Every drop's band box as a tube_construction sweep of its whole array
+// would measure it now.  The first sweep then needs only that box grown by
+// the step's own spread: outside it the sweep would write +6dz, the value
+// the box's far field stands for.  The stored arrays stay valid everywhere
+// (a download still returns them as uploaded).
+int measure_bands(Ctx& c) {
+  if (!c.use_boxes) return ICLS_OK;
+  const int L = c.P.L;
+  collect_bbox(c);
+  CK(cudaMemsetAsync(c.d_bbox, 0x7F, sizeof(int) * 5 * L, c.s));
+  CK(cudaMemsetAsync(c.d_bbox + 5 * L, 0x80, sizeof(int) * 5 * L, c.s));
+  for (int l = 0; l < L; ++l) launch_band_extents(c, l);
+  CK(cudaMemcpyAsync(c.h_bbox, c.d_bbox, sizeof(int) * 10 * L, cudaMemcpyDeviceToHost, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  for (int l = 0; l < L; ++l) {
+    DropWin& w = c.win[l];
+    w.valid = full_region(c.P);
+    if (!read_band(c, l)) {
+      w.have_D = false;
+      w.box = w.valid;
+      continue;
+    }
+    w.grow = 0;
+    w.have_D = true;
+    w.bg = c.P.NB;
+    w.bg_ghost = c.P.NB;
+    w.bg_valid = true;
+    w.box = sweep_region(c, l, 0);
+  }
+  return ICLS_OK;
+}
+
+// A drop without a measured band (the first step after its array was
+// uploaded or swept whole) runs its tube construction over the whole array.
+// That sweep leaves every cell outside the band box it measures at +6dz, so
+// the rest of the step needs only that box grown by this step's own spread:
+// read the extents now (one wait on the stream, on such steps only) and make
+// that region the drop's sweep and valid region.
+int narrow_after_tube(Ctx& c, const std::vector<int>& drops, int g_now) {
+  CK(cudaMemcpyAsync(c.h_bbox, c.d_bbox, sizeof(int) * 10 * c.P.L, cudaMemcpyDeviceToHost, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  for (int l : drops) {
+    DropWin& w = c.win[l];
+    if (w.have_D || !read_band(c, l)) continue;
+    w.grow = 0;
+    w.have_D = true;
+    w.box = sweep_region(c, l, g_now);
+    w.valid = w.box;
+  }
+  return ICLS_OK;
+}
+
 int ls_main(Ctx& c, int istep) {
   c.last_inflated = 0;
   int rc = collect_bbox(c);
@@ -741,7 +800,14 @@ int ls_main(Ctx& c, int istep) {
   for (int g = 0; g < n_groups(c); ++g) {
     const std::vector<int> drops = group_drops(c, g);
     std::vector<LsBatch> bs = make_batches(drops, kStageRows, [&](int l) { return c.win[l].box; });
+    bool unmeasured = false;
+    for (int l : drops) unmeasured = unmeasured || (c.use_boxes && !c.win[l].have_D);
     tube_batches(c, bs);
+    if (unmeasured) {
+      rc = narrow_after_tube(c, drops, g_now);
+      if (rc) return rc;
+      bs = make_batches(drops, kStageRows, [&](int l) { return c.win[l].box; });
+    }
     rk3_batches(c, bs, c.cfg.ls_adv_space, true, c.ucc, c.vcc, c.wcc);
     if (c.cfg.mass_correction)
       for (int l : drops) {
@@ -1101,6 +1167,8 @@ int icls_init_program(icls_ctx* h) {
   launch_bounduvw(c, c.u, c.v, c.w);
   launch_bounduvw(c, c.dudt, c.dvdt, c.dwdt);
   for (int l = 0; l < c.P.L; ++l) launch_boundmls(c, c.lv[l]);
+  int rc = measure_bands(c);
+  if (rc) return rc;
   launch_boundp(c, c.pnew);
   launch_average_vel(c);
   update_materials(c);

@@ -227,6 +227,8 @@ void launch_boundp(Ctx& c, double* p);
 void launch_ywalls_uvw(Ctx& c, double* u, double* v, double* w);
 void launch_ywalls_p(Ctx& c, double* p);
 void launch_nan_probe(Ctx& c);
+// drop l's band box as a whole-array tube sweep would measure it, into d_bbox
+void launch_band_extents(Ctx& c, int l);
 // dst(j,k) = d(ioff + nx j + nx ny k) in FP64 (d holds float when f32)
 void launch_gather_plane_x(Ctx& c, const double* d, bool f32, long long nx, long long ny, long long ioff, int n1,
                            int n2, double* dst);
@@ -237,6 +239,8 @@ void launch_chkdiv(Ctx& c);
 void launch_chkdt(Ctx& c);
 void launch_maxvel(Ctx& c);
 void launch_nan_probe(Ctx& c);
+// drop l's band box as a whole-array tube sweep would measure it, into d_bbox
+void launch_band_extents(Ctx& c, int l);
 // dst(j,k) = d(ioff + nx j + nx ny k) in FP64 (d holds float when f32)
 void launch_gather_plane_x(Ctx& c, const double* d, bool f32, long long nx, long long ny, long long ioff, int n1,
                            int n2, double* dst);

@@ -55,6 +55,54 @@ __device__ __forceinline__ bool interior(const Params& p, int i, int j, int k) {
   return i >= 1 && i <= p.imax && j >= 1 && j <= p.jmax && k >= 1 && k <= p.kmax;
 }
 
+// ---------------------------------------------------------------- band extents
+// The band box a tube_construction sweep of the whole array would measure
+// (the cells of rows -2..k1+2 whose clipped value differs from +NB, rows 0
+// and k1 by the wall extrapolation), in the same two frames per periodic
+// axis, without writing anything: one thread per (i,j) column.
+template <typename T>
+__global__ void __launch_bounds__(NT) k_band_extents(Params p, const T* __restrict__ phi, int l,
+                                                     int* __restrict__ bbox_lo, int* __restrict__ bbox_hi) {
+  const long long q = blockIdx.x * (long long)NT + threadIdx.x;
+  int lo[5] = {INT_MAX, INT_MAX, INT_MAX, INT_MAX, INT_MAX};
+  int hi[5] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN};
+  if (q < (long long)p.imax * p.jmax) {
+    const int i = (int)(q % p.imax) + 1, j = (int)(q / p.imax) + 1;
+    const int hx = p.imax / 2, hy = p.jmax / 2;
+    const int ib = i + hx > p.imax ? i + hx - p.imax : i + hx;
+    const int jb = j + hy > p.jmax ? j + hy - p.jmax : j + hy;
+    const T NB = TC(p.NB);
+    const long long sz = (long long)p.nLx * p.nLy, c0 = idxL(p, i, j, 0);
+    for (int k = -2; k <= p.k1 + 2; ++k) {
+      T val;
+      if (k == 0)
+        val = TC(2.) * clipNB(phi[c0 + sz], NB) - clipNB(phi[c0 + 2 * sz], NB);
+      else if (k == p.k1)
+        val = TC(2.) * clipNB(phi[c0 + p.kmax * sz], NB) - clipNB(phi[c0 + (p.kmax - 1) * sz], NB);
+      else
+        val = clipNB(phi[c0 + k * sz], NB);
+      if (val != NB) {
+        lo[0] = min(lo[0], i); hi[0] = max(hi[0], i);
+        lo[1] = min(lo[1], ib); hi[1] = max(hi[1], ib);
+        lo[2] = min(lo[2], j); hi[2] = max(hi[2], j);
+        lo[3] = min(lo[3], jb); hi[3] = max(hi[3], jb);
+        lo[4] = min(lo[4], k); hi[4] = max(hi[4], k);
+      }
+    }
+  }
+  for (int a = 0; a < 5; ++a) {
+    int lv = lo[a], h = hi[a];
+    for (int o = 16; o > 0; o >>= 1) {
+      lv = min(lv, __shfl_down_sync(0xffffffffu, lv, o));
+      h = max(h, __shfl_down_sync(0xffffffffu, h, o));
+    }
+    if ((threadIdx.x & 31) == 0 && lv != INT_MAX) {
+      atomicMin(&bbox_lo[5 * l + a], lv);
+      atomicMax(&bbox_hi[5 * l + a], h);
+    }
+  }
+}
+
 // ---------------------------------------------------------------- tube
 // Clip to +-NB (levelset.f90:120-128) and the band mask (130-160) over the
 // tasks' regions.  phi0 holds valid data on vin's written cells, bgin
@@ -1019,6 +1067,15 @@ void launch_tube(Ctx& c, const LsBatch& b) {
   int* hi = c.d_bbox + 5 * c.P.L;
   BY_FORM(c, (k_tube<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.d_nbcnt, lo, hi)),
           (k_tube<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.d_nbcnt, lo, hi)));
+}
+
+void launch_band_extents(Ctx& c, int l) {
+  Scope sc_(c.prof, c.s, "band_extents", 1);
+  int* lo = c.d_bbox;
+  int* hi = c.d_bbox + 5 * c.P.L;
+  const unsigned g = (unsigned)(((long long)c.P.imax * c.P.jmax + NT - 1) / NT);
+  BY_FORM(c, (k_band_extents<float><<<g, NT, 0, c.s>>>(c.P, reinterpret_cast<const float*>(c.lv[l]), l, lo, hi)),
+          (k_band_extents<double><<<g, NT, 0, c.s>>>(c.P, c.lv[l], l, lo, hi)));
 }
 
 template <typename T>
