@@ -58,6 +58,15 @@ def make_workload(name):
         return rising_bubble(128)
     if name == "combined_96_12":  # the same kinds of input at 96^3 (16 x 6), 12 drops of 7-10 cells
         return combined(96, 12, rmin=0.07, rmax=0.1)
+    if name.endswith("_walls") and name.startswith("multi_drop_"):
+        # the same drops between walls at y = 0 and y = ly (BC_in_y = 'Walls':
+        # solver2d_cos, no driving gradient)
+        from icls_gpu.config import BCY_WALLS
+        wl = make_workload(name[:-len("_walls")])
+        wl.cfg.bc_y = BCY_WALLS
+        wl.cfg.constPoi = 0
+        wl.name = name
+        return wl
     raise SystemExit("unknown workload %s" % name)
 
 
