@@ -727,23 +727,26 @@ std::vector<int> group_drops(const Ctx& c, int g) {
 }
 int n_groups(const Ctx& c) { return (c.P.L + (int)c.mem.size() - 1) / (int)c.mem.size(); }
 
-// Every drop's band box as a tube_construction sweep of its whole array
-// would measure it now.  The first sweep then needs only that box grown by
-// the step's own spread: outside it the sweep would write +6dz, the value
-// the box's far field stands for.  The stored arrays stay valid everywhere
-// (a download still returns them as uploaded).
+// The band box a tube_construction sweep of the whole array would measure
+// now, for every drop whose stored array is valid everywhere (as after an
+// upload).  The first sweep then needs only that box grown by the step's
+// own spread: outside it the sweep would write +6dz, the value the box's far
+// field stands for.  The stored arrays stay valid everywhere (a download
+// still returns them as uploaded); a drop already swept by boxes keeps its
+// state.
 int measure_bands(Ctx& c) {
   if (!c.use_boxes) return ICLS_OK;
   const int L = c.P.L;
   collect_bbox(c);
   CK(cudaMemsetAsync(c.d_bbox, 0x7F, sizeof(int) * 5 * L, c.s));
   CK(cudaMemsetAsync(c.d_bbox + 5 * L, 0x80, sizeof(int) * 5 * L, c.s));
-  for (int l = 0; l < L; ++l) launch_band_extents(c, l);
+  for (int l = 0; l < L; ++l)
+    if (is_full(c.P, c.win[l].valid)) launch_band_extents(c, l);
   CK(cudaMemcpyAsync(c.h_bbox, c.d_bbox, sizeof(int) * 10 * L, cudaMemcpyDeviceToHost, c.s));
   CK(cudaStreamSynchronize(c.s));
   for (int l = 0; l < L; ++l) {
     DropWin& w = c.win[l];
-    w.valid = full_region(c.P);
+    if (!is_full(c.P, w.valid)) continue;
     if (!read_band(c, l)) {
       w.have_D = false;
       w.box = w.valid;
