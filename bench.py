@@ -42,14 +42,21 @@ UNIT = "Mcell-steps/s"
 
 
 # ------------------------------------------------------------------ workload
+MULTI_DROP = {"multi_drop_256_48": dict(n=256, ndrop=48, seed=2024),
+              "multi_drop_256_4": dict(n=256, ndrop=4, seed=2024),
+              "multi_drop_128_12": dict(n=128, ndrop=12, seed=2024, rmin=0.06, rmax=0.12)}
+
+
 def make_workload(name):
     from icls_gpu.config import combined, multi_drop, rising_bubble, static_drop
-    if name == "multi_drop_256_48":
-        return multi_drop(n=256, ndrop=48, seed=2024)
-    if name == "multi_drop_256_4":
-        return multi_drop(n=256, ndrop=4, seed=2024)
-    if name == "multi_drop_128_12":
-        return multi_drop(n=128, ndrop=12, seed=2024, rmin=0.06, rmax=0.12)
+    if name in MULTI_DROP:
+        return multi_drop(**MULTI_DROP[name])
+    if name.endswith("_walls") and name[:-len("_walls")] in MULTI_DROP:
+        # the same kind of box between walls at y = 0 and y = ly (BC_in_y =
+        # 'Walls'), its drops seeded clear of them as of the z walls
+        wl = multi_drop(**MULTI_DROP[name[:-len("_walls")]], y_walls=True)
+        wl.name = name
+        return wl
     if name == "static_drop_64":
         return static_drop(64)
     if name == "static_drop_256":  # one drop: full-size field kernels with a few GB on the device
@@ -58,15 +65,6 @@ def make_workload(name):
         return rising_bubble(128)
     if name == "combined_96_12":  # the same kinds of input at 96^3 (16 x 6), 12 drops of 7-10 cells
         return combined(96, 12, rmin=0.07, rmax=0.1)
-    if name.endswith("_walls") and name.startswith("multi_drop_"):
-        # the same drops between walls at y = 0 and y = ly (BC_in_y = 'Walls':
-        # solver2d_cos, no driving gradient)
-        from icls_gpu.config import BCY_WALLS
-        wl = make_workload(name[:-len("_walls")])
-        wl.cfg.bc_y = BCY_WALLS
-        wl.cfg.constPoi = 0
-        wl.name = name
-        return wl
     raise SystemExit("unknown workload %s" % name)
 
 

@@ -632,21 +632,23 @@ __global__ void __launch_bounds__(256) k_cosq_z(Params p, const double* __restri
 //   VCOSQF: V_k = W_k (y_k - i y_{N-k})/2 (y_N = 0), z = sum_k V_k e^{+2 pi i kn/N},
 //           out_{2n} = z_n/sqrt N, out_{2n+1} = z_{N-1-n}/sqrt N.
 // Columns 2c and 2c+1 of the CTA's 32 i travel as the real and imaginary
-// parts of complex line c; the transform is smem_fft (bit-reversed input).
-constexpr int CZ_LINES = CZ_TI / 2;
+// parts of complex line c (16 lines, 66 KB of shared memory per CTA for
+// N = 256; 16 columns per CTA measured no faster); the transform is
+// smem_fft (bit-reversed input).
+constexpr int CZF_TI = 32, CZ_LINES = CZF_TI / 2;  // columns and complex lines per CTA
 __device__ __forceinline__ int makhoul_pos(int k, int N) { return (k & 1) ? N - 1 - (k >> 1) : (k >> 1); }
 __global__ void __launch_bounds__(256) k_cosq_fft_z(Params p, int dir, int logN, const double2* __restrict__ tw,
                                                     const double2* __restrict__ cw, double* __restrict__ spec) {
   extern __shared__ double2 czb[];  // [CZ_LINES][N+1]
   const int N = p.kmax, ld = N + 1;
-  const int i0 = 1 + CZ_TI * (int)blockIdx.x, j = 1 + (int)blockIdx.y;
+  const int i0 = 1 + CZF_TI * (int)blockIdx.x, j = 1 + (int)blockIdx.y;
   const long long plane = (long long)p.imax * p.jmax;
   double* __restrict__ base = spec + (i0 - 1) + (long long)p.imax * (j - 1);
-  const int ni = min(CZ_TI, p.imax - i0 + 1);
+  const int ni = min(CZF_TI, p.imax - i0 + 1);
   const double rs = 1. / sqrt((double)N);
   if (dir == 0) {
-    for (int t = threadIdx.x; t < N * CZ_TI; t += blockDim.x) {
-      const int k = t / CZ_TI, l = t - k * CZ_TI;
+    for (int t = threadIdx.x; t < N * CZF_TI; t += blockDim.x) {
+      const int k = t / CZF_TI, l = t - k * CZF_TI;
       double* slot = reinterpret_cast<double*>(&czb[(l >> 1) * ld + bitrev(makhoul_pos(k, N), logN)]) + (l & 1);
       *slot = l < ni ? base[l + plane * k] : 0.;
     }
@@ -664,8 +666,8 @@ __global__ void __launch_bounds__(256) k_cosq_fft_z(Params p, int dir, int logN,
   }
   __syncthreads();
   smem_fft(czb, CZ_LINES, N, logN, ld, tw, dir);
-  for (int t = threadIdx.x; t < N * CZ_TI; t += blockDim.x) {
-    const int k = t / CZ_TI, l = t - k * CZ_TI;
+  for (int t = threadIdx.x; t < N * CZF_TI; t += blockDim.x) {
+    const int k = t / CZF_TI, l = t - k * CZF_TI;
     if (l >= ni) continue;
     const double2* L = czb + (l >> 1) * ld;
     double out;
@@ -952,8 +954,9 @@ void launch_solver2d_cos(Ctx& c, int write_halos) {
   const bool fz = (P.kmax & (P.kmax - 1)) == 0 && P.kmax >= 8 && P.kmax <= kCosqFftMaxN;
   const int lz = ilog2(P.kmax);
   const size_t smf = (size_t)CZ_LINES * (P.kmax + 1) * sizeof(double2);
+  const dim3 gzf((unsigned)((P.imax + CZF_TI - 1) / CZF_TI), (unsigned)P.jmax, 1);
   auto cosq = [&](int dir) {
-    if (fz) k_cosq_fft_z<<<gz, 256, smf, c.s>>>(P, dir, lz, c.twy, c.czw, c.spec);
+    if (fz) k_cosq_fft_z<<<gzf, 256, smf, c.s>>>(P, dir, lz, c.twy, c.czw, c.spec);
     else k_cosq_z<<<gz, 256, smz, c.s>>>(P, dir ? c.cosf : c.cosb, c.spec);
   };
   if (!fft2_pass<false>(c, 0, 0)) k_fft_x<<<gx, FT, smx, c.s>>>(P, 0, CL, lx, c.twx, c.p, c.spec, 0);

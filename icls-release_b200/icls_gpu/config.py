@@ -227,11 +227,11 @@ def init_drops_boxed(cfg: IclsConfig, centres, radii, cap_cells: float = 12.0) -
 
 
 def seeded_drops(cfg: IclsConfig, ndrop: int, rmin: float, rmax: float, seed: int,
-                 gap_cells: float = 4.0, max_tries: int = 200000):
+                 gap_cells: float = 4.0, max_tries: int = 200000, y_walls: bool = False):
     """Seeded drop radii/centres: radii uniform in [rmin,rmax], centres uniform
-    in the box (kept one radius plus the gap away from the z walls), rejected
-    until every pair keeps ``gap_cells`` cells between surfaces (periodic in
-    x and y)."""
+    in the box (kept one radius plus the gap away from the z walls, and from
+    the y walls too with ``y_walls``), rejected until every pair keeps
+    ``gap_cells`` cells between surfaces (periodic in x and y)."""
     rng = np.random.default_rng(seed)
     dx = cfg.lx / cfg.itot
     gap = gap_cells * dx
@@ -242,8 +242,8 @@ def seeded_drops(cfg: IclsConfig, ndrop: int, rmin: float, rmax: float, seed: in
         if tries > max_tries:
             raise RuntimeError("could not place drops with the requested gap")
         r = rng.uniform(rmin, rmax)
-        c = np.array([rng.uniform(0, cfg.lx), rng.uniform(0, cfg.ly),
-                      rng.uniform(r + gap, cfg.lz - r - gap)])
+        cy = rng.uniform(r + gap, cfg.ly - r - gap) if y_walls else rng.uniform(0, cfg.ly)
+        c = np.array([rng.uniform(0, cfg.lx), cy, rng.uniform(r + gap, cfg.lz - r - gap)])
         ok = True
         for c2, r2 in zip(centres, radii):
             d = c - c2
@@ -295,7 +295,8 @@ def rising_bubble(nx: int = 128, steps: int = 2000, dt: float = 4e-5) -> Workloa
 
 
 def multi_drop(n: int = 256, ndrop: int = 48, seed: int = 2024, steps: int = 1000,
-               rmin: float = 0.03, rmax: float = 0.06, dt: float | None = None) -> Workload:
+               rmin: float = 0.03, rmax: float = 0.06, dt: float | None = None,
+               y_walls: bool = False) -> Workload:
     """Seeded multi-drop shear box: n^3 on [0,1]^3, ndrop drops with radii
     uniform in [rmin,rmax] and a 4-cell surface gap, rho and miu ratio 10,
     We=2 (sigma=0.5), Re=10 (param.f90 default), shear v=0.5(2z-1) between
@@ -306,7 +307,10 @@ def multi_drop(n: int = 256, ndrop: int = 48, seed: int = 2024, steps: int = 100
                       rho1=1.0, rho2=10.0, miu1=1.0, miu2=10.0, Re=10.0, We=2.0,
                       v_wall_lower=-0.5, v_wall_upper=0.5, ls_adv_space=HOUC5,
                       reinit_step=20, reinit_iter_max=1, inflate_step=20)
-    centres, radii = seeded_drops(cfg, ndrop, rmin, rmax, seed)
+    centres, radii = seeded_drops(cfg, ndrop, rmin, rmax, seed, y_walls=y_walls)
+    if y_walls:  # BC_in_y = 'Walls': solver2d_cos, no driving gradient (ab2.f90:103-118)
+        cfg.bc_y = BCY_WALLS
+        cfg.constPoi = 0
     if dt is not None:
         cfg.timestep = dt
     return Workload("multi_drop_%d_%d" % (n, ndrop), cfg, centres, radii, True, 0.5, steps)

@@ -201,3 +201,33 @@ def test_gpu_walls_multistep_parity(bc, yc):
     v = g.download("v")
     if bc == BCY_WALLS:
         assert np.all(v[1:-1, 0, 1:-1] == 0) and np.all(v[1:-1, -2, 1:-1] == 0)
+
+
+@pytest.mark.gpu
+def test_gpu_walls_fp32_form_tracks_fp64():
+    """The FP32 form between y walls: 8 steps stay within the form's
+    tolerances of the FP64 path (volume to 1e-6, velocities to 1e-4 of their
+    scale) with the wall rows exact."""
+    from icls_gpu import FP32
+    from icls_gpu.config import IclsConfig
+    cfg = _walls_config(n=32, bc=BCY_WALLS, inflate_step=4, reinit_step=1, reinit_iter_max=2)
+    cfg.timestep = 1e-4
+    cf = IclsConfig.from_buffer_copy(cfg)
+    cf.precision = FP32
+    ls = init_drops(cfg, [(0.5, 0.5 * cfg.ly, 0.5)], [0.2])
+    uvw = initial_velocity(cfg, 0.0)
+    sims = []
+    for c in (cfg, cf):
+        s = _gpu_solver(c)
+        s.setup(ls, *uvw)
+        for i in range(1, 9):
+            s.step(i, 0)
+        sims.append(s)
+    p64, p32 = sims
+    v0, v1 = p64.volumes()[0][0], p32.volumes()[0][0]
+    assert abs(v1 - v0) / v0 <= 1e-6
+    for k in ("u", "v", "w"):
+        a, b = p32.download(k), p64.download(k)
+        assert np.max(np.abs(a - b)) <= 1e-4 * max(1e-3, np.max(np.abs(b))), k
+    v = p32.download("v")
+    assert np.all(v[1:-1, 0, 1:-1] == 0) and np.all(v[1:-1, -2, 1:-1] == 0)
