@@ -242,8 +242,9 @@ def seeded_drops(cfg: IclsConfig, ndrop: int, rmin: float, rmax: float, seed: in
         if tries > max_tries:
             raise RuntimeError("could not place drops with the requested gap")
         r = rng.uniform(rmin, rmax)
+        cx = rng.uniform(0, cfg.lx)  # draw order x, y, z: the seeded layouts stay fixed
         cy = rng.uniform(r + gap, cfg.ly - r - gap) if y_walls else rng.uniform(0, cfg.ly)
-        c = np.array([rng.uniform(0, cfg.lx), cy, rng.uniform(r + gap, cfg.lz - r - gap)])
+        c = np.array([cx, cy, rng.uniform(r + gap, cfg.lz - r - gap)])
         ok = True
         for c2, r2 in zip(centres, radii):
             d = c - c2
