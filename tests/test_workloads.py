@@ -52,3 +52,25 @@ def test_combined_configuration():
             assert np.linalg.norm(d) >= wl.radii[a] + wl.radii[b] + gap - 1e-12
     u, v, w = workload_velocity(wl)
     assert np.max(np.abs(_divergence(cfg, u, v, w))) <= 1e-12 * 0.2 * 96
+
+
+def test_seeded_layouts_are_fixed():
+    """The benchmark's drop layout is a function of its seed alone: the first
+    and last drops of multi_drop(256, 48) as seeded (draws x, y, z per drop)."""
+    from icls_gpu import multi_drop
+    w = multi_drop(256, 48)
+    assert np.allclose(w.centres[0], (0.21432320123825765, 0.3094520308816917, 0.7599965010723276), rtol=0, atol=1e-15)
+    assert w.radii[0] == 0.05027494013943845
+    assert np.allclose(w.centres[-1], (0.033898820090026094, 0.5818307796575592, 0.630942175696876), rtol=0, atol=1e-15)
+    assert w.radii[-1] == 0.041416709589228044
+
+
+def test_y_walls_seeding_keeps_clear():
+    """With walls in y, every drop keeps one radius plus the 4-cell gap from
+    y = 0 and y = ly, as from the z walls."""
+    from icls_gpu import BCY_WALLS, multi_drop
+    w = multi_drop(128, 12, rmin=0.06, rmax=0.12, y_walls=True)
+    assert w.cfg.bc_y == BCY_WALLS and w.cfg.constPoi == 0
+    gap = 4.0 / 128
+    for c, r in zip(w.centres, w.radii):
+        assert c[1] - r >= gap - 1e-15 and 1.0 - c[1] - r >= gap - 1e-15
