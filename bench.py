@@ -638,6 +638,114 @@ def run_e2e(args, wl, ls, u, v, w, torch, world, net=None):
             "ms_total": ms}
 
 
+def combined_full(args):
+    """The combined configuration at its full size (384^3, 200 drops of
+    radius 0.02-0.04, random solenoidal k^-5/3 velocity, rms 0.2): the plain
+    FP64 context, then the FP32 + learned-curvature form, each alone on the
+    device (together they would not fit: 200 whole-domain level sets are
+    95 GB in FP64).  Each drop's level set is built on the host and uploaded
+    one at a time.  After the FP64 run, the quantities the form is compared
+    with (velocities, volumes, the first four drops' bands, the first eight
+    drops' shell curvature) are kept on the host.  One JSON line."""
+    import gc
+    import torch
+    from icls_gpu import CURV_MLP, FP32, Solver, field_shape
+    from icls_gpu.binding import curvature_stats
+    from icls_gpu.config import IclsConfig, combined, init_drops_boxed, workload_velocity
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    wl = combined()
+    cfg = wl.cfg
+    h = cfg.lz / cfg.ktot
+    cells = cfg.itot * cfg.jtot * cfg.ktot
+    u, v, w = workload_velocity(wl)
+    zeros = np.zeros(field_shape(cfg, "p"), order="F")
+    shells = drop_shells(wl)[:8]
+    net, net_info = train_network(torch)
+    torch.cuda.empty_cache()  # the training's cached blocks back to the device
+
+    def start(c, attach):
+        s = Solver(c)
+        if attach:
+            net.attach(s)
+        for name, a in (("u", u), ("v", v), ("w", w), ("pnew", zeros)):
+            s.upload(name, a)
+        for l, (cen, r) in enumerate(zip(wl.centres, wl.radii), start=1):
+            s.upload("lvset", init_drops_boxed(cfg, [cen], [r])[..., 0], l)
+        s.init_program()
+        return s
+
+    band_idx = []  # the FP64 run's |phi| <= 4dz cells of drops 1-4 (flat indices)
+
+    def state(s):
+        out = {k: s.download(k) for k in ("u", "v", "w")}
+        out["vol"], out["vol0"] = s.volumes()
+        out["bands"] = []
+        for l in range(1, 5):
+            phi = s.download("lvset", l).ravel(order="F")
+            if len(band_idx) < l:
+                band_idx.append(np.flatnonzero(np.abs(phi) <= 4 * h))
+            out["bands"].append(phi[band_idx[l - 1]].copy())
+            del phi
+        out["curv"] = []
+        for l, (flat, r) in enumerate(shells, start=1):
+            s.get_curvature(l)
+            out["curv"].append(s.download("curv").ravel(order="F")[flat].copy())
+        return out
+
+    res = {}
+    for label, c, attach in (("fp64", cfg, False), ("fp32_learned_kappa", None, True)):
+        if c is None:
+            c = IclsConfig.from_buffer_copy(cfg)
+            c.precision = FP32
+            c.curvature_model = CURV_MLP
+        s = start(c, attach)
+        ms, istep, launches, clocks = timed_steps(s, args, world, torch, 0, label, ClockSampler(local))
+        r = {"value": cells * args.steps / (ms / 1000.0) / 1e6, "ms_per_step": ms / args.steps,
+             "gpu_launches": launches, "clocks": clocks}
+        if attach:
+            ev, fb = curvature_stats(s, reset=True)
+            r["fallback_fraction"] = fb / max(ev, 1)
+            r["network_cells_per_step"] = ev / max(args.warmup + args.steps, 1)
+        r["state"] = state(s)
+        res[label] = r
+        s.close()
+        del s
+        gc.collect()
+        torch.cuda.synchronize()
+
+    def rel(a, b):
+        return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+    a, b = res["fp32_learned_kappa"].pop("state"), res["fp64"].pop("state")
+    band = max(rel(pa, pb) for pa, pb in zip(a["bands"], b["bands"]))
+    e_form = sum(float(np.sum((ka + 2.0 / r) ** 2)) for ka, (_, r) in zip(a["curv"], shells))
+    e_fp64 = sum(float(np.sum((kb + 2.0 / r) ** 2)) for kb, (_, r) in zip(b["curv"], shells))
+    ncell = sum(f.size for f, _ in shells)
+    errors = {
+        "steps": args.warmup + args.steps, "phi_band_rel_l2_first4": band,
+        "u_rel_l2": rel(a["u"], b["u"]), "v_rel_l2": rel(a["v"], b["v"]), "w_rel_l2": rel(a["w"], b["w"]),
+        "volume_max_rel_vs_fp64": float(np.max(np.abs(a["vol"] - b["vol"]) / b["vol"])),
+        "volume_drift_max_rel": {"form": float(np.max(np.abs(a["vol"] - a["vol0"]) / a["vol0"])),
+                                 "fp64": float(np.max(np.abs(b["vol"] - b["vol0"]) / b["vol0"]))},
+        "curv_vs_analytic_first8": {"form_kdx_rms": float(np.sqrt(e_form / max(ncell, 1))) * h,
+                                    "fp64_stencil_kdx_rms": float(np.sqrt(e_fp64 / max(ncell, 1))) * h,
+                                    "shell_cells": ncell},
+    }
+    form = res["fp32_learned_kappa"]
+    line = {"metric": "Mcell-steps/s at 384\u00b3 with 200 drops: FP32+learned-\u03ba vs plain FP64 on B200",
+            "workload": "combined_384_200", "value": form["value"], "unit": UNIT,
+            "ms_per_step": form["ms_per_step"], "steps": args.steps, "warmup": args.warmup,
+            "dtype": "f32 (f64 Poisson/pressure, volume integral, GFM jumps; bf16 network, f32 accumulate)",
+            "data": "synthetic (seeded drops, seeded solenoidal velocity)",
+            "config": {"grid": [cfg.itot, cfg.jtot, cfg.ktot], "drops": cfg.lmax, "dt": cfg.timestep,
+                       "We": cfg.We, "Re": cfg.Re},
+            "fp32_learned_kappa": form, "plain_fp64": res["fp64"],
+            "speedup_vs_fp64": form["value"] / res["fp64"]["value"], "errors": errors, "network": net_info}
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -654,6 +762,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload == "combined_384_200":
+        return combined_full(args)
     return ours_arm(args)
 
 
