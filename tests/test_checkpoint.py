@@ -147,3 +147,16 @@ def test_gpu_checkpoint_reads_in_oracle(tmp_path):
     for k in ("u", "v", "w", "lvset"):
         a, b = g.download(k), o.download(k)
         assert np.max(np.abs(a - b)) <= 1e-12 * max(1.0, np.max(np.abs(b))), k
+
+
+@pytest.mark.gpu
+def test_gpu_restart_fp32_form_continues_exactly(tmp_path):
+    """The FP32 form stores its fields as floats; the checkpoint holds them as
+    doubles (exact both ways), so its restart is exact too."""
+    from icls_gpu import FP32, Solver
+    from icls_gpu.config import IclsConfig
+    wl = _workload(32)
+    cf = IclsConfig.from_buffer_copy(wl.cfg)
+    cf.precision = FP32
+    wl.cfg = cf
+    _check_restart(Solver, tmp_path, wl)
