@@ -468,6 +468,10 @@ std::vector<LsBatch> make_batches(const std::vector<int>& drops, int kc, RegionO
 }
 
 constexpr int kStageRows = 8;  // z rows per block of the level-set stage kernels
+// the chunk that starts at row -2 must reach row 2: a column's wall row 0 is
+// written by the thread that holds rows 1 and 2 (measured: 8 rows beat 4
+// and 16)
+static_assert(kStageRows >= 5, "level-set chunks must span rows -2..2");
 
 Ctx::Member& member(Ctx& c, int l) { return c.mem[l % (int)c.mem.size()]; }
 
