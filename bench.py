@@ -708,6 +708,9 @@ def combined_full(args):
             r["fallback_fraction"] = fb / max(ev, 1)
             r["network_cells_per_step"] = ev / max(args.warmup + args.steps, 1)
         r["state"] = state(s)
+        # per-scope times over K more steps (the compared state is taken first)
+        stats = {"band_total": float(sum(s.band_count(l + 1) for l in range(cfg.lmax))), "shell_total": 0.0}
+        _, r["kernels"], istep = kernel_table(s, args, cfg, stats, istep, attach)
         res[label] = r
         s.close()
         del s
