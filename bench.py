@@ -194,11 +194,14 @@ def dist_env():
 
 
 def max_over_ranks(x, world):
+    """The maximum of x over the ranks (the job's time is its slowest rank's),
+    on the process group's own device (NCCL: the GPU; gloo: the host)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
