@@ -260,7 +260,8 @@ def seeded_drops(cfg: IclsConfig, ndrop: int, rmin: float, rmax: float, seed: in
 
 
 # --------------------------------------------------------------------------
-# workloads named by BASELINE configs (see DESIGN.md for the mapping)
+# the measured workloads: a static drop, the rising bubble, seeded multi-drop
+# layouts and the combined turbulent case, each with its grid and step count
 @dataclass
 class Workload:
     name: str
