@@ -7,6 +7,7 @@ drop, materials, AB2 predictor, Poisson RHS with GFM jumps, FFT/Thomas
 pressure solve, projection, pressure update.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --drift-steps 1000 [--inflate-step S] [--dt DT]   (volume record, no timing)
 
 Default workload: the 256^3 box with 48 seeded drops.  The headline value is
 the FP32 form with the learned curvature in the loop (FP64 kept for the
@@ -752,6 +753,92 @@ def combined_full(args):
     return 0
 
 
+def volume_drift(args):
+    """The volume record over a long run: the plain FP64 context and the FP32
+    + learned-curvature form advance the same initial state side by side for
+    --drift-steps steps.  Every drop's volume is read after each sampled step
+    (k_volumes integrates it every step); the line gives, for each context,
+    the largest |V - V0| / V0 seen over the run and at its end, the form's
+    largest per-drop volume difference from FP64, and at the end the phi band
+    and velocity differences.  It is a report, not a throughput line."""
+    import torch
+    rank, world, local = dist_env()
+    if world != 1:
+        raise SystemExit("--drift-steps runs on one GPU")
+    torch.cuda.set_device(local)
+    from icls_gpu import CURV_MLP, FP32, Solver
+    from icls_gpu.binding import curvature_stats
+    from icls_gpu.config import IclsConfig
+    wl = make_workload(args.workload)
+    cfg = wl.cfg
+    if args.dt:
+        cfg.timestep = args.dt
+    if args.inflate_step:
+        cfg.inflate_step = args.inflate_step
+    ls, u, v, w = initial_state(wl)
+    h = cfg.lz / cfg.ktot
+    net, net_info = train_network(torch)
+    ref = Solver(cfg)
+    ref.setup(ls, u, v, w)
+    cf = IclsConfig.from_buffer_copy(cfg)
+    cf.precision = FP32
+    cf.curvature_model = CURV_MLP
+    s = Solver(cf)
+    net.attach(s)
+    s.setup(ls, u, v, w)
+    n = args.drift_steps
+    every = max(n // 50, 1)
+    worst = {"form": 0.0, "fp64": 0.0}
+    vs_fp64 = 0.0
+    record = []
+    stopped = None
+    t0 = time.perf_counter()
+    for istep in range(1, n + 1):
+        try:
+            ref.step(istep, 0)
+            s.step(istep, 0)
+        except Exception as e:  # a divergence or time-step check of either context
+            stopped = {"step": istep, "error": str(e)}
+            break
+        if istep % every == 0 or istep == n or istep % cfg.inflate_step in (0, 1):
+            va, va0 = s.volumes()
+            vb, vb0 = ref.volumes()
+            da = float(np.max(np.abs(va - va0) / va0))
+            db = float(np.max(np.abs(vb - vb0) / vb0))
+            worst["form"] = max(worst["form"], da)
+            worst["fp64"] = max(worst["fp64"], db)
+            vs_fp64 = max(vs_fp64, float(np.max(np.abs(va - vb) / vb)))
+            if istep % every == 0 or istep == n:
+                record.append([istep, da, db])
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+
+    def rel(a, b):
+        return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+    band = 0.0
+    for l in range(1, min(cfg.lmax, 4) + 1):
+        pa, pb = s.download("lvset", l), ref.download("lvset", l)
+        m = np.abs(pb) <= 4.0 * h
+        band = max(band, rel(pa[m], pb[m]))
+    ev, fb = curvature_stats(s, reset=True)
+    sc = ref.scalars()
+    line = {
+        "report": "volume_drift", "workload": wl.name, "steps": n, "dt": sc["dt"], "time": sc["time"],
+        "inflate_step": cfg.inflate_step, "reinit_step": cfg.reinit_step, "drops": cfg.lmax,
+        "drift_max_rel_over_run": worst, "drift_max_rel_at_end": {"form": record[-1][1] if record else None,
+                                                           "fp64": record[-1][2] if record else None},
+        "volume_max_rel_form_vs_fp64": vs_fp64,
+        "at_end": {"phi_band_rel_l2_first4": band, "u_rel_l2": rel(s.download("u"), ref.download("u")),
+                   "v_rel_l2": rel(s.download("v"), ref.download("v")),
+                   "w_rel_l2": rel(s.download("w"), ref.download("w"))},
+        "network_fallback_fraction": fb / max(ev, 1), "network": net_info,
+        "record_step_drift_form_fp64": record, "stopped": stopped, "wall_s": round(wall, 1)}
+    del s, ref
+    net.close()
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -763,11 +850,19 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-forms", action="store_true",
                     help="plain FP64 only (no network training, no FP32 forms)")
+    ap.add_argument("--dt", type=float, default=0.0, help="with --drift-steps: the time step (default: the workload's)")
+    ap.add_argument("--inflate-step", type=int, default=0,
+                    help="with --drift-steps: the mass-correction cadence (default: the workload's)")
+    ap.add_argument("--drift-steps", type=int, default=0,
+                    help="instead of timing: run FP64 and the form side by side this many steps, "
+                         "report the drop volumes' drift")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
         return reference_arm(args)
+    if args.drift_steps > 0:
+        return volume_drift(args)
     if args.workload == "combined_384_200":
         return combined_full(args)
     return ours_arm(args)

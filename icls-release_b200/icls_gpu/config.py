@@ -304,7 +304,11 @@ def multi_drop(n: int = 256, ndrop: int = 48, seed: int = 2024, steps: int = 100
     We=2 (sigma=0.5), Re=10 (param.f90 default), shear v=0.5(2z-1) between
     walls moving at -+0.5 (the shear is put along y, the direction the
     reference's moving-wall boundary acts on; x and y are equivalent
-    periodic directions), HOUC5, reference reinit/inflation cadence (20)."""
+    periodic directions), HOUC5, reference reinit/inflation cadence (20).
+    That cadence is stable for the mass correction only below n ~= 90 on the
+    unit box (each correction multiplies the volume error by 1 - K/20, K ~=
+    0.44 n); at 256^3 the first correction, near step 280, starts a
+    growing oscillation, and inflate_step ~= 112 corrects in one go."""
     cfg = make_config(itot=n, jtot=n, ktot=n, lmax=ndrop, timestep=1e-5,
                       rho1=1.0, rho2=10.0, miu1=1.0, miu2=10.0, Re=10.0, We=2.0,
                       v_wall_lower=-0.5, v_wall_upper=0.5, ls_adv_space=HOUC5,

@@ -1,0 +1,50 @@
+"""The gain of the reference's mass correction (levelset.f90:377-582).
+
+inflation() advects the level set for one time step with the velocity
+-temp * grad(H) (times kappa / the kappa-weighted area in the 'curv' mode),
+temp = loss_rate / area and loss_rate = (V - V0) / (inflate_step * dt).  The
+interface therefore moves at temp * H'(0) = temp / s1 (s1 = 1.5 dz), and one
+correction removes K / inflate_step of the volume error, K ~= 0.66 / s1 in
+the units of the grid.  The error is multiplied by 1 - K / inflate_step at
+each correction: it shrinks while inflate_step > K / 2 and grows otherwise
+(at 256^3 in a unit box K ~= 112, so the reference cadence of 20 multiplies
+it by about -4.6).  These tests pin that gain on the oracle with a static
+drop whose level set is replaced, after init_program, by a slightly smaller
+sphere's."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from icls_gpu import init_drops, initial_velocity, make_config
+
+
+def _factor(n, inflate_step, make=Oracle, shrink=1e-3, R=0.25):
+    """The volume error after the first correction over the error before."""
+    cfg = make_config(itot=n, jtot=n, ktot=n, lmax=1, timestep=1e-5,
+                      inflate_step=inflate_step, reinit_step=100000)
+    o = make(cfg)
+    o.setup(init_drops(cfg, [(0.5, 0.5, 0.5)], [R]), *initial_velocity(cfg, 0.0))
+    o.upload("lvset", init_drops(cfg, [(0.5, 0.5, 0.5)], [R * (1 - shrink)])[..., 0], 1)
+    for s in range(1, inflate_step):
+        o.step(s, 0)
+    v, v0 = o.volumes()
+    before = (v[0] - v0[0]) / v0[0]
+    o.step(inflate_step, 0)
+    assert o.scalars()["maxchk_glb"] != 0.0   # the correction ran
+    v, v0 = o.volumes()
+    return ((v[0] - v0[0]) / v0[0]) / before
+
+
+@pytest.mark.parametrize("n,inflate_step", [(32, 20), (32, 10), (64, 20)])
+def test_correction_gain_scales_with_one_over_s1(n, inflate_step):
+    K = 0.656 * n / 1.5          # 0.656 / s1 on the unit box
+    assert abs(_factor(n, inflate_step) - (1.0 - K / inflate_step)) < 0.05
+
+
+@pytest.mark.gpu
+def test_gpu_correction_gain_matches_oracle():
+    """The CUDA path applies the same correction: the same factor within the
+    FP64 parity bound."""
+    from icls_gpu import Solver
+    a, b = _factor(32, 10, Solver), _factor(32, 10)
+    assert abs(a - b) <= 1e-8 * abs(b)
