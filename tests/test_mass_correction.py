@@ -16,12 +16,13 @@ import pytest
 
 from oracle.oracle import Oracle
 from icls_gpu import init_drops, initial_velocity, make_config
+from icls_gpu.config import SPEED_CURV, SPEED_UNFM
 
 
-def _factor(n, inflate_step, make=Oracle, shrink=1e-3, R=0.25):
+def _factor(n, inflate_step, make=Oracle, speed=SPEED_CURV, shrink=1e-3, R=0.25):
     """The volume error after the first correction over the error before."""
     cfg = make_config(itot=n, jtot=n, ktot=n, lmax=1, timestep=1e-5,
-                      inflate_step=inflate_step, reinit_step=100000)
+                      inflate_step=inflate_step, reinit_step=100000, ispeed_dependence=speed)
     o = make(cfg)
     o.setup(init_drops(cfg, [(0.5, 0.5, 0.5)], [R]), *initial_velocity(cfg, 0.0))
     o.upload("lvset", init_drops(cfg, [(0.5, 0.5, 0.5)], [R * (1 - shrink)])[..., 0], 1)
@@ -35,10 +36,13 @@ def _factor(n, inflate_step, make=Oracle, shrink=1e-3, R=0.25):
     return ((v[0] - v0[0]) / v0[0]) / before
 
 
-@pytest.mark.parametrize("n,inflate_step", [(32, 20), (32, 10), (64, 20)])
-def test_correction_gain_scales_with_one_over_s1(n, inflate_step):
+@pytest.mark.parametrize("n,inflate_step,speed", [(32, 20, SPEED_CURV), (32, 10, SPEED_CURV),
+                                                   (64, 20, SPEED_CURV), (32, 10, SPEED_UNFM)])
+def test_correction_gain_scales_with_one_over_s1(n, inflate_step, speed):
+    """Both speed modes: for a sphere the curvature weighting of 'curv'
+    cancels against its kappa-weighted area."""
     K = 0.656 * n / 1.5          # 0.656 / s1 on the unit box
-    assert abs(_factor(n, inflate_step) - (1.0 - K / inflate_step)) < 0.05
+    assert abs(_factor(n, inflate_step, speed=speed) - (1.0 - K / inflate_step)) < 0.05
 
 
 @pytest.mark.gpu
