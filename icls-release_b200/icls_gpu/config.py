@@ -338,7 +338,12 @@ def combined(n: int = 384, ndrop: int = 200, seed: int = 2024, steps: int = 2000
     where the phases mix binds first; chkdt's estimate (chkdt.f90:62-104, the
     larger of the two pure phases' mu/rho) does not see it.  At 384^3 with
     dt = 1e-5 the velocity grows without bound from step 14 (max|u| 0.9 ->
-    58 by step 23), while 4e-6 and 2e-6 stay steady over 60 steps."""
+    58 by step 23), while 4e-6 and 2e-6 stay steady over 60 steps.
+
+    inflate_step stays at the reference's 20, which the timed steps never
+    reach with a volume error above the 1e-5 trigger.  A long run at this
+    size needs it near K ~= 0.44 n (about 170 at 384^3): at 20 each mass
+    correction multiplies the volume error by 1 - K/20."""
     if dt is None:
         dt = 1e-5 if n <= 256 else float("%.2g" % (0.9e-5 * (256.0 / n) ** 2))
     cfg = make_config(itot=n, jtot=n, ktot=n, lmax=ndrop, timestep=dt,
