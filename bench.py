@@ -7,7 +7,8 @@ drop, materials, AB2 predictor, Poisson RHS with GFM jumps, FFT/Thomas
 pressure solve, projection, pressure update.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-  python bench.py --drift-steps 1000 [--inflate-step S] [--dt DT]   (volume record, no timing)
+  python bench.py --drift-steps 1000 [--inflate-step S] [--mass-threshold T] [--dt DT]
+                                                  (volume record, no timing)
 
 Default workload: the 256^3 box with 48 seeded drops.  The headline value is
 the FP32 form with the learned curvature in the loop (FP64 kept for the
@@ -775,6 +776,8 @@ def volume_drift(args):
         cfg.timestep = args.dt
     if args.inflate_step:
         cfg.inflate_step = args.inflate_step
+    if args.mass_threshold:
+        cfg.mass_threshold = args.mass_threshold
     ls, u, v, w = initial_state(wl)
     h = cfg.lz / cfg.ktot
     net, net_info = train_network(torch)
@@ -825,6 +828,7 @@ def volume_drift(args):
     line = {
         "report": "volume_drift", "workload": wl.name, "steps": n, "dt": sc["dt"], "time": sc["time"],
         "inflate_step": cfg.inflate_step, "reinit_step": cfg.reinit_step, "drops": cfg.lmax,
+        "mass_threshold": cfg.mass_threshold or 1e-5,
         "drift_max_rel_over_run": worst, "drift_max_rel_at_end": {"form": record[-1][1] if record else None,
                                                            "fp64": record[-1][2] if record else None},
         "volume_max_rel_form_vs_fp64": vs_fp64,
@@ -853,6 +857,8 @@ def main():
     ap.add_argument("--dt", type=float, default=0.0, help="with --drift-steps: the time step (default: the workload's)")
     ap.add_argument("--inflate-step", type=int, default=0,
                     help="with --drift-steps: the mass-correction cadence (default: the workload's)")
+    ap.add_argument("--mass-threshold", type=float, default=0.0,
+                    help="with --drift-steps: the volume error that triggers a correction (default 1e-5)")
     ap.add_argument("--drift-steps", type=int, default=0,
                     help="instead of timing: run FP64 and the form side by side this many steps, "
                          "report the drop volumes' drift")

@@ -97,6 +97,7 @@ int validate(const icls_config* c) {
   if (c->ktot < 6 || c->lmax < 1) return ICLS_E_CONFIG;
   if (!(c->lx > 0 && c->ly > 0 && c->lz > 0 && c->timestep > 0)) return ICLS_E_CONFIG;
   if (c->reinit_step < 1 || c->inflate_step < 1 || c->reinit_iter_max < 1) return ICLS_E_CONFIG;
+  if (!(c->mass_threshold >= 0.)) return ICLS_E_CONFIG;
   if (c->ls_adv_space != ICLS_HOUC5 && c->ls_adv_space != ICLS_WENO5) return ICLS_E_CONFIG;
   if (c->i_space != ICLS_HOUC5 && c->i_space != ICLS_WENO5) return ICLS_E_CONFIG;
   if (c->precision != ICLS_FP64 && c->precision != ICLS_FP32) return ICLS_E_CONFIG;
@@ -632,7 +633,8 @@ int ls_mass_correction(Ctx& c, int istep, int l) {
     if (rc) return rc;
     const double v0 = c.init_volume_h[l];
     const double massloss = (vol - v0) / v0;
-    if (std::fabs(massloss) > 1e-5) inflation(c, l);
+    const double eps = c.cfg.mass_threshold > 0. ? c.cfg.mass_threshold : 1e-5;
+    if (std::fabs(massloss) > eps) inflation(c, l);
   }
   return ICLS_OK;
 }
@@ -959,6 +961,7 @@ void icls_config_default(icls_config* c) {
   c->ioutchk = 20;
   c->precision = ICLS_FP64; c->curvature_model = ICLS_CURV_STENCIL;
   c->mlp_fallback_tol = 0.02;
+  c->mass_threshold = 0.;
 }
 
 int icls_status_string(int code, char* buf, int n) {

@@ -47,6 +47,7 @@ class IclsConfig(C.Structure):
         ("ioutchk", C.c_int), ("precision", C.c_int), ("curvature_model", C.c_int),
         ("mlp_fallback_tol", C.c_double),
         ("bc_y", C.c_int), ("ns_conv", C.c_int),
+        ("mass_threshold", C.c_double),
     ]
 
     def as_dict(self):
@@ -113,6 +114,7 @@ def make_config(**kw) -> IclsConfig:
     c.precision = FP64
     c.curvature_model = CURV_STENCIL
     c.mlp_fallback_tol = 0.02
+    c.mass_threshold = 0.0                 # 0: the fixed 1e-5 of levelset.f90:382
     for k, v in kw.items():
         if k == "g_unit":
             c.g_unit[:] = list(v)

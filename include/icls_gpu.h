@@ -93,6 +93,9 @@ typedef struct icls_config {
                                     stencil value is kept (MLP form only)   */
   int bc_y;                      /* ICLS_BCY_* (param.f90:115)               */
   int ns_conv;                   /* ICLS_NS_* (param.f90:135)                */
+  double mass_threshold;         /* |V-V0|/V0 above which ls_mass_correction
+                                    inflates a drop; 0 = the reference's
+                                    fixed 1e-5 (levelset.f90:382)           */
 } icls_config;
 
 /* Fill *cfg with the reference defaults of src/param.f90 for a 3-D run. */

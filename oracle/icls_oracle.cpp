@@ -248,6 +248,7 @@ struct ora_ctx {
     if (c.bc_y < ICLS_BCY_PERIODIC || c.bc_y > ICLS_BCY_OUTOUT) return ICLS_E_CONFIG;
     if (c.ns_conv == ICLS_NS_WENO5) return ICLS_E_UNSUPPORTED;  // boundfu stops (bound.f90:310-322)
     if (c.ns_conv != ICLS_NS_CNTR2) return ICLS_E_CONFIG;
+    if (!(c.mass_threshold >= 0.)) return ICLS_E_CONFIG;
     bcy = c.bc_y;
     imax = itot; jmax = jtot; kmax = ktot;
     i1 = imax + 1; j1 = jmax + 1; k1 = kmax + 1;
@@ -1018,7 +1019,8 @@ struct ora_ctx {
     maxchk_glb = 0.;
     if (istep % c.inflate_step == 0) {
       double massloss = (volume[l] - init_volume[l]) / init_volume[l];
-      if (std::fabs(massloss) > 1e-5) { inflation(l); ++last_inflated; }
+      const double eps = c.mass_threshold > 0. ? c.mass_threshold : 1e-5;
+      if (std::fabs(massloss) > eps) { inflation(l); ++last_inflated; }
     }
   }
 

@@ -52,3 +52,32 @@ def test_gpu_correction_gain_matches_oracle():
     from icls_gpu import Solver
     a, b = _factor(32, 10, Solver), _factor(32, 10)
     assert abs(a - b) <= 1e-8 * abs(b)
+
+
+def _first_correction_runs(make, threshold, deficit=3e-6):
+    cfg = make_config(itot=32, jtot=32, ktot=32, lmax=1, timestep=1e-5, inflate_step=2,
+                      reinit_step=100000, mass_threshold=threshold)
+    o = make(cfg)
+    o.setup(init_drops(cfg, [(0.5, 0.5, 0.5)], [0.25]), *initial_velocity(cfg, 0.0))
+    o.upload("lvset", init_drops(cfg, [(0.5, 0.5, 0.5)], [0.25 * (1 - deficit)])[..., 0], 1)
+    o.step(1, 0)
+    o.step(2, 0)
+    return o.scalars()["last_inflated"], o.volumes()
+
+
+@pytest.mark.parametrize("make", [Oracle, pytest.param("gpu", marks=pytest.mark.gpu)])
+def test_mass_threshold(make):
+    """mass_threshold = 0 keeps the reference's fixed 1e-5: a drift of about
+    9e-6 is left alone; a threshold of 1e-6 corrects it."""
+    if make == "gpu":
+        from icls_gpu import Solver as make
+    n0, (v, v0) = _first_correction_runs(make, 0.0)
+    assert n0 == 0 and 1e-6 < abs(v[0] / v0[0] - 1) < 1e-5
+    n1, _ = _first_correction_runs(make, 1e-6)
+    assert n1 == 1
+
+
+def test_negative_mass_threshold_rejected():
+    from icls_gpu import IclsError
+    with pytest.raises(IclsError):
+        Oracle(make_config(itot=16, jtot=16, ktot=16, mass_threshold=-1.0))
