@@ -63,6 +63,25 @@ def test_config_default_matches_python_defaults(lib):
             assert a == b, name
 
 
+def test_config_layout_matches_header(tmp_path):
+    """The ctypes mirror of icls_config has the header's size and offsets
+    (a C program built against include/icls_gpu.h prints them)."""
+    import shutil
+    import subprocess
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    names = [n for n, _ in IclsConfig._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "%s"\nint main(void) {\n'
+                   '  printf("%%zu\\n", sizeof(icls_config));\n%s  return 0;\n}\n'
+                   % (HEADER, "".join('  printf("%%zu\\n", offsetof(icls_config, %s));\n' % n for n in names)))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-o", str(exe), str(src)], check=True)
+    out = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert out[0] == C.sizeof(IclsConfig)
+    assert out[1:] == [getattr(IclsConfig, n).offset for n in names]
+
+
 @pytest.mark.parametrize("change,code", [
     (dict(itot=24), "E_CONFIG"),            # radix-2 FFT in x
     (dict(jtot=40), "E_CONFIG"),               # no FFT of that length
@@ -80,6 +99,7 @@ def test_config_default_matches_python_defaults(lib):
     (dict(curvature_model=2), "E_CONFIG"),      # neither stencil nor network
     (dict(curvature_model=1, lx=2.0), "E_UNSUPPORTED"),  # the network needs isotropic spacing
     (dict(curvature_model=1, mlp_fallback_tol=0.0), "E_CONFIG"),
+    (dict(mass_threshold=-1e-6), "E_CONFIG"),
 ])
 def test_create_rejects_bad_configs_on_host(lib, change, code):
     cfg = make_config(itot=32, jtot=32, ktot=32, lmax=1)
