@@ -84,6 +84,8 @@ namespace {
   } while (0)
 
 
+constexpr long long kMaxFieldElems = 1LL << 30;
+
 int validate(const icls_config* c) {
   if (!c) return ICLS_E_ARG;
   if (c->bc_y < ICLS_BCY_PERIODIC || c->bc_y > ICLS_BCY_OUTOUT) return ICLS_E_CONFIG;
@@ -95,6 +97,10 @@ int validate(const icls_config* c) {
   if (c->itot > 4096 || c->jtot > 4096) return ICLS_E_CONFIG;
   if (c->itot < 8 || c->jtot < 8) return ICLS_E_CONFIG;  // periodic images of 3 halo layers
   if (c->ktot < 6 || c->lmax < 1) return ICLS_E_CONFIG;
+  // grid-stride loops index cells with 32-bit integers: keep the largest
+  // array (a level set with its 3 halo layers per side) below 2^30 elements
+  // so that no index plus one grid stride can pass INT_MAX
+  if ((long long)(c->itot + 6) * (c->jtot + 6) * (c->ktot + 6) > kMaxFieldElems) return ICLS_E_CONFIG;
   if (!(c->lx > 0 && c->ly > 0 && c->lz > 0 && c->timestep > 0)) return ICLS_E_CONFIG;
   if (c->reinit_step < 1 || c->inflate_step < 1 || c->reinit_iter_max < 1) return ICLS_E_CONFIG;
   if (!(c->mass_threshold >= 0.)) return ICLS_E_CONFIG;

@@ -53,15 +53,18 @@ __global__ void __launch_bounds__(kThreads) k_div_partials(const double* __restr
                                                            double* __restrict__ scratch) {
   const int nCx = imax + 2, nCy = jmax + 2;
   const long long sz = (long long)nCx * nCy;
-  const int nI = imax * jmax * kmax;
+  // 64-bit counter and stride: with nI up to 2^31-1 the last q + stride
+  // passes INT_MAX and would wrap a 32-bit index to a negative cell
+  const long long nI = (long long)imax * jmax * kmax;
+  const long long stride = (long long)gridDim.x * kThreads;
   double s = 0., m = 0.;
   long long loc = -1;
-  for (int q = blockIdx.x * kThreads + threadIdx.x; q < nI; q += gridDim.x * kThreads) {
-    const int i = q % imax + 1;
-    const int r = q / imax;
-    const int j = r % jmax + 1;
-    const int k = r / jmax + 1;
-    const long long c = (long long)i + (long long)nCx * ((long long)j + (long long)nCy * (long long)k);
+  for (long long q = (long long)blockIdx.x * kThreads + threadIdx.x; q < nI; q += stride) {
+    const int i = (int)(q % imax) + 1;
+    const long long r = q / imax;
+    const int j = (int)(r % jmax) + 1;
+    const long long k = r / jmax + 1;
+    const long long c = (long long)i + (long long)nCx * ((long long)j + (long long)nCy * k);
     double div = ((w[c] - w[c - sz]) * dzi + (v[c] - v[c - nCx]) * dyi) + (u[c] - u[c - 1]) * dxi;
     s += div;
     div = fabs(div);
@@ -141,7 +144,8 @@ extern "C" int icls_chkdiv_noalloc(const double* u, const double* v, const doubl
                                    double dxi, double dyi, double dzi, double* result, void* stream) {
   if (!u || !v || !w || !result) return ICLS_E_ARG;
   if (imax < 1 || jmax < 1 || kmax < 1) return ICLS_E_ARG;
-  // interior cells are indexed with 32-bit integers in the kernel
+  // locations travel as doubles and the result's k is computed from them:
+  // the limit keeps every cell index exact and far inside 64-bit arithmetic
   if ((long long)imax * jmax * kmax > (long long)ICLS_NOALLOC_MAX_CELLS) return ICLS_E_SIZE;
   double* scratch = nullptr;
   int rc = scratch_address(&scratch);

@@ -95,7 +95,8 @@ typedef struct icls_config {
   int ns_conv;                   /* ICLS_NS_* (param.f90:135)                */
   double mass_threshold;         /* |V-V0|/V0 above which ls_mass_correction
                                     inflates a drop; 0 = the reference's
-                                    fixed 1e-5 (levelset.f90:382)           */
+                                    fixed 1e-5 (levelset.f90:382); any
+                                    value > 0 overrides it                  */
 } icls_config;
 
 /* Fill *cfg with the reference defaults of src/param.f90 for a 3-D run. */
@@ -294,7 +295,8 @@ int icls_tc_gemm_bf16(const void* a, const void* b, float* d, int n, int k, void
  * GPU that loads the library, until exit); the first call on a device looks
  * up its address, so make it before any stream capture.  Calls share that
  * array: calls that overlap on the GPU race.  Grids above
- * ICLS_NOALLOC_MAX_CELLS interior cells return ICLS_E_SIZE.  Nothing is
+ * ICLS_NOALLOC_MAX_CELLS interior cells return ICLS_E_SIZE; up to it the
+ * kernel indexes cells with 64-bit integers.  Nothing is
  * allocated; the call is asynchronous on `stream` (a cudaStream_t, 0 for
  * the default stream).                                                   */
 #define ICLS_NOALLOC_MAX_CELLS 2147483647LL

@@ -245,6 +245,8 @@ struct ora_ctx {
     itot = c.itot; jtot = c.jtot; ktot = c.ktot; L = c.lmax;
     if (itot < 4 || jtot < 4 || ktot < 6 || L < 1) return ICLS_E_CONFIG;
     if (itot % 2 || jtot % 2) return ICLS_E_CONFIG;
+    // the CUDA path's limit: a level set with its halos below 2^30 elements
+    if ((long long)(itot + 6) * (jtot + 6) * (ktot + 6) > (1LL << 30)) return ICLS_E_CONFIG;
     if (c.bc_y < ICLS_BCY_PERIODIC || c.bc_y > ICLS_BCY_OUTOUT) return ICLS_E_CONFIG;
     if (c.ns_conv == ICLS_NS_WENO5) return ICLS_E_UNSUPPORTED;  // boundfu stops (bound.f90:310-322)
     if (c.ns_conv != ICLS_NS_CNTR2) return ICLS_E_CONFIG;

@@ -145,3 +145,22 @@ def test_noalloc_argument_checks_run_before_cuda(lib):
     assert STATUS_NAMES.get(fn(None, dummy, dummy, 8, 8, 8, 1., 1., 1., dummy, None)) == "E_ARG"
     assert STATUS_NAMES.get(fn(dummy, dummy, dummy, 0, 8, 8, 1., 1., 1., dummy, None)) == "E_ARG"
     assert STATUS_NAMES.get(fn(dummy, dummy, dummy, 2048, 2048, 2048, 1., 1., 1., dummy, None)) == "E_SIZE"
+    # the limit itself: 2^31 cells (one above ICLS_NOALLOC_MAX_CELLS) is refused on the host
+    assert 2048 * 1024 * 1024 == 2**31
+    assert STATUS_NAMES.get(fn(dummy, dummy, dummy, 2048, 1024, 1024, 1., 1., 1., dummy, None)) == "E_SIZE"
+
+
+def test_config_beyond_32bit_indexing_is_rejected(lib):
+    """A grid whose level set with halos exceeds 2^30 elements is refused by
+    icls_create before any allocation (the kernels' 32-bit grid-stride
+    loops stay below INT_MAX); one just inside the limit passes validation."""
+    lib.icls_create.argtypes = [C.POINTER(IclsConfig), C.POINTER(C.c_void_p)]
+    lib.icls_create.restype = C.c_int
+    h = C.c_void_p()
+    cfg = make_config(itot=1024, jtot=1024, ktot=1024, lmax=1)  # 1030^3 > 2^30
+    assert STATUS_NAMES.get(lib.icls_create(C.byref(cfg), C.byref(h))) == "E_CONFIG"
+    cfg = make_config(itot=1024, jtot=1024, ktot=8, lmax=1)
+    rc = lib.icls_create(C.byref(cfg), C.byref(h))
+    if rc == 0:
+        lib.icls_destroy(h)
+    assert STATUS_NAMES.get(rc) != "E_CONFIG"
