@@ -7,7 +7,7 @@ drop, materials, AB2 predictor, Poisson RHS with GFM jumps, FFT/Thomas
 pressure solve, projection, pressure update.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-  python bench.py --drift-steps 1000 [--inflate-step S] [--mass-threshold T] [--dt DT]
+  python bench.py --drift-steps 1000 [--inflate-step S] [--mass-threshold T] [--dt DT] [--gain-one]
                                                   (volume record, no timing)
 
 Default workload: the 256^3 box with 48 seeded drops.  The headline value is
@@ -484,6 +484,13 @@ def ours_arm(args):
     if not args.no_e2e:
         e2e = run_e2e(args, wl, ls, u, v, w, torch, world, net)
 
+    # ---- volume drift over 1000 steps: both contexts side by side from the
+    # initial state, the gain-one mass correction at the workload's cadence
+    # with a 1e-7 trigger (icls_config.mass_gain_one / mass_threshold)
+    drift = None
+    if world == 1 and net is not None and not args.no_drift:
+        drift = drift_record(wl, ls, u, v, w, net, 1000, torch, mass_threshold=1e-7, gain_one=True)
+
     # ---- CPU baseline: the oracle on a bounded sample ---------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -508,7 +515,7 @@ def ours_arm(args):
                 "gpu_launches": form["gpu_launches"], "clocks": form["clocks"],
                 "speedup_vs_fp64": form["value"] / v64, "errors": form["errors"],
                 "plain_fp64": plain, "fp32_stencil": form["fp32_stencil"], "network": net_info,
-                "kernels": form["kernels"]}
+                "kernels": form["kernels"], "volume_drift_1000": drift}
         else:
             line = {
                 "metric": METRIC, "value": v64, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -754,33 +761,26 @@ def combined_full(args):
     return 0
 
 
-def volume_drift(args):
-    """The volume record over a long run: the plain FP64 context and the FP32
-    + learned-curvature form advance the same initial state side by side for
-    --drift-steps steps.  Every drop's volume is read after each sampled step
-    (k_volumes integrates it every step); the line gives, for each context,
-    the largest |V - V0| / V0 seen over the run and at its end, the form's
-    largest per-drop volume difference from FP64, and at the end the phi band
-    and velocity differences.  It is a report, not a throughput line."""
-    import torch
-    rank, world, local = dist_env()
-    if world != 1:
-        raise SystemExit("--drift-steps runs on one GPU")
-    torch.cuda.set_device(local)
+def drift_record(wl, ls, u, v, w, net, n, torch, inflate_step=0, mass_threshold=0.0, dt=0.0, gain_one=False,
+                 record_every=0):
+    """The plain FP64 context and the FP32 + learned-curvature form advance
+    the same initial state side by side for n steps; every drop's volume is
+    read after every step.  Returns the largest |V - V0| / V0 of each
+    context over the run and at its end, the form's largest per-drop volume
+    difference from FP64, and at the end the phi band and velocity
+    differences."""
     from icls_gpu import CURV_MLP, FP32, Solver
     from icls_gpu.binding import curvature_stats
     from icls_gpu.config import IclsConfig
-    wl = make_workload(args.workload)
-    cfg = wl.cfg
-    if args.dt:
-        cfg.timestep = args.dt
-    if args.inflate_step:
-        cfg.inflate_step = args.inflate_step
-    if args.mass_threshold:
-        cfg.mass_threshold = args.mass_threshold
-    ls, u, v, w = initial_state(wl)
+    cfg = IclsConfig.from_buffer_copy(wl.cfg)
+    if dt:
+        cfg.timestep = dt
+    if inflate_step:
+        cfg.inflate_step = inflate_step
+    if mass_threshold:
+        cfg.mass_threshold = mass_threshold
+    cfg.mass_gain_one = 1 if gain_one else 0
     h = cfg.lz / cfg.ktot
-    net, net_info = train_network(torch)
     ref = Solver(cfg)
     ref.setup(ls, u, v, w)
     cf = IclsConfig.from_buffer_copy(cfg)
@@ -789,11 +789,12 @@ def volume_drift(args):
     s = Solver(cf)
     net.attach(s)
     s.setup(ls, u, v, w)
-    n = args.drift_steps
-    every = max(n // 50, 1)
+    every = record_every or max(n // 50, 1)
     worst = {"form": 0.0, "fp64": 0.0}
+    worst_step = {"form": 0, "fp64": 0}
     vs_fp64 = 0.0
     record = []
+    last = (0.0, 0.0)
     stopped = None
     t0 = time.perf_counter()
     for istep in range(1, n + 1):
@@ -803,16 +804,17 @@ def volume_drift(args):
         except Exception as e:  # a divergence or time-step check of either context
             stopped = {"step": istep, "error": str(e)}
             break
-        if istep % every == 0 or istep == n or istep % cfg.inflate_step in (0, 1):
-            va, va0 = s.volumes()
-            vb, vb0 = ref.volumes()
-            da = float(np.max(np.abs(va - va0) / va0))
-            db = float(np.max(np.abs(vb - vb0) / vb0))
-            worst["form"] = max(worst["form"], da)
-            worst["fp64"] = max(worst["fp64"], db)
-            vs_fp64 = max(vs_fp64, float(np.max(np.abs(va - vb) / vb)))
-            if istep % every == 0 or istep == n:
-                record.append([istep, da, db])
+        va, va0 = s.volumes()
+        vb, vb0 = ref.volumes()
+        da = float(np.max(np.abs(va - va0) / va0))
+        db = float(np.max(np.abs(vb - vb0) / vb0))
+        for key, d in (("form", da), ("fp64", db)):
+            if d > worst[key]:
+                worst[key], worst_step[key] = d, istep
+        vs_fp64 = max(vs_fp64, float(np.max(np.abs(va - vb) / vb)))
+        last = (da, db)
+        if istep % every == 0 or istep == n:
+            record.append([istep, da, db])
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
 
@@ -825,19 +827,38 @@ def volume_drift(args):
         band = max(band, rel(pa[m], pb[m]))
     ev, fb = curvature_stats(s, reset=True)
     sc = ref.scalars()
-    line = {
-        "report": "volume_drift", "workload": wl.name, "steps": n, "dt": sc["dt"], "time": sc["time"],
-        "inflate_step": cfg.inflate_step, "reinit_step": cfg.reinit_step, "drops": cfg.lmax,
-        "mass_threshold": cfg.mass_threshold or 1e-5,
-        "drift_max_rel_over_run": worst, "drift_max_rel_at_end": {"form": record[-1][1] if record else None,
-                                                           "fp64": record[-1][2] if record else None},
+    out = {
+        "steps": n, "dt": sc["dt"], "time": sc["time"], "inflate_step": cfg.inflate_step,
+        "reinit_step": cfg.reinit_step, "drops": cfg.lmax, "mass_threshold": cfg.mass_threshold or 1e-5,
+        "gain_one": bool(gain_one), "sampled": "every step",
+        "drift_max_rel_over_run": worst, "at_step": worst_step,
+        "drift_max_rel_at_end": {"form": last[0], "fp64": last[1]},
         "volume_max_rel_form_vs_fp64": vs_fp64,
         "at_end": {"phi_band_rel_l2_first4": band, "u_rel_l2": rel(s.download("u"), ref.download("u")),
                    "v_rel_l2": rel(s.download("v"), ref.download("v")),
                    "w_rel_l2": rel(s.download("w"), ref.download("w"))},
-        "network_fallback_fraction": fb / max(ev, 1), "network": net_info,
+        "network_fallback_fraction": fb / max(ev, 1),
         "record_step_drift_form_fp64": record, "stopped": stopped, "wall_s": round(wall, 1)}
-    del s, ref
+    s.close()
+    ref.close()
+    return out
+
+
+def volume_drift(args):
+    """The volume record over a long run (drift_record), as its own JSON
+    line: a report, not a throughput line."""
+    import torch
+    rank, world, local = dist_env()
+    if world != 1:
+        raise SystemExit("--drift-steps runs on one GPU")
+    torch.cuda.set_device(local)
+    wl = make_workload(args.workload)
+    ls, u, v, w = initial_state(wl)
+    net, net_info = train_network(torch)
+    line = {"report": "volume_drift", "workload": wl.name}
+    line.update(drift_record(wl, ls, u, v, w, net, args.drift_steps, torch, args.inflate_step,
+                             args.mass_threshold, args.dt, args.gain_one))
+    line["network"] = net_info
     net.close()
     print(json.dumps(line))
     return 0
@@ -852,6 +873,7 @@ def main():
     ap.add_argument("--workload", default="multi_drop_256_48")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-drift", action="store_true", help="skip the 1000-step volume record")
     ap.add_argument("--no-forms", action="store_true",
                     help="plain FP64 only (no network training, no FP32 forms)")
     ap.add_argument("--dt", type=float, default=0.0, help="with --drift-steps: the time step (default: the workload's)")
@@ -859,6 +881,8 @@ def main():
                     help="with --drift-steps: the mass-correction cadence (default: the workload's)")
     ap.add_argument("--mass-threshold", type=float, default=0.0,
                     help="with --drift-steps: the volume error that triggers a correction (default 1e-5)")
+    ap.add_argument("--gain-one", action="store_true",
+                    help="with --drift-steps: the gain-one mass correction (icls_config.mass_gain_one)")
     ap.add_argument("--drift-steps", type=int, default=0,
                     help="instead of timing: run FP64 and the form side by side this many steps, "
                          "report the drop volumes' drift")

@@ -310,5 +310,7 @@ void ab2_launch(Ctx& c, const MomArgs& a, int o) {
 
 // the FP32 form's instance (k_ab2_f32.cu)
 void ab2_launch_f32(Ctx& c, const MomArgs& a, int o);
+// the TMA-fed FP64 predictor (k_ab2_tma.cu); false when it does not apply
+bool ab2_tma_launch(Ctx& c, const MomArgs& a, int o);
 
 }  // namespace icls

@@ -104,6 +104,7 @@ int validate(const icls_config* c) {
   if (!(c->lx > 0 && c->ly > 0 && c->lz > 0 && c->timestep > 0)) return ICLS_E_CONFIG;
   if (c->reinit_step < 1 || c->inflate_step < 1 || c->reinit_iter_max < 1) return ICLS_E_CONFIG;
   if (!(c->mass_threshold >= 0.)) return ICLS_E_CONFIG;
+  if (c->mass_gain_one != 0 && c->mass_gain_one != 1) return ICLS_E_CONFIG;
   if (c->ls_adv_space != ICLS_HOUC5 && c->ls_adv_space != ICLS_WENO5) return ICLS_E_CONFIG;
   if (c->i_space != ICLS_HOUC5 && c->i_space != ICLS_WENO5) return ICLS_E_CONFIG;
   if (c->precision != ICLS_FP64 && c->precision != ICLS_FP32) return ICLS_E_CONFIG;
@@ -220,7 +221,9 @@ int allocate(Ctx& c) {
   AL(c.dvol, (size_t)P.L); AL(c.dvol0, (size_t)P.L); AL(c.dmaxchk, (size_t)P.L);
   AL(c.drs, (size_t)P.L);
   c.red_cap = ((P.imax + TBX - 1) / TBX) * ((P.jmax + TBY - 1) / TBY);
-  AL(c.hpart, (size_t)std::max(P.L, 2) * c.red_cap);
+  // per-tile exact sums of H (4 words each) for every drop; the inflation
+  // uses red_cap area sums and red_cap exact sums
+  AL(c.hpart, (size_t)std::max(4 * P.L, 5) * c.red_cap);
   CK(cudaMallocHost((void**)&c.h_vol, sizeof(double) * P.L));
   CK(cudaMallocHost((void**)&c.h_sc, sizeof(DevScalars)));
   CK(cudaEventCreateWithFlags(&c.ev_vol, cudaEventDisableTiming));
@@ -236,6 +239,10 @@ int allocate(Ctx& c) {
   // bookkeeping: both give bit-identical fields)
   const char* fs = std::getenv("ICLS_FULL_SWEEP");
   c.use_boxes = (P.L <= kMaxDropsParam) && !(fs && fs[0] == '1');
+  // ICLS_AB2=ring runs the FP64 predictor on the cp.async-ring kernel in
+  // place of the TMA-fed one (the same arithmetic: bit-identical fields)
+  const char* ab = std::getenv("ICLS_AB2");
+  c.ab2_ring = ab && std::strcmp(ab, "ring") == 0;
   // working buffers of a group of drops: as many drops as half the free
   // HBM holds (ICLS_GROUP=n caps the group, e.g. to test the grouped path)
   {
@@ -610,7 +617,37 @@ void inflation(Ctx& c, int l) {
   std::vector<LsBatch> bvel = single(c, l, kStageRows, c_region(c.P, b, 0));
   launch_inflate_vel(c, bvel[0]);
   std::vector<LsBatch> bs = single(c, l, kStageRows, b);
+  // gain one: keep phi0 on the written cells of the RK3 region (member s3
+  // is free after the advection) and its far-field values
+  DropWin& w = c.win[l];
+  const double bg0 = w.bg, bgg0 = w.bg_ghost;
+  if (c.cfg.mass_gain_one) {
+    std::vector<LsBatch> bcp = single(c, l, kStageRows, b);
+    bcp[0].t[0].phi0 = c.lv[l];
+    bcp[0].t[0].out = member(c, l).s3;
+    launch_region_copy(c, bcp[0]);
+  }
   rk3_batches(c, bs, c.cfg.i_space, false, c.ulc, c.vlc, c.wlc);
+  if (c.cfg.mass_gain_one) {
+    std::vector<LsBatch> bv = single(c, l, 0, r1);
+    bv[0].t[0].phi0 = c.lv[l];
+    launch_gain(c, bv[0], outside_count(c, b));
+    std::vector<LsBatch> bb = single(c, l, kStageRows, b);
+    bb[0].t[0].phi0 = member(c, l).s3;
+    bb[0].t[0].out = c.lv[l];
+    launch_region_blend(c, bb[0]);
+    // the far field (uniform, velocity zero there) keeps its value unless the
+    // RK3 combinations rounded it; then it is blended like every cell
+    if (w.bg != bg0 || w.bg_ghost != bgg0) {
+      double gain = 0.;
+      if (cudaMemcpyAsync(&gain, &c.dsc->inflate_gain, sizeof(double), cudaMemcpyDeviceToHost, c.s) ==
+              cudaSuccess &&
+          cudaStreamSynchronize(c.s) == cudaSuccess) {
+        w.bg = bg0 + gain * (w.bg - bg0);
+        w.bg_ghost = bgg0 + gain * (w.bg_ghost - bgg0);
+      }
+    }
+  }
   c.inflated[l] = 1;
   c.vol_dirty[l] = 1;
   ++c.last_inflated;
@@ -920,6 +957,7 @@ int gfm4p(Ctx& c) {
 int read_scalars(Ctx& c) {
   CK(cudaMemcpyAsync(c.h_sc, c.dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c.s));
   CK(cudaStreamSynchronize(c.s));
+  if (c.h_sc->wait_err) return ICLS_E_TIMEOUT;
   return ICLS_OK;
 }
 
@@ -976,8 +1014,9 @@ int icls_status_string(int code, char* buf, int n) {
                                 "device allocation failed", "context not initialised",
                                 "option not built into this library",
                                 "grid larger than the no-allocation divergence check handles",
-                                "checkpoint file could not be written or read"};
-  const char* s = (code >= 0 && code <= 10) ? names[code] : "unknown status";
+                                "checkpoint file could not be written or read",
+                                "a kernel's bounded pipeline wait gave up"};
+  const char* s = (code >= 0 && code <= 11) ? names[code] : "unknown status";
   if (buf && n > 0) {
     std::strncpy(buf, s, (size_t)n - 1);
     buf[n - 1] = 0;

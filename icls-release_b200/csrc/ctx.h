@@ -76,6 +76,14 @@ struct DropWin {
 };
 
 struct Ctx {
+  // tensor maps of the TMA predictor for up to four sets of its 18 input
+  // pointers (the AB2 history and the p_x/p_xold pairs alternate between
+  // buffers), keyed by the pointers themselves
+  alignas(64) unsigned char ab2_maps[4][18 * 128];
+  const void* ab2_keys[4][18] = {};
+  int ab2_nmaps = 0, ab2_next = 0;
+  bool ab2_tma_failed = false;  // a map could not be encoded: use the ring
+  bool ab2_ring = false;  // FP64 predictor on the cp.async ring (ICLS_AB2=ring)
   icls_config cfg;
   Params P;
   cudaStream_t s = nullptr;
@@ -128,7 +136,7 @@ struct Ctx {
   double* dmaxchk = nullptr;            // per drop maxchk of the last inflation
   ReinitState* drs = nullptr;           // per drop
   double* stage = nullptr;              // precision form: FP64 staging of one field (upload/download)
-  double* hpart = nullptr;              // per-tile partial sums, red_cap per drop
+  double* hpart = nullptr;              // per-tile exact sums of H (XSum), red_cap per drop
   int red_cap = 0;                      // column tiles of a whole x-y plane
   // pinned host mirrors
   double* h_vol = nullptr;
@@ -188,6 +196,9 @@ void launch_fill(Ctx& c, double* a, long long n, double v, bool tfield);
 void launch_materials_final(Ctx& c, const double* outside, const int* ntiles);
 void launch_inflate_sums(Ctx& c, const LsBatch& b, double outside);
 void launch_inflate_vel(Ctx& c, const LsBatch& b);
+void launch_region_copy(Ctx& c, const LsBatch& b);
+void launch_gain(Ctx& c, const LsBatch& b, double outside);
+void launch_region_blend(Ctx& c, const LsBatch& b);
 void launch_copy(Ctx& c, double* dst, const double* src, long long n);
 void launch_boundmls(Ctx& c, double* phi);
 void launch_materialize(Ctx& c, const Region& r, double bg, double bgg, double* phi);

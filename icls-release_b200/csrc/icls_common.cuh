@@ -182,6 +182,129 @@ __device__ __forceinline__ T block_max(T v) {
   __syncthreads();
   return r;
 }
+// ------------------------------------------------------- exact sums of H
+// The drop volume is volume = 1 - sum(H)/N (misc.f90:127-139,
+// levelset.f90:505-506): a sum of N ~ 1e7 values near 1 whose complement
+// ~1e-4 is kept, so a floating-point sum's rounding, which depends on its
+// order, is magnified 1e4-fold in the volume and again, by the correction's
+// gain, in the mass-correction step that follows it.  (The reference's own
+// result depends on its MPI rank count through that order.)  These sums are
+// therefore accumulated exactly: each element is truncated toward zero to a
+// multiple of 2^-144 and added as an integer, held in four signed 64-bit
+// limbs of 48 bits (value = sum_q L[q] 2^(48q - 144)); the integer does
+// not depend on the order of the additions, and it is rounded once to the
+// nearest double (ties to even).  Elements must satisfy |x| < 32.
+struct XSum {
+  long long L[4];
+};
+constexpr long long kXMask = (1LL << 48) - 1;
+__device__ __forceinline__ void xs_zero(XSum& a) { a.L[0] = a.L[1] = a.L[2] = a.L[3] = 0; }
+// carry limbs 0..2 into [0, 2^48); limb 3 keeps the sign
+__device__ __forceinline__ void xs_norm(XSum& a) {
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const long long c = a.L[q] >> 48;  // arithmetic shift: floor(L / 2^48)
+    a.L[q] -= c * (1LL << 48);
+    a.L[q + 1] += c;
+  }
+}
+__device__ __forceinline__ void xs_add(XSum& a, double x) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  int e = (int)((b >> 52) & 0x7FF);
+  unsigned long long m = b & ((1ULL << 52) - 1);
+  if (e == 0) e = 1;
+  else m |= 1ULL << 52;
+  if (m == 0) return;
+  // |x| = m 2^(e-1075) = m 2^(e-931) units of 2^-144
+  int s = e - 931;
+  if (s < 0) {
+    if (s <= -53) return;
+    m >>= -s;
+    s = 0;
+  }
+  // bits s .. s+52 of the integer: limb q = s/48 and the two above it
+  const int q = s / 48, o = s - 48 * q;
+  const long long sg = (b >> 63) ? -1LL : 1LL;
+  const long long lo = sg * (long long)((m << o) & (unsigned long long)kXMask);
+  const long long mid = sg * (long long)((m >> (48 - o)) & (unsigned long long)kXMask);
+  const long long hi = (96 - o < 64) ? sg * (long long)(m >> (96 - o)) : 0LL;
+  if (q == 0) {
+    a.L[0] += lo; a.L[1] += mid; a.L[2] += hi;
+  } else if (q == 1) {
+    a.L[1] += lo; a.L[2] += mid; a.L[3] += hi;
+  } else {  // 16 <= |x| < 32: s = 96, nothing above limb 3
+    a.L[2] += lo; a.L[3] += mid;
+  }
+  xs_norm(a);
+}
+// n elements equal to exactly 1 (the far field of H)
+__device__ __forceinline__ void xs_add_count(XSum& a, long long n) { a.L[3] += n; }
+__device__ __forceinline__ void xs_merge(XSum& a, const XSum& b) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) a.L[q] += b.L[q];
+  xs_norm(a);
+}
+// the sum rounded to the nearest double, ties to even
+__device__ __forceinline__ double xs_value(XSum a) {
+  xs_norm(a);
+  bool neg = false;
+  if (a.L[3] < 0) {
+    neg = true;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) a.L[q] = -a.L[q];
+    xs_norm(a);
+  }
+  unsigned long long w[3];
+  w[0] = (unsigned long long)a.L[0] | ((unsigned long long)a.L[1] << 48);
+  w[1] = ((unsigned long long)a.L[1] >> 16) | ((unsigned long long)a.L[2] << 32);
+  w[2] = ((unsigned long long)a.L[2] >> 32) | ((unsigned long long)a.L[3] << 16);
+  int top = -1;
+  for (int q = 2; q >= 0 && top < 0; --q)
+    if (w[q]) top = 64 * q + 63 - __clzll((long long)w[q]);
+  if (top < 0) return 0.;
+  double r;
+  if (top <= 52) {
+    r = ldexp((double)w[0], -144);
+  } else {
+    const int sh = top - 52;
+    auto bits = [&](int pos) {  // 64 bits of the integer from bit pos up
+      const int wd = pos >> 6, of = pos & 63;
+      unsigned long long v = wd < 3 ? w[wd] >> of : 0ULL;
+      if (of && wd + 1 < 3) v |= w[wd + 1] << (64 - of);
+      return v;
+    };
+    unsigned long long mant = bits(sh) & ((1ULL << 53) - 1);
+    const bool half = (bits(sh - 1) & 1ULL) != 0;
+    bool sticky = false;
+    for (int pos = 0; pos < sh - 1 && !sticky; pos += 64) {
+      const int n = min(64, sh - 1 - pos);
+      const unsigned long long v = bits(pos);
+      sticky = (n == 64 ? v : (v & ((1ULL << n) - 1))) != 0ULL;
+    }
+    int ex = sh;
+    if (half && (sticky || (mant & 1ULL))) {
+      ++mant;
+      if (mant == (1ULL << 53)) {
+        mant >>= 1;
+        ++ex;
+      }
+    }
+    r = ldexp((double)mant, ex - 144);
+  }
+  return neg ? -r : r;
+}
+// block-wide exact sum (valid in thread 0): limbs in [0, 2^48) after the
+// threads' own normalisation, so a block of up to 2^14 threads cannot
+// overflow a limb
+template <int NT>
+__device__ __forceinline__ XSum block_xsum(XSum a) {
+  xs_norm(a);
+  XSum r;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) r.L[q] = block_sum<long long, NT>(a.L[q]);
+  return r;
+}
+
 // atomic max of a non-negative double through its ordered bit pattern
 __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
   atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
@@ -197,6 +320,7 @@ struct DevScalars {
   double area;            // levelset.f90:499-501
   double heav_sum;        // levelset.f90:505
   double inflate_temp;    // levelset.f90:514
+  double inflate_gain;    // blend factor of the last gain-one inflation
   double maxchk;          // levelset.f90:521
   double divtot, divmax;  // chkdiv.f90
   double umax, vmax, wmax;// chkdt.f90:42-44
@@ -205,7 +329,7 @@ struct DevScalars {
   int reinit_done;        // residual < dz**5 reached (levelset.f90:833)
   int reinit_iters;
   int nan_flag;           // main.f90:207
-  int pad;
+  int wait_err;           // a kernel's bounded mbarrier wait gave up
 };
 
 }  // namespace icls

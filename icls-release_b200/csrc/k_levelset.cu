@@ -685,13 +685,14 @@ __device__ __forceinline__ void min_into(float* a, float v) {
 }
 template <typename T>
 __global__ void __launch_bounds__(NT) k_heaviside(Params p, const __grid_constant__ LsBatch B,
-                                                  T* __restrict__ jiemian, double* __restrict__ part, int cap) {
+                                                  T* __restrict__ jiemian, XSum* __restrict__ part, int cap) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
   const T eps = TC(1.5 * p.dz);
   const T* __restrict__ phi = cT<T>(t.phi0);
-  double s = 0.;
+  XSum s;
+  xs_zero(s);
   if (c.ok && c.cxy) {
     const int i = c.i, j = c.j;
     const int ii = image_of<1>(i, p.imax), jj = image_of<1>(j, p.jmax);
@@ -716,11 +717,11 @@ __global__ void __launch_bounds__(NT) k_heaviside(Params p, const __grid_constan
             if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, jj, k), H);
           }
         }
-        if (k >= 1 && k <= p.kmax) s += (double)H;
+        if (k >= 1 && k <= p.kmax) xs_add(s, (double)H);
       }
     }
   }
-  const double bs = block_sum<double, NT>(s);
+  const XSum bs = block_xsum<NT>(s);
   if (flat_tid() == 0) part[(long long)t.l * cap + c.tile] = bs;
 }
 
@@ -730,15 +731,16 @@ struct PerDrop {
   double v[kMaxDropsParam];
   int n[kMaxDropsParam];
 };
-__global__ void k_volumes(Params p, const double* __restrict__ part, int cap, PerDrop pd, int uniform,
+__global__ void k_volumes(Params p, const XSum* __restrict__ part, int cap, PerDrop pd, int uniform,
                           double* __restrict__ vol, DevScalars* __restrict__ dsc) {
   const double N = (1. * p.imax * p.jmax) * p.kmax;
   for (int l = threadIdx.x; l < p.L; l += blockDim.x) {
     const int nb = uniform ? cap : pd.n[l];
-    double s = 0.;
-    for (int b = 0; b < nb; ++b) s += part[(long long)l * cap + b];
-    if (!uniform) s += pd.v[l];
-    vol[l] = 1. - s / N;
+    XSum s;
+    xs_zero(s);
+    for (int b = 0; b < nb; ++b) xs_merge(s, part[(long long)l * cap + b]);
+    if (!uniform) xs_add_count(s, (long long)pd.v[l]);
+    vol[l] = 1. - xs_value(s) / N;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -792,13 +794,15 @@ template <typename T>
 __global__ void __launch_bounds__(NT) k_inflate_sums(Params p, const __grid_constant__ LsBatch B,
                                                      const T* __restrict__ kappa, const T* __restrict__ nrm_m,
                                                      T* __restrict__ dheav, double* __restrict__ part_area,
-                                                     double* __restrict__ part_heav) {
+                                                     XSum* __restrict__ part_heav) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
   const T s1 = TC(1.5 * p.dz);
   const T* phi = cT<T>(t.phi0);
-  double sa = 0., sh = 0.;
+  double sa = 0.;
+  XSum sh;
+  xs_zero(sh);
   if (c.ok) {
     const int i = c.i, j = c.j;
     for (int k = c.ka; k <= c.kb; ++k) {
@@ -814,12 +818,12 @@ __global__ void __launch_bounds__(NT) k_inflate_sums(Params p, const __grid_cons
         const T del = dirac_trig(p, ph, s1);
         const T m = nrm_m[idxI(p, i, j, k)];
         sa += (double)(p.ispeed_curv ? (del * kappa[idxC(p, i, j, k)]) * m : del * m);
-        sh += (double)H;
+        xs_add(sh, (double)H);
       }
     }
   }
   const double ba = block_sum<double, NT>(sa);
-  const double bh = block_sum<double, NT>(sh);
+  const XSum bh = block_xsum<NT>(sh);
   if (flat_tid() == 0) {
     part_area[c.tile] = ba;
     part_heav[c.tile] = bh;
@@ -827,13 +831,19 @@ __global__ void __launch_bounds__(NT) k_inflate_sums(Params p, const __grid_cons
 }
 
 __global__ void k_inflate_final(Params p, const double* __restrict__ part_area,
-                                const double* __restrict__ part_heav, int nblk, int l, double istep_dt,
+                                const XSum* __restrict__ part_heav, int nblk, int l, double istep_dt,
                                 double outside, double* __restrict__ vol, const double* __restrict__ vol0,
                                 double* __restrict__ maxchk, DevScalars* __restrict__ dsc) {
   if (threadIdx.x != 0) return;
-  double sa = 0., sh = 0.;
-  for (int b = 0; b < nblk; ++b) { sa += part_area[b]; sh += part_heav[b]; }
-  sh += outside;
+  double sa = 0.;
+  XSum hs;
+  xs_zero(hs);
+  for (int b = 0; b < nblk; ++b) {
+    sa += part_area[b];
+    xs_merge(hs, part_heav[b]);
+  }
+  xs_add_count(hs, (long long)outside);
+  const double sh = xs_value(hs);
   double area = sa * p.dx * p.dy * p.dz;
   if (p.TwoD) area = area / p.lx;
   const double volume = 1. - sh / ((1. * p.imax * p.jmax) * p.kmax);
@@ -845,6 +855,77 @@ __global__ void k_inflate_final(Params p, const double* __restrict__ part_area,
   dsc->area = area;
   dsc->heav_sum = sh;
   maxchk[l] = temp / (1.5 * p.dz);
+}
+
+// ------------------------------------------------ gain-one mass correction
+// icls_config.mass_gain_one (no counterpart in the reference).  The
+// reference's inflation moves the interface by about K/inflate_step times
+// the volume error it measured (K ~ 0.66/s1 in grid units), so with the
+// option the inflated level set phi1 is blended with the one before it,
+// phi = phi0 + g (phi1 - phi0), g = (V0 - V)/(V1 - V) from the exact
+// volumes before (V) and after (V1) the inflation: the blend removes the
+// measured error to first order in the (small) displacement.
+
+// t.out = t.phi0 on the task's written cells (rows of the chunk, images)
+template <typename T>
+__global__ void __launch_bounds__(NT) k_region_copy(Params p, const __grid_constant__ LsBatch B) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  if (!c.ok) return;
+  const T* __restrict__ src = cT<T>(t.phi0);
+  T* __restrict__ dst = mT<T>(t.out);
+  for (int k = c.ka; k <= c.kb; ++k) putL(p, dst, c.i, c.j, k, src[idxL(p, c.i, c.j, k)]);
+}
+
+// per-tile exact sums of H(phi1) over the task's computed interior cells
+template <typename T>
+__global__ void __launch_bounds__(NT) k_region_heav(Params p, const __grid_constant__ LsBatch B,
+                                                    XSum* __restrict__ part) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  const T s1 = TC(1.5 * p.dz);
+  const T* __restrict__ phi = cT<T>(t.phi0);
+  XSum sh;
+  xs_zero(sh);
+  if (c.ok)
+    for (int k = max(c.ka, 1); k <= min(c.kb, p.kmax); ++k)
+      if (computed(c, t.r, k)) xs_add(sh, (double)heav_trig(p, phi[idxL(p, c.i, c.j, k)], s1));
+  const XSum bh = block_xsum<NT>(sh);
+  if (flat_tid() == 0) part[c.tile] = bh;
+}
+
+// g = (V0 - V)/(V1 - V), V1 from the tiles and the far-field count
+__global__ void k_gain_final(Params p, const XSum* __restrict__ part, int nblk, int l, double outside,
+                             const double* __restrict__ vol, const double* __restrict__ vol0,
+                             DevScalars* __restrict__ dsc) {
+  if (threadIdx.x != 0) return;
+  XSum hs;
+  xs_zero(hs);
+  for (int b = 0; b < nblk; ++b) xs_merge(hs, part[b]);
+  xs_add_count(hs, (long long)outside);
+  const double v1 = 1. - xs_value(hs) / ((1. * p.imax * p.jmax) * p.kmax);
+  const double d = v1 - vol[l];
+  dsc->inflate_gain = d != 0. ? (vol0[l] - vol[l]) / d : 0.;
+}
+
+// t.out (phi1, in place) = phi0 + g (phi1 - phi0) on the written cells
+template <typename T>
+__global__ void __launch_bounds__(NT) k_region_blend(Params p, const __grid_constant__ LsBatch B,
+                                                     const DevScalars* __restrict__ dsc) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  if (!c.ok) return;
+  const double g = dsc->inflate_gain;
+  const T* __restrict__ p0 = cT<T>(t.phi0);
+  T* __restrict__ p1 = mT<T>(t.out);
+  for (int k = c.ka; k <= c.kb; ++k) {
+    const long long n = idxL(p, c.i, c.j, k);
+    const double a0 = (double)p0[n];
+    putL(p, p1, c.i, c.j, k, TC(a0 + g * ((double)p1[n] - a0)));
+  }
 }
 
 // u_lc, v_lc, w_lc of levelset.f90:527-548, with u_l,v_l,w_l of 530-532
@@ -1114,13 +1195,16 @@ void launch_reinit_check(Ctx& c, const LsBatch& b, int it, int maxiter, double t
   k_reinit_check<<<1, 64, 0, c.s>>>(b, it, maxiter, thr, c.drs, c.dsc, c.P.L - 1);
 }
 
+// the per-tile exact sums of H: red_cap per drop (4 words each)
+XSum* hparts(Ctx& c) { return reinterpret_cast<XSum*>(c.hpart); }
+
 void launch_heaviside(Ctx& c, const LsBatch& b) {
   if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "heaviside", 1);
   BY_FORM(c,
-          (k_heaviside<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, reinterpret_cast<float*>(c.jiemian), c.hpart,
+          (k_heaviside<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, reinterpret_cast<float*>(c.jiemian), hparts(c),
                                                                 c.red_cap)),
-          (k_heaviside<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.jiemian, c.hpart, c.red_cap)));
+          (k_heaviside<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.jiemian, hparts(c), c.red_cap)));
 }
 
 // n elements of a; tfield: a holds the form's field type (else FP64)
@@ -1151,7 +1235,7 @@ void launch_materials_final(Ctx& c, const double* outside, const int* ntiles) {
     o.v[l] = (!uniform && l < c.P.L) ? outside[l] : 0.;
     o.n[l] = (!uniform && l < c.P.L) ? ntiles[l] : 0;
   }
-  k_volumes<<<1, 256, 0, c.s>>>(c.P, c.hpart, c.red_cap, o, uniform, c.dvol, c.dsc);
+  k_volumes<<<1, 256, 0, c.s>>>(c.P, hparts(c), c.red_cap, o, uniform, c.dvol, c.dsc);
   const int r0[3] = {0, 0, 0}, r1[3] = {c.P.i1, c.P.j1, c.P.k1};
   if (c.P.f32) {
     auto f = [](double* q) { return reinterpret_cast<float*>(q); };
@@ -1167,7 +1251,7 @@ void launch_materials_final(Ctx& c, const double* outside, const int* ntiles) {
 void launch_inflate_sums(Ctx& c, const LsBatch& b, double outside) {
   Scope sc_(c.prof, c.s, "inflate_sums", 2);
   double* pa = c.hpart;
-  double* ph = c.hpart + c.red_cap;
+  XSum* ph = reinterpret_cast<XSum*>(c.hpart + c.red_cap);
   if (c.P.f32) {
     auto f = [](double* q) { return reinterpret_cast<float*>(q); };
     k_inflate_sums<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, f(c.kappa), f(c.nrm_m), f(c.dheav), pa, ph);
@@ -1176,6 +1260,25 @@ void launch_inflate_sums(Ctx& c, const LsBatch& b, double outside) {
   }
   k_inflate_final<<<1, 32, 0, c.s>>>(c.P, pa, ph, b.start[b.n], b.t[0].l, (double)c.cfg.inflate_step * c.dt, outside,
                                      c.dvol, c.dvol0, c.dmaxchk, c.dsc);
+}
+
+// gain-one inflation: phi0 copy, the volume after, and the blend
+void launch_region_copy(Ctx& c, const LsBatch& b) {
+  Scope sc_(c.prof, c.s, "gain_one", 1);
+  BY_FORM(c, (k_region_copy<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b)),
+          (k_region_copy<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b)));
+}
+void launch_gain(Ctx& c, const LsBatch& b, double outside) {
+  Scope sc_(c.prof, c.s, "gain_one", 2);
+  XSum* ph = reinterpret_cast<XSum*>(c.hpart + c.red_cap);
+  BY_FORM(c, (k_region_heav<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, ph)),
+          (k_region_heav<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, ph)));
+  k_gain_final<<<1, 32, 0, c.s>>>(c.P, ph, b.start[b.n], b.t[0].l, outside, c.dvol, c.dvol0, c.dsc);
+}
+void launch_region_blend(Ctx& c, const LsBatch& b) {
+  Scope sc_(c.prof, c.s, "gain_one", 1);
+  BY_FORM(c, (k_region_blend<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.dsc)),
+          (k_region_blend<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.dsc)));
 }
 
 // b: one task (shape-C region of the drop, apron 0)

@@ -22,11 +22,11 @@ BCY_PERIODIC, BCY_WALLS, BCY_INOUT, BCY_OUTOUT = 0, 1, 2, 3
 NS_CNTR2, NS_WENO5 = 0, 1
 
 # status codes
-OK, E_CONFIG, E_CUDA, E_NAN, E_DIVERGENCE, E_ARG, E_NOMEM, E_STATE, E_UNSUPPORTED, E_SIZE, E_IO = range(11)
+OK, E_CONFIG, E_CUDA, E_NAN, E_DIVERGENCE, E_ARG, E_NOMEM, E_STATE, E_UNSUPPORTED, E_SIZE, E_IO, E_TIMEOUT = range(12)
 STATUS_NAMES = {
     0: "OK", 1: "E_CONFIG", 2: "E_CUDA", 3: "E_NAN", 4: "E_DIVERGENCE",
     5: "E_ARG", 6: "E_NOMEM", 7: "E_STATE", 8: "E_UNSUPPORTED", 9: "E_SIZE",
-    10: "E_IO",
+    10: "E_IO", 11: "E_TIMEOUT",
 }
 
 
@@ -48,6 +48,7 @@ class IclsConfig(C.Structure):
         ("mlp_fallback_tol", C.c_double),
         ("bc_y", C.c_int), ("ns_conv", C.c_int),
         ("mass_threshold", C.c_double),
+        ("mass_gain_one", C.c_int),
     ]
 
     def as_dict(self):
@@ -115,6 +116,7 @@ def make_config(**kw) -> IclsConfig:
     c.curvature_model = CURV_STENCIL
     c.mlp_fallback_tol = 0.02
     c.mass_threshold = 0.0                 # 0: the fixed 1e-5 of levelset.f90:382
+    c.mass_gain_one = 0                    # 0: the reference's inflation gain
     for k, v in kw.items():
         if k == "g_unit":
             c.g_unit[:] = list(v)

@@ -38,7 +38,9 @@ enum {
   ICLS_E_STATE = 7,       /* call made before icls_init_program            */
   ICLS_E_UNSUPPORTED = 8, /* scheme/option not built into this library    */
   ICLS_E_SIZE = 9,        /* grid larger than icls_chkdiv_noalloc handles */
-  ICLS_E_IO = 10          /* checkpoint file could not be written or read  */
+  ICLS_E_IO = 10,         /* checkpoint file could not be written or read  */
+  ICLS_E_TIMEOUT = 11     /* a kernel's bounded wait on its own pipeline
+                             gave up (the step's results are invalid)     */
 };
 
 /* ---- scheme selectors (param.f90 / mod_param_ls character parameters) */
@@ -97,6 +99,12 @@ typedef struct icls_config {
                                     inflates a drop; 0 = the reference's
                                     fixed 1e-5 (levelset.f90:382); any
                                     value > 0 overrides it                  */
+  int mass_gain_one;             /* 0: the reference's inflation
+                                    (levelset.f90:407-582); 1: the same
+                                    inflation blended with the level set
+                                    before it so that it removes exactly the
+                                    measured volume error (no counterpart in
+                                    the reference)                          */
 } icls_config;
 
 /* Fill *cfg with the reference defaults of src/param.f90 for a 3-D run. */

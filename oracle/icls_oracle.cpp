@@ -26,6 +26,15 @@
 //  * the real FFTs implement the VFFTPACK input/output contract
 //    (fft.f:1123-1142, 403-452: half-complex layout, sqrt(1/N) both ways)
 //    with a radix-2 complex FFT instead of FFTPACK's mixed-radix passes.
+//
+// One deliberate difference that the CUDA path shares: the sum of the
+// Heaviside function in the drop volume (misc.f90:127-133) and in the
+// inflation (levelset.f90:505-506) is exact (XSum below), not a running
+// double sum.  volume = 1 - sum(H)/N keeps a 1e-4 complement of a sum near
+// N, so a running sum's rounding, which depends on the order (the
+// reference's depends on its MPI rank count through MPI_ALLREDUCE), shows
+// up 1e4-fold in the volume and again, multiplied by the correction's gain,
+// in the mass correction; with an exact sum every order gives one value.
 
 #include "icls_oracle.h"
 
@@ -40,6 +49,77 @@
 #endif
 
 namespace {
+
+// Exact, order-independent sum of doubles: every element is truncated
+// toward zero to a multiple of 2^-144, the integers are added exactly, and
+// the total is rounded once to the nearest double (ties to even).  The
+// magnitudes of the positive and of the negative elements are kept apart
+// as base-2^32 digits (digit d weighs 2^(32d-144)), carried lazily.
+struct XSum {
+  static constexpr int ND = 8;  // 256 bits: |total| < 2^112
+  uint64_t pos[ND] = {0, 0, 0, 0, 0, 0, 0, 0}, neg[ND] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int pending = 0;
+  void add(double x) {
+    if (x == 0.) return;
+    uint64_t* a = x < 0. ? neg : pos;
+    int E = 0;
+    const double f = std::frexp(std::fabs(x), &E);  // |x| = f 2^E, f in [0.5, 1)
+    uint64_t m = (uint64_t)std::ldexp(f, 53);        // exact: |x| = m 2^(E-53)
+    int sh = E - 53 + 144;                            // |x| = m 2^sh units
+    if (sh < 0) {
+      if (sh <= -64) return;
+      m >>= -sh;
+      sh = 0;
+    }
+    unsigned __int128 t = (unsigned __int128)m << (sh % 32);
+    for (int d = sh / 32; t != 0; ++d, t >>= 32) a[d] += (uint64_t)(t & 0xffffffffu);
+    if (++pending == (1 << 20)) carry();
+  }
+  void carry() {
+    for (uint64_t* a : {pos, neg})
+      for (int d = 0; d + 1 < ND; ++d) {
+        a[d + 1] += a[d] >> 32;
+        a[d] &= 0xffffffffu;
+      }
+    pending = 0;
+  }
+  double value() {
+    carry();
+    int cmp = 0;
+    for (int d = ND - 1; d >= 0 && !cmp; --d)
+      if (pos[d] != neg[d]) cmp = pos[d] > neg[d] ? 1 : -1;
+    if (!cmp) return 0.;
+    const uint64_t* big = cmp > 0 ? pos : neg;
+    const uint64_t* sml = cmp > 0 ? neg : pos;
+    uint64_t dg[ND];
+    int64_t borrow = 0;
+    for (int d = 0; d < ND; ++d) {
+      int64_t v = (int64_t)big[d] - (int64_t)sml[d] - borrow;
+      borrow = v < 0;
+      if (v < 0) v += (int64_t)1 << 32;
+      dg[d] = (uint64_t)v;
+    }
+    auto bit = [&](int b) { return b < 0 ? 0 : (int)((dg[b / 32] >> (b % 32)) & 1u); };
+    int top = 32 * ND - 1;
+    while (!bit(top)) --top;
+    const int sh = top > 52 ? top - 52 : 0;
+    uint64_t mant = 0;
+    for (int b = top; b >= sh; --b) mant = (mant << 1) | (uint64_t)bit(b);
+    int ex = sh;
+    if (sh > 0 && bit(sh - 1)) {
+      bool sticky = false;
+      for (int b = 0; b < sh - 1 && !sticky; ++b) sticky = bit(b);
+      if (sticky || (mant & 1u)) {
+        if (++mant == (1ULL << 53)) {
+          mant >>= 1;
+          ++ex;
+        }
+      }
+    }
+    const double r = std::ldexp((double)mant, ex - 144);
+    return cmp > 0 ? r : -r;
+  }
+};
 
 // Fortran-bounds 3-D array, column-major (i fastest).
 struct F3 {
@@ -223,6 +303,7 @@ struct ora_ctx {
   double P[10][27];                        // pseudo_inv_A
   double rho_avr = 0, v_bulk = 0, forceytot = 0, maxchk_glb = 0;
   double reinit_residual = 0; int reinit_iters = 0, last_inflated = 0;
+  double last_gain = 0;  // blend factor of the last gain-one inflation
   // main.f90 locals
   F3 duold, dvold, dwold, pold, p_jump, p;
   double norm_old = 0;
@@ -251,6 +332,7 @@ struct ora_ctx {
     if (c.ns_conv == ICLS_NS_WENO5) return ICLS_E_UNSUPPORTED;  // boundfu stops (bound.f90:310-322)
     if (c.ns_conv != ICLS_NS_CNTR2) return ICLS_E_CONFIG;
     if (!(c.mass_threshold >= 0.)) return ICLS_E_CONFIG;
+    if (c.mass_gain_one != 0 && c.mass_gain_one != 1) return ICLS_E_CONFIG;
     bcy = c.bc_y;
     imax = itot; jmax = jtot; kmax = ktot;
     i1 = imax + 1; j1 = jmax + 1; k1 = kmax + 1;
@@ -528,6 +610,14 @@ struct ora_ctx {
           del(i, j, k) = d;
         }
   }
+  // sum(a(1:imax,1:jmax,1:kmax)) of the volume integral, exactly (XSum)
+  double exact_sum_interior(const F3& a) {
+    XSum s;
+    for (int k = 1; k <= kmax; ++k)
+      for (int j = 1; j <= jmax; ++j)
+        for (int i = 1; i <= imax; ++i) s.add(a(i, j, k));
+    return s.value();
+  }
   double sum_interior(const F3& a) {  // sum(a(1:imax,1:jmax,1:kmax)), column order
     double s = 0.;
     for (int k = 1; k <= kmax; ++k)
@@ -555,7 +645,7 @@ struct ora_ctx {
     F3 h_temp; shapeC(h_temp);
     for (int l = 0; l < L; ++l) {
       heaviside_c(l, 1.5 * dz, h_temp);
-      double vol = sum_interior(h_temp);
+      double vol = exact_sum_interior(h_temp);  // misc.f90:127-133, order-free
       volume[l] = 1. - vol / ((1. * itot * jtot) * ktot);
       if (l == 0) h_rho.v = h_temp.v;
       else for (size_t n = 0; n < h_rho.size(); ++n) h_rho.v[n] = std::min(h_rho.v[n], h_temp.v[n]);
@@ -984,7 +1074,7 @@ struct ora_ctx {
     }
     area = temp;
     if (c.TwoD) area = area / lx;
-    temp = sum_interior(dheav);
+    temp = exact_sum_interior(dheav);  // levelset.f90:505-506, order-free
     volume[l] = 1. - temp / ((1. * itot * jtot) * ktot);
     double loss_rate = lx * ly * lz * (volume[l] - init_volume[l]) / ((double)c.inflate_step * dt);
     if (c.TwoD) loss_rate = loss_rate / lx;
@@ -1013,7 +1103,28 @@ struct ora_ctx {
         }
     F3 phi3; shapeL(phi3);
     rk3_advect(c.i_space, u_lc, v_lc, w_lc, phi, phi3);
+    if (c.mass_gain_one) gain_one(l, phi, phi3);
     phi.v.swap(phi3.v);
+  }
+
+  // icls_config.mass_gain_one (no counterpart in the reference): the
+  // inflation moves the interface by about K/inflate_step times the volume
+  // error it measured (K ~ 0.66/s1 in grid units), so with the option the
+  // inflated level set phi1 is blended with the one before it,
+  // phi = phi0 + g (phi1 - phi0), g = (V0 - V)/(V1 - V), V and V1 the exact
+  // volumes before and after the inflation: the blend removes the measured
+  // error V - V0 to first order in the (small) displacement
+  void gain_one(int l, const F3& phi0, F3& phi1) {
+    const double s1 = 1.5 * dz;
+    lvset[l].v.swap(phi1.v);  // heaviside_c reads lvset[l]
+    F3 h1; shapeC(h1);
+    heaviside_c(l, s1, h1);
+    lvset[l].v.swap(phi1.v);
+    const double v1 = 1. - exact_sum_interior(h1) / ((1. * itot * jtot) * ktot);
+    const double d = v1 - volume[l];
+    const double g = d != 0. ? (init_volume[l] - volume[l]) / d : 0.;
+    for (size_t n = 0; n < phi1.size(); ++n) phi1.v[n] = phi0.v[n] + g * (phi1.v[n] - phi0.v[n]);
+    last_gain = g;
   }
 
   // ls_mass_correction (levelset.f90:377-400)
@@ -1634,6 +1745,13 @@ int ora_get_scalars(ora_ctx* o, icls_scalars* s) {
   return ICLS_OK;
 }
 int ora_set_dt(ora_ctx* o, double dt) { o->dt = dt; return ICLS_OK; }
+// the exact sum of n doubles (XSum), for the tests of its contract
+double ora_exact_sum(const double* x, long long n) {
+  XSum s;
+  for (long long q = 0; q < n; ++q) s.add(x[q]);
+  return s.value();
+}
+
 int ora_get_volumes(ora_ctx* o, double* v, double* v0) {
   for (int l = 0; l < o->L; ++l) { if (v) v[l] = o->volume[l]; if (v0) v0[l] = o->init_volume[l]; }
   return ICLS_OK;

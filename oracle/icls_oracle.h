@@ -28,6 +28,8 @@ int ora_download_field(ora_ctx* ctx, int field_id, int l, double* host);
 int ora_get_scalars(ora_ctx* ctx, icls_scalars* out);
 int ora_set_dt(ora_ctx* ctx, double dt);
 int ora_get_volumes(ora_ctx* ctx, double* volume, double* init_volume);
+/* exact, order-independent sum of n doubles (the volume integral's sum) */
+double ora_exact_sum(const double* x, long long n);
 int ora_get_pseudo_inv(ora_ctx* ctx, double* P /* 10x27 row-major */);
 
 int ora_init_program(ora_ctx* ctx);

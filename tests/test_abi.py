@@ -100,6 +100,7 @@ def test_config_layout_matches_header(tmp_path):
     (dict(curvature_model=1, lx=2.0), "E_UNSUPPORTED"),  # the network needs isotropic spacing
     (dict(curvature_model=1, mlp_fallback_tol=0.0), "E_CONFIG"),
     (dict(mass_threshold=-1e-6), "E_CONFIG"),
+    (dict(mass_gain_one=2), "E_CONFIG"),
 ])
 def test_create_rejects_bad_configs_on_host(lib, change, code):
     cfg = make_config(itot=32, jtot=32, ktot=32, lmax=1)

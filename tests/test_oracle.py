@@ -198,3 +198,46 @@ def test_error_paths():
     assert e.value.code == 4
     # step 0 only reports (chkdiv.f90:63)
     assert o.chkdiv(0)[3] == 0
+
+
+def _exact_sum(x):
+    import ctypes as C
+    from oracle.oracle import backend
+    lib = backend().lib
+    lib.ora_exact_sum.argtypes = [C.POINTER(C.c_double), C.c_longlong]
+    lib.ora_exact_sum.restype = C.c_double
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    return lib.ora_exact_sum(a.ctypes.data_as(C.POINTER(C.c_double)), len(a))
+
+
+def test_exact_sum_is_correctly_rounded_and_order_free():
+    """The volume integral's sum of H: exact, rounded once (ties to even).
+    For elements of magnitude above 2^-92 (none is truncated) it equals
+    math.fsum, the correctly rounded sum, in every order."""
+    import math
+    rng = np.random.default_rng(3)
+    # a drop's Heaviside field: far field exactly 1, a shell of fractions
+    h = np.ones(200_000)
+    shell = rng.integers(0, h.size, 4_000)
+    h[shell] = rng.uniform(0.0, 1.0, shell.size)
+    h[rng.integers(0, h.size, 50)] = -rng.uniform(0, 1e-17, 50)  # H < 0 by rounding
+    for x in (h, rng.standard_normal(10_000) * 10.0 ** rng.integers(-20, 1, 10_000)):
+        ref = math.fsum(x)
+        assert _exact_sum(x) == ref
+        assert _exact_sum(x[::-1]) == ref
+        assert _exact_sum(rng.permutation(x)) == ref
+    # ties to even and the sticky bit
+    assert _exact_sum([1.0, 2.0 ** -53]) == 1.0
+    assert _exact_sum([1.0 + 2.0 ** -52, 2.0 ** -53]) == 1.0 + 2.0 ** -51
+    assert _exact_sum([1.0, 2.0 ** -53, 2.0 ** -100]) == 1.0 + 2.0 ** -52
+    assert _exact_sum([1e-300, -1e-300, 0.0]) == 0.0
+    assert _exact_sum([-0.75, 0.25]) == -0.5
+    # a running double sum of the same shell depends on the order; this does not
+    run = [0.0, 0.0]
+    for t, x in enumerate((h, h[::-1])):
+        s = 0.0
+        for v in x:
+            s += v
+        run[t] = s
+    assert _exact_sum(h) == _exact_sum(h[::-1])
+    assert run[0] != run[1] or run[0] == math.fsum(h)
