@@ -9,6 +9,8 @@ pressure solve, projection, pressure update.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
   python bench.py --drift-steps 1000 [--inflate-step S] [--mass-threshold T] [--dt DT] [--gain-one]
                                                   (volume record, no timing)
+  python bench.py --rise-steps 2000 [--gain-one] [--workload rising_bubble_128]
+                                                  (rising bubble: centroid, rise velocity, drift)
 
 Default workload: the 256^3 box with 48 seeded drops.  The headline value is
 the FP32 form with the learned curvature in the loop (FP64 kept for the
@@ -84,16 +86,18 @@ def initial_state(wl):
 # -------------------------------------------------- algorithmic byte model
 # Compulsory HBM values of one launcher scope (the unit the per-kernel device
 # timer brackets), as (bulk values, FP64 values, unit): bulk values are the
-# form's field type (8 B in plain FP64, 4 B in the FP32 form), FP64 values stay
-# 8 B in both (pressures, pressure gradients, Poisson RHS, jumps).  Units:
-# N interior cells, B band cells of all drops (one batched scope covers every
-# drop), S |phi| <= 2dz shell cells of all drops.
+# form's field type (8 B in plain FP64, 4 B in the FP32 form: velocities,
+# materials, AB2 history, level sets, and the pressures pnew, pold with the
+# face jumps p_x,y,z and their old values), FP64 values stay 8 B in both (the
+# Poisson work array p and the jump Laplacian p_jump).  Units: N interior
+# cells, B band cells of all drops (one batched scope covers every drop),
+# S |phi| <= 2dz shell cells of all drops.
 ALG_VALUES = {
-    "ab2": (16, 8, "N"),             # u,v,w,miu,rho_uvw,duold x3 | pnew,pold,p_xyz,p_xyz_old -> dudt x3,duold x3
-    "correc": (9, 4, "N"),           # dudt x3 | p, p_xyz -> u,v,w, ucc,vcc,wcc
+    "ab2": (24, 0, "N"),             # u,v,w,miu,rho_uvw,duold x3,pnew,pold,p_xyz,p_xyz_old -> dudt x3,duold x3
+    "correc": (12, 1, "N"),          # dudt x3,p_xyz | p -> u,v,w, ucc,vcc,wcc
     "fillps": (3, 2, "N"),           # dudt x3 | pjump -> p
     "solver2d": (0, 2, "N"),         # p -> p (the transposes and sweeps between are not compulsory)
-    "pressure_update": (0, 4, "N"),  # p, pnew -> pnew, pold
+    "pressure_update": (3, 1, "N"),  # pnew | p -> pnew, pold
     "stream_vel": (1, 0, "N"),
     "materials_final": (6, 0, "N"),  # jiemian -> miu, rho, rho_uvw
     "tube": (2, 0, "B"),             # phi -> clipped phi on the band
@@ -101,7 +105,7 @@ ALG_VALUES = {
     "heaviside": (1, 0, "B"),
     "curvature": (2, 0, "S"),
     "recurvature": (2, 0, "S"),
-    "jumps": (4, 6, "S"),
+    "jumps": (8, 2, "S"),            # phi, kappa_re, p_xyz (read+write) | p_jump (read+write)
 }
 
 
@@ -309,6 +313,16 @@ def timed_steps(s, args, world, torch, istep, label, sampler=None):
     return ms, istep, s.launch_count() - launches0, clocks
 
 
+def step_roofline(roof, ms_step):
+    """The whole step against the HBM roofline: the algorithmic bytes of
+    every scope with a byte model (ALG_VALUES), per step, over the measured
+    (unprofiled) step time."""
+    peak = load_peaks().get("hbm_gbs", 6650.0)
+    b = roof.get("step_alg_bytes") or 0.0
+    roof["step_ms"] = ms_step
+    roof["step_frac"] = (b / (ms_step / 1000.0) / 1e9 / peak) if ms_step > 0 else None
+
+
 def kernel_table(s, args, cfg, stats, istep, f32, mlp_cells=None):
     """K more steps with every launcher scope bracketed by CUDA events: the
     per-kernel shares and the roofline of the dominant one.  The network's
@@ -328,19 +342,28 @@ def kernel_table(s, args, cfg, stats, istep, f32, mlp_cells=None):
     peaks = load_peaks()
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = (alg / (per_launch_ms / 1000.0) / 1e9) if alg else None
-    tpeak = peaks.get("bf16_tflops", 1590.0)
+    # the network runs inside a long step: its denominator is the sustained
+    # bf16 figure (the power-capped clock), not the burst one
+    tpeak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops", 1590.0))
+    tsrc = ("measured (cuBLAS bf16 sustained)" if "bf16_tflops_sustained" in peaks else
+            "measured (cuBLAS bf16 burst)" if "bf16_tflops" in peaks else "fallback")
     if name == "mlp_curvature" and mlp_cells:
         tf = MLP_FLOPS_PER_CELL * mlp_cells / (per_launch_ms / 1000.0) / 1e12
         roofline = {"bound": "tensor", "kernel": name, "achieved": tf, "peak": tpeak, "unit": "TFLOP/s",
                     "frac": tf / tpeak, "traffic": TRAFFIC.get((name, f32)), "flops": MLP_FLOPS_PER_CELL * mlp_cells,
-                    "share": ent["ms"] / tot, "launch_ms": per_launch_ms,
-                    "peak_source": "measured (cuBLAS bf16 burst)" if "bf16_tflops" in peaks else "fallback"}
+                    "share": ent["ms"] / tot, "launch_ms": per_launch_ms, "peak_source": tsrc}
     else:
         roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": (achieved / peak) if achieved else None, "traffic": TRAFFIC.get((name, f32)),
                     "alg_bytes": alg, "share": ent["ms"] / tot, "launch_ms": per_launch_ms,
                     "peak_source": "measured (burst copy)" if "hbm_gbs" in peaks else "fallback"}
     kernels = {}
+    step_bytes = 0.0  # algorithmic bytes of one step: the scopes with a byte model
+    for k, e in table.items():
+        ab = alg_bytes_per_launch(k, cfg, stats, f32)
+        if ab:
+            step_bytes += ab * e["timed"] / args.steps
+    roofline["step_alg_bytes"] = step_bytes
     for k, e in sorted(table.items(), key=lambda kv: -kv[1]["ms"]):
         if e["timed"] == 0:
             continue
@@ -439,6 +462,7 @@ def ours_arm(args):
     stats = {"band_total": float(sum(ref.band_count(l + 1) for l in range(cfg.lmax))),
              "shell_total": shell * cfg.lmax}
     roof64, kern64, istep = kernel_table(ref, args, cfg, stats, istep, False)
+    step_roofline(roof64, ms64 / args.steps)
     v64 = cells * args.steps * world / (ms64 / 1000.0) / 1e6
     plain = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / args.steps, "dtype": "f64",
              "gpu_launches": launches64, "clocks": clocks64, "roofline": roof64, "kernels": kern64}
@@ -458,6 +482,7 @@ def ours_arm(args):
         ev, fb = curvature_stats(s, reset=True)
         roof, kern, istep_f = kernel_table(s, args, cfg, stats, istep_f, True,
                                            ev / max(args.warmup + args.steps, 1))
+        step_roofline(roof, ms / args.steps)
         assert istep_f == istep
         errors = form_errors(s, ref, wl, shells, h, istep)
         errors["fallback_fraction"] = fb / max(ev, 1)
@@ -668,6 +693,12 @@ def combined_full(args):
     torch.cuda.set_device(local)
     wl = combined()
     cfg = wl.cfg
+    if args.gain_one:  # a stable correction for long runs (at 384^3 the reference's gain is about -7)
+        cfg.mass_gain_one = 1
+    if args.mass_threshold:
+        cfg.mass_threshold = args.mass_threshold
+    if args.inflate_step:
+        cfg.inflate_step = args.inflate_step
     h = cfg.lz / cfg.ktot
     cells = cfg.itot * cfg.jtot * cfg.ktot
     u, v, w = workload_velocity(wl)
@@ -753,7 +784,8 @@ def combined_full(args):
             "dtype": "f32 (f64 Poisson/pressure, volume integral, GFM jumps; bf16 network, f32 accumulate)",
             "data": "synthetic (seeded drops, seeded solenoidal velocity)",
             "config": {"grid": [cfg.itot, cfg.jtot, cfg.ktot], "drops": cfg.lmax, "dt": cfg.timestep,
-                       "We": cfg.We, "Re": cfg.Re},
+                       "We": cfg.We, "Re": cfg.Re, "inflate_step": cfg.inflate_step,
+                       "mass_threshold": cfg.mass_threshold or 1e-5, "gain_one": bool(cfg.mass_gain_one)},
             "fp32_learned_kappa": form, "plain_fp64": res["fp64"],
             "speedup_vs_fp64": form["value"] / res["fp64"]["value"], "errors": errors, "network": net_info}
     if rank == 0:
@@ -844,6 +876,71 @@ def drift_record(wl, ls, u, v, w, net, n, torch, inflate_step=0, mass_threshold=
     return out
 
 
+def rise_record(args):
+    """The rising bubble's record (--rise-steps N): the plain FP64 context
+    alone for N steps on its workload (default rising_bubble_128: 128 x 128 x
+    256 on [0,1]x[0,1]x[0,2], reinitialisation and the mass-correction check
+    every step), the bubble's centroid z and rise velocity (disp_cg,
+    disp_speed, write_vtk.f90:438-566) and its volume drift every --record
+    steps, and the device time per step.  --gain-one takes the gain-one mass
+    correction (the reference's, at inflate_step = 1, multiplies the volume
+    error by about 1 - 0.44 n = -55 per correction at this resolution)."""
+    import torch
+    rank, world, local = dist_env()
+    if world != 1:
+        raise SystemExit("--rise-steps runs on one GPU")
+    torch.cuda.set_device(local)
+    from icls_gpu import Solver
+    wl = make_workload(args.workload if args.workload != "multi_drop_256_48" else "rising_bubble_128")
+    cfg = wl.cfg
+    if args.dt:
+        cfg.timestep = args.dt
+    if args.inflate_step:
+        cfg.inflate_step = args.inflate_step
+    if args.mass_threshold:
+        cfg.mass_threshold = args.mass_threshold
+    cfg.mass_gain_one = 1 if args.gain_one else 0
+    ls, u, v, w = initial_state(wl)
+    s = Solver(cfg)
+    s.setup(ls, u, v, w)
+    stream = torch.cuda.ExternalStream(s.stream_ptr())
+    cg0, _ = s.disp(1)
+    every = max(args.record, 1)
+    rec, worst, stopped = [], 0.0, None
+    ms = 0.0
+    for istep in range(1, args.rise_steps + 1):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        try:
+            s.step(istep, 0)
+        except Exception as e:  # the reference's divergence or NaN checks
+            stopped = {"step": istep, "error": str(e)}
+            break
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        vol, v0 = s.volumes()
+        d = abs(vol[0] - v0[0]) / v0[0]
+        worst = max(worst, d)
+        if istep % every == 0 or istep == args.rise_steps:
+            cg, vel = s.disp(1)
+            sc = s.scalars()
+            rec.append([istep, sc["time"], cg[2], vel[2], d])
+    cells = cfg.itot * cfg.jtot * cfg.ktot
+    n = rec[-1][0] if rec else 0
+    line = {"report": "rising_bubble", "workload": wl.name, "steps": args.rise_steps, "dt": cfg.timestep,
+            "inflate_step": cfg.inflate_step, "reinit_step": cfg.reinit_step,
+            "mass_threshold": cfg.mass_threshold or 1e-5, "gain_one": bool(args.gain_one),
+            "centroid_z0": cg0[2], "volume_drift_max_rel": worst,
+            "mcell_steps_per_s": cells * n / (ms / 1000.0) / 1e6 if ms > 0 else None,
+            "ms_per_step": ms / max(n, 1),
+            "record_step_time_cgz_wz_drift": rec, "stopped": stopped}
+    s.close()
+    print(json.dumps(line))
+    return 0
+
+
 def volume_drift(args):
     """The volume record over a long run (drift_record), as its own JSON
     line: a report, not a throughput line."""
@@ -874,6 +971,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-drift", action="store_true", help="skip the 1000-step volume record")
+    ap.add_argument("--rise-steps", type=int, default=0,
+                    help="the rising bubble's centroid / rise-velocity / volume record over N steps")
+    ap.add_argument("--record", type=int, default=50, help="with --rise-steps: record every N steps")
     ap.add_argument("--no-forms", action="store_true",
                     help="plain FP64 only (no network training, no FP32 forms)")
     ap.add_argument("--dt", type=float, default=0.0, help="with --drift-steps: the time step (default: the workload's)")
@@ -893,6 +993,8 @@ def main():
         return reference_arm(args)
     if args.drift_steps > 0:
         return volume_drift(args)
+    if args.rise_steps > 0:
+        return rise_record(args)
     if args.workload == "combined_384_200":
         return combined_full(args)
     return ours_arm(args)

@@ -11,6 +11,8 @@
 
 namespace icls {
 
+// the fields of the predictor, type-erased: all but rho_avr hold the form's
+// field type (FP64, or FP32 in the precision form)
 struct MomArgs {
   const double *u, *v, *w, *miu, *rho_u, *rho_v, *rho_w;
   const double *duold, *dvold, *dwold;
@@ -182,7 +184,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 constexpr int MX = 32, MY = 8, MSX = MX + 2, MSY = MY + 2, MPX = MX + 1, MPY = MY + 1, MRING = 4;
 template <typename T>
 constexpr int ab2_smem() {
-  return (int)(4 * MRING * MSY * MSX * sizeof(T) + 2 * MRING * MPY * MPX * sizeof(double));
+  return (int)(4 * MRING * MSY * MSX * sizeof(T) + 2 * MRING * MPY * MPX * sizeof(T));
 }
 template <typename T>
 __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
           T* __restrict__ duold_out, T* __restrict__ dvold_out, T* __restrict__ dwold_out, int kc, int nch) {
   extern __shared__ __align__(16) unsigned char ab2_dyn[];
   typedef T Plane[MSY][MSX];
-  typedef double PPlane[MPY][MPX];
+  typedef T PPlane[MPY][MPX];  // pnew, pold in the form's field type
   Plane* ring = reinterpret_cast<Plane*>(ab2_dyn);  // [field * MRING + slot]
   PPlane* pring = reinterpret_cast<PPlane*>(ab2_dyn + 4 * MRING * sizeof(Plane));
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + MX * ty;
@@ -222,8 +224,8 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
       const int gi = i0 + sx, gj = j0 + sy;
       if (gi <= p.imax + 1 && gj <= p.jmax + 1) {
         const long long g = idxC(p, gi, gj, kk);
-        cp_async_el(&pring[s][sy][sx], a.pnew + g);
-        cp_async_el(&pring[MRING + s][sy][sx], a.pold + g);
+        cp_async_el(&pring[s][sy][sx], cT<T>(a.pnew) + g);
+        cp_async_el(&pring[MRING + s][sy][sx], cT<T>(a.pold) + g);
       }
     }
   };
@@ -239,7 +241,9 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
     if (ok) {
       ru = rhu[q]; rv = rhv[q]; rw = rhw[q];
       ou = hu[q]; ov = hv[q]; ow = hw[q];
-      qx = a.px[c]; qxo = a.pxold[c]; qy = a.py[c]; qyo = a.pyold[c]; qz = a.pz[c]; qzo = a.pzold[c];
+      qx = (double)cT<T>(a.px)[c]; qxo = (double)cT<T>(a.pxold)[c];
+      qy = (double)cT<T>(a.py)[c]; qyo = (double)cT<T>(a.pyold)[c];
+      qz = (double)cT<T>(a.pz)[c]; qzo = (double)cT<T>(a.pzold)[c];
     }
     issue_plane(k + 1);
     cp_async_wait_all();
@@ -252,7 +256,7 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
       auto W = [&](int di, int dj, int dk) { return ring[2 * MRING + sl(dk)][ty + 1 + dj][tx + 1 + di]; };
       auto M = [&](int di, int dj, int dk) { return ring[3 * MRING + sl(dk)][ty + 1 + dj][tx + 1 + di]; };
       auto PH = [&](int di, int dj, int dk) {
-        return 2. * pring[sl(dk)][ty + dj][tx + di] - pring[MRING + sl(dk)][ty + dj][tx + di];
+        return 2. * (double)pring[sl(dk)][ty + dj][tx + di] - (double)pring[MRING + sl(dk)][ty + dj][tx + di];
       };
       const double ph0 = PH(0, 0, 0);
       const T Ru = rhs_u<T>(p, U, V, W, M, ru, rho_avr);

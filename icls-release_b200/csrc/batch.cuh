@@ -38,6 +38,9 @@ struct Col {
   bool ok;     // inside the written spans
   bool cxy;    // a computed column
 };
+// Flat tasks: block bx of a chunk takes the region's written columns
+// 256 bx .. 256 bx + 255 in row-major order (x fastest), so a region of any
+// width fills whole warps; otherwise a block is a TBX x TBY column tile.
 __device__ __forceinline__ Col col_of(const Params& p, const LsTask& t, int local) {
   Col c;
   const int bx = local % t.tx;
@@ -45,8 +48,14 @@ __device__ __forceinline__ Col col_of(const Params& p, const LsTask& t, int loca
   const int by = r % t.ty;
   const int ch = r / t.ty;
   c.tile = bx + t.tx * by;
-  c.X = bx * TBX + (int)threadIdx.x;
-  c.Y = by * TBY + (int)threadIdx.y;
+  if (t.flat) {
+    const int col = bx * (TBX * TBY) + (int)threadIdx.x + TBX * (int)threadIdx.y;
+    c.Y = col / t.r.xn;
+    c.X = col - c.Y * t.r.xn;
+  } else {
+    c.X = bx * TBX + (int)threadIdx.x;
+    c.Y = by * TBY + (int)threadIdx.y;
+  }
   c.ok = c.X < t.r.xn && c.Y < t.r.yn;
   c.i = t.r.xa + c.X;
   if (c.i > p.imax) c.i -= p.imax;

@@ -182,13 +182,14 @@ size_t tn(const Params& P, long long n) { return P.f32 ? (size_t)(n + 1) / 2 : (
 
 int allocate(Ctx& c) {
   const Params& P = c.P;
-  // FP64 in both forms: pressures, jumps (the Poisson solve and the GFM
-  // assembly stay FP64)
-  for (double** f : {&c.pnew, &c.pold, &c.p, &c.px, &c.py, &c.pz, &c.pxold, &c.pyold, &c.pzold, &c.pjump})
-    AL(*f, (size_t)P.nC);
-  // the form's field type
+  // FP64 in both forms: the Poisson work array and the Laplacian of the
+  // jumps (the solve's right-hand side)
+  for (double** f : {&c.p, &c.pjump}) AL(*f, (size_t)P.nC);
+  // the form's field type, the pressures and face jumps included: the FP32
+  // momentum and correction stencils read them (the jumps are assembled in
+  // FP64 and stored in the field type)
   for (double** f : {&c.u, &c.v, &c.w, &c.dudt, &c.dvdt, &c.dwdt, &c.miu, &c.rho, &c.jiemian, &c.curv, &c.dheav,
-                     &c.kappa})
+                     &c.kappa, &c.pnew, &c.pold, &c.px, &c.py, &c.pz, &c.pxold, &c.pyold, &c.pzold})
     AL(*f, tn(P, P.nC));
   for (int h = 0; h < 2; ++h) {
     AL(c.duold[h], tn(P, P.nI)); AL(c.dvold[h], tn(P, P.nI)); AL(c.dwold[h], tn(P, P.nI));
@@ -338,8 +339,7 @@ double* field_ptr(Ctx& c, int id, int l, long long* n) {
 // the field is stored in the form's field type (else FP64 in both forms)
 bool tfield(int id) {
   switch (id) {
-    case ICLS_F_PNEW: case ICLS_F_POLD: case ICLS_F_P: case ICLS_F_PX: case ICLS_F_PY: case ICLS_F_PZ:
-    case ICLS_F_PXOLD: case ICLS_F_PYOLD: case ICLS_F_PZOLD: case ICLS_F_PJUMP:
+    case ICLS_F_P: case ICLS_F_PJUMP:
       return false;
     default:
       return true;
@@ -912,10 +912,10 @@ int gfm4p(Ctx& c) {
   std::swap(c.px, c.pxold);
   std::swap(c.py, c.pyold);
   std::swap(c.pz, c.pzold);
-  const size_t bytes = sizeof(double) * (size_t)c.P.nC;
-  cudaMemsetAsync(c.px, 0, bytes, c.s);
-  cudaMemsetAsync(c.py, 0, bytes, c.s);
-  cudaMemsetAsync(c.pz, 0, bytes, c.s);
+  const size_t bytes = sizeof(double) * (size_t)c.P.nC, tbytes = sizeof(double) * tn(c.P, c.P.nC);
+  cudaMemsetAsync(c.px, 0, tbytes, c.s);
+  cudaMemsetAsync(c.py, 0, tbytes, c.s);
+  cudaMemsetAsync(c.pz, 0, tbytes, c.s);
   cudaMemsetAsync(c.pjump, 0, bytes, c.s);
   for (int g = 0; g < n_groups(c); ++g) {
     const std::vector<int> drops = group_drops(c, g);
@@ -1224,7 +1224,7 @@ int icls_init_program(icls_ctx* h) {
   for (int l = 0; l < c.P.L; ++l) launch_boundmls(c, c.lv[l]);
   int rc = measure_bands(c);
   if (rc) return rc;
-  launch_boundp(c, c.pnew);
+  launch_boundp(c, c.pnew, true);
   launch_average_vel(c);
   update_materials(c);
   CK(cudaMemcpyAsync(c.dvol0, c.dvol, sizeof(double) * c.P.L, cudaMemcpyDeviceToDevice, c.s));
@@ -1233,7 +1233,7 @@ int icls_init_program(icls_ctx* h) {
   for (int l = 0; l < c.P.L; ++l) c.init_volume_h[l] = c.h_vol[l];
   c.hist = 0;
   launch_mom_main(c, c.duold[0], c.dvold[0], c.dwold[0]);
-  const size_t bytes = sizeof(double) * (size_t)c.P.nC;
+  const size_t bytes = sizeof(double) * tn(c.P, c.P.nC);  // the pressures are in the field type
   CK(cudaMemcpyAsync(c.pold, c.pnew, bytes, cudaMemcpyDeviceToDevice, c.s));
   CK(cudaMemcpyAsync(c.pxold, c.px, bytes, cudaMemcpyDeviceToDevice, c.s));
   CK(cudaMemcpyAsync(c.pyold, c.py, bytes, cudaMemcpyDeviceToDevice, c.s));
@@ -1311,8 +1311,8 @@ int icls_boundp(icls_ctx* h, int id) {
   if (!h) return ICLS_E_ARG;
   long long n;
   double* d = field_ptr(h->c, id, 1, &n);
-  if (!d || n != h->c.P.nC || (h->c.P.f32 && tfield(id))) return ICLS_E_ARG;
-  launch_boundp(h->c, d);
+  if (!d || n != h->c.P.nC) return ICLS_E_ARG;
+  launch_boundp(h->c, d, tfield(id));
   return check_launch();
 }
 

@@ -32,7 +32,7 @@ constexpr int TBX = 32, TBY = 8;    // column tile of a batched launch
 struct LsTask {
   Region r;
   int tx, ty, nch, kc;
-  int l, pad;
+  int l, flat;           // flat: a block takes 256 consecutive columns (else TBX x TBY tiles)
   double bg, bgg;        // far-field values of the apron: rows 0..k1 / ghost rows
   const double* phi0;    // RK base (read at the thread's own cell only)
   const double* phis;    // stage input (stencil reads)
@@ -184,7 +184,7 @@ void set_pseudo_inverse(const double* P270, cudaStream_t s);
 Region full_region(const Params& P);
 bool region_full(const Params& P, const Region& r);
 Region c_region(const Params& P, const Region& r, int apron);
-void set_tiles(LsBatch& b, int kc);
+void set_tiles(LsBatch& b, int kc, bool flat = true);
 void launch_tube(Ctx& c, const LsBatch& b);
 void launch_adv_stage(Ctx& c, const LsBatch& b, int scheme, int stage1, double a, double bb, double fdt,
                       const double* vu, const double* vv, const double* vw);
@@ -232,7 +232,8 @@ void launch_fillps(Ctx& c, int add_pjump);
 void launch_add_pjump(Ctx& c);
 void launch_correc(Ctx& c, int fused_bc);
 void launch_bounduvw(Ctx& c, double* u, double* v, double* w);
-void launch_boundp(Ctx& c, double* p);
+// tfield: the array holds the form's field type (FP32 in the precision form)
+void launch_boundp(Ctx& c, double* p, bool tfield = false);
 // the y-wall rows of bounduvw / boundp (bound.f90:81-282) for bc_y != periodic,
 // applied after the periodic halos (i = 1..imax, k = 1..kmax)
 void launch_ywalls_uvw(Ctx& c, double* u, double* v, double* w);

@@ -5,26 +5,27 @@
 // The arithmetic per cell is the one of k_ab2 in ab2.cuh (the same rhs_u/v/w
 // and ab2_update_v templates, compiled with -fmad=false), so the result is
 // bit-identical to it.  What changes is how the 18 input fields reach the
-// SM.  A persistent CTA (one per SM) walks work items = (32 x 8 column tile,
-// chunk of z rows).  One producer thread issues, per row, 3-D TMA box loads
-// of every field into shared-memory rings and completes them on mbarriers;
-// eight consumer warps compute row k from the rings while rows k+2..k+4 are
-// in flight, and release each slot with one arrive per warp.  No thread
-// issues a global load and no block-wide barrier runs inside the loop.
+// SM.  A persistent CTA (one per SM, 16 warps) walks work items = (32 x 16
+// column tile, chunk of z rows).  Thread 0 issues, per row, 3-D TMA box
+// loads of every field into two shared-memory rings, completed on
+// mbarriers: the stencil fields two rows ahead of the row being computed,
+// the pointwise fields one row ahead.  Each warp waits for the rows it
+// needs and releases a slot with one arrive; no thread issues a global load
+// and no block-wide barrier runs inside the loop.
 //
-//   stencil ring (SR = 6 rows):   u, v, w, miu, pnew, pold — shape C,
-//                                 box 34 x 10 at (i0-1, j0-1, k)
-//   pointwise ring (PR = 4 rows): p_x, p_y, p_z and their old values —
-//                                 shape C, box 34 x 8 at (i0-1, j0, k);
+//   stencil ring (SR = 4 rows):   u, v, w, miu, pnew, pold — shape C,
+//                                 box 34 x 18 at (i0-1, j0-1, k)
+//   pointwise ring (PR = 2 rows): p_x, p_y, p_z and their old values —
+//                                 shape C, box 34 x 16 at (i0-1, j0, k);
 //                                 rho_u, rho_v, rho_w, duold, dvold, dwold —
-//                                 shape I, box 32 x 8 at (i0, j0, k)
+//                                 shape I, box 32 x 16 at (i0, j0, k)
 //
 // The tensor maps cover this GPU's own arrays only; no load uses cluster
 // multicast.  Every box starts at an even x index (32 * tile, element
 // size 8 B), every row pitch is a multiple of 16 B (imax even), and each
 // shared-memory box starts on a 128-byte boundary.  Every mbarrier wait has
-// an iteration limit: on expiry the kernel sets DevScalars::wait_err, the
-// producer lets its outstanding copies land (bounded again) and all threads
+// an iteration limit: on expiry the kernel sets DevScalars::wait_err, thread
+// 0 lets its outstanding copies land (bounded again) and all threads
 // return.
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -38,22 +39,24 @@
 namespace icls {
 namespace {
 
-constexpr int TX = 32, TY = 8;                 // column tile
-constexpr int SW = TX + 2, SH = TY + 2;         // stencil box 34 x 10
-constexpr int SR = 6, PR = 4;                   // ring slots
-constexpr int NCW = TY;                          // consumer warps
-constexpr int kThreadsTma = 32 * (NCW + 1);      // + one producer warp
-constexpr int kStBox = 2816;                     // 34*10*8 = 2720 B, padded to 128 B
-constexpr int kStBytes = SW * SH * 8;            // bytes one stencil box delivers
-constexpr int kPgBox = SW * TY * 8;              // 34*8*8 = 2176 B (17 x 128)
-constexpr int kPiBox = TX * TY * 8;              // 32*8*8 = 2048 B
-constexpr int kStSlot = 6 * kStBox;              // 16896
-constexpr int kPwSlot = 6 * kPgBox + 6 * kPiBox; // 25344
+constexpr int TX = 32, TY = 16;                  // column tile
+constexpr int SW = TX + 2, SH = TY + 2;          // stencil box 34 x 18
+constexpr int SR = 4, PR = 2;                    // ring slots
+constexpr int NW = TY;                           // warps: one tile row each
+constexpr int kThreadsTma = 32 * NW;
+constexpr int kStBytes = SW * SH * 8;            // 4896 B a stencil box delivers
+constexpr int kStBox = 4992;                     // padded to 128 B
+constexpr int kPgBox = SW * TY * 8;              // 4352 B (34 x 128)
+constexpr int kPiBox = TX * TY * 8;              // 4096 B
+constexpr int kStSlot = 6 * kStBox;              // 29952
+constexpr int kPwSlot = 6 * kPgBox + 6 * kPiBox; // 50688
 constexpr int kStTx = 6 * kStBytes;              // expect-tx bytes per stencil row
 constexpr int kPwTx = kPwSlot;                   // per pointwise row
 constexpr int kRowsPerItem = 32;
 constexpr long long kSpin = 1 << 24;             // mbarrier polls before giving up
-constexpr int kSmemTma = SR * kStSlot + PR * kPwSlot + 2 * (SR + PR) * 8 + 16;
+constexpr int kSmemTma = SR * kStSlot + PR * kPwSlot + 2 * (SR + PR) * 8 + 16 + 32;  // + flag, cursors
+static_assert(kStBytes <= kStBox && kStBox % 128 == 0 && kPgBox % 128 == 0 && kPiBox % 128 == 0, "box layout");
+static_assert(kSmemTma <= 232448, "shared memory of one CTA");
 
 struct Ab2Maps {
   CUtensorMap st[6];  // u v w miu pnew pold
@@ -109,6 +112,14 @@ __device__ __forceinline__ Item item_of(const Params& p, int it, int ntx, int nt
   return r;
 }
 
+// The issuing side of one ring: the next row to load (item `it`, row kk)
+// and the positions issued so far.  Stencil rows of an item run ka-1 ..
+// kb+1, pointwise rows ka .. kb.
+struct Cursor {
+  int it, kk;
+  long long n;
+};
+
 __global__ void __launch_bounds__(kThreadsTma, 1)
     k_ab2_tma(const __grid_constant__ Ab2Maps maps, Params p, const double* __restrict__ rho_avr_p,
               double* __restrict__ dudt, double* __restrict__ dvdt, double* __restrict__ dwdt,
@@ -123,80 +134,86 @@ __global__ void __launch_bounds__(kThreadsTma, 1)
   uint64_t* pw_full = bars + 2 * SR;
   uint64_t* pw_empty = bars + 2 * SR + PR;
   volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 2 * (SR + PR));
+  // thread 0's issuing state, in shared memory to keep the compute
+  // threads' registers free
+  Cursor& cs = *reinterpret_cast<Cursor*>(tsm + SR * kStSlot + PR * kPwSlot + 2 * (SR + PR) * 8 + 16);
+  Cursor& cp = *(&cs + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nitems = ntx * nty * nch;
   if (threadIdx.x == 0) {
     for (int s = 0; s < SR; ++s) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&st_full[s])));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(&st_empty[s])), "r"(NCW));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(&st_empty[s])), "r"(NW));
     }
     for (int s = 0; s < PR; ++s) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&pw_full[s])));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(&pw_empty[s])), "r"(NCW));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(&pw_empty[s])), "r"(NW));
     }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    cs.it = cp.it = (int)blockIdx.x;
+    if (cs.it < nitems) {
+      const Item I = item_of(p, cs.it, ntx, nty, nch, kc);
+      cs.kk = I.ka - 1;
+      cp.kk = I.ka;
+    }
+    cs.n = cp.n = 0;
   }
   __syncthreads();
 
-  const int nitems = ntx * nty * nch;
-
-  if (warp == NCW) {
-    // ------------------------------------------------------------ producer
-    if (lane != 0) return;
-    long long ns = 0, np = 0;  // stream positions issued
-    bool ok = true;
-    for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
-      const Item I = item_of(p, it, ntx, nty, nch, kc);
-      const int x0 = I.i0 - 1;  // box origin: even (32 * tile)
-      for (int kk = I.ka - 1; kk <= I.kb + 1 && ok; ++kk) {
-        {
-          const int s = (int)(ns % SR);
-          if (ns >= SR && !bar_wait(su32(&st_empty[s]), (uint32_t)(((ns / SR) - 1) & 1), abort_flag)) {
-            ok = false;
-            break;
-          }
-          if (*abort_flag) { ok = false; break; }
-          const uint32_t fb = su32(&st_full[s]);
-          bar_expect(fb, kStTx);
-          const uint32_t dst = su32(st_base + s * kStSlot);
+  // thread 0: issue stencil rows until `ts` positions and pointwise rows
+  // until `tp` positions are issued (or the CTA's items end); a slot is
+  // reused once every warp released its previous row.  False if a wait
+  // gave up.
+  auto produce = [&](long long ts, long long tp) -> bool {
+    while (cs.n < ts && cs.it < nitems) {
+      const int s = (int)(cs.n % SR);
+      if (cs.n >= SR && !bar_wait(su32(&st_empty[s]), (uint32_t)(((cs.n / SR) - 1) & 1), abort_flag)) return false;
+      const Item I = item_of(p, cs.it, ntx, nty, nch, kc);
+      const uint32_t fb = su32(&st_full[s]);
+      bar_expect(fb, kStTx);
+      const uint32_t dst = su32(st_base + s * kStSlot);
 #pragma unroll
-          for (int f = 0; f < 6; ++f) tma3(dst + f * kStBox, &maps.st[f], x0, I.j0 - 1, kk, fb);
-          ++ns;
-        }
-        if (kk >= I.ka && kk <= I.kb) {
-          const int s = (int)(np % PR);
-          if (np >= PR && !bar_wait(su32(&pw_empty[s]), (uint32_t)(((np / PR) - 1) & 1), abort_flag)) {
-            ok = false;
-            break;
-          }
-          if (*abort_flag) { ok = false; break; }
-          const uint32_t fb = su32(&pw_full[s]);
-          bar_expect(fb, kPwTx);
-          const uint32_t dst = su32(pw_base + s * kPwSlot);
-#pragma unroll
-          for (int f = 0; f < 6; ++f) tma3(dst + f * kPgBox, &maps.pg[f], x0, I.j0, kk, fb);
-#pragma unroll
-          for (int f = 0; f < 6; ++f) tma3(dst + 6 * kPgBox + f * kPiBox, &maps.pi[f], x0, I.j0 - 1, kk - 1, fb);
-          ++np;
-        }
+      for (int f = 0; f < 6; ++f) tma3(dst + f * kStBox, &maps.st[f], I.i0 - 1, I.j0 - 1, cs.kk, fb);
+      ++cs.n;
+      if (++cs.kk > I.kb + 1) {
+        cs.it += gridDim.x;
+        if (cs.it < nitems) cs.kk = item_of(p, cs.it, ntx, nty, nch, kc).ka - 1;
       }
     }
-    if (!ok) {
-      *abort_flag = 1;
-      atomicExch(&dsc->wait_err, 1);
-      // let the copies still in flight land before the CTA's shared memory
-      // is released: the last min(SR, ns) stencil and min(PR, np) pointwise
-      // positions each have one outstanding phase
-      for (long long n = std::max(0LL, ns - SR); n < ns; ++n)
+    while (cp.n < tp && cp.it < nitems) {
+      const int s = (int)(cp.n % PR);
+      if (cp.n >= PR && !bar_wait(su32(&pw_empty[s]), (uint32_t)(((cp.n / PR) - 1) & 1), abort_flag)) return false;
+      const Item I = item_of(p, cp.it, ntx, nty, nch, kc);
+      const uint32_t fb = su32(&pw_full[s]);
+      bar_expect(fb, kPwTx);
+      const uint32_t dst = su32(pw_base + s * kPwSlot);
+#pragma unroll
+      for (int f = 0; f < 6; ++f) tma3(dst + f * kPgBox, &maps.pg[f], I.i0 - 1, I.j0, cp.kk, fb);
+#pragma unroll
+      for (int f = 0; f < 6; ++f) tma3(dst + 6 * kPgBox + f * kPiBox, &maps.pi[f], I.i0 - 1, I.j0 - 1, cp.kk - 1, fb);
+      ++cp.n;
+      if (++cp.kk > I.kb) {
+        cp.it += gridDim.x;
+        if (cp.it < nitems) cp.kk = item_of(p, cp.it, ntx, nty, nch, kc).ka;
+      }
+    }
+    return true;
+  };
+  // on a failed wait: flag it; thread 0 lets the copies it issued land
+  // before the CTA's shared memory is released
+  auto give_up = [&]() {
+    *abort_flag = 1;
+    if (lane == 0) atomicExch(&dsc->wait_err, 1);
+    if (threadIdx.x == 0) {
+      for (long long n = std::max(0LL, cs.n - SR); n < cs.n; ++n)
         bar_wait(su32(&st_full[n % SR]), (uint32_t)((n / SR) & 1), nullptr);
-      for (long long n = std::max(0LL, np - PR); n < np; ++n)
+      for (long long n = std::max(0LL, cp.n - PR); n < cp.n; ++n)
         bar_wait(su32(&pw_full[n % PR]), (uint32_t)((n / PR) & 1), nullptr);
     }
-    return;
-  }
+  };
 
-  // -------------------------------------------------------------- consumers
   const int tx = lane, ty = warp;
   const double rho_avr = *rho_avr_p;
   long long ns = 0, np = 0;  // stream positions consumed
@@ -204,22 +221,25 @@ __global__ void __launch_bounds__(kThreadsTma, 1)
     const Item I = item_of(p, it, ntx, nty, nch, kc);
     const int i = I.i0 + tx, j = I.j0 + ty;
     const bool ok = i <= p.imax && j <= p.jmax;
-    const long long sb = ns;  // position of row ka-1
+    const long long sb = ns;   // stencil position of row ka-1
+    const long long pb = np;   // pointwise position of row ka
     double dw_km1 = 0.;
-    bool fail = false;
     for (int k = I.ka; k <= I.kb; ++k) {
       const long long r = k - I.ka;
+      // stencil through row k+2, pointwise through row k+1
+      bool fail = false;
+      if (threadIdx.x == 0) fail = !produce(sb + r + 4, pb + r + 2);
+      __syncwarp();
       if (r == 0) {
         fail |= !bar_wait(su32(&st_full[sb % SR]), (uint32_t)((sb / SR) & 1), abort_flag);
         fail |= !bar_wait(su32(&st_full[(sb + 1) % SR]), (uint32_t)(((sb + 1) / SR) & 1), abort_flag);
       }
       const long long n2 = sb + r + 2;
       fail |= !bar_wait(su32(&st_full[n2 % SR]), (uint32_t)((n2 / SR) & 1), abort_flag);
-      const long long pn = np + r;
+      const long long pn = pb + r;
       fail |= !bar_wait(su32(&pw_full[pn % PR]), (uint32_t)((pn / PR) & 1), abort_flag);
       if (fail || *abort_flag) {
-        *abort_flag = 1;
-        if (lane == 0) atomicExch(&dsc->wait_err, 1);
+        give_up();
         return;
       }
       const double* sm_ = reinterpret_cast<const double*>(st_base + ((sb + r) % SR) * kStSlot);
@@ -287,7 +307,7 @@ __global__ void __launch_bounds__(kThreadsTma, 1)
       bar_arrive(su32(&st_empty[(sb + nr + 1) % SR]));
     }
     ns = sb + nr + 2;
-    np += nr;
+    np = pb + nr;
   }
 }
 

@@ -201,8 +201,8 @@ __device__ __forceinline__ double axis_jump(const Params& p, const T* __restrict
 // shells of three or more drops may differ in the last bit.
 template <typename T>
 __global__ void __launch_bounds__(NT, 3) k_jumps(Params p, const __grid_constant__ LsBatch B,
-                                              double* __restrict__ pjump, double* __restrict__ px,
-                                              double* __restrict__ py, double* __restrict__ pz) {
+                                              double* __restrict__ pjump, T* __restrict__ px,
+                                              T* __restrict__ py, T* __restrict__ pz) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const T* __restrict__ cv = cT<T>(t.phis);
@@ -229,9 +229,9 @@ __global__ void __launch_bounds__(NT, 3) k_jumps(Params p, const __grid_constant
       pj = 0.; fx = 0.; fy = 0.; fz = 0.;
     }
     atomicAdd(pjump + cc, pj);
-    atomicAdd(px + cc, fx);
-    atomicAdd(py + cc, fy);
-    atomicAdd(pz + cc, fz);
+    atomicAdd(px + cc, (T)fx);  // assembled in FP64, stored in the field type
+    atomicAdd(py + cc, (T)fy);
+    atomicAdd(pz + cc, (T)fz);
   }
 }
 
@@ -310,7 +310,8 @@ void launch_jumps(Ctx& c, const LsBatch& b) {
   if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "jumps", 1);
   if (c.P.f32)
-    k_jumps<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.pjump, c.px, c.py, c.pz);
+    k_jumps<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.pjump, reinterpret_cast<float*>(c.px),
+                                                     reinterpret_cast<float*>(c.py), reinterpret_cast<float*>(c.pz));
   else
     k_jumps<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.pjump, c.px, c.py, c.pz);
 }

@@ -1109,13 +1109,20 @@ Region c_region(const Params& P, const Region& r, int ap) {
 }
 
 // tiles, z chunks (kc rows each, the last one longer; kc <= 0: one chunk)
-// and block offsets of a batch
-void set_tiles(LsBatch& b, int kc) {
+// and block offsets of a batch; flat tiles of 256 consecutive columns
+// (col_of), or TBX x TBY tiles for the kernels that stage a 2-D tile
+void set_tiles(LsBatch& b, int kc, bool flat) {
   int s = 0;
   for (int q = 0; q < b.n; ++q) {
     LsTask& t = b.t[q];
-    t.tx = (t.r.xn + TBX - 1) / TBX;
-    t.ty = (t.r.yn + TBY - 1) / TBY;
+    t.flat = flat ? 1 : 0;
+    if (flat) {
+      t.tx = (t.r.xn * t.r.yn + TBX * TBY - 1) / (TBX * TBY);
+      t.ty = 1;
+    } else {
+      t.tx = (t.r.xn + TBX - 1) / TBX;
+      t.ty = (t.r.yn + TBY - 1) / TBY;
+    }
     const int nz = t.r.z1 - t.r.z0 + 1;
     if (kc <= 0 || kc >= nz) {
       t.nch = 1;
@@ -1141,9 +1148,22 @@ void set_tiles(LsBatch& b, int kc) {
     }                                   \
   } while (0)
 
-void launch_tube(Ctx& c, const LsBatch& b) {
-  if (b.n == 0) return;
+void launch_tube(Ctx& c, const LsBatch& flat) {
+  if (flat.n == 0) return;
   Scope sc_(c.prof, c.s, "tube", 1);
+  // k_tube stages a TBX x TBY tile with its halo in shared memory: the same
+  // tasks and z chunks on 2-D tiles
+  LsBatch b = flat;
+  int s = 0;
+  for (int q = 0; q < b.n; ++q) {
+    LsTask& t = b.t[q];
+    t.flat = 0;
+    t.tx = (t.r.xn + TBX - 1) / TBX;
+    t.ty = (t.r.yn + TBY - 1) / TBY;
+    b.start[q] = s;
+    s += t.tx * t.ty * t.nch;
+  }
+  b.start[b.n] = s;
   int* lo = c.d_bbox;
   int* hi = c.d_bbox + 5 * c.P.L;
   BY_FORM(c, (k_tube<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.d_nbcnt, lo, hi)),

@@ -97,26 +97,26 @@ __global__ void __launch_bounds__(NT) k_add(Params p, double* __restrict__ a, co
 // correc of one component (correc.f90:27-39)
 // (the pressure gradient in FP64, the result in the form's type T)
 template <typename T>
-__device__ __forceinline__ T corr_u(const Params& p, const T* dudt, const double* pp, const double* px, int i, int j,
+__device__ __forceinline__ T corr_u(const Params& p, const T* dudt, const double* pp, const T* px, int i, int j,
                                     int k) {
   const long long c = idxC(p, i, j, k);
-  if (sizeof(T) == sizeof(double)) return (T)(dudt[c] - div_rho0(p, p.dt * p.dxi * ((pp[c + 1] - pp[c]) - px[c])));
-  return dudt[c] - (T)(div_rho0(p, p.dt * p.dxi * ((pp[c + 1] - pp[c]) - px[c])));
+  if (sizeof(T) == sizeof(double)) return (T)(dudt[c] - div_rho0(p, p.dt * p.dxi * ((pp[c + 1] - pp[c]) - (double)px[c])));
+  return dudt[c] - (T)(div_rho0(p, p.dt * p.dxi * ((pp[c + 1] - pp[c]) - (double)px[c])));
 }
 template <typename T>
-__device__ __forceinline__ T corr_v(const Params& p, const T* dvdt, const double* pp, const double* py, int i, int j,
+__device__ __forceinline__ T corr_v(const Params& p, const T* dvdt, const double* pp, const T* py, int i, int j,
                                     int k) {
   const long long c = idxC(p, i, j, k);
-  if (sizeof(T) == sizeof(double)) return (T)(dvdt[c] - div_rho0(p, p.dt * p.dyi * ((pp[c + p.nCx] - pp[c]) - py[c])));
-  return dvdt[c] - (T)(div_rho0(p, p.dt * p.dyi * ((pp[c + p.nCx] - pp[c]) - py[c])));
+  if (sizeof(T) == sizeof(double)) return (T)(dvdt[c] - div_rho0(p, p.dt * p.dyi * ((pp[c + p.nCx] - pp[c]) - (double)py[c])));
+  return dvdt[c] - (T)(div_rho0(p, p.dt * p.dyi * ((pp[c + p.nCx] - pp[c]) - (double)py[c])));
 }
 template <typename T>
-__device__ __forceinline__ T corr_w(const Params& p, const T* dwdt, const double* pp, const double* pz, int i, int j,
+__device__ __forceinline__ T corr_w(const Params& p, const T* dwdt, const double* pp, const T* pz, int i, int j,
                                     int k) {
   const long long c = idxC(p, i, j, k);
   const long long sz = (long long)p.nCx * p.nCy;
-  if (sizeof(T) == sizeof(double)) return (T)(dwdt[c] - div_rho0(p, p.dt * p.dzi * ((pp[c + sz] - pp[c]) - pz[c])));
-  return dwdt[c] - (T)(div_rho0(p, p.dt * p.dzi * ((pp[c + sz] - pp[c]) - pz[c])));
+  if (sizeof(T) == sizeof(double)) return (T)(dwdt[c] - div_rho0(p, p.dt * p.dzi * ((pp[c + sz] - pp[c]) - (double)pz[c])));
+  return dwdt[c] - (T)(div_rho0(p, p.dt * p.dzi * ((pp[c + sz] - pp[c]) - (double)pz[c])));
 }
 
 struct CorrArgs {
@@ -131,9 +131,9 @@ __global__ void __launch_bounds__(NT) k_correc_interior(Params p, CorrArgs a) {
   int i, j, k;
   if (!cell3(kI0, cI1(p).v, i, j, k)) return;
   const long long c = idxC(p, i, j, k);
-  mT<T>(a.u)[c] = corr_u(p, cT<T>(a.dudt), a.p, a.px, i, j, k);
-  mT<T>(a.v)[c] = corr_v(p, cT<T>(a.dvdt), a.p, a.py, i, j, k);
-  mT<T>(a.w)[c] = corr_w(p, cT<T>(a.dwdt), a.p, a.pz, i, j, k);
+  mT<T>(a.u)[c] = corr_u(p, cT<T>(a.dudt), a.p, cT<T>(a.px), i, j, k);
+  mT<T>(a.v)[c] = corr_v(p, cT<T>(a.dvdt), a.p, cT<T>(a.py), i, j, k);
+  mT<T>(a.w)[c] = corr_w(p, cT<T>(a.dwdt), a.p, cT<T>(a.pz), i, j, k);
 }
 
 // correc + bounduvw(unew,vnew,wnew) + average_vel_at_center + NaN probe
@@ -147,26 +147,26 @@ __global__ void __launch_bounds__(NT) k_correc_fused(Params p, CorrArgs a) {
   const T *du = cT<T>(a.dudt), *dv = cT<T>(a.dvdt), *dw = cT<T>(a.dwdt);
   T uu, vv, ww;
   if (k >= 1 && k <= p.kmax) {
-    uu = corr_u(p, du, a.p, a.px, I, J, k);
-    vv = corr_v(p, dv, a.p, a.py, I, J, k);
-    ww = (k == p.kmax) ? TC(0.) : corr_w(p, dw, a.p, a.pz, I, J, k);
+    uu = corr_u(p, du, a.p, cT<T>(a.px), I, J, k);
+    vv = corr_v(p, dv, a.p, cT<T>(a.py), I, J, k);
+    ww = (k == p.kmax) ? TC(0.) : corr_w(p, dw, a.p, cT<T>(a.pz), I, J, k);
   } else if (k == 0) {
-    uu = -corr_u(p, du, a.p, a.px, I, J, 1);
-    vv = TC(2. * p.v_lower) - corr_v(p, dv, a.p, a.py, I, J, 1);
+    uu = -corr_u(p, du, a.p, cT<T>(a.px), I, J, 1);
+    vv = TC(2. * p.v_lower) - corr_v(p, dv, a.p, cT<T>(a.py), I, J, 1);
     ww = TC(0.);
   } else {
-    uu = -corr_u(p, du, a.p, a.px, I, J, p.kmax);
-    vv = TC(2. * p.v_upper) - corr_v(p, dv, a.p, a.py, I, J, p.kmax);
-    ww = corr_w(p, dw, a.p, a.pz, I, J, p.kmax - 1);
+    uu = -corr_u(p, du, a.p, cT<T>(a.px), I, J, p.kmax);
+    vv = TC(2. * p.v_upper) - corr_v(p, dv, a.p, cT<T>(a.py), I, J, p.kmax);
+    ww = corr_w(p, dw, a.p, cT<T>(a.pz), I, J, p.kmax - 1);
   }
   mT<T>(a.u)[n] = uu;
   mT<T>(a.v)[n] = vv;
   mT<T>(a.w)[n] = ww;
   if (i == I && j == J && k >= 1 && k <= p.kmax) {
     const long long q = idxI(p, i, j, k);
-    const T um = corr_u(p, du, a.p, a.px, wrapx(p, i - 1), j, k);
-    const T vm = corr_v(p, dv, a.p, a.py, i, wrapy(p, j - 1), k);
-    const T wm = (k == 1) ? TC(0.) : corr_w(p, dw, a.p, a.pz, i, j, k - 1);
+    const T um = corr_u(p, du, a.p, cT<T>(a.px), wrapx(p, i - 1), j, k);
+    const T vm = corr_v(p, dv, a.p, cT<T>(a.py), i, wrapy(p, j - 1), k);
+    const T wm = (k == 1) ? TC(0.) : corr_w(p, dw, a.p, cT<T>(a.pz), i, j, k - 1);
     mT<T>(a.ucc)[q] = (um + uu) / TC(2.);
     mT<T>(a.vcc)[q] = (vm + vv) / TC(2.);
     mT<T>(a.wcc)[q] = (wm + ww) / TC(2.);
@@ -201,7 +201,8 @@ __global__ void __launch_bounds__(NT) k_bounduvw(Params p, T* __restrict__ u, T*
 }
 
 // boundp (bound.f90:182-287, BC_in_y='Periodic')
-__global__ void __launch_bounds__(NT) k_boundp(Params p, double* __restrict__ a) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_boundp(Params p, T* __restrict__ a) {
   int i, j, k;
   if (!cell3(kC0, cC1(p).v, i, j, k)) return;
   const long long n = idxC(p, i, j, k);
@@ -243,10 +244,11 @@ __global__ void __launch_bounds__(NT) k_ywalls_uvw(Params p, T* __restrict__ u, 
 }
 // the y boundaries of boundp (bound.f90:207-282): zero Neumann, or zero
 // Dirichlet at an outflow end
-__global__ void __launch_bounds__(NT) k_ywalls_p(Params p, double* __restrict__ a) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_ywalls_p(Params p, T* __restrict__ a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y + 1;
   if (i > p.imax) return;
-  const double f = a[idxC(p, i, 1, k)], b = a[idxC(p, i, p.jmax, k)];
+  const T f = a[idxC(p, i, 1, k)], b = a[idxC(p, i, p.jmax, k)];
   a[idxC(p, i, 0, k)] = p.bcy == ICLS_BCY_OUTOUT ? -f : f;
   a[idxC(p, i, p.j1, k)] = p.bcy == ICLS_BCY_WALLS ? b : -b;
 }
@@ -299,20 +301,22 @@ __global__ void __launch_bounds__(kNormThreads) k_plane_norm(Params p, const dou
     dsc->norm = s / (1. * (p.imax) * p.jmax);
   }
 }
+// pnew and pold in the form's field type T (the arithmetic in FP64)
+template <typename T>
 __global__ void __launch_bounds__(NT) k_pupdate(Params p, const double* __restrict__ pp,
-                                                double* __restrict__ pnew, double* __restrict__ pold, int first,
+                                                T* __restrict__ pnew, T* __restrict__ pold, int first,
                                                 int normalise, const DevScalars* __restrict__ dsc) {
   const long long n = blockIdx.x * (long long)NT + threadIdx.x;
   if (n >= p.nC) return;
   if (!normalise) {
     pold[n] = pnew[n];
-    pnew[n] = pp[n];
+    pnew[n] = TC(pp[n]);
     return;
   }
   const double norm = dsc->norm;
-  const double po = pnew[n];
-  pold[n] = first ? po - norm : (po + dsc->norm_old) - norm;
-  pnew[n] = pp[n] - norm;
+  const double po = (double)pnew[n];
+  pold[n] = TC(first ? po - norm : (po + dsc->norm_old) - norm);
+  pnew[n] = TC(pp[n] - norm);
 }
 
 // ---- reductions ------------------------------------------------------------
@@ -501,12 +505,17 @@ void launch_bounduvw(Ctx& c, double* u, double* v, double* w) {
   else k_bounduvw<double><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, u, v, w);
   launch_ywalls_uvw(c, u, v, w);
 }
-void launch_boundp(Ctx& c, double* pp) {
+inline dim3 grid_ik(const Params& p) { return dim3((unsigned)((p.imax + NT - 1) / NT), (unsigned)p.kmax, 1); }
+void launch_boundp(Ctx& c, double* pp, bool tfield) {
   Scope sc_(c.prof, c.s, "boundp", 1);
-  k_boundp<<<gridC(c.P), kBlock, 0, c.s>>>(c.P, pp);
+  if (tfield && c.P.f32) {
+    k_boundp<float><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, fp<float>(pp));
+    if (c.P.bcy != ICLS_BCY_PERIODIC) k_ywalls_p<float><<<grid_ik(c.P), NT, 0, c.s>>>(c.P, fp<float>(pp));
+    return;
+  }
+  k_boundp<double><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, pp);
   launch_ywalls_p(c, pp);
 }
-inline dim3 grid_ik(const Params& p) { return dim3((unsigned)((p.imax + NT - 1) / NT), (unsigned)p.kmax, 1); }
 void launch_ywalls_uvw(Ctx& c, double* u, double* v, double* w) {
   if (c.P.bcy == ICLS_BCY_PERIODIC) return;
   if (c.P.f32)
@@ -516,7 +525,7 @@ void launch_ywalls_uvw(Ctx& c, double* u, double* v, double* w) {
 }
 void launch_ywalls_p(Ctx& c, double* pp) {
   if (c.P.bcy == ICLS_BCY_PERIODIC) return;
-  k_ywalls_p<<<grid_ik(c.P), NT, 0, c.s>>>(c.P, pp);
+  k_ywalls_p<double><<<grid_ik(c.P), NT, 0, c.s>>>(c.P, pp);
 }
 void launch_gather_plane_x(Ctx& c, const double* d, bool f32, long long nx, long long ny, long long ioff, int n1,
                            int n2, double* dst) {
@@ -542,7 +551,11 @@ void launch_pressure_update(Ctx& c, int first) {
   // (main.f90:169-185); otherwise pold = pnew, pnew = p
   const int norm = c.P.bcy == ICLS_BCY_PERIODIC || c.P.bcy == ICLS_BCY_WALLS;
   if (norm) k_plane_norm<<<1, kNormThreads, 0, c.s>>>(c.P, c.p, c.dsc);
-  k_pupdate<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, c.pnew, c.pold, first, norm, c.dsc);
+  if (c.P.f32)
+    k_pupdate<float><<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, fp<float>(c.pnew), fp<float>(c.pold), first, norm,
+                                                       c.dsc);
+  else
+    k_pupdate<double><<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, c.pnew, c.pold, first, norm, c.dsc);
 }
 void launch_stream_vel(Ctx& c) {
   Scope sc_(c.prof, c.s, "stream_vel", 2);

@@ -427,8 +427,13 @@ def test_tma_predictor_bit_identical_to_ring(monkeypatch):
     """The TMA-fed FP64 predictor (persistent CTAs, mbarrier rings) computes
     the same expressions as the cp.async-ring kernel: every field after
     several steps is bit-identical, on a grid whose x tiles are partial
-    (48 = 32 + 16) and on the 128^3 multi-drop box."""
-    for wl in (static_drop(48, steps=4), boxed_case(steps=4)):
+    (48 = 32 + 16), on a slab thinner than one 16-row y tile (32 x 8 x 32)
+    and on the 128^3 multi-drop box."""
+    from icls_gpu.config import Workload
+    slab_cfg = make_config(itot=32, jtot=8, ktot=32, lmax=1, ly=0.25, timestep=2e-4, rho2=10.0, miu2=10.0,
+                           Re=100.0, We=0.5)
+    slab = Workload("slab_32x8x32", slab_cfg, [(0.5, 0.125, 0.5)], [0.1], True, 0.0, 4)
+    for wl in (static_drop(48, steps=4), slab, boxed_case(steps=4)):
         cfg = wl.cfg
         ls = init_drops(cfg, wl.centres, wl.radii, wl.all_images)
         u, v, w = smooth_velocity(cfg, amp=0.3, seed=12)

@@ -249,7 +249,7 @@ def test_combined_form_96(trained_net):
     vf, vf0 = sf.volumes()
     ev, fb = curvature_stats(sf)
     du = float(np.linalg.norm(sf.download("u") - sp.download("u")) / np.linalg.norm(sp.download("u")))
-    print("\\ncombined 96^3 x 12, 10 steps: volume vs FP64 %.2e, drift FP64 %.2e form %.2e, u rel L2 %.2e, "
+    print("\ncombined 96^3 x 12, 10 steps: volume vs FP64 %.2e, drift FP64 %.2e form %.2e, u rel L2 %.2e, "
           "max|u| FP64 %.3e form %.3e, fallback %.3f"
           % (np.max(np.abs(vf - vp) / vp), np.max(np.abs(vp - vp0) / vp0), np.max(np.abs(vf - vf0) / vf0), du,
              sp.max_vel_at_center(), sf.max_vel_at_center(), fb / max(ev, 1)))

@@ -1,8 +1,10 @@
 """The precision form (ICLS_FP32) against the plain FP64 path (needs a B200).
 
 The form stores and computes advection, reinitialisation, momentum,
-correction and curvature in FP32 and keeps FP64 for the Poisson solve, the
-volume integral and the GFM jump assembly.  Its errors against the FP64 run
+correction and curvature in FP32, stores the pressures and face jumps that
+those stencils read in FP32, and keeps FP64 for the Poisson solve (its
+right-hand side and work array), the volume integral and the GFM jump
+assembly.  Its errors against the FP64 run
 of the same input are reported (printed, run with -s) and bounded here:
 
   phi      relative L2 <= 1e-5 on the band |phi| <= 4dz around the
@@ -77,8 +79,10 @@ def test_field_round_trip_fp32():
     s.upload("u", a)
     b = s.download("u")
     assert np.array_equal(b, a.astype(np.float32).astype(np.float64))
-    s.upload("pnew", a)  # an FP64 field in both forms
-    assert np.array_equal(s.download("pnew"), a)
+    s.upload("pnew", a)  # the pressures are stored in the field type too
+    assert np.array_equal(s.download("pnew"), a.astype(np.float32).astype(np.float64))
+    s.upload("p", a)  # the Poisson work array stays FP64 in both forms
+    assert np.array_equal(s.download("p"), a)
 
 
 def test_static_drop_fp32_vs_fp64():
