@@ -83,7 +83,7 @@ struct Ctx {
   const void* ab2_keys[4][18] = {};
   int ab2_nmaps = 0, ab2_next = 0;
   bool ab2_tma_failed = false;  // a map could not be encoded: use the ring
-  bool ab2_ring = false;  // FP64 predictor on the cp.async ring (ICLS_AB2=ring)
+  bool ab2_ring = true;  // FP64 predictor on the cp.async ring (else TMA: ICLS_AB2=tma)
   icls_config cfg;
   Params P;
   cudaStream_t s = nullptr;

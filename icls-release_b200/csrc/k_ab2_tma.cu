@@ -2,6 +2,12 @@
 // mom_main's RHS, mom.f90:13-301, and the wall rows of bounduvw(dudt,..),
 // bound.f90:36-75) fed by the Tensor Memory Accelerator.
 //
+// Opt-in (ICLS_AB2=tma): at 256^3 it measured 1.68 ms against the
+// cp.async-ring kernel's 1.37 ms, so the ring stays the default; 16 compute
+// warps per SM (the most the 128-register budget of the FP64 stencil
+// arithmetic allows with one CTA) hide less latency than the ring's two
+// CTAs, each of which overlaps the other's waits.
+//
 // The arithmetic per cell is the one of k_ab2 in ab2.cuh (the same rhs_u/v/w
 // and ab2_update_v templates, compiled with -fmad=false), so the result is
 // bit-identical to it.  What changes is how the 18 input fields reach the

@@ -466,7 +466,7 @@ void launch_ab2(Ctx& c) {
   MomArgs a = mom_args(c);
   const int o = c.hist ^ 1;
   if (c.P.f32) ab2_launch_f32(c, a, o);     // k_ab2_f32.cu
-  else if (!ab2_tma_launch(c, a, o)) ab2_launch<double>(c, a, o);  // k_ab2_tma.cu, else the cp.async ring
+  else if (!ab2_tma_launch(c, a, o)) ab2_launch<double>(c, a, o);  // k_ab2_tma.cu when chosen, else the ring
   launch_ywalls_uvw(c, c.dudt, c.dvdt, c.dwdt);  // the y walls of bounduvw(dudt,dvdt,dwdt)
   c.hist = o;
 }

@@ -1187,8 +1187,12 @@ struct ora_ctx {
     for (int l = 0; l < L; ++l) {
       tube_construction(l);
       ls_advection(l);
+      // with the gain-one correction (no counterpart in the reference) the
+      // correction follows the reinitialisation, so it also removes the
+      // reinitialisation's volume change in the same step
+      if (c.mass_gain_one && c.re_initialization) ls_reinit_main(istep, l);
       if (c.mass_correction) ls_mass_correction(istep, l);
-      if (c.re_initialization) ls_reinit_main(istep, l);
+      if (!c.mass_gain_one && c.re_initialization) ls_reinit_main(istep, l);
     }
     update_materials();
   }

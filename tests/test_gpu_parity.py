@@ -437,10 +437,10 @@ def test_tma_predictor_bit_identical_to_ring(monkeypatch):
         cfg = wl.cfg
         ls = init_drops(cfg, wl.centres, wl.radii, wl.all_images)
         u, v, w = smooth_velocity(cfg, amp=0.3, seed=12)
-        monkeypatch.setenv("ICLS_AB2", "ring")
         ring = Solver(cfg)
-        monkeypatch.delenv("ICLS_AB2")
+        monkeypatch.setenv("ICLS_AB2", "tma")
         tma = Solver(cfg)
+        monkeypatch.delenv("ICLS_AB2")
         for s in (ring, tma):
             s.setup(ls, u, v, w)
         for istep in range(1, 5):
