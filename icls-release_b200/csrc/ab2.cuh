@@ -169,6 +169,16 @@ __device__ __forceinline__ void cp_async_el(T* dst, const T* src) {
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
 }
+// two consecutive elements (8 bytes in FP32, 16 in FP64); both addresses
+// aligned to the pair's size
+template <typename T>
+__device__ __forceinline__ void cp_async_pair(T* dst, const T* src) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  if (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // ab2 over shape C with bounduvw(dudt,dvdt,dwdt) (bound.f90:36-75) in-kernel.
@@ -180,11 +190,13 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // memory latency is exposed per row and the ring needs one barrier per row
 // (the slot a row's copies fill is not one any thread can still be reading).
 // A thread writes its column's periodic halo images and, at k = 1 and
-// k = kmax, the wall rows k = 0 and k = k1.
-constexpr int MX = 32, MY = 8, MSX = MX + 2, MSY = MY + 2, MPX = MX + 1, MPY = MY + 1, MRING = 4;
+// k = kmax, the wall rows k = 0 and k = k1.  Every plane row starts at
+// column i0 - 1 (even), and the copies move two columns at a time (16 bytes
+// in FP64, 8 in FP32).
+constexpr int MX = 32, MY = 8, MSX = MX + 2, MSY = MY + 2, MPY = MY + 1, MRING = 4;
 template <typename T>
 constexpr int ab2_smem() {
-  return (int)(4 * MRING * MSY * MSX * sizeof(T) + 2 * MRING * MPY * MPX * sizeof(T));
+  return (int)(4 * MRING * MSY * MSX * sizeof(T) + 2 * MRING * MPY * MSX * sizeof(T));
 }
 template <typename T>
 __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
@@ -192,7 +204,7 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
           T* __restrict__ duold_out, T* __restrict__ dvold_out, T* __restrict__ dwold_out, int kc, int nch) {
   extern __shared__ __align__(16) unsigned char ab2_dyn[];
   typedef T Plane[MSY][MSX];
-  typedef T PPlane[MPY][MPX];  // pnew, pold in the form's field type
+  typedef T PPlane[MPY][MSX];  // pnew, pold (columns i0-1.., rows j0..) in the form's field type
   Plane* ring = reinterpret_cast<Plane*>(ab2_dyn);  // [field * MRING + slot]
   PPlane* pring = reinterpret_cast<PPlane*>(ab2_dyn + 4 * MRING * sizeof(Plane));
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + MX * ty;
@@ -208,24 +220,28 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
   const T* __restrict__ hu = cT<T>(a.duold);
   const T* __restrict__ hv = cT<T>(a.dvold);
   const T* __restrict__ hw = cT<T>(a.dwold);
+  // imax is even (every FFT length validate() admits is), so the rows of
+  // shape C have an even length and each plane row's first element (column
+  // i0-1, even) sits at an even index: the pair copies are aligned
   auto issue_plane = [&](int kk) {
     const int s = kk & (MRING - 1);
-    for (int e = tid; e < MSX * MSY; e += MX * MY) {
-      const int sy = e / MSX, sx = e - sy * MSX;
+    constexpr int NP = MSX / 2;
+    for (int e = tid; e < NP * MSY; e += MX * MY) {
+      const int sy = e / NP, sx = 2 * (e - sy * NP);
       const int gi = i0 - 1 + sx, gj = j0 - 1 + sy;
-      if (gi <= p.imax + 1 && gj <= p.jmax + 1) {
+      if (gi <= p.imax && gj <= p.jmax + 1) {  // gi even: gi + 1 <= imax + 1
         const long long g = idxC(p, gi, gj, kk);
 #pragma unroll
-        for (int f = 0; f < 4; ++f) cp_async_el(&ring[f * MRING + s][sy][sx], F[f] + g);
+        for (int f = 0; f < 4; ++f) cp_async_pair(&ring[f * MRING + s][sy][sx], F[f] + g);
       }
     }
-    for (int e = tid; e < MPX * MPY; e += MX * MY) {
-      const int sy = e / MPX, sx = e - sy * MPX;
-      const int gi = i0 + sx, gj = j0 + sy;
-      if (gi <= p.imax + 1 && gj <= p.jmax + 1) {
+    for (int e = tid; e < NP * MPY; e += MX * MY) {
+      const int sy = e / NP, sx = 2 * (e - sy * NP);
+      const int gi = i0 - 1 + sx, gj = j0 + sy;
+      if (gi <= p.imax && gj <= p.jmax + 1) {
         const long long g = idxC(p, gi, gj, kk);
-        cp_async_el(&pring[s][sy][sx], cT<T>(a.pnew) + g);
-        cp_async_el(&pring[MRING + s][sy][sx], cT<T>(a.pold) + g);
+        cp_async_pair(&pring[s][sy][sx], cT<T>(a.pnew) + g);
+        cp_async_pair(&pring[MRING + s][sy][sx], cT<T>(a.pold) + g);
       }
     }
   };
@@ -256,7 +272,7 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
       auto W = [&](int di, int dj, int dk) { return ring[2 * MRING + sl(dk)][ty + 1 + dj][tx + 1 + di]; };
       auto M = [&](int di, int dj, int dk) { return ring[3 * MRING + sl(dk)][ty + 1 + dj][tx + 1 + di]; };
       auto PH = [&](int di, int dj, int dk) {
-        return 2. * (double)pring[sl(dk)][ty + dj][tx + di] - (double)pring[MRING + sl(dk)][ty + dj][tx + di];
+        return 2. * (double)pring[sl(dk)][ty + dj][tx + 1 + di] - (double)pring[MRING + sl(dk)][ty + dj][tx + 1 + di];
       };
       const double ph0 = PH(0, 0, 0);
       const T Ru = rhs_u<T>(p, U, V, W, M, ru, rho_avr);

@@ -96,6 +96,7 @@ int validate(const icls_config* c) {
   if (c->bc_y != ICLS_BCY_PERIODIC && c->ktot > kCosqMaxN) return ICLS_E_CONFIG;  // z cosine lines
   if (c->itot > 4096 || c->jtot > 4096) return ICLS_E_CONFIG;
   if (c->itot < 8 || c->jtot < 8) return ICLS_E_CONFIG;  // periodic images of 3 halo layers
+  if (c->itot % 2) return ICLS_E_CONFIG;  // (implied by the FFT lengths) the predictor copies column pairs
   if (c->ktot < 6 || c->lmax < 1) return ICLS_E_CONFIG;
   // grid-stride loops index cells with 32-bit integers: keep the largest
   // array (a level set with its 3 halo layers per side) below 2^30 elements
@@ -220,12 +221,14 @@ int allocate(Ctx& c) {
   AL(c.lpartials, (size_t)kRedBlocks);
   AL(c.dsc, 1);
   AL(c.dvol, (size_t)P.L); AL(c.dvol0, (size_t)P.L); AL(c.dmaxchk, (size_t)P.L);
+  AL(c.dvolnow, (size_t)P.L);
   AL(c.drs, (size_t)P.L);
   c.red_cap = ((P.imax + TBX - 1) / TBX) * ((P.jmax + TBY - 1) / TBY);
   // per-tile exact sums of H (4 words each) for every drop; the inflation
   // uses red_cap area sums and red_cap exact sums
   AL(c.hpart, (size_t)std::max(4 * P.L, 5) * c.red_cap);
   CK(cudaMallocHost((void**)&c.h_vol, sizeof(double) * P.L));
+  CK(cudaMallocHost((void**)&c.h_volnow, sizeof(double) * P.L));
   CK(cudaMallocHost((void**)&c.h_sc, sizeof(DevScalars)));
   CK(cudaEventCreateWithFlags(&c.ev_vol, cudaEventDisableTiming));
   // normal%m = 1 outside the curvature band (interface.f90:44)
@@ -276,7 +279,7 @@ void release(Ctx& c) {
   for (double* f : {c.u, c.v, c.w, c.pnew, c.pold, c.p, c.dudt, c.dvdt, c.dwdt, c.px, c.py, c.pz, c.pxold,
                     c.pyold, c.pzold, c.pjump, c.miu, c.rho, c.jiemian, c.curv, c.dheav, c.kappa,
                     c.rho_u, c.rho_v, c.rho_w, c.ucc, c.vcc, c.wcc, c.nrm_m, c.ulc, c.vlc, c.wlc, c.spec,
-                    c.xyrt, c.zpiv, c.tri_a, c.tri_b, c.tri_c, c.partials, c.diag, c.dvol, c.dvol0, c.dmaxchk,
+                    c.xyrt, c.zpiv, c.tri_a, c.tri_b, c.tri_c, c.partials, c.diag, c.dvol, c.dvol0, c.dmaxchk, c.dvolnow,
                     c.hpart, c.cosb, c.cosf, c.vin})
     if (f) cudaFree(f);
   for (int h = 0; h < 2; ++h) {
@@ -300,6 +303,7 @@ void release(Ctx& c) {
     if (f) cudaFree(f);
   if (c.dsc) cudaFree(c.dsc);
   if (c.h_vol) cudaFreeHost(c.h_vol);
+  if (c.h_volnow) cudaFreeHost(c.h_volnow);
   if (c.h_sc) cudaFreeHost(c.h_sc);
   if (c.ev_vol) cudaEventDestroy(c.ev_vol);
   if (c.d_bbox) cudaFree(c.d_bbox);
@@ -668,12 +672,31 @@ int volume_of(Ctx& c, int l, double* v) {
   return ICLS_OK;
 }
 
-// ls_mass_correction (levelset.f90:377-400)
+// each of the drops' volumes as they are now (the exact sum of H over the
+// drop's box plus its far-field count), into h_volnow: one read-back
+int measure_volumes_now(Ctx& c, const std::vector<int>& drops) {
+  for (int l : drops) {
+    const Region b = c.win[l].box;
+    std::vector<LsBatch> bv = single(c, l, 0, c_region(c.P, b, 1));
+    bv[0].t[0].phi0 = c.lv[l];
+    launch_volume_now(c, bv[0], outside_count(c, b));
+  }
+  CK(cudaMemcpyAsync(c.h_volnow, c.dvolnow, sizeof(double) * c.P.L, cudaMemcpyDeviceToHost, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  return ICLS_OK;
+}
+
+// ls_mass_correction (levelset.f90:377-400).  The reference tests the
+// volume of the last update_materials; the gain-one correction tests the
+// drop's volume as it is now (after this step's advection and
+// reinitialisation, measured by measure_volumes_now into h_volnow)
 int ls_mass_correction(Ctx& c, int istep, int l) {
   c.inflated[l] = 0;
   if (istep % c.cfg.inflate_step == 0) {
     double vol;
-    int rc = volume_of(c, l, &vol);
+    int rc = ICLS_OK;
+    if (c.cfg.mass_gain_one) vol = c.h_volnow[l];
+    else rc = volume_of(c, l, &vol);
     if (rc) return rc;
     const double v0 = c.init_volume_h[l];
     const double massloss = (vol - v0) / v0;
@@ -867,6 +890,10 @@ int ls_main(Ctx& c, int istep) {
     // removes the volume change of the reinitialisation in the same step
     const bool correct_last = c.cfg.mass_gain_one != 0;
     if (reinit_now && correct_last) reinit_batches(c, bs);
+    if (c.cfg.mass_correction && correct_last && istep % c.cfg.inflate_step == 0) {
+      rc = measure_volumes_now(c, drops);
+      if (rc) return rc;
+    }
     if (c.cfg.mass_correction)
       for (int l : drops) {
         rc = ls_mass_correction(c, istep, l);

@@ -133,6 +133,8 @@ struct Ctx {
   DevScalars* dsc = nullptr;
   double* dvol = nullptr;               // volume(1:L)
   double* dvol0 = nullptr;              // init_volume(1:L)
+  double* dvolnow = nullptr;            // gain-one trigger: each drop's volume after its reinitialisation
+  double* h_volnow = nullptr;           // pinned host copy
   double* dmaxchk = nullptr;            // per drop maxchk of the last inflation
   ReinitState* drs = nullptr;           // per drop
   double* stage = nullptr;              // precision form: FP64 staging of one field (upload/download)
@@ -199,6 +201,7 @@ void launch_inflate_vel(Ctx& c, const LsBatch& b);
 void launch_region_copy(Ctx& c, const LsBatch& b);
 void launch_gain(Ctx& c, const LsBatch& b, double outside);
 void launch_region_blend(Ctx& c, const LsBatch& b);
+void launch_volume_now(Ctx& c, const LsBatch& b, double outside);
 void launch_copy(Ctx& c, double* dst, const double* src, long long n);
 void launch_boundmls(Ctx& c, double* phi);
 void launch_materialize(Ctx& c, const Region& r, double bg, double bgg, double* phi);

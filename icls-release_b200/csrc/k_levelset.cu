@@ -910,6 +910,17 @@ __global__ void k_gain_final(Params p, const XSum* __restrict__ part, int nblk, 
   dsc->inflate_gain = d != 0. ? (vol0[l] - vol[l]) / d : 0.;
 }
 
+// the volume of drop l now, from the tiles and the far-field count
+__global__ void k_volume_now(Params p, const XSum* __restrict__ part, int nblk, int l, double outside,
+                             double* __restrict__ vnow) {
+  if (threadIdx.x != 0) return;
+  XSum hs;
+  xs_zero(hs);
+  for (int b = 0; b < nblk; ++b) xs_merge(hs, part[b]);
+  xs_add_count(hs, (long long)outside);
+  vnow[l] = 1. - xs_value(hs) / ((1. * p.imax * p.jmax) * p.kmax);
+}
+
 // t.out (phi1, in place) = phi0 + g (phi1 - phi0) on the written cells
 template <typename T>
 __global__ void __launch_bounds__(NT) k_region_blend(Params p, const __grid_constant__ LsBatch B,
@@ -1294,6 +1305,13 @@ void launch_gain(Ctx& c, const LsBatch& b, double outside) {
   BY_FORM(c, (k_region_heav<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, ph)),
           (k_region_heav<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, ph)));
   k_gain_final<<<1, 32, 0, c.s>>>(c.P, ph, b.start[b.n], b.t[0].l, outside, c.dvol, c.dvol0, c.dsc);
+}
+void launch_volume_now(Ctx& c, const LsBatch& b, double outside) {
+  Scope sc_(c.prof, c.s, "gain_one", 2);
+  XSum* ph = reinterpret_cast<XSum*>(c.hpart + c.red_cap);
+  BY_FORM(c, (k_region_heav<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, ph)),
+          (k_region_heav<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, ph)));
+  k_volume_now<<<1, 32, 0, c.s>>>(c.P, ph, b.start[b.n], b.t[0].l, outside, c.dvolnow);
 }
 void launch_region_blend(Ctx& c, const LsBatch& b) {
   Scope sc_(c.prof, c.s, "gain_one", 1);

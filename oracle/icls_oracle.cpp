@@ -1131,7 +1131,16 @@ struct ora_ctx {
   void ls_mass_correction(int istep, int l) {
     maxchk_glb = 0.;
     if (istep % c.inflate_step == 0) {
-      double massloss = (volume[l] - init_volume[l]) / init_volume[l];
+      // the gain-one correction tests the drop's volume as it is now (after
+      // this step's advection and reinitialisation); the reference, the
+      // volume of the last update_materials
+      double v = volume[l];
+      if (c.mass_gain_one) {
+        F3 h; shapeC(h);
+        heaviside_c(l, 1.5 * dz, h);
+        v = 1. - exact_sum_interior(h) / ((1. * itot * jtot) * ktot);
+      }
+      double massloss = (v - init_volume[l]) / init_volume[l];
       const double eps = c.mass_threshold > 0. ? c.mass_threshold : 1e-5;
       if (std::fabs(massloss) > eps) { inflation(l); ++last_inflated; }
     }
