@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(NT, 3) k_curvature(Params p, const __grid_cons
 // re_curvature + boundc (interface.f90:186-218) over the tasks' regions:
 // phis (get_curvature) -> out
 template <typename T>
-__global__ void __launch_bounds__(NT, 3) k_recurvature(Params p, const __grid_constant__ LsBatch B) {
+__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 4 : 3)) k_recurvature(Params p, const __grid_constant__ LsBatch B) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const T* __restrict__ cin = cT<T>(t.phis);
