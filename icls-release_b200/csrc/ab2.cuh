@@ -7,6 +7,8 @@
 // own anonymous namespace.
 #pragma once
 
+#include <type_traits>
+
 #include "batch.cuh"
 
 namespace icls {
@@ -151,12 +153,15 @@ __device__ __forceinline__ T rhs_w(const Params& p, const FU& U, const FV& V, co
 // term is formed in FP64 (the pressures are FP64 fields) from: ph_p / ph_0 the
 // extrapolated pressures 2 pnew - pold at the + neighbour and the cell,
 // pjh the extrapolated pressure gradient 2 p_x - p_x,old
-template <typename T>
-__device__ __forceinline__ T ab2_update_v(const Params& p, T u0, T R, T rold, T rf, double ph_p, double ph_0,
-                                          double pjh, double dhi) {
+// PT is the pressure term's arithmetic: FP64 in the plain path; in the FP32
+// form, whose pressures are stored in FP32, the term is formed in FP32 too
+// (it is part of the momentum predictor, which that form computes in FP32)
+template <typename T, typename PT>
+__device__ __forceinline__ T ab2_update_v(const Params& p, T u0, T R, T rold, T rf, PT ph_p, PT ph_0, PT pjh,
+                                          double dhi) {
   T d = u0 + TC(p.dt) * (TC(1.5) * R - TC(0.5) * rold);
-  const double dn = -((1. / (double)rf - p.rrho0) * dhi * ((ph_p - pjh) - ph_0));
-  return d + TC(p.dt * dn);
+  const PT dn = -((PT(1.) / (PT)rf - (PT)p.rrho0) * (PT)dhi * ((ph_p - pjh) - ph_0));
+  return d + TC((PT)p.dt * dn);
 }
 
 // element copies global -> shared that complete asynchronously (waited for
@@ -275,14 +280,15 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
   for (int k = ka; k <= kb; ++k) {
     // this cell's own operands, in flight together with row k+1's planes
     T ru = TC(1.), rv = TC(1.), rw = TC(1.), ou = TC(0.), ov = TC(0.), ow = TC(0.);
-    double qx = 0., qxo = 0., qy = 0., qyo = 0., qz = 0., qzo = 0.;
+    typedef typename std::conditional<sizeof(T) == 8, double, float>::type PT;
+    PT qx = 0., qxo = 0., qy = 0., qyo = 0., qz = 0., qzo = 0.;
     const long long c = idxC(p, i, j, k), q = idxI(p, i, j, k);
     if (ok) {
       ru = rhu[q]; rv = rhv[q]; rw = rhw[q];
       ou = hu[q]; ov = hv[q]; ow = hw[q];
-      qx = (double)cT<T>(a.px)[c]; qxo = (double)cT<T>(a.pxold)[c];
-      qy = (double)cT<T>(a.py)[c]; qyo = (double)cT<T>(a.pyold)[c];
-      qz = (double)cT<T>(a.pz)[c]; qzo = (double)cT<T>(a.pzold)[c];
+      qx = (PT)cT<T>(a.px)[c]; qxo = (PT)cT<T>(a.pxold)[c];
+      qy = (PT)cT<T>(a.py)[c]; qyo = (PT)cT<T>(a.pyold)[c];
+      qz = (PT)cT<T>(a.pz)[c]; qzo = (PT)cT<T>(a.pzold)[c];
     }
     issue_plane(k + 1);
     cp_async_wait_all();
@@ -295,16 +301,16 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
       auto W = [&](int di, int dj, int dk) { return ring[2 * MRING + sl(dk)][ty + 1 + dj][tx + 1 + di]; };
       auto M = [&](int di, int dj, int dk) { return ring[3 * MRING + sl(dk)][ty + 1 + dj][tx + 1 + di]; };
       auto PH = [&](int di, int dj, int dk) {
-        return 2. * (double)pring[sl(dk)][ty + dj][tx + 1 + di] - (double)pring[MRING + sl(dk)][ty + dj][tx + 1 + di];
+        return PT(2.) * (PT)pring[sl(dk)][ty + dj][tx + 1 + di] - (PT)pring[MRING + sl(dk)][ty + dj][tx + 1 + di];
       };
-      const double ph0 = PH(0, 0, 0);
+      const PT ph0 = PH(0, 0, 0);
       const T Ru = rhs_u<T>(p, U, V, W, M, ru, rho_avr);
       const T Rv = rhs_v<T>(p, U, V, W, M, rv, rho_avr);
       const T Rw = rhs_w<T>(p, U, V, W, M, rw, rho_avr);
-      const T du = ab2_update_v(p, U(0, 0, 0), Ru, ou, ru, PH(1, 0, 0), ph0, 2. * qx - qxo, p.dxi);
-      T dv = ab2_update_v(p, V(0, 0, 0), Rv, ov, rv, PH(0, 1, 0), ph0, 2. * qy - qyo, p.dyi);
+      const T du = ab2_update_v<T, PT>(p, U(0, 0, 0), Ru, ou, ru, PH(1, 0, 0), ph0, PT(2.) * qx - qxo, p.dxi);
+      T dv = ab2_update_v<T, PT>(p, V(0, 0, 0), Rv, ov, rv, PH(0, 1, 0), ph0, PT(2.) * qy - qyo, p.dyi);
       if (p.forceytot != 0.) dv = dv - TC(p.forceytot * p.dt) / rv;  // constPoi driving (exact zero otherwise)
-      T dw = ab2_update_v(p, W(0, 0, 0), Rw, ow, rw, PH(0, 0, 1), ph0, 2. * qz - qzo, p.dzi);
+      T dw = ab2_update_v<T, PT>(p, W(0, 0, 0), Rw, ow, rw, PH(0, 0, 1), ph0, PT(2.) * qz - qzo, p.dzi);
       duold_out[q] = Ru;
       dvold_out[q] = Rv;
       dwold_out[q] = Rw;
