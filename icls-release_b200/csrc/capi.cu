@@ -222,6 +222,10 @@ int allocate(Ctx& c) {
   AL(c.dsc, 1);
   AL(c.dvol, (size_t)P.L); AL(c.dvol0, (size_t)P.L); AL(c.dmaxchk, (size_t)P.L);
   AL(c.dvolnow, (size_t)P.L);
+  // band list of the advection stages: up to one entry per interior cell
+  c.band_cap = P.nI;
+  if (cudaMalloc(&c.band_list, (size_t)c.band_cap * 8) != cudaSuccess) return ICLS_E_NOMEM;
+  if (cudaMalloc((void**)&c.band_count, sizeof(int)) != cudaSuccess) return ICLS_E_NOMEM;
   AL(c.drs, (size_t)P.L);
   c.red_cap = ((P.imax + TBX - 1) / TBX) * ((P.jmax + TBY - 1) / TBY);
   // per-tile exact sums of H (4 words each) for every drop; the inflation
@@ -243,11 +247,26 @@ int allocate(Ctx& c) {
   // bookkeeping: both give bit-identical fields)
   const char* fs = std::getenv("ICLS_FULL_SWEEP");
   c.use_boxes = (P.L <= kMaxDropsParam) && !(fs && fs[0] == '1');
-  // ICLS_AB2=tma runs the FP64 predictor on the TMA-fed kernel in place of
-  // the cp.async-ring one (the same arithmetic: bit-identical fields; the
-  // ring kernel measured faster at 256^3, 1.37 vs 1.68 ms)
+  {
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && nsm > 0) c.num_sms = nsm;
+  }
+  // Alternative kernels of the same arithmetic (bit-identical fields), kept
+  // for comparison:
+  // ICLS_AB2=tma: the FP64 predictor on the TMA-fed kernel in place of the
+  // cp.async-ring one (the ring kernel measured faster at 256^3, 1.37 vs
+  // 1.68 ms);
+  // ICLS_ADV=band: the advection stages after tube_construction as the
+  // band-list split (measured no faster in FP64, slower in FP32, with the
+  // list build included);
+  // ICLS_CORREC=cell: the velocity correction one thread per cell.
   const char* ab = std::getenv("ICLS_AB2");
   c.ab2_ring = !(ab && std::strcmp(ab, "tma") == 0);
+  const char* av = std::getenv("ICLS_ADV");
+  c.adv_column = !(av && std::strcmp(av, "band") == 0);
+  const char* cv = std::getenv("ICLS_CORREC");
+  c.correc_col = !(cv && std::strcmp(cv, "cell") == 0);
   // working buffers of a group of drops: as many drops as half the free
   // HBM holds (ICLS_GROUP=n caps the group, e.g. to test the grouped path)
   {
@@ -304,6 +323,8 @@ void release(Ctx& c) {
   if (c.dsc) cudaFree(c.dsc);
   if (c.h_vol) cudaFreeHost(c.h_vol);
   if (c.h_volnow) cudaFreeHost(c.h_volnow);
+  if (c.band_list) cudaFree(c.band_list);
+  if (c.band_count) cudaFree(c.band_count);
   if (c.h_sc) cudaFreeHost(c.h_sc);
   if (c.ev_vol) cudaEventDestroy(c.ev_vol);
   if (c.d_bbox) cudaFree(c.d_bbox);
@@ -554,10 +575,32 @@ void tube_batches(Ctx& c, std::vector<LsBatch>& bs) {
 // SSP-RK3 of ls_advection / inflation (levelset.f90:235-243, 558-565) on
 // the batches' drops, with their members' buffers: from_tube, s1 -> s2 ->
 // s3 -> the drop's own array; else the drop's array -> s1 -> s2 -> itself
+// the band cells a batch's list can hold at most: its tasks' computed
+// interior cells
+long long band_bound(const Ctx& c, const LsBatch& b) {
+  long long n = 0;
+  for (int q = 0; q < b.n; ++q) {
+    const Region& r = b.t[q].r;
+    const long long z = std::max(0, std::min(r.cz1, c.P.kmax) - std::max(r.cz0, 1) + 1);
+    n += (long long)(r.cx1 - r.cx0 + 1) * (r.cy1 - r.cy0 + 1) * z;
+  }
+  return n;
+}
+
 void rk3_batches(Ctx& c, std::vector<LsBatch>& bs, int scheme, bool from_tube, const double* vu, const double* vv,
                  const double* vw) {
   const double dt = c.dt;
   for (LsBatch& b : bs) {
+    // after tube_construction the band flags are fresh: one band list serves
+    // the three stages
+    // (a list entry holds i and j in 12 bits each)
+    const bool packs = c.P.imax <= 4096 && c.P.jmax <= 4096;
+    const long long need = from_tube && !c.adv_column && packs ? band_bound(c, b) : -1;
+    const bool split = need >= 0 && need <= c.band_cap;
+    if (split) {
+      for (int q = 0; q < b.n; ++q) b.t[q].mask = member(c, b.t[q].l).mask;
+      launch_band_list(c, b);
+    }
     double g[kTasks][4], h[kTasks][4];
     for (int q = 0; q < b.n; ++q) {
       const DropWin& w = c.win[b.t[q].l];
@@ -584,7 +627,8 @@ void rk3_batches(Ctx& c, std::vector<LsBatch>& bs, int scheme, bool from_tube, c
         t.bg = g[q][st];
         t.bgg = h[q][st];
       }
-      launch_adv_stage(c, b, scheme, st == 1 ? 1 : 0, a, bb, fdt, vu, vv, vw);
+      if (split) launch_adv_split(c, b, scheme, st == 1 ? 1 : 0, a, bb, fdt, vu, vv, vw, need);
+      else launch_adv_stage(c, b, scheme, st == 1 ? 1 : 0, a, bb, fdt, vu, vv, vw);
     };
     stage(1, 1., 0., 1. * dt);
     stage(2, 3. / 4., 1. / 4., 1. / 4. * dt);

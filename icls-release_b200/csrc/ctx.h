@@ -83,6 +83,8 @@ struct Ctx {
   const void* ab2_keys[4][18] = {};
   int ab2_nmaps = 0, ab2_next = 0;
   bool ab2_tma_failed = false;  // a map could not be encoded: use the ring
+  int num_sms = 148;
+  bool correc_col = true;  // correc streamed along z (else one thread per cell: ICLS_CORREC=cell)
   bool ab2_ring = true;  // FP64 predictor on the cp.async ring (else TMA: ICLS_AB2=tma)
   icls_config cfg;
   Params P;
@@ -134,6 +136,11 @@ struct Ctx {
   double* dvol = nullptr;               // volume(1:L)
   double* dvol0 = nullptr;              // init_volume(1:L)
   double* dvolnow = nullptr;            // gain-one trigger: each drop's volume after its reinitialisation
+  // band-list advection: the band cells of a batch (8 bytes each) and their number
+  void* band_list = nullptr;
+  int* band_count = nullptr;
+  long long band_cap = 0;
+  bool adv_column = true;               // the one-kernel column stage (else the band-list split: ICLS_ADV=band)
   double* h_volnow = nullptr;           // pinned host copy
   double* dmaxchk = nullptr;            // per drop maxchk of the last inflation
   ReinitState* drs = nullptr;           // per drop
@@ -201,6 +208,9 @@ void launch_inflate_vel(Ctx& c, const LsBatch& b);
 void launch_region_copy(Ctx& c, const LsBatch& b);
 void launch_gain(Ctx& c, const LsBatch& b, double outside);
 void launch_region_blend(Ctx& c, const LsBatch& b);
+void launch_band_list(Ctx& c, const LsBatch& b);
+void launch_adv_split(Ctx& c, const LsBatch& b, int scheme, int stage1, double a, double bb, double fdt,
+                      const double* vu, const double* vv, const double* vw, long long need);
 void launch_volume_now(Ctx& c, const LsBatch& b, double outside);
 void launch_copy(Ctx& c, double* dst, const double* src, long long n);
 void launch_boundmls(Ctx& c, double* phi);

@@ -405,6 +405,123 @@ __global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 4 : 3)) k_adv_stage(Para
   }
 }
 
+// ------------------------------------------------- band-list advection
+// One RK stage of k_adv_stage split in three launches over the same tasks,
+// with the same arithmetic per cell (bit-identical):
+//   k_adv_base   every written cell its value without the transport term:
+//                the far field outside the computed part, else f0 (stage
+//                1) or a f0 + bb fs; the wall rows 0 and k1 are left
+//   k_adv_band   adds fdt * dfdt on the band cells of a compacted list
+//                (k_band_list, built once after tube_construction for all
+//                three stages): full warps, and no lane walks a clipped
+//                column only to copy it
+//   k_adv_walls  rows 0 and k1 from the finished rows next to them, under
+//                the conditions k_adv_stage writes them
+// The list holds the computed interior cells whose band flag is set, as
+// (i-1) | (j-1) << 12 | task << 24 and k.
+struct BandCell {
+  unsigned ijt;
+  int k;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(NT) k_band_list(Params p, const __grid_constant__ LsBatch B,
+                                                  BandCell* __restrict__ list, int* __restrict__ count, int cap) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  const unsigned lane = threadIdx.x & 31u;
+  const long long q0 = c.ok ? idxI(p, c.i, c.j, 1) : 0;
+  const long long szI = (long long)p.imax * p.jmax;
+  // every lane of a block walks the same rows, so the ballots line up
+  for (int k = max(c.ka, 1); k <= min(c.kb, p.kmax); ++k) {
+    const bool take = c.ok && computed(c, t.r, k) && t.mask[q0 + (k - 1) * szI];
+    const unsigned msk = __ballot_sync(0xffffffffu, take);
+    if (!msk) continue;
+    int base = 0;
+    if (lane == (unsigned)(__ffs(msk) - 1)) base = atomicAdd(count, __popc(msk));
+    base = __shfl_sync(0xffffffffu, base, __ffs(msk) - 1);
+    const int slot = base + __popc(msk & ((1u << lane) - 1u));
+    if (take && slot < cap)
+      list[slot] = BandCell{(unsigned)(c.i - 1) | ((unsigned)(c.j - 1) << 12) | ((unsigned)ti << 24), k};
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NT) k_adv_base(Params p, const __grid_constant__ LsBatch B, int stage1, double a_,
+                                                 double bb_) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  if (!c.ok) return;
+  const T a = TC(a_), bb = TC(bb_);
+  const T* __restrict__ f0c = cT<T>(t.phi0);
+  const T* __restrict__ fsc = cT<T>(t.phis);
+  T* out = mT<T>(t.out);
+  for (int k = c.ka; k <= c.kb; ++k) {
+    if (!computed(c, t.r, k)) {
+      putL(p, out, c.i, c.j, k, (k < 0 || k > p.k1) ? TC(t.bgg) : TC(t.bg));
+      continue;
+    }
+    if (k == 0 || k == p.k1) continue;  // k_adv_walls
+    const long long o = idxL(p, c.i, c.j, k);
+    const T f0 = f0c[o];
+    putL(p, out, c.i, c.j, k, stage1 ? f0 : a * f0 + bb * fsc[o]);
+  }
+}
+
+template <int SCHEME, typename T>
+__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 4 : 3))
+    k_adv_band(Params p, const __grid_constant__ LsBatch B, const BandCell* __restrict__ list,
+               const int* __restrict__ count, double fdt_, const T* __restrict__ vu, const T* __restrict__ vv,
+               const T* __restrict__ vw) {
+  const int n = (int)(blockIdx.x * NT + threadIdx.x);
+  if (n >= *count) return;
+  const BandCell bc = list[n];
+  const int i = (int)(bc.ijt & 0xFFFu) + 1, j = (int)((bc.ijt >> 12) & 0xFFFu) + 1, ti = (int)(bc.ijt >> 24);
+  const int k = bc.k;
+  const LsTask& t = B.t[ti];
+  const T fdt = TC(fdt_);
+  const long long sy = p.nLx, sz = (long long)p.nLx * p.nLy;
+  const long long o = idxL(p, i, j, k);
+  const long long q = idxI(p, i, j, k);
+  const T* __restrict__ f = cT<T>(t.phis) + o;
+  T* out = mT<T>(t.out);
+  const T base = out[o];  // k_adv_base's value of this cell
+  Axial19<T> S;
+  S.c = f[0];
+#pragma unroll
+  for (int d = -3; d <= 3; ++d) {
+    if (d == 0) continue;
+    S.x[d + 3] = f[d];
+    S.y[d + 3] = f[d * sy];
+    S.z[d + 3] = f[d * sz];
+  }
+  S.x[3] = S.y[3] = S.z[3] = S.c;
+  putL(p, out, i, j, k, base + fdt * adv_rhs<SCHEME>(p, S, vu[q], vv[q], vw[q], k));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NT) k_adv_walls(Params p, const __grid_constant__ LsBatch B) {
+  const int ti = task_of(B);
+  const LsTask& t = B.t[ti];
+  const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
+  if (!c.ok) return;
+  T* out = mT<T>(t.out);
+  auto at = [&](int k) { return out[idxL(p, c.i, c.j, k)]; };
+  // the rows of this block's chunk that were computed, as k_adv_stage sees them
+  auto row = [&](int k) { return k >= c.ka && k <= c.kb && computed(c, t.r, k); };
+  // k = 0: written when row 2 of the same chunk was computed, from rows 1
+  // (0 if not computed) and 2
+  if (row(0) && row(2)) putL(p, out, c.i, c.j, 0, TC(2.) * (row(1) ? at(1) : TC(0.)) - at(2));
+  // k = k1: from rows kmax and kmax-1 of the same chunk (0 where not computed)
+  if (row(p.k1)) {
+    const T vk = row(p.kmax) ? at(p.kmax) : TC(0.);
+    const T vkm = row(p.kmax - 1) ? at(p.kmax - 1) : TC(0.);
+    putL(p, out, c.i, c.j, p.k1, TC(2.) * vk - vkm);
+  }
+}
+
 // ------------------------------------------------------------ reinit
 // sgn(phi_0) of ls_reinit (levelset.f90:668-678)
 template <typename T>
@@ -1201,6 +1318,43 @@ void adv_launch(Ctx& c, const LsBatch& b, int scheme, int stage1, double a, doub
   else
     k_adv_stage<ICLS_WENO5, T><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
 }
+// the band list of a batch (its tasks' masks set): entries in c.band_list,
+// their number in c.band_count on the device; need = the upper bound the
+// caller checked against c.band_cap
+void launch_band_list(Ctx& c, const LsBatch& b) {
+  if (b.n == 0) return;
+  Scope sc_(c.prof, c.s, "band_list", 1);
+  cudaMemsetAsync(c.band_count, 0, sizeof(int), c.s);
+  BandCell* list = reinterpret_cast<BandCell*>(c.band_list);
+  BY_FORM(c, (k_band_list<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, list, c.band_count, (int)c.band_cap)),
+          (k_band_list<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, list, c.band_count, (int)c.band_cap)));
+}
+template <typename T>
+void adv_split_launch(Ctx& c, const LsBatch& b, int scheme, int stage1, double a, double bb, double fdt,
+                      const double* vu, const double* vv, const double* vw, long long need) {
+  const T* u = reinterpret_cast<const T*>(vu);
+  const T* v = reinterpret_cast<const T*>(vv);
+  const T* w = reinterpret_cast<const T*>(vw);
+  const BandCell* list = reinterpret_cast<const BandCell*>(c.band_list);
+  const unsigned nb = (unsigned)((need + NT - 1) / NT);
+  k_adv_base<T><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage1, a, bb);
+  if (nb > 0) {
+    if (scheme == ICLS_HOUC5)
+      k_adv_band<ICLS_HOUC5, T><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
+    else
+      k_adv_band<ICLS_WENO5, T><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
+  }
+  k_adv_walls<T><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b);
+}
+// one RK stage over the batch from its band list (launch_band_list first)
+void launch_adv_split(Ctx& c, const LsBatch& b, int scheme, int stage1, double a, double bb, double fdt,
+                      const double* vu, const double* vv, const double* vw, long long need) {
+  if (b.n == 0) return;
+  Scope sc_(c.prof, c.s, "adv_stage", 3);
+  BY_FORM(c, adv_split_launch<float>(c, b, scheme, stage1, a, bb, fdt, vu, vv, vw, need),
+          adv_split_launch<double>(c, b, scheme, stage1, a, bb, fdt, vu, vv, vw, need));
+}
+
 void launch_adv_stage(Ctx& c, const LsBatch& b, int scheme, int stage1, double a, double bb, double fdt,
                       const double* vu, const double* vv, const double* vw) {
   if (b.n == 0) return;

@@ -457,3 +457,75 @@ def test_tma_predictor_bit_identical_to_ring(monkeypatch):
             assert np.array_equal(ring.download(name), tma.download(name)), (wl.name, name)
         ring.close()
         tma.close()
+
+
+def test_band_list_advection_bit_identical_to_column(monkeypatch):
+    """The advection stages of the fused step can run as a base copy over the
+    drop's region, the right-hand side over a list of the band cells, and the
+    wall rows (ICLS_ADV=band); the one-kernel column stage computes the same
+    expressions, so every field is bit-identical after several steps: both
+    schemes, a drop whose region reaches both z walls' ghost rows, the 128^3
+    multi-drop box, and the FP32 form."""
+    from icls_gpu import FP32
+    from icls_gpu.config import IclsConfig, Workload
+    cases = []
+    for scheme in (HOUC5, WENO5):
+        cfg = make_config(itot=32, jtot=32, ktot=32, lmax=2, ls_adv_space=scheme, timestep=2e-4, rho2=10.0,
+                          miu2=10.0, Re=100.0, We=0.5)
+        cases.append(Workload("walls_32_%d" % scheme, cfg, [(0.5, 0.45, 0.1), (0.4, 0.6, 0.88)], [0.09, 0.1],
+                              True, 0.0, 4))
+    cases.append(boxed_case(steps=4))
+    f32 = boxed_case(steps=4)
+    f32.cfg = IclsConfig.from_buffer_copy(f32.cfg)
+    f32.cfg.precision = FP32
+    cases.append(f32)
+    for wl in cases:
+        cfg = wl.cfg
+        ls = init_drops(cfg, wl.centres, wl.radii, wl.all_images)
+        u, v, w = smooth_velocity(cfg, amp=0.8, seed=21)
+        col = Solver(cfg)
+        monkeypatch.setenv("ICLS_ADV", "band")
+        band = Solver(cfg)
+        monkeypatch.delenv("ICLS_ADV")
+        for s in (col, band):
+            s.setup(ls, u, v, w)
+        for istep in range(1, 5):
+            col.step(istep, 0)
+            band.step(istep, 0)
+        for l in range(1, cfg.lmax + 1):
+            assert np.array_equal(col.download("lvset", l), band.download("lvset", l)), (wl.name, l)
+        for name in ("u", "v", "w", "pnew", "curv"):
+            assert np.array_equal(col.download(name), band.download(name)), (wl.name, name)
+        col.close()
+        band.close()
+
+
+def test_correc_column_bit_identical_to_cell(monkeypatch):
+    """The velocity correction of the fused step (correc, bounduvw and the
+    cell-centre velocities) streamed along z per column gives the same bits
+    as one thread per cell (ICLS_CORREC=cell): moving walls (the k = 0 and
+    k1 rows), z chunks of several lengths (64^3 and 128^3), both forms."""
+    from icls_gpu import FP32
+    from icls_gpu.config import IclsConfig
+    cases = [multi_drop(n=64, ndrop=3, seed=7, steps=3, rmin=0.08, rmax=0.1, dt=2e-5), boxed_case(steps=3)]
+    f32 = boxed_case(steps=3)
+    f32.cfg = IclsConfig.from_buffer_copy(f32.cfg)
+    f32.cfg.precision = FP32
+    cases.append(f32)
+    for wl in cases:
+        cfg = wl.cfg
+        ls = init_drops(cfg, wl.centres, wl.radii, wl.all_images)
+        u, v, w = initial_velocity(cfg, wl.shear_v)
+        monkeypatch.setenv("ICLS_CORREC", "cell")
+        cell = Solver(cfg)
+        monkeypatch.delenv("ICLS_CORREC")
+        col = Solver(cfg)
+        for s in (cell, col):
+            s.setup(ls, u, v, w)
+        for istep in range(1, 4):
+            cell.step(istep, 0)
+            col.step(istep, 0)
+        for name in ("u", "v", "w", "ucc", "vcc", "wcc", "pnew"):
+            assert np.array_equal(cell.download(name), col.download(name)), (wl.name, name)
+        cell.close()
+        col.close()
