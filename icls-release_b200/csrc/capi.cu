@@ -247,11 +247,6 @@ int allocate(Ctx& c) {
   // bookkeeping: both give bit-identical fields)
   const char* fs = std::getenv("ICLS_FULL_SWEEP");
   c.use_boxes = (P.L <= kMaxDropsParam) && !(fs && fs[0] == '1');
-  {
-    int dev = 0, nsm = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && nsm > 0) c.num_sms = nsm;
-  }
   // Alternative kernels of the same arithmetic (bit-identical fields), kept
   // for comparison:
   // ICLS_AB2=tma: the FP64 predictor on the TMA-fed kernel in place of the
@@ -259,14 +254,11 @@ int allocate(Ctx& c) {
   // 1.68 ms);
   // ICLS_ADV=band: the advection stages after tube_construction as the
   // band-list split (measured no faster in FP64, slower in FP32, with the
-  // list build included);
-  // ICLS_CORREC=cell: the velocity correction one thread per cell.
+  // list build included).
   const char* ab = std::getenv("ICLS_AB2");
   c.ab2_ring = !(ab && std::strcmp(ab, "tma") == 0);
   const char* av = std::getenv("ICLS_ADV");
   c.adv_column = !(av && std::strcmp(av, "band") == 0);
-  const char* cv = std::getenv("ICLS_CORREC");
-  c.correc_col = !(cv && std::strcmp(cv, "cell") == 0);
   // working buffers of a group of drops: as many drops as half the free
   // HBM holds (ICLS_GROUP=n caps the group, e.g. to test the grouped path)
   {
@@ -1709,14 +1701,16 @@ int icls_step(icls_ctx* h, int istep, int begin) {
   }
   launch_solver2d(c, 1);   // solver2d + boundp(p)
   if (c.P.bcy == ICLS_BCY_PERIODIC) {
-    launch_correc(c, 1);   // correc + bounduvw + average_vel_at_center + NaN probe
+    // correc + bounduvw + average_vel_at_center + NaN probe + the pressure
+    // update (p is final after the solve)
+    launch_correc(c, 1, istep == begin + 1 ? 1 : 0);
   } else {                 // the y walls change vnew before the cell-centre averages
     launch_correc(c, 0);
     launch_bounduvw(c, c.u, c.v, c.w);
     launch_average_vel(c);
     launch_nan_probe(c);
+    launch_pressure_update(c, istep == begin + 1);
   }
-  launch_pressure_update(c, istep == begin + 1);
   rc = check_launch();
   if (rc) return rc;
   rc = read_scalars(c);

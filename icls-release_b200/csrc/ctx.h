@@ -83,8 +83,6 @@ struct Ctx {
   const void* ab2_keys[4][18] = {};
   int ab2_nmaps = 0, ab2_next = 0;
   bool ab2_tma_failed = false;  // a map could not be encoded: use the ring
-  int num_sms = 148;
-  bool correc_col = true;  // correc streamed along z (else one thread per cell: ICLS_CORREC=cell)
   bool ab2_ring = true;  // FP64 predictor on the cp.async ring (else TMA: ICLS_AB2=tma)
   icls_config cfg;
   Params P;
@@ -243,7 +241,10 @@ void launch_ab2(Ctx& c);
 void launch_mom_main(Ctx& c, double* du, double* dv, double* dw);
 void launch_fillps(Ctx& c, int add_pjump);
 void launch_add_pjump(Ctx& c);
-void launch_correc(Ctx& c, int fused_bc);
+// fused_bc: with bounduvw, the cell-centre velocities and the NaN probe;
+// pupdate_first >= 0 (with fused_bc): also the pressure update, first step
+// when 1
+void launch_correc(Ctx& c, int fused_bc, int pupdate_first = -1);
 void launch_bounduvw(Ctx& c, double* u, double* v, double* w);
 // tfield: the array holds the form's field type (FP32 in the precision form)
 void launch_boundp(Ctx& c, double* p, bool tfield = false);

@@ -123,7 +123,29 @@ struct CorrArgs {
   const double *dudt, *dvdt, *dwdt, *p, *px, *py, *pz;
   double *u, *v, *w, *ucc, *vcc, *wcc;
   DevScalars* dsc;
+  // the pressure update of the same cell, in k_correc_fused when pupd is set
+  // (k_plane_norm has run on p before): pnew, pold in the form's type T
+  double *pnew, *pold;
+  int pupd, first, norm;
 };
+
+// the pressure update of cell n (main.f90:169-191): pold = pnew - norm
+// (the previous norm added back after the first step), pnew = p - norm;
+// without the plane-1 normalisation pold = pnew, pnew = p
+template <typename T>
+__device__ __forceinline__ void pupdate_cell(const Params& p, long long n, double pv, T* __restrict__ pnew,
+                                             T* __restrict__ pold, int first, int normalise,
+                                             const DevScalars* __restrict__ dsc) {
+  if (!normalise) {
+    pold[n] = pnew[n];
+    pnew[n] = TC(pv);
+    return;
+  }
+  const double norm = dsc->norm;
+  const double po = (double)pnew[n];
+  pold[n] = TC(first ? po - norm : (po + dsc->norm_old) - norm);
+  pnew[n] = TC(pv - norm);
+}
 
 // correc over the interior only (the separate reference call)
 template <typename T>
@@ -172,86 +194,7 @@ __global__ void __launch_bounds__(NT) k_correc_fused(Params p, CorrArgs a) {
     mT<T>(a.wcc)[q] = (wm + ww) / TC(2.);
     if (i == 1 && j == 1 && k == 1 && isnan(vv)) a.dsc->nan_flag = 1;
   }
-}
-
-// One correc value from its operands: d - dt dxi ((p_hi - p_lo) - jump) / rho0
-// (correc.f90:27-39), the expression of corr_u/v/w.
-template <typename T>
-__device__ __forceinline__ T corr1(const Params& p, T d, double hi, double lo, T jump, double dxi) {
-  const double g = div_rho0(p, p.dt * dxi * ((hi - lo) - (double)jump));
-  if (sizeof(T) == sizeof(double)) return (T)((double)d - g);
-  return d - (T)g;
-}
-
-// k_correc_fused streamed along z: a thread walks rows ka..kb of one
-// shape-C column (i, j) with its offsets advanced by one plane per row,
-// reads the pressure of row k+1 once for the w correction of row k and the
-// gradients of row k+1, and takes the w correction of row k-1 for the
-// cell-centre average from the row before.  Every value is the expression
-// k_correc_fused evaluates, so the fields are the same bits.
-template <typename T>
-__global__ void __launch_bounds__(NT) k_correc_col(Params p, CorrArgs a, int kc) {
-  const int i = (int)(blockIdx.x * BX + threadIdx.x), j = (int)(blockIdx.y * BY + threadIdx.y);
-  if (i > p.imax + 1 || j > p.jmax + 1) return;
-  const int ka = (int)blockIdx.z * kc, kb = min(ka + kc - 1, p.k1);
-  const int I = wrapx(p, i), J = wrapy(p, j);
-  const bool own = I == i && J == j;
-  const long long sy = p.nCx, sz = (long long)p.nCx * p.nCy, szI = (long long)p.imax * p.jmax;
-  const T* __restrict__ du = cT<T>(a.dudt);
-  const T* __restrict__ dv = cT<T>(a.dvdt);
-  const T* __restrict__ dw = cT<T>(a.dwdt);
-  const T* __restrict__ px = cT<T>(a.px);
-  const T* __restrict__ py = cT<T>(a.py);
-  const T* __restrict__ pz = cT<T>(a.pz);
-  const double* __restrict__ pp = a.p;
-  T* __restrict__ u = mT<T>(a.u);
-  T* __restrict__ v = mT<T>(a.v);
-  T* __restrict__ w = mT<T>(a.w);
-  const long long s0 = idxC(p, I, J, 0), d0 = idxC(p, i, j, 0);
-  // the (i-1) and (j-1) source columns of the cell-centre average
-  const long long sm_u = idxC(p, wrapx(p, i - 1), j, 0), sm_v = idxC(p, i, wrapy(p, j - 1), 0);
-  auto cw = [&](int k) {
-    const long long c = s0 + k * sz;
-    return corr1<T>(p, dw[c], pp[c + sz], pp[c], pz[c], p.dzi);
-  };
-  T wprev = (own && ka >= 2 && ka <= p.kmax) ? cw(ka - 1) : TC(0.);
-  for (int k = ka; k <= kb; ++k) {
-    const int ks = k == 0 ? 1 : (k == p.k1 ? p.kmax : k);
-    const long long c = s0 + ks * sz;
-    const double p0 = pp[c];
-    const T u0 = corr1<T>(p, du[c], pp[c + 1], p0, px[c], p.dxi);
-    const T v0 = corr1<T>(p, dv[c], pp[c + sy], p0, py[c], p.dyi);
-    T uu, vv, ww;
-    if (k >= 1 && k <= p.kmax) {
-      uu = u0;
-      vv = v0;
-      ww = (k == p.kmax) ? TC(0.) : corr1<T>(p, dw[c], pp[c + sz], p0, pz[c], p.dzi);
-    } else if (k == 0) {
-      uu = -u0;
-      vv = TC(2. * p.v_lower) - v0;
-      ww = TC(0.);
-    } else {
-      uu = -u0;
-      vv = TC(2. * p.v_upper) - v0;
-      ww = cw(p.kmax - 1);
-    }
-    const long long n = d0 + k * sz;
-    u[n] = uu;
-    v[n] = vv;
-    w[n] = ww;
-    if (own && k >= 1 && k <= p.kmax) {
-      const long long cu = sm_u + k * sz, cv = sm_v + k * sz;
-      const T um = corr1<T>(p, du[cu], pp[cu + 1], pp[cu], px[cu], p.dxi);
-      const T vm = corr1<T>(p, dv[cv], pp[cv + sy], pp[cv], py[cv], p.dyi);
-      const T wm = (k == 1) ? TC(0.) : wprev;
-      const long long q = (long long)(i - 1) + (long long)p.imax * (j - 1) + (k - 1) * szI;
-      mT<T>(a.ucc)[q] = (um + uu) / TC(2.);
-      mT<T>(a.vcc)[q] = (vm + vv) / TC(2.);
-      mT<T>(a.wcc)[q] = (wm + ww) / TC(2.);
-      if (i == 1 && j == 1 && k == 1 && isnan(vv)) a.dsc->nan_flag = 1;
-    }
-    wprev = ww;
-  }
+  if (a.pupd) pupdate_cell<T>(p, n, a.p[n], mT<T>(a.pnew), mT<T>(a.pold), a.first, a.norm, a.dsc);
 }
 
 // bounduvw (bound.f90:15-177, Dirichl z, periodic x,y) on an existing triple
@@ -388,15 +331,7 @@ __global__ void __launch_bounds__(NT) k_pupdate(Params p, const double* __restri
                                                 int normalise, const DevScalars* __restrict__ dsc) {
   const long long n = blockIdx.x * (long long)NT + threadIdx.x;
   if (n >= p.nC) return;
-  if (!normalise) {
-    pold[n] = pnew[n];
-    pnew[n] = TC(pp[n]);
-    return;
-  }
-  const double norm = dsc->norm;
-  const double po = (double)pnew[n];
-  pold[n] = TC(first ? po - norm : (po + dsc->norm_old) - norm);
-  pnew[n] = TC(pp[n] - norm);
+  pupdate_cell<T>(p, n, pp[n], pnew, pold, first, normalise, dsc);
 }
 
 // ---- reductions ------------------------------------------------------------
@@ -531,6 +466,8 @@ CorrArgs corr_args(Ctx& c) {
   CorrArgs a;
   a.dudt = c.dudt; a.dvdt = c.dvdt; a.dwdt = c.dwdt; a.p = c.p; a.px = c.px; a.py = c.py; a.pz = c.pz;
   a.u = c.u; a.v = c.v; a.w = c.w; a.ucc = c.ucc; a.vcc = c.vcc; a.wcc = c.wcc; a.dsc = c.dsc;
+  a.pnew = c.pnew; a.pold = c.pold;
+  a.pupd = a.first = a.norm = 0;
   return a;
 }
 
@@ -568,23 +505,24 @@ void launch_fillps(Ctx& c, int add_pjump) {
 }
 void launch_add_pjump(Ctx& c) {
   Scope sc_(c.prof, c.s, "add_pjump", 1); k_add<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, c.pjump); }
-void launch_correc(Ctx& c, int fused_bc) {
-  Scope sc_(c.prof, c.s, "correc", 1);
+// the plane-1 normalisation of the pressure update runs for BC_in_y
+// Periodic and Walls only (main.f90:169-185)
+bool pressure_normalised(const Ctx& c) { return c.P.bcy == ICLS_BCY_PERIODIC || c.P.bcy == ICLS_BCY_WALLS; }
+
+void launch_correc(Ctx& c, int fused_bc, int pupdate_first) {
+  Scope sc_(c.prof, c.s, "correc", pupdate_first >= 0 ? 2 : 1);
   CorrArgs a = corr_args(c);
-  // the column launch: z split into chunks of kc rows so that the grid
-  // holds about eight blocks per SM
-  const unsigned gx = (unsigned)((c.P.imax + 2 + BX - 1) / BX), gy = (unsigned)((c.P.jmax + 2 + BY - 1) / BY);
-  const int rows = c.P.kmax + 2;
-  const int nz = std::max(1, std::min(rows, (int)((8LL * c.num_sms + gx * gy - 1) / ((long long)gx * gy))));
-  const int kc = (rows + nz - 1) / nz;
-  const dim3 g(gx, gy, (unsigned)((rows + kc - 1) / kc));
+  if (fused_bc && pupdate_first >= 0) {  // with the pressure update of each cell
+    a.pupd = 1;
+    a.first = pupdate_first;
+    a.norm = pressure_normalised(c) ? 1 : 0;
+    if (a.norm) k_plane_norm<<<1, kNormThreads, 0, c.s>>>(c.P, c.p, c.dsc);
+  }
   if (c.P.f32) {
-    if (fused_bc && c.correc_col) k_correc_col<float><<<g, kBlock, 0, c.s>>>(c.P, a, kc);
-    else if (fused_bc) k_correc_fused<float><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, a);
+    if (fused_bc) k_correc_fused<float><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, a);
     else k_correc_interior<float><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);
   } else {
-    if (fused_bc && c.correc_col) k_correc_col<double><<<g, kBlock, 0, c.s>>>(c.P, a, kc);
-    else if (fused_bc) k_correc_fused<double><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, a);
+    if (fused_bc) k_correc_fused<double><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, a);
     else k_correc_interior<double><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);
   }
 }
@@ -636,9 +574,8 @@ void launch_average_vel(Ctx& c) {
 }
 void launch_pressure_update(Ctx& c, int first) {
   Scope sc_(c.prof, c.s, "pressure_update", 2);
-  // the plane-1 normalisation runs for BC_in_y Periodic and Walls only
-  // (main.f90:169-185); otherwise pold = pnew, pnew = p
-  const int norm = c.P.bcy == ICLS_BCY_PERIODIC || c.P.bcy == ICLS_BCY_WALLS;
+  // otherwise pold = pnew, pnew = p
+  const int norm = pressure_normalised(c) ? 1 : 0;
   if (norm) k_plane_norm<<<1, kNormThreads, 0, c.s>>>(c.P, c.p, c.dsc);
   if (c.P.f32)
     k_pupdate<float><<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, fp<float>(c.pnew), fp<float>(c.pold), first, norm,

@@ -213,9 +213,13 @@ def test_solver2d_lengths(ni, nj, nk):
     assert np.max(np.abs(pg - po)) <= 1e-11 * np.max(np.abs(po))
 
 
-def test_fused_step_equals_call_sequence():
-    """icls_step (fused kernels) == the main.f90 sequence of separate calls."""
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fused_step_equals_call_sequence(precision):
+    """icls_step (fused kernels: the projection's correc, bounduvw, cell-centre
+    velocities, NaN probe and pressure update in one) == the main.f90
+    sequence of separate calls, in FP64 and in the FP32 form."""
     cfg, ls = drop_case(L=2, reinit_step=2, inflate_step=2)
+    cfg.precision = precision
     u, v, w = smooth_velocity(cfg, amp=0.3, seed=8)
     a = Solver(cfg)
     b = Solver(cfg)
@@ -499,33 +503,3 @@ def test_band_list_advection_bit_identical_to_column(monkeypatch):
         col.close()
         band.close()
 
-
-def test_correc_column_bit_identical_to_cell(monkeypatch):
-    """The velocity correction of the fused step (correc, bounduvw and the
-    cell-centre velocities) streamed along z per column gives the same bits
-    as one thread per cell (ICLS_CORREC=cell): moving walls (the k = 0 and
-    k1 rows), z chunks of several lengths (64^3 and 128^3), both forms."""
-    from icls_gpu import FP32
-    from icls_gpu.config import IclsConfig
-    cases = [multi_drop(n=64, ndrop=3, seed=7, steps=3, rmin=0.08, rmax=0.1, dt=2e-5), boxed_case(steps=3)]
-    f32 = boxed_case(steps=3)
-    f32.cfg = IclsConfig.from_buffer_copy(f32.cfg)
-    f32.cfg.precision = FP32
-    cases.append(f32)
-    for wl in cases:
-        cfg = wl.cfg
-        ls = init_drops(cfg, wl.centres, wl.radii, wl.all_images)
-        u, v, w = initial_velocity(cfg, wl.shear_v)
-        monkeypatch.setenv("ICLS_CORREC", "cell")
-        cell = Solver(cfg)
-        monkeypatch.delenv("ICLS_CORREC")
-        col = Solver(cfg)
-        for s in (cell, col):
-            s.setup(ls, u, v, w)
-        for istep in range(1, 4):
-            cell.step(istep, 0)
-            col.step(istep, 0)
-        for name in ("u", "v", "w", "ucc", "vcc", "wcc", "pnew"):
-            assert np.array_equal(cell.download(name), col.download(name)), (wl.name, name)
-        cell.close()
-        col.close()
