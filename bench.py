@@ -94,7 +94,7 @@ def initial_state(wl):
 # S |phi| <= 2dz shell cells of all drops.
 ALG_VALUES = {
     "ab2": (24, 0, "N"),             # u,v,w,miu,rho_uvw,duold x3,pnew,pold,p_xyz,p_xyz_old -> dudt x3,duold x3
-    "correc": (15, 1, "N"),          # dudt x3,p_xyz,pnew | p -> u,v,w, ucc,vcc,wcc, pnew,pold (with the pressure update)
+    "correc": (12, 1, "N"),          # dudt x3,p_xyz | p -> u,v,w, ucc,vcc,wcc
     "fillps": (3, 2, "N"),           # dudt x3 | pjump -> p
     "solver2d": (0, 2, "N"),         # p -> p (the transposes and sweeps between are not compulsory)
     "pressure_update": (3, 1, "N"),  # pnew | p -> pnew, pold

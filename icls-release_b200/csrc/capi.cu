@@ -1701,16 +1701,14 @@ int icls_step(icls_ctx* h, int istep, int begin) {
   }
   launch_solver2d(c, 1);   // solver2d + boundp(p)
   if (c.P.bcy == ICLS_BCY_PERIODIC) {
-    // correc + bounduvw + average_vel_at_center + NaN probe + the pressure
-    // update (p is final after the solve)
-    launch_correc(c, 1, istep == begin + 1 ? 1 : 0);
+    launch_correc(c, 1);   // correc + bounduvw + average_vel_at_center + NaN probe
   } else {                 // the y walls change vnew before the cell-centre averages
     launch_correc(c, 0);
     launch_bounduvw(c, c.u, c.v, c.w);
     launch_average_vel(c);
     launch_nan_probe(c);
-    launch_pressure_update(c, istep == begin + 1);
   }
+  launch_pressure_update(c, istep == begin + 1);
   rc = check_launch();
   if (rc) return rc;
   rc = read_scalars(c);

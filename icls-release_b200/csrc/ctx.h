@@ -241,10 +241,8 @@ void launch_ab2(Ctx& c);
 void launch_mom_main(Ctx& c, double* du, double* dv, double* dw);
 void launch_fillps(Ctx& c, int add_pjump);
 void launch_add_pjump(Ctx& c);
-// fused_bc: with bounduvw, the cell-centre velocities and the NaN probe;
-// pupdate_first >= 0 (with fused_bc): also the pressure update, first step
-// when 1
-void launch_correc(Ctx& c, int fused_bc, int pupdate_first = -1);
+// fused_bc: with bounduvw, the cell-centre velocities and the NaN probe
+void launch_correc(Ctx& c, int fused_bc);
 void launch_bounduvw(Ctx& c, double* u, double* v, double* w);
 // tfield: the array holds the form's field type (FP32 in the precision form)
 void launch_boundp(Ctx& c, double* p, bool tfield = false);

@@ -123,29 +123,7 @@ struct CorrArgs {
   const double *dudt, *dvdt, *dwdt, *p, *px, *py, *pz;
   double *u, *v, *w, *ucc, *vcc, *wcc;
   DevScalars* dsc;
-  // the pressure update of the same cell, in k_correc_fused when pupd is set
-  // (k_plane_norm has run on p before): pnew, pold in the form's type T
-  double *pnew, *pold;
-  int pupd, first, norm;
 };
-
-// the pressure update of cell n (main.f90:169-191): pold = pnew - norm
-// (the previous norm added back after the first step), pnew = p - norm;
-// without the plane-1 normalisation pold = pnew, pnew = p
-template <typename T>
-__device__ __forceinline__ void pupdate_cell(const Params& p, long long n, double pv, T* __restrict__ pnew,
-                                             T* __restrict__ pold, int first, int normalise,
-                                             const DevScalars* __restrict__ dsc) {
-  if (!normalise) {
-    pold[n] = pnew[n];
-    pnew[n] = TC(pv);
-    return;
-  }
-  const double norm = dsc->norm;
-  const double po = (double)pnew[n];
-  pold[n] = TC(first ? po - norm : (po + dsc->norm_old) - norm);
-  pnew[n] = TC(pv - norm);
-}
 
 // correc over the interior only (the separate reference call)
 template <typename T>
@@ -194,7 +172,6 @@ __global__ void __launch_bounds__(NT) k_correc_fused(Params p, CorrArgs a) {
     mT<T>(a.wcc)[q] = (wm + ww) / TC(2.);
     if (i == 1 && j == 1 && k == 1 && isnan(vv)) a.dsc->nan_flag = 1;
   }
-  if (a.pupd) pupdate_cell<T>(p, n, a.p[n], mT<T>(a.pnew), mT<T>(a.pold), a.first, a.norm, a.dsc);
 }
 
 // bounduvw (bound.f90:15-177, Dirichl z, periodic x,y) on an existing triple
@@ -331,7 +308,15 @@ __global__ void __launch_bounds__(NT) k_pupdate(Params p, const double* __restri
                                                 int normalise, const DevScalars* __restrict__ dsc) {
   const long long n = blockIdx.x * (long long)NT + threadIdx.x;
   if (n >= p.nC) return;
-  pupdate_cell<T>(p, n, pp[n], pnew, pold, first, normalise, dsc);
+  if (!normalise) {
+    pold[n] = pnew[n];
+    pnew[n] = TC(pp[n]);
+    return;
+  }
+  const double norm = dsc->norm;
+  const double po = (double)pnew[n];
+  pold[n] = TC(first ? po - norm : (po + dsc->norm_old) - norm);
+  pnew[n] = TC(pp[n] - norm);
 }
 
 // ---- reductions ------------------------------------------------------------
@@ -466,8 +451,6 @@ CorrArgs corr_args(Ctx& c) {
   CorrArgs a;
   a.dudt = c.dudt; a.dvdt = c.dvdt; a.dwdt = c.dwdt; a.p = c.p; a.px = c.px; a.py = c.py; a.pz = c.pz;
   a.u = c.u; a.v = c.v; a.w = c.w; a.ucc = c.ucc; a.vcc = c.vcc; a.wcc = c.wcc; a.dsc = c.dsc;
-  a.pnew = c.pnew; a.pold = c.pold;
-  a.pupd = a.first = a.norm = 0;
   return a;
 }
 
@@ -505,19 +488,9 @@ void launch_fillps(Ctx& c, int add_pjump) {
 }
 void launch_add_pjump(Ctx& c) {
   Scope sc_(c.prof, c.s, "add_pjump", 1); k_add<<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, c.pjump); }
-// the plane-1 normalisation of the pressure update runs for BC_in_y
-// Periodic and Walls only (main.f90:169-185)
-bool pressure_normalised(const Ctx& c) { return c.P.bcy == ICLS_BCY_PERIODIC || c.P.bcy == ICLS_BCY_WALLS; }
-
-void launch_correc(Ctx& c, int fused_bc, int pupdate_first) {
-  Scope sc_(c.prof, c.s, "correc", pupdate_first >= 0 ? 2 : 1);
+void launch_correc(Ctx& c, int fused_bc) {
+  Scope sc_(c.prof, c.s, "correc", 1);
   CorrArgs a = corr_args(c);
-  if (fused_bc && pupdate_first >= 0) {  // with the pressure update of each cell
-    a.pupd = 1;
-    a.first = pupdate_first;
-    a.norm = pressure_normalised(c) ? 1 : 0;
-    if (a.norm) k_plane_norm<<<1, kNormThreads, 0, c.s>>>(c.P, c.p, c.dsc);
-  }
   if (c.P.f32) {
     if (fused_bc) k_correc_fused<float><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, a);
     else k_correc_interior<float><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);
@@ -574,8 +547,9 @@ void launch_average_vel(Ctx& c) {
 }
 void launch_pressure_update(Ctx& c, int first) {
   Scope sc_(c.prof, c.s, "pressure_update", 2);
-  // otherwise pold = pnew, pnew = p
-  const int norm = pressure_normalised(c) ? 1 : 0;
+  // the plane-1 normalisation runs for BC_in_y Periodic and Walls only
+  // (main.f90:169-185); otherwise pold = pnew, pnew = p
+  const int norm = c.P.bcy == ICLS_BCY_PERIODIC || c.P.bcy == ICLS_BCY_WALLS;
   if (norm) k_plane_norm<<<1, kNormThreads, 0, c.s>>>(c.P, c.p, c.dsc);
   if (c.P.f32)
     k_pupdate<float><<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, fp<float>(c.pnew), fp<float>(c.pold), first, norm,

@@ -215,9 +215,8 @@ def test_solver2d_lengths(ni, nj, nk):
 
 @pytest.mark.parametrize("precision", [0, 1])
 def test_fused_step_equals_call_sequence(precision):
-    """icls_step (fused kernels: the projection's correc, bounduvw, cell-centre
-    velocities, NaN probe and pressure update in one) == the main.f90
-    sequence of separate calls, in FP64 and in the FP32 form."""
+    """icls_step (fused kernels) == the main.f90 sequence of separate calls,
+    in FP64 and in the FP32 form."""
     cfg, ls = drop_case(L=2, reinit_step=2, inflate_step=2)
     cfg.precision = precision
     u, v, w = smooth_velocity(cfg, amp=0.3, seed=8)
