@@ -33,7 +33,7 @@ namespace {
 // the same expressions serve the shared-memory march of k_ab2 and the
 // global-memory k_mom_main.  T is the form's field type; TC(x) the
 // constant x in T.
-template <typename T, class FU, class FV, class FW, class FM>
+template <typename T, int PW = -1, class FU, class FV, class FW, class FM>
 __device__ __forceinline__ T rhs_u(const Params& p, const FU& U, const FV& V, const FW& W, const FM& M,
                                         T rho_u, T rho_avr) {
   T RCu = TC(0.);
@@ -44,29 +44,29 @@ __device__ __forceinline__ T rhs_u(const Params& p, const FU& U, const FV& V, co
     T uvjm = TC(0.25) * (U(0, -1, 0) + U(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
     T uwkp = TC(0.25) * (U(0, 0, 1) + U(0, 0, 0)) * (W(1, 0, 0) + W(0, 0, 0));
     T uwkm = TC(0.25) * (U(0, 0, -1) + U(0, 0, 0)) * (W(1, 0, -1) + W(0, 0, -1));
-    RCu = (divx(p, (-uuip + uuim)) + divy(p, (-uvjp + uvjm))) + divz(p, (-uwkp + uwkm));
+    RCu = (divx<PW>(p, (-uuip + uuim)) + divy<PW>(p, (-uvjp + uvjm))) + divz<PW>(p, (-uwkp + uwkm));
   }
   T RDu = TC(0.);
   if (!p.TwoD) {
-    T dudxp = divx(p, (U(1, 0, 0) - U(0, 0, 0)));
-    T dudxm = divx(p, (U(0, 0, 0) - U(-1, 0, 0)));
-    T dudyp = divy(p, (U(0, 1, 0) - U(0, 0, 0)));
-    T dudym = divy(p, (U(0, 0, 0) - U(0, -1, 0)));
-    T dvdxp = divx(p, (V(1, 0, 0) - V(0, 0, 0)));
-    T dvdxm = divx(p, (V(1, -1, 0) - V(0, -1, 0)));
-    T dudzp = divz(p, (U(0, 0, 1) - U(0, 0, 0)));
-    T dudzm = divz(p, (U(0, 0, 0) - U(0, 0, -1)));
-    T dwdxp = divx(p, (W(1, 0, 0) - W(0, 0, 0)));
-    T dwdxm = divx(p, (W(1, 0, -1) - W(0, 0, -1)));
+    T dudxp = divx<PW>(p, (U(1, 0, 0) - U(0, 0, 0)));
+    T dudxm = divx<PW>(p, (U(0, 0, 0) - U(-1, 0, 0)));
+    T dudyp = divy<PW>(p, (U(0, 1, 0) - U(0, 0, 0)));
+    T dudym = divy<PW>(p, (U(0, 0, 0) - U(0, -1, 0)));
+    T dvdxp = divx<PW>(p, (V(1, 0, 0) - V(0, 0, 0)));
+    T dvdxm = divx<PW>(p, (V(1, -1, 0) - V(0, -1, 0)));
+    T dudzp = divz<PW>(p, (U(0, 0, 1) - U(0, 0, 0)));
+    T dudzm = divz<PW>(p, (U(0, 0, 0) - U(0, 0, -1)));
+    T dwdxp = divx<PW>(p, (W(1, 0, 0) - W(0, 0, 0)));
+    T dwdxm = divx<PW>(p, (W(1, 0, -1) - W(0, 0, -1)));
     T ma1 = TC(0.25) * (((M(0, 0, 0) + M(0, -1, 0)) + M(1, -1, 0)) + M(1, 0, 0));
     T ma2 = TC(0.25) * (((M(0, 0, 0) + M(0, 1, 0)) + M(1, 1, 0)) + M(1, 0, 0));
     T ma3 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, -1)) + M(1, 0, -1)) + M(1, 0, 0));
     T ma4 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, 1)) + M(1, 0, 1)) + M(1, 0, 0));
-    T RD1 = divx(p, TC(2.) * (dudxp * M(1, 0, 0) - dudxm * M(0, 0, 0)));
-    T RD2 = divy(p, (dudyp * ma2 - dudym * ma1));
-    T RD3 = divy(p, (dvdxp * ma2 - dvdxm * ma1));
-    T RD4 = divz(p, (dudzp * ma4 - dudzm * ma3));
-    T RD5 = divz(p, (dwdxp * ma4 - dwdxm * ma3));
+    T RD1 = divx<PW>(p, TC(2.) * (dudxp * M(1, 0, 0) - dudxm * M(0, 0, 0)));
+    T RD2 = divy<PW>(p, (dudyp * ma2 - dudym * ma1));
+    T RD3 = divy<PW>(p, (dvdxp * ma2 - dvdxm * ma1));
+    T RD4 = divz<PW>(p, (dudzp * ma4 - dudzm * ma3));
+    T RD5 = divz<PW>(p, (dwdxp * ma4 - dwdxm * ma3));
     RDu = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rho_u;
   }
   // buoyancy iFr (1 - rho_avr/rho) g: skipped (with its divide) where iFr or
@@ -77,7 +77,7 @@ __device__ __forceinline__ T rhs_u(const Params& p, const FU& U, const FV& V, co
   return (RCu + RDu * TC(p.visc)) + RGu;
 }
 
-template <typename T, class FU, class FV, class FW, class FM>
+template <typename T, int PW = -1, class FU, class FV, class FW, class FM>
 __device__ __forceinline__ T rhs_v(const Params& p, const FU& U, const FV& V, const FW& W, const FM& M,
                                         T rv, T rho_avr) {
   T uvip = TC(0.25) * (U(0, 0, 0) + U(0, 1, 0)) * (V(0, 0, 0) + V(1, 0, 0));
@@ -86,33 +86,33 @@ __device__ __forceinline__ T rhs_v(const Params& p, const FU& U, const FV& V, co
   T vvjm = TC(0.25) * (V(0, 0, 0) + V(0, -1, 0)) * (V(0, 0, 0) + V(0, -1, 0));
   T wvkp = TC(0.25) * (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 1) + V(0, 0, 0));
   T wvkm = TC(0.25) * (W(0, 0, -1) + W(0, 1, -1)) * (V(0, 0, -1) + V(0, 0, 0));
-  T RCv = (divx(p, (-uvip + uvim)) + divy(p, (-vvjp + vvjm))) + divz(p, (-wvkp + wvkm));
-  T dvdxp = divx(p, (V(1, 0, 0) - V(0, 0, 0)));
-  T dvdxm = divx(p, (V(0, 0, 0) - V(-1, 0, 0)));
-  T dudyp = divy(p, (U(0, 1, 0) - U(0, 0, 0)));
-  T dudym = divy(p, (U(-1, 1, 0) - U(-1, 0, 0)));
-  T dvdyp = divy(p, (V(0, 1, 0) - V(0, 0, 0)));
-  T dvdym = divy(p, (V(0, 0, 0) - V(0, -1, 0)));
-  T dvdzp = divz(p, (V(0, 0, 1) - V(0, 0, 0)));
-  T dvdzm = divz(p, (V(0, 0, 0) - V(0, 0, -1)));
-  T dwdyp = divy(p, (W(0, 1, 0) - W(0, 0, 0)));
-  T dwdym = divy(p, (W(0, 1, -1) - W(0, 0, -1)));
+  T RCv = (divx<PW>(p, (-uvip + uvim)) + divy<PW>(p, (-vvjp + vvjm))) + divz<PW>(p, (-wvkp + wvkm));
+  T dvdxp = divx<PW>(p, (V(1, 0, 0) - V(0, 0, 0)));
+  T dvdxm = divx<PW>(p, (V(0, 0, 0) - V(-1, 0, 0)));
+  T dudyp = divy<PW>(p, (U(0, 1, 0) - U(0, 0, 0)));
+  T dudym = divy<PW>(p, (U(-1, 1, 0) - U(-1, 0, 0)));
+  T dvdyp = divy<PW>(p, (V(0, 1, 0) - V(0, 0, 0)));
+  T dvdym = divy<PW>(p, (V(0, 0, 0) - V(0, -1, 0)));
+  T dvdzp = divz<PW>(p, (V(0, 0, 1) - V(0, 0, 0)));
+  T dvdzm = divz<PW>(p, (V(0, 0, 0) - V(0, 0, -1)));
+  T dwdyp = divy<PW>(p, (W(0, 1, 0) - W(0, 0, 0)));
+  T dwdym = divy<PW>(p, (W(0, 1, -1) - W(0, 0, -1)));
   T ma2 = TC(0.25) * (((M(0, 0, 0) + M(0, 1, 0)) + M(1, 1, 0)) + M(1, 0, 0));
   T ma5 = TC(0.25) * (((M(0, 0, 0) + M(0, 1, 0)) + M(-1, 1, 0)) + M(-1, 0, 0));
   T ma6 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, -1)) + M(0, 1, -1)) + M(0, 1, 0));
   T ma7 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, 1)) + M(0, 1, 1)) + M(0, 1, 0));
-  T RD1 = divx(p, (dvdxp * ma2 - dvdxm * ma5));
-  T RD2 = divx(p, (dudyp * ma2 - dudym * ma5));
-  T RD3 = divy(p, TC(2.) * (dvdyp * M(0, 1, 0) - dvdym * M(0, 0, 0)));
-  T RD4 = divz(p, (dvdzp * ma7 - dvdzm * ma6));
-  T RD5 = divz(p, (dwdyp * ma7 - dwdym * ma6));
+  T RD1 = divx<PW>(p, (dvdxp * ma2 - dvdxm * ma5));
+  T RD2 = divx<PW>(p, (dudyp * ma2 - dudym * ma5));
+  T RD3 = divy<PW>(p, TC(2.) * (dvdyp * M(0, 1, 0) - dvdym * M(0, 0, 0)));
+  T RD4 = divz<PW>(p, (dvdzp * ma7 - dvdzm * ma6));
+  T RD5 = divz<PW>(p, (dwdyp * ma7 - dwdym * ma6));
   T RDv = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rv;
   if (p.iFr == 0. || p.g2 == 0.) return RCv + RDv * TC(p.visc);  // buoyancy as in rhs_u
   T RGv = TC(p.iFr) * (TC(1.) - rho_avr / rv) * TC(p.g2);
   return (RCv + RDv * TC(p.visc)) + RGv;
 }
 
-template <typename T, class FU, class FV, class FW, class FM>
+template <typename T, int PW = -1, class FU, class FV, class FW, class FM>
 __device__ __forceinline__ T rhs_w(const Params& p, const FU& U, const FV& V, const FW& W, const FM& M,
                                         T rw, T rho_avr) {
   T uwip = TC(0.25) * (W(0, 0, 0) + W(1, 0, 0)) * (U(0, 0, 0) + U(0, 0, 1));
@@ -121,26 +121,26 @@ __device__ __forceinline__ T rhs_w(const Params& p, const FU& U, const FV& V, co
   T vwjm = TC(0.25) * (W(0, 0, 0) + W(0, -1, 0)) * (V(0, -1, 0) + V(0, -1, 1));
   T wwkp = TC(0.25) * (W(0, 0, 0) + W(0, 0, 1)) * (W(0, 0, 0) + W(0, 0, 1));
   T wwkm = TC(0.25) * (W(0, 0, 0) + W(0, 0, -1)) * (W(0, 0, 0) + W(0, 0, -1));
-  T RCw = (divx(p, (-uwip + uwim)) + divy(p, (-vwjp + vwjm))) + divz(p, (-wwkp + wwkm));
-  T dwdxp = divx(p, (W(1, 0, 0) - W(0, 0, 0)));
-  T dwdxm = divx(p, (W(0, 0, 0) - W(-1, 0, 0)));
-  T dudzp = divz(p, (U(0, 0, 1) - U(0, 0, 0)));
-  T dudzm = divz(p, (U(-1, 0, 1) - U(-1, 0, 0)));
-  T dwdyp = divy(p, (W(0, 1, 0) - W(0, 0, 0)));
-  T dwdym = divy(p, (W(0, 0, 0) - W(0, -1, 0)));
-  T dvdzp = divz(p, (V(0, 0, 1) - V(0, 0, 0)));
-  T dvdzm = divz(p, (V(0, -1, 1) - V(0, -1, 0)));
-  T dwdzp = divz(p, (W(0, 0, 1) - W(0, 0, 0)));
-  T dwdzm = divz(p, (W(0, 0, 0) - W(0, 0, -1)));
+  T RCw = (divx<PW>(p, (-uwip + uwim)) + divy<PW>(p, (-vwjp + vwjm))) + divz<PW>(p, (-wwkp + wwkm));
+  T dwdxp = divx<PW>(p, (W(1, 0, 0) - W(0, 0, 0)));
+  T dwdxm = divx<PW>(p, (W(0, 0, 0) - W(-1, 0, 0)));
+  T dudzp = divz<PW>(p, (U(0, 0, 1) - U(0, 0, 0)));
+  T dudzm = divz<PW>(p, (U(-1, 0, 1) - U(-1, 0, 0)));
+  T dwdyp = divy<PW>(p, (W(0, 1, 0) - W(0, 0, 0)));
+  T dwdym = divy<PW>(p, (W(0, 0, 0) - W(0, -1, 0)));
+  T dvdzp = divz<PW>(p, (V(0, 0, 1) - V(0, 0, 0)));
+  T dvdzm = divz<PW>(p, (V(0, -1, 1) - V(0, -1, 0)));
+  T dwdzp = divz<PW>(p, (W(0, 0, 1) - W(0, 0, 0)));
+  T dwdzm = divz<PW>(p, (W(0, 0, 0) - W(0, 0, -1)));
   T ma4 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, 1)) + M(1, 0, 1)) + M(1, 0, 0));
   T ma8 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, 1)) + M(-1, 0, 1)) + M(-1, 0, 0));
   T ma7 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, 1)) + M(0, 1, 1)) + M(0, 1, 0));
   T ma9 = TC(0.25) * (((M(0, 0, 0) + M(0, 0, 1)) + M(0, -1, 1)) + M(0, -1, 0));
-  T RD1 = divx(p, (dwdxp * ma4 - dwdxm * ma8));
-  T RD2 = divx(p, (dudzp * ma4 - dudzm * ma8));
-  T RD3 = divy(p, (dwdyp * ma7 - dwdym * ma9));
-  T RD4 = divy(p, (dvdzp * ma7 - dvdzm * ma9));
-  T RD5 = divz(p, TC(2.) * (dwdzp * M(0, 0, 1) - dwdzm * M(0, 0, 0)));
+  T RD1 = divx<PW>(p, (dwdxp * ma4 - dwdxm * ma8));
+  T RD2 = divx<PW>(p, (dudzp * ma4 - dudzm * ma8));
+  T RD3 = divy<PW>(p, (dwdyp * ma7 - dwdym * ma9));
+  T RD4 = divy<PW>(p, (dvdzp * ma7 - dvdzm * ma9));
+  T RD5 = divz<PW>(p, TC(2.) * (dwdzp * M(0, 0, 1) - dwdzm * M(0, 0, 0)));
   T RDw = ((((RD1 + RD2) + RD3) + RD4) + RD5) / rw;
   if (p.iFr == 0. || p.g3 == 0.) return RCw + RDw * TC(p.visc);  // buoyancy as in rhs_u
   T RGw = TC(p.iFr) * (TC(1.) - rho_avr / rw) * TC(p.g3);
@@ -202,7 +202,7 @@ template <typename T>
 constexpr int ab2_smem() {
   return (int)(4 * MRING * MSY * MSX * sizeof(T) + 2 * MRING * MPY * MSX * sizeof(T));
 }
-template <typename T>
+template <typename T, int PW>
 __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
     k_ab2(Params p, MomArgs a, T* __restrict__ dudt, T* __restrict__ dvdt, T* __restrict__ dwdt,
           T* __restrict__ duold_out, T* __restrict__ dvold_out, T* __restrict__ dwold_out, int kc, int nch) {
@@ -304,9 +304,9 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
         return PT(2.) * (PT)pring[sl(dk)][ty + dj][tx + 1 + di] - (PT)pring[MRING + sl(dk)][ty + dj][tx + 1 + di];
       };
       const PT ph0 = PH(0, 0, 0);
-      const T Ru = rhs_u<T>(p, U, V, W, M, ru, rho_avr);
-      const T Rv = rhs_v<T>(p, U, V, W, M, rv, rho_avr);
-      const T Rw = rhs_w<T>(p, U, V, W, M, rw, rho_avr);
+      const T Ru = rhs_u<T, PW>(p, U, V, W, M, ru, rho_avr);
+      const T Rv = rhs_v<T, PW>(p, U, V, W, M, rv, rho_avr);
+      const T Rw = rhs_w<T, PW>(p, U, V, W, M, rw, rho_avr);
       const T du = ab2_update_v<T, PT>(p, U(0, 0, 0), Ru, ou, ru, PH(1, 0, 0), ph0, PT(2.) * qx - qxo, p.dxi);
       T dv = ab2_update_v<T, PT>(p, V(0, 0, 0), Rv, ov, rv, PH(0, 1, 0), ph0, PT(2.) * qy - qyo, p.dyi);
       if (p.forceytot != 0.) dv = dv - TC(p.forceytot * p.dt) / rv;  // constPoi driving (exact zero otherwise)
@@ -336,8 +336,8 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
 template <typename T>
 T* ab2_ptr(double* q) { return reinterpret_cast<T*>(q); }
 
-template <typename T>
-void ab2_launch(Ctx& c, const MomArgs& a, int o) {
+template <typename T, int PW>
+void ab2_launch_pw(Ctx& c, const MomArgs& a, int o) {
   // rows per block: 32 for the FP32 form (four blocks per SM, shorter
   // ring prologues), 16 for FP64 (two blocks per SM, more blocks per wave)
   const int kc = sizeof(T) == 8 ? 16 : 32, nch = std::max(1, c.P.kmax / kc);
@@ -346,12 +346,19 @@ void ab2_launch(Ctx& c, const MomArgs& a, int o) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (!(attr & (1u << (dev & 31)))) {
-    cudaFuncSetAttribute(k_ab2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ab2_smem<T>());
+    cudaFuncSetAttribute(k_ab2<T, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, ab2_smem<T>());
     attr |= 1u << (dev & 31);
   }
-  k_ab2<T><<<grid, dim3(MX, MY, 1), ab2_smem<T>(), c.s>>>(c.P, a, ab2_ptr<T>(c.dudt), ab2_ptr<T>(c.dvdt), ab2_ptr<T>(c.dwdt),
-                                               ab2_ptr<T>(c.duold[o]), ab2_ptr<T>(c.dvold[o]), ab2_ptr<T>(c.dwold[o]),
-                                               nch == 1 ? c.P.kmax : kc, nch);
+  k_ab2<T, PW><<<grid, dim3(MX, MY, 1), ab2_smem<T>(), c.s>>>(
+      c.P, a, ab2_ptr<T>(c.dudt), ab2_ptr<T>(c.dvdt), ab2_ptr<T>(c.dwdt), ab2_ptr<T>(c.duold[o]),
+      ab2_ptr<T>(c.dvold[o]), ab2_ptr<T>(c.dwold[o]), nch == 1 ? c.P.kmax : kc, nch);
+}
+// one instance per spacing case: with power-of-two spacings every a/dx is
+// the product, so neither the test nor the division is in the kernel
+template <typename T>
+void ab2_launch(Ctx& c, const MomArgs& a, int o) {
+  if (c.P.pow2) ab2_launch_pw<T, 1>(c, a, o);
+  else ab2_launch_pw<T, 0>(c, a, o);
 }
 
 #undef TC

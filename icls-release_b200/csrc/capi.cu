@@ -1692,14 +1692,13 @@ int icls_step(icls_ctx* h, int istep, int begin) {
   }
   launch_stream_vel(c);
   launch_ab2(c);
+  int add_pjump = 0;
   if (c.cfg.solveLS) {
     rc = gfm4p(c);
     if (rc) return rc;
-    launch_fillps(c, 1);  // fillps, then p = p + p_jump (main.f90:139-142)
-  } else {
-    launch_fillps(c, 0);
+    add_pjump = 1;  // fillps, then p = p + p_jump (main.f90:139-142)
   }
-  launch_solver2d(c, 1);   // solver2d + boundp(p)
+  launch_fillps_solver2d(c, 1, add_pjump);  // fillps + solver2d + boundp(p)
   if (c.P.bcy == ICLS_BCY_PERIODIC) {
     launch_correc(c, 1);   // correc + bounduvw + average_vel_at_center + NaN probe
   } else {                 // the y walls change vnew before the cell-centre averages

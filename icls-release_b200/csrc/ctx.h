@@ -272,6 +272,9 @@ void launch_gather_plane_x(Ctx& c, const double* d, bool f32, long long nx, long
 // Poisson (k_poisson.cu)
 void poisson_setup(Ctx& c);
 void launch_solver2d(Ctx& c, int write_halos);
+// fillps (+ p_jump when add) and solver2d, fillps folded into the solve's
+// first pass where it can be
+void launch_fillps_solver2d(Ctx& c, int write_halos, int add);
 void launch_disp(Ctx& c, int l);
 
 }  // namespace icls

@@ -64,13 +64,27 @@ template <typename T>
 __device__ __forceinline__ T sq(T x) { return x * x; }
 
 // a/dx, a/dy, a/dz exactly as the reference divides (a product when the
-// spacing is a power of two, which is then bit-identical)
-template <typename T>
-__device__ __forceinline__ T divx(const Params& p, T a) { return p.pow2 ? a * (T)p.rdx : a / (T)p.dx; }
-template <typename T>
-__device__ __forceinline__ T divy(const Params& p, T a) { return p.pow2 ? a * (T)p.rdy : a / (T)p.dy; }
-template <typename T>
-__device__ __forceinline__ T divz(const Params& p, T a) { return p.pow2 ? a * (T)p.rdz : a / (T)p.dz; }
+// spacing is a power of two, which is then bit-identical).  PW fixes the
+// choice at compile time for a kernel instantiated per case (1: the
+// spacings are powers of two, 0: they are not); -1 reads p.pow2.
+template <int PW = -1, typename T>
+__device__ __forceinline__ T divx(const Params& p, T a) {
+  if constexpr (PW == 1) return a * (T)p.rdx;
+  else if constexpr (PW == 0) return a / (T)p.dx;
+  else return p.pow2 ? a * (T)p.rdx : a / (T)p.dx;
+}
+template <int PW = -1, typename T>
+__device__ __forceinline__ T divy(const Params& p, T a) {
+  if constexpr (PW == 1) return a * (T)p.rdy;
+  else if constexpr (PW == 0) return a / (T)p.dy;
+  else return p.pow2 ? a * (T)p.rdy : a / (T)p.dy;
+}
+template <int PW = -1, typename T>
+__device__ __forceinline__ T divz(const Params& p, T a) {
+  if constexpr (PW == 1) return a * (T)p.rdz;
+  else if constexpr (PW == 0) return a / (T)p.dz;
+  else return p.pow2 ? a * (T)p.rdz : a / (T)p.dz;
+}
 // a / rho0: a product by the exact reciprocal when rho0 is a power of two
 __device__ __forceinline__ double div_rho0(const Params& p, double a) { return p.rho0_pow2 ? a * p.rrho0 : a / p.rho0; }
 

@@ -251,7 +251,7 @@ struct Axial19 {
 
 // dfdt of HOUC5_nb (hyperPDE.f90:397-495) or WENO5_nb (503-800) at row k
 // from its axial stencil S
-template <int SCHEME, typename T>
+template <int SCHEME, int PW = -1, typename T>
 __device__ __forceinline__ T adv_rhs(const Params& p, const Axial19<T>& S, T vu, T vv, T vw, int k) {
 #define PX(d) S.x[(d) + 3]
 #define PY(d) S.y[(d) + 3]
@@ -265,32 +265,32 @@ __device__ __forceinline__ T adv_rhs(const Params& p, const Axial19<T>& S, T vu,
         dfx = houc5_pos(PX(-3), PX(-2), PX(-1), PX(0), PX(1), PX(2));
       else
         dfx = houc5_neg(PX(3), PX(2), PX(1), PX(0), PX(-1), PX(-2));
-      udfdx = -divx(p, vu * dfx);
+      udfdx = -divx<PW>(p, vu * dfx);
     }
     if (vv >= TC(0.))
       dfy = houc5_pos(PY(-3), PY(-2), PY(-1), PY(0), PY(1), PY(2));
     else
       dfy = houc5_neg(PY(3), PY(2), PY(1), PY(0), PY(-1), PY(-2));
-    vdfdy = -divy(p, vv * dfy);
+    vdfdy = -divy<PW>(p, vv * dfy);
   } else {
     if (p.TwoD) {
       udfdx = TC(0.);
     } else {
       if (vu >= TC(0.))
-        dfx = weno5(divx(p, PX(-2) - PX(-3)), divx(p, PX(-1) - PX(-2)), divx(p, PX(0) - PX(-1)),
-                    divx(p, PX(1) - PX(0)), divx(p, PX(2) - PX(1)));
+        dfx = weno5(divx<PW>(p, PX(-2) - PX(-3)), divx<PW>(p, PX(-1) - PX(-2)), divx<PW>(p, PX(0) - PX(-1)),
+                    divx<PW>(p, PX(1) - PX(0)), divx<PW>(p, PX(2) - PX(1)));
       else
-        dfx = weno5(divx(p, PX(3) - PX(2)), divx(p, PX(2) - PX(1)), divx(p, PX(1) - PX(0)),
-                    divx(p, PX(0) - PX(-1)), divx(p, PX(-1) - PX(-2)));
+        dfx = weno5(divx<PW>(p, PX(3) - PX(2)), divx<PW>(p, PX(2) - PX(1)), divx<PW>(p, PX(1) - PX(0)),
+                    divx<PW>(p, PX(0) - PX(-1)), divx<PW>(p, PX(-1) - PX(-2)));
       udfdx = -(vu * dfx);
     }
     // y uses dx, as in the reference (hyperPDE.f90:622-626)
     if (vv >= TC(0.))
-      dfy = weno5(divx(p, PY(-2) - PY(-3)), divx(p, PY(-1) - PY(-2)), divx(p, PY(0) - PY(-1)),
-                  divx(p, PY(1) - PY(0)), divx(p, PY(2) - PY(1)));
+      dfy = weno5(divx<PW>(p, PY(-2) - PY(-3)), divx<PW>(p, PY(-1) - PY(-2)), divx<PW>(p, PY(0) - PY(-1)),
+                  divx<PW>(p, PY(1) - PY(0)), divx<PW>(p, PY(2) - PY(1)));
     else
-      dfy = weno5(divx(p, PY(3) - PY(2)), divx(p, PY(2) - PY(1)), divx(p, PY(1) - PY(0)),
-                  divx(p, PY(0) - PY(-1)), divx(p, PY(-1) - PY(-2)));
+      dfy = weno5(divx<PW>(p, PY(3) - PY(2)), divx<PW>(p, PY(2) - PY(1)), divx<PW>(p, PY(1) - PY(0)),
+                  divx<PW>(p, PY(0) - PY(-1)), divx<PW>(p, PY(-1) - PY(-2)));
     vdfdy = -(vv * dfy);
   }
   if (k > 2 && k < p.kmax - 1) {
@@ -299,14 +299,14 @@ __device__ __forceinline__ T adv_rhs(const Params& p, const Axial19<T>& S, T vu,
         dfz = houc5_pos(PZ(-3), PZ(-2), PZ(-1), PZ(0), PZ(1), PZ(2));
       else
         dfz = houc5_neg(PZ(3), PZ(2), PZ(1), PZ(0), PZ(-1), PZ(-2));
-      wdfdz = -divz(p, vw * dfz);
+      wdfdz = -divz<PW>(p, vw * dfz);
     } else {
       if (vw >= TC(0.))
-        dfz = weno5(divz(p, PZ(-2) - PZ(-3)), divz(p, PZ(-1) - PZ(-2)), divz(p, PZ(0) - PZ(-1)),
-                    divz(p, PZ(1) - PZ(0)), divz(p, PZ(2) - PZ(1)));
+        dfz = weno5(divz<PW>(p, PZ(-2) - PZ(-3)), divz<PW>(p, PZ(-1) - PZ(-2)), divz<PW>(p, PZ(0) - PZ(-1)),
+                    divz<PW>(p, PZ(1) - PZ(0)), divz<PW>(p, PZ(2) - PZ(1)));
       else
-        dfz = weno5(divz(p, PZ(3) - PZ(2)), divz(p, PZ(2) - PZ(1)), divz(p, PZ(1) - PZ(0)),
-                    divz(p, PZ(0) - PZ(-1)), divz(p, PZ(-1) - PZ(-2)));
+        dfz = weno5(divz<PW>(p, PZ(3) - PZ(2)), divz<PW>(p, PZ(2) - PZ(1)), divz<PW>(p, PZ(1) - PZ(0)),
+                    divz<PW>(p, PZ(0) - PZ(-1)), divz<PW>(p, PZ(-1) - PZ(-2)));
       wdfdz = -(vw * dfz);
     }
   } else if (k == 2 || k == p.kmax - 1) {  // HOUC3 near the walls
@@ -314,18 +314,18 @@ __device__ __forceinline__ T adv_rhs(const Params& p, const Axial19<T>& S, T vu,
       dfz = ((TC(1. / 6.) * PZ(-2) - PZ(-1)) + TC(1. / 2.) * PZ(0)) + TC(1. / 3.) * PZ(1);
     else
       dfz = ((-(TC(1. / 6.) * PZ(2)) + PZ(1)) - TC(1. / 2.) * PZ(0)) - TC(1. / 3.) * PZ(-1);
-    wdfdz = -divz(p, vw * dfz);
+    wdfdz = -divz<PW>(p, vw * dfz);
   } else {  // first-order upwinding at k=1,kmax
     if (vw >= TC(0.)) dfz = PZ(0) - PZ(-1);
     else dfz = PZ(1) - PZ(0);
-    wdfdz = -divz(p, vw * dfz);
+    wdfdz = -divz<PW>(p, vw * dfz);
   }
 #undef PX
 #undef PY
 #undef PZ
   return (udfdx + vdfdy) + wdfdz;
 }
-template <int SCHEME, typename T>
+template <int SCHEME, typename T, int PW>
 __global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 4 : 3)) k_adv_stage(Params p, const __grid_constant__ LsBatch B, int stage1,
                                                      double a_, double bb_, double fdt_, const T* __restrict__ vu,
                                                      const T* __restrict__ vv, const T* __restrict__ vw) {
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 4 : 3)) k_adv_stage(Para
         }
         S.x[3] = S.y[3] = S.z[3] = S.c;
         val = stage1 ? f0 : a * f0 + bb * S.c;
-        if (m) val = val + fdt * adv_rhs<SCHEME>(p, S, u, v, w, k);
+        if (m) val = val + fdt * adv_rhs<SCHEME, PW>(p, S, u, v, w, k);
       }
       if (k == 1) v1 = val;
       if (k == 2) v2 = val;
@@ -470,7 +470,7 @@ __global__ void __launch_bounds__(NT) k_adv_base(Params p, const __grid_constant
   }
 }
 
-template <int SCHEME, typename T>
+template <int SCHEME, typename T, int PW>
 __global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 4 : 3))
     k_adv_band(Params p, const __grid_constant__ LsBatch B, const BandCell* __restrict__ list,
                const int* __restrict__ count, double fdt_, const T* __restrict__ vu, const T* __restrict__ vv,
@@ -498,7 +498,7 @@ __global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 4 : 3))
     S.z[d + 3] = f[d * sz];
   }
   S.x[3] = S.y[3] = S.z[3] = S.c;
-  putL(p, out, i, j, k, base + fdt * adv_rhs<SCHEME>(p, S, vu[q], vv[q], vw[q], k));
+  putL(p, out, i, j, k, base + fdt * adv_rhs<SCHEME, PW>(p, S, vu[q], vv[q], vw[q], k));
 }
 
 template <typename T>
@@ -533,7 +533,7 @@ __device__ __forceinline__ T reinit_sgn(const Params& p, T p0) {
 }
 
 // RHS of WENO5_reinit at an interior cell (hyperPDE.f90:2646-2746)
-template <typename T>
+template <int PW, typename T>
 __device__ __forceinline__ T reinit_rhs(const Params& p, const T* __restrict__ phi, const T* __restrict__ orig,
                                         int i, int j, int k) {
   const long long c = idxL(p, i, j, k);
@@ -556,23 +556,23 @@ __device__ __forceinline__ T reinit_rhs(const Params& p, const T* __restrict__ p
   }
   T A = TC(0.), B = TC(0.), C, D, E, F;
   if (!p.TwoD) {
-    A = weno5(divx(p, PH(-2 * sx) - PH(-3 * sx)), divx(p, PH(-sx) - PH(-2 * sx)), divx(p, PH(0) - PH(-sx)),
-              divx(p, PH(sx) - PH(0)), divx(p, PH(2 * sx) - PH(sx)));
-    B = weno5(divx(p, PH(3 * sx) - PH(2 * sx)), divx(p, PH(2 * sx) - PH(sx)), divx(p, PH(sx) - PH(0)),
-              divx(p, PH(0) - PH(-sx)), divx(p, PH(-sx) - PH(-2 * sx)));
+    A = weno5(divx<PW>(p, PH(-2 * sx) - PH(-3 * sx)), divx<PW>(p, PH(-sx) - PH(-2 * sx)), divx<PW>(p, PH(0) - PH(-sx)),
+              divx<PW>(p, PH(sx) - PH(0)), divx<PW>(p, PH(2 * sx) - PH(sx)));
+    B = weno5(divx<PW>(p, PH(3 * sx) - PH(2 * sx)), divx<PW>(p, PH(2 * sx) - PH(sx)), divx<PW>(p, PH(sx) - PH(0)),
+              divx<PW>(p, PH(0) - PH(-sx)), divx<PW>(p, PH(-sx) - PH(-2 * sx)));
   }
-  C = weno5(divx(p, PH(-2 * sy) - PH(-3 * sy)), divx(p, PH(-sy) - PH(-2 * sy)), divx(p, PH(0) - PH(-sy)),
-            divx(p, PH(sy) - PH(0)), divx(p, PH(2 * sy) - PH(sy)));
-  D = weno5(divx(p, PH(3 * sy) - PH(2 * sy)), divx(p, PH(2 * sy) - PH(sy)), divx(p, PH(sy) - PH(0)),
-            divx(p, PH(0) - PH(-sy)), divx(p, PH(-sy) - PH(-2 * sy)));
+  C = weno5(divx<PW>(p, PH(-2 * sy) - PH(-3 * sy)), divx<PW>(p, PH(-sy) - PH(-2 * sy)), divx<PW>(p, PH(0) - PH(-sy)),
+            divx<PW>(p, PH(sy) - PH(0)), divx<PW>(p, PH(2 * sy) - PH(sy)));
+  D = weno5(divx<PW>(p, PH(3 * sy) - PH(2 * sy)), divx<PW>(p, PH(2 * sy) - PH(sy)), divx<PW>(p, PH(sy) - PH(0)),
+            divx<PW>(p, PH(0) - PH(-sy)), divx<PW>(p, PH(-sy) - PH(-2 * sy)));
   if (k >= 3 && k <= p.kmax - 2) {
-    E = weno5(divz(p, PH(-2 * sz) - PH(-3 * sz)), divz(p, PH(-sz) - PH(-2 * sz)), divz(p, PH(0) - PH(-sz)),
-              divz(p, PH(sz) - PH(0)), divz(p, PH(2 * sz) - PH(sz)));
-    F = weno5(divz(p, PH(3 * sz) - PH(2 * sz)), divz(p, PH(2 * sz) - PH(sz)), divz(p, PH(sz) - PH(0)),
-              divz(p, PH(0) - PH(-sz)), divz(p, PH(-sz) - PH(-2 * sz)));
+    E = weno5(divz<PW>(p, PH(-2 * sz) - PH(-3 * sz)), divz<PW>(p, PH(-sz) - PH(-2 * sz)), divz<PW>(p, PH(0) - PH(-sz)),
+              divz<PW>(p, PH(sz) - PH(0)), divz<PW>(p, PH(2 * sz) - PH(sz)));
+    F = weno5(divz<PW>(p, PH(3 * sz) - PH(2 * sz)), divz<PW>(p, PH(2 * sz) - PH(sz)), divz<PW>(p, PH(sz) - PH(0)),
+              divz<PW>(p, PH(0) - PH(-sz)), divz<PW>(p, PH(-sz) - PH(-2 * sz)));
   } else {
-    E = divz(p, PH(0) - PH(-sz));
-    F = divz(p, PH(sz) - PH(0));
+    E = divz<PW>(p, PH(0) - PH(-sz));
+    F = divz<PW>(p, PH(sz) - PH(0));
   }
 #undef PH
   const T s = reinit_sgn(p, orig[c]);
@@ -594,12 +594,12 @@ __device__ __forceinline__ T reinit_rhs(const Params& p, const T* __restrict__ p
 }
 
 // one SSP-RK3 stage value of ls_reinit (levelset.f90:800-810)
-template <typename T>
+template <int PW, typename T>
 __device__ __forceinline__ T reinit_val(const Params& p, int stage, const T* __restrict__ phi0,
                                         const T* __restrict__ phis, const T* __restrict__ orig, T dtau, int I, int J,
                                         int k) {
   const long long n = idxL(p, I, J, k);
-  const T rhs = (k >= 1 && k <= p.kmax) ? reinit_rhs(p, phis, orig, I, J, k) : TC(0.);
+  const T rhs = (k >= 1 && k <= p.kmax) ? reinit_rhs<PW>(p, phis, orig, I, J, k) : TC(0.);
   if (stage == 1) return phi0[n] + dtau * rhs;
   if (stage == 2) return TC(3. / 4.) * phi0[n] + TC(1. / 4.) * (phis[n] + dtau * rhs);
   return TC(1. / 3.) * phi0[n] + TC(2. / 3.) * (phis[n] + dtau * rhs);
@@ -607,7 +607,7 @@ __device__ __forceinline__ T reinit_val(const Params& p, int stage, const T* __r
 
 // One SSP-RK3 stage of ls_reinit over the tasks' regions; stage 3 folds
 // max|phi_new - phi_0| into the drop's residual.  out may equal phi0.
-template <typename T>
+template <typename T, int PW>
 __global__ void __launch_bounds__(NT, 2) k_reinit_stage(Params p, const __grid_constant__ LsBatch B, int stage,
                                                         double dtau_, ReinitState* __restrict__ rs) {
   const int ti = task_of(B);
@@ -642,7 +642,7 @@ __global__ void __launch_bounds__(NT, 2) k_reinit_stage(Params p, const __grid_c
       if (k == p.k1) {
         val = TC(2.) * vk - vkm;
       } else {
-        val = reinit_val(p, stage, phi0, phis, orig, dtau, i, j, k);
+        val = reinit_val<PW>(p, stage, phi0, phis, orig, dtau, i, j, k);
         if (k == 1) v1 = val;
         if (k == 2) v2 = val;
         if (k == p.kmax - 1) vkm = val;
@@ -1313,10 +1313,15 @@ void adv_launch(Ctx& c, const LsBatch& b, int scheme, int stage1, double a, doub
   const T* u = reinterpret_cast<const T*>(vu);
   const T* v = reinterpret_cast<const T*>(vv);
   const T* w = reinterpret_cast<const T*>(vw);
-  if (scheme == ICLS_HOUC5)
-    k_adv_stage<ICLS_HOUC5, T><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
-  else
-    k_adv_stage<ICLS_WENO5, T><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
+  // one instance per scheme and spacing case (PW: every a/dx a product)
+  const unsigned g = b.start[b.n];
+  if (scheme == ICLS_HOUC5) {
+    if (c.P.pow2) k_adv_stage<ICLS_HOUC5, T, 1><<<g, kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
+    else k_adv_stage<ICLS_HOUC5, T, 0><<<g, kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
+  } else {
+    if (c.P.pow2) k_adv_stage<ICLS_WENO5, T, 1><<<g, kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
+    else k_adv_stage<ICLS_WENO5, T, 0><<<g, kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
+  }
 }
 // the band list of a batch (its tasks' masks set): entries in c.band_list,
 // their number in c.band_count on the device; need = the upper bound the
@@ -1339,10 +1344,13 @@ void adv_split_launch(Ctx& c, const LsBatch& b, int scheme, int stage1, double a
   const unsigned nb = (unsigned)((need + NT - 1) / NT);
   k_adv_base<T><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage1, a, bb);
   if (nb > 0) {
-    if (scheme == ICLS_HOUC5)
-      k_adv_band<ICLS_HOUC5, T><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
-    else
-      k_adv_band<ICLS_WENO5, T><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
+    if (scheme == ICLS_HOUC5) {
+      if (c.P.pow2) k_adv_band<ICLS_HOUC5, T, 1><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
+      else k_adv_band<ICLS_HOUC5, T, 0><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
+    } else {
+      if (c.P.pow2) k_adv_band<ICLS_WENO5, T, 1><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
+      else k_adv_band<ICLS_WENO5, T, 0><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
+    }
   }
   k_adv_walls<T><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b);
 }
@@ -1366,8 +1374,13 @@ void launch_adv_stage(Ctx& c, const LsBatch& b, int scheme, int stage1, double a
 void launch_reinit_stage(Ctx& c, const LsBatch& b, int stage, double dtau) {
   if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "reinit_stage", 1);
-  BY_FORM(c, (k_reinit_stage<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs)),
-          (k_reinit_stage<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs)));
+  const unsigned g = b.start[b.n];
+  if (c.P.pow2)
+    BY_FORM(c, (k_reinit_stage<float, 1><<<g, kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs)),
+            (k_reinit_stage<double, 1><<<g, kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs)));
+  else
+    BY_FORM(c, (k_reinit_stage<float, 0><<<g, kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs)),
+            (k_reinit_stage<double, 0><<<g, kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs)));
 }
 void launch_reinit_reset(Ctx& c, const LsBatch& b, int maxiter) {
   if (b.n == 0) return;

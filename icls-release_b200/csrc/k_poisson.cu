@@ -10,7 +10,9 @@
 // (fft.f:403-452).  The 2decomp transposes of the reference
 // (transpose_*.f90) are replaced by the access pattern of each kernel: the
 // x pass streams contiguous lines, the y pass loads 16-wide column tiles,
-// the z pass walks k with one thread per (i,j).
+// the z pass walks k with one thread per (i,j).  In the fused time step the
+// forward x pass forms fillps' right-hand side itself from the predicted
+// velocities (and p_jump), so p is not written and read back in between.
 //
 // Two real lines share one complex FFT (z = a + i b).  Lines of 64, 128 or
 // 256 points, and of 48, 96, 192 or 384 (a radix-3 factor), take the
@@ -20,6 +22,7 @@
 // radix-R2 DFT in registers; other powers of two take radix-2 passes in
 // shared memory (k_fft_x, k_fft_y).
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "ctx.h"
@@ -333,18 +336,43 @@ __device__ __forceinline__ void reg_dft(double2 (&x)[R], const double2* __restri
   for (int n = 0; n < R; ++n) x[n] = y[n];
 }
 
+// The Poisson right-hand side of fillps (fillps.f90:36-53), plus p_jump when
+// add is set, at shape-C index c from the predicted velocities of type T
+// (float in the FP32 form): the expression of k_fillps, so the same bits.
+struct RhsArgs {
+  const void *du, *dv, *dw;
+  const double* pj;
+  int add;
+};
+template <typename T>
+__device__ __forceinline__ double rhs_at(const Params& p, const RhsArgs& r, long long c) {
+  const T* __restrict__ du = static_cast<const T*>(r.du);
+  const T* __restrict__ dv = static_cast<const T*>(r.dv);
+  const T* __restrict__ dw = static_cast<const T*>(r.dw);
+  const double coef = p.rho0 / p.dt;
+  const double vel_x = ((double)du[c] - (double)du[c - 1]) * p.dxi;
+  const double vel_y = ((double)dv[c] - (double)dv[c - p.nCx]) * p.dyi;
+  const double vel_z = ((double)dw[c] - (double)dw[c - (long long)p.nCx * p.nCy]) * p.dzi;
+  double v = coef * ((vel_x + vel_y) + vel_z);
+  if (r.add) v = v + r.pj[c];
+  return v;
+}
+
 // One CTA transforms LPC complex lines (2 LPC real lines).  YPASS false:
 // x lines (j,k), contiguous; the R lanes of a line are adjacent threads.
 // YPASS true: columns (i,k), columns adjacent in memory; the lines of a CTA
 // are adjacent threads.  dir 0: p (x) or spec (y) -> half-complex spec;
 // dir 1: the inverse, into spec (y) or p (x, with the boundp images when
-// halos is set).
+// halos is set).  RHS (forward x pass only): 0 reads p; 4 or 8 forms
+// fillps' right-hand side from float or double velocities instead (rhs_at),
+// so p is neither written by fillps nor read here.
 // LPC complex lines per CTA of 256 threads, TPL = max(R1, R2) threads per
 // line; LPC * TPL <= 256 (the other threads idle)
-template <int R1, int R2, bool YPASS, int LPC>
+template <int R1, int R2, bool YPASS, int LPC, int RHS = 0>
 __global__ void __launch_bounds__(256, (R1 > 16 || R2 > 16) ? 1 : 2)
     k_fft2(Params p, int dir, const double2* __restrict__ tw, double* __restrict__ pp, double* __restrict__ spec,
-           int halos) {
+           int halos, RhsArgs ra) {
+  static_assert(RHS == 0 || !YPASS, "the right-hand side is formed in the forward x pass");
   constexpr int N = R1 * R2;
   constexpr int TPL = R1 > R2 ? R1 : R2;
   static_assert(LPC * TPL <= 256, "a CTA holds LPC lines of TPL threads");
@@ -394,7 +422,12 @@ __global__ void __launch_bounds__(256, (R1 > 16 || R2 > 16) ? 1 : 2)
 #pragma unroll
     for (int n1 = 0; n1 < R1; ++n1) {
       const int n = R2 * n1 + lane;
-      x[n1] = dir == 0 ? make_double2(A[n * st], B[n * st]) : pack_hc(A, B, N, n, st);
+      if constexpr (RHS != 0) {  // dir 0: lines a and b start at columns 1 of (ja,ka), (jb,kb)
+        using T = typename std::conditional<RHS == 4, float, double>::type;
+        x[n1] = make_double2(rhs_at<T>(p, ra, idxC(p, 1, ja, ka) + n), rhs_at<T>(p, ra, idxC(p, 1, jb, kb) + n));
+      } else {
+        x[n1] = dir == 0 ? make_double2(A[n * st], B[n * st]) : pack_hc(A, B, N, n, st);
+      }
     }
     reg_dft<R1>(x, tw, N, dir);
 #pragma unroll
@@ -842,45 +875,54 @@ static int y_tile(int imax) {
   return ti;
 }
 
-template <int R1, int R2, bool Y, int LPC>
-void fft2_launch(Ctx& c, int dir, const double2* tw, int halos) {
+template <int R1, int R2, bool Y, int LPC, int RHS = 0>
+void fft2_launch(Ctx& c, int dir, const double2* tw, int halos, const RhsArgs& ra) {
   const Params& P = c.P;
   static unsigned attr = 0;  // devices this instance's shared-memory limit is raised on
   int dev = 0;
   cudaGetDevice(&dev);
   if (!(attr & (1u << (dev & 31)))) {
-    cudaFuncSetAttribute(k_fft2<R1, R2, Y, LPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_fft2<R1, R2, Y, LPC, RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)fft2_smem<R1, R2, LPC>());
     attr |= 1u << (dev & 31);
   }
   const long long units = Y ? (long long)(P.imax / (2 * LPC)) * P.kmax
                             : ((long long)P.jmax * P.kmax + 2 * LPC - 1) / (2 * LPC);
-  k_fft2<R1, R2, Y, LPC><<<(unsigned)units, 256, fft2_smem<R1, R2, LPC>(), c.s>>>(P, dir, tw, c.p, c.spec, halos);
+  k_fft2<R1, R2, Y, LPC, RHS>
+      <<<(unsigned)units, 256, fft2_smem<R1, R2, LPC>(), c.s>>>(P, dir, tw, c.p, c.spec, halos, ra);
 }
 // the lengths with a radix-3 factor: 16 lines per CTA where the columns tile
 // by 32 (y pass) and the lines need at most 16 threads, else 8
-template <int R2, bool Y>
-void fft2_launch3(Ctx& c, int dir, const double2* tw, int halos) {
-  if (R2 <= 16 && (!Y || c.P.imax % 32 == 0)) fft2_launch<16, R2, Y, R2 <= 16 ? 16 : 8>(c, dir, tw, halos);
-  else fft2_launch<16, R2, Y, 8>(c, dir, tw, halos);
+template <int R2, bool Y, int RHS = 0>
+void fft2_launch3(Ctx& c, int dir, const double2* tw, int halos, const RhsArgs& ra) {
+  if (R2 <= 16 && (!Y || c.P.imax % 32 == 0)) fft2_launch<16, R2, Y, R2 <= 16 ? 16 : 8, RHS>(c, dir, tw, halos, ra);
+  else fft2_launch<16, R2, Y, 8, RHS>(c, dir, tw, halos, ra);
 }
 
 // the two-level transform of one pass if its length has one (and, for the
-// y pass, the columns tile the CTAs); false: the radix-2 kernels
-template <bool Y>
-bool fft2_pass(Ctx& c, int dir, int halos) {
+// y pass, the columns tile the CTAs); false: the radix-2 kernels.  RHS (the
+// forward x pass): fillps' right-hand side formed in the pass (k_fft2).
+template <bool Y, int RHS = 0>
+bool fft2_pass(Ctx& c, int dir, int halos, const RhsArgs& ra = RhsArgs{}) {
   const Params& P = c.P;
   const int N = Y ? P.jmax : P.imax;
   const double2* tw = Y ? c.twy : c.twx;
   auto fits = [&](int lpc) { return !Y || P.imax % (2 * lpc) == 0; };
   switch (N) {
-    case 64: if (!fits(16)) return false; fft2_launch<16, 4, Y, 16>(c, dir, tw, halos); return true;
-    case 128: if (!fits(16)) return false; fft2_launch<16, 8, Y, 16>(c, dir, tw, halos); return true;
-    case 256: if (!fits(16)) return false; fft2_launch<16, 16, Y, 16>(c, dir, tw, halos); return true;
-    case 48: if (!fits(8)) return false; fft2_launch3<3, Y>(c, dir, tw, halos); return true;
-    case 96: if (!fits(8)) return false; fft2_launch3<6, Y>(c, dir, tw, halos); return true;
-    case 192: if (!fits(8)) return false; fft2_launch3<12, Y>(c, dir, tw, halos); return true;
-    case 384: if (!fits(8)) return false; fft2_launch3<24, Y>(c, dir, tw, halos); return true;
+    case 64: if (!fits(16)) return false; fft2_launch<16, 4, Y, 16, RHS>(c, dir, tw, halos, ra); return true;
+    case 128: if (!fits(16)) return false; fft2_launch<16, 8, Y, 16, RHS>(c, dir, tw, halos, ra); return true;
+    case 256: if (!fits(16)) return false; fft2_launch<16, 16, Y, 16, RHS>(c, dir, tw, halos, ra); return true;
+    case 48: if (!fits(8)) return false; fft2_launch3<3, Y, RHS>(c, dir, tw, halos, ra); return true;
+    case 96: if (!fits(8)) return false; fft2_launch3<6, Y, RHS>(c, dir, tw, halos, ra); return true;
+    case 192: if (!fits(8)) return false; fft2_launch3<12, Y, RHS>(c, dir, tw, halos, ra); return true;
+    case 384: if (!fits(8)) return false; fft2_launch3<24, Y, RHS>(c, dir, tw, halos, ra); return true;
+    default: return false;
+  }
+}
+// x line lengths the two-level transform takes
+bool fft2_x_length(int n) {
+  switch (n) {
+    case 64: case 128: case 256: case 48: case 96: case 192: case 384: return true;
     default: return false;
   }
 }
@@ -898,11 +940,27 @@ bool fft_length_ok(int n, bool y_pass, int imax) {
 }
 
 void launch_solver2d_cos(Ctx& c, int write_halos);
+void solver2d_periodic(Ctx& c, int write_halos, const RhsArgs* ra);
 void launch_solver2d(Ctx& c, int write_halos) {
   if (c.P.bcy != ICLS_BCY_PERIODIC) {
     launch_solver2d_cos(c, write_halos);
     return;
   }
+  solver2d_periodic(c, write_halos, nullptr);
+}
+// fillps (+ p_jump when add) and solver2d: the right-hand side formed in the
+// forward x pass where that pass is the two-level transform, else fillps
+// into p first
+void launch_fillps_solver2d(Ctx& c, int write_halos, int add) {
+  if (c.P.bcy != ICLS_BCY_PERIODIC || !fft2_x_length(c.P.imax)) {
+    launch_fillps(c, add);
+    launch_solver2d(c, write_halos);
+    return;
+  }
+  RhsArgs ra{c.dudt, c.dvdt, c.dwdt, c.pjump, add};
+  solver2d_periodic(c, write_halos, &ra);
+}
+void solver2d_periodic(Ctx& c, int write_halos, const RhsArgs* ra) {
   Scope sc_(c.prof, c.s, "solver2d", 5);
   const Params& P = c.P;
   const int lx = ilog2(P.imax), ly = ilog2(P.jmax);
@@ -921,7 +979,12 @@ void launch_solver2d(Ctx& c, int write_halos) {
     cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr |= 1u << (dev & 31);
   }
-  if (!fft2_pass<false>(c, 0, 0)) k_fft_x<<<gx, FT, smx, c.s>>>(P, 0, CL, lx, c.twx, c.p, c.spec, 0);
+  if (ra) {  // fft2_x_length(imax): the two-level x pass exists
+    if (P.f32) fft2_pass<false, 4>(c, 0, 0, *ra);
+    else fft2_pass<false, 8>(c, 0, 0, *ra);
+  } else if (!fft2_pass<false>(c, 0, 0)) {
+    k_fft_x<<<gx, FT, smx, c.s>>>(P, 0, CL, lx, c.twx, c.p, c.spec, 0);
+  }
   if (!fft2_pass<true>(c, 0, 0)) k_fft_y<<<gy, FT, smy, c.s>>>(P, 0, TI, ly, c.twy, c.spec);
   const long long nxy = (long long)P.imax * P.jmax;
   k_thomas<<<(unsigned)((nxy + 127) / 128), 128, 0, c.s>>>(P, c.tri_a, c.tri_c, c.zpiv, c.spec);

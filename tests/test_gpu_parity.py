@@ -213,11 +213,14 @@ def test_solver2d_lengths(ni, nj, nk):
     assert np.max(np.abs(pg - po)) <= 1e-11 * np.max(np.abs(po))
 
 
+@pytest.mark.parametrize("n", [32, 48])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_fused_step_equals_call_sequence(precision):
+def test_fused_step_equals_call_sequence(precision, n):
     """icls_step (fused kernels) == the main.f90 sequence of separate calls,
-    in FP64 and in the FP32 form."""
-    cfg, ls = drop_case(L=2, reinit_step=2, inflate_step=2)
+    in FP64 and in the FP32 form.  At n = 48 the fused step forms fillps'
+    right-hand side inside the solve's forward x pass (the two-level
+    transform); at n = 32 (radix-2 passes) fillps writes p first."""
+    cfg, ls = drop_case(n=n, L=2, reinit_step=2, inflate_step=2)
     cfg.precision = precision
     u, v, w = smooth_velocity(cfg, amp=0.3, seed=8)
     a = Solver(cfg)
