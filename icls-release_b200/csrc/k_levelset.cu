@@ -903,6 +903,57 @@ __global__ void __launch_bounds__(NT) k_materials_final(Params p, const T* __res
   }
 }
 
+// k_materials_final over two rows per thread (k0 = 2 blockIdx.z and k0 + 1):
+// both rows' jiemian values are read before any store, so a thread has its
+// two cells' loads in flight at once; the same expressions per cell
+template <typename T>
+__device__ __forceinline__ void materials_cell(const Params& p, long long n, long long q, bool in, T J0, T Jx, T Jy,
+                                               T Jz, T* __restrict__ miu, T* __restrict__ rho, T* __restrict__ rho_u,
+                                               T* __restrict__ rho_v, T* __restrict__ rho_w) {
+  const T rho1 = TC(p.rho1), rho2 = TC(p.rho2);
+  miu[n] = TC(p.miu1) * J0 + TC(p.miu2) * (TC(1.) - J0);
+  const T r0v = rho1 * J0 + rho2 * (TC(1.) - J0);
+  rho[n] = r0v;
+  if (!in) return;
+  if (p.rho1 == p.rho2) {
+    rho_u[q] = rho1; rho_v[q] = rho1; rho_w[q] = rho1;
+  } else {
+    const T rx = rho1 * Jx + rho2 * (TC(1.) - Jx);
+    const T ry = rho1 * Jy + rho2 * (TC(1.) - Jy);
+    const T rz = rho1 * Jz + rho2 * (TC(1.) - Jz);
+    rho_u[q] = (r0v + rx) / TC(2.);
+    rho_v[q] = (r0v + ry) / TC(2.);
+    rho_w[q] = (r0v + rz) / TC(2.);
+  }
+}
+template <typename T>
+__global__ void __launch_bounds__(NT) k_materials_rows2(Params p, const T* __restrict__ jiemian, T* __restrict__ miu,
+                                                        T* __restrict__ rho, T* __restrict__ rho_u,
+                                                        T* __restrict__ rho_v, T* __restrict__ rho_w) {
+  const int i = (int)(blockIdx.x * BX + threadIdx.x), j = (int)(blockIdx.y * BY + threadIdx.y);
+  const int k0 = 2 * (int)blockIdx.z;
+  if (i > p.i1 || j > p.j1) return;
+  const bool two = k0 + 1 <= p.k1;
+  const long long sz = (long long)p.nCx * p.nCy;
+  const long long n0 = idxC(p, i, j, k0), n1 = n0 + sz;
+  const bool in0 = interior(p, i, j, k0), in1 = two && interior(p, i, j, k0 + 1);
+  const T Ja = jiemian[n0];
+  const T Jb = two ? jiemian[n1] : TC(0.);
+  T Jxa = TC(0.), Jya = TC(0.), Jxb = TC(0.), Jyb = TC(0.), Jzb = TC(0.);
+  if (in0) {
+    Jxa = jiemian[n0 + 1];
+    Jya = jiemian[n0 + p.nCx];
+  }
+  if (in1) {
+    Jxb = jiemian[n1 + 1];
+    Jyb = jiemian[n1 + p.nCx];
+    Jzb = jiemian[n1 + sz];
+  }
+  materials_cell<T>(p, n0, in0 ? idxI(p, i, j, k0) : 0, in0, Ja, Jxa, Jya, Jb, miu, rho, rho_u, rho_v, rho_w);
+  if (two)
+    materials_cell<T>(p, n1, in1 ? idxI(p, i, j, k0 + 1) : 0, in1, Jb, Jxb, Jyb, Jzb, miu, rho, rho_u, rho_v, rho_w);
+}
+
 // ------------------------------------------------------------ inflation
 // dheav with boundp semantics over the task's shape-C region (one task),
 // the far-field value 1 on its apron, and per-tile area/volume sums (FP64)
@@ -1435,13 +1486,22 @@ void launch_materials_final(Ctx& c, const double* outside, const int* ntiles) {
   }
   k_volumes<<<1, 256, 0, c.s>>>(c.P, hparts(c), c.red_cap, o, uniform, c.dvol, c.dsc);
   const int r0[3] = {0, 0, 0}, r1[3] = {c.P.i1, c.P.j1, c.P.k1};
+  dim3 g2 = grid_of(r0, r1);
+  g2.z = (g2.z + 1) / 2;  // two rows per thread
   if (c.P.f32) {
     auto f = [](double* q) { return reinterpret_cast<float*>(q); };
-    k_materials_final<float><<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, f(c.jiemian), f(c.miu), f(c.rho), f(c.rho_u),
-                                                                   f(c.rho_v), f(c.rho_w));
+    if (c.materials_rows1)
+      k_materials_final<float><<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, f(c.jiemian), f(c.miu), f(c.rho),
+                                                                     f(c.rho_u), f(c.rho_v), f(c.rho_w));
+    else
+      k_materials_rows2<float><<<g2, kBlock, 0, c.s>>>(c.P, f(c.jiemian), f(c.miu), f(c.rho), f(c.rho_u),
+                                                       f(c.rho_v), f(c.rho_w));
   } else {
-    k_materials_final<double><<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, c.jiemian, c.miu, c.rho, c.rho_u, c.rho_v,
-                                                                    c.rho_w);
+    if (c.materials_rows1)
+      k_materials_final<double><<<grid_of(r0, r1), kBlock, 0, c.s>>>(c.P, c.jiemian, c.miu, c.rho, c.rho_u,
+                                                                      c.rho_v, c.rho_w);
+    else
+      k_materials_rows2<double><<<g2, kBlock, 0, c.s>>>(c.P, c.jiemian, c.miu, c.rho, c.rho_u, c.rho_v, c.rho_w);
   }
 }
 

@@ -174,6 +174,69 @@ __global__ void __launch_bounds__(NT) k_correc_fused(Params p, CorrArgs a) {
   }
 }
 
+// One correc value (correc.f90:27-39) at shape-C index c: d - dt dhi
+// ((p(c+off) - p(c)) - jump) / rho0, the expression of corr_u/v/w, with
+// the division by rho0 chosen at compile time (RP 1: rho0 a power of two,
+// the product by its exact reciprocal)
+template <typename T, int RP>
+__device__ __forceinline__ T corr_at(const Params& p, const T* __restrict__ d, const double* __restrict__ pp,
+                                     const T* __restrict__ jump, long long c, long long off, double dhi) {
+  const double a = p.dt * dhi * ((pp[c + off] - pp[c]) - (double)jump[c]);
+  const double g = RP == 1 ? a * p.rrho0 : a / p.rho0;
+  if (sizeof(T) == sizeof(double)) return (T)((double)d[c] - g);
+  return d[c] - (T)g;
+}
+
+// k_correc_fused's fields with one thread per interior cell: the thread
+// writes its cell's u, v, w with their periodic images (putC), at k = 1 and
+// k = kmax the wall rows k = 0 and k1 with theirs, and the cell-centre
+// velocities.  The halo and wall cells are the images k_correc_fused
+// computes from the same source cells, so the fields are the same bits;
+// every warp is a full row segment and no thread recomputes a source
+// column's corrections for a halo cell.
+template <typename T, int RP>
+__global__ void __launch_bounds__(NT) k_correc_own(Params p, CorrArgs a) {
+  int i, j, k;
+  if (!cell3(kI0, cI1(p).v, i, j, k)) return;
+  const long long sy = p.nCx, sz = (long long)p.nCx * p.nCy;
+  const long long c = idxC(p, i, j, k);
+  const T* __restrict__ du = cT<T>(a.dudt);
+  const T* __restrict__ dv = cT<T>(a.dvdt);
+  const T* __restrict__ dw = cT<T>(a.dwdt);
+  const T* __restrict__ px = cT<T>(a.px);
+  const T* __restrict__ py = cT<T>(a.py);
+  const T* __restrict__ pz = cT<T>(a.pz);
+  const double* __restrict__ pp = a.p;
+  const T uu = corr_at<T, RP>(p, du, pp, px, c, 1, p.dxi);
+  const T vv = corr_at<T, RP>(p, dv, pp, py, c, sy, p.dyi);
+  const T ww = (k == p.kmax) ? TC(0.) : corr_at<T, RP>(p, dw, pp, pz, c, sz, p.dzi);
+  // the cell-centre average's (i-1), (j-1) and (k-1) corrections
+  const T um = corr_at<T, RP>(p, du, pp, px, idxC(p, wrapx(p, i - 1), j, k), 1, p.dxi);
+  const T vm = corr_at<T, RP>(p, dv, pp, py, idxC(p, i, wrapy(p, j - 1), k), sy, p.dyi);
+  const T wm = (k == 1) ? TC(0.) : corr_at<T, RP>(p, dw, pp, pz, c - sz, sz, p.dzi);
+  T* u = mT<T>(a.u);
+  T* v = mT<T>(a.v);
+  T* w = mT<T>(a.w);
+  putC(p, u, i, j, k, uu);
+  putC(p, v, i, j, k, vv);
+  putC(p, w, i, j, k, ww);
+  if (k == 1) {
+    putC(p, u, i, j, 0, -uu);
+    putC(p, v, i, j, 0, TC(2. * p.v_lower) - vv);
+    putC(p, w, i, j, 0, TC(0.));
+  }
+  if (k == p.kmax) {
+    putC(p, u, i, j, p.k1, -uu);
+    putC(p, v, i, j, p.k1, TC(2. * p.v_upper) - vv);
+    putC(p, w, i, j, p.k1, corr_at<T, RP>(p, dw, pp, pz, c - sz, sz, p.dzi));
+  }
+  const long long q = idxI(p, i, j, k);
+  mT<T>(a.ucc)[q] = (um + uu) / TC(2.);
+  mT<T>(a.vcc)[q] = (vm + vv) / TC(2.);
+  mT<T>(a.wcc)[q] = (wm + ww) / TC(2.);
+  if (i == 1 && j == 1 && k == 1 && isnan(vv)) a.dsc->nan_flag = 1;
+}
+
 // bounduvw (bound.f90:15-177, Dirichl z, periodic x,y) on an existing triple
 template <typename T>
 __global__ void __launch_bounds__(NT) k_bounduvw(Params p, T* __restrict__ u, T* __restrict__ v, T* __restrict__ w) {
@@ -491,6 +554,19 @@ void launch_add_pjump(Ctx& c) {
 void launch_correc(Ctx& c, int fused_bc) {
   Scope sc_(c.prof, c.s, "correc", 1);
   CorrArgs a = corr_args(c);
+  // the fused form: one thread per interior cell writing the halo and wall
+  // images (ICLS_CORREC=shapec: one thread per shape-C cell)
+  if (fused_bc && !c.correc_shapec) {
+    const bool rp = c.P.rho0_pow2 != 0;
+    if (c.P.f32) {
+      if (rp) k_correc_own<float, 1><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);
+      else k_correc_own<float, 0><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);
+    } else {
+      if (rp) k_correc_own<double, 1><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);
+      else k_correc_own<double, 0><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);
+    }
+    return;
+  }
   if (c.P.f32) {
     if (fused_bc) k_correc_fused<float><<<gridC(c.P), kBlock, 0, c.s>>>(c.P, a);
     else k_correc_interior<float><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);

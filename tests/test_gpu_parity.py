@@ -505,3 +505,57 @@ def test_band_list_advection_bit_identical_to_column(monkeypatch):
         col.close()
         band.close()
 
+
+
+def test_correc_own_cells_bit_identical_to_shape_c(monkeypatch):
+    """The fused correction with one thread per interior cell writing the
+    halo and wall images gives the same bits as one thread per shape-C cell
+    (ICLS_CORREC=shapec): moving walls (the k = 0 and k1 rows), both forms."""
+    from icls_gpu import FP32
+    from icls_gpu.config import IclsConfig
+    cases = [multi_drop(n=64, ndrop=3, seed=7, steps=3, rmin=0.08, rmax=0.1, dt=2e-5), boxed_case(steps=3)]
+    f32 = boxed_case(steps=3)
+    f32.cfg = IclsConfig.from_buffer_copy(f32.cfg)
+    f32.cfg.precision = FP32
+    cases.append(f32)
+    for wl in cases:
+        cfg = wl.cfg
+        ls = init_drops(cfg, wl.centres, wl.radii, wl.all_images)
+        u, v, w = initial_velocity(cfg, wl.shear_v)
+        own = Solver(cfg)
+        monkeypatch.setenv("ICLS_CORREC", "shapec")
+        shc = Solver(cfg)
+        monkeypatch.delenv("ICLS_CORREC")
+        for s in (own, shc):
+            s.setup(ls, u, v, w)
+        for istep in range(1, 4):
+            own.step(istep, 0)
+            shc.step(istep, 0)
+        for name in ("u", "v", "w", "ucc", "vcc", "wcc", "pnew"):
+            assert np.array_equal(own.download(name), shc.download(name)), (wl.name, name)
+        own.close()
+        shc.close()
+
+
+def test_materials_two_rows_bit_identical(monkeypatch):
+    """The materials with two rows per thread give the same miu, rho and
+    face densities as one row per thread (ICLS_MATERIALS=rows1), at an odd
+    and an even number of shape-C rows, both forms."""
+    from icls_gpu import FP32
+    from icls_gpu.config import IclsConfig
+    for n, prec in ((32, 0), (48, 1), (64, 0)):
+        cfg, ls = drop_case(n=n, L=2)
+        cfg.ktot = n - 1 if n == 48 else n  # 49 or n + 2 shape-C rows
+        cfg.precision = prec
+        ls = init_drops(cfg, [(0.3, 0.3, 0.35), (0.7, 0.65, 0.6)], [0.15, 0.17], all_images=True)
+        two = Solver(cfg)
+        monkeypatch.setenv("ICLS_MATERIALS", "rows1")
+        one = Solver(cfg)
+        monkeypatch.delenv("ICLS_MATERIALS")
+        for s in (two, one):
+            s.setup(ls)
+            s.update_materials()
+        for name in ("miu", "rho", "rho_u", "rho_v", "rho_w"):
+            assert np.array_equal(two.download(name), one.download(name)), (n, name)
+        two.close()
+        one.close()
