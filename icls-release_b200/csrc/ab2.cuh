@@ -230,45 +230,53 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
   // aligned, and halve the copy instructions (1.37 -> 1.30 ms at 256^3).
   // FP32 keeps one 4-byte copy per element: at its 64-register budget the
   // pair loop spilled and measured slower (0.77 -> 0.84 ms).
+  // This thread's copy slots, the same for every row: slot r is element
+  // tid + r MX MY of a plane (a pair of elements in FP64), at plane offset
+  // gi + nCx gj of storage row 0 (row kk is kk nCx nCy further), -1 where
+  // the element lies outside the grid.  NS slots cover a plane.
+  constexpr int EPC = sizeof(T) == 8 ? 2 : 1;  // elements per copy
+  constexpr int RW = MSX / EPC;                // copies per plane row
+  constexpr int NS = (RW * MSY + MX * MY - 1) / (MX * MY);
+  int ro[NS], po[NS];
+#pragma unroll
+  for (int r = 0; r < NS; ++r) {
+    const int e = tid + r * MX * MY;
+    const int sy = e / RW, sx = EPC * (e - sy * RW);
+    const int gi = i0 - 1 + sx;
+    // gi even in FP64: gi + 1 <= imax + 1
+    const bool xin = sizeof(T) == 8 ? gi <= p.imax : gi <= p.imax + 1;
+    ro[r] = (e < RW * MSY && xin && j0 - 1 + sy <= p.jmax + 1) ? gi + p.nCx * (j0 - 1 + sy) : -1;
+    // pnew, pold rows start at j0; their column i0-1 is not read (FP32
+    // skips it, FP64 copies it with its pair)
+    po[r] = (e < RW * MPY && xin && j0 + sy <= p.jmax + 1 && (sizeof(T) == 8 || sx > 0)) ? gi + p.nCx * (j0 + sy)
+                                                                                        : -1;
+  }
+  const long long psz = (long long)p.nCx * p.nCy;
   auto issue_plane = [&](int kk) {
     const int s = kk & (MRING - 1);
-    if constexpr (sizeof(T) == 8) {
-      constexpr int NP = MSX / 2;
-      for (int e = tid; e < NP * MSY; e += MX * MY) {
-        const int sy = e / NP, sx = 2 * (e - sy * NP);
-        const int gi = i0 - 1 + sx, gj = j0 - 1 + sy;
-        if (gi <= p.imax && gj <= p.jmax + 1) {  // gi even: gi + 1 <= imax + 1
-          const long long g = idxC(p, gi, gj, kk);
+    const long long kb = (long long)kk * psz;
 #pragma unroll
-          for (int f = 0; f < 4; ++f) cp_async_pair(&ring[f * MRING + s][sy][sx], F[f] + g);
-        }
-      }
-      for (int e = tid; e < NP * MPY; e += MX * MY) {
-        const int sy = e / NP, sx = 2 * (e - sy * NP);
-        const int gi = i0 - 1 + sx, gj = j0 + sy;
-        if (gi <= p.imax && gj <= p.jmax + 1) {
-          const long long g = idxC(p, gi, gj, kk);
-          cp_async_pair(&pring[s][sy][sx], cT<T>(a.pnew) + g);
-          cp_async_pair(&pring[MRING + s][sy][sx], cT<T>(a.pold) + g);
-        }
-      }
-    } else {
-      for (int e = tid; e < MSX * MSY; e += MX * MY) {
-        const int sy = e / MSX, sx = e - sy * MSX;
-        const int gi = i0 - 1 + sx, gj = j0 - 1 + sy;
-        if (gi <= p.imax + 1 && gj <= p.jmax + 1) {
-          const long long g = idxC(p, gi, gj, kk);
+    for (int r = 0; r < NS; ++r) {
+      const int e = EPC * (tid + r * MX * MY);  // element offset in the plane
+      if (ro[r] >= 0) {
+        const long long g = kb + ro[r];
 #pragma unroll
-          for (int f = 0; f < 4; ++f) cp_async_el(&ring[f * MRING + s][sy][sx], F[f] + g);
+        for (int f = 0; f < 4; ++f) {
+          T* dst = &ring[f * MRING + s][0][0] + e;
+          if constexpr (sizeof(T) == 8) cp_async_pair(dst, F[f] + g);
+          else cp_async_el(dst, F[f] + g);
         }
       }
-      for (int e = tid; e < MSX * MPY; e += MX * MY) {
-        const int sy = e / MSX, sx = e - sy * MSX;
-        const int gi = i0 - 1 + sx, gj = j0 + sy;
-        if (sx > 0 && gi <= p.imax + 1 && gj <= p.jmax + 1) {  // column i0-1 is not read
-          const long long g = idxC(p, gi, gj, kk);
-          cp_async_el(&pring[s][sy][sx], cT<T>(a.pnew) + g);
-          cp_async_el(&pring[MRING + s][sy][sx], cT<T>(a.pold) + g);
+      if (po[r] >= 0) {
+        const long long g = kb + po[r];
+        T* d0 = &pring[s][0][0] + e;
+        T* d1 = &pring[MRING + s][0][0] + e;
+        if constexpr (sizeof(T) == 8) {
+          cp_async_pair(d0, cT<T>(a.pnew) + g);
+          cp_async_pair(d1, cT<T>(a.pold) + g);
+        } else {
+          cp_async_el(d0, cT<T>(a.pnew) + g);
+          cp_async_el(d1, cT<T>(a.pold) + g);
         }
       }
     }
