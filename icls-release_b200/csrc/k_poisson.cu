@@ -595,96 +595,6 @@ __device__ __forceinline__ void thomas_line(double* __restrict__ col, long long 
       }
   }
 }
-// thomas_line with each thread's rows streamed through a ring of TD rows in
-// shared memory by asynchronous copies issued TD rows ahead: the forward
-// sweep's line and pivots, then the back substitution's (the values the
-// forward sweep stored and the pivots, in descending rows).  A thread only
-// reads its own slots, so no barrier is needed: one copy group per row, and
-// wait_group(TD - 1) before a row is used.  The same operations in the same
-// order as thomas_line.
-constexpr int TD = 16;
-__device__ __forceinline__ void cp8(double* dst, const double* src) {
-  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_wait_ring() { asm volatile("cp.async.wait_group %0;" ::"n"(TD - 1) : "memory"); }
-__device__ __forceinline__ void thomas_ring(double* __restrict__ col, long long st, int K,
-                                            const double* __restrict__ zc, long long nd,
-                                            const double* __restrict__ a, const double* __restrict__ c,
-                                            double* __restrict__ sv, double* __restrict__ sz) {
-  // slot s of this thread: sv[s * 128], sz[s * 128]
-  // forward: rows m = 0..K-1 (k = m + 1)
-#pragma unroll 1
-  for (int m = 0; m < TD; ++m) {
-    if (m < K) {
-      cp8(sv + m * 128, col + m * st);
-      cp8(sz + m * 128, zc + m * nd);
-    }
-    cp_commit();
-  }
-  double prev = 0.;
-#pragma unroll 1
-  for (int m = 0; m < K; ++m) {
-    cp_wait_ring();
-    const int s = m % TD;
-    const double cv = sv[s * 128], zv = sz[s * 128];
-    if (m == 0) {
-      prev = cv * zv;
-      col[0] = prev;
-    } else if (m < K - 1) {
-      const double v = (cv - a[m + 1] * prev) * zv;
-      col[m * st] = v;
-      prev = v;
-    } else {  // the last row: the zero-pivot rule
-      prev = zv != 0. ? (cv - a[K] * prev) / zv : 0.;
-      col[m * st] = prev;
-    }
-    if (m + TD < K) {
-      cp8(sv + s * 128, col + (m + TD) * st);
-      cp8(sz + s * 128, zc + (m + TD) * nd);
-    }
-    cp_commit();
-  }
-  // back substitution: rows m = K-2 .. 0 (k = m + 1), nxt = row m + 1
-  double nxt = prev;
-#pragma unroll 1
-  for (int t = 0; t < TD; ++t) {
-    const int m = K - 2 - t;
-    if (m >= 0) {
-      cp8(sv + t * 128, col + m * st);
-      cp8(sz + t * 128, zc + m * nd);
-    }
-    cp_commit();
-  }
-#pragma unroll 1
-  for (int t = 0; t < K - 1; ++t) {
-    cp_wait_ring();
-    const int m = K - 2 - t, s = t % TD;
-    const double cv = sv[s * 128], zv = sz[s * 128];
-    const double d = c[m + 1] * zv;
-    const double v = cv - d * nxt;
-    col[m * st] = v;
-    nxt = v;
-    if (m - TD >= 0) {
-      cp8(sv + s * 128, col + (m - TD) * st);
-      cp8(sz + s * 128, zc + (m - TD) * nd);
-    }
-    cp_commit();
-  }
-  asm volatile("cp.async.wait_all;" ::: "memory");
-}
-__global__ void __launch_bounds__(128) k_thomas_ring(Params p, const double* __restrict__ a,
-                                                     const double* __restrict__ c, const double* __restrict__ zpiv,
-                                                     double* __restrict__ spec) {
-  __shared__ double ring[2 * TD * 128];
-  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long nxy = (long long)p.imax * p.jmax, nd = pivot_columns(p);
-  if (q >= nxy) return;
-  const int i = (int)(q % p.imax) + 1, j = (int)(q / p.imax) + 1;
-  thomas_ring(spec + q, nxy, p.kmax, zpiv + (i >> 1) + (long long)(p.imax / 2 + 1) * (j >> 1), nd, a, c,
-              ring + threadIdx.x, ring + TD * 128 + threadIdx.x);
-}
 // solver2d: lines along z, one thread per (i,j)
 __global__ void __launch_bounds__(128) k_thomas(Params p, const double* __restrict__ a, const double* __restrict__ c,
                                                 const double* __restrict__ zpiv, double* __restrict__ spec) {
@@ -1077,8 +987,7 @@ void solver2d_periodic(Ctx& c, int write_halos, const RhsArgs* ra) {
   }
   if (!fft2_pass<true>(c, 0, 0)) k_fft_y<<<gy, FT, smy, c.s>>>(P, 0, TI, ly, c.twy, c.spec);
   const long long nxy = (long long)P.imax * P.jmax;
-  if (c.thomas_regs) k_thomas<<<(unsigned)((nxy + 127) / 128), 128, 0, c.s>>>(P, c.tri_a, c.tri_c, c.zpiv, c.spec);
-  else k_thomas_ring<<<(unsigned)((nxy + 127) / 128), 128, 0, c.s>>>(P, c.tri_a, c.tri_c, c.zpiv, c.spec);
+  k_thomas<<<(unsigned)((nxy + 127) / 128), 128, 0, c.s>>>(P, c.tri_a, c.tri_c, c.zpiv, c.spec);
   if (!fft2_pass<true>(c, 1, 0)) k_fft_y<<<gy, FT, smy, c.s>>>(P, 1, TI, ly, c.twy, c.spec);
   if (!fft2_pass<false>(c, 1, write_halos)) k_fft_x<<<gx, FT, smx, c.s>>>(P, 1, CL, lx, c.twx, c.p, c.spec, write_halos);
 }

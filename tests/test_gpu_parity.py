@@ -560,24 +560,3 @@ def test_materials_two_rows_bit_identical(monkeypatch):
         two.close()
         one.close()
 
-
-@pytest.mark.parametrize("ni,nj,nk", [(64, 64, 12), (48, 32, 37), (32, 16, 6)])
-def test_thomas_ring_bit_identical_to_register_batches(monkeypatch, ni, nj, nk):
-    """The z Thomas sweeps streamed through a shared-memory ring give the same
-    solution bits as the register-batch sweeps (ICLS_THOMAS=regs), at
-    columns longer and shorter than the ring."""
-    cfg = make_config(itot=ni, jtot=nj, ktot=nk, lmax=1, lx=ni / 64.0, ly=nj / 64.0, lz=nk / 64.0)
-    ls = init_drops(cfg, [(0.5 * cfg.lx, 0.5 * cfg.ly, 0.5 * cfg.lz)], [0.02])
-    rng = np.random.default_rng(ni + nk)
-    p = np.asfortranarray(rng.standard_normal(field_shape(cfg, "p")))
-    ring = Solver(cfg)
-    monkeypatch.setenv("ICLS_THOMAS", "regs")
-    regs = Solver(cfg)
-    monkeypatch.delenv("ICLS_THOMAS")
-    for s in (ring, regs):
-        s.setup(ls, p=p)
-        s.upload("p", p)
-        s.solver2d()
-    assert np.array_equal(ring.download("p"), regs.download("p"))
-    ring.close()
-    regs.close()
