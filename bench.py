@@ -96,7 +96,7 @@ ALG_VALUES = {
     "ab2": (24, 0, "N"),             # u,v,w,miu,rho_uvw,duold x3,pnew,pold,p_xyz,p_xyz_old -> dudt x3,duold x3
     "correc": (12, 1, "N"),          # dudt x3,p_xyz | p -> u,v,w, ucc,vcc,wcc
     "fillps": (3, 2, "N"),           # dudt x3 | pjump -> p
-    "solver2d": (0, 2, "N"),         # p -> p (the transposes and sweeps between are not compulsory)
+    "solver2d": (3, 2, "N"),         # dudt x3 | p_jump -> p: fillps folded into the first pass (the transposes and sweeps between are not compulsory)
     "pressure_update": (3, 1, "N"),  # pnew | p -> pnew, pold
     "stream_vel": (1, 0, "N"),
     "materials_final": (6, 0, "N"),  # jiemian -> miu, rho, rho_uvw
@@ -114,11 +114,13 @@ ALG_VALUES = {
 MLP_FLOPS_PER_CELL = 2 * (128 * 64 + 128 * 128 + 64 * 128)
 
 # DRAM bytes (read + write) of one launch of the dominant kernel at 256^3,
-# (kernel, FP32 form) -> bytes: ncu's dram__bytes_read.sum + write.sum of
-# the launch on the 128^3 workload (profiles/k_ab2_*_multi_drop_128_12.md),
+# (kernel, FP32 form) -> bytes: ncu's dram__bytes_read.sum + write.sum.
+# FP64: the launch on the 128^3 workload (profiles/k_ab2_fp64_multi_drop_128_12.md)
 # times the 8x cells (the traffic equals the algorithmic bytes there, so it
-# scales with the cells)
-TRAFFIC = {("ab2", False): 8 * (318.163968e6 + 83.975936e6), ("ab2", True): 8 * (226.014976e6 + 37.924352e6)}
+# scales with the cells); FP32: the launch at 256^3 itself
+# (profiles/k_ab2_fp32_static_drop_256.md; the predictor's grid and fields do
+# not depend on the drops)
+TRAFFIC = {("ab2", False): 8 * (318.163968e6 + 83.975936e6), ("ab2", True): 1.243471e9 + 0.390145e9}
 
 
 def alg_bytes_per_launch(name, cfg, stats, f32=False):
