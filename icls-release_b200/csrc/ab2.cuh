@@ -362,10 +362,12 @@ void ab2_launch_pw(Ctx& c, const MomArgs& a, int o) {
       ab2_ptr<T>(c.dvold[o]), ab2_ptr<T>(c.dwold[o]), nch == 1 ? c.P.kmax : kc, nch);
 }
 // one instance per spacing case: with power-of-two spacings every a/dx is
-// the product, so neither the test nor the division is in the kernel
+// the product, so neither the test nor the division is in the kernel.  The
+// FP32 form, held to tolerances rather than to the reference's rounding,
+// always takes the product by the reciprocal (within an ulp of the quotient).
 template <typename T>
 void ab2_launch(Ctx& c, const MomArgs& a, int o) {
-  if (c.P.pow2) ab2_launch_pw<T, 1>(c, a, o);
+  if (c.P.pow2 || sizeof(T) == 4) ab2_launch_pw<T, 1>(c, a, o);
   else ab2_launch_pw<T, 0>(c, a, o);
 }
 

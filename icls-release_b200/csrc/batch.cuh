@@ -35,6 +35,7 @@ struct Col {
   int i, j;    // interior column (1..imax, 1..jmax)
   int ka, kb;  // rows of this block's chunk
   int tile;    // column tile index within the task
+  int ch;      // z chunk index within the task
   bool ok;     // inside the written spans
   bool cxy;    // a computed column
 };
@@ -48,6 +49,7 @@ __device__ __forceinline__ Col col_of(const Params& p, const LsTask& t, int loca
   const int by = r % t.ty;
   const int ch = r / t.ty;
   c.tile = bx + t.tx * by;
+  c.ch = ch;
   if (t.flat) {
     const int col = bx * (TBX * TBY) + (int)threadIdx.x + TBX * (int)threadIdx.y;
     c.Y = col / t.r.xn;

@@ -228,9 +228,10 @@ int allocate(Ctx& c) {
   if (cudaMalloc((void**)&c.band_count, sizeof(int)) != cudaSuccess) return ICLS_E_NOMEM;
   AL(c.drs, (size_t)P.L);
   c.red_cap = ((P.imax + TBX - 1) / TBX) * ((P.jmax + TBY - 1) / TBY);
-  // per-tile exact sums of H (4 words each) for every drop; the inflation
-  // uses red_cap area sums and red_cap exact sums
-  AL(c.hpart, (size_t)std::max(4 * P.L, 5) * c.red_cap);
+  c.hcap = c.red_cap * ((P.kmax + 2 + kHeavRows - 1) / kHeavRows);
+  // per-(tile, chunk) exact sums of H (4 words each) for every drop; the
+  // inflation uses red_cap area sums and red_cap exact sums
+  AL(c.hpart, std::max((size_t)4 * P.L * c.hcap, (size_t)5 * c.red_cap));
   CK(cudaMallocHost((void**)&c.h_vol, sizeof(double) * P.L));
   CK(cudaMallocHost((void**)&c.h_volnow, sizeof(double) * P.L));
   CK(cudaMallocHost((void**)&c.h_sc, sizeof(DevScalars)));
@@ -257,13 +258,17 @@ int allocate(Ctx& c) {
   // list build included);
   // ICLS_CORREC=shapec: the fused correction one thread per shape-C cell
   // in place of one per interior cell writing the images;
-  // ICLS_MATERIALS=rows1: the materials one row per thread, not two.
+  // ICLS_MATERIALS=rows1: the materials one row per thread, not two;
+  // ICLS_FFT=whole: each FFT pass of solver2d over all planes at once
+  // instead of x and y passes slab by slab.
   const char* ab = std::getenv("ICLS_AB2");
   c.ab2_ring = !(ab && std::strcmp(ab, "tma") == 0);
   const char* cv = std::getenv("ICLS_CORREC");
   c.correc_shapec = cv && std::strcmp(cv, "shapec") == 0;
   const char* mv = std::getenv("ICLS_MATERIALS");
   c.materials_rows1 = mv && std::strcmp(mv, "rows1") == 0;
+  const char* fv = std::getenv("ICLS_FFT");
+  c.fft_whole = fv && std::strcmp(fv, "whole") == 0;
   const char* av = std::getenv("ICLS_ADV");
   c.adv_column = !(av && std::strcmp(av, "band") == 0);
   // working buffers of a group of drops: as many drops as half the free
@@ -529,11 +534,11 @@ void update_materials(Ctx& c) {
   launch_fill(c, c.jiemian, c.P.nC, 1.0, true);
   std::vector<int> all(L);
   for (int l = 0; l < L; ++l) all[l] = l;
-  std::vector<int> ntiles(L, 0);
-  for (LsBatch& b : make_batches(all, 0, [&](int l) { return c_region(c.P, c.win[l].box, 0); })) {
+  std::vector<int> ntiles(L, 0);  // partial sums per drop: column tiles x z chunks
+  for (LsBatch& b : make_batches(all, kHeavRows, [&](int l) { return c_region(c.P, c.win[l].box, 0); })) {
     for (int q = 0; q < b.n; ++q) {
       b.t[q].phi0 = c.lv[b.t[q].l];
-      ntiles[b.t[q].l] = b.t[q].tx * b.t[q].ty;
+      ntiles[b.t[q].l] = b.t[q].tx * b.t[q].ty * b.t[q].nch;
     }
     launch_heaviside(c, b);
   }

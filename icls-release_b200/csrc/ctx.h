@@ -75,6 +75,10 @@ struct DropWin {
   int grow = 0;
 };
 
+// z rows per chunk of update_materials' Heaviside sweep (one exact partial
+// sum per column tile and chunk)
+constexpr int kHeavRows = 8;
+
 struct Ctx {
   // tensor maps of the TMA predictor for up to four sets of its 18 input
   // pointers (the AB2 history and the p_x/p_xold pairs alternate between
@@ -84,6 +88,7 @@ struct Ctx {
   int ab2_nmaps = 0, ab2_next = 0;
   bool ab2_tma_failed = false;  // a map could not be encoded: use the ring
   bool ab2_ring = true;  // FP64 predictor on the cp.async ring (else TMA: ICLS_AB2=tma)
+  bool fft_whole = false;  // solver2d passes over all planes at once (ICLS_FFT=whole), not in L2 slabs
   bool materials_rows1 = false;  // materials one row per thread (ICLS_MATERIALS=rows1)
   bool correc_shapec = false;  // fused correction one thread per shape-C cell (ICLS_CORREC=shapec)
   icls_config cfg;
@@ -147,6 +152,7 @@ struct Ctx {
   double* stage = nullptr;              // precision form: FP64 staging of one field (upload/download)
   double* hpart = nullptr;              // per-tile exact sums of H (XSum), red_cap per drop
   int red_cap = 0;                      // column tiles of a whole x-y plane
+  int hcap = 0;                         // Heaviside partials per drop: red_cap x the z chunks of shape C
   // pinned host mirrors
   double* h_vol = nullptr;
   DevScalars* h_sc = nullptr;

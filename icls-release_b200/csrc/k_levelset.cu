@@ -822,24 +822,26 @@ __global__ void __launch_bounds__(NT) k_heaviside(Params p, const __grid_constan
 #pragma unroll
       for (int u = 0; u < 8; ++u) f[u] = (k0 + u <= kb) ? phi[c0 + u * sz] : TC(1.);
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < 8; ++u) {  // rows past kb skipped without a break, so f stays in registers
         const int k = k0 + u;
-        if (k > kb) break;
-        const T H = heav_trig(p, f[u], eps);
-        if (H < TC(1.)) {
-          min_into(jiemian + idxC(p, i, j, k), H);
-          if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, j, k), H);
-          if (jj != INT_MIN) {
-            min_into(jiemian + idxC(p, i, jj, k), H);
-            if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, jj, k), H);
+        if (k <= kb) {
+          const T H = heav_trig(p, f[u], eps);
+          if (H < TC(1.)) {
+            min_into(jiemian + idxC(p, i, j, k), H);
+            if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, j, k), H);
+            if (jj != INT_MIN) {
+              min_into(jiemian + idxC(p, i, jj, k), H);
+              if (ii != INT_MIN) min_into(jiemian + idxC(p, ii, jj, k), H);
+            }
           }
+          if (k >= 1 && k <= p.kmax) xs_add(s, (double)H);
         }
-        if (k >= 1 && k <= p.kmax) xs_add(s, (double)H);
       }
     }
   }
   const XSum bs = block_xsum<NT>(s);
-  if (flat_tid() == 0) part[(long long)t.l * cap + c.tile] = bs;
+  // one partial per (column tile, z chunk) of the task
+  if (flat_tid() == 0) part[(long long)t.l * cap + c.tile + (long long)t.tx * t.ty * c.ch] = bs;
 }
 
 // volume(l) and rho_avr from the per-tile sums (misc.f90:139-173);
@@ -848,11 +850,11 @@ struct PerDrop {
   double v[kMaxDropsParam];
   int n[kMaxDropsParam];
 };
-__global__ void k_volumes(Params p, const XSum* __restrict__ part, int cap, PerDrop pd, int uniform,
+__global__ void k_volumes(Params p, const XSum* __restrict__ part, int cap, PerDrop pd, int uniform, int nb_all,
                           double* __restrict__ vol, DevScalars* __restrict__ dsc) {
   const double N = (1. * p.imax * p.jmax) * p.kmax;
   for (int l = threadIdx.x; l < p.L; l += blockDim.x) {
-    const int nb = uniform ? cap : pd.n[l];
+    const int nb = uniform ? nb_all : pd.n[l];
     XSum s;
     xs_zero(s);
     for (int b = 0; b < nb; ++b) xs_merge(s, part[(long long)l * cap + b]);
@@ -1364,13 +1366,15 @@ void adv_launch(Ctx& c, const LsBatch& b, int scheme, int stage1, double a, doub
   const T* u = reinterpret_cast<const T*>(vu);
   const T* v = reinterpret_cast<const T*>(vv);
   const T* w = reinterpret_cast<const T*>(vw);
-  // one instance per scheme and spacing case (PW: every a/dx a product)
+  // one instance per scheme and spacing case (PW: every a/dx a product;
+  // the FP32 form always takes the product by the reciprocal)
   const unsigned g = b.start[b.n];
+  const bool pw = c.P.pow2 || sizeof(T) == 4;
   if (scheme == ICLS_HOUC5) {
-    if (c.P.pow2) k_adv_stage<ICLS_HOUC5, T, 1><<<g, kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
+    if (pw) k_adv_stage<ICLS_HOUC5, T, 1><<<g, kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
     else k_adv_stage<ICLS_HOUC5, T, 0><<<g, kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
   } else {
-    if (c.P.pow2) k_adv_stage<ICLS_WENO5, T, 1><<<g, kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
+    if (pw) k_adv_stage<ICLS_WENO5, T, 1><<<g, kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
     else k_adv_stage<ICLS_WENO5, T, 0><<<g, kTile, 0, c.s>>>(c.P, b, stage1, a, bb, fdt, u, v, w);
   }
 }
@@ -1395,11 +1399,12 @@ void adv_split_launch(Ctx& c, const LsBatch& b, int scheme, int stage1, double a
   const unsigned nb = (unsigned)((need + NT - 1) / NT);
   k_adv_base<T><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, stage1, a, bb);
   if (nb > 0) {
+    const bool pw = c.P.pow2 || sizeof(T) == 4;
     if (scheme == ICLS_HOUC5) {
-      if (c.P.pow2) k_adv_band<ICLS_HOUC5, T, 1><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
+      if (pw) k_adv_band<ICLS_HOUC5, T, 1><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
       else k_adv_band<ICLS_HOUC5, T, 0><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
     } else {
-      if (c.P.pow2) k_adv_band<ICLS_WENO5, T, 1><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
+      if (pw) k_adv_band<ICLS_WENO5, T, 1><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
       else k_adv_band<ICLS_WENO5, T, 0><<<nb, NT, 0, c.s>>>(c.P, b, list, c.band_count, fdt, u, v, w);
     }
   }
@@ -1426,12 +1431,10 @@ void launch_reinit_stage(Ctx& c, const LsBatch& b, int stage, double dtau) {
   if (b.n == 0) return;
   Scope sc_(c.prof, c.s, "reinit_stage", 1);
   const unsigned g = b.start[b.n];
-  if (c.P.pow2)
-    BY_FORM(c, (k_reinit_stage<float, 1><<<g, kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs)),
-            (k_reinit_stage<double, 1><<<g, kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs)));
-  else
-    BY_FORM(c, (k_reinit_stage<float, 0><<<g, kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs)),
-            (k_reinit_stage<double, 0><<<g, kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs)));
+  // the FP32 form takes the product by the reciprocal at any spacing
+  if (c.P.f32) k_reinit_stage<float, 1><<<g, kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs);
+  else if (c.P.pow2) k_reinit_stage<double, 1><<<g, kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs);
+  else k_reinit_stage<double, 0><<<g, kTile, 0, c.s>>>(c.P, b, stage, dtau, c.drs);
 }
 void launch_reinit_reset(Ctx& c, const LsBatch& b, int maxiter) {
   if (b.n == 0) return;
@@ -1444,7 +1447,7 @@ void launch_reinit_check(Ctx& c, const LsBatch& b, int it, int maxiter, double t
   k_reinit_check<<<1, 64, 0, c.s>>>(b, it, maxiter, thr, c.drs, c.dsc, c.P.L - 1);
 }
 
-// the per-tile exact sums of H: red_cap per drop (4 words each)
+// the per-(tile, chunk) exact sums of H: hcap per drop (4 words each)
 XSum* hparts(Ctx& c) { return reinterpret_cast<XSum*>(c.hpart); }
 
 void launch_heaviside(Ctx& c, const LsBatch& b) {
@@ -1452,8 +1455,8 @@ void launch_heaviside(Ctx& c, const LsBatch& b) {
   Scope sc_(c.prof, c.s, "heaviside", 1);
   BY_FORM(c,
           (k_heaviside<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, reinterpret_cast<float*>(c.jiemian), hparts(c),
-                                                                c.red_cap)),
-          (k_heaviside<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.jiemian, hparts(c), c.red_cap)));
+                                                                c.hcap)),
+          (k_heaviside<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, c.jiemian, hparts(c), c.hcap)));
 }
 
 // n elements of a; tfield: a holds the form's field type (else FP64)
@@ -1484,7 +1487,10 @@ void launch_materials_final(Ctx& c, const double* outside, const int* ntiles) {
     o.v[l] = (!uniform && l < c.P.L) ? outside[l] : 0.;
     o.n[l] = (!uniform && l < c.P.L) ? ntiles[l] : 0;
   }
-  k_volumes<<<1, 256, 0, c.s>>>(c.P, hparts(c), c.red_cap, o, uniform, c.dvol, c.dsc);
+  // uniform: every drop swept whole, (kmax + 2) / kStageRows z chunks of
+  // red_cap column tiles
+  k_volumes<<<1, 256, 0, c.s>>>(c.P, hparts(c), c.hcap, o, uniform, c.red_cap * ((c.P.kmax + 2) / kHeavRows), c.dvol,
+                                c.dsc);
   const int r0[3] = {0, 0, 0}, r1[3] = {c.P.i1, c.P.j1, c.P.k1};
   dim3 g2 = grid_of(r0, r1);
   g2.z = (g2.z + 1) / 2;  // two rows per thread
