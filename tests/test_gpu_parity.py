@@ -591,10 +591,10 @@ def test_volumes_beyond_the_per_drop_parameter_limit():
     drop is swept whole and its Heaviside partial sums are merged by count;
     after update_materials and after a step the volumes equal the oracle's
     exactly (both sum H exactly)."""
-    from icls_gpu import seeded_drops
     L = 257
     cfg = make_config(itot=16, jtot=16, ktot=16, lmax=L, timestep=1e-4)
-    centres, radii = seeded_drops(cfg, 4, seed=3, rmin=0.15, rmax=0.2)
+    centres = [(0.3, 0.3, 0.35), (0.7, 0.65, 0.6), (0.28, 0.75, 0.7), (0.72, 0.28, 0.3)]
+    radii = [0.15, 0.17, 0.13, 0.16]
     ls = init_drops(cfg, [centres[l % 4] for l in range(L)], [radii[l % 4] for l in range(L)])
     g, o = paired(cfg, ls)
     for s in (g, o):
