@@ -371,9 +371,8 @@ __device__ __forceinline__ double rhs_at(const Params& p, const RhsArgs& r, long
 template <int R1, int R2, bool YPASS, int LPC, int RHS = 0>
 __global__ void __launch_bounds__(256, (R1 > 16 || R2 > 16) ? 1 : 2)
     k_fft2(Params p, int dir, const double2* __restrict__ tw, double* __restrict__ pp, double* __restrict__ spec,
-           int halos, RhsArgs ra, int boff) {
+           int halos, RhsArgs ra) {
   static_assert(RHS == 0 || !YPASS, "the right-hand side is formed in the forward x pass");
-  const long long bx = (long long)blockIdx.x + boff;  // this CTA's unit (a launch may cover a range of planes)
   constexpr int N = R1 * R2;
   constexpr int TPL = R1 > R2 ? R1 : R2;
   static_assert(LPC * TPL <= 256, "a CTA holds LPC lines of TPL threads");
@@ -394,7 +393,7 @@ __global__ void __launch_bounds__(256, (R1 > 16 || R2 > 16) ? 1 : 2)
   double* colbase = nullptr;            // y pass: the first column of the pair
   if (!YPASS) {
     const long long nlines = (long long)p.jmax * p.kmax;
-    const long long la = 2 * (bx * LPC + lt), lb = la + 1;
+    const long long la = 2 * ((long long)blockIdx.x * LPC + lt), lb = la + 1;
     live = used && lb < nlines;
     ja = (int)(la % p.jmax) + 1; ka = (int)(la / p.jmax) + 1;
     jb = (int)(lb % p.jmax) + 1; kb = (int)(lb / p.jmax) + 1;
@@ -408,8 +407,8 @@ __global__ void __launch_bounds__(256, (R1 > 16 || R2 > 16) ? 1 : 2)
     }
   } else {
     const int tiles_i = p.imax / (2 * LPC);
-    const int k = (int)(bx / tiles_i) + 1;
-    const int i0 = (int)(bx % tiles_i) * (2 * LPC) + 2 * lt;  // 0-based column
+    const int k = (int)blockIdx.x / tiles_i + 1;
+    const int i0 = ((int)blockIdx.x % tiles_i) * (2 * LPC) + 2 * lt;  // 0-based column
     live = used;
     colbase = spec + (long long)i0 + (long long)p.imax * p.jmax * (k - 1);
     st = p.imax;
@@ -503,7 +502,7 @@ __global__ void __launch_bounds__(256, (R1 > 16 || R2 > 16) ? 1 : 2)
       colbase[(long long)n * st] = ha;
       colbase[(long long)n * st + 1] = hb;
     } else {
-      const long long la = 2 * (bx * LPC + lt);
+      const long long la = 2 * ((long long)blockIdx.x * LPC + lt);
       spec[la * N + n] = ha;
       spec[(la + 1) * N + n] = hb;
     }
@@ -876,11 +875,8 @@ static int y_tile(int imax) {
   return ti;
 }
 
-// planes k0 <= k - 1 < k1 of the pass: x pass, lines k0 jmax .. k1 jmax - 1
-// (whole CTAs when jmax is a multiple of 2 LPC, which the caller ensures
-// for a partial range); y pass, column tiles of planes k0 .. k1 - 1
 template <int R1, int R2, bool Y, int LPC, int RHS = 0>
-void fft2_launch(Ctx& c, int dir, const double2* tw, int halos, const RhsArgs& ra, int k0, int k1) {
+void fft2_launch(Ctx& c, int dir, const double2* tw, int halos, const RhsArgs& ra) {
   const Params& P = c.P;
   static unsigned attr = 0;  // devices this instance's shared-memory limit is raised on
   int dev = 0;
@@ -890,54 +886,36 @@ void fft2_launch(Ctx& c, int dir, const double2* tw, int halos, const RhsArgs& r
                          (int)fft2_smem<R1, R2, LPC>());
     attr |= 1u << (dev & 31);
   }
-  long long u0, u1;
-  if (Y) {
-    u0 = (long long)(P.imax / (2 * LPC)) * k0;
-    u1 = (long long)(P.imax / (2 * LPC)) * k1;
-  } else {
-    u0 = (long long)P.jmax * k0 / (2 * LPC);
-    u1 = ((long long)P.jmax * k1 + 2 * LPC - 1) / (2 * LPC);
-  }
-  k_fft2<R1, R2, Y, LPC, RHS><<<(unsigned)(u1 - u0), 256, fft2_smem<R1, R2, LPC>(), c.s>>>(
-      P, dir, tw, c.p, c.spec, halos, ra, (int)u0);
+  const long long units = Y ? (long long)(P.imax / (2 * LPC)) * P.kmax
+                            : ((long long)P.jmax * P.kmax + 2 * LPC - 1) / (2 * LPC);
+  k_fft2<R1, R2, Y, LPC, RHS>
+      <<<(unsigned)units, 256, fft2_smem<R1, R2, LPC>(), c.s>>>(P, dir, tw, c.p, c.spec, halos, ra);
 }
 // the lengths with a radix-3 factor: 16 lines per CTA where the columns tile
 // by 32 (y pass) and the lines need at most 16 threads, else 8
 template <int R2, bool Y, int RHS = 0>
-void fft2_launch3(Ctx& c, int dir, const double2* tw, int halos, const RhsArgs& ra, int k0, int k1) {
-  if (R2 <= 16 && (!Y || c.P.imax % 32 == 0))
-    fft2_launch<16, R2, Y, R2 <= 16 ? 16 : 8, RHS>(c, dir, tw, halos, ra, k0, k1);
-  else
-    fft2_launch<16, R2, Y, 8, RHS>(c, dir, tw, halos, ra, k0, k1);
+void fft2_launch3(Ctx& c, int dir, const double2* tw, int halos, const RhsArgs& ra) {
+  if (R2 <= 16 && (!Y || c.P.imax % 32 == 0)) fft2_launch<16, R2, Y, R2 <= 16 ? 16 : 8, RHS>(c, dir, tw, halos, ra);
+  else fft2_launch<16, R2, Y, 8, RHS>(c, dir, tw, halos, ra);
 }
 
 // the two-level transform of one pass if its length has one (and, for the
 // y pass, the columns tile the CTAs); false: the radix-2 kernels.  RHS (the
 // forward x pass): fillps' right-hand side formed in the pass (k_fft2).
 template <bool Y, int RHS = 0>
-bool fft2_pass(Ctx& c, int dir, int halos, const RhsArgs& ra = RhsArgs{}, int k0 = 0, int k1 = -1) {
+bool fft2_pass(Ctx& c, int dir, int halos, const RhsArgs& ra = RhsArgs{}) {
   const Params& P = c.P;
   const int N = Y ? P.jmax : P.imax;
   const double2* tw = Y ? c.twy : c.twx;
-  if (k1 < 0) k1 = P.kmax;
   auto fits = [&](int lpc) { return !Y || P.imax % (2 * lpc) == 0; };
   switch (N) {
-    case 64: if (!fits(16)) return false; fft2_launch<16, 4, Y, 16, RHS>(c, dir, tw, halos, ra, k0, k1); return true;
-    case 128: if (!fits(16)) return false; fft2_launch<16, 8, Y, 16, RHS>(c, dir, tw, halos, ra, k0, k1); return true;
-    case 256: if (!fits(16)) return false; fft2_launch<16, 16, Y, 16, RHS>(c, dir, tw, halos, ra, k0, k1); return true;
-    case 48: if (!fits(8)) return false; fft2_launch3<3, Y, RHS>(c, dir, tw, halos, ra, k0, k1); return true;
-    case 96: if (!fits(8)) return false; fft2_launch3<6, Y, RHS>(c, dir, tw, halos, ra, k0, k1); return true;
-    case 192: if (!fits(8)) return false; fft2_launch3<12, Y, RHS>(c, dir, tw, halos, ra, k0, k1); return true;
-    case 384: if (!fits(8)) return false; fft2_launch3<24, Y, RHS>(c, dir, tw, halos, ra, k0, k1); return true;
-    default: return false;
-  }
-}
-// the y pass takes the two-level transform (its length is one, and the
-// column pairs tile the CTAs)
-bool fft2_y_applies(const Params& P) {
-  switch (P.jmax) {
-    case 64: case 128: case 256: return P.imax % 32 == 0;
-    case 48: case 96: case 192: case 384: return P.imax % 16 == 0;
+    case 64: if (!fits(16)) return false; fft2_launch<16, 4, Y, 16, RHS>(c, dir, tw, halos, ra); return true;
+    case 128: if (!fits(16)) return false; fft2_launch<16, 8, Y, 16, RHS>(c, dir, tw, halos, ra); return true;
+    case 256: if (!fits(16)) return false; fft2_launch<16, 16, Y, 16, RHS>(c, dir, tw, halos, ra); return true;
+    case 48: if (!fits(8)) return false; fft2_launch3<3, Y, RHS>(c, dir, tw, halos, ra); return true;
+    case 96: if (!fits(8)) return false; fft2_launch3<6, Y, RHS>(c, dir, tw, halos, ra); return true;
+    case 192: if (!fits(8)) return false; fft2_launch3<12, Y, RHS>(c, dir, tw, halos, ra); return true;
+    case 384: if (!fits(8)) return false; fft2_launch3<24, Y, RHS>(c, dir, tw, halos, ra); return true;
     default: return false;
   }
 }
@@ -983,6 +961,7 @@ void launch_fillps_solver2d(Ctx& c, int write_halos, int add) {
   solver2d_periodic(c, write_halos, &ra);
 }
 void solver2d_periodic(Ctx& c, int write_halos, const RhsArgs* ra) {
+  Scope sc_(c.prof, c.s, "solver2d", 5);
   const Params& P = c.P;
   const int lx = ilog2(P.imax), ly = ilog2(P.jmax);
   const int CL = x_lines_per_cta(P.imax);
@@ -1000,34 +979,6 @@ void solver2d_periodic(Ctx& c, int write_halos, const RhsArgs* ra) {
     cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr |= 1u << (dev & 31);
   }
-  const long long nxy = (long long)P.imax * P.jmax;
-  // Both passes two-level: run the x and y passes of a slab of planes back
-  // to back, so the spectrum the x pass writes is still in L2 when the y
-  // pass reads it (the slab's spectrum is at most 32 MB of the 126 MB L2),
-  // likewise the inverse y and x passes after the z sweeps.  Lines of the x
-  // pass then split into whole CTAs at slab edges (jmax a multiple of 32).
-  const long long plane_bytes = nxy * (long long)sizeof(double);
-  const int slab = (int)std::max(1LL, (32LL << 20) / plane_bytes);
-  const bool slabs = !c.fft_whole && fft2_x_length(P.imax) && fft2_y_applies(P) && P.jmax % 32 == 0 &&
-                     slab < P.kmax;
-  const int nslab = (P.kmax + slab - 1) / slab;
-  Scope sc_(c.prof, c.s, "solver2d", slabs ? 4 * nslab + 1 : 5);
-  if (slabs) {
-    for (int k0 = 0; k0 < P.kmax; k0 += slab) {
-      const int k1 = std::min(P.kmax, k0 + slab);
-      if (!ra) fft2_pass<false>(c, 0, 0, RhsArgs{}, k0, k1);
-      else if (P.f32) fft2_pass<false, 4>(c, 0, 0, *ra, k0, k1);
-      else fft2_pass<false, 8>(c, 0, 0, *ra, k0, k1);
-      fft2_pass<true>(c, 0, 0, RhsArgs{}, k0, k1);
-    }
-    k_thomas<<<(unsigned)((nxy + 127) / 128), 128, 0, c.s>>>(P, c.tri_a, c.tri_c, c.zpiv, c.spec);
-    for (int k0 = 0; k0 < P.kmax; k0 += slab) {
-      const int k1 = std::min(P.kmax, k0 + slab);
-      fft2_pass<true>(c, 1, 0, RhsArgs{}, k0, k1);
-      fft2_pass<false>(c, 1, write_halos, RhsArgs{}, k0, k1);
-    }
-    return;
-  }
   if (ra) {  // fft2_x_length(imax): the two-level x pass exists
     if (P.f32) fft2_pass<false, 4>(c, 0, 0, *ra);
     else fft2_pass<false, 8>(c, 0, 0, *ra);
@@ -1035,6 +986,7 @@ void solver2d_periodic(Ctx& c, int write_halos, const RhsArgs* ra) {
     k_fft_x<<<gx, FT, smx, c.s>>>(P, 0, CL, lx, c.twx, c.p, c.spec, 0);
   }
   if (!fft2_pass<true>(c, 0, 0)) k_fft_y<<<gy, FT, smy, c.s>>>(P, 0, TI, ly, c.twy, c.spec);
+  const long long nxy = (long long)P.imax * P.jmax;
   k_thomas<<<(unsigned)((nxy + 127) / 128), 128, 0, c.s>>>(P, c.tri_a, c.tri_c, c.zpiv, c.spec);
   if (!fft2_pass<true>(c, 1, 0)) k_fft_y<<<gy, FT, smy, c.s>>>(P, 1, TI, ly, c.twy, c.spec);
   if (!fft2_pass<false>(c, 1, write_halos)) k_fft_x<<<gx, FT, smx, c.s>>>(P, 1, CL, lx, c.twx, c.p, c.spec, write_halos);

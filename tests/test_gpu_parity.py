@@ -562,30 +562,6 @@ def test_materials_two_rows_bit_identical(monkeypatch):
 
 
 
-@pytest.mark.parametrize("ni,nj,nk", [(256, 256, 70), (96, 128, 350)])
-def test_fft_slabs_bit_identical_to_whole_passes(monkeypatch, ni, nj, nk):
-    """solver2d with its x and y passes run slab by slab (so a slab's
-    spectrum is still in L2 between them) gives the same bits as each pass
-    over all planes (ICLS_FFT=whole), including a last, shorter slab and
-    the halos of p."""
-    cfg = make_config(itot=ni, jtot=nj, ktot=nk, lmax=1, lx=ni / 64.0, ly=nj / 64.0, lz=nk / 64.0)
-    ls = init_drops(cfg, [(0.5 * cfg.lx, 0.5 * cfg.ly, 0.5 * cfg.lz)], [0.02])
-    rng = np.random.default_rng(ni + nk)
-    p = np.asfortranarray(rng.standard_normal(field_shape(cfg, "p")))
-    slab = Solver(cfg)
-    monkeypatch.setenv("ICLS_FFT", "whole")
-    whole = Solver(cfg)
-    monkeypatch.delenv("ICLS_FFT")
-    for s in (slab, whole):
-        s.setup(ls, p=p)
-        s.upload("p", p)
-        s.solver2d()
-        s.boundp("p")
-    assert np.array_equal(slab.download("p"), whole.download("p"))
-    slab.close()
-    whole.close()
-
-
 def test_volumes_beyond_the_per_drop_parameter_limit():
     """With more drops than travel as a kernel parameter (257 > 256) every
     drop is swept whole and its Heaviside partial sums are merged by count;
