@@ -43,19 +43,32 @@ __device__ __forceinline__ T curvature_at(const Params& p, const T* __restrict__
   T x[10];
 #pragma unroll
   for (int r = 1; r < 10; ++r) x[r] = TC(0.);
-  int n = 0;
   const long long sy = p.nLx, sz = (long long)p.nLx * p.nLy;
+  if constexpr (sizeof(T) == 4) {
+    // FP32: the 27 values first, then each x[r] as one chain over q in the
+    // same order, every coefficient index a compile-time constant (an
+    // operand of the product, no separate load)
+    T v[27];
+#pragma unroll
+    for (int q = 0; q < 27; ++q) v[q] = phi[c + (q % 3 - 1) + (q / 3 % 3 - 1) * sy + (q / 9 - 1) * sz];
+#pragma unroll
+    for (int r = 1; r < 10; ++r)
+#pragma unroll
+      for (int q = 0; q < 27; ++q) x[r] = x[r] + coef<T>(r * 27 + q) * v[q];
+  } else {
+    int n = 0;
 #pragma unroll 1
-  for (int dk = -1; dk <= 1; ++dk)
+    for (int dk = -1; dk <= 1; ++dk)
 #pragma unroll
-    for (int dj = -1; dj <= 1; ++dj)
+      for (int dj = -1; dj <= 1; ++dj)
 #pragma unroll
-      for (int di = -1; di <= 1; ++di) {
-        const T v = phi[c + di + dj * sy + dk * sz];
+        for (int di = -1; di <= 1; ++di) {
+          const T v = phi[c + di + dj * sy + dk * sz];
 #pragma unroll
-        for (int r = 1; r < 10; ++r) x[r] = x[r] + coef<T>(r * 27 + n) * v;
-        ++n;
-      }
+          for (int r = 1; r < 10; ++r) x[r] = x[r] + coef<T>(r * 27 + n) * v;
+          ++n;
+        }
+  }
   const T dphidx = x[1], dphidy = x[2], dphidz = x[3];
   const T d2phidx = x[4], d2phidy = x[5], d2phidz = x[6];
   const T d2phidxdy = x[7], d2phidxdz = x[8], d2phidydz = x[9];
@@ -85,7 +98,7 @@ __device__ __forceinline__ T curvature_at(const Params& p, const T* __restrict__
 // periodic copies (bound.f90:292-305), the apron (far field, |phi| > 5dz)
 // is 0.
 template <typename T>
-__global__ void __launch_bounds__(NT, 3) k_curvature(Params p, const __grid_constant__ LsBatch B, T* __restrict__ nrm_m,
+__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 4 : 3)) k_curvature(Params p, const __grid_constant__ LsBatch B, T* __restrict__ nrm_m,
                                                   MlpCell* __restrict__ rec, int* __restrict__ count, int cap) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];

@@ -850,16 +850,26 @@ struct PerDrop {
   double v[kMaxDropsParam];
   int n[kMaxDropsParam];
 };
+// One warp per drop: its lanes merge every 32nd partial, the lanes' sums
+// (limbs below 2^48 after each merge) add limb by limb across the warp
+// (below 2^53), and lane 0 rounds the exact total once.
 __global__ void k_volumes(Params p, const XSum* __restrict__ part, int cap, PerDrop pd, int uniform, int nb_all,
                           double* __restrict__ vol, DevScalars* __restrict__ dsc) {
   const double N = (1. * p.imax * p.jmax) * p.kmax;
-  for (int l = threadIdx.x; l < p.L; l += blockDim.x) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int l = warp; l < p.L; l += nw) {
     const int nb = uniform ? nb_all : pd.n[l];
     XSum s;
     xs_zero(s);
-    for (int b = 0; b < nb; ++b) xs_merge(s, part[(long long)l * cap + b]);
-    if (!uniform) xs_add_count(s, (long long)pd.v[l]);
-    vol[l] = 1. - xs_value(s) / N;
+    for (int b = lane; b < nb; b += 32) xs_merge(s, part[(long long)l * cap + b]);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      for (int d = 16; d > 0; d >>= 1) s.L[q] += __shfl_down_sync(0xffffffffu, s.L[q], d);
+    if (lane == 0) {
+      xs_norm(s);
+      if (!uniform) xs_add_count(s, (long long)pd.v[l]);
+      vol[l] = 1. - xs_value(s) / N;
+    }
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1489,7 +1499,7 @@ void launch_materials_final(Ctx& c, const double* outside, const int* ntiles) {
   }
   // uniform: every drop swept whole, (kmax + 2) / kStageRows z chunks of
   // red_cap column tiles
-  k_volumes<<<1, 256, 0, c.s>>>(c.P, hparts(c), c.hcap, o, uniform, c.red_cap * ((c.P.kmax + 2) / kHeavRows), c.dvol,
+  k_volumes<<<1, 1024, 0, c.s>>>(c.P, hparts(c), c.hcap, o, uniform, c.red_cap * ((c.P.kmax + 2) / kHeavRows), c.dvol,
                                 c.dsc);
   const int r0[3] = {0, 0, 0}, r1[3] = {c.P.i1, c.P.j1, c.P.k1};
   dim3 g2 = grid_of(r0, r1);
