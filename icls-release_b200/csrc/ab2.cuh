@@ -202,8 +202,8 @@ template <typename T>
 constexpr int ab2_smem() {
   return (int)(4 * MRING * MSY * MSX * sizeof(T) + 2 * MRING * MPY * MSX * sizeof(T));
 }
-template <typename T, int PW>
-__global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
+template <typename T, int PW, int MB>
+__global__ void __launch_bounds__(MX * MY, MB)
     k_ab2(Params p, MomArgs a, T* __restrict__ dudt, T* __restrict__ dvdt, T* __restrict__ dwdt,
           T* __restrict__ duold_out, T* __restrict__ dvold_out, T* __restrict__ dwold_out, int kc, int nch) {
   extern __shared__ __align__(16) unsigned char ab2_dyn[];
@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(MX * MY, (sizeof(T) == 8 ? 2 : 4))
 template <typename T>
 T* ab2_ptr(double* q) { return reinterpret_cast<T*>(q); }
 
-template <typename T, int PW>
+template <typename T, int PW, int MB>
 void ab2_launch_pw(Ctx& c, const MomArgs& a, int o) {
   // rows per block: 32 for the FP32 form (four blocks per SM, shorter
   // ring prologues), 16 for FP64 (two blocks per SM, more blocks per wave)
@@ -354,10 +354,10 @@ void ab2_launch_pw(Ctx& c, const MomArgs& a, int o) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (!(attr & (1u << (dev & 31)))) {
-    cudaFuncSetAttribute(k_ab2<T, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, ab2_smem<T>());
+    cudaFuncSetAttribute(k_ab2<T, PW, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ab2_smem<T>());
     attr |= 1u << (dev & 31);
   }
-  k_ab2<T, PW><<<grid, dim3(MX, MY, 1), ab2_smem<T>(), c.s>>>(
+  k_ab2<T, PW, MB><<<grid, dim3(MX, MY, 1), ab2_smem<T>(), c.s>>>(
       c.P, a, ab2_ptr<T>(c.dudt), ab2_ptr<T>(c.dvdt), ab2_ptr<T>(c.dwdt), ab2_ptr<T>(c.duold[o]),
       ab2_ptr<T>(c.dvold[o]), ab2_ptr<T>(c.dwold[o]), nch == 1 ? c.P.kmax : kc, nch);
 }
@@ -365,10 +365,21 @@ void ab2_launch_pw(Ctx& c, const MomArgs& a, int o) {
 // the product, so neither the test nor the division is in the kernel.  The
 // FP32 form, held to tolerances rather than to the reference's rounding,
 // always takes the product by the reciprocal (within an ulp of the quotient).
+// MB: blocks per SM the registers are budgeted for (FP64 two, or three with
+// ICLS_AB2_BLOCKS=3; FP32 four)
 template <typename T>
 void ab2_launch(Ctx& c, const MomArgs& a, int o) {
-  if (c.P.pow2 || sizeof(T) == 4) ab2_launch_pw<T, 1>(c, a, o);
-  else ab2_launch_pw<T, 0>(c, a, o);
+  if constexpr (sizeof(T) == 8) {
+    if (c.ab2_blocks3) {
+      if (c.P.pow2) ab2_launch_pw<T, 1, 3>(c, a, o);
+      else ab2_launch_pw<T, 0, 3>(c, a, o);
+      return;
+    }
+    if (c.P.pow2) ab2_launch_pw<T, 1, 2>(c, a, o);
+    else ab2_launch_pw<T, 0, 2>(c, a, o);
+  } else {
+    ab2_launch_pw<T, 1, 4>(c, a, o);
+  }
 }
 
 #undef TC
