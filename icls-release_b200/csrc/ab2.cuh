@@ -347,7 +347,7 @@ T* ab2_ptr(double* q) { return reinterpret_cast<T*>(q); }
 template <typename T, int PW, int MB>
 void ab2_launch_pw(Ctx& c, const MomArgs& a, int o) {
   // rows per block: 32 for the FP32 form (four blocks per SM, shorter
-  // ring prologues), 16 for FP64 (two blocks per SM, more blocks per wave)
+  // ring prologues), 16 for FP64 (three blocks per SM, more blocks per wave)
   const int kc = sizeof(T) == 8 ? 16 : 32, nch = std::max(1, c.P.kmax / kc);
   const dim3 grid((unsigned)((c.P.imax + MX - 1) / MX), (unsigned)((c.P.jmax + MY - 1) / MY), (unsigned)nch);
   static unsigned attr = 0;  // devices this instance's shared-memory limit is raised on
@@ -365,18 +365,14 @@ void ab2_launch_pw(Ctx& c, const MomArgs& a, int o) {
 // the product, so neither the test nor the division is in the kernel.  The
 // FP32 form, held to tolerances rather than to the reference's rounding,
 // always takes the product by the reciprocal (within an ulp of the quotient).
-// MB: blocks per SM the registers are budgeted for (FP64 two, or three with
-// ICLS_AB2_BLOCKS=3; FP32 four)
+// MB: blocks per SM the registers are budgeted for.  FP64 three (80
+// registers, a few spilled: 0.895 -> 0.840 ms at 256^3 against two blocks
+// at 120 registers); FP32 four (64 registers).
 template <typename T>
 void ab2_launch(Ctx& c, const MomArgs& a, int o) {
   if constexpr (sizeof(T) == 8) {
-    if (c.ab2_blocks3) {
-      if (c.P.pow2) ab2_launch_pw<T, 1, 3>(c, a, o);
-      else ab2_launch_pw<T, 0, 3>(c, a, o);
-      return;
-    }
-    if (c.P.pow2) ab2_launch_pw<T, 1, 2>(c, a, o);
-    else ab2_launch_pw<T, 0, 2>(c, a, o);
+    if (c.P.pow2) ab2_launch_pw<T, 1, 3>(c, a, o);
+    else ab2_launch_pw<T, 0, 3>(c, a, o);
   } else {
     ab2_launch_pw<T, 1, 4>(c, a, o);
   }

@@ -258,17 +258,13 @@ int allocate(Ctx& c) {
   // list build included);
   // ICLS_CORREC=shapec: the fused correction one thread per shape-C cell
   // in place of one per interior cell writing the images;
-  // ICLS_MATERIALS=rows1: the materials one row per thread, not two;
-  // ICLS_AB2_BLOCKS=3: the FP64 predictor's registers budgeted for three
-  // blocks per SM instead of two.
+  // ICLS_MATERIALS=rows1: the materials one row per thread, not two.
   const char* ab = std::getenv("ICLS_AB2");
   c.ab2_ring = !(ab && std::strcmp(ab, "tma") == 0);
   const char* cv = std::getenv("ICLS_CORREC");
   c.correc_shapec = cv && std::strcmp(cv, "shapec") == 0;
   const char* mv = std::getenv("ICLS_MATERIALS");
   c.materials_rows1 = mv && std::strcmp(mv, "rows1") == 0;
-  const char* bv = std::getenv("ICLS_AB2_BLOCKS");
-  c.ab2_blocks3 = bv && std::strcmp(bv, "3") == 0;
   const char* av = std::getenv("ICLS_ADV");
   c.adv_column = !(av && std::strcmp(av, "band") == 0);
   // working buffers of a group of drops: as many drops as half the free

@@ -88,7 +88,6 @@ struct Ctx {
   int ab2_nmaps = 0, ab2_next = 0;
   bool ab2_tma_failed = false;  // a map could not be encoded: use the ring
   bool ab2_ring = true;  // FP64 predictor on the cp.async ring (else TMA: ICLS_AB2=tma)
-  bool ab2_blocks3 = false;  // FP64 predictor budgeted for three blocks per SM (ICLS_AB2_BLOCKS=3)
   bool materials_rows1 = false;  // materials one row per thread (ICLS_MATERIALS=rows1)
   bool correc_shapec = false;  // fused correction one thread per shape-C cell (ICLS_CORREC=shapec)
   icls_config cfg;
