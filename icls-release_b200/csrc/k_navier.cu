@@ -364,22 +364,54 @@ __global__ void __launch_bounds__(kNormThreads) k_plane_norm(Params p, const dou
     dsc->norm = s / (1. * (p.imax) * p.jmax);
   }
 }
-// pnew and pold in the form's field type T (the arithmetic in FP64)
+// pnew and pold in the form's field type T (the arithmetic in FP64), two
+// consecutive cells per thread through vector loads and stores (the
+// buffers are 256-byte aligned and n is even); the same expressions per cell
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<float> {
+  typedef float2 type;
+};
+template <>
+struct Vec2<double> {
+  typedef double2 type;
+};
+template <typename T>
+__device__ __forceinline__ void pupdate_pair(double p0, double p1, T o0, T o1, T& n0, T& n1, T& d0, T& d1,
+                                             int first, int normalise, double norm, double norm_old) {
+  if (!normalise) {
+    d0 = o0; d1 = o1;
+    n0 = TC(p0); n1 = TC(p1);
+    return;
+  }
+  const double a = (double)o0, b = (double)o1;
+  d0 = TC(first ? a - norm : (a + norm_old) - norm);
+  d1 = TC(first ? b - norm : (b + norm_old) - norm);
+  n0 = TC(p0 - norm);
+  n1 = TC(p1 - norm);
+}
 template <typename T>
 __global__ void __launch_bounds__(NT) k_pupdate(Params p, const double* __restrict__ pp,
                                                 T* __restrict__ pnew, T* __restrict__ pold, int first,
                                                 int normalise, const DevScalars* __restrict__ dsc) {
-  const long long n = blockIdx.x * (long long)NT + threadIdx.x;
+  typedef typename Vec2<T>::type T2;
+  const long long n = 2 * (blockIdx.x * (long long)NT + threadIdx.x);
   if (n >= p.nC) return;
-  if (!normalise) {
-    pold[n] = pnew[n];
-    pnew[n] = TC(pp[n]);
-    return;
+  const double norm = normalise ? dsc->norm : 0., norm_old = normalise ? dsc->norm_old : 0.;
+  if (n + 1 < p.nC) {
+    const double2 pv = *reinterpret_cast<const double2*>(pp + n);
+    const T2 ov = *reinterpret_cast<const T2*>(pnew + n);
+    T2 nv, dv;
+    pupdate_pair<T>(pv.x, pv.y, ov.x, ov.y, nv.x, nv.y, dv.x, dv.y, first, normalise, norm, norm_old);
+    *reinterpret_cast<T2*>(pold + n) = dv;
+    *reinterpret_cast<T2*>(pnew + n) = nv;
+  } else {  // an odd last cell
+    T n0, n1, d0, d1;
+    pupdate_pair<T>(pp[n], 0., pnew[n], TC(0.), n0, n1, d0, d1, first, normalise, norm, norm_old);
+    pold[n] = d0;
+    pnew[n] = n0;
   }
-  const double norm = dsc->norm;
-  const double po = (double)pnew[n];
-  pold[n] = TC(first ? po - norm : (po + dsc->norm_old) - norm);
-  pnew[n] = TC(pp[n] - norm);
 }
 
 // ---- reductions ------------------------------------------------------------
@@ -628,10 +660,10 @@ void launch_pressure_update(Ctx& c, int first) {
   const int norm = c.P.bcy == ICLS_BCY_PERIODIC || c.P.bcy == ICLS_BCY_WALLS;
   if (norm) k_plane_norm<<<1, kNormThreads, 0, c.s>>>(c.P, c.p, c.dsc);
   if (c.P.f32)
-    k_pupdate<float><<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, fp<float>(c.pnew), fp<float>(c.pold), first, norm,
+    k_pupdate<float><<<nblocks((c.P.nC + 1) / 2), NT, 0, c.s>>>(c.P, c.p, fp<float>(c.pnew), fp<float>(c.pold), first, norm,
                                                        c.dsc);
   else
-    k_pupdate<double><<<nblocks(c.P.nC), NT, 0, c.s>>>(c.P, c.p, c.pnew, c.pold, first, norm, c.dsc);
+    k_pupdate<double><<<nblocks((c.P.nC + 1) / 2), NT, 0, c.s>>>(c.P, c.p, c.pnew, c.pold, first, norm, c.dsc);
 }
 void launch_stream_vel(Ctx& c) {
   Scope sc_(c.prof, c.s, "stream_vel", 2);
