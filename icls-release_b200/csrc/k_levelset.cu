@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(NT) k_band_extents(Params p, const T* __restri
 // 15 axial neighbours clip to +-NB, so the test stops at the first that
 // does not (the reference's sums of |clip|-NB <= 0 are zero exactly then).
 template <typename T>
-__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 4 : 3)) k_tube(Params p, const __grid_constant__ LsBatch B,
+__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 5 : 4)) k_tube(Params p, const __grid_constant__ LsBatch B,
                                              long long* __restrict__ cnt, int* __restrict__ bbox_lo,
                                              int* __restrict__ bbox_hi) {
   const int ti = task_of(B);
@@ -326,7 +326,7 @@ __device__ __forceinline__ T adv_rhs(const Params& p, const Axial19<T>& S, T vu,
   return (udfdx + vdfdy) + wdfdz;
 }
 template <int SCHEME, typename T, int PW>
-__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 4 : 3)) k_adv_stage(Params p, const __grid_constant__ LsBatch B, int stage1,
+__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 5 : 4)) k_adv_stage(Params p, const __grid_constant__ LsBatch B, int stage1,
                                                      double a_, double bb_, double fdt_, const T* __restrict__ vu,
                                                      const T* __restrict__ vv, const T* __restrict__ vw) {
   const int ti = task_of(B);
@@ -608,7 +608,7 @@ __device__ __forceinline__ T reinit_val(const Params& p, int stage, const T* __r
 // One SSP-RK3 stage of ls_reinit over the tasks' regions; stage 3 folds
 // max|phi_new - phi_0| into the drop's residual.  out may equal phi0.
 template <typename T, int PW>
-__global__ void __launch_bounds__(NT, 2) k_reinit_stage(Params p, const __grid_constant__ LsBatch B, int stage,
+__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 3 : 2)) k_reinit_stage(Params p, const __grid_constant__ LsBatch B, int stage,
                                                         double dtau_, ReinitState* __restrict__ rs) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
