@@ -534,6 +534,12 @@ __device__ __forceinline__ double urand(unsigned long long seed, unsigned long l
 }
 
 __constant__ double cPu[270];  // the least-squares pseudo-inverse for unit spacing
+__constant__ float cPuf[270];  // the same rounded to FP32 (the FP32 features)
+template <typename R>
+__device__ __forceinline__ R cpu_coef(int q) {
+  if constexpr (sizeof(R) == 4) return cPuf[q];
+  else return (R)cPu[q];
+}
 
 // The network's inputs from a stencil f (phi(x + o) - phi(x), in cells,
 // o in {-1,0,1}^3 with z outer): the stencil minus its least-squares linear
@@ -545,7 +551,7 @@ template <typename R>
 __device__ __forceinline__ void mlp_features(const R* f, float* out) {
   R g[3] = {0, 0, 0};
   for (int q = 0; q < 27; ++q)
-    for (int r = 1; r <= 3; ++r) g[r - 1] += (R)cPu[r * 27 + q] * f[q];
+    for (int r = 1; r <= 3; ++r) g[r - 1] += cpu_coef<R>(r * 27 + q) * f[q];
   int q = 0;
   for (int dk = -1; dk <= 1; ++dk)
     for (int dj = -1; dj <= 1; ++dj)
@@ -947,12 +953,17 @@ int launch_mlp_curvature(Ctx& c, const LsBatch& b) {
 // the unit-spacing pseudo-inverse the features and the labels use (once per
 // process and device-wide)
 int mlp_constants() {
-  static bool set = false;
-  if (set) return 0;
+  static unsigned set = 0;  // devices the constants are on
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  if (set & (1u << (dev & 31))) return 0;
   double pu[270];
+  float puf[270];
   pseudo_inverse(1., 1., 1., pu);
+  for (int q = 0; q < 270; ++q) puf[q] = (float)pu[q];
   if (cudaMemcpyToSymbol(cPu, pu, sizeof(pu)) != cudaSuccess) return 1;
-  set = true;
+  if (cudaMemcpyToSymbol(cPuf, puf, sizeof(puf)) != cudaSuccess) return 1;
+  set |= 1u << (dev & 31);
   return 0;
 }
 
