@@ -257,14 +257,12 @@ int allocate(Ctx& c) {
   // band-list split (measured no faster in FP64, slower in FP32, with the
   // list build included);
   // ICLS_CORREC=shapec: the fused correction one thread per shape-C cell
-  // in place of one per interior cell writing the images; ICLS_CORREC=rows1:
-  // one interior cell per thread instead of two rows;
+  // in place of one per interior cell writing the images;
   // ICLS_MATERIALS=rows1: the materials one row per thread, not two.
   const char* ab = std::getenv("ICLS_AB2");
   c.ab2_ring = !(ab && std::strcmp(ab, "tma") == 0);
   const char* cv = std::getenv("ICLS_CORREC");
   c.correc_shapec = cv && std::strcmp(cv, "shapec") == 0;
-  c.correc_rows1 = cv && std::strcmp(cv, "rows1") == 0;
   const char* mv = std::getenv("ICLS_MATERIALS");
   c.materials_rows1 = mv && std::strcmp(mv, "rows1") == 0;
   const char* av = std::getenv("ICLS_ADV");

@@ -89,7 +89,6 @@ struct Ctx {
   bool ab2_tma_failed = false;  // a map could not be encoded: use the ring
   bool ab2_ring = true;  // FP64 predictor on the cp.async ring (else TMA: ICLS_AB2=tma)
   bool materials_rows1 = false;  // materials one row per thread (ICLS_MATERIALS=rows1)
-  bool correc_rows1 = false;  // fused correction one row per thread (ICLS_CORREC=rows1), not two
   bool correc_shapec = false;  // fused correction one thread per shape-C cell (ICLS_CORREC=shapec)
   icls_config cfg;
   Params P;

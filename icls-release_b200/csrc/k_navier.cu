@@ -237,102 +237,6 @@ __global__ void __launch_bounds__(NT) k_correc_own(Params p, CorrArgs a) {
   if (i == 1 && j == 1 && k == 1 && isnan(vv)) a.dsc->nan_flag = 1;
 }
 
-// k_correc_own over two rows per thread (k0 = 2 blockIdx.z + 1 and k0 + 1):
-// every operand of both rows is read before any store, and the upper row's
-// w correction of the row below is the lower row's own; the same
-// expressions per cell as k_correc_own
-template <typename T>
-struct CorrQ {  // the operands of one corr_at
-  T d, jump;
-  double hi, lo;
-};
-template <typename T>
-__device__ __forceinline__ CorrQ<T> corr_ld(const T* __restrict__ d, const double* __restrict__ pp,
-                                           const T* __restrict__ jump, long long c, long long off) {
-  return CorrQ<T>{d[c], jump[c], pp[c + off], pp[c]};
-}
-template <typename T, int RP>
-__device__ __forceinline__ T corr_ev(const Params& p, const CorrQ<T>& q, double dhi) {
-  const double a = p.dt * dhi * ((q.hi - q.lo) - (double)q.jump);
-  const double g = RP == 1 ? a * p.rrho0 : a / p.rho0;
-  if (sizeof(T) == sizeof(double)) return (T)((double)q.d - g);
-  return q.d - (T)g;
-}
-template <typename T, int RP>
-__global__ void __launch_bounds__(NT, 3) k_correc_own2(Params p, CorrArgs a) {
-  const int i = 1 + (int)(blockIdx.x * BX + threadIdx.x), j = 1 + (int)(blockIdx.y * BY + threadIdx.y);
-  const int k0 = 1 + 2 * (int)blockIdx.z;
-  if (i > p.imax || j > p.jmax || k0 > p.kmax) return;
-  const bool two = k0 + 1 <= p.kmax;
-  const long long sy = p.nCx, sz = (long long)p.nCx * p.nCy;
-  const T* __restrict__ du = cT<T>(a.dudt);
-  const T* __restrict__ dv = cT<T>(a.dvdt);
-  const T* __restrict__ dw = cT<T>(a.dwdt);
-  const T* __restrict__ px = cT<T>(a.px);
-  const T* __restrict__ py = cT<T>(a.py);
-  const T* __restrict__ pz = cT<T>(a.pz);
-  const double* __restrict__ pp = a.p;
-  const long long c0 = idxC(p, i, j, k0), c1 = c0 + sz;
-  const long long cu0 = idxC(p, wrapx(p, i - 1), j, k0), cv0 = idxC(p, i, wrapy(p, j - 1), k0);
-  // loads: row k0, its (i-1), (j-1) and (k0-1) operands, then row k0+1's
-  const CorrQ<T> U0 = corr_ld(du, pp, px, c0, 1), V0 = corr_ld(dv, pp, py, c0, sy);
-  const CorrQ<T> W0 = corr_ld(dw, pp, pz, c0, sz);
-  const CorrQ<T> UM0 = corr_ld(du, pp, px, cu0, 1), VM0 = corr_ld(dv, pp, py, cv0, sy);
-  CorrQ<T> WM0 = CorrQ<T>{TC(0.), TC(0.), 0., 0.};
-  if (k0 > 1) WM0 = corr_ld(dw, pp, pz, c0 - sz, sz);
-  CorrQ<T> U1 = U0, V1 = V0, W1 = W0, UM1 = UM0, VM1 = VM0;
-  if (two) {
-    U1 = corr_ld(du, pp, px, c1, 1);
-    V1 = corr_ld(dv, pp, py, c1, sy);
-    W1 = corr_ld(dw, pp, pz, c1, sz);
-    UM1 = corr_ld(du, pp, px, cu0 + sz, 1);
-    VM1 = corr_ld(dv, pp, py, cv0 + sz, sy);
-  }
-  T* u = mT<T>(a.u);
-  T* v = mT<T>(a.v);
-  T* w = mT<T>(a.w);
-  const long long q0 = idxI(p, i, j, k0), szI = (long long)p.imax * p.jmax;
-  // row k0
-  const T uu0 = corr_ev<T, RP>(p, U0, p.dxi), vv0 = corr_ev<T, RP>(p, V0, p.dyi);
-  const T ww0 = (k0 == p.kmax) ? TC(0.) : corr_ev<T, RP>(p, W0, p.dzi);
-  const T wm0 = (k0 == 1) ? TC(0.) : corr_ev<T, RP>(p, WM0, p.dzi);
-  putC(p, u, i, j, k0, uu0);
-  putC(p, v, i, j, k0, vv0);
-  putC(p, w, i, j, k0, ww0);
-  if (k0 == 1) {
-    putC(p, u, i, j, 0, -uu0);
-    putC(p, v, i, j, 0, TC(2. * p.v_lower) - vv0);
-    putC(p, w, i, j, 0, TC(0.));
-  }
-  if (k0 == p.kmax) {  // an odd kmax: the last pair has one row
-    putC(p, u, i, j, p.k1, -uu0);
-    putC(p, v, i, j, p.k1, TC(2. * p.v_upper) - vv0);
-    putC(p, w, i, j, p.k1, wm0);
-  }
-  mT<T>(a.ucc)[q0] = (corr_ev<T, RP>(p, UM0, p.dxi) + uu0) / TC(2.);
-  mT<T>(a.vcc)[q0] = (corr_ev<T, RP>(p, VM0, p.dyi) + vv0) / TC(2.);
-  mT<T>(a.wcc)[q0] = (wm0 + ww0) / TC(2.);
-  if (i == 1 && j == 1 && k0 == 1 && isnan(vv0)) a.dsc->nan_flag = 1;
-  if (!two) return;
-  // row k0 + 1 (>= 2): its (k-1) w correction is row k0's
-  const int k1r = k0 + 1;
-  const T uu1 = corr_ev<T, RP>(p, U1, p.dxi), vv1 = corr_ev<T, RP>(p, V1, p.dyi);
-  const T ww1 = (k1r == p.kmax) ? TC(0.) : corr_ev<T, RP>(p, W1, p.dzi);
-  const T wk0 = corr_ev<T, RP>(p, W0, p.dzi);  // row k0's w correction (k0 < kmax here)
-  putC(p, u, i, j, k1r, uu1);
-  putC(p, v, i, j, k1r, vv1);
-  putC(p, w, i, j, k1r, ww1);
-  if (k1r == p.kmax) {
-    putC(p, u, i, j, p.k1, -uu1);
-    putC(p, v, i, j, p.k1, TC(2. * p.v_upper) - vv1);
-    putC(p, w, i, j, p.k1, wk0);
-  }
-  const long long q1 = q0 + szI;
-  mT<T>(a.ucc)[q1] = (corr_ev<T, RP>(p, UM1, p.dxi) + uu1) / TC(2.);
-  mT<T>(a.vcc)[q1] = (corr_ev<T, RP>(p, VM1, p.dyi) + vv1) / TC(2.);
-  mT<T>(a.wcc)[q1] = (wk0 + ww1) / TC(2.);
-}
-
 // bounduvw (bound.f90:15-177, Dirichl z, periodic x,y) on an existing triple
 template <typename T>
 __global__ void __launch_bounds__(NT) k_bounduvw(Params p, T* __restrict__ u, T* __restrict__ v, T* __restrict__ w) {
@@ -686,18 +590,6 @@ void launch_correc(Ctx& c, int fused_bc) {
   // images (ICLS_CORREC=shapec: one thread per shape-C cell)
   if (fused_bc && !c.correc_shapec) {
     const bool rp = c.P.rho0_pow2 != 0;
-    if (!c.correc_rows1) {  // two rows per thread
-      dim3 g2 = gridI(c.P);
-      g2.z = (g2.z + 1) / 2;
-      if (c.P.f32) {
-        if (rp) k_correc_own2<float, 1><<<g2, kBlock, 0, c.s>>>(c.P, a);
-        else k_correc_own2<float, 0><<<g2, kBlock, 0, c.s>>>(c.P, a);
-      } else {
-        if (rp) k_correc_own2<double, 1><<<g2, kBlock, 0, c.s>>>(c.P, a);
-        else k_correc_own2<double, 0><<<g2, kBlock, 0, c.s>>>(c.P, a);
-      }
-      return;
-    }
     if (c.P.f32) {
       if (rp) k_correc_own<float, 1><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);
       else k_correc_own<float, 0><<<gridI(c.P), kBlock, 0, c.s>>>(c.P, a);

@@ -580,30 +580,3 @@ def test_volumes_beyond_the_per_drop_parameter_limit():
         s.step(1, 0)
     assert np.array_equal(g.volumes()[0], o.volumes()[0])
 
-
-@pytest.mark.parametrize("nk", [32, 33])
-def test_correc_two_rows_bit_identical(monkeypatch, nk):
-    """The fused correction with two rows per thread gives the same bits as
-    one interior cell per thread (ICLS_CORREC=rows1): moving walls, an even
-    and an odd kmax (a last pair of one row), both forms."""
-    from icls_gpu import FP32
-    for prec in (0, FP32):
-        wl = multi_drop(n=32, ndrop=2, seed=9, steps=3, rmin=0.12, rmax=0.14, dt=2e-5)
-        cfg = wl.cfg
-        cfg.ktot = nk
-        cfg.precision = prec
-        ls = init_drops(cfg, wl.centres, wl.radii, wl.all_images)
-        u, v, w = initial_velocity(cfg, wl.shear_v)
-        two = Solver(cfg)
-        monkeypatch.setenv("ICLS_CORREC", "rows1")
-        one = Solver(cfg)
-        monkeypatch.delenv("ICLS_CORREC")
-        for s in (two, one):
-            s.setup(ls, u, v, w)
-        for istep in range(1, 4):
-            two.step(istep, 0)
-            one.step(istep, 0)
-        for name in ("u", "v", "w", "ucc", "vcc", "wcc", "pnew"):
-            assert np.array_equal(two.download(name), one.download(name)), (nk, prec, name)
-        two.close()
-        one.close()
