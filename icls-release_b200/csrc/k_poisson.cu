@@ -1,5 +1,6 @@
 // k_poisson.cu — the pressure Poisson solve of solver2d (solver.f90:68-196),
-// FP64, -fmad=false.
+// FP64, with multiply-add contraction (the transforms and the elimination
+// are held to a tolerance against the oracle, not to its rounding).
 //
 // Forward: real FFT along x of every (j,k) line, then along y of every
 // (i,k) column of those coefficients, with VFFTPACK's contract (fft.f:
@@ -349,12 +350,14 @@ __device__ __forceinline__ double rhs_at(const Params& p, const RhsArgs& r, long
   const T* __restrict__ du = static_cast<const T*>(r.du);
   const T* __restrict__ dv = static_cast<const T*>(r.dv);
   const T* __restrict__ dw = static_cast<const T*>(r.dw);
+  // explicitly rounded operations: this file allows multiply-add
+  // contraction, k_fillps (k_navier.cu) does not
   const double coef = p.rho0 / p.dt;
-  const double vel_x = ((double)du[c] - (double)du[c - 1]) * p.dxi;
-  const double vel_y = ((double)dv[c] - (double)dv[c - p.nCx]) * p.dyi;
-  const double vel_z = ((double)dw[c] - (double)dw[c - (long long)p.nCx * p.nCy]) * p.dzi;
-  double v = coef * ((vel_x + vel_y) + vel_z);
-  if (r.add) v = v + r.pj[c];
+  const double vel_x = __dmul_rn(__dsub_rn((double)du[c], (double)du[c - 1]), p.dxi);
+  const double vel_y = __dmul_rn(__dsub_rn((double)dv[c], (double)dv[c - p.nCx]), p.dyi);
+  const double vel_z = __dmul_rn(__dsub_rn((double)dw[c], (double)dw[c - (long long)p.nCx * p.nCy]), p.dzi);
+  double v = __dmul_rn(coef, __dadd_rn(__dadd_rn(vel_x, vel_y), vel_z));
+  if (r.add) v = __dadd_rn(v, r.pj[c]);
   return v;
 }
 
