@@ -25,6 +25,12 @@ namespace {
 constexpr int NT = 256;
 #define TC(x) static_cast<T>(x)
 
+// acc + a b: one fused multiply-add in the FP32 form (held to tolerances;
+// this file is compiled without contraction), separately rounded in FP64
+// as the reference evaluates it
+__device__ __forceinline__ float mac(float acc, float a, float b) { return __fmaf_rn(a, b, acc); }
+__device__ __forceinline__ double mac(double acc, double a, double b) { return acc + a * b; }
+
 template <typename T>
 __device__ __forceinline__ T coef(int q);
 template <>
@@ -54,7 +60,7 @@ __device__ __forceinline__ T curvature_at(const Params& p, const T* __restrict__
 #pragma unroll
     for (int r = 1; r < 10; ++r)
 #pragma unroll
-      for (int q = 0; q < 27; ++q) x[r] = x[r] + coef<T>(r * 27 + q) * v[q];
+      for (int q = 0; q < 27; ++q) x[r] = mac(x[r], coef<T>(r * 27 + q), v[q]);
   } else {
     int n = 0;
 #pragma unroll 1
@@ -155,7 +161,7 @@ __global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 5 : 4)) k_recurvature(Pa
 #pragma unroll
         for (int dj = -1; dj <= 1; ++dj)
 #pragma unroll
-          for (int di = -1; di <= 1; ++di) acc = acc + coef<T>(q++) * cin[cc + di + dj * sy + dk * sz];
+          for (int di = -1; di <= 1; ++di) acc = mac(acc, coef<T>(q++), cin[cc + di + dj * sy + dk * sz]);
     }
     putC(p, out, c.i, c.j, k, acc);
   }
