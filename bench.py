@@ -114,13 +114,11 @@ ALG_VALUES = {
 MLP_FLOPS_PER_CELL = 2 * (128 * 64 + 128 * 128 + 64 * 128)
 
 # DRAM bytes (read + write) of one launch of the dominant kernel at 256^3,
-# (kernel, FP32 form) -> bytes: ncu's dram__bytes_read.sum + write.sum.
-# FP64: the launch on the 128^3 workload (profiles/k_ab2_fp64_multi_drop_128_12.md)
-# times the 8x cells (the traffic equals the algorithmic bytes there, so it
-# scales with the cells); FP32: the launch at 256^3 itself
-# (profiles/k_ab2_fp32_static_drop_256.md; the predictor's grid and fields do
+# (kernel, FP32 form) -> bytes: ncu's dram__bytes_read.sum + write.sum of the
+# launch at 256^3 (profiles/k_ab2_fp64_static_drop_256.md,
+# profiles/k_ab2_fp32_static_drop_256.md; the predictor's grid and fields do
 # not depend on the drops)
-TRAFFIC = {("ab2", False): 8 * (318.163968e6 + 83.975936e6), ("ab2", True): 1.243471e9 + 0.390145e9}
+TRAFFIC = {("ab2", False): 2.504199e9 + 0.801062e9, ("ab2", True): 1.245101e9 + 0.389982e9}
 
 
 def alg_bytes_per_launch(name, cfg, stats, f32=False):
