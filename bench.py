@@ -115,9 +115,8 @@ MLP_FLOPS_PER_CELL = 2 * (128 * 64 + 128 * 128 + 64 * 128)
 
 # DRAM bytes (read + write) of one launch of the dominant kernel at 256^3,
 # (kernel, FP32 form) -> bytes: ncu's dram__bytes_read.sum + write.sum of the
-# launch at 256^3 (profiles/k_ab2_fp64_static_drop_256.md,
-# profiles/k_ab2_fp32_static_drop_256.md; the predictor's grid and fields do
-# not depend on the drops)
+# launch in a capture of the static_drop_256 workload (the predictor's grid
+# and fields do not depend on the drops)
 TRAFFIC = {("ab2", False): 2.504199e9 + 0.801062e9, ("ab2", True): 1.245101e9 + 0.389982e9}
 
 

@@ -26,8 +26,8 @@
 //                                 rho_u, rho_v, rho_w, duold, dvold, dwold —
 //                                 shape I, box 32 x 16 at (i0, j0, k)
 //
-// The tensor maps cover this GPU's own arrays only; no load uses cluster
-// multicast.  Every box starts at an even x index (32 * tile, element
+// The tensor maps cover this GPU's own arrays only, and each load fills
+// only the issuing CTA's shared memory.  Every box starts at an even x index (32 * tile, element
 // size 8 B), every row pitch is a multiple of 16 B (imax even), and each
 // shared-memory box starts on a 128-byte boundary.  Every mbarrier wait has
 // an iteration limit: on expiry the kernel sets DevScalars::wait_err, thread
@@ -95,7 +95,7 @@ __device__ __forceinline__ void bar_arrive(uint32_t bar) {
 __device__ __forceinline__ void bar_expect(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
-// 3-D tiled TMA load of one box into this CTA's shared memory (no multicast)
+// 3-D tiled TMA load of one box into this CTA's own shared memory
 __device__ __forceinline__ void tma3(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
