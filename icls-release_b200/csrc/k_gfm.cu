@@ -19,7 +19,6 @@ namespace icls {
 
 __constant__ double cP[270];
 __constant__ float cPf[270];  // the same coefficients rounded to FP32
-__constant__ float cPu1[270];  // the pseudo-inverse for unit spacing in FP32 (the network's features)
 
 namespace {
 
@@ -39,11 +38,9 @@ __device__ __forceinline__ double coef<double>(int q) { return cP[q]; }
 template <>
 __device__ __forceinline__ float coef<float>(int q) { return cPf[q]; }
 
-// curvature at an interior cell (interface.f90:57-111); m = |grad phi| or 1.
-// FP32: st, if given, receives the 27 stencil values.
+// curvature at an interior cell (interface.f90:57-111); m = |grad phi| or 1
 template <typename T>
-__device__ __forceinline__ T curvature_at(const Params& p, const T* __restrict__ phi, int i, int j, int k, T& m,
-                                          T* st = nullptr) {
+__device__ __forceinline__ T curvature_at(const Params& p, const T* __restrict__ phi, int i, int j, int k, T& m) {
   const long long c = idxL(p, i, j, k);
   m = TC(1.);
   if (!(fabs(phi[c]) <= TC(p.NB - 1. * p.dz))) return TC(0.);
@@ -60,10 +57,6 @@ __device__ __forceinline__ T curvature_at(const Params& p, const T* __restrict__
     T v[27];
 #pragma unroll
     for (int q = 0; q < 27; ++q) v[q] = phi[c + (q % 3 - 1) + (q / 3 % 3 - 1) * sy + (q / 9 - 1) * sz];
-    if (st) {
-#pragma unroll
-      for (int q = 0; q < 27; ++q) st[q] = v[q];
-    }
 #pragma unroll
     for (int r = 1; r < 10; ++r)
 #pragma unroll
@@ -106,59 +99,32 @@ __device__ __forceinline__ T curvature_at(const Params& p, const T* __restrict__
   return cv;
 }
 
-// The network's 32 inputs of one cell from its 27 stencil values st (the
-// features of mlp_features in k_mlp.cu: (phi(x+o) - phi(x))/dz, minus their
-// least-squares linear part g.o, then g/|g| and two zeros), with the same
-// roundings: multiply-adds fused, IEEE square root and reciprocal.
-__device__ __forceinline__ void network_inputs(const float* st, float rdz, float* __restrict__ X) {
-  float f[27];
-#pragma unroll
-  for (int q = 0; q < 27; ++q) f[q] = __fmul_rn(__fsub_rn(st[q], st[13]), rdz);
-  float g[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-  for (int q = 0; q < 27; ++q)
-#pragma unroll
-    for (int r = 1; r <= 3; ++r) g[r - 1] = __fmaf_rn(cPu1[r * 27 + q], f[q], g[r - 1]);
-  float o[32];
-#pragma unroll
-  for (int q = 0; q < 27; ++q) {
-    const float di = (float)(q % 3 - 1), dj = (float)(q / 3 % 3 - 1), dk = (float)(q / 9 - 1);
-    o[q] = __fsub_rn(f[q], __fmaf_rn(g[2], dk, __fmaf_rn(g[1], dj, __fmul_rn(g[0], di))));
-  }
-  const float n = __fsqrt_rn(__fmaf_rn(g[2], g[2], __fmaf_rn(g[1], g[1], __fmul_rn(g[0], g[0]))));
-  const float rn = n > 0.f ? __fdiv_rn(1.f, n) : 0.f;
-  o[27] = __fmul_rn(g[0], rn);
-  o[28] = __fmul_rn(g[1], rn);
-  o[29] = __fmul_rn(g[2], rn);
-  o[30] = 0.f;
-  o[31] = 0.f;
-  float4* dst = reinterpret_cast<float4*>(X);
-#pragma unroll
-  for (int q = 0; q < 8; ++q) dst[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
-}
-
 // get_curvature + boundc over the tasks' shape-C regions (phi0 = the
 // drop's level set, out = its curvature): wall rows stay 0, halos are the
 // periodic copies (bound.f90:292-305), the apron (far field, |phi| > 5dz)
-// is 0.  With rec, the network's cells (|phi| <= 4dz) get slots from a
-// warp-aggregated counter; in the FP32 form (X given) their 32 inputs are
-// formed here from the stencil the fit has just read.
+// is 0.
 template <typename T>
 __global__ void __launch_bounds__(NT, 4) k_curvature(Params p, const __grid_constant__ LsBatch B, T* __restrict__ nrm_m,
-                                                  MlpCell* __restrict__ rec, int* __restrict__ count, int cap,
-                                                  float* __restrict__ X) {
+                                                  MlpCell* __restrict__ rec, int* __restrict__ count, int cap) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const Col c = col_of(p, t, (int)blockIdx.x - B.start[ti]);
   const T* phi = cT<T>(t.phi0);
   T* out = mT<T>(t.out);
   const T lim = TC(4. * p.dz);
-  const float rdz = (float)(1. / p.dz);
   const unsigned lane = threadIdx.x & 31u;
   // every lane of the warp walks the same rows, so the ballots line up
   for (int k = c.ka; k <= c.kb; ++k) {
-    int slot = -1;  // this cell's network slot, if it has one
-    if (rec) {
+    if (c.ok) {
+      T v = TC(0.);
+      if (k != 0 && k != p.k1 && computed(c, t.r, k)) {
+        T m;
+        v = curvature_at(p, phi, c.i, c.j, k, m);
+        if (nrm_m) nrm_m[idxI(p, c.i, c.j, k)] = m;
+      }
+      putC(p, out, c.i, c.j, k, v);
+    }
+    if (rec) {  // the network's cells: slots by a warp-aggregated counter
       const bool take = c.ok && k >= 1 && k <= p.kmax && computed(c, t.r, k) &&
                         fabs(phi[idxL(p, c.i, c.j, k)]) <= lim;
       const unsigned msk = __ballot_sync(0xffffffffu, take);
@@ -166,29 +132,9 @@ __global__ void __launch_bounds__(NT, 4) k_curvature(Params p, const __grid_cons
         int base = 0;
         if (lane == (unsigned)(__ffs(msk) - 1)) base = atomicAdd(count, __popc(msk));
         base = __shfl_sync(0xffffffffu, base, __ffs(msk) - 1);
-        const int s = base + __popc(msk & ((1u << lane) - 1u));
-        if (take && s < cap) {
-          rec[s] = MlpCell{ti, c.i, c.j, k};
-          slot = s;
-        }
+        const int slot = base + __popc(msk & ((1u << lane) - 1u));
+        if (take && slot < cap) rec[slot] = MlpCell{ti, c.i, c.j, k};
       }
-    }
-    if (c.ok) {
-      T v = TC(0.);
-      if (k != 0 && k != p.k1 && computed(c, t.r, k)) {
-        T m;
-        if constexpr (sizeof(T) == 4) {
-          // a network cell (|phi| <= 4dz) is within the fit's |phi| <= 5dz,
-          // so its stencil has been read
-          T st[27];
-          v = curvature_at(p, phi, c.i, c.j, k, m, st);
-          if (X && slot >= 0) network_inputs(st, rdz, X + (long long)slot * 32);
-        } else {
-          v = curvature_at(p, phi, c.i, c.j, k, m);
-        }
-        if (nrm_m) nrm_m[idxI(p, c.i, c.j, k)] = m;
-      }
-      putC(p, out, c.i, c.j, k, v);
     }
   }
 }
@@ -351,14 +297,10 @@ __global__ void __launch_bounds__(NT) k_ipot_pair(Params p, const __grid_constan
 }  // namespace
 
 void set_pseudo_inverse(const double* P270, cudaStream_t s) {
-  static float f[270], u1[270];
-  static double pu[270];
+  static float f[270];
   for (int q = 0; q < 270; ++q) f[q] = (float)P270[q];
-  pseudo_inverse(1., 1., 1., pu);
-  for (int q = 0; q < 270; ++q) u1[q] = (float)pu[q];
   cudaMemcpyToSymbolAsync(cP, P270, 270 * sizeof(double), 0, cudaMemcpyHostToDevice, s);
   cudaMemcpyToSymbolAsync(cPf, f, 270 * sizeof(float), 0, cudaMemcpyHostToDevice, s);
-  cudaMemcpyToSymbolAsync(cPu1, u1, 270 * sizeof(float), 0, cudaMemcpyHostToDevice, s);
   cudaStreamSynchronize(s);
 }
 
@@ -369,12 +311,11 @@ void launch_curvature(Ctx& c, const LsBatch& b, double* nrm_m_out, bool collect)
   Scope sc_(c.prof, c.s, "curvature", 1);
   MlpCell* rec = collect ? reinterpret_cast<MlpCell*>(c.mlp_rec) : nullptr;
   if (collect) cudaMemsetAsync(c.mlp_count, 0, sizeof(int), c.s);
-  // the FP32 form forms the network's inputs in this sweep (mlp_X)
   if (c.P.f32)
     k_curvature<float><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, reinterpret_cast<float*>(nrm_m_out), rec, c.mlp_count,
-                                                        c.mlp_cap, collect ? c.mlp_X : nullptr);
+                                                        c.mlp_cap);
   else
-    k_curvature<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, nrm_m_out, rec, c.mlp_count, c.mlp_cap, nullptr);
+    k_curvature<double><<<b.start[b.n], kTile, 0, c.s>>>(c.P, b, nrm_m_out, rec, c.mlp_count, c.mlp_cap);
 }
 void launch_recurvature(Ctx& c, const LsBatch& b) {
   if (b.n == 0) return;

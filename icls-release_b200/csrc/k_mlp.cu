@@ -932,9 +932,11 @@ namespace icls {
 int launch_mlp_curvature(Ctx& c, const LsBatch& b) {
   if (b.n == 0) return ICLS_OK;
   if (!c.net) return ICLS_E_STATE;
-  // the FP32 form's inputs were formed by launch_curvature (k_curvature)
-  Scope sc_(c.prof, c.s, "mlp_curvature", c.P.f32 ? 1 : 2);
-  if (!c.P.f32)
+  Scope sc_(c.prof, c.s, "mlp_curvature", 2);
+  if (c.P.f32)
+    k_mlp_features<float><<<4 * 148, 256, 0, c.s>>>(c.P, b, (const MlpCell*)c.mlp_rec, c.mlp_count, c.mlp_cap,
+                                                    c.mlp_X);
+  else
     k_mlp_features<double><<<4 * 148, 256, 0, c.s>>>(c.P, b, (const MlpCell*)c.mlp_rec, c.mlp_count, c.mlp_cap,
                                                      c.mlp_X);
   const int grid = std::min((c.mlp_cap + kRows - 1) / kRows, 2 * 148);
