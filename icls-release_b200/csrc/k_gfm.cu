@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(NT, 4) k_curvature(Params p, const __grid_cons
 // re_curvature + boundc (interface.f90:186-218) over the tasks' regions:
 // phis (get_curvature) -> out
 template <typename T>
-__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 5 : 4)) k_recurvature(Params p, const __grid_constant__ LsBatch B) {
+__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 6 : 5)) k_recurvature(Params p, const __grid_constant__ LsBatch B) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
   const T* __restrict__ cin = cT<T>(t.phis);
@@ -219,7 +219,7 @@ __device__ __forceinline__ double axis_jump(const Params& p, const T* __restrict
 // the reference's exactly (0+a+b is exact in either order); a cell in the
 // shells of three or more drops may differ in the last bit.
 template <typename T>
-__global__ void __launch_bounds__(NT, 4) k_jumps(Params p, const __grid_constant__ LsBatch B,
+__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 5 : 4)) k_jumps(Params p, const __grid_constant__ LsBatch B,
                                               double* __restrict__ pjump, T* __restrict__ px,
                                               T* __restrict__ py, T* __restrict__ pz) {
   const int ti = task_of(B);

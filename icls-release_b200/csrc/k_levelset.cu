@@ -608,7 +608,7 @@ __device__ __forceinline__ T reinit_val(const Params& p, int stage, const T* __r
 // One SSP-RK3 stage of ls_reinit over the tasks' regions; stage 3 folds
 // max|phi_new - phi_0| into the drop's residual.  out may equal phi0.
 template <typename T, int PW>
-__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 3 : 2)) k_reinit_stage(Params p, const __grid_constant__ LsBatch B, int stage,
+__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 4 : 3)) k_reinit_stage(Params p, const __grid_constant__ LsBatch B, int stage,
                                                         double dtau_, ReinitState* __restrict__ rs) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
@@ -801,7 +801,7 @@ __device__ __forceinline__ void min_into(float* a, float v) {
   }
 }
 template <typename T>
-__global__ void __launch_bounds__(NT) k_heaviside(Params p, const __grid_constant__ LsBatch B,
+__global__ void __launch_bounds__(NT, 4) k_heaviside(Params p, const __grid_constant__ LsBatch B,
                                                   T* __restrict__ jiemian, XSum* __restrict__ part, int cap) {
   const int ti = task_of(B);
   const LsTask& t = B.t[ti];
