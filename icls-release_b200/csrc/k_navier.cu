@@ -195,7 +195,7 @@ __device__ __forceinline__ T corr_at(const Params& p, const T* __restrict__ d, c
 // every warp is a full row segment and no thread recomputes a source
 // column's corrections for a halo cell.
 template <typename T, int RP>
-__global__ void __launch_bounds__(NT) k_correc_own(Params p, CorrArgs a) {
+__global__ void __launch_bounds__(NT, (sizeof(T) == 4 ? 8 : 5)) k_correc_own(Params p, CorrArgs a) {
   int i, j, k;
   if (!cell3(kI0, cI1(p).v, i, j, k)) return;
   const long long sy = p.nCx, sz = (long long)p.nCx * p.nCy;
