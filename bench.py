@@ -322,6 +322,14 @@ def step_roofline(roof, ms_step):
     roof["step_frac"] = (b / (ms_step / 1000.0) / 1e9 / peak) if ms_step > 0 else None
 
 
+def dominant_scope(table):
+    """The roofline's dominant kernel: the largest scope of one kernel launch
+    (solver2d, for one, is five kernels: the x and y transforms both ways
+    and the z sweeps); the largest scope if none is single."""
+    single = {k: e for k, e in table.items() if e["timed"] > 0 and e["launches"] == e["timed"]}
+    return max((single or table).items(), key=lambda kv: kv[1]["ms"])
+
+
 def kernel_table(s, args, cfg, stats, istep, f32, mlp_cells=None):
     """K more steps with every launcher scope bracketed by CUDA events: the
     per-kernel shares and the roofline of the dominant one.  The network's
@@ -335,11 +343,7 @@ def kernel_table(s, args, cfg, stats, istep, f32, mlp_cells=None):
     table = s.profile_table()
     s.profile(False)
     tot = sum(e["ms"] for e in table.values()) or 1.0
-    # the dominant kernel: the largest scope of one kernel launch (solver2d,
-    # for one, is five kernels: the x and y transforms both ways and the z
-    # sweeps)
-    single = {k: e for k, e in table.items() if e["timed"] > 0 and e["launches"] == e["timed"]}
-    name, ent = max((single or table).items(), key=lambda kv: kv[1]["ms"])
+    name, ent = dominant_scope(table)
     per_launch_ms = ent["ms"] / max(ent["timed"], 1)
     alg = alg_bytes_per_launch(name, cfg, stats, f32)
     peaks = load_peaks()

@@ -51,3 +51,17 @@ def test_reference_arm_under_torchrun_prints_once():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "port"
+
+
+def test_dominant_kernel_is_a_single_kernel_scope():
+    """The roofline's dominant kernel is the largest scope of one kernel
+    launch: a multi-kernel scope (the five passes of solver2d) that takes
+    longer is passed over; with no single-kernel scope the largest stands."""
+    sys.path.insert(0, ROOT)
+    import bench
+    table = {"solver2d": {"ms": 10.0, "launches": 100, "timed": 20},
+             "ab2": {"ms": 9.8, "launches": 20, "timed": 20},
+             "adv_stage": {"ms": 6.0, "launches": 60, "timed": 60},
+             "unused": {"ms": 0.0, "launches": 0, "timed": 0}}
+    assert bench.dominant_scope(table)[0] == "ab2"
+    assert bench.dominant_scope({"solver2d": table["solver2d"]})[0] == "solver2d"
